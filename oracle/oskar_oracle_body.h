@@ -1,0 +1,540 @@
+/*
+ * Precision-generic body of the CPU oracle (TEST INFRASTRUCTURE ONLY).
+ * Included twice by oskar_oracle.c with REAL/S/ORC_SIN/... defined for
+ * double and for float. Each function states the reference code it restates.
+ */
+
+typedef struct { REAL re, im; } ORC_T(cx);
+typedef struct { ORC_T(cx) a, b, c, d; } ORC_T(mat);
+
+static inline ORC_T(cx) ORC_T(cmul)(ORC_T(cx) x, ORC_T(cx) y)
+{
+    ORC_T(cx) r;
+    r.re = x.re * y.re - x.im * y.im;
+    r.im = x.re * y.im + x.im * y.re;
+    return r;
+}
+
+/* x * conj(y) */
+static inline ORC_T(cx) ORC_T(cmulc)(ORC_T(cx) x, ORC_T(cx) y)
+{
+    ORC_T(cx) r;
+    r.re = x.re * y.re + x.im * y.im;
+    r.im = x.im * y.re - x.re * y.im;
+    return r;
+}
+
+static inline ORC_T(cx) ORC_T(cadd)(ORC_T(cx) x, ORC_T(cx) y)
+{
+    ORC_T(cx) r; r.re = x.re + y.re; r.im = x.im + y.im; return r;
+}
+
+static inline ORC_T(mat) ORC_T(load_mat)(const REAL* p)
+{
+    ORC_T(mat) m;
+    m.a.re = p[0]; m.a.im = p[1]; m.b.re = p[2]; m.b.im = p[3];
+    m.c.re = p[4]; m.c.im = p[5]; m.d.re = p[6]; m.d.im = p[7];
+    return m;
+}
+
+/*
+ * J * B for the Hermitian brightness matrix
+ * B = [[I+Q, U+iV], [U-iV, I-Q]]
+ * (correlate/define_correlate_utils.h:36-39 builds B;
+ *  math/define_multiply.h:74-87 multiplies by it).
+ */
+static inline ORC_T(mat) ORC_T(mul_brightness)(ORC_T(mat) J, REAL I, REAL Q,
+        REAL U, REAL V)
+{
+    ORC_T(mat) r;
+    ORC_T(cx) buv, buv_c;
+    const REAL xx = I + Q, yy = I - Q;
+    buv.re = U; buv.im = V;       /* B.b */
+    buv_c.re = U; buv_c.im = -V;  /* B.c = conj(B.b) */
+    r.a.re = J.a.re * xx; r.a.im = J.a.im * xx;
+    r.a = ORC_T(cadd)(r.a, ORC_T(cmul)(J.b, buv_c));
+    r.c.re = J.c.re * xx; r.c.im = J.c.im * xx;
+    r.c = ORC_T(cadd)(r.c, ORC_T(cmul)(J.d, buv_c));
+    r.b.re = J.b.re * yy; r.b.im = J.b.im * yy;
+    r.b = ORC_T(cadd)(r.b, ORC_T(cmul)(J.a, buv));
+    r.d.re = J.d.re * yy; r.d.im = J.d.im * yy;
+    r.d = ORC_T(cadd)(r.d, ORC_T(cmul)(J.c, buv));
+    return r;
+}
+
+/* M * N^H (math/define_multiply.h:54-67). */
+static inline ORC_T(mat) ORC_T(mul_herm)(ORC_T(mat) M, ORC_T(mat) N)
+{
+    ORC_T(mat) r;
+    r.a = ORC_T(cadd)(ORC_T(cmulc)(M.a, N.a), ORC_T(cmulc)(M.b, N.b));
+    r.c = ORC_T(cadd)(ORC_T(cmulc)(M.c, N.a), ORC_T(cmulc)(M.d, N.b));
+    r.b = ORC_T(cadd)(ORC_T(cmulc)(M.a, N.c), ORC_T(cmulc)(M.b, N.d));
+    r.d = ORC_T(cadd)(ORC_T(cmulc)(M.c, N.c), ORC_T(cmulc)(M.d, N.d));
+    return r;
+}
+
+/* sinc used for smearing (utility/oskar_kernel_macros.h:281). */
+static inline REAL ORC_T(sinc)(REAL x)
+{
+    return x == (REAL)0 ? (REAL)1 : ORC_SIN(x) / x;
+}
+
+/*
+ * Per-baseline terms: uu, vv, ww in wavelengths scaled by pi*frac_bandwidth,
+ * the Gaussian quadratic-form terms and the uv length
+ * (correlate/define_correlate_utils.h:5-13).
+ */
+typedef struct {
+    REAL uu, vv, ww, uu2, vv2, uuvv, uv_len, du, dv, dw;
+} ORC_T(bl);
+
+static inline ORC_T(bl) ORC_T(baseline_terms)(int p, int q,
+        const REAL* st_u, const REAL* st_v, const REAL* st_w,
+        const REAL* st_x, const REAL* st_y, REAL inv_wavelength,
+        REAL frac_bandwidth, int time_smearing, REAL time_int_sec,
+        REAL gha0_rad, REAL dec0_rad)
+{
+    ORC_T(bl) t;
+    REAL f;
+    t.uu = (st_u[p] - st_u[q]) * inv_wavelength;
+    t.vv = (st_v[p] - st_v[q]) * inv_wavelength;
+    t.ww = (st_w[p] - st_w[q]) * inv_wavelength;
+    t.uu2 = t.uu * t.uu;
+    t.vv2 = t.vv * t.vv;
+    t.uv_len = ORC_SQRT((REAL)(t.uu2 + t.vv2));
+    t.uuvv = 2 * t.uu * t.vv;
+    f = ((REAL) ORC_PI) * frac_bandwidth;
+    t.uu *= f; t.vv *= f; t.ww *= f;
+    t.du = t.dv = t.dw = 0;
+    if (time_smearing)
+    {
+        /* Rotation of the baseline during the averaging time
+         * (correlate/define_correlate_utils.h:15-27). */
+        const REAL s_ha = ORC_SIN(gha0_rad), c_ha = ORC_COS(gha0_rad);
+        const REAL s_dec = ORC_SIN(dec0_rad), c_dec = ORC_COS(dec0_rad);
+        const REAL k = ((REAL) ORC_PI) * inv_wavelength;
+        const REAL xx = (st_x[p] - st_x[q]) * k;
+        const REAL yy = (st_y[p] - st_y[q]) * k;
+        const REAL rot = ((REAL) ORC_OMEGA_EARTH) * time_int_sec;
+        const REAL tmp = (xx * s_ha + yy * c_ha) * rot;
+        t.du = (xx * c_ha - yy * s_ha) * rot;
+        t.dv = tmp * s_dec;
+        t.dw = -tmp * c_dec;
+    }
+    return t;
+}
+
+/* Smearing factor of one source on one baseline
+ * (correlate/oskar_cross_correlate_omp.cpp:100-124). */
+static inline REAL ORC_T(smearing)(const ORC_T(bl)* t, int i, int gaussian,
+        int bw, int ts, const REAL* l, const REAL* m, const REAL* n,
+        const REAL* a, const REAL* b, const REAL* c)
+{
+    REAL s = 1;
+    if (gaussian)
+    {
+        const REAL e = a[i] * t->uu2 + b[i] * t->uuvv + c[i] * t->vv2;
+        s = ORC_EXP((REAL) -e);
+    }
+    if (bw || ts)
+    {
+        const REAL ll = l[i], mm = m[i], nn = n[i] - (REAL)1;
+        if (bw) s *= ORC_T(sinc)(t->uu * ll + t->vv * mm + t->ww * nn);
+        if (ts) s *= ORC_T(sinc)(t->du * ll + t->dv * mm + t->dw * nn);
+    }
+    return s;
+}
+
+static inline int ORC_T(bl_index)(int num_st, int p, int q)
+{
+    return q * (num_st - 1) - (q - 1) * q / 2 + p - q - 1;
+}
+
+/*
+ * Matrix cross-correlation: vis[bl] += sum_s smear * J_p B J_q^H.
+ * Restates correlate/oskar_cross_correlate_omp.cpp:27-156 (kernel selection
+ * by frac_bandwidth / time_int_sec as in XCORR_SELECT, :172-180). Single
+ * precision uses Kahan summation as the reference does (:140-148).
+ */
+void ORC_FN(orc_xcorr_matrix)(int casa, int gaussian, int num_src,
+        int num_st, int offset_out, const REAL* jones, const REAL* I,
+        const REAL* Q, const REAL* U, const REAL* V, const REAL* l,
+        const REAL* m, const REAL* n, const REAL* a, const REAL* b,
+        const REAL* c, const REAL* st_u, const REAL* st_v, const REAL* st_w,
+        const REAL* st_x, const REAL* st_y, REAL uv_min_lambda,
+        REAL uv_max_lambda, REAL inv_wavelength, REAL frac_bandwidth,
+        REAL time_int_sec, REAL gha0_rad, REAL dec0_rad, REAL* vis)
+{
+    const int bw = (frac_bandwidth != (REAL)0), ts = (time_int_sec != (REAL)0);
+    int q;
+#pragma omp parallel for schedule(dynamic, 1)
+    for (q = 0; q < num_st; ++q)
+    {
+        int p;
+        for (p = q + 1; p < num_st; ++p)
+        {
+            REAL sum[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+            REAL guard[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+            const int first = casa ? q : p, second = casa ? p : q;
+            const REAL* jp = jones + 8 * (size_t) num_src * first;
+            const REAL* jq = jones + 8 * (size_t) num_src * second;
+            const ORC_T(bl) t = ORC_T(baseline_terms)(p, q, st_u, st_v, st_w,
+                    st_x, st_y, inv_wavelength, frac_bandwidth, ts,
+                    time_int_sec, gha0_rad, dec0_rad);
+            int i, k;
+            if (t.uv_len < uv_min_lambda || t.uv_len > uv_max_lambda)
+                continue;
+            for (i = 0; i < num_src; ++i)
+            {
+                const REAL s = ORC_T(smearing)(&t, i, gaussian, bw, ts,
+                        l, m, n, a, b, c);
+                const ORC_T(mat) mb = ORC_T(mul_brightness)(
+                        ORC_T(load_mat)(jp + 8 * (size_t) i),
+                        I[i], Q[i], U[i], V[i]);
+                const ORC_T(mat) r = ORC_T(mul_herm)(mb,
+                        ORC_T(load_mat)(jq + 8 * (size_t) i));
+                const REAL term[8] = {r.a.re, r.a.im, r.b.re, r.b.im,
+                        r.c.re, r.c.im, r.d.re, r.d.im};
+                for (k = 0; k < 8; ++k)
+                {
+                    if (ORC_KAHAN)
+                    {
+                        const REAL y = term[k] * s - guard[k];
+                        const REAL tt = sum[k] + y;
+                        guard[k] = (tt - sum[k]) - y;
+                        sum[k] = tt;
+                    }
+                    else sum[k] += term[k] * s;
+                }
+            }
+            {
+                REAL* out = vis + 8 * (size_t) (
+                        ORC_T(bl_index)(num_st, p, q) + offset_out);
+                for (k = 0; k < 8; ++k) out[k] += sum[k];
+            }
+        }
+    }
+}
+
+/*
+ * Scalar cross-correlation: vis[bl] += sum_s smear * I_s * J_p conj(J_q).
+ * Restates the scalar CPU kernel (correlate/define_cross_correlate.h:157-187,
+ * instantiated in correlate/src/oskar_cross_correlate_scalar_omp.cpp).
+ */
+void ORC_FN(orc_xcorr_scalar)(int casa, int gaussian, int num_src,
+        int num_st, int offset_out, const REAL* jones, const REAL* I,
+        const REAL* Q, const REAL* U, const REAL* V, const REAL* l,
+        const REAL* m, const REAL* n, const REAL* a, const REAL* b,
+        const REAL* c, const REAL* st_u, const REAL* st_v, const REAL* st_w,
+        const REAL* st_x, const REAL* st_y, REAL uv_min_lambda,
+        REAL uv_max_lambda, REAL inv_wavelength, REAL frac_bandwidth,
+        REAL time_int_sec, REAL gha0_rad, REAL dec0_rad, REAL* vis)
+{
+    const int bw = (frac_bandwidth != (REAL)0), ts = (time_int_sec != (REAL)0);
+    int q;
+    (void) Q; (void) U; (void) V;
+#pragma omp parallel for schedule(dynamic, 1)
+    for (q = 0; q < num_st; ++q)
+    {
+        int p;
+        for (p = q + 1; p < num_st; ++p)
+        {
+            REAL sre = 0, sim = 0;
+            const int first = casa ? q : p, second = casa ? p : q;
+            const REAL* jp = jones + 2 * (size_t) num_src * first;
+            const REAL* jq = jones + 2 * (size_t) num_src * second;
+            const ORC_T(bl) t = ORC_T(baseline_terms)(p, q, st_u, st_v, st_w,
+                    st_x, st_y, inv_wavelength, frac_bandwidth, ts,
+                    time_int_sec, gha0_rad, dec0_rad);
+            int i;
+            if (t.uv_len < uv_min_lambda || t.uv_len > uv_max_lambda)
+                continue;
+            for (i = 0; i < num_src; ++i)
+            {
+                const REAL s = ORC_T(smearing)(&t, i, gaussian, bw, ts,
+                        l, m, n, a, b, c) * I[i];
+                ORC_T(cx) x, y;
+                x.re = jp[2 * i]; x.im = jp[2 * i + 1];
+                y.re = jq[2 * i]; y.im = jq[2 * i + 1];
+                x = ORC_T(cmulc)(x, y);
+                sre += x.re * s;
+                sim += x.im * s;
+            }
+            {
+                REAL* out = vis + 2 * (size_t) (
+                        ORC_T(bl_index)(num_st, p, q) + offset_out);
+                out[0] += sre; out[1] += sim;
+            }
+        }
+    }
+}
+
+/* Auto-correlation, matrix form (correlate/define_auto_correlate.h:36-57). */
+void ORC_FN(orc_acorr_matrix)(int num_src, int num_st, int offset_out,
+        const REAL* jones, const REAL* I, const REAL* Q, const REAL* U,
+        const REAL* V, REAL* vis)
+{
+    int s;
+#pragma omp parallel for
+    for (s = 0; s < num_st; ++s)
+    {
+        REAL sum[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+        const REAL* js = jones + 8 * (size_t) num_src * s;
+        int i, k;
+        for (i = 0; i < num_src; ++i)
+        {
+            const ORC_T(mat) j = ORC_T(load_mat)(js + 8 * (size_t) i);
+            const ORC_T(mat) r = ORC_T(mul_herm)(
+                    ORC_T(mul_brightness)(j, I[i], Q[i], U[i], V[i]), j);
+            sum[0] += r.a.re; sum[1] += r.a.im; sum[2] += r.b.re;
+            sum[3] += r.b.im; sum[4] += r.c.re; sum[5] += r.c.im;
+            sum[6] += r.d.re; sum[7] += r.d.im;
+        }
+        sum[1] = sum[7] = 0;
+        for (k = 0; k < 8; ++k) vis[8 * (size_t) (s + offset_out) + k] += sum[k];
+    }
+}
+
+/* Auto-correlation, scalar form (correlate/define_auto_correlate.h:84-101). */
+void ORC_FN(orc_acorr_scalar)(int num_src, int num_st, int offset_out,
+        const REAL* jones, const REAL* I, REAL* vis)
+{
+    int s;
+#pragma omp parallel for
+    for (s = 0; s < num_st; ++s)
+    {
+        REAL sum = 0;
+        const REAL* js = jones + 2 * (size_t) num_src * s;
+        int i;
+        for (i = 0; i < num_src; ++i)
+            sum += (js[2 * i] * js[2 * i] + js[2 * i + 1] * js[2 * i + 1])
+                    * I[i];
+        vis[2 * (size_t) (s + offset_out)] += sum;
+    }
+}
+
+/*
+ * Interferometer phase K[station][source] = exp(i * wavenumber *
+ * (u l + v m + w (n - 1))), zero where the filter value is outside
+ * (filter_min, filter_max]
+ * (interferometer/define_evaluate_jones_K.h:56-70).
+ */
+void ORC_FN(orc_jones_k)(int num_src, const REAL* l, const REAL* m,
+        const REAL* n, int num_st, const REAL* u, const REAL* v,
+        const REAL* w, REAL wavenumber, const REAL* filter,
+        REAL filter_min, REAL filter_max, int ignore_w, REAL* jones)
+{
+    int a;
+#pragma omp parallel for
+    for (a = 0; a < num_st; ++a)
+    {
+        int s;
+        for (s = 0; s < num_src; ++s)
+        {
+            REAL re = 0, im = 0;
+            if (filter[s] > filter_min && filter[s] <= filter_max)
+            {
+                REAL ph = u[a] * l[s] + v[a] * m[s];
+                if (!ignore_w) ph += w[a] * (n[s] - (REAL)1);
+                ph *= wavenumber;
+                im = ORC_SIN(ph);
+                re = ORC_COS(ph);
+            }
+            jones[2 * ((size_t) s + (size_t) num_src * a)] = re;
+            jones[2 * ((size_t) s + (size_t) num_src * a) + 1] = im;
+        }
+    }
+}
+
+/* Element-wise products used by oskar_jones_join / oskar_mem_multiply
+ * (mem/define_mem_multiply.h:14-89). */
+void ORC_FN(orc_mem_mul_cc_c)(int n, const REAL* a, const REAL* b, REAL* c)
+{
+    int i;
+    for (i = 0; i < n; ++i)
+    {
+        ORC_T(cx) x, y, r;
+        x.re = a[2 * i]; x.im = a[2 * i + 1];
+        y.re = b[2 * i]; y.im = b[2 * i + 1];
+        r = ORC_T(cmul)(x, y);
+        c[2 * i] = r.re; c[2 * i + 1] = r.im;
+    }
+}
+
+void ORC_FN(orc_mem_mul_cc_m)(int n, const REAL* a, const REAL* b, REAL* c)
+{
+    int i;
+    for (i = 0; i < n; ++i)
+    {
+        ORC_T(cx) x, y, r;
+        x.re = a[2 * i]; x.im = a[2 * i + 1];
+        y.re = b[2 * i]; y.im = b[2 * i + 1];
+        r = ORC_T(cmul)(x, y);
+        c[8 * i + 0] = r.re; c[8 * i + 1] = r.im;
+        c[8 * i + 2] = 0; c[8 * i + 3] = 0;
+        c[8 * i + 4] = 0; c[8 * i + 5] = 0;
+        c[8 * i + 6] = r.re; c[8 * i + 7] = r.im;
+    }
+}
+
+/* complex scalar (a) times matrix (b) */
+void ORC_FN(orc_mem_mul_cm_m)(int n, const REAL* a, const REAL* b, REAL* c)
+{
+    int i, k;
+    for (i = 0; i < n; ++i)
+    {
+        ORC_T(cx) s;
+        s.re = a[2 * i]; s.im = a[2 * i + 1];
+        for (k = 0; k < 4; ++k)
+        {
+            ORC_T(cx) x, r;
+            x.re = b[8 * i + 2 * k]; x.im = b[8 * i + 2 * k + 1];
+            r = ORC_T(cmul)(x, s);
+            c[8 * i + 2 * k] = r.re; c[8 * i + 2 * k + 1] = r.im;
+        }
+    }
+}
+
+/* matrix (a) times complex scalar (b) */
+void ORC_FN(orc_mem_mul_mc_m)(int n, const REAL* a, const REAL* b, REAL* c)
+{
+    int i, k;
+    for (i = 0; i < n; ++i)
+    {
+        ORC_T(cx) s;
+        s.re = b[2 * i]; s.im = b[2 * i + 1];
+        for (k = 0; k < 4; ++k)
+        {
+            ORC_T(cx) x, r;
+            x.re = a[8 * i + 2 * k]; x.im = a[8 * i + 2 * k + 1];
+            r = ORC_T(cmul)(x, s);
+            c[8 * i + 2 * k] = r.re; c[8 * i + 2 * k + 1] = r.im;
+        }
+    }
+}
+
+/* matrix (a) times matrix (b) */
+void ORC_FN(orc_mem_mul_mm_m)(int n, const REAL* a, const REAL* b, REAL* c)
+{
+    int i;
+    for (i = 0; i < n; ++i)
+    {
+        const ORC_T(mat) x = ORC_T(load_mat)(a + 8 * (size_t) i);
+        const ORC_T(mat) y = ORC_T(load_mat)(b + 8 * (size_t) i);
+        ORC_T(mat) r;
+        r.a = ORC_T(cadd)(ORC_T(cmul)(x.a, y.a), ORC_T(cmul)(x.b, y.c));
+        r.c = ORC_T(cadd)(ORC_T(cmul)(x.c, y.a), ORC_T(cmul)(x.d, y.c));
+        r.b = ORC_T(cadd)(ORC_T(cmul)(x.a, y.b), ORC_T(cmul)(x.b, y.d));
+        r.d = ORC_T(cadd)(ORC_T(cmul)(x.c, y.b), ORC_T(cmul)(x.d, y.d));
+        c[8 * i + 0] = r.a.re; c[8 * i + 1] = r.a.im;
+        c[8 * i + 2] = r.b.re; c[8 * i + 3] = r.b.im;
+        c[8 * i + 4] = r.c.re; c[8 * i + 5] = r.c.im;
+        c[8 * i + 6] = r.d.re; c[8 * i + 7] = r.d.im;
+    }
+}
+
+/*
+ * Weighted DFT of element signals to output directions.
+ *   out[d] = norm * sum_e w_e * exp(i k (x_e X_d + y_e Y_d [+ z_e Z_d]))
+ *                 * data[idx_e][d]
+ * matrix = 0: complex data [num_types][num_out], output [num_out];
+ * matrix = 1: data [num_types][num_out][4] (xx, xy, yx, yy), only the pairs
+ * selected by eval_x / eval_y are written.
+ * Restates math/define_dftw_c2c.h:79-106 and math/define_dftw_m2m.h:109-167.
+ */
+void ORC_FN(orc_dftw)(int matrix, int is_3d, int num_in, REAL wavenumber,
+        const REAL* weights_in, const REAL* x_in, const REAL* y_in,
+        const REAL* z_in, int offset_coord_out, int num_out,
+        const REAL* x_out, const REAL* y_out, const REAL* z_out,
+        const int* data_idx, const REAL* data, int eval_x, int eval_y,
+        int offset_out, REAL* output, REAL norm_factor)
+{
+    int d;
+#pragma omp parallel for
+    for (d = 0; d < num_out; ++d)
+    {
+        REAL acc[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+        const REAL xo = wavenumber * x_out[d + offset_coord_out];
+        const REAL yo = wavenumber * y_out[d + offset_coord_out];
+        const REAL zo = is_3d ? wavenumber * z_out[d + offset_coord_out] : 0;
+        int e, k;
+        for (e = 0; e < num_in; ++e)
+        {
+            REAL ph = xo * x_in[e] + yo * y_in[e];
+            REAL re, im, cre;
+            const int src = data_idx ? data_idx[e] : e;
+            if (is_3d) ph += zo * z_in[e];
+            im = ORC_SIN(ph);
+            re = ORC_COS(ph);
+            /* phasor times weight */
+            cre = re;
+            re = re * weights_in[2 * e] - weights_in[2 * e + 1] * im;
+            im = im * weights_in[2 * e] + weights_in[2 * e + 1] * cre;
+            if (!matrix)
+            {
+                const REAL* in = data + 2 * ((size_t) src * num_out + d);
+                acc[0] += in[0] * re - in[1] * im;
+                acc[1] += in[1] * re + in[0] * im;
+            }
+            else
+            {
+                const REAL* in = data + 8 * ((size_t) src * num_out + d);
+                const int k0 = eval_x ? 0 : 2, k1 = eval_y ? 4 : 2;
+                for (k = k0; k < k1; ++k)
+                {
+                    acc[2 * k] += in[2 * k] * re - in[2 * k + 1] * im;
+                    acc[2 * k + 1] += in[2 * k + 1] * re + in[2 * k] * im;
+                }
+            }
+        }
+        if (!matrix)
+        {
+            output[2 * ((size_t) d + offset_out)] = acc[0] * norm_factor;
+            output[2 * ((size_t) d + offset_out) + 1] = acc[1] * norm_factor;
+        }
+        else
+        {
+            REAL* o = output + 8 * ((size_t) d + offset_out);
+            const int k0 = eval_x ? 0 : 2, k1 = eval_y ? 4 : 2;
+            for (k = k0; k < k1; ++k)
+            {
+                o[2 * k] = acc[2 * k] * norm_factor;
+                o[2 * k + 1] = acc[2 * k + 1] * norm_factor;
+            }
+        }
+    }
+}
+
+/* Beamforming weights w_e = exp(-i k (x x1 + y y1 + z z1 + cable_e))
+ * (telescope/station/define_evaluate_element_weights_dft.h:3-16). */
+void ORC_FN(orc_element_weights_dft)(int n, const REAL* x, const REAL* y,
+        const REAL* z, const REAL* cable_length_error, REAL wavenumber,
+        REAL x1, REAL y1, REAL z1, REAL* weights)
+{
+    int i;
+    for (i = 0; i < n; ++i)
+    {
+        const REAL p = wavenumber * (x[i] * x1 + y[i] * y1 + z[i] * z1 +
+                cable_length_error[i]);
+        weights[2 * i] = ORC_COS(-p);
+        weights[2 * i + 1] = ORC_SIN(-p);
+    }
+}
+
+/* Station ECEF offsets to (u, v, w) at hour angle ha0
+ * (convert/define_convert_ecef_to_station_uvw.h:3-29). */
+void ORC_FN(orc_ecef_to_station_uvw)(int n, const REAL* x, const REAL* y,
+        const REAL* z, REAL sin_ha0, REAL cos_ha0, REAL sin_dec0,
+        REAL cos_dec0, int ignore_w, int offset_out, REAL* u, REAL* v,
+        REAL* w)
+{
+    int i;
+    for (i = 0; i < n; ++i)
+    {
+        const REAL xx = x[i], yy = y[i], zz = z[i];
+        const REAL t = xx * cos_ha0 - yy * sin_ha0;
+        u[i + offset_out] = xx * sin_ha0 + yy * cos_ha0;
+        v[i + offset_out] = zz * cos_dec0 - t * sin_dec0;
+        w[i + offset_out] = ignore_w ? (REAL)0 : zz * sin_dec0 + t * cos_dec0;
+    }
+}

@@ -1,0 +1,88 @@
+/*
+ * Instantiates the reference's own CPU kernels (their macro bodies, included
+ * from the reference source tree) under exported names, so that tests can
+ * run them next to the oracle. Built by `make -C oracle ref` into
+ * oracle/_ref/liboskar_ref.so; nothing in the product links it.
+ * The cross-correlation CPU kernels come from the reference's
+ * correlate/src/oskar_cross_correlate{,_scalar}_omp.cpp, compiled as they are.
+ */
+#include <stddef.h>
+#include "oskar_global.h"
+#include "utility/oskar_kernel_macros.h"
+#include "utility/oskar_vector_types.h"
+#include "math/define_multiply.h"
+#include "correlate/define_correlate_utils.h"
+#include "correlate/define_auto_correlate.h"
+#include "interferometer/define_evaluate_jones_K.h"
+#include "mem/define_mem_multiply.h"
+#include "math/define_dftw_c2c.h"
+#include "math/define_dftw_m2m.h"
+#include "telescope/station/define_evaluate_element_weights_dft.h"
+#include "convert/define_convert_ecef_to_station_uvw.h"
+
+#define INST(REAL, S, REAL2, REAL4c) \
+OSKAR_ACORR_CPU(k_acorr_##S, REAL, REAL2, REAL4c) \
+OSKAR_ACORR_SCALAR_CPU(k_acorr_scalar_##S, REAL, REAL2) \
+OSKAR_JONES_K_CPU(k_jones_k_##S, REAL, REAL2) \
+OSKAR_MEM_MUL_CC_C(k_mul_cc_c_##S, REAL2) \
+OSKAR_MEM_MUL_CC_M(k_mul_cc_m_##S, REAL, REAL2, REAL4c) \
+OSKAR_MEM_MUL_CM_M(k_mul_cm_m_##S, REAL2, REAL4c) \
+OSKAR_MEM_MUL_MC_M(k_mul_mc_m_##S, REAL2, REAL4c) \
+OSKAR_MEM_MUL_MM_M(k_mul_mm_m_##S, REAL2, REAL4c) \
+OSKAR_DFTW_C2C_CPU(k_dftw_c2c_2d_##S, 0, REAL, REAL2) \
+OSKAR_DFTW_C2C_CPU(k_dftw_c2c_3d_##S, 1, REAL, REAL2) \
+OSKAR_DFTW_M2M_CPU(k_dftw_m2m_2d_##S, 0, REAL, REAL2) \
+OSKAR_DFTW_M2M_CPU(k_dftw_m2m_3d_##S, 1, REAL, REAL2) \
+OSKAR_ELEMENT_WEIGHTS_DFT(k_weights_##S, REAL, REAL2) \
+OSKAR_CONVERT_ECEF_TO_STATION_UVW(k_uvw_##S, REAL) \
+void ref_acorr_matrix_##S(int ns, int nst, int off, const REAL4c* j, \
+        const REAL* sI, const REAL* sQ, const REAL* sU, const REAL* sV, \
+        REAL4c* vis) \
+{ k_acorr_##S(ns, nst, off, sI, sQ, sU, sV, j, vis); } \
+void ref_acorr_scalar_##S(int ns, int nst, int off, const REAL2* j, \
+        const REAL* sI, REAL2* vis) \
+{ k_acorr_scalar_##S(ns, nst, off, sI, sI, sI, sI, j, vis); } \
+void ref_jones_k_##S(int ns, const REAL* l, const REAL* m, const REAL* n, \
+        int nst, const REAL* u, const REAL* v, const REAL* w, REAL k, \
+        const REAL* f, REAL fmin, REAL fmax, int ignore_w, REAL2* out) \
+{ k_jones_k_##S(ns, l, m, n, nst, u, v, w, k, f, fmin, fmax, ignore_w, out); } \
+void ref_mem_mul_cc_c_##S(int n, const REAL2* a, const REAL2* b, REAL2* c) \
+{ k_mul_cc_c_##S(0, 0, 0, (unsigned) n, a, b, c); } \
+void ref_mem_mul_cc_m_##S(int n, const REAL2* a, const REAL2* b, REAL4c* c) \
+{ k_mul_cc_m_##S(0, 0, 0, (unsigned) n, a, b, c); } \
+void ref_mem_mul_cm_m_##S(int n, const REAL2* a, const REAL4c* b, REAL4c* c) \
+{ k_mul_cm_m_##S(0, 0, 0, (unsigned) n, a, b, c); } \
+void ref_mem_mul_mc_m_##S(int n, const REAL4c* a, const REAL2* b, REAL4c* c) \
+{ k_mul_mc_m_##S(0, 0, 0, (unsigned) n, a, b, c); } \
+void ref_mem_mul_mm_m_##S(int n, const REAL4c* a, const REAL4c* b, REAL4c* c) \
+{ k_mul_mm_m_##S(0, 0, 0, (unsigned) n, a, b, c); } \
+void ref_dftw_##S(int matrix, int is_3d, int num_in, REAL k, \
+        const REAL2* w, const REAL* xi, const REAL* yi, const REAL* zi, \
+        int off_coord, int num_out, const REAL* xo, const REAL* yo, \
+        const REAL* zo, const int* idx, const REAL2* data, int ex, int ey, \
+        int off_out, REAL2* out, REAL norm) \
+{ \
+    if (!matrix && !is_3d) k_dftw_c2c_2d_##S(num_in, k, w, xi, yi, zi, \
+            off_coord, num_out, xo, yo, zo, idx, data, ex, ey, off_out, out, \
+            norm, 0); \
+    else if (!matrix) k_dftw_c2c_3d_##S(num_in, k, w, xi, yi, zi, \
+            off_coord, num_out, xo, yo, zo, idx, data, ex, ey, off_out, out, \
+            norm, 0); \
+    else if (!is_3d) k_dftw_m2m_2d_##S(num_in, k, w, xi, yi, zi, \
+            off_coord, num_out, xo, yo, zo, idx, data, ex, ey, off_out, out, \
+            norm, 0); \
+    else k_dftw_m2m_3d_##S(num_in, k, w, xi, yi, zi, \
+            off_coord, num_out, xo, yo, zo, idx, data, ex, ey, off_out, out, \
+            norm, 0); \
+} \
+void ref_element_weights_dft_##S(int n, const REAL* x, const REAL* y, \
+        const REAL* z, const REAL* cable, REAL k, REAL x1, REAL y1, REAL z1, \
+        REAL2* w) \
+{ k_weights_##S(n, x, y, z, cable, k, x1, y1, z1, w); } \
+void ref_ecef_to_station_uvw_##S(int n, const REAL* x, const REAL* y, \
+        const REAL* z, REAL sh, REAL ch, REAL sd, REAL cd, int ignore_w, \
+        int off, REAL* u, REAL* v, REAL* w) \
+{ k_uvw_##S(n, x, y, z, sh, ch, sd, cd, ignore_w, off, u, v, w); }
+
+INST(double, d, double2, double4c)
+INST(float, f, float2, float4c)

@@ -1,0 +1,156 @@
+"""Pins the CPU oracle against the reference's own CPU kernels.
+
+oracle/_ref/liboskar_ref.so is the reference's code compiled from its sources
+(oracle/Makefile, target "ref"); the oracle must agree with it on every
+function and variant the hot path uses. Both run on the same seeded inputs.
+"""
+import itertools
+
+import numpy as np
+import pytest
+
+from oracle_lib import oracle, reference, reference_xcorr, suffix
+from xcorr_cases import XcorrCase
+
+pytestmark = pytest.mark.skipif(reference() is None,
+                                reason="reference sources not present")
+
+TOL = {np.float64: 1e-13, np.float32: 2e-5}
+
+
+def _close(a, b, real):
+    a = np.asarray(a, np.float64)
+    b = np.asarray(b, np.float64)
+    scale = np.max(np.abs(b)) + 1e-300
+    return np.max(np.abs(a - b)) / scale <= TOL[real]
+
+
+@pytest.mark.parametrize("real", [np.float64, np.float32])
+@pytest.mark.parametrize("matrix", [True, False])
+@pytest.mark.parametrize("gaussian", [False, True])
+@pytest.mark.parametrize("bw,ts", [(0.0, 0.0), (10e3, 0.0), (0.0, 10.0),
+                                   (10e3, 10.0)])
+@pytest.mark.parametrize("casa", [0, 1])
+def test_xcorr(real, matrix, gaussian, bw, ts, casa):
+    c = XcorrCase(19, 277, real=real, matrix=matrix, gaussian=gaussian,
+                  bandwidth_hz=bw, time_avg=ts, casa=casa, offset_out=3)
+    v_orc, v_ref = c.vis0.copy(), c.vis0.copy()
+    oracle().call("xcorr_" + ("matrix_" if matrix else "scalar_")
+                  + suffix(real), real, casa, int(gaussian),
+                  *c.oracle_args(v_orc))
+    reference_xcorr(real, matrix, gaussian, casa, *c.oracle_args(v_ref))
+    assert _close(v_orc, v_ref, real)
+    assert not np.array_equal(v_orc, c.vis0)
+
+
+@pytest.mark.parametrize("real", [np.float64, np.float32])
+def test_xcorr_uv_filter(real):
+    c = XcorrCase(12, 50, real=real, uv_min=0.5, uv_max=1.2)
+    v_orc, v_ref = c.vis0.copy(), c.vis0.copy()
+    oracle().call("xcorr_matrix_" + suffix(real), real, 0, 0,
+                  *c.oracle_args(v_orc))
+    reference_xcorr(real, True, False, 0, *c.oracle_args(v_ref))
+    assert _close(v_orc, v_ref, real)
+    # some baselines filtered out, some kept
+    changed = np.any((v_orc != c.vis0).reshape(-1, 8), axis=1)
+    assert changed.any() and not changed.all()
+
+
+@pytest.mark.parametrize("real", [np.float64, np.float32])
+@pytest.mark.parametrize("matrix", [True, False])
+def test_acorr(real, matrix):
+    c = XcorrCase(9, 101, real=real, matrix=matrix)
+    nc = 8 if matrix else 2
+    v0 = np.random.default_rng(5).uniform(-1, 1, 12 * nc).astype(real)
+    v_orc, v_ref = v0.copy(), v0.copy()
+    if matrix:
+        args = (c.num_src, c.num_st, 2, c.jones, c.I, c.Q, c.U, c.V)
+    else:
+        args = (c.num_src, c.num_st, 2, c.jones, c.I)
+    name = "acorr_" + ("matrix_" if matrix else "scalar_") + suffix(real)
+    oracle().call(name, real, *args, v_orc)
+    reference().call(name, real, *args, v_ref)
+    assert _close(v_orc, v_ref, real)
+
+
+@pytest.mark.parametrize("real", [np.float64, np.float32])
+@pytest.mark.parametrize("ignore_w", [0, 1])
+def test_jones_k(real, ignore_w):
+    rng = np.random.default_rng(3)
+    ns, nst = 1000, 100
+    l, m, n = (rng.uniform(0.1, 0.9, ns).astype(real) for _ in range(3))
+    u, v, w = (rng.uniform(-1e3, 1e3, nst).astype(real) for _ in range(3))
+    f = rng.uniform(0, 2, ns).astype(real)
+    k = 2 * np.pi * 100e6 / 299792458.0
+    out_o = np.zeros(2 * ns * nst, real)
+    out_r = np.zeros(2 * ns * nst, real)
+    args = (ns, l, m, n, nst, u, v, w, k, f, 0.5, 1.5, ignore_w)
+    oracle().call("jones_k_" + suffix(real), real, *args, out_o)
+    reference().call("jones_k_" + suffix(real), real, *args, out_r)
+    assert _close(out_o, out_r, real)
+    assert np.count_nonzero(out_o) < out_o.size  # the filter zeroed some
+
+
+@pytest.mark.parametrize("real", [np.float64, np.float32])
+@pytest.mark.parametrize("kind,na,nb,nc", [("cc_c", 2, 2, 2),
+                                           ("cc_m", 2, 2, 8),
+                                           ("cm_m", 2, 8, 8),
+                                           ("mc_m", 8, 2, 8),
+                                           ("mm_m", 8, 8, 8)])
+def test_mem_mul(real, kind, na, nb, nc):
+    rng = np.random.default_rng(4)
+    n = 777
+    a = rng.uniform(-2, 2, n * na).astype(real)
+    b = rng.uniform(-2, 2, n * nb).astype(real)
+    co, cr = np.zeros(n * nc, real), np.zeros(n * nc, real)
+    oracle().call("mem_mul_%s_%s" % (kind, suffix(real)), real, n, a, b, co)
+    reference().call("mem_mul_%s_%s" % (kind, suffix(real)), real, n, a, b,
+                     cr)
+    assert _close(co, cr, real)
+
+
+@pytest.mark.parametrize("real", [np.float64, np.float32])
+@pytest.mark.parametrize("matrix,is_3d,use_idx,ex,ey",
+                         [(0, 0, 0, 1, 1), (0, 1, 1, 1, 1), (1, 0, 0, 1, 1),
+                          (1, 1, 1, 1, 1), (1, 1, 1, 1, 0), (1, 0, 1, 0, 1)])
+def test_dftw(real, matrix, is_3d, use_idx, ex, ey):
+    rng = np.random.default_rng(6)
+    n_in, n_out, n_types, off_c, off_o = 64, 301, 3, 5, 7
+    k = 2 * np.pi * 100e6 / 299792458.0
+    w = rng.uniform(-1, 1, 2 * n_in).astype(real)
+    xi, yi, zi = (rng.uniform(-20, 20, n_in).astype(real) for _ in range(3))
+    xo, yo, zo = (rng.uniform(-1, 1, n_out + off_c).astype(real)
+                  for _ in range(3))
+    idx = (rng.integers(0, n_types, n_in).astype(np.int32) if use_idx
+           else None)
+    nd = n_types if use_idx else n_in
+    nc = 8 if matrix else 2
+    data = rng.uniform(-1, 1, nd * n_out * nc).astype(real)
+    out0 = rng.uniform(-1, 1, (n_out + off_o) * nc).astype(real)
+    oo, orr = out0.copy(), out0.copy()
+    args = (matrix, is_3d, n_in, k, w, xi, yi, zi if is_3d else None, off_c,
+            n_out, xo, yo, zo if is_3d else None, idx, data, ex, ey, off_o)
+    oracle().call("dftw_" + suffix(real), real, *args, oo, 1.0 / n_in)
+    reference().call("dftw_" + suffix(real), real, *args, orr, 1.0 / n_in)
+    assert _close(oo, orr, real)
+
+
+@pytest.mark.parametrize("real", [np.float64, np.float32])
+def test_element_weights_and_uvw(real):
+    rng = np.random.default_rng(7)
+    n = 256
+    x, y, z, cab = (rng.uniform(-20, 20, n).astype(real) for _ in range(4))
+    k = 2 * np.pi * 110e6 / 299792458.0
+    wo, wr = np.zeros(2 * n, real), np.zeros(2 * n, real)
+    args = (n, x, y, z, cab, k, 0.3, -0.2, 0.93)
+    oracle().call("element_weights_dft_" + suffix(real), real, *args, wo)
+    reference().call("element_weights_dft_" + suffix(real), real, *args, wr)
+    assert _close(wo, wr, real)
+    outs = [[np.zeros(n + 2, real) for _ in range(3)] for _ in range(2)]
+    for ign, (lib, o) in itertools.product([0, 1], zip(
+            [oracle(), reference()], outs)):
+        lib.call("ecef_to_station_uvw_" + suffix(real), real, n, x, y, z,
+                 0.3, 0.95, -0.5, 0.86, ign, 2, *o)
+        if lib is reference():
+            for a, b in zip(outs[0], outs[1]):
+                assert _close(a, b, real)
