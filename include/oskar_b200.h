@@ -1,0 +1,214 @@
+/*
+ * oskar_b200 -- B200 (sm_100a) kernels for OSKAR's interferometer visibility
+ * hot path: station-beam DFT, Jones K and join, cross-/auto-correlation.
+ *
+ * This is the C ABI of liboskar_b200.so. Every entry point takes plain
+ * pointers, sizes and a CUDA stream (passed as void*, 0 = legacy default
+ * stream). Unless stated otherwise all array pointers are DEVICE pointers.
+ *
+ * Conventions (the same as the reference's kernel launchers):
+ *  - a complex value is two reals {re, im}; a 2x2 complex matrix is eight
+ *    reals {a, b, c, d} = {xx, xy, yx, yy}
+ *    (oskar/utility/oskar_vector_types.h:85-98);
+ *  - Jones arrays are [station][source], source fastest
+ *    (oskar/interferometer/private_jones.h:34-41);
+ *  - visibility index of the baseline between stations q < p is
+ *    q*(N-1) - (q-1)*q/2 + p - q - 1, plus offset_out
+ *    (oskar/correlate/define_correlate_utils.h:42);
+ *  - correlation outputs are ACCUMULATED (+=) into vis, as in the reference;
+ *  - every function returns 0 on success or a negative OSKAR error code
+ *    (oskar/oskar_global.h:20-55); nothing is launched after an error.
+ *
+ * Each function names the reference interface it replaces.
+ */
+#ifndef OSKAR_B200_H_
+#define OSKAR_B200_H_
+
+#include <stddef.h>
+
+#if defined(__GNUC__)
+#define OSKB_API __attribute__((visibility("default")))
+#else
+#define OSKB_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Error codes shared with the reference (oskar/oskar_global.h:20-55). */
+#define OSKB_ERR_INVALID_ARGUMENT      (-3)
+#define OSKB_ERR_OUT_OF_RANGE          (-5)
+#define OSKB_ERR_MEMORY_ALLOC_FAILURE  (-6)
+#define OSKB_ERR_MEMORY_COPY_FAILURE   (-7)
+#define OSKB_ERR_TYPE_MISMATCH         (-9)
+#define OSKB_ERR_LOCATION_MISMATCH     (-10)
+#define OSKB_ERR_DIMENSION_MISMATCH    (-11)
+#define OSKB_ERR_BAD_DATA_TYPE         (-13)
+#define OSKB_ERR_CUDA_NOT_AVAILABLE    (-16)
+#define OSKB_ERR_KERNEL_LAUNCH_FAILURE (-18)
+
+/* Library version string and the CUDA error text of the last failure. */
+OSKB_API const char* oskb_version(void);
+OSKB_API const char* oskb_last_error(void);
+
+/* ------------------------------------------------------------------------
+ * Cross-correlation, direct kernel (all source types and smearing modes).
+ * ------------------------------------------------------------------------
+ * V[bl] += sum_s smear(s, bl) * J_p(s) B(s) J_q(s)^H, with the brightness
+ * matrix B built from Stokes I, Q, U, V. Bandwidth smearing is on when
+ * frac_bandwidth != 0, time-average smearing when time_int_sec != 0.
+ * gaussian != 0 selects Gaussian sources (a, b, c used); else a, b, c may be
+ * NULL.
+ * Replaces oskar_cross_correlate_{point,gaussian}_cuda_{f,d}
+ * (oskar/correlate/oskar_cross_correlate_cuda.h:60-71, 113-124, 172-184,
+ * 232-244). The FP64 form matches the reference CPU FP64 path to 1e-12
+ * relative; the FP32 form accumulates per source chunk with compensated
+ * cross-chunk sums. */
+OSKB_API int oskb_cross_correlate_d(int use_casa_phase_convention, int gaussian,
+        int num_sources, int num_stations, int offset_out,
+        const double* jones, const double* I, const double* Q,
+        const double* U, const double* V, const double* l, const double* m,
+        const double* n, const double* a, const double* b, const double* c,
+        const double* station_u, const double* station_v,
+        const double* station_w, const double* station_x,
+        const double* station_y, double uv_min_lambda, double uv_max_lambda,
+        double inv_wavelength, double frac_bandwidth, double time_int_sec,
+        double gha0_rad, double dec0_rad, double* vis, void* stream);
+OSKB_API int oskb_cross_correlate_f(int use_casa_phase_convention, int gaussian,
+        int num_sources, int num_stations, int offset_out,
+        const float* jones, const float* I, const float* Q,
+        const float* U, const float* V, const float* l, const float* m,
+        const float* n, const float* a, const float* b, const float* c,
+        const float* station_u, const float* station_v,
+        const float* station_w, const float* station_x,
+        const float* station_y, float uv_min_lambda, float uv_max_lambda,
+        float inv_wavelength, float frac_bandwidth, float time_int_sec,
+        float gha0_rad, float dec0_rad, float* vis, void* stream);
+
+/* Scalar (Stokes-I only) polarisation mode: V += sum smear * I J_p conj(J_q).
+ * jones is complex [station][source]. Replaces
+ * oskar_cross_correlate_scalar_{point,gaussian}_cuda_{f,d}
+ * (oskar/correlate/oskar_cross_correlate_scalar_cuda.h:56, 103, 156, 211). */
+OSKB_API int oskb_cross_correlate_scalar_d(int use_casa_phase_convention,
+        int gaussian, int num_sources, int num_stations, int offset_out,
+        const double* jones, const double* I, const double* l,
+        const double* m, const double* n, const double* a, const double* b,
+        const double* c, const double* station_u, const double* station_v,
+        const double* station_w, const double* station_x,
+        const double* station_y, double uv_min_lambda, double uv_max_lambda,
+        double inv_wavelength, double frac_bandwidth, double time_int_sec,
+        double gha0_rad, double dec0_rad, double* vis, void* stream);
+OSKB_API int oskb_cross_correlate_scalar_f(int use_casa_phase_convention,
+        int gaussian, int num_sources, int num_stations, int offset_out,
+        const float* jones, const float* I, const float* l,
+        const float* m, const float* n, const float* a, const float* b,
+        const float* c, const float* station_u, const float* station_v,
+        const float* station_w, const float* station_x,
+        const float* station_y, float uv_min_lambda, float uv_max_lambda,
+        float inv_wavelength, float frac_bandwidth, float time_int_sec,
+        float gha0_rad, float dec0_rad, float* vis, void* stream);
+
+/* Auto-correlation: vis[s + offset_out] += sum_src J B J^H (matrix) or
+ * sum |J|^2 I (scalar, real part only). Replaces the kernels behind
+ * oskar_auto_correlate (oskar/correlate/oskar_auto_correlate.h:37;
+ * oskar/correlate/define_auto_correlate.h:8-82). */
+OSKB_API int oskb_auto_correlate_d(int matrix, int num_sources, int num_stations,
+        int offset_out, const double* jones, const double* I,
+        const double* Q, const double* U, const double* V, double* vis,
+        void* stream);
+OSKB_API int oskb_auto_correlate_f(int matrix, int num_sources, int num_stations,
+        int offset_out, const float* jones, const float* I,
+        const float* Q, const float* U, const float* V, float* vis,
+        void* stream);
+
+/* ------------------------------------------------------------------------
+ * Jones K and join.
+ * ------------------------------------------------------------------------
+ * K[station][source] = exp(i wavenumber (u l + v m + w (n - 1))), zero for
+ * sources whose filter value lies outside (filter_min, filter_max].
+ * Replaces the kernels behind oskar_evaluate_jones_K
+ * (oskar/interferometer/oskar_evaluate_jones_K.h:49;
+ *  oskar/interferometer/define_evaluate_jones_K.h:22-70). */
+OSKB_API int oskb_evaluate_jones_K_d(int num_sources, const double* l,
+        const double* m, const double* n, int num_stations, const double* u,
+        const double* v, const double* w, double wavenumber,
+        const double* source_filter, double filter_min, double filter_max,
+        int ignore_w_components, double* jones, void* stream);
+OSKB_API int oskb_evaluate_jones_K_f(int num_sources, const float* l,
+        const float* m, const float* n, int num_stations, const float* u,
+        const float* v, const float* w, float wavenumber,
+        const float* source_filter, float filter_min, float filter_max,
+        int ignore_w_components, float* jones, void* stream);
+
+/* Element-wise products c[i+off_c] = a[i+off_a] * b[i+off_b] behind
+ * oskar_jones_join / oskar_mem_multiply
+ * (oskar/interferometer/oskar_jones_join.h:69; oskar/mem/oskar_mem_multiply.h:63;
+ *  kernels oskar/mem/define_mem_multiply.h:3-89). kind selects the operand
+ * shapes: OSKB_MUL_RR_R (real*real), OSKB_MUL_CC_C (complex*complex),
+ * OSKB_MUL_CC_M (complex*complex -> diagonal matrix), OSKB_MUL_CM_M
+ * (complex*matrix), OSKB_MUL_MC_M (matrix*complex), OSKB_MUL_MM_M
+ * (matrix*matrix). c may alias a or b exactly. */
+#define OSKB_MUL_RR_R 0
+#define OSKB_MUL_CC_C 1
+#define OSKB_MUL_CC_M 2
+#define OSKB_MUL_CM_M 3
+#define OSKB_MUL_MC_M 4
+#define OSKB_MUL_MM_M 5
+OSKB_API int oskb_mem_multiply_d(int kind, size_t off_a, size_t off_b, size_t off_c,
+        size_t n, const double* a, const double* b, double* c, void* stream);
+OSKB_API int oskb_mem_multiply_f(int kind, size_t off_a, size_t off_b, size_t off_c,
+        size_t n, const float* a, const float* b, float* c, void* stream);
+
+/* ------------------------------------------------------------------------
+ * Station beam: weighted DFT and beamforming weights.
+ * ------------------------------------------------------------------------
+ * output[d + offset_out] = norm_factor * sum_e w_e
+ *     * exp(i wavenumber (x_e X_d + y_e Y_d [+ z_e Z_d])) * data[idx_e][d]
+ * with (X, Y, Z) = (x_out, y_out, z_out)[d + offset_coord_out]; 3-D when
+ * both z_in and z_out are non-NULL; idx_e = data_idx[e] or e if data_idx is
+ * NULL. matrix = 0: data complex [n_idx][num_out], output complex;
+ * matrix = 1: data [n_idx][num_out][2x2], output 2x2, the xx/xy pair written
+ * if eval_x and the yx/yy pair if eval_y.
+ * Replaces the kernels behind oskar_dftw (oskar/math/oskar_dftw.h:92-111;
+ * oskar/math/define_dftw_c2c.h:24-77, define_dftw_m2m.h:24-107). */
+OSKB_API int oskb_dftw_d(int matrix, int num_in, double wavenumber,
+        const double* weights_in, const double* x_in, const double* y_in,
+        const double* z_in, int offset_coord_out, int num_out,
+        const double* x_out, const double* y_out, const double* z_out,
+        const int* data_idx, const double* data, int eval_x, int eval_y,
+        int offset_out, double* output, double norm_factor, void* stream);
+OSKB_API int oskb_dftw_f(int matrix, int num_in, float wavenumber,
+        const float* weights_in, const float* x_in, const float* y_in,
+        const float* z_in, int offset_coord_out, int num_out,
+        const float* x_out, const float* y_out, const float* z_out,
+        const int* data_idx, const float* data, int eval_x, int eval_y,
+        int offset_out, float* output, float norm_factor, void* stream);
+
+/* Beamforming weights w_e = exp(-i wavenumber (x x1 + y y1 + z z1 + cable_e)).
+ * Replaces the kernel behind oskar_evaluate_element_weights_dft
+ * (oskar/telescope/station/oskar_evaluate_element_weights_dft.h:66;
+ *  define_evaluate_element_weights_dft.h:3-16). */
+OSKB_API int oskb_evaluate_element_weights_dft_d(int num_elements, const double* x,
+        const double* y, const double* z, const double* cable_length_error,
+        double wavenumber, double x1, double y1, double z1, double* weights,
+        void* stream);
+OSKB_API int oskb_evaluate_element_weights_dft_f(int num_elements, const float* x,
+        const float* y, const float* z, const float* cable_length_error,
+        float wavenumber, float x1, float y1, float z1, float* weights,
+        void* stream);
+
+/* Station ECEF offsets to (u, v, w) metres at hour angle ha0 = gast - ra0.
+ * Replaces the kernel behind oskar_convert_ecef_to_station_uvw
+ * (oskar/convert/oskar_convert_ecef_to_station_uvw.h:67;
+ *  define_convert_ecef_to_station_uvw.h:3-29). */
+OSKB_API int oskb_convert_ecef_to_station_uvw_d(int num_stations, const double* x,
+        const double* y, const double* z, double ra0_rad, double dec0_rad,
+        double gast, int ignore_w_components, int offset_out, double* u,
+        double* v, double* w, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* OSKAR_B200_H_ */
