@@ -214,6 +214,303 @@ def run_reference(args):
 
 
 # ---------------------------------------------------------------- ours
+def _load_peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        with open(path) as f:
+            pk = json.load(f)
+        return pk, "measured"
+    return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0,
+            "bf16_tflops_sustained": 1400.0}, "fallback"
+
+
+def _load_traffic():
+    """DRAM bytes per launch of the contraction kernel from the committed
+    ncu summary (profiles/tc_gemm_c3_traffic.json), or None."""
+    path = os.path.join(ROOT, "profiles", "tc_gemm_c3_traffic.json")
+    if not os.path.exists(path):
+        return None
+    with open(path) as f:
+        return json.load(f).get("dram_bytes_per_launch")
+
+
+def run_ours(args):
+    import torch
+    import torch.distributed as dist
+    import oskar_b200 as ob
+    from oskar_b200 import workloads
+
+    world, rank, local = dist_setup()
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(
+            seconds=300), device_id=torch.device("cuda", local))
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    cfg = workloads.c3()
+    nst, nsrc, nch = cfg.num_st, cfg.num_src, len(cfg.freqs_hz)
+    nbl = cfg.num_baselines
+    dev = lambda a: torch.from_numpy(np.ascontiguousarray(a)).cuda()
+    l, m, n, I, Q, U, V = (dev(x) for x in (cfg.l, cfg.m, cfg.n, cfg.I,
+                                            cfg.Q, cfg.U, cfg.V))
+    E = workloads.jones_e_device(cfg, torch.float32)
+    uvw_all = dev(np.stack([cfg.station_uvw(t)
+                            for t in range(cfg.num_times)]))
+    inv_wl = dev(cfg.freqs_hz / 299792458.0)
+    vis = torch.zeros((nch, nbl, 8), dtype=torch.float64, device="cuda")
+    stream = ob.stream_ptr()
+    sb_step = nbl * nsrc * nch  # source-baselines per step
+
+    if args.path == "tc":
+        ws_bytes = ob.call("oskb_correlate_block_tc_workspace_bytes", nsrc,
+                           nst, nch, check=False)
+        ws = torch.empty(ws_bytes, dtype=torch.uint8, device="cuda")
+        launches_per_step = 3
+
+        def step(d):
+            vis.zero_()
+            ob.call("oskb_correlate_block_tc", 0, nsrc, nst, 1, nch, E, l, m,
+                    n, I, Q, U, V, uvw_all[d], inv_wl, 0.0, 3e38, vis, ws,
+                    ws_bytes, stream)
+    else:
+        Ed = E.double()
+        K = torch.empty((nst, nsrc, 2), dtype=torch.float64, device="cuda")
+        J = torch.empty((nst, nsrc, 8), dtype=torch.float64, device="cuda")
+        z = torch.zeros(nst, dtype=torch.float64, device="cuda")
+        launches_per_step = 3 * nch + 0
+
+        def step(d):
+            vis.zero_()
+            u, v, w = uvw_all[d]
+            for c in range(nch):
+                f = float(cfg.freqs_hz[c])
+                ob.call("oskb_evaluate_jones_K_d", nsrc, l, m, n, nst, u, v,
+                        w, 2 * math.pi * f / 299792458.0, I, 0.0, 1e300, 0,
+                        K, stream)
+                ob.call("oskb_mem_multiply_d", 3, 0, 0, 0, nst * nsrc, K, Ed,
+                        J, stream)
+                ob.call("oskb_cross_correlate_d", 0, 0, nsrc, nst, 0, J, I,
+                        Q, U, V, l, m, n, None, None, None, u, v, w, z, z,
+                        0.0, 3e38, f / 299792458.0, 0.0, 0.0, 0.0, 0.0,
+                        vis[c], stream)
+
+    dump = lambda i: (rank + i * world) % cfg.num_times
+    for i in range(args.warmup):
+        step(dump(i))
+    torch.cuda.synchronize()
+    barrier()
+    torch.cuda.synchronize()
+    clocks = ClockSampler(local)
+    clocks.start()
+    if args.path == "tc":
+        ob.call("oskb_tc_timing", 1)
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for i in range(args.steps):
+        step(dump(args.warmup + i))
+    e1.record()
+    torch.cuda.synchronize()
+    barrier()
+    torch.cuda.synchronize()
+    clk = clocks.stop()
+    ms_total = e0.elapsed_time(e1)
+    gemm_ms, gemm_launches = None, 0
+    if args.path == "tc":
+        import ctypes
+        t_ms, n_l = ctypes.c_double(0), ctypes.c_int(0)
+        ob.call("oskb_tc_timing_read", ctypes.addressof(t_ms),
+                ctypes.addressof(n_l))
+        ob.call("oskb_tc_timing", 0)
+        gemm_ms, gemm_launches = t_ms.value, n_l.value
+    t = torch.tensor([ms_total], dtype=torch.float64, device="cuda")
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    ms_max = float(t.item())
+    value = sb_step * args.steps * world / (ms_max * 1e-3) / 1e9
+
+    result = None
+    if rank == 0:
+        peaks, peak_kind = _load_peaks()
+        # ---- roofline of the dominant kernel
+        if args.path == "tc":
+            avg = gemm_ms / max(gemm_launches, 1)
+            sb_launch = sb_step * args.steps / max(gemm_launches, 1)
+            ach = 64.0 * sb_launch / (avg * 1e-3) / 1e12
+            pk = peaks["bf16_tflops_sustained"]
+            nrb = (nst + 31) // 32
+            kp = 2 * 32 * ((nsrc + 31) // 32)
+            issued = (nch * nrb * (nrb + 1) // 2 * 128 * 128 * kp * 2 * 3)
+            issued_tf = issued / (avg * 1e-3) / 1e12
+            traffic = _load_traffic()
+            roof = {"bound": "tensor", "achieved": ach, "peak": pk,
+                    "unit": "TFLOP/s", "frac": ach / pk, "traffic": traffic,
+                    "kernel": "oskb::tc::gemm_kernel",
+                    "peak_kind": "%s bf16 sustained (fp16 same rate)"
+                                 % peak_kind,
+                    "algorithmic_flops_per_launch": 64.0 * sb_launch,
+                    "issued_tflops": issued_tf,
+                    "issued_frac": issued_tf / pk,
+                    "avg_launch_ms": avg,
+                    "share_of_step": gemm_ms / ms_total}
+        else:
+            roof = {"bound": "fp64", "achieved": None, "peak": None,
+                    "unit": "TFLOP/s", "frac": None, "traffic": None}
+        # ---- direct FP64 comparison and error on dump 0, channel 0
+        cmp_ = compare_direct(args, cfg, ob, torch, dev, E, l, m, n, I, Q, U,
+                              V, uvw_all, inv_wl, stream)
+        result = {
+            "metric": METRIC, "value": value, "unit": UNIT,
+            "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": ms_max / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None,
+            "dtype": "fp16x3->f32->f64 (TC), f64 phase" if args.path == "tc"
+                     else "f64",
+            "data": "synthetic",
+            "config": {"workload": "c3: 512 stations log-radial to 65 km, "
+                       "100,000 point sources (full Stokes), 2x2 E per "
+                       "station-source, 16 ch x 64 dumps; step = 1 dump x "
+                       "16 ch", "stations": nst, "sources": nsrc,
+                       "channels": nch, "dumps": cfg.num_times,
+                       "path": args.path,
+                       "parallelism": "dumps sharded over %d rank(s)" % world,
+                       "l2": "inputs larger than L2 (E 1.6 GB; operand "
+                             "images 26 GB per step)"},
+            "gpu_launches": launches_per_step * args.steps,
+            "roofline": roof, "clocks": clk,
+            "direct_fp64": cmp_["direct"],
+            "speedup_vs_direct_fp64": value / cmp_["direct"]["value"],
+            "rel_err_vs_fp64": cmp_["err"],
+        }
+    # ---- end to end through the host-buffer entry point
+    e2e = run_e2e(args, cfg, ob, torch, E, world, rank)
+    if rank == 0:
+        result["e2e"] = e2e
+        if world == 1 and not args.no_cpu_baseline:
+            result["cpu_baseline"] = cpu_baseline(cfg)
+        print(json.dumps(result))
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+def compare_direct(args, cfg, ob, torch, dev, E, l, m, n, I, Q, U, V,
+                   uvw_all, inv_wl, stream):
+    """FP64 direct kernel on dump 0, channel 0: its throughput, and the
+    tensor-core result's error against it (L2 relative and max |err| /
+    max |V|)."""
+    nst, nsrc, nbl = cfg.num_st, cfg.num_src, cfg.num_baselines
+    f = float(cfg.freqs_hz[0])
+    u, v, w = uvw_all[0]
+    Ed = E.double()
+    K = torch.empty((nst, nsrc, 2), dtype=torch.float64, device="cuda")
+    J = torch.empty((nst, nsrc, 8), dtype=torch.float64, device="cuda")
+    ob.call("oskb_evaluate_jones_K_d", nsrc, l, m, n, nst, u, v, w,
+            2 * math.pi * f / 299792458.0, I, 0.0, 1e300, 0, K, stream)
+    ob.call("oskb_mem_multiply_d", 3, 0, 0, 0, nst * nsrc, K, Ed, J, stream)
+    del Ed
+    z = torch.zeros(nst, dtype=torch.float64, device="cuda")
+    vd = torch.zeros((nbl, 8), dtype=torch.float64, device="cuda")
+
+    def direct():
+        ob.call("oskb_cross_correlate_d", 0, 0, nsrc, nst, 0, J, I, Q, U, V,
+                l, m, n, None, None, None, u, v, w, z, z, 0.0, 3e38,
+                f / 299792458.0, 0.0, 0.0, 0.0, 0.0, vd, stream)
+    direct()
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    reps = 3
+    e0.record()
+    for _ in range(reps):
+        direct()
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / reps
+    vd.zero_()
+    direct()
+    vt = torch.zeros((1, nbl, 8), dtype=torch.float64, device="cuda")
+    ob.call("oskb_correlate_block_tc", 0, nsrc, nst, 1, 1, E, l, m, n, I, Q,
+            U, V, uvw_all[0], inv_wl[0:1], 0.0, 3e38, vt, None, 0, stream)
+    torch.cuda.synchronize()
+    a = vt[0].cpu().numpy()
+    b = vd.cpu().numpy()
+    err = {"l2": float(np.linalg.norm(a - b) / np.linalg.norm(b)),
+           "max_over_max": float(np.max(np.abs(a - b)) / np.max(np.abs(b))),
+           "sample": "dump 0, channel 0 (100 MHz): all 130,816 baselines x "
+                     "4 pols; reference = FP64 direct kernel on the same "
+                     "inputs"}
+    direct_v = nbl * nsrc / (ms * 1e-3) / 1e9
+    del J, K
+    torch.cuda.empty_cache()
+    return {"direct": {"value": direct_v, "unit": UNIT,
+                       "kernel": "oskb direct FP64 cross-correlation",
+                       "ms_per_channel": ms}, "err": err}
+
+
+def run_e2e(args, cfg, ob, torch, E, world, rank):
+    """Source-baselines per second through oskb_run_block_tc_host with
+    page-locked host buffers; a step is one block of 8 dumps x 16 channels
+    (the reference's default block length), host copies included."""
+    nst, nsrc, nch = cfg.num_st, cfg.num_src, len(cfg.freqs_hz)
+    nbl = cfg.num_baselines
+    nt = 8
+    pin = lambda a: torch.from_numpy(np.ascontiguousarray(a)).pin_memory()
+    Eh = E.cpu().pin_memory()
+    sky = [pin(x) for x in (cfg.l, cfg.m, cfg.n, cfg.I, cfg.Q, cfg.U, cfg.V)]
+    freqs = pin(cfg.freqs_hz)
+    visb = torch.empty((nt, nch, nbl, 8), dtype=torch.float64).pin_memory()
+    nblocks = max(1, args.steps // nt)
+    uvws = [pin(np.stack([cfg.station_uvw((rank + (b * world) * nt + i)
+                                          % cfg.num_times)
+                          for i in range(nt)])) for b in range(nblocks + 1)]
+    stream = ob.stream_ptr()
+
+    def block(b):
+        ob.call("oskb_run_block_tc_host", 0, nsrc, nst, nt, nch, Eh, *sky,
+                uvws[b], freqs, 0.0, 3e38, visb, stream)
+    block(nblocks)  # warm-up (allocates the library's device buffers)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for b in range(nblocks):
+        block(b)
+    dt = time.perf_counter() - t0
+    t = torch.tensor([dt], dtype=torch.float64, device="cuda")
+    if world > 1:
+        import torch.distributed as dist
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    dt = float(t.item())
+    sb = nbl * nsrc * nch * nt * nblocks * world
+    h2d = (Eh.numel() * 4 + 7 * nsrc * 8 + nt * 3 * nst * 8 + nch * 8)
+    d2h = visb.numel() * 8
+    del Eh, visb
+    return {"value": sb / dt / 1e9, "unit": UNIT, "h2d_bytes_per_step": h2d,
+            "d2h_bytes_per_step": d2h,
+            "step": "one block of 8 dumps x 16 channels via "
+                    "oskb_run_block_tc_host (host buffers, page-locked)",
+            "blocks": nblocks, "seconds": dt}
+
+
+def cpu_baseline(cfg):
+    cores = cpu_cores()
+    if ref_lib() is None:
+        return {"value": None, "unit": UNIT, "cores": cores,
+                "kind": "reference", "sample": "unavailable: "
+                "oracle/_ref/liboskar_ref.so not built"}
+    nsrc = calibrate_cpu_sample(cfg, 8.0)
+    dt, work = reference_cpu_sample(cfg, nsrc)
+    return {"value": work / dt / 1e9, "unit": UNIT, "cores": cores,
+            "kind": "reference",
+            "sample": "1 dump x 1 channel x %d of 100000 sources x 130816 "
+                      "baselines (reference OpenMP Jones K + join + FP64 "
+                      "cross-correlation, %.1f s)" % (nsrc, dt)}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -223,11 +520,10 @@ def main():
     ap.add_argument("--path", default="tc", choices=["tc", "direct"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()
+    os.environ.setdefault("OMP_NUM_THREADS", str(cpu_cores()))
     if args.impl == "reference":
         return run_reference(args)
-    from oskar_b200 import benchpath
-    return benchpath.run(args, ClockSampler, dist_setup, reference_cpu_sample,
-                         calibrate_cpu_sample, cpu_cores, METRIC, UNIT)
+    return run_ours(args)
 
 
 if __name__ == "__main__":

@@ -207,6 +207,85 @@ OSKB_API int oskb_convert_ecef_to_station_uvw_d(int num_stations, const double* 
         double gast, int ignore_w_components, int offset_out, double* u,
         double* v, double* w, void* stream);
 
+/* ------------------------------------------------------------------------
+ * Tensor-core compensated cross-correlation (point sources, no smearing).
+ * ------------------------------------------------------------------------
+ * Same result as oskb_cross_correlate_d with gaussian = 0,
+ * frac_bandwidth = 0 and time_int_sec = 0, computed as a Hermitian rank-k
+ * update on the sm_100a tensor cores (tcgen05, FP16 hi/lo split, three
+ * products, FP32 accumulation drained to FP64); relative visibility error
+ * against FP64 below 1e-6. Every brightness matrix must be positive
+ * semi-definite (I >= sqrt(Q^2 + U^2 + V^2)); oskb_tc_status() reports a
+ * violation. It is the fast branch of oskar_cross_correlate
+ * (oskar/correlate/oskar_cross_correlate.h:49) for source_type 0 without
+ * smearing; station_u/v are only used by the uv filter.
+ * workspace: device scratch of at least
+ * oskb_cross_correlate_tc_workspace_bytes() bytes, or NULL to let the library
+ * keep one per device (allocated on first use, grown on demand). */
+OSKB_API size_t oskb_cross_correlate_tc_workspace_bytes(int num_sources,
+        int num_stations);
+OSKB_API int oskb_cross_correlate_tc_d(int use_casa_phase_convention,
+        int num_sources, int num_stations, int offset_out,
+        const double* jones, const double* I, const double* Q,
+        const double* U, const double* V, const double* station_u,
+        const double* station_v, double uv_min_lambda, double uv_max_lambda,
+        double inv_wavelength, double* vis, void* workspace,
+        size_t workspace_bytes, void* stream);
+
+/* Fused block: for every (time t, channel c) of a block,
+ *   vis[t][c] += sum_s (K_p E_p C)(s) (K_q E_q C)(s)^H
+ * with K_p(s) = exp(2 pi i (u_p l + v_p m + w_p (n - 1)) / lambda_c) formed
+ * in FP64 (mod-1 reduced) from station_uvw[t][3][num_stations] (metres) and
+ * inv_wavelength[c]; E is FP32 [station][source][2x2], shared by the whole
+ * block. vis is [num_times][num_channels][num_baselines][2x2] FP64 in the
+ * reference's baseline order. This replaces the per-channel sequence
+ * Jones K -> join -> correlate of sim_baselines
+ * (oskar/interferometer/src/oskar_interferometer_run_block.c:277-334) for
+ * point sources without smearing. The (t, c) problems are processed in
+ * groups that fit the workspace (NULL: a library-kept workspace sized for
+ * the whole block; query oskb_correlate_block_tc_workspace_bytes with
+ * num_problems = num_times * num_channels). */
+OSKB_API size_t oskb_correlate_block_tc_workspace_bytes(int num_sources,
+        int num_stations, int num_problems);
+OSKB_API int oskb_correlate_block_tc(int use_casa_phase_convention,
+        int num_sources, int num_stations, int num_times, int num_channels,
+        const float* E, const double* l, const double* m, const double* n,
+        const double* I, const double* Q, const double* U, const double* V,
+        const double* station_uvw, const double* inv_wavelength,
+        double uv_min_lambda, double uv_max_lambda, double* vis,
+        void* workspace, size_t workspace_bytes, void* stream);
+
+/* Host-buffer block driver: the same computation as
+ * oskb_correlate_block_tc with every array in HOST memory (page-locked for
+ * full-speed copies): the inputs are copied to library-kept device buffers,
+ * the visibility block is cleared, correlated and copied back into vis
+ * ([num_times][num_channels][num_baselines][2x2] FP64, overwritten). The
+ * call returns when vis holds the result. freqs_hz has num_channels
+ * entries. The role of oskar_interferometer_run_block
+ * (oskar/interferometer/oskar_interferometer.h:80) for a block of point
+ * sources without smearing. */
+OSKB_API int oskb_run_block_tc_host(int use_casa_phase_convention,
+        int num_sources, int num_stations, int num_times, int num_channels,
+        const float* E, const double* l, const double* m, const double* n,
+        const double* I, const double* Q, const double* U, const double* V,
+        const double* station_uvw, const double* freqs_hz,
+        double uv_min_lambda, double uv_max_lambda, double* vis,
+        void* stream);
+
+/* Timing of the tensor-core contraction kernel: while enabled, CUDA events
+ * are recorded around every launch of it; oskb_tc_timing_read() waits for
+ * them and returns the summed milliseconds and the launch count since the
+ * last read (or enable). No effect on results. */
+OSKB_API int oskb_tc_timing(int enable);
+OSKB_API int oskb_tc_timing_read(double* total_ms, int* launches);
+
+/* Status words of the last tensor-core call that used this workspace (NULL:
+ * the library-kept one; synchronises with the device): flags bit 0 = a
+ * brightness matrix was not positive semi-definite; wait_error != 0 = a
+ * bounded device-side wait expired (the call's result is invalid). */
+OSKB_API int oskb_tc_status(const void* workspace, int* flags,
+        int* wait_error);
+
 #ifdef __cplusplus
 }
 #endif

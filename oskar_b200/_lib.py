@@ -38,7 +38,7 @@ def parse_headers(paths=None):
         text = re.sub(r"//[^\n]*", " ", text)
         text = re.sub(r"#[^\n]*", " ", text)
         for m in re.finditer(
-                r"(int|void|const\s+char\s*\*)\s+(oskb_\w+)\s*\(([^)]*)\)\s*;",
+                r"(int|void|size_t|const\s+char\s*\*)\s+(oskb_\w+)\s*\(([^)]*)\)\s*;",
                 text):
             ret, name, args = m.group(1), m.group(2), m.group(3)
             argtypes = []
@@ -55,8 +55,8 @@ def parse_headers(paths=None):
                         raise ValueError("%s: unsupported type '%s'"
                                          % (name, base))
                     argtypes.append(_SCALARS[base])
-            restype = {"int": ctypes.c_int, "void": None}.get(
-                ret, ctypes.c_char_p)
+            restype = {"int": ctypes.c_int, "void": None,
+                       "size_t": ctypes.c_size_t}.get(ret, ctypes.c_char_p)
             protos[name] = (restype, argtypes)
     return protos
 

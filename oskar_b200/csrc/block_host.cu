@@ -1,0 +1,133 @@
+// Host-buffer form of the fused tensor-core block: the call a simulator's
+// per-block driver makes (the role of oskar_interferometer_run_block,
+// oskar/interferometer/src/oskar_interferometer_run_block.c:28-153, for
+// point sources without smearing): copy the block's inputs from host memory,
+// correlate every (time, channel) of the block on the GPU, copy the
+// visibility block back. Device buffers are kept by the library per device
+// and grown on demand; with page-locked host buffers the copies run at full
+// link speed.
+#include <string.h>
+
+#include <vector>
+
+#include "common.cuh"
+
+namespace oskb {
+namespace {
+
+struct DevBuf
+{
+    void* ptr = nullptr;
+    size_t bytes = 0;
+};
+
+struct BlockBuffers
+{
+    DevBuf E, sky, uvw, wl, vis;
+};
+
+BlockBuffers g_bufs[64];
+
+int ensure(DevBuf& b, size_t bytes)
+{
+    if (b.bytes >= bytes) return 0;
+    if (b.ptr) cudaFree(b.ptr);
+    b.ptr = nullptr;
+    b.bytes = 0;
+    if (cudaMalloc(&b.ptr, bytes) != cudaSuccess)
+    {
+        set_last_error("block buffers", cudaGetLastError());
+        return OSKB_ERR_MEMORY_ALLOC_FAILURE;
+    }
+    b.bytes = bytes;
+    return 0;
+}
+
+int copy_in(void* dst, const void* src, size_t bytes, cudaStream_t s)
+{
+    if (cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, s) !=
+            cudaSuccess)
+    {
+        set_last_error("block H2D", cudaGetLastError());
+        return OSKB_ERR_MEMORY_COPY_FAILURE;
+    }
+    return 0;
+}
+
+}  // namespace
+}  // namespace oskb
+
+using namespace oskb;
+
+extern "C" int oskb_run_block_tc_host(int casa, int num_sources,
+        int num_stations, int num_times, int num_channels, const float* E,
+        const double* l, const double* m, const double* n, const double* I,
+        const double* Q, const double* U, const double* V,
+        const double* station_uvw, const double* freqs_hz,
+        double uv_min_lambda, double uv_max_lambda, double* vis,
+        void* stream)
+{
+    if (num_sources < 0 || num_stations < 0 || num_times < 0 ||
+            num_channels < 0)
+        return OSKB_ERR_INVALID_ARGUMENT;
+    if (num_times == 0 || num_channels == 0 || num_stations < 2) return 0;
+    if (!vis || !station_uvw || !freqs_hz) return OSKB_ERR_INVALID_ARGUMENT;
+    const size_t nbl = (size_t) num_stations * (num_stations - 1) / 2;
+    const size_t vis_bytes = (size_t) num_times * num_channels * nbl * 64;
+    cudaStream_t s = as_stream(stream);
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (dev < 0 || dev >= 64) return OSKB_ERR_INVALID_ARGUMENT;
+    BlockBuffers& b = g_bufs[dev];
+    int err = ensure(b.vis, vis_bytes);
+    if (err) return err;
+    if (num_sources == 0)
+    {
+        memset(vis, 0, vis_bytes);
+        return 0;
+    }
+    if (!E || !l || !m || !n || !I || !Q || !U || !V)
+        return OSKB_ERR_INVALID_ARGUMENT;
+    const size_t e_bytes = (size_t) num_stations * num_sources * 8 *
+            sizeof(float);
+    const size_t sky_bytes = 7 * (size_t) num_sources * sizeof(double);
+    const size_t uvw_bytes = (size_t) num_times * 3 * num_stations *
+            sizeof(double);
+    if ((err = ensure(b.E, e_bytes)) || (err = ensure(b.sky, sky_bytes)) ||
+            (err = ensure(b.uvw, uvw_bytes)) ||
+            (err = ensure(b.wl, num_channels * sizeof(double))))
+        return err;
+    double* sky = static_cast<double*>(b.sky.ptr);
+    const double* src[7] = {l, m, n, I, Q, U, V};
+    std::vector<double> wl(num_channels);
+    for (int c = 0; c < num_channels; ++c) wl[c] = freqs_hz[c] / 299792458.0;
+    if ((err = copy_in(b.E.ptr, E, e_bytes, s))) return err;
+    for (int k = 0; k < 7; ++k)
+        if ((err = copy_in(sky + (size_t) k * num_sources, src[k],
+                num_sources * sizeof(double), s)))
+            return err;
+    if ((err = copy_in(b.uvw.ptr, station_uvw, uvw_bytes, s))) return err;
+    if ((err = copy_in(b.wl.ptr, wl.data(), num_channels * sizeof(double),
+            s)))
+        return err;
+    // The block is cleared, then accumulated, as the reference does.
+    cudaMemsetAsync(b.vis.ptr, 0, vis_bytes, s);
+    err = oskb_correlate_block_tc(casa, num_sources, num_stations, num_times,
+            num_channels, static_cast<const float*>(b.E.ptr), sky,
+            sky + num_sources, sky + 2 * (size_t) num_sources,
+            sky + 3 * (size_t) num_sources, sky + 4 * (size_t) num_sources,
+            sky + 5 * (size_t) num_sources, sky + 6 * (size_t) num_sources,
+            static_cast<const double*>(b.uvw.ptr),
+            static_cast<const double*>(b.wl.ptr), uv_min_lambda,
+            uv_max_lambda, static_cast<double*>(b.vis.ptr), nullptr, 0,
+            stream);
+    if (err) return err;
+    if (cudaMemcpyAsync(vis, b.vis.ptr, vis_bytes, cudaMemcpyDeviceToHost, s)
+            != cudaSuccess ||
+            cudaStreamSynchronize(s) != cudaSuccess)
+    {
+        set_last_error("block D2H", cudaGetLastError());
+        return OSKB_ERR_MEMORY_COPY_FAILURE;
+    }
+    return 0;
+}

@@ -133,7 +133,7 @@ xcorr_direct_kernel(const XcorrParams<T> prm)
             const bool in = (st < N) && (sl < ns);
             // Left factor (J B, or I J) lives in the row block unless CASA.
             const bool left = (blk == 0) != CASA;
-            T2* dst = blk ? &sm.col[0][sl][stl] : &sm.row[0][sl][stl];
+            T2 (*dst)[kChunk][kTile] = blk ? sm.col : sm.row;
             if (MATRIX)
             {
                 Mat2<T> J;
@@ -156,10 +156,10 @@ xcorr_direct_kernel(const XcorrParams<T> prm)
                     M.d = T2{J.d.x * yy + t3.x, J.d.y * yy + t3.y};
                     J = M;
                 }
-                dst[0] = J.a;
-                dst[1 * kChunk * kTile] = J.b;
-                dst[2 * kChunk * kTile] = J.c;
-                dst[3 * kChunk * kTile] = J.d;
+                dst[0][sl][stl] = J.a;
+                dst[1][sl][stl] = J.b;
+                dst[2][sl][stl] = J.c;
+                dst[3][sl][stl] = J.d;
             }
             else
             {
@@ -172,7 +172,7 @@ xcorr_direct_kernel(const XcorrParams<T> prm)
                     const T I = prm.I[s];
                     J.x *= I; J.y *= I;
                 }
-                dst[0] = J;
+                dst[0][sl][stl] = J;
             }
             if (BW || TS)
             {
@@ -246,7 +246,7 @@ xcorr_direct_kernel(const XcorrParams<T> prm)
                     const T2* L = CASA ? C[j] : R[i];
                     const T2* Rt = CASA ? R[i] : C[j];
                     T t[2 * NC];
-                    if (MATRIX)
+                    if constexpr (MATRIX)
                     {
                         // a = La Ra* + Lb Rb*, b = La Rc* + Lb Rd*,
                         // c = Lc Ra* + Ld Rb*, d = Lc Rc* + Ld Rd*

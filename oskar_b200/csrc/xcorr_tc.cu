@@ -1,0 +1,956 @@
+// Tensor-core (tcgen05) compensated cross-correlation of point sources
+// without smearing.
+//
+// Algebra. With the brightness factored as B(s) = C(s) C(s)^H (C the lower
+// Cholesky factor of [[I+Q, U+iV], [U-iV, I-Q]]), A_p(s) = J_p(s) C(s) and
+//     V_pq = sum_s A_p(s) A_q(s)^H,
+// i.e. V = X X^H, a Hermitian rank-k update over sources. Interleaving the
+// real and imaginary parts as rows, W[(p, i, c)][(s, kk)] = part c of
+// A_p(s)[i][kk], turns it into the real symmetric product G = W W^T:
+//     Re V_pq[i][j] = G[(p,i,0),(q,j,0)] + G[(p,i,1),(q,j,1)]
+//     Im V_pq[i][j] = G[(p,i,1),(q,j,0)] - G[(p,i,0),(q,j,1)]
+// and only the upper block triangle of G is computed.
+//
+// Precision. W is scaled by a power of two S (largest |entry| -> 2^14) and
+// split into two FP16 pieces, W = hi + lo (22 significant bits); G is formed
+// from the three products hi hi^T + hi lo^T + lo hi^T on the tensor cores
+// (FP16 x FP16 products are exact in FP32), accumulated in FP32 in TMEM for
+// a bounded number of k-blocks and then added into FP64 registers (the
+// cross-tile sum is FP64). The hi hi^T products go to their own TMEM
+// accumulator: the tensor core rounds its FP32 accumulator once per MMA,
+// and keeping the 2^-11-smaller correction products out of it leaves only
+// four full-size accumulate steps per k-block. The interferometer phase is formed in FP64 and
+// reduced mod 1 cycle before an FP32 sincospi.
+//
+// Layout of the operand image (per problem): tiles of 128 rows (32 stations)
+// x 64 columns (32 sources) of FP16, each 16 KB, stored exactly as the MMA
+// reads them from shared memory (K-major, 128-byte swizzle), hi tile then lo
+// tile, ordered [row block][k block][hi, lo]. A pipeline stage is therefore
+// one 32 KB bulk copy per operand.
+#include <cuda_fp16.h>
+
+#include <utility>
+#include <vector>
+
+#include "common.cuh"
+#include "tc_ptx.cuh"
+
+namespace oskb {
+namespace tc {
+
+constexpr int kStPerBlock = 32;              // stations per 128-row block
+constexpr int kSrcPerBlock = 32;             // sources per 64-column block
+constexpr int kTileBytes = 128 * 128;        // 128 rows x 128 bytes
+constexpr int kPairBytes = 2 * kTileBytes;   // hi + lo
+constexpr float kScaleTarget = 16384.0f;     // largest scaled |entry|
+
+__host__ __device__ inline size_t image_bytes(int num_st, int num_src)
+{
+    const size_t nrb = (num_st + kStPerBlock - 1) / kStPerBlock;
+    const size_t nkb = (num_src + kSrcPerBlock - 1) / kSrcPerBlock;
+    return nrb * nkb * kPairBytes;
+}
+
+// Power-of-two scale that maps the largest |entry| to at most 2^14.
+__device__ __forceinline__ float scale_from_bits(unsigned int bits)
+{
+    const float m = __uint_as_float(bits);
+    if (!(m > 0.0f) || !isfinite(m)) return 1.0f;
+    const float e = floorf(log2f(kScaleTarget / m));
+    return exp2f(fminf(fmaxf(e, -100.0f), 100.0f));
+}
+
+// Byte offset of the 4-byte word holding columns (2*sl, 2*sl+1) of tile row
+// r, with the 128-byte swizzle applied (16-byte chunk index XOR row % 8).
+__device__ __forceinline__ uint32_t swz_offset(int r, int sl)
+{
+    return (uint32_t) (r * 128 + ((((sl >> 2) ^ (r & 7)) & 7) << 4) +
+                       (sl & 3) * 4);
+}
+
+// Lower Cholesky factor C of B = [[I+Q, U+iV], [U-iV, I-Q]]:
+// C = [[c11, 0], [c21, c22]], c11 and c22 real. Returns false when B is not
+// positive semi-definite (beyond rounding); C is then the factor of the
+// nearest PSD matrix with that diagonal clipped at zero.
+__device__ __forceinline__ bool brightness_factor(double I, double Q,
+        double U, double V, float& c11, float& c21r, float& c21i, float& c22)
+{
+    const double xx = I + Q, yy = I - Q;
+    const double tol = 1e-12 * (fabs(I) + fabs(Q) + fabs(U) + fabs(V));
+    bool ok = true;
+    if (xx > tol)
+    {
+        const double a = sqrt(xx);
+        const double br = U / a, bi = -V / a;
+        const double d = yy - (br * br + bi * bi);
+        if (d < -tol) ok = false;
+        c11 = (float) a; c21r = (float) br; c21i = (float) bi;
+        c22 = (float) sqrt(fmax(d, 0.0));
+    }
+    else
+    {
+        if (xx < -tol || fabs(U) > tol || fabs(V) > tol) ok = false;
+        c11 = 0.0f; c21r = 0.0f; c21i = 0.0f;
+        c22 = (float) sqrt(fmax(yy, 0.0));
+    }
+    return ok;
+}
+
+// A = J C for a 2x2 complex J (row-major {a, b, c, d}) and lower-triangular
+// C; out[i][kk][part].
+__device__ __forceinline__ void apply_factor(const float* J, float c11,
+        float c21r, float c21i, float c22, float out[2][2][2])
+{
+#pragma unroll
+    for (int i = 0; i < 2; ++i)
+    {
+        const float j0r = J[4 * i + 0], j0i = J[4 * i + 1];
+        const float j1r = J[4 * i + 2], j1i = J[4 * i + 3];
+        out[i][0][0] = j0r * c11 + (j1r * c21r - j1i * c21i);
+        out[i][0][1] = j0i * c11 + (j1r * c21i + j1i * c21r);
+        out[i][1][0] = j1r * c22;
+        out[i][1][1] = j1i * c22;
+    }
+}
+
+template <typename TJ>
+__device__ __forceinline__ void load_jones(const TJ* p, float* J)
+{
+#pragma unroll
+    for (int k = 0; k < 8; ++k) J[k] = (float) p[k];
+}
+
+template <>
+__device__ __forceinline__ void load_jones<float>(const float* p, float* J)
+{
+    const float4 a = __ldg(reinterpret_cast<const float4*>(p));
+    const float4 b = __ldg(reinterpret_cast<const float4*>(p) + 1);
+    J[0] = a.x; J[1] = a.y; J[2] = a.z; J[3] = a.w;
+    J[4] = b.x; J[5] = b.y; J[6] = b.z; J[7] = b.w;
+}
+
+template <>
+__device__ __forceinline__ void load_jones<double>(const double* p, float* J)
+{
+    const double2* q = reinterpret_cast<const double2*>(p);
+#pragma unroll
+    for (int k = 0; k < 4; ++k)
+    {
+        const double2 v = __ldg(q + k);
+        J[2 * k] = (float) v.x; J[2 * k + 1] = (float) v.y;
+    }
+}
+
+// Writes one station-source's 2x2 A (already scaled) as 4 tile rows of the
+// hi and lo tiles.
+__device__ __forceinline__ void store_entry(uint8_t* tile_hi, int pl, int sl,
+        const float A[2][2][2])
+{
+    uint8_t* tile_lo = tile_hi + kTileBytes;
+#pragma unroll
+    for (int i = 0; i < 2; ++i)
+#pragma unroll
+        for (int c = 0; c < 2; ++c)
+        {
+            const int r = 4 * pl + 2 * i + c;
+            const float x0 = A[i][0][c], x1 = A[i][1][c];
+            const __half h0 = __float2half_rn(x0), h1 = __float2half_rn(x1);
+            const __half l0 = __float2half_rn(x0 - __half2float(h0));
+            const __half l1 = __float2half_rn(x1 - __half2float(h1));
+            const uint32_t off = swz_offset(r, sl);
+            *reinterpret_cast<__half2*>(tile_hi + off) = __halves2half2(h0, h1);
+            *reinterpret_cast<__half2*>(tile_lo + off) = __halves2half2(l0, l1);
+        }
+}
+
+// ---------------------------------------------------------------------------
+// Largest |component| of J C over all station-sources (-> the scale S).
+// ---------------------------------------------------------------------------
+// The bound uses the complex modulus of each entry, so it also holds after
+// the unit-modulus phase K is applied.
+template <typename TJ, typename TF>
+__global__ void __launch_bounds__(256) maxabs_kernel(const TJ* __restrict__ jones,
+        int num_src, int num_st, const TF* __restrict__ I,
+        const TF* __restrict__ Q, const TF* __restrict__ U,
+        const TF* __restrict__ V, unsigned int* maxabs_bits, int* flags)
+{
+    float mx = 0.0f;
+    bool psd = true;
+    const size_t total = (size_t) num_st * num_src;
+    for (size_t idx = (size_t) blockIdx.x * blockDim.x + threadIdx.x;
+            idx < total; idx += (size_t) gridDim.x * blockDim.x)
+    {
+        const int s = (int) (idx % num_src);
+        float c11, c21r, c21i, c22, J[8], A[2][2][2];
+        psd &= brightness_factor(I[s], Q[s], U[s], V[s], c11, c21r, c21i,
+                c22);
+        load_jones<TJ>(jones + 8 * idx, J);
+        apply_factor(J, c11, c21r, c21i, c22, A);
+#pragma unroll
+        for (int i = 0; i < 2; ++i)
+#pragma unroll
+            for (int kk = 0; kk < 2; ++kk)
+                mx = fmaxf(mx, hypotf(A[i][kk][0], A[i][kk][1]));
+    }
+    for (int o = 16; o > 0; o >>= 1)
+        mx = fmaxf(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+    if ((threadIdx.x & 31) == 0) atomicMax(maxabs_bits, __float_as_uint(mx));
+    if (!psd) atomicOr(flags, 1);
+}
+
+// ---------------------------------------------------------------------------
+// Operand image from joined Jones J (the oskar_cross_correlate input).
+// grid (k blocks, row blocks, problems); 8 warps, warp = 4 stations,
+// lane = source.
+// ---------------------------------------------------------------------------
+template <typename TJ>
+__global__ void __launch_bounds__(256) prep_jones_kernel(
+        const TJ* __restrict__ jones, int num_src, int num_st,
+        const TJ* __restrict__ I, const TJ* __restrict__ Q,
+        const TJ* __restrict__ U, const TJ* __restrict__ V,
+        const unsigned int* __restrict__ maxabs_bits, uint8_t* W)
+{
+    const int kb = blockIdx.x, rb = blockIdx.y, nkb = gridDim.x;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int s = kb * kSrcPerBlock + lane;
+    const bool src_ok = s < num_src;
+    float c11 = 0, c21r = 0, c21i = 0, c22 = 0;
+    if (src_ok) brightness_factor(I[s], Q[s], U[s], V[s], c11, c21r, c21i, c22);
+    const float S = scale_from_bits(*maxabs_bits);
+    uint8_t* tile = W + (size_t) (rb * nkb + kb) * kPairBytes;
+    for (int pl = warp; pl < kStPerBlock; pl += 8)
+    {
+        const int p = rb * kStPerBlock + pl;
+        float A[2][2][2] = {{{0, 0}, {0, 0}}, {{0, 0}, {0, 0}}};
+        if (src_ok && p < num_st)
+        {
+            float J[8];
+            load_jones<TJ>(jones + 8 * ((size_t) p * num_src + s), J);
+            apply_factor(J, c11, c21r, c21i, c22, A);
+#pragma unroll
+            for (int k = 0; k < 8; ++k) (&A[0][0][0])[k] *= S;
+        }
+        store_entry(tile, pl, lane, A);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Fused operand image: A = K (E C) with the interferometer phase
+//   K_p(s) = exp(2 pi i x),  x = (u_p l + v_p m + w_p (n - 1)) / lambda,
+// x formed in FP64 and reduced to [-1/2, 1/2] before an FP32 sincospi.
+// E is FP32 [station][source][2x2], shared by every problem. Problems are
+// (time, channel) pairs, prob = t * nch + c: station (u, v, w) of time t at
+// uvw[t][3][num_st], 1/lambda of channel c. One launch writes the images of
+// problems [p0, p0 + np) (image prob - p0 at W + (prob - p0) * image_stride),
+// reading E and forming E C once per station-source for all of them.
+// grid (k blocks, row blocks); 8 warps, warp = 4 stations, lane = source.
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(256) prep_fused_kernel(
+        const float* __restrict__ E, int num_src, int num_st,
+        const double* __restrict__ l, const double* __restrict__ m,
+        const double* __restrict__ n, const double* __restrict__ I,
+        const double* __restrict__ Q, const double* __restrict__ U,
+        const double* __restrict__ V, const double* __restrict__ uvw,
+        const double* __restrict__ inv_wavelength, int nch, int p0, int np,
+        const unsigned int* __restrict__ maxabs_bits, uint8_t* W,
+        size_t image_stride)
+{
+    const int kb = blockIdx.x, rb = blockIdx.y;
+    const int nkb = gridDim.x;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int s = kb * kSrcPerBlock + lane;
+    const bool src_ok = s < num_src;
+    float c11 = 0, c21r = 0, c21i = 0, c22 = 0;
+    double sl = 0, sm = 0, sn1 = 0;
+    if (src_ok)
+    {
+        brightness_factor(I[s], Q[s], U[s], V[s], c11, c21r, c21i, c22);
+        sl = l[s]; sm = m[s]; sn1 = n[s] - 1.0;
+    }
+    const float S = scale_from_bits(*maxabs_bits);
+    uint8_t* tile0 = W + (size_t) (rb * nkb + kb) * kPairBytes;
+    for (int pl = warp; pl < kStPerBlock; pl += 8)
+    {
+        const int p = rb * kStPerBlock + pl;
+        const bool ok = src_ok && p < num_st;
+        float A0[2][2][2] = {{{0, 0}, {0, 0}}, {{0, 0}, {0, 0}}};
+        if (ok)
+        {
+            float J[8];
+            load_jones<float>(E + 8 * ((size_t) p * num_src + s), J);
+            apply_factor(J, c11, c21r, c21i, c22, A0);
+#pragma unroll
+            for (int k = 0; k < 8; ++k) (&A0[0][0][0])[k] *= S;
+        }
+        for (int j = 0; j < np; ++j)
+        {
+            const int prob = p0 + j, t = prob / nch, c = prob - t * nch;
+            float A[2][2][2] = {{{0, 0}, {0, 0}}, {{0, 0}, {0, 0}}};
+            if (ok)
+            {
+                const double* pu = uvw + (size_t) t * 3 * num_st;
+                const double x = (pu[p] * sl + pu[num_st + p] * sm +
+                                  pu[2 * num_st + p] * sn1) *
+                                 inv_wavelength[c];
+                const float f = (float) (x - rint(x));
+                float sn, cs;
+                sincospif(2.0f * f, &sn, &cs);
+#pragma unroll
+                for (int i = 0; i < 2; ++i)
+#pragma unroll
+                    for (int kk = 0; kk < 2; ++kk)
+                    {
+                        const float re = A0[i][kk][0], im = A0[i][kk][1];
+                        A[i][kk][0] = re * cs - im * sn;
+                        A[i][kk][1] = re * sn + im * cs;
+                    }
+            }
+            store_entry(tile0 + (size_t) j * image_stride, pl, lane, A);
+        }
+    }
+}
+
+}  // namespace tc
+}  // namespace oskb
+
+// ===========================================================================
+// G = W W^T on the tensor cores, upper block triangle, fused visibility
+// epilogue. Persistent CTAs (one per SM) walk the task list
+//     task = problem * ntile + tile,  tile -> (rb <= cb)
+// Warp roles (320 threads):
+//   warp 0 (one lane): bulk copies of the A (row block rb) and B (row block
+//     cb) hi/lo tile pairs into a kStages-deep shared-memory ring;
+//   warp 1 (one lane): issues the tcgen05 MMAs (3 products per 16-wide k
+//     step) into one of two TMEM buffers, each a pair of 128-column FP32
+//     accumulators (hi hi^T, and hi lo^T + lo hi^T);
+//   warps 2-9: drain the accumulator every drain_kb k-blocks into FP64
+//     registers (one TMEM lane = one row of G, 64 columns per warp), then
+//     form the four polarisations and add them into vis.
+// ===========================================================================
+namespace oskb {
+namespace tc {
+
+constexpr int kStages = 3;
+constexpr int kStageBytes = 2 * kPairBytes;   // A pair + B pair
+constexpr int kGemmThreads = 320;
+constexpr int kAccCols = 128;                 // one FP32 accumulator
+constexpr int kBufCols = 2 * kAccCols;        // main + correction
+constexpr uint32_t kTmemCols = 2 * kBufCols;  // double-buffered: all 512
+
+struct GemmParams
+{
+    const uint8_t* W;
+    size_t image_stride;        // bytes per problem
+    int nrb, nkb, num_problems, num_st;
+    int drain_kb;
+    const unsigned int* maxabs_bits;
+    int maxabs_stride;          // 0: one scale for all problems
+    // Problem j of this launch is global problem g = prob0 + j of a
+    // (time, channel) block, g = t * nch + c.
+    int prob0, nch;
+    double* vis;                // vis of global problem g at
+    size_t vis_stride;          //   vis + 8 * (g * vis_stride + offset_out)
+    int offset_out;
+    const double* st_u;         // station u, v (metres) of time t at
+    const double* st_v;         //   st_u + t * uv_stride, st_v + ...
+    size_t uv_stride;
+    const double* inv_wavelength;  // [nch], or NULL: use kw_scalar
+    double kw_scalar;
+    double uv_min, uv_max;
+    int casa;
+    int* err;
+};
+
+struct GemmCtl
+{
+    uint64_t full[kStages], empty[kStages], tfull[2], tempty[2], done;
+    uint32_t tmem_base;
+    int abort;
+};
+
+constexpr size_t gemm_smem_bytes()
+{
+    return 1024 + (size_t) kStages * kStageBytes + sizeof(GemmCtl);
+}
+
+__device__ __forceinline__ void tile_of(int t, int& rb, int& cb)
+{
+    int c = (int) ((sqrt(8.0 * t + 1.0) - 1.0) * 0.5);
+    while ((c + 1) * (c + 2) / 2 <= t) ++c;
+    while (c * (c + 1) / 2 > t) --c;
+    cb = c;
+    rb = t - c * (c + 1) / 2;
+}
+
+__global__ void __launch_bounds__(kGemmThreads, 1)
+gemm_kernel(const GemmParams prm)
+{
+    extern __shared__ uint8_t smem_raw[];
+    uint8_t* smem = reinterpret_cast<uint8_t*>(
+            (reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~(uintptr_t) 1023);
+    GemmCtl* ctl = reinterpret_cast<GemmCtl*>(smem + kStages * kStageBytes);
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    volatile int* abort = &ctl->abort;
+
+    if (threadIdx.x == 0)
+    {
+        for (int s = 0; s < kStages; ++s)
+        {
+            ptx::mbar_init(&ctl->full[s], 1);
+            ptx::mbar_init(&ctl->empty[s], 1);
+        }
+        for (int b = 0; b < 2; ++b)
+        {
+            ptx::mbar_init(&ctl->tfull[b], 1);
+            ptx::mbar_init(&ctl->tempty[b], 8);
+        }
+        ptx::mbar_init(&ctl->done, 1);
+        ctl->abort = 0;
+        ptx::fence_mbar_init();
+    }
+    if (warp == 1) ptx::tmem_alloc(&ctl->tmem_base, kTmemCols);
+    ptx::tc_fence_before();
+    __syncthreads();
+    ptx::tc_fence_after();
+    const uint32_t tmem = ctl->tmem_base;
+
+    const int ntile = prm.nrb * (prm.nrb + 1) / 2;
+    const int ntasks = ntile * prm.num_problems;
+    const int nchunk = (prm.nkb + prm.drain_kb - 1) / prm.drain_kb;
+
+    if (warp == 0)
+    {
+        if (lane == 0)
+        {
+            // ---------------- producer
+            int stage = 0;
+            uint32_t phase = 0;
+            uint32_t issued = 0, issued_par = 0;  // bit s: stage s
+            for (int task = blockIdx.x; task < ntasks && !*abort;
+                    task += gridDim.x)
+            {
+                const int prob = task / ntile;
+                int rb, cb;
+                tile_of(task - prob * ntile, rb, cb);
+                const bool diag = rb == cb;
+                const uint8_t* img = prm.W + (size_t) prob * prm.image_stride;
+                for (int kb = 0; kb < prm.nkb; ++kb)
+                {
+                    if (!ptx::mbar_wait(&ctl->empty[stage], phase ^ 1,
+                            prm.err, 11, abort))
+                        break;
+                    uint8_t* dst = smem + (size_t) stage * kStageBytes;
+                    ptx::mbar_arrive_expect_tx(&ctl->full[stage],
+                            diag ? kPairBytes : 2 * kPairBytes);
+                    ptx::bulk_g2s(dst, img + ((size_t) rb * prm.nkb + kb) *
+                            kPairBytes, kPairBytes, &ctl->full[stage]);
+                    if (!diag)
+                        ptx::bulk_g2s(dst + kPairBytes, img +
+                                ((size_t) cb * prm.nkb + kb) * kPairBytes,
+                                kPairBytes, &ctl->full[stage]);
+                    issued |= 1u << stage;
+                    issued_par = (issued_par & ~(1u << stage)) |
+                            (phase << stage);
+                    if (++stage == kStages) { stage = 0; phase ^= 1; }
+                }
+            }
+            // Copies still in flight must land before the CTA can exit.
+            for (int s = 0; s < kStages; ++s)
+                if ((issued >> s) & 1)
+                    ptx::mbar_wait(&ctl->full[s], (issued_par >> s) & 1,
+                            prm.err, 12, abort);
+        }
+        __syncwarp();
+    }
+    else if (warp == 1)
+    {
+        if (lane == 0)
+        {
+            // ---------------- MMA issuer
+            const uint32_t idesc = ptx::idesc_f16_f32(128, kAccCols);
+            int stage = 0;
+            uint32_t phase = 0, tpar = 0;  // tpar bit b: use parity of buf b
+            int buf = 0;
+            bool ok = true;
+            for (int task = blockIdx.x; task < ntasks && ok;
+                    task += gridDim.x)
+            {
+                const int prob = task / ntile;
+                int rb, cb;
+                tile_of(task - prob * ntile, rb, cb);
+                const bool diag = rb == cb;
+                for (int ch = 0; ch < nchunk && ok; ++ch)
+                {
+                    if (!ptx::mbar_wait(&ctl->tempty[buf],
+                            ((tpar >> buf) & 1) ^ 1, prm.err, 13, abort))
+                    {
+                        ok = false;
+                        break;
+                    }
+                    ptx::tc_fence_after();
+                    const uint32_t d = tmem + (uint32_t) (buf * kBufCols);
+                    const uint32_t dc = d + kAccCols;
+                    const int kb0 = ch * prm.drain_kb;
+                    const int kb1 = min(prm.nkb, kb0 + prm.drain_kb);
+                    for (int kb = kb0; kb < kb1; ++kb)
+                    {
+                        if (!ptx::mbar_wait(&ctl->full[stage], phase, prm.err,
+                                14, abort))
+                        {
+                            ok = false;
+                            break;
+                        }
+                        ptx::tc_fence_after();
+                        const uint32_t a = ptx::smem_u32(smem +
+                                (size_t) stage * kStageBytes);
+                        const uint32_t b = diag ? a : a + kPairBytes;
+#pragma unroll
+                        for (int k = 0; k < 4; ++k)
+                        {
+                            const uint64_t ah = ptx::sdesc_sw128(a + 32 * k);
+                            const uint64_t al = ptx::sdesc_sw128(
+                                    a + kTileBytes + 32 * k);
+                            const uint64_t bh = ptx::sdesc_sw128(b + 32 * k);
+                            const uint64_t bl = ptx::sdesc_sw128(
+                                    b + kTileBytes + 32 * k);
+                            const uint32_t acc =
+                                    (kb > kb0 || k > 0) ? 1u : 0u;
+                            ptx::mma_f16(d, ah, bh, idesc, acc);
+                            ptx::mma_f16(dc, ah, bl, idesc, acc);
+                            ptx::mma_f16(dc, al, bh, idesc, 1u);
+                        }
+                        ptx::mma_commit(&ctl->empty[stage]);
+                        if (++stage == kStages) { stage = 0; phase ^= 1; }
+                    }
+                    if (!ok) break;
+                    ptx::mma_commit(&ctl->tfull[buf]);
+                    tpar ^= 1u << buf;
+                    buf ^= 1;
+                }
+            }
+            // All issued MMAs must finish before TMEM is released.
+            ptx::mma_commit(&ctl->done);
+            ptx::mbar_wait(&ctl->done, 0, prm.err, 15, abort);
+        }
+        __syncwarp();
+    }
+    else
+    {
+        // ---------------- epilogue: 8 warps
+        const int q4 = warp & 3;          // TMEM lane quadrant of this warp
+        const int h = (warp - 2) >> 2;    // column half
+        const int row = 32 * q4 + lane;   // row of the G tile
+        const uint32_t taddr = tmem + ((uint32_t) (32 * q4) << 16) +
+                (uint32_t) (64 * h);
+        int buf = 0;
+        uint32_t tpar = 0;
+        bool ok = true;
+        for (int task = blockIdx.x; task < ntasks && ok; task += gridDim.x)
+        {
+            const int prob = task / ntile;
+            int rb, cb;
+            tile_of(task - prob * ntile, rb, cb);
+            double acc[64];
+#pragma unroll
+            for (int j = 0; j < 64; ++j) acc[j] = 0.0;
+            for (int ch = 0; ch < nchunk; ++ch)
+            {
+                if (!ptx::mbar_wait(&ctl->tfull[buf], (tpar >> buf) & 1,
+                        prm.err, 16, abort))
+                {
+                    ok = false;
+                    break;
+                }
+                ptx::tc_fence_after();
+                const uint32_t ta = taddr + (uint32_t) (buf * kBufCols);
+#pragma unroll
+                for (int j0 = 0; j0 < 64; j0 += 16)
+                {
+                    uint32_t vm[16], vc[16];
+                    ptx::tmem_ld16(ta + j0, vm);
+                    ptx::tmem_ld16(ta + kAccCols + j0, vc);
+                    ptx::tmem_ld_wait();
+#pragma unroll
+                    for (int j = 0; j < 16; ++j)
+                        acc[j0 + j] += (double) (__uint_as_float(vm[j]) +
+                                                 __uint_as_float(vc[j]));
+                }
+                ptx::tc_fence_before();
+                __syncwarp();
+                if (lane == 0) ptx::mbar_arrive(&ctl->tempty[buf]);
+                tpar ^= 1u << buf;
+                buf ^= 1;
+            }
+            if (!ok) break;
+            // ---- visibilities of this tile
+            const int g = prm.prob0 + prob, t = g / prm.nch;
+            const int chan = g - t * prm.nch;
+            const float S = scale_from_bits(
+                    prm.maxabs_bits[prm.maxabs_stride * g]);
+            const double inv_s2 = 1.0 / ((double) S * (double) S);
+            const int c = row & 1, i = (row >> 1) & 1;
+            const int p = rb * kStPerBlock + (row >> 2);
+            const int N = prm.num_st;
+            const double* su = prm.st_u + prm.uv_stride * t;
+            const double* sv = prm.st_v + prm.uv_stride * t;
+            const double kw = prm.inv_wavelength ? prm.inv_wavelength[chan]
+                                                  : prm.kw_scalar;
+            double* vbase = prm.vis + 8 * ((size_t) g * prm.vis_stride +
+                    (size_t) prm.offset_out);
+#pragma unroll
+            for (int ql = 0; ql < 16; ++ql)
+            {
+                const int jb = 4 * ql;
+                const double s0 = c ? acc[jb + 0] : acc[jb + 2];
+                const double s1 = c ? acc[jb + 1] : acc[jb + 3];
+                const double r0 = __shfl_xor_sync(0xffffffffu, s0, 1);
+                const double r1 = __shfl_xor_sync(0xffffffffu, s1, 1);
+                const double g00 = c ? r0 : acc[jb + 0];
+                const double g01 = c ? r1 : acc[jb + 1];
+                const double g10 = c ? acc[jb + 2] : r0;
+                const double g11 = c ? acc[jb + 3] : r1;
+                const int q = cb * kStPerBlock + 16 * h + ql;
+                if (p < q && q < N)
+                {
+                    const double uu = (su[p] - su[q]) * kw;
+                    const double vv = (sv[p] - sv[q]) * kw;
+                    const double len = sqrt(uu * uu + vv * vv);
+                    if (!(len < prm.uv_min || len > prm.uv_max))
+                    {
+                        const double re = (g00 + g11) * inv_s2;
+                        const double im = (g10 - g01) * inv_s2;
+                        // this thread holds V_pq[i][j] with j = c; the
+                        // reference stores J_q B J_p^H (p < q) unless CASA
+                        const int ro = prm.casa ? i : c;
+                        const int co = prm.casa ? c : i;
+                        double* o = vbase + 8 * (size_t) baseline_index(N, q, p)
+                                + 2 * (2 * ro + co);
+                        o[0] += re;
+                        o[1] += prm.casa ? im : -im;
+                    }
+                }
+            }
+        }
+    }
+
+    ptx::tc_fence_before();
+    __syncthreads();
+    ptx::tc_fence_after();
+    if (warp == 1) ptx::tmem_dealloc(tmem, kTmemCols);
+}
+
+}  // namespace tc
+}  // namespace oskb
+
+// ===========================================================================
+// Host side
+// ===========================================================================
+namespace oskb {
+namespace tc {
+namespace {
+
+constexpr size_t kHeaderBytes = 256;  // maxabs bits, flags, error word
+
+struct Header
+{
+    unsigned int maxabs_bits;
+    int flags;   // bit 0: a brightness matrix was not positive semi-definite
+    int err;     // non-zero: a bounded wait expired (code of the wait)
+};
+
+int num_sms()
+{
+    static int n = 0;
+    if (!n)
+    {
+        int dev = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev);
+        if (n <= 0) n = 148;
+    }
+    return n;
+}
+
+int drain_kblocks()
+{
+    static int d = 0;
+    if (!d)
+    {
+        const char* e = getenv("OSKB_TC_DRAIN_KB");
+        d = e ? atoi(e) : 2;
+        if (d < 1) d = 1;
+    }
+    return d;
+}
+
+// Problems per group when the library keeps the workspace (each problem's
+// operand image is 16 bytes per station-source).
+int max_group()
+{
+    static int g = 0;
+    if (!g)
+    {
+        const char* e = getenv("OSKB_TC_MAX_GROUP");
+        g = e ? atoi(e) : 16;
+        if (g < 1) g = 1;
+    }
+    return g;
+}
+
+// Library-managed workspace, one per device, grown on demand.
+struct CachedWorkspace
+{
+    void* ptr = nullptr;
+    size_t bytes = 0;
+};
+CachedWorkspace g_ws[64];
+
+int get_workspace(void*& ws, size_t& ws_bytes, size_t need)
+{
+    if (ws)
+        return ws_bytes >= need ? 0 : OSKB_ERR_MEMORY_ALLOC_FAILURE;
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (dev < 0 || dev >= 64) return OSKB_ERR_INVALID_ARGUMENT;
+    CachedWorkspace& c = g_ws[dev];
+    if (c.bytes < need)
+    {
+        if (c.ptr) cudaFree(c.ptr);
+        c.ptr = nullptr;
+        c.bytes = 0;
+        if (cudaMalloc(&c.ptr, need) != cudaSuccess)
+        {
+            set_last_error("tc workspace", cudaGetLastError());
+            return OSKB_ERR_MEMORY_ALLOC_FAILURE;
+        }
+        c.bytes = need;
+    }
+    ws = c.ptr;
+    ws_bytes = c.bytes;
+    return 0;
+}
+
+// Optional CUDA-event timing of every GEMM launch (for roofline reports).
+bool g_timing = false;
+std::vector<std::pair<cudaEvent_t, cudaEvent_t>> g_ev;
+size_t g_ev_used = 0;
+
+int launch_gemm(GemmParams& gp, cudaStream_t stream)
+{
+    static bool attr_set = false;
+    if (!attr_set)
+    {
+        cudaFuncSetAttribute(gemm_kernel,
+                cudaFuncAttributeMaxDynamicSharedMemorySize,
+                (int) gemm_smem_bytes());
+        attr_set = true;
+    }
+    const long long ntasks = (long long) gp.nrb * (gp.nrb + 1) / 2 *
+            gp.num_problems;
+    const int grid = (int) (ntasks < num_sms() ? ntasks : num_sms());
+    gp.drain_kb = drain_kblocks();
+    cudaEvent_t ev_stop = nullptr;
+    if (g_timing)
+    {
+        if (g_ev_used == g_ev.size())
+        {
+            cudaEvent_t e0, e1;
+            cudaEventCreate(&e0);
+            cudaEventCreate(&e1);
+            g_ev.emplace_back(e0, e1);
+        }
+        cudaEventRecord(g_ev[g_ev_used].first, stream);
+        ev_stop = g_ev[g_ev_used].second;
+        ++g_ev_used;
+    }
+    gemm_kernel<<<grid, kGemmThreads, gemm_smem_bytes(), stream>>>(gp);
+    if (ev_stop) cudaEventRecord(ev_stop, stream);
+    return check_launch("tc gemm");
+}
+
+}  // namespace
+}  // namespace tc
+}  // namespace oskb
+
+using namespace oskb;
+using namespace oskb::tc;
+
+extern "C" {
+
+size_t oskb_cross_correlate_tc_workspace_bytes(int num_sources,
+        int num_stations)
+{
+    if (num_sources <= 0 || num_stations <= 0) return kHeaderBytes;
+    return kHeaderBytes + image_bytes(num_stations, num_sources);
+}
+
+int oskb_cross_correlate_tc_d(int casa, int num_sources, int num_stations,
+        int offset_out, const double* jones, const double* I,
+        const double* Q, const double* U, const double* V,
+        const double* station_u, const double* station_v,
+        double uv_min_lambda, double uv_max_lambda, double inv_wavelength,
+        double* vis, void* workspace, size_t workspace_bytes, void* stream)
+{
+    if (num_sources < 0 || num_stations < 0) return OSKB_ERR_INVALID_ARGUMENT;
+    if (num_sources == 0 || num_stations < 2) return 0;
+    if (!jones || !I || !Q || !U || !V || !station_u || !station_v || !vis)
+        return OSKB_ERR_INVALID_ARGUMENT;
+    const size_t need = oskb_cross_correlate_tc_workspace_bytes(num_sources,
+            num_stations);
+    int err = get_workspace(workspace, workspace_bytes, need);
+    if (err) return err;
+    cudaStream_t s = as_stream(stream);
+    Header* hdr = reinterpret_cast<Header*>(workspace);
+    uint8_t* W = reinterpret_cast<uint8_t*>(workspace) + kHeaderBytes;
+    cudaMemsetAsync(hdr, 0, sizeof(Header), s);
+    maxabs_kernel<double, double><<<num_sms() * 8, 256, 0, s>>>(jones,
+            num_sources, num_stations, I, Q, U, V, &hdr->maxabs_bits,
+            &hdr->flags);
+    if ((err = check_launch("tc maxabs"))) return err;
+    const int nrb = (num_stations + kStPerBlock - 1) / kStPerBlock;
+    const int nkb = (num_sources + kSrcPerBlock - 1) / kSrcPerBlock;
+    prep_jones_kernel<double><<<dim3(nkb, nrb), 256, 0, s>>>(jones,
+            num_sources, num_stations, I, Q, U, V, &hdr->maxabs_bits, W);
+    if ((err = check_launch("tc prep"))) return err;
+    GemmParams gp;
+    gp.W = W; gp.image_stride = 0; gp.nrb = nrb; gp.nkb = nkb;
+    gp.num_problems = 1; gp.num_st = num_stations;
+    gp.maxabs_bits = &hdr->maxabs_bits; gp.maxabs_stride = 0;
+    gp.prob0 = 0; gp.nch = 1;
+    gp.vis = vis; gp.vis_stride = 0; gp.offset_out = offset_out;
+    gp.st_u = station_u; gp.st_v = station_v; gp.uv_stride = 0;
+    gp.inv_wavelength = nullptr; gp.kw_scalar = inv_wavelength;
+    gp.uv_min = uv_min_lambda; gp.uv_max = uv_max_lambda;
+    gp.casa = casa; gp.err = &hdr->err;
+    return launch_gemm(gp, s);
+}
+
+size_t oskb_correlate_block_tc_workspace_bytes(int num_sources,
+        int num_stations, int num_problems)
+{
+    if (num_sources <= 0 || num_stations <= 0 || num_problems <= 0)
+        return kHeaderBytes;
+    return kHeaderBytes + (size_t) num_problems *
+            image_bytes(num_stations, num_sources);
+}
+
+int oskb_correlate_block_tc(int casa, int num_sources, int num_stations,
+        int num_times, int num_channels, const float* E, const double* l,
+        const double* m, const double* n, const double* I, const double* Q,
+        const double* U, const double* V, const double* station_uvw,
+        const double* inv_wavelength, double uv_min_lambda,
+        double uv_max_lambda, double* vis, void* workspace,
+        size_t workspace_bytes, void* stream)
+{
+    if (num_sources < 0 || num_stations < 0 || num_times < 0 ||
+            num_channels < 0)
+        return OSKB_ERR_INVALID_ARGUMENT;
+    const int num_problems = num_times * num_channels;
+    if (num_sources == 0 || num_stations < 2 || num_problems == 0) return 0;
+    if (!E || !l || !m || !n || !I || !Q || !U || !V || !station_uvw ||
+            !inv_wavelength || !vis)
+        return OSKB_ERR_INVALID_ARGUMENT;
+    // Problems (t, c) are processed in groups that fit the workspace.
+    const size_t img = image_bytes(num_stations, num_sources);
+    int group = num_problems;
+    if (workspace)
+    {
+        if (workspace_bytes < kHeaderBytes + img)
+            return OSKB_ERR_MEMORY_ALLOC_FAILURE;
+        const size_t fit = (workspace_bytes - kHeaderBytes) / img;
+        if ((size_t) group > fit) group = (int) fit;
+    }
+    else
+    {
+        // Library-kept workspace: at most max_group() images, and no more
+        // than half of the device memory that is free now.
+        size_t free_b = 0, total_b = 0;
+        cudaMemGetInfo(&free_b, &total_b);
+        size_t fit = free_b / 2 / img;
+        if (fit < 1) fit = 1;
+        if ((size_t) group > fit) group = (int) fit;
+        if (group > max_group()) group = max_group();
+    }
+    int err = get_workspace(workspace, workspace_bytes,
+            kHeaderBytes + (size_t) group * img);
+    if (err) return err;
+    cudaStream_t s = as_stream(stream);
+    Header* hdr = reinterpret_cast<Header*>(workspace);
+    uint8_t* W = reinterpret_cast<uint8_t*>(workspace) + kHeaderBytes;
+    cudaMemsetAsync(hdr, 0, sizeof(Header), s);
+    // |K| = 1: one scale from E C serves every problem of the block.
+    maxabs_kernel<float, double><<<num_sms() * 8, 256, 0, s>>>(E,
+            num_sources, num_stations, I, Q, U, V, &hdr->maxabs_bits,
+            &hdr->flags);
+    if ((err = check_launch("tc maxabs"))) return err;
+    const int nrb = (num_stations + kStPerBlock - 1) / kStPerBlock;
+    const int nkb = (num_sources + kSrcPerBlock - 1) / kSrcPerBlock;
+    const size_t nbl = (size_t) num_stations * (num_stations - 1) / 2;
+    for (int p0 = 0; p0 < num_problems; p0 += group)
+    {
+        const int np = min(group, num_problems - p0);
+        prep_fused_kernel<<<dim3(nkb, nrb), 256, 0, s>>>(E, num_sources,
+                num_stations, l, m, n, I, Q, U, V, station_uvw,
+                inv_wavelength, num_channels, p0, np, &hdr->maxabs_bits, W,
+                img);
+        if ((err = check_launch("tc prep fused"))) return err;
+        GemmParams gp;
+        gp.W = W; gp.image_stride = img; gp.nrb = nrb; gp.nkb = nkb;
+        gp.num_problems = np; gp.num_st = num_stations;
+        gp.maxabs_bits = &hdr->maxabs_bits; gp.maxabs_stride = 0;
+        gp.prob0 = p0; gp.nch = num_channels;
+        gp.vis = vis; gp.vis_stride = nbl; gp.offset_out = 0;
+        gp.st_u = station_uvw; gp.st_v = station_uvw + num_stations;
+        gp.uv_stride = 3 * (size_t) num_stations;
+        gp.inv_wavelength = inv_wavelength; gp.kw_scalar = 0.0;
+        gp.uv_min = uv_min_lambda; gp.uv_max = uv_max_lambda;
+        gp.casa = casa; gp.err = &hdr->err;
+        if ((err = launch_gemm(gp, s))) return err;
+    }
+    return 0;
+}
+
+int oskb_tc_timing(int enable)
+{
+    g_timing = enable != 0;
+    g_ev_used = 0;
+    return 0;
+}
+
+int oskb_tc_timing_read(double* total_ms, int* launches)
+{
+    double sum = 0.0;
+    for (size_t i = 0; i < g_ev_used; ++i)
+    {
+        float ms = 0.0f;
+        if (cudaEventSynchronize(g_ev[i].second) != cudaSuccess ||
+                cudaEventElapsedTime(&ms, g_ev[i].first, g_ev[i].second)
+                != cudaSuccess)
+            return OSKB_ERR_KERNEL_LAUNCH_FAILURE;
+        sum += ms;
+    }
+    if (total_ms) *total_ms = sum;
+    if (launches) *launches = (int) g_ev_used;
+    g_ev_used = 0;
+    return 0;
+}
+
+int oskb_tc_status(const void* workspace, int* flags, int* wait_error)
+{
+    const void* ws = workspace;
+    if (!ws)
+    {
+        int dev = 0;
+        cudaGetDevice(&dev);
+        ws = (dev >= 0 && dev < 64) ? g_ws[dev].ptr : nullptr;
+    }
+    if (!ws) return OSKB_ERR_INVALID_ARGUMENT;
+    Header h;
+    if (cudaMemcpy(&h, ws, sizeof(h), cudaMemcpyDeviceToHost) != cudaSuccess)
+        return OSKB_ERR_MEMORY_COPY_FAILURE;
+    if (flags) *flags = h.flags;
+    if (wait_error) *wait_error = h.err;
+    return 0;
+}
+
+}  // extern "C"

@@ -1,0 +1,192 @@
+"""GPU parity of the tensor-core compensated cross-correlation.
+
+The tensor-core form (FP16 hi/lo split, three products, FP32 accumulation
+drained to FP64, FP64 phase) must agree with the FP64 CPU oracle to
+    L2 relative <= 1e-6  and  max |err| <= 1e-6 * max |V|
+on every test here (the stated tolerance of the compensated path). Calls go
+through the C ABI with torch device buffers.
+"""
+import numpy as np
+import pytest
+
+torch = pytest.importorskip("torch")
+pytestmark = [pytest.mark.gpu,
+              pytest.mark.skipif(not torch.cuda.is_available(),
+                                 reason="needs a CUDA device")]
+
+import oskar_b200 as ob  # noqa: E402
+from oracle_lib import oracle  # noqa: E402
+
+TOL = 1e-6
+C0 = 299792458.0
+
+
+def dev(a):
+    return torch.from_numpy(np.ascontiguousarray(a)).cuda()
+
+
+def errors(got, ref):
+    got = np.asarray(got, np.float64)
+    ref = np.asarray(ref, np.float64)
+    l2 = np.linalg.norm(got - ref) / np.linalg.norm(ref)
+    mx = np.max(np.abs(got - ref)) / np.max(np.abs(ref))
+    return l2, mx
+
+
+def sky(rng, nsrc, radius_deg=5.0, smin=0.01, smax=10.0):
+    r = np.sqrt(rng.uniform(0, 1, nsrc)) * np.sin(np.radians(radius_deg))
+    th = rng.uniform(0, 2 * np.pi, nsrc)
+    l, m = r * np.cos(th), r * np.sin(th)
+    n = np.sqrt(1 - l * l - m * m)
+    a = -0.5
+    u = rng.uniform(0, 1, nsrc)
+    I = (smin ** a + u * (smax ** a - smin ** a)) ** (1 / a)
+    Q, U, V = (I * rng.uniform(-0.1, 0.1, nsrc) for _ in range(3))
+    return l, m, n, I, Q, U, V
+
+
+def stations(rng, nst, rmax=5e3):
+    r = np.exp(rng.uniform(np.log(20.0), np.log(rmax), nst))
+    th = rng.uniform(0, 2 * np.pi, nst)
+    return (r * np.cos(th), r * np.sin(th), rng.uniform(-30, 30, nst))
+
+
+def oracle_vis(nst, nsrc, J, I, Q, U, V, l, m, n, u, v, w, inv_wl, casa=0,
+               uv_min=0.0, uv_max=3e38, vis0=None, offset_out=0):
+    nbl = nst * (nst - 1) // 2
+    out = np.zeros(8 * (nbl + offset_out)) if vis0 is None else vis0.copy()
+    z = np.zeros(nst)
+    oracle().call("xcorr_matrix_d", np.float64, casa, 0, nsrc, nst,
+                  offset_out, J, I, Q, U, V, l, m, n, None, None, None, u, v,
+                  w, z, z, uv_min, uv_max, inv_wl, 0.0, 0.0, 0.0, 0.0, out)
+    return out
+
+
+@pytest.mark.parametrize("nst,nsrc", [(2, 1), (5, 33), (31, 100), (33, 64),
+                                      (64, 1000), (100, 2500), (130, 777)])
+@pytest.mark.parametrize("casa", [0, 1])
+def test_tc_jones_api(nst, nsrc, casa):
+    rng = np.random.default_rng(nst * 1000 + nsrc)
+    l, m, n, I, Q, U, V = sky(rng, nsrc)
+    u, v, w = stations(rng, nst)
+    J = rng.normal(0, 0.3, (nst, nsrc, 8))
+    J[..., 0] += 1
+    J[..., 6] += 1
+    J = J.ravel()
+    inv_wl = 110e6 / C0
+    ref = oracle_vis(nst, nsrc, J, I, Q, U, V, l, m, n, u, v, w, inv_wl,
+                     casa=casa, offset_out=2)
+    nbl = nst * (nst - 1) // 2
+    vis = torch.zeros(8 * (nbl + 2), dtype=torch.float64, device="cuda")
+    ob.call("oskb_cross_correlate_tc_d", casa, nsrc, nst, 2, dev(J), dev(I),
+            dev(Q), dev(U), dev(V), dev(u), dev(v), 0.0, 3e38, inv_wl, vis,
+            None, 0, ob.stream_ptr())
+    torch.cuda.synchronize()
+    l2, mx = errors(vis.cpu().numpy()[16:], ref[16:])
+    assert l2 <= TOL and mx <= TOL, (l2, mx)
+    flags = (ob._lib.ctypes.c_int * 2)()
+    ob.call("oskb_tc_status", None, ob._lib.ctypes.addressof(flags),
+            ob._lib.ctypes.addressof(flags) + 4)
+    assert flags[0] == 0 and flags[1] == 0
+
+
+def test_tc_accumulates_and_filters():
+    """vis is accumulated (+=), and baselines outside the uv range are left
+    untouched, as in the reference dispatcher."""
+    rng = np.random.default_rng(9)
+    nst, nsrc = 40, 300
+    l, m, n, I, Q, U, V = sky(rng, nsrc)
+    u, v, w = stations(rng, nst, rmax=800.0)
+    J = rng.normal(0, 0.2, (nst, nsrc, 8)).ravel()
+    inv_wl = 100e6 / C0
+    nbl = nst * (nst - 1) // 2
+    vis0 = rng.normal(0, 1, 8 * nbl)
+    ref = oracle_vis(nst, nsrc, J, I, Q, U, V, l, m, n, u, v, w, inv_wl,
+                     uv_min=20.0, uv_max=150.0, vis0=vis0)
+    vis = dev(vis0)
+    ob.call("oskb_cross_correlate_tc_d", 0, nsrc, nst, 0, dev(J), dev(I),
+            dev(Q), dev(U), dev(V), dev(u), dev(v), 20.0, 150.0, inv_wl, vis,
+            None, 0, ob.stream_ptr())
+    torch.cuda.synchronize()
+    got = vis.cpu().numpy()
+    l2, mx = errors(got - vis0, ref - vis0)
+    assert l2 <= TOL and mx <= TOL, (l2, mx)
+    unchanged = np.all((got == vis0).reshape(-1, 8), axis=1)
+    assert unchanged.any() and not unchanged.all()
+
+
+def test_tc_caller_workspace_too_small():
+    nst, nsrc = 8, 40
+    need = ob.call("oskb_cross_correlate_tc_workspace_bytes", nsrc, nst,
+                   check=False)
+    ws = torch.zeros(need // 2, dtype=torch.uint8, device="cuda")
+    z = torch.zeros(8 * nst * nsrc, dtype=torch.float64, device="cuda")
+    st = ob.call("oskb_cross_correlate_tc_d", 0, nsrc, nst, 0, z, z, z, z,
+                 z, z, z, 0.0, 3e38, 1.0, z, ws, ws.numel(), ob.stream_ptr(),
+                 check=False)
+    assert st == -6
+
+
+@pytest.mark.parametrize("nst,nsrc,ntime,nchan", [(17, 50, 1, 3),
+                                                  (64, 1500, 2, 2),
+                                                  (97, 640, 3, 1)])
+def test_tc_fused_block(nst, nsrc, ntime, nchan):
+    """K (FP64 phase) x E x brightness for a block of (time, channel)
+    problems in one call, against the oracle's Jones K -> join -> correlate
+    for each problem."""
+    rng = np.random.default_rng(nst + nsrc)
+    l, m, n, I, Q, U, V = sky(rng, nsrc)
+    E = rng.normal(0, 0.1, (nst, nsrc, 8))
+    E[..., 0] += 1
+    E[..., 6] += 1
+    E32 = E.astype(np.float32)
+    uvw = np.stack([np.stack(stations(rng, nst, rmax=20e3))
+                    for _ in range(ntime)])
+    inv_wl = (100e6 + 7e6 * np.arange(nchan)) / C0
+    nbl = nst * (nst - 1) // 2
+    vis = torch.zeros(ntime * nchan * nbl * 8, dtype=torch.float64,
+                      device="cuda")
+    ob.call("oskb_correlate_block_tc", 0, nsrc, nst, ntime, nchan, dev(E32),
+            dev(l), dev(m), dev(n), dev(I), dev(Q), dev(U), dev(V), dev(uvw),
+            dev(inv_wl), 0.0, 3e38, vis, None, 0, ob.stream_ptr())
+    torch.cuda.synchronize()
+    got = vis.cpu().numpy().reshape(ntime, nchan, -1)
+    Ed = E32.astype(np.float64).ravel()
+    for t in range(ntime):
+        u, v, w = uvw[t]
+        for c in range(nchan):
+            K = np.zeros(2 * nst * nsrc)
+            oracle().call("jones_k_d", np.float64, nsrc, l, m, n, nst, u, v,
+                          w, 2 * np.pi * inv_wl[c], I, 0.0, 1e300, 0, K)
+            J = np.zeros(8 * nst * nsrc)
+            oracle().call("mem_mul_cm_m_d", np.float64, nst * nsrc, K, Ed, J)
+            ref = oracle_vis(nst, nsrc, J, I, Q, U, V, l, m, n, u, v, w,
+                             inv_wl[c])
+            l2, mx = errors(got[t, c], ref)
+            assert l2 <= TOL and mx <= TOL, (t, c, l2, mx)
+
+
+def test_tc_block_small_workspace_groups():
+    """A caller workspace holding one image forces one problem per group;
+    the result must equal the single-group run."""
+    rng = np.random.default_rng(77)
+    nst, nsrc, ntime, nchan = 40, 200, 2, 3
+    l, m, n, I, Q, U, V = sky(rng, nsrc)
+    E = rng.normal(0, 0.1, (nst, nsrc, 8)).astype(np.float32)
+    uvw = np.stack([np.stack(stations(rng, nst)) for _ in range(ntime)])
+    inv_wl = (120e6 + 1e6 * np.arange(nchan)) / C0
+    nbl = nst * (nst - 1) // 2
+    args = [dev(E), dev(l), dev(m), dev(n), dev(I), dev(Q), dev(U), dev(V),
+            dev(uvw), dev(inv_wl), 0.0, 3e38]
+    out = []
+    for nprob in (ntime * nchan, 1):
+        need = ob.call("oskb_correlate_block_tc_workspace_bytes", nsrc, nst,
+                       nprob, check=False)
+        ws = torch.empty(need, dtype=torch.uint8, device="cuda")
+        vis = torch.zeros(ntime * nchan * nbl * 8, dtype=torch.float64,
+                          device="cuda")
+        ob.call("oskb_correlate_block_tc", 0, nsrc, nst, ntime, nchan, *args,
+                vis, ws, ws.numel(), ob.stream_ptr())
+        torch.cuda.synchronize()
+        out.append(vis.cpu().numpy())
+    assert np.array_equal(out[0], out[1])
