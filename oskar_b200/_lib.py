@@ -14,7 +14,9 @@ import re
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
-LIB_PATH = os.path.join(HERE, "liboskar_b200.so")
+# OSKB_LIBRARY selects another build of the same library (same C ABI).
+LIB_PATH = os.environ.get("OSKB_LIBRARY",
+                          os.path.join(HERE, "liboskar_b200.so"))
 
 _SCALARS = {
     "int": ctypes.c_int,

@@ -467,6 +467,11 @@ gemm_kernel(const GemmParams prm)
         if (lane == 0)
         {
             // ---------------- MMA issuer
+            // hi hi^T and hi lo^T in one N = 256 MMA: the B hi and lo tiles
+            // are consecutive in shared memory, so they form one 256-row
+            // operand whose result columns land in the main (0-127) and
+            // correction (128-255) accumulators of the buffer.
+            const uint32_t idesc2 = ptx::idesc_f16_f32(128, 2 * kAccCols);
             const uint32_t idesc = ptx::idesc_f16_f32(128, kAccCols);
             int stage = 0;
             uint32_t phase = 0, tpar = 0;  // tpar bit b: use parity of buf b
@@ -511,12 +516,9 @@ gemm_kernel(const GemmParams prm)
                             const uint64_t al = ptx::sdesc_sw128(
                                     a + kTileBytes + 32 * k);
                             const uint64_t bh = ptx::sdesc_sw128(b + 32 * k);
-                            const uint64_t bl = ptx::sdesc_sw128(
-                                    b + kTileBytes + 32 * k);
                             const uint32_t acc =
                                     (kb > kb0 || k > 0) ? 1u : 0u;
-                            ptx::mma_f16(d, ah, bh, idesc, acc);
-                            ptx::mma_f16(dc, ah, bl, idesc, acc);
+                            ptx::mma_f16(d, ah, bh, idesc2, acc);
                             ptx::mma_f16(dc, al, bh, idesc, 1u);
                         }
                         ptx::mma_commit(&ctl->empty[stage]);
