@@ -279,6 +279,34 @@ OSKB_API int oskb_run_block_tc_host(int use_casa_phase_convention,
 OSKB_API int oskb_tc_timing(int enable);
 OSKB_API int oskb_tc_timing_read(double* total_ms, int* launches);
 
+/* Allocation-free form of oskb_cross_correlate_tc_d (no counterpart in the
+ * reference). For callers that cannot allocate device memory while they
+ * correlate: a process holding a fixed device-memory budget reserved at
+ * start-up (for example a real-time pipeline stage sharing the GPU), or a
+ * latency-critical loop that cannot afford the device-wide synchronisation
+ * that cudaMalloc may cause. It computes the same visibilities but takes its
+ * scratch from a 64 MiB array that the library declares in device memory
+ * (held by every GPU that loads the library until the process exits), and
+ * calls no cudaMalloc, cudaFree or allocating library routine.
+ *  - Limit: 16 bytes per station-source after rounding up to 32 stations x
+ *    32 sources, plus 256 bytes (e.g. 512 stations x 8,160 sources). Larger
+ *    calls return OSKB_ERR_OUT_OF_RANGE (-5) with the sizes in
+ *    oskb_last_error(); split the sources into chunks, since vis is
+ *    accumulated.
+ *  - The first call on a device takes the array's device address
+ *    (cudaGetSymbolAddress, with that device current); make that first call
+ *    before any stream capture.
+ *  - Every call shares the one array: calls whose work overlaps on the GPU
+ *    (different streams without ordering between them, or several host
+ *    threads) race and corrupt each other's results. Order them, for example
+ *    on one stream. oskb_tc_status() does not read this array. */
+OSKB_API int oskb_cross_correlate_tc_noalloc_d(int use_casa_phase_convention,
+        int num_sources, int num_stations, int offset_out,
+        const double* jones, const double* I, const double* Q,
+        const double* U, const double* V, const double* station_u,
+        const double* station_v, double uv_min_lambda, double uv_max_lambda,
+        double inv_wavelength, double* vis, void* stream);
+
 /* Status words of the last tensor-core call that used this workspace (NULL:
  * the library-kept one; synchronises with the device): flags bit 0 = a
  * brightness matrix was not positive semi-definite; wait_error != 0 = a

@@ -15,6 +15,7 @@ namespace oskb {
 
 // Last CUDA error text, kept per thread for oskb_last_error().
 void set_last_error(const char* where, cudaError_t err);
+void set_last_error_msg(const char* msg);
 
 // Maps a CUDA error after a launch to the OSKAR status convention.
 inline int check_launch(const char* where)

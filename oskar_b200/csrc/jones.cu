@@ -16,6 +16,11 @@ void set_last_error(const char* where, cudaError_t err)
             cudaGetErrorString(err));
 }
 
+void set_last_error_msg(const char* msg)
+{
+    snprintf(g_last_error, sizeof(g_last_error), "%s", msg);
+}
+
 namespace {
 
 int grid_for(size_t n, int threads)

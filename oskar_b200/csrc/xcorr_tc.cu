@@ -956,3 +956,115 @@ int oskb_tc_status(const void* workspace, int* flags, int* wait_error)
 }
 
 }  // extern "C"
+
+// ===========================================================================
+// Allocation-free form of the tensor-core correlation.
+//
+// Some callers cannot allocate device memory at the time they correlate: a
+// process that reserves a fixed device-memory budget at start-up (a real-time
+// correlator or pipeline stage sharing the GPU with other software) must not
+// grow past it, and cudaMalloc may synchronise the whole device, which a
+// latency-critical caller cannot afford in its processing loop. For them this
+// entry point takes its scratch (status words and the FP16 operand image)
+// from a file-scope device array of fixed size instead of a workspace.
+// ===========================================================================
+#include <mutex>
+
+namespace oskb {
+namespace tc {
+namespace {
+
+// Maximum scratch of the allocation-free entry point: 64 MiB, held by every
+// GPU that loads the library until the process exits. The operand image
+// needs 16 bytes per station-source (rounded up to 32 stations x 32 sources),
+// e.g. up to 512 stations x 8,160 sources per call.
+constexpr size_t kStaticScratchBytes = (size_t) 64 << 20;
+
+static __device__ __align__(256) uint8_t g_static_scratch[kStaticScratchBytes];
+
+// Device address of g_static_scratch for each device, taken once per device
+// with that device current (the host-side symbol is not a device address).
+std::mutex g_static_mutex;
+void* g_static_ptr[64] = {};
+
+int static_scratch(void** ptr)
+{
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64)
+        return OSKB_ERR_CUDA_NOT_AVAILABLE;
+    std::lock_guard<std::mutex> lock(g_static_mutex);
+    if (!g_static_ptr[dev])
+    {
+        void* p = nullptr;
+        const cudaError_t e = cudaGetSymbolAddress(&p, g_static_scratch);
+        if (e != cudaSuccess || !p)
+        {
+            set_last_error("static scratch address", e);
+            return OSKB_ERR_CUDA_NOT_AVAILABLE;
+        }
+        g_static_ptr[dev] = p;
+    }
+    *ptr = g_static_ptr[dev];
+    return 0;
+}
+
+}  // namespace
+}  // namespace tc
+}  // namespace oskb
+
+extern "C" int oskb_cross_correlate_tc_noalloc_d(int casa, int num_sources,
+        int num_stations, int offset_out, const double* jones,
+        const double* I, const double* Q, const double* U, const double* V,
+        const double* station_u, const double* station_v,
+        double uv_min_lambda, double uv_max_lambda, double inv_wavelength,
+        double* vis, void* stream)
+{
+    if (num_sources < 0 || num_stations < 0) return OSKB_ERR_INVALID_ARGUMENT;
+    if (num_sources == 0 || num_stations < 2) return 0;
+    if (!jones || !I || !Q || !U || !V || !station_u || !station_v || !vis)
+        return OSKB_ERR_INVALID_ARGUMENT;
+    const size_t need = kHeaderBytes + image_bytes(num_stations, num_sources);
+    if (need > kStaticScratchBytes)
+    {
+        char msg[200];
+        snprintf(msg, sizeof(msg), "oskb_cross_correlate_tc_noalloc_d: %d "
+                "stations x %d sources need %zu bytes of scratch; the static "
+                "scratch holds %zu (split the sources into chunks)",
+                num_stations, num_sources, need, kStaticScratchBytes);
+        set_last_error_msg(msg);
+        return OSKB_ERR_OUT_OF_RANGE;
+    }
+    void* scratch = nullptr;
+    int err = static_scratch(&scratch);
+    if (err) return err;
+    cudaStream_t s = as_stream(stream);
+    Header* hdr = reinterpret_cast<Header*>(scratch);
+    uint8_t* W = reinterpret_cast<uint8_t*>(scratch) + kHeaderBytes;
+    // The array keeps the previous call's contents: the status words must
+    // start at zero; the operand image is fully rewritten by the prep kernel.
+    if (cudaMemsetAsync(hdr, 0, sizeof(Header), s) != cudaSuccess)
+    {
+        set_last_error("static scratch clear", cudaGetLastError());
+        return OSKB_ERR_KERNEL_LAUNCH_FAILURE;
+    }
+    maxabs_kernel<double, double><<<num_sms() * 8, 256, 0, s>>>(jones,
+            num_sources, num_stations, I, Q, U, V, &hdr->maxabs_bits,
+            &hdr->flags);
+    if ((err = check_launch("tc maxabs (static scratch)"))) return err;
+    const int nrb = (num_stations + kStPerBlock - 1) / kStPerBlock;
+    const int nkb = (num_sources + kSrcPerBlock - 1) / kSrcPerBlock;
+    prep_jones_kernel<double><<<dim3(nkb, nrb), 256, 0, s>>>(jones,
+            num_sources, num_stations, I, Q, U, V, &hdr->maxabs_bits, W);
+    if ((err = check_launch("tc prep (static scratch)"))) return err;
+    GemmParams gp;
+    gp.W = W; gp.image_stride = 0; gp.nrb = nrb; gp.nkb = nkb;
+    gp.num_problems = 1; gp.num_st = num_stations;
+    gp.maxabs_bits = &hdr->maxabs_bits; gp.maxabs_stride = 0;
+    gp.prob0 = 0; gp.nch = 1;
+    gp.vis = vis; gp.vis_stride = 0; gp.offset_out = offset_out;
+    gp.st_u = station_u; gp.st_v = station_v; gp.uv_stride = 0;
+    gp.inv_wavelength = nullptr; gp.kw_scalar = inv_wavelength;
+    gp.uv_min = uv_min_lambda; gp.uv_max = uv_max_lambda;
+    gp.casa = casa; gp.err = &hdr->err;
+    return launch_gemm(gp, s);
+}
