@@ -298,7 +298,8 @@ def run_ours(args):
                         0.0, 3e38, f / 299792458.0, 0.0, 0.0, 0.0, 0.0,
                         vis[c], stream)
 
-    dump = lambda i: (rank + i * world) % cfg.num_times
+    from oskar_b200.sharding import dump_of_step, max_over_ranks
+    dump = lambda i: dump_of_step(i, world, rank, cfg.num_times)
     for i in range(args.warmup):
         step(dump(i))
     torch.cuda.synchronize()
@@ -327,10 +328,7 @@ def run_ours(args):
                 ctypes.addressof(n_l))
         ob.call("oskb_tc_timing", 0)
         gemm_ms, gemm_launches = t_ms.value, n_l.value
-    t = torch.tensor([ms_total], dtype=torch.float64, device="cuda")
-    if world > 1:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    ms_max = float(t.item())
+    ms_max = max_over_ranks(ms_total)
     value = sb_step * args.steps * world / (ms_max * 1e-3) / 1e9
 
     result = None
@@ -480,11 +478,8 @@ def run_e2e(args, cfg, ob, torch, E, world, rank):
     for b in range(nblocks):
         block(b)
     dt = time.perf_counter() - t0
-    t = torch.tensor([dt], dtype=torch.float64, device="cuda")
-    if world > 1:
-        import torch.distributed as dist
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    dt = float(t.item())
+    from oskar_b200.sharding import max_over_ranks
+    dt = max_over_ranks(dt)
     sb = nbl * nsrc * nch * nt * nblocks * world
     h2d = (Eh.numel() * 4 + 7 * nsrc * 8 + nt * 3 * nst * 8 + nch * 8)
     d2h = visb.numel() * 8
