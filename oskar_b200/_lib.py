@@ -40,9 +40,12 @@ def parse_headers(paths=None):
         text = re.sub(r"//[^\n]*", " ", text)
         text = re.sub(r"#[^\n]*", " ", text)
         for m in re.finditer(
-                r"(int|void|size_t|const\s+char\s*\*)\s+(oskb_\w+)\s*\(([^)]*)\)\s*;",
-                text):
-            ret, name, args = m.group(1), m.group(2), m.group(3)
+                r"((?:const\s+)?\w+\s*\**)\s*\b((?:oskb|oskar)_\w+)\s*"
+                r"\(([^)]*)\)\s*;", text):
+            ret, name, args = " ".join(m.group(1).split()), m.group(2), \
+                m.group(3)
+            if ret.startswith("typedef") or ret == "struct":
+                continue
             argtypes = []
             args = args.strip()
             if args and args != "void":
@@ -57,8 +60,13 @@ def parse_headers(paths=None):
                         raise ValueError("%s: unsupported type '%s'"
                                          % (name, base))
                     argtypes.append(_SCALARS[base])
-            restype = {"int": ctypes.c_int, "void": None,
-                       "size_t": ctypes.c_size_t}.get(ret, ctypes.c_char_p)
+            if ret.replace(" ", "") == "constchar*":
+                restype = ctypes.c_char_p
+            elif "*" in ret:
+                restype = ctypes.c_void_p
+            else:
+                restype = {"int": ctypes.c_int, "void": None,
+                           "size_t": ctypes.c_size_t}[ret]
             protos[name] = (restype, argtypes)
     return protos
 
@@ -115,7 +123,8 @@ def call(name, *args, check=True):
     conv = [(_ptr(a) if t is ctypes.c_void_p else a)
             for a, t in zip(args, argtypes)]
     status = getattr(lib, name)(*conv)
-    if check and restype is ctypes.c_int and status != 0:
+    if check and name.startswith("oskb_") and restype is ctypes.c_int \
+            and status != 0:
         detail = lib.oskb_last_error().decode()
         raise OskbError(name, status, detail)
     return status

@@ -25,15 +25,25 @@ def test_nm_matches_header():
                          capture_output=True, text=True, check=True).stdout
     exported = {ln.split()[-1] for ln in out.splitlines()
                 if " T " in ln and ln.split()[-1].startswith("oskb_")}
-    declared = set(_lib.parse_headers())
+    declared = {k for k in _lib.parse_headers() if k.startswith("oskb_")}
     assert declared <= exported, declared - exported
     # nothing else from the library leaks out under the oskb_ prefix
     assert exported <= declared, exported - declared
 
 
+def test_oskar_api_symbols_exported():
+    out = subprocess.run(["nm", "-D", "--defined-only", _lib.LIB_PATH],
+                         capture_output=True, text=True, check=True).stdout
+    exported = {ln.split()[-1] for ln in out.splitlines() if " T " in ln}
+    declared = {k for k in _lib.parse_headers() if k.startswith("oskar_")}
+    assert len(declared) >= 30
+    assert declared <= exported, declared - exported
+
+
 def test_header_compiles_as_c():
     inc = os.path.join(_lib.ROOT, "include")
-    src = "#include <oskar_b200.h>\nint main(void){return 0;}\n"
+    src = ("#include <oskar_b200.h>\n#include <oskar_b200_api.h>\n"
+           "int main(void){return 0;}\n")
     r = subprocess.run(["gcc", "-std=c99", "-Wall", "-Werror", "-I" + inc,
                         "-x", "c", "-", "-o", os.devnull], input=src,
                        capture_output=True, text=True)
