@@ -491,6 +491,83 @@ def run_e2e(args, cfg, ob, torch, E, world, rank):
             "blocks": nblocks, "seconds": dt}
 
 
+def run_profile_case(args):
+    """One small invocation of a single kernel, for ncu captures: inputs
+    larger than L2 but a few GB on the device at most, two launches.
+      tc_small      the tensor-core contraction (gemm_kernel) and its
+                    operand preparation (prep_fused_kernel): 512 stations x
+                    20,000 sources x 1 channel, 1/80 of a bench launch;
+      direct_small  the FP64 direct cross-correlation: 512 stations x 2,000
+                    sources, 1 channel;
+      beam_small    the fused station beam: 32 stations x 256 dipoles x
+                    12,001 directions (FP64)."""
+    import torch
+    import oskar_b200 as ob
+    from oskar_b200 import workloads
+    torch.cuda.set_device(0)
+    dev = lambda a: torch.from_numpy(np.ascontiguousarray(a)).cuda()
+    stream = ob.stream_ptr()
+    case = args.profile_case
+    if case in ("tc_small", "direct_small"):
+        nsrc = 20_000 if case == "tc_small" else 2_000
+        cfg = workloads.c3(num_src=nsrc, num_channels=1, num_times=1)
+        nst, nbl = cfg.num_st, cfg.num_baselines
+        l, m, n, I, Q, U, V = (dev(x) for x in (cfg.l, cfg.m, cfg.n, cfg.I,
+                                                cfg.Q, cfg.U, cfg.V))
+        E = workloads.jones_e_device(cfg, torch.float32)
+        uvw = dev(cfg.station_uvw(0)[None])
+        inv_wl = dev(cfg.freqs_hz / 299792458.0)
+        vis = torch.zeros((1, nbl, 8), dtype=torch.float64, device="cuda")
+        if case == "tc_small":
+            ws_bytes = ob.call("oskb_correlate_block_tc_workspace_bytes",
+                               nsrc, nst, 1, check=False)
+            ws = torch.empty(ws_bytes, dtype=torch.uint8, device="cuda")
+            for _ in range(2):
+                ob.call("oskb_correlate_block_tc", 0, nsrc, nst, 1, 1, E, l,
+                        m, n, I, Q, U, V, uvw, inv_wl, 0.0, 3e38, vis, ws,
+                        ws_bytes, stream)
+        else:
+            f = float(cfg.freqs_hz[0])
+            u, v, w = uvw[0]
+            K = torch.empty((nst, nsrc, 2), dtype=torch.float64,
+                            device="cuda")
+            J = torch.empty((nst, nsrc, 8), dtype=torch.float64,
+                            device="cuda")
+            z = torch.zeros(nst, dtype=torch.float64, device="cuda")
+            ob.call("oskb_evaluate_jones_K_d", nsrc, l, m, n, nst, u, v, w,
+                    2 * math.pi * f / 299792458.0, I, 0.0, 1e300, 0, K,
+                    stream)
+            ob.call("oskb_mem_multiply_d", 3, 0, 0, 0, nst * nsrc, K,
+                    E.double(), J, stream)
+            for _ in range(2):
+                ob.call("oskb_cross_correlate_d", 0, 0, nsrc, nst, 0, J, I,
+                        Q, U, V, l, m, n, None, None, None, u, v, w, z, z,
+                        0.0, 3e38, f / 299792458.0, 0.0, 0.0, 0.0, 0.0,
+                        vis[0], stream)
+    elif case == "beam_small":
+        st, ne, nd = 32, 256, 12_001
+        rng = np.random.default_rng(2)
+        r = 19.0 * np.sqrt(rng.uniform(0, 1, (st, ne)))
+        t = rng.uniform(0, 2 * math.pi, (st, ne))
+        ex, ey = dev(r * np.cos(t)), dev(r * np.sin(t))
+        ez = torch.zeros_like(ex)
+        az = rng.uniform(0, 2 * math.pi, nd)
+        el = np.arcsin(rng.uniform(0, 1, nd))
+        dx, dy, dz = (dev(a) for a in (np.cos(el) * np.sin(az),
+                                       np.cos(el) * np.cos(az), np.sin(el)))
+        ori = dev(rng.uniform(0, 2 * math.pi, st))
+        ori_y = ori + math.pi / 2
+        b = dev(np.tile([0.0, 0.0, 1.0], (st, 1)))
+        beam = torch.empty((st, nd, 8), dtype=torch.float64, device="cuda")
+        for _ in range(2):
+            ob.call("oskb_station_beam_aa_d", st, ne, ex, ey, ez, None, None,
+                    None, None, ori, ori_y, 1.5, 1, 1, 1, 0, 0, 110e6, b, b,
+                    nd, dx, dy, dz, 0, beam, stream)
+    torch.cuda.synchronize()
+    print(json.dumps({"profile_case": case, "ok": True}))
+    return 0
+
+
 def cpu_baseline(cfg):
     cores = cpu_cores()
     if ref_lib() is None:
@@ -514,7 +591,12 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--path", default="tc", choices=["tc", "direct"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--profile-case", default=None,
+                    choices=["tc_small", "direct_small", "beam_small"],
+                    help="run one small kernel case for an ncu capture")
     args = ap.parse_args()
+    if args.profile_case:
+        return run_profile_case(args)
     os.environ.setdefault("OMP_NUM_THREADS", str(cpu_cores()))
     if args.impl == "reference":
         return run_reference(args)

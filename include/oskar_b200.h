@@ -207,6 +207,57 @@ OSKB_API int oskb_convert_ecef_to_station_uvw_d(int num_stations, const double* 
         double gast, int ignore_w_components, int offset_out, double* u,
         double* v, double* w, void* stream);
 
+/* Aperture-array station beam (Jones E) of num_stations stations in one
+ * launch: dipole element pattern (optionally normalised at the pole), array
+ * factor with weights from the measured element positions (true positions
+ * where meas_* is NULL) and cable-length errors (NULL: none), optional 1/N
+ * array normalisation, horizon blanking, and optional division by the beam
+ * amplitude in the normalisation direction. Replaces the chain of
+ * oskar_station_beam (oskar/telescope/station/src/oskar_station_beam.c:
+ * 84-182) and oskar_evaluate_station_beam_aperture_array
+ * (oskar_evaluate_station_beam_aperture_array.c:150-240) for stations with
+ * one dipole element type, common orientation, no child stations.
+ *   el_*, meas_*, cable_length_error: [station][element] metres (ENU);
+ *   orientation_{x,y}_rad: [station] element Euler angles (the reference's
+ *     oskar_station_element_euler_index_rad(s, 0|1, 0, 0));
+ *   beam_enu, norm_enu: [station][3] ENU direction cosines (double);
+ *   x, y, z: ENU direction cosines, [station][num_directions] when
+ *     directions_per_station, else [num_directions] shared;
+ *   beam: [station][num_directions] complex 2x2 (the Jones E layout).
+ * All pointers are device memory. */
+OSKB_API int oskb_station_beam_aa_d(int num_stations, int num_elements,
+        const double* el_x, const double* el_y, const double* el_z,
+        const double* meas_x, const double* meas_y, const double* meas_z,
+        const double* cable_length_error, const double* orientation_x_rad,
+        const double* orientation_y_rad, double dipole_length_m,
+        int normalise_element, int normalise_array, int normalise_final,
+        int swap_xy, int is_3d, double frequency_hz, const double* beam_enu,
+        const double* norm_enu, int num_directions, const double* x,
+        const double* y, const double* z, int directions_per_station,
+        double* beam, void* stream);
+OSKB_API int oskb_station_beam_aa_f(int num_stations, int num_elements,
+        const float* el_x, const float* el_y, const float* el_z,
+        const float* meas_x, const float* meas_y, const float* meas_z,
+        const float* cable_length_error, const double* orientation_x_rad,
+        const double* orientation_y_rad, double dipole_length_m,
+        int normalise_element, int normalise_array, int normalise_final,
+        int swap_xy, int is_3d, double frequency_hz, const double* beam_enu,
+        const double* norm_enu, int num_directions, const float* x,
+        const float* y, const float* z, int directions_per_station,
+        float* beam, void* stream);
+
+/* Parallactic-angle rotation R [station][source] (real 2x2 rotation) for
+ * stations at latitude lat_rad[station] and local sidereal time
+ * lst_rad[station] = gast + longitude. Replaces the kernel behind
+ * oskar_evaluate_jones_R (oskar/interferometer/src/oskar_evaluate_jones_R.c:
+ * 21-147; define_evaluate_jones_R.h:3-29). Device pointers. */
+OSKB_API int oskb_evaluate_jones_R_d(int num_sources, const double* ra_rad,
+        const double* dec_rad, int num_stations, const double* lat_rad,
+        const double* lst_rad, double* jones, void* stream);
+OSKB_API int oskb_evaluate_jones_R_f(int num_sources, const float* ra_rad,
+        const float* dec_rad, int num_stations, const double* lat_rad,
+        const double* lst_rad, float* jones, void* stream);
+
 /* ------------------------------------------------------------------------
  * Tensor-core compensated cross-correlation (point sources, no smearing).
  * ------------------------------------------------------------------------

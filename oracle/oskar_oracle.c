@@ -5,6 +5,7 @@
  */
 #include <math.h>
 #include <stddef.h>
+#include <stdlib.h>
 #include "oskar_oracle.h"
 
 #define ORC_PI 3.14159265358979323846264338327950288
@@ -21,6 +22,8 @@
 #define ORC_COS cos
 #define ORC_EXP exp
 #define ORC_SQRT sqrt
+#define ORC_ATAN2 atan2
+#define ORC_FMOD fmod
 #define ORC_KAHAN 0
 #include "oskar_oracle_body.h"
 #undef REAL
@@ -30,6 +33,8 @@
 #undef ORC_COS
 #undef ORC_EXP
 #undef ORC_SQRT
+#undef ORC_ATAN2
+#undef ORC_FMOD
 #undef ORC_KAHAN
 
 /* ---- float ---- */
@@ -40,5 +45,7 @@
 #define ORC_COS cosf
 #define ORC_EXP expf
 #define ORC_SQRT sqrtf
+#define ORC_ATAN2 atan2f
+#define ORC_FMOD fmodf
 #define ORC_KAHAN 1
 #include "oskar_oracle_body.h"

@@ -70,7 +70,27 @@ void orc_element_weights_dft_##S(int n, const REAL* x, const REAL* y, \
 void orc_ecef_to_station_uvw_##S(int n, const REAL* x, const REAL* y, \
         const REAL* z, REAL sin_ha0, REAL cos_ha0, REAL sin_dec0, \
         REAL cos_dec0, int ignore_w, int offset_out, REAL* u, REAL* v, \
-        REAL* w);
+        REAL* w); \
+void orc_enu_to_theta_phi_##S(int off_in, int num, const REAL* x, \
+        const REAL* y, const REAL* z, int extra_point_at_pole, REAL dphi1, \
+        REAL dphi2, REAL* theta, REAL* phi1, REAL* phi2); \
+void orc_dipole_pattern_##S(int n, const REAL* theta, const REAL* phi_x, \
+        const REAL* phi_y, REAL kL, REAL cos_kL, int swap_xy, \
+        int offset_out, REAL* pattern); \
+void orc_mem_normalise_matrix_##S(int offset, int n, REAL* a, int idx); \
+void orc_blank_below_horizon_##S(int off_mask, int n, const REAL* mask, \
+        int off_out, REAL* jones); \
+void orc_jones_r_##S(int num_sources, const REAL* ra, const REAL* dec, \
+        REAL cos_lat, REAL sin_lat, REAL lst_rad, int offset_out, \
+        REAL* jones); \
+void orc_station_beam_aa_##S(int num_el, const REAL* x, const REAL* y, \
+        const REAL* z, const REAL* x_meas, const REAL* y_meas, \
+        const REAL* z_meas, const REAL* cable, double orientation_x_rad, \
+        double orientation_y_rad, double dipole_length_m, int norm_element, \
+        int norm_array, int norm_final, int swap_xy, int is_3d, \
+        double frequency_hz, double bx, double by, double bz, double nx, \
+        double ny, double nz, int num_dir, const REAL* dx, const REAL* dy, \
+        const REAL* dz, REAL* beam);
 
 ORC_DECLARE(double, d)
 ORC_DECLARE(float, f)

@@ -538,3 +538,195 @@ void ORC_FN(orc_ecef_to_station_uvw)(int n, const REAL* x, const REAL* y,
         w[i + offset_out] = ignore_w ? (REAL)0 : zz * sin_dec0 + t * cos_dec0;
     }
 }
+
+/* ENU direction cosines to element-frame (theta, phi_x, phi_y), phi wrapped
+ * into [0, 2 pi), with an optional extra point at the pole carrying the
+ * unwrapped phase offsets
+ * (convert/define_convert_enu_directions_to_theta_phi.h:3-31). */
+void ORC_FN(orc_enu_to_theta_phi)(int off_in, int num, const REAL* x,
+        const REAL* y, const REAL* z, int extra_point_at_pole, REAL dphi1,
+        REAL dphi2, REAL* theta, REAL* phi1, REAL* phi2)
+{
+    const REAL twopi = 2 * (REAL) ORC_PI;
+    int i;
+    for (i = 0; i < num; ++i)
+    {
+        const REAL xx = x[i + off_in], yy = y[i + off_in], zz = z[i + off_in];
+        const REAL p0 = ORC_ATAN2(yy, xx);
+        REAL p1 = ORC_FMOD(p0 + dphi1, twopi);
+        REAL p2 = ORC_FMOD(p0 + dphi2, twopi);
+        if (p1 < 0) p1 += twopi;
+        if (p2 < 0) p2 += twopi;
+        theta[i] = ORC_ATAN2(ORC_SQRT(xx * xx + yy * yy), zz);
+        phi1[i] = p1;
+        phi2[i] = p2;
+    }
+    if (extra_point_at_pole)
+    {
+        theta[num] = 0;
+        phi1[num] = dphi1;
+        phi2[num] = dphi2;
+    }
+}
+
+/* Far field of one half-wave-style dipole of electrical half-length kL
+ * along the direction phi (define_evaluate_dipole_pattern.h:3-15). */
+static void ORC_T(dipole)(REAL kL, REAL cos_kL, REAL sin_th, REAL cos_th,
+        REAL phi, REAL* e_theta, REAL* e_phi)
+{
+    const REAL sp = ORC_SIN(phi), cp = ORC_COS(phi);
+    const REAL denom = 1 + cp * cp * (cos_th * cos_th - 1);
+    REAL t;
+    if (denom == 0)
+    {
+        *e_theta = *e_phi = 0;
+        return;
+    }
+    t = (ORC_COS(kL * cp * sin_th) - cos_kL) / denom;
+    *e_theta = -cp * cos_th * t;
+    *e_phi = sp * t;
+}
+
+/* Polarised dipole pattern {x_theta, x_phi, y_theta, y_phi}, X and Y rows
+ * swapped if swap_xy (define_evaluate_dipole_pattern.h:17-48). */
+void ORC_FN(orc_dipole_pattern)(int n, const REAL* theta, const REAL* phi_x,
+        const REAL* phi_y, REAL kL, REAL cos_kL, int swap_xy, int offset_out,
+        REAL* pattern)
+{
+    int i;
+    for (i = 0; i < n; ++i)
+    {
+        REAL xt, xp, yt, yp;
+        const REAL st = ORC_SIN(theta[i]), ct = ORC_COS(theta[i]);
+        REAL* o = pattern + 8 * ((size_t) i + offset_out);
+        ORC_T(dipole)(kL, cos_kL, st, ct, phi_x[i], &xt, &xp);
+        ORC_T(dipole)(kL, cos_kL, st, ct, phi_y[i], &yt, &yp);
+        o[0] = swap_xy ? yt : xt;
+        o[2] = swap_xy ? yp : xp;
+        o[4] = swap_xy ? xt : yt;
+        o[6] = swap_xy ? xp : yp;
+        o[1] = o[3] = o[5] = o[7] = 0;
+    }
+}
+
+/* Scales matrices [offset, offset + n), except the one at idx, by
+ * 1 / sqrt(|M_idx|_F^2 / 2) (mem/define_mem_normalise.h:31-51). */
+void ORC_FN(orc_mem_normalise_matrix)(int offset, int n, REAL* a, int idx)
+{
+    const REAL* v = a + 8 * (size_t) idx;
+    REAL amp = 0, scal;
+    int j, k;
+    for (k = 0; k < 8; ++k) amp += v[k] * v[k];
+    scal = 1 / ORC_SQRT(amp / 2);
+    for (j = offset; j < offset + n; ++j)
+    {
+        if (j == idx) continue;
+        for (k = 0; k < 8; ++k) a[8 * (size_t) j + k] *= scal;
+    }
+}
+
+/* Zeroes matrices whose direction has z < 0
+ * (telescope/station/define_blank_below_horizon.h:15-29). */
+void ORC_FN(orc_blank_below_horizon)(int off_mask, int n, const REAL* mask,
+        int off_out, REAL* jones)
+{
+    int i, k;
+    for (i = 0; i < n; ++i)
+        if (mask[i + off_mask] < 0)
+            for (k = 0; k < 8; ++k) jones[8 * ((size_t) i + off_out) + k] = 0;
+}
+
+/* Parallactic-angle rotation R for each source as seen from a station at
+ * latitude lat and local sidereal time lst
+ * (interferometer/define_evaluate_jones_R.h:3-29). */
+void ORC_FN(orc_jones_r)(int num_sources, const REAL* ra, const REAL* dec,
+        REAL cos_lat, REAL sin_lat, REAL lst_rad, int offset_out, REAL* jones)
+{
+    int i;
+    for (i = 0; i < num_sources; ++i)
+    {
+        const REAL ha = lst_rad - ra[i];
+        const REAL sh = ORC_SIN(ha), ch = ORC_COS(ha);
+        const REAL sd = ORC_SIN(dec[i]), cd = ORC_COS(dec[i]);
+        const REAL q = ORC_ATAN2(cos_lat * sh, sin_lat * cd - cos_lat * sd * ch);
+        const REAL sq = ORC_SIN(q), cq = ORC_COS(q);
+        REAL* o = jones + 8 * ((size_t) i + offset_out);
+        o[0] = cq; o[2] = -sq; o[4] = sq; o[6] = cq;
+        o[1] = o[3] = o[5] = o[7] = 0;
+    }
+}
+
+/* Aperture-array station beam for one station with a single element type
+ * (dipoles, common orientation) and one feed set, composed exactly as the
+ * reference composes it:
+ *  - oskar_station_beam (telescope/station/src/oskar_station_beam.c:84-91,
+ *    107-135, 178-182): zero beam if the pointing is below the horizon; the
+ *    normalisation direction appended as an extra point and the beam
+ *    divided by its amplitude at the end;
+ *  - oskar_evaluate_station_beam_aperture_array
+ *    (telescope/station/src/oskar_evaluate_station_beam_aperture_array.c:
+ *    150-240): element pattern (oskar_element_evaluate.c:76-80, 134-138,
+ *    153-157, orientation_x offset by pi/2), weights from the measured
+ *    element positions (oskar_station_evaluate_element_weights.c:25-31),
+ *    weighted DFT over the true positions, horizon blanking.
+ * Scalars that the reference derives in double (wavenumber, kL, delta phi)
+ * are derived in double here too, then rounded to REAL. */
+void ORC_FN(orc_station_beam_aa)(int num_el, const REAL* x, const REAL* y,
+        const REAL* z, const REAL* x_meas, const REAL* y_meas,
+        const REAL* z_meas, const REAL* cable, double orientation_x_rad,
+        double orientation_y_rad, double dipole_length_m, int norm_element,
+        int norm_array, int norm_final, int swap_xy, int is_3d,
+        double frequency_hz, double bx, double by, double bz, double nx,
+        double ny, double nz, int num_dir, const REAL* dx, const REAL* dy,
+        const REAL* dz, REAL* beam)
+{
+    const double c0 = 299792458.0;
+    const int np = num_dir + (norm_final ? 1 : 0);
+    const int npe = np + (norm_element ? 1 : 0);
+    const double wavenumber = 2.0 * ORC_PI * frequency_hz / c0;
+    const double kL = dipole_length_m * (ORC_PI * frequency_hz / c0);
+    const double dphi1 = ORC_PI / 2 - (orientation_x_rad + ORC_PI / 2);
+    const double dphi2 = ORC_PI / 2 - orientation_y_rad;
+    REAL *X, *Y, *Z, *theta, *phi1, *phi2, *signal, *w, *out;
+    int* types;
+    int i;
+    if (bz < 0)
+    {
+        for (i = 0; i < 8 * num_dir; ++i) beam[i] = 0;
+        return;
+    }
+    X = (REAL*) malloc(sizeof(REAL) * np);
+    Y = (REAL*) malloc(sizeof(REAL) * np);
+    Z = (REAL*) malloc(sizeof(REAL) * np);
+    theta = (REAL*) malloc(sizeof(REAL) * npe);
+    phi1 = (REAL*) malloc(sizeof(REAL) * npe);
+    phi2 = (REAL*) malloc(sizeof(REAL) * npe);
+    signal = (REAL*) calloc((size_t) 8 * npe, sizeof(REAL));
+    out = (REAL*) calloc((size_t) 8 * np, sizeof(REAL));
+    w = (REAL*) malloc(sizeof(REAL) * 2 * num_el);
+    types = (int*) calloc((size_t) num_el, sizeof(int));
+    for (i = 0; i < num_dir; ++i)
+    {
+        X[i] = dx[i]; Y[i] = dy[i]; Z[i] = dz[i];
+    }
+    if (norm_final)
+    {
+        X[num_dir] = (REAL) nx; Y[num_dir] = (REAL) ny; Z[num_dir] = (REAL) nz;
+    }
+    ORC_FN(orc_enu_to_theta_phi)(0, np, X, Y, Z, norm_element,
+            (REAL) dphi1, (REAL) dphi2, theta, phi1, phi2);
+    ORC_FN(orc_dipole_pattern)(npe, theta, phi1, phi2, (REAL) kL,
+            (REAL) cos(kL), swap_xy, 0, signal);
+    if (norm_element) ORC_FN(orc_mem_normalise_matrix)(0, np, signal, np);
+    ORC_FN(orc_element_weights_dft)(num_el, x_meas ? x_meas : x,
+            y_meas ? y_meas : y, z_meas ? z_meas : z, cable,
+            (REAL) wavenumber, (REAL) bx, (REAL) by, (REAL) bz, w);
+    ORC_FN(orc_dftw)(1, is_3d, num_el, (REAL) wavenumber, w, x, y, z, 0, np,
+            X, Y, is_3d ? Z : 0, types, signal, 1, 1, 0, out,
+            norm_array ? (REAL) (1.0 / num_el) : (REAL) 1);
+    ORC_FN(orc_blank_below_horizon)(0, np, Z, 0, out);
+    if (norm_final) ORC_FN(orc_mem_normalise_matrix)(0, np, out, np - 1);
+    for (i = 0; i < 8 * num_dir; ++i) beam[i] = out[i];
+    free(X); free(Y); free(Z); free(theta); free(phi1); free(phi2);
+    free(signal); free(out); free(w); free(types);
+}

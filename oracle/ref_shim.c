@@ -19,6 +19,11 @@
 #include "math/define_dftw_m2m.h"
 #include "telescope/station/define_evaluate_element_weights_dft.h"
 #include "convert/define_convert_ecef_to_station_uvw.h"
+#include "convert/define_convert_enu_directions_to_theta_phi.h"
+#include "telescope/station/element/define_evaluate_dipole_pattern.h"
+#include "telescope/station/define_blank_below_horizon.h"
+#include "mem/define_mem_normalise.h"
+#include "interferometer/define_evaluate_jones_R.h"
 
 #define INST(REAL, S, REAL2, REAL4c) \
 OSKAR_ACORR_CPU(k_acorr_##S, REAL, REAL2, REAL4c) \
@@ -86,3 +91,35 @@ void ref_ecef_to_station_uvw_##S(int n, const REAL* x, const REAL* y, \
 
 INST(double, d, double2, double4c)
 INST(float, f, float2, float4c)
+
+/* Station-beam pieces: element coordinates, dipole pattern, normalisation,
+ * horizon blanking and the parallactic-angle rotation R. */
+#define INST_BEAM(REAL, S, REAL2, REAL4c) \
+OSKAR_CONVERT_ENU_DIR_TO_THETA_PHI(k_theta_phi_##S, REAL) \
+OSKAR_EVALUATE_DIPOLE_PATTERN(k_dipole_##S, REAL, REAL2, REAL4c) \
+OSKAR_BLANK_BELOW_HORIZON_MATRIX(k_blank_##S, REAL, REAL4c) \
+OSKAR_MEM_NORMALISE_MATRIX_CPU(k_normalise_##S, REAL, REAL4c) \
+OSKAR_JONES_R(k_jones_r_##S, REAL, REAL4c) \
+void ref_enu_to_theta_phi_##S(int off_in, int num, const REAL* x, \
+        const REAL* y, const REAL* z, int extra_point_at_pole, REAL dphi1, \
+        REAL dphi2, REAL* theta, REAL* phi1, REAL* phi2) \
+{ k_theta_phi_##S(off_in, num, x, y, z, extra_point_at_pole, dphi1, dphi2, \
+        theta, phi1, phi2); } \
+void ref_dipole_pattern_##S(int n, const REAL* theta, const REAL* phi_x, \
+        const REAL* phi_y, REAL kL, REAL cos_kL, int swap_xy, \
+        int offset_out, REAL4c* pattern) \
+{ k_dipole_##S(n, theta, phi_x, phi_y, kL, cos_kL, swap_xy, offset_out, \
+        pattern); } \
+void ref_blank_below_horizon_##S(int off_mask, int n, const REAL* mask, \
+        int off_out, REAL4c* jones) \
+{ k_blank_##S(off_mask, n, mask, off_out, jones); } \
+void ref_mem_normalise_matrix_##S(int offset, int n, REAL4c* a, int idx) \
+{ k_normalise_##S((unsigned) offset, (unsigned) n, a, (unsigned) idx); } \
+void ref_jones_r_##S(int num_sources, const REAL* ra, const REAL* dec, \
+        REAL cos_lat, REAL sin_lat, REAL lst_rad, int offset_out, \
+        REAL4c* jones) \
+{ k_jones_r_##S(num_sources, ra, dec, cos_lat, sin_lat, lst_rad, \
+        offset_out, jones); }
+
+INST_BEAM(double, d, double2, double4c)
+INST_BEAM(float, f, float2, float4c)

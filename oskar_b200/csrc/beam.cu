@@ -1,0 +1,379 @@
+// Aperture-array station beam (Jones E) for many stations in one launch, and
+// the parallactic-angle rotation (Jones R).
+//
+// Replaces the chain the reference runs per station and per feed
+// (oskar/telescope/station/src/oskar_station_beam.c:84-182 and
+// oskar_evaluate_station_beam_aperture_array.c:150-240): element pattern
+// (dipole, oskar_element_evaluate.c:76-157), element weights
+// (define_evaluate_element_weights_dft.h:3-16), weighted DFT
+// (define_dftw_m2m.h:24-107), horizon blanking
+// (define_blank_below_horizon.h:15-29) and final normalisation
+// (define_mem_normalise.h:31-51). The reference runs these as six kernels
+// with five round trips through a per-station signal buffer; here one thread
+// owns one (station, direction) and the pieces stay in registers.
+//
+// With a single element type the weighted DFT of the element signals is
+// pattern(dir) x AF(dir), AF = sum_e w_e exp(i k r_e . dir): the pattern is
+// evaluated once per direction and the element loop carries only the array
+// factor (one sincos and one complex multiply-add per element-direction).
+// Element weights and positions are staged in shared memory in chunks.
+// The normalisation direction's beam (one per station) is recomputed by each
+// CTA cooperatively before the main loop, so there is no second launch.
+#include "common.cuh"
+
+namespace oskb {
+namespace {
+
+constexpr int kThreads = 128;
+constexpr int kChunk = 512;
+
+struct BeamFlags
+{
+    int normalise_element, normalise_array, normalise_final, swap_xy;
+};
+
+// Dipole far field along phi for a direction with (sin, cos) theta
+// (oskar/telescope/station/element/define_evaluate_dipole_pattern.h:3-15).
+template <typename T>
+__device__ __forceinline__ void dipole(T kL, T cos_kL, T sin_th, T cos_th,
+        T phi, T& e_theta, T& e_phi)
+{
+    T sp, cp;
+    sincos(phi, &sp, &cp);
+    const T denom = (T) 1 + cp * cp * (cos_th * cos_th - (T) 1);
+    if (denom == (T) 0)
+    {
+        e_theta = e_phi = (T) 0;
+        return;
+    }
+    const T t = (cos(kL * cp * sin_th) - cos_kL) / denom;
+    e_theta = -cp * cos_th * t;
+    e_phi = sp * t;
+}
+
+// Real element-pattern matrix {a, b, c, d} for one direction
+// (define_convert_enu_directions_to_theta_phi.h:3-31 then
+// define_evaluate_dipole_pattern.h:17-48). pole: the extra point at theta = 0
+// whose phi values are the unwrapped offsets.
+template <typename T>
+__device__ __forceinline__ void element_pattern(T X, T Y, T Z, bool pole,
+        T dphi1, T dphi2, T kL, T cos_kL, int swap_xy, T p[4])
+{
+    T theta, phi1, phi2;
+    if (pole)
+    {
+        theta = (T) 0;
+        phi1 = dphi1;
+        phi2 = dphi2;
+    }
+    else
+    {
+        const T twopi = (T) 2 * (T) kPi;
+        const T p0 = atan2(Y, X);
+        phi1 = fmod(p0 + dphi1, twopi);
+        phi2 = fmod(p0 + dphi2, twopi);
+        if (phi1 < (T) 0) phi1 += twopi;
+        if (phi2 < (T) 0) phi2 += twopi;
+        theta = atan2(sqrt(X * X + Y * Y), Z);
+    }
+    T st, ct, xt, xp, yt, yp;
+    sincos(theta, &st, &ct);
+    dipole(kL, cos_kL, st, ct, phi1, xt, xp);
+    dipole(kL, cos_kL, st, ct, phi2, yt, yp);
+    p[0] = swap_xy ? yt : xt;
+    p[1] = swap_xy ? yp : xp;
+    p[2] = swap_xy ? xt : yt;
+    p[3] = swap_xy ? xp : yp;
+}
+
+template <typename T>
+__device__ __forceinline__ T half_frobenius(const T p[4], T ar, T ai)
+{
+    // |p * af|_F^2 / 2 with p real and af complex.
+    const T a2 = ar * ar + ai * ai;
+    return (p[0] * p[0] + p[1] * p[1] + p[2] * p[2] + p[3] * p[3]) * a2 /
+            (T) 2;
+}
+
+template <typename T, bool IS3D>
+__global__ void __launch_bounds__(kThreads)
+station_beam_kernel(int num_elements, const T* __restrict__ el_x,
+        const T* __restrict__ el_y, const T* __restrict__ el_z,
+        const T* __restrict__ meas_x, const T* __restrict__ meas_y,
+        const T* __restrict__ meas_z, const T* __restrict__ cable,
+        const double* __restrict__ orientation_x,
+        const double* __restrict__ orientation_y, T kL, T cos_kL,
+        BeamFlags flags, T wavenumber, const double* __restrict__ beam_enu,
+        const double* __restrict__ norm_enu, int num_dir,
+        const T* __restrict__ dir_x, const T* __restrict__ dir_y,
+        const T* __restrict__ dir_z, int directions_per_station,
+        T* __restrict__ beam)
+{
+    typedef typename vec2<T>::type T2;
+    __shared__ T2 s_w[kChunk];
+    __shared__ T s_x[kChunk], s_y[kChunk], s_z[IS3D ? kChunk : 1];
+    __shared__ T s_red[2][kThreads / 32];
+    const int st = blockIdx.y;
+    const int d = blockIdx.x * kThreads + threadIdx.x;
+    const bool active = d < num_dir;
+    const size_t el0 = (size_t) st * num_elements;
+    const size_t dir0 = directions_per_station ? (size_t) st * num_dir : 0;
+    T2* out = reinterpret_cast<T2*>(beam) + 4 * ((size_t) st * num_dir + d);
+
+    const T bx = (T) beam_enu[3 * st], by = (T) beam_enu[3 * st + 1],
+            bz = (T) beam_enu[3 * st + 2];
+    if (beam_enu[3 * st + 2] < 0.0)  // pointing below the horizon
+    {
+        if (active)
+            for (int k = 0; k < 4; ++k) out[k] = T2{(T) 0, (T) 0};
+        return;
+    }
+    const T dphi1 = (T) (kPi / 2 - (orientation_x[st] + kPi / 2));
+    const T dphi2 = (T) (kPi / 2 - orientation_y[st]);
+
+    T X = 0, Y = 0, Z = 0;
+    if (active)
+    {
+        X = dir_x[dir0 + d];
+        Y = dir_y[dir0 + d];
+        Z = dir_z[dir0 + d];
+    }
+    T nX = 0, nY = 0, nZ = 1;
+    if (flags.normalise_final)
+    {
+        nX = (T) norm_enu[3 * st];
+        nY = (T) norm_enu[3 * st + 1];
+        nZ = (T) norm_enu[3 * st + 2];
+    }
+    const T kX = wavenumber * X, kY = wavenumber * Y, kZ = wavenumber * Z;
+    const T knX = wavenumber * nX, knY = wavenumber * nY,
+            knZ = wavenumber * nZ;
+
+    T ar = 0, ai = 0;    // array factor, this thread's direction
+    T nr = 0, ni = 0;    // array factor of the normalisation direction
+    for (int e0 = 0; e0 < num_elements; e0 += kChunk)
+    {
+        const int ne = min(kChunk, num_elements - e0);
+        for (int t = threadIdx.x; t < ne; t += kThreads)
+        {
+            const size_t g = el0 + e0 + t;
+            const T mx = meas_x ? meas_x[g] : el_x[g];
+            const T my = meas_y ? meas_y[g] : el_y[g];
+            const T mz = meas_z ? meas_z[g] : (el_z ? el_z[g] : (T) 0);
+            const T p = wavenumber * (mx * bx + my * by + mz * bz +
+                    (cable ? cable[g] : (T) 0));
+            T sn, cs;
+            sincos(-p, &sn, &cs);
+            s_w[t] = T2{cs, sn};
+            s_x[t] = el_x[g];
+            s_y[t] = el_y[g];
+            if (IS3D) s_z[t] = el_z[g];
+            // The normalisation direction: elements split across threads.
+            if (flags.normalise_final)
+            {
+                T ph = knX * s_x[t] + knY * s_y[t];
+                if (IS3D) ph += knZ * s_z[t];
+                T s2, c2;
+                sincos(ph, &s2, &c2);
+                nr += c2 * cs - sn * s2;
+                ni += s2 * cs + sn * c2;
+            }
+        }
+        __syncthreads();
+        if (active)
+        {
+#pragma unroll 4
+            for (int i = 0; i < ne; ++i)
+            {
+                T ph = kX * s_x[i] + kY * s_y[i];
+                if (IS3D) ph += kZ * s_z[i];
+                T sn, cs;
+                sincos(ph, &sn, &cs);
+                const T2 w = s_w[i];
+                ar += cs * w.x - w.y * sn;
+                ai += sn * w.x + w.y * cs;
+            }
+        }
+        __syncthreads();
+    }
+
+    // Element normalisation: 1 / |pattern at the pole|.
+    T pole_scale = (T) 1;
+    if (flags.normalise_element)
+    {
+        T pp[4];
+        element_pattern<T>(0, 0, 1, true, dphi1, dphi2, kL, cos_kL,
+                flags.swap_xy, pp);
+        pole_scale = (T) 1 / sqrt(half_frobenius<T>(pp, 1, 0));
+    }
+    const T array_scale = flags.normalise_array ?
+            (T) (1.0 / num_elements) : (T) 1;
+
+    // Final normalisation: amplitude of the beam in the normalisation
+    // direction (block reduction of its array factor first).
+    T final_scale = (T) 1;
+    if (flags.normalise_final)
+    {
+        for (int o = 16; o > 0; o >>= 1)
+        {
+            nr += __shfl_xor_sync(0xffffffffu, nr, o);
+            ni += __shfl_xor_sync(0xffffffffu, ni, o);
+        }
+        if ((threadIdx.x & 31) == 0)
+        {
+            s_red[0][threadIdx.x >> 5] = nr;
+            s_red[1][threadIdx.x >> 5] = ni;
+        }
+        __syncthreads();
+        nr = ni = 0;
+        for (int w = 0; w < kThreads / 32; ++w)
+        {
+            nr += s_red[0][w];
+            ni += s_red[1][w];
+        }
+        T pn[4];
+        element_pattern<T>(nX, nY, nZ, false, dphi1, dphi2, kL, cos_kL,
+                flags.swap_xy, pn);
+        for (int k = 0; k < 4; ++k) pn[k] *= pole_scale * array_scale;
+        // A normalisation direction below the horizon is blanked, as in the
+        // reference, which then divides by zero.
+        if (nZ < (T) 0) nr = ni = (T) 0;
+        final_scale = (T) 1 / sqrt(half_frobenius<T>(pn, nr, ni));
+    }
+    if (!active) return;
+
+    T p[4];
+    element_pattern<T>(X, Y, Z, false, dphi1, dphi2, kL, cos_kL,
+            flags.swap_xy, p);
+    const bool blank = Z < (T) 0;
+    for (int k = 0; k < 4; ++k)
+    {
+        // The reference's order: pattern (normalised), times the weighted
+        // element sum, times the DFT norm, then the final scale.
+        const T pk = p[k] * pole_scale;
+        T2 v{pk * ar * array_scale, pk * ai * array_scale};
+        if (blank) v = T2{(T) 0, (T) 0};
+        v.x *= final_scale;
+        v.y *= final_scale;
+        out[k] = v;
+    }
+}
+
+template <typename T>
+__global__ void __launch_bounds__(256)
+jones_r_kernel(int num_sources, const T* __restrict__ ra,
+        const T* __restrict__ dec, const double* __restrict__ lat_rad,
+        const double* __restrict__ lst_rad, T* __restrict__ jones)
+{
+    typedef typename vec2<T>::type T2;
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    const int st = blockIdx.y;
+    if (s >= num_sources) return;
+    // (define_evaluate_jones_R.h:3-29; per-station latitude and LST as the
+    // driver oskar_evaluate_jones_R.c:42-49 derives them in double.)
+    const T cos_lat = (T) cos(lat_rad[st]), sin_lat = (T) sin(lat_rad[st]);
+    const T lst = (T) lst_rad[st];
+    T sh, ch, sd, cd, sq, cq;
+    sincos(lst - ra[s], &sh, &ch);
+    sincos(dec[s], &sd, &cd);
+    const T q = atan2(cos_lat * sh, sin_lat * cd - cos_lat * sd * ch);
+    sincos(q, &sq, &cq);
+    T2* o = reinterpret_cast<T2*>(jones) + 4 * ((size_t) st * num_sources + s);
+    o[0] = T2{cq, (T) 0};
+    o[1] = T2{-sq, (T) 0};
+    o[2] = T2{sq, (T) 0};
+    o[3] = T2{cq, (T) 0};
+}
+
+}  // namespace
+}  // namespace oskb
+
+namespace oskb {
+namespace {
+
+template <typename T>
+int station_beam_aa(int num_stations, int num_elements, const T* el_x,
+        const T* el_y, const T* el_z, const T* meas_x, const T* meas_y,
+        const T* meas_z, const T* cable, const double* orientation_x,
+        const double* orientation_y, double dipole_length_m,
+        int normalise_element, int normalise_array, int normalise_final,
+        int swap_xy, int is_3d, double frequency_hz, const double* beam_enu,
+        const double* norm_enu, int num_directions, const T* x, const T* y,
+        const T* z, int directions_per_station, T* beam, void* stream)
+{
+    if (num_stations < 0 || num_elements < 0 || num_directions < 0)
+        return OSKB_ERR_INVALID_ARGUMENT;
+    if (num_stations == 0 || num_directions == 0) return 0;
+    if (num_elements == 0 || !el_x || !el_y || (is_3d && !el_z) ||
+            !orientation_x || !orientation_y || !beam_enu ||
+            (normalise_final && !norm_enu) || !x || !y || !z || !beam)
+        return OSKB_ERR_INVALID_ARGUMENT;
+    if (num_stations > 65535) return OSKB_ERR_INVALID_ARGUMENT;
+    const double c0 = 299792458.0;
+    const double kL = dipole_length_m * (kPi * frequency_hz / c0);
+    const T wavenumber = (T) (2.0 * kPi * frequency_hz / c0);
+    BeamFlags flags{normalise_element, normalise_array, normalise_final,
+            swap_xy};
+    dim3 grid((num_directions + kThreads - 1) / kThreads, num_stations);
+    cudaStream_t s = as_stream(stream);
+#define OSKB_BEAM(D) station_beam_kernel<T, D><<<grid, kThreads, 0, s>>>(     \
+        num_elements, el_x, el_y, el_z, meas_x, meas_y, meas_z, cable,       \
+        orientation_x, orientation_y, (T) kL, (T) cos(kL), flags,            \
+        wavenumber, beam_enu, norm_enu, num_directions, x, y, z,             \
+        directions_per_station, beam)
+    if (is_3d) OSKB_BEAM(true); else OSKB_BEAM(false);
+#undef OSKB_BEAM
+    return check_launch("station_beam_aa");
+}
+
+template <typename T>
+int jones_r(int num_sources, const T* ra, const T* dec, int num_stations,
+        const double* lat_rad, const double* lst_rad, T* jones, void* stream)
+{
+    if (num_sources < 0 || num_stations < 0 || num_stations > 65535)
+        return OSKB_ERR_INVALID_ARGUMENT;
+    if (num_sources == 0 || num_stations == 0) return 0;
+    if (!ra || !dec || !lat_rad || !lst_rad || !jones)
+        return OSKB_ERR_INVALID_ARGUMENT;
+    dim3 grid((num_sources + 255) / 256, num_stations);
+    jones_r_kernel<T><<<grid, 256, 0, as_stream(stream)>>>(num_sources, ra,
+            dec, lat_rad, lst_rad, jones);
+    return check_launch("evaluate_jones_R");
+}
+
+}  // namespace
+}  // namespace oskb
+
+extern "C" {
+
+#define OSKB_BEAM_ENTRY(T, S)                                                \
+int oskb_station_beam_aa_##S(int num_stations, int num_elements,             \
+        const T* el_x, const T* el_y, const T* el_z, const T* meas_x,        \
+        const T* meas_y, const T* meas_z, const T* cable_length_error,       \
+        const double* orientation_x_rad, const double* orientation_y_rad,    \
+        double dipole_length_m, int normalise_element, int normalise_array,  \
+        int normalise_final, int swap_xy, int is_3d, double frequency_hz,    \
+        const double* beam_enu, const double* norm_enu, int num_directions,  \
+        const T* x, const T* y, const T* z, int directions_per_station,      \
+        T* beam, void* stream)                                               \
+{                                                                            \
+    return oskb::station_beam_aa<T>(num_stations, num_elements, el_x, el_y,  \
+            el_z, meas_x, meas_y, meas_z, cable_length_error,                \
+            orientation_x_rad, orientation_y_rad, dipole_length_m,           \
+            normalise_element, normalise_array, normalise_final, swap_xy,    \
+            is_3d, frequency_hz, beam_enu, norm_enu, num_directions, x, y,   \
+            z, directions_per_station, beam, stream);                        \
+}                                                                            \
+int oskb_evaluate_jones_R_##S(int num_sources, const T* ra_rad,              \
+        const T* dec_rad, int num_stations, const double* lat_rad,           \
+        const double* lst_rad, T* jones, void* stream)                       \
+{                                                                            \
+    return oskb::jones_r<T>(num_sources, ra_rad, dec_rad, num_stations,      \
+            lat_rad, lst_rad, jones, stream);                                \
+}
+
+OSKB_BEAM_ENTRY(double, d)
+OSKB_BEAM_ENTRY(float, f)
+#undef OSKB_BEAM_ENTRY
+
+}  // extern "C"

@@ -1,0 +1,123 @@
+"""GPU parity of the fused station beam (Jones E) and of Jones R against the
+CPU oracle, whose composite station beam is pinned step by step against the
+reference's own kernels (tests/test_oracle_pin.py).
+
+Three stations with different layouts, element orientations and pointings
+are evaluated in one launch and compared with the oracle station by station.
+Tolerances: FP64 1e-12 of the largest beam value (max and L2 relative);
+FP32 2e-5.
+"""
+import numpy as np
+import pytest
+
+torch = pytest.importorskip("torch")
+pytestmark = [pytest.mark.gpu,
+              pytest.mark.skipif(not torch.cuda.is_available(),
+                                 reason="needs a CUDA device")]
+
+import oskar_b200 as ob  # noqa: E402
+from beam_cases import beam_case, oracle_beam  # noqa: E402
+from oracle_lib import oracle, suffix  # noqa: E402
+
+TOL = {np.float64: 1e-12, np.float32: 2e-5}
+
+
+def dev(a):
+    return torch.from_numpy(np.ascontiguousarray(a)).cuda()
+
+
+def rel(got, ref):
+    got = np.asarray(got, np.float64)
+    ref = np.asarray(ref, np.float64)
+    return max(np.max(np.abs(got - ref)) / np.max(np.abs(ref)),
+               np.linalg.norm(got - ref) / np.linalg.norm(ref))
+
+
+def stations(real, num_st=3, num_el=256, num_dir=1001, is_3d=1):
+    cases = [beam_case(real, seed=30 + s, num_el=num_el, num_dir=num_dir,
+                       is_3d=is_3d) for s in range(num_st)]
+    for s, c in enumerate(cases):
+        c["orient"] = (0.1 * s, 0.1 * s + np.pi / 2)
+        c["dirs"] = cases[0]["dirs"]  # shared directions unless per-station
+    return cases
+
+
+def run_gpu(cases, real, flags, per_station_dirs=False):
+    norm_el, norm_arr, norm_fin, swap, is_3d = flags
+    st = len(cases)
+    cat = lambda key, i: dev(np.concatenate([c[key][i] for c in cases]))
+    el = [cat("el", i) for i in range(3)]
+    me = [cat("meas", i) for i in range(3)]
+    cable = dev(np.concatenate([c["cable"] for c in cases]))
+    ox = dev(np.array([c["orient"][0] for c in cases]))
+    oy = dev(np.array([c["orient"][1] for c in cases]))
+    b = dev(np.stack([c["b"] for c in cases]))
+    nrm = dev(np.stack([c["norm"] for c in cases]))
+    nd = len(cases[0]["dirs"][0])
+    if per_station_dirs:
+        dirs = [cat("dirs", i) for i in range(3)]
+    else:
+        dirs = [dev(cases[0]["dirs"][i]) for i in range(3)]
+    out = torch.zeros(st * nd * 8, dtype=torch.float64 if real == np.float64
+                      else torch.float32, device="cuda")
+    ob.call("oskb_station_beam_aa_" + suffix(real), st, len(cases[0]["cable"]),
+            *el, *me, cable, ox, oy, cases[0]["L"], norm_el, norm_arr,
+            norm_fin, swap, is_3d, cases[0]["freq"], b, nrm, nd, *dirs,
+            int(per_station_dirs), out, ob.stream_ptr())
+    torch.cuda.synchronize()
+    return out.cpu().numpy().reshape(st, nd * 8)
+
+
+@pytest.mark.parametrize("real", [np.float64, np.float32])
+@pytest.mark.parametrize("flags", [(1, 1, 1, 0, 1), (0, 1, 1, 1, 0),
+                                   (1, 0, 0, 0, 1), (0, 0, 1, 0, 0)])
+def test_station_beam_vs_oracle(real, flags):
+    cases = stations(real, is_3d=flags[4])
+    cases[2]["b"] = np.array([-0.5, 0.1, np.sqrt(1 - 0.26)])
+    cases[2]["norm"] = cases[2]["b"].copy()
+    got = run_gpu(cases, real, flags)
+    for s, c in enumerate(cases):
+        ref = oracle_beam(c, real, flags)
+        assert rel(got[s], ref) <= TOL[real], (s, rel(got[s], ref))
+        blank = c["dirs"][2] < 0
+        assert not got[s].reshape(-1, 8)[blank].any()
+
+
+@pytest.mark.parametrize("real", [np.float64, np.float32])
+def test_station_beam_per_station_directions(real):
+    """Per-station direction cosines ([station][direction])."""
+    cases = [beam_case(real, seed=40 + s, num_el=200, num_dir=513)
+             for s in range(2)]
+    flags = (1, 1, 1, 0, 1)
+    got = run_gpu(cases, real, flags, per_station_dirs=True)
+    for s, c in enumerate(cases):
+        assert rel(got[s], oracle_beam(c, real, flags)) <= TOL[real]
+
+
+def test_station_beam_pointing_below_horizon_is_zero():
+    cases = stations(np.float64, num_st=2, num_dir=300)
+    cases[1]["b"] = np.array([0.0, 0.6, -0.8])
+    got = run_gpu(cases, np.float64, (1, 1, 1, 0, 1))
+    assert got[0].any() and not got[1].any()
+
+
+@pytest.mark.parametrize("real", [np.float64, np.float32])
+def test_jones_r_vs_oracle(real):
+    rng = np.random.default_rng(15)
+    ns, nst = 2000, 4
+    ra = rng.uniform(-np.pi, np.pi, ns).astype(real)
+    dec = rng.uniform(-1.5, 1.5, ns).astype(real)
+    lat = rng.uniform(-0.8, 0.8, nst)
+    lst = rng.uniform(0, 2 * np.pi, nst)
+    out = torch.zeros(nst * ns * 8, dtype=torch.float64 if real == np.float64
+                      else torch.float32, device="cuda")
+    ob.call("oskb_evaluate_jones_R_" + suffix(real), ns, dev(ra), dev(dec),
+            nst, dev(lat), dev(lst), out, ob.stream_ptr())
+    torch.cuda.synchronize()
+    got = out.cpu().numpy().reshape(nst, -1)
+    for s in range(nst):
+        ref = np.zeros(8 * ns, real)
+        oracle().call("jones_r_" + suffix(real), real, ns, ra, dec,
+                      real(np.cos(lat[s])), real(np.sin(lat[s])),
+                      real(lst[s]), 0, ref)
+        assert rel(got[s], ref) <= (1e-13 if real == np.float64 else 2e-5)

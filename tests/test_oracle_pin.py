@@ -11,6 +11,7 @@ import pytest
 
 from oracle_lib import oracle, reference, reference_xcorr, suffix
 from xcorr_cases import XcorrCase
+from beam_cases import enu_dirs as _enu_dirs, beam_case, oracle_beam
 
 pytestmark = pytest.mark.skipif(reference() is None,
                                 reason="reference sources not present")
@@ -154,3 +155,100 @@ def test_element_weights_and_uvw(real):
         if lib is reference():
             for a, b in zip(outs[0], outs[1]):
                 assert _close(a, b, real)
+
+
+@pytest.mark.parametrize("real", [np.float64, np.float32])
+@pytest.mark.parametrize("pole", [0, 1])
+def test_enu_to_theta_phi(real, pole):
+    rng = np.random.default_rng(11)
+    n, off = 500, 3
+    x, y, z = _enu_dirs(rng, n + off, real)
+    outs = [[np.zeros(n + 1, real) for _ in range(3)] for _ in range(2)]
+    for lib, o in zip([oracle(), reference()], outs):
+        lib.call("enu_to_theta_phi_" + suffix(real), real, off, n, x, y, z,
+                 pole, -0.7, 1.2, *o)
+    for a, b in zip(*outs):
+        assert _close(a, b, real)
+
+
+@pytest.mark.parametrize("real", [np.float64, np.float32])
+@pytest.mark.parametrize("swap", [0, 1])
+def test_dipole_pattern(real, swap):
+    rng = np.random.default_rng(12)
+    n = 700
+    th = rng.uniform(0, np.pi / 2, n).astype(real)
+    th[:3] = 0  # at the pole the pattern denominator may vanish
+    px, py = (rng.uniform(0, 2 * np.pi, n).astype(real) for _ in range(2))
+    px[1], py[2] = 0, np.pi / 2
+    kL = 1.5 * np.pi * 150e6 / 299792458.0
+    outs = [np.zeros(8 * (n + 2), real) for _ in range(2)]
+    for lib, o in zip([oracle(), reference()], outs):
+        lib.call("dipole_pattern_" + suffix(real), real, n, th, px, py,
+                 real(kL), real(np.cos(kL)), swap, 2, o)
+    assert _close(outs[0], outs[1], real)
+
+
+@pytest.mark.parametrize("real", [np.float64, np.float32])
+def test_normalise_blank_jones_r(real):
+    rng = np.random.default_rng(13)
+    n = 300
+    a0 = rng.uniform(-1, 1, 8 * n).astype(real)
+    a = [a0.copy(), a0.copy()]
+    for lib, o in zip([oracle(), reference()], a):
+        lib.call("mem_normalise_matrix_" + suffix(real), real, 5, 200, o, 77)
+    assert _close(a[0], a[1], real)
+    mask = rng.uniform(-1, 1, n + 4).astype(real)
+    b = [a0.copy(), a0.copy()]
+    for lib, o in zip([oracle(), reference()], b):
+        lib.call("blank_below_horizon_" + suffix(real), real, 4, n - 2, mask,
+                 2, o)
+    assert np.array_equal(b[0], b[1])
+    ra, dec = (rng.uniform(-1.5, 1.5, n).astype(real) for _ in range(2))
+    lat, lst = -0.47, 2.1
+    r = [np.zeros(8 * (n + 1), real) for _ in range(2)]
+    for lib, o in zip([oracle(), reference()], r):
+        lib.call("jones_r_" + suffix(real), real, n, ra, dec,
+                 real(np.cos(lat)), real(np.sin(lat)), real(lst), 1, o)
+    assert _close(r[0], r[1], real)
+
+
+@pytest.mark.parametrize("real", [np.float64, np.float32])
+@pytest.mark.parametrize("flags", [(1, 1, 1, 0, 1), (0, 1, 1, 1, 0),
+                                   (1, 0, 0, 0, 1), (0, 0, 1, 0, 0)])
+def test_station_beam_composition(real, flags):
+    """The oracle's composite station beam equals the same chain built from
+    the reference's own kernels, step by step."""
+    norm_el, norm_arr, norm_fin, swap, is_3d = flags
+    c = beam_case(real, num_dir=301)
+    got = oracle_beam(c, real, flags)
+    ref, s = reference(), suffix(real)
+    nd = len(c["dirs"][0])
+    npt = nd + norm_fin
+    X, Y, Z = (np.ascontiguousarray(np.append(d, real(v)), dtype=real)
+               [:npt].copy() for d, v in zip(c["dirs"], c["norm"]))
+    th, p1, p2 = (np.zeros(npt + 1, real) for _ in range(3))
+    dphi1 = np.pi / 2 - (c["orient"][0] + np.pi / 2)
+    dphi2 = np.pi / 2 - c["orient"][1]
+    ref.call("enu_to_theta_phi_" + s, real, 0, npt, X, Y, Z, norm_el,
+             real(dphi1), real(dphi2), th, p1, p2)
+    kL = c["L"] * (np.pi * c["freq"] / 299792458.0)
+    sig = np.zeros(8 * (npt + 1), real)
+    ref.call("dipole_pattern_" + s, real, npt + norm_el, th, p1, p2,
+             real(kL), real(np.cos(kL)), swap, 0, sig)
+    if norm_el:
+        ref.call("mem_normalise_matrix_" + s, real, 0, npt, sig, npt)
+    k = 2 * np.pi * c["freq"] / 299792458.0
+    w = np.zeros(2 * len(c["el"][0]), real)
+    ref.call("element_weights_dft_" + s, real, len(w) // 2, *c["meas"],
+             c["cable"], real(k), *(real(v) for v in c["b"]), w)
+    out = np.zeros(8 * npt, real)
+    ref.call("dftw_" + s, real, 1, is_3d, len(w) // 2, real(k), w, *c["el"],
+             0, npt, X, Y, Z if is_3d else None,
+             np.zeros(len(w) // 2, np.int32), sig, 1, 1, 0, out,
+             real(1.0 / (len(w) // 2)) if norm_arr else real(1))
+    ref.call("blank_below_horizon_" + s, real, 0, npt, Z, 0, out)
+    if norm_fin:
+        ref.call("mem_normalise_matrix_" + s, real, 0, npt, out, npt - 1)
+    assert np.array_equal(got, out[:8 * nd]) or _close(got, out[:8 * nd],
+                                                        real)
+    assert np.count_nonzero(got) > 0
