@@ -103,6 +103,28 @@ def test_xcorr_uv_filter(real):
     assert changed.any() and not changed.all()  # filtered baselines kept
 
 
+@pytest.mark.parametrize("slices", ["1", "3", "7"])
+@pytest.mark.parametrize("real", [np.float64, np.float32])
+def test_xcorr_source_slices(slices, real, monkeypatch):
+    """The source loop split across CTAs (partial sums per slice, reduced in
+    slice order) gives the oracle's result for any slice count, with the uv
+    filter on so that filtered baselines must come out untouched."""
+    monkeypatch.setenv("OSKB_XCORR_SLICES", slices)
+    c = XcorrCase(70, 300, real=real, uv_min=0.5, uv_max=1.2, offset_out=5,
+                  bandwidth_hz=10e3)
+    got, ref = run_gpu_xcorr(c, real), run_oracle_xcorr(c, real)
+    assert_close(got, ref, real)
+    changed = np.any((got != c.vis0).reshape(-1, 8), axis=1)
+    assert changed.any() and not changed.all()
+
+
+def test_xcorr_slices_deterministic():
+    """Two runs with the default slicing give bit-identical output."""
+    c = XcorrCase(100, 5000, ranges="physical", seed=9)
+    assert np.array_equal(run_gpu_xcorr(c, np.float64),
+                          run_gpu_xcorr(c, np.float64))
+
+
 def test_xcorr_empty_inputs():
     c = XcorrCase(5, 4)
     vis = dev(c.vis0)
