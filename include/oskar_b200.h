@@ -283,6 +283,60 @@ OSKB_API int oskb_cross_correlate_tc_d(int use_casa_phase_convention,
         double inv_wavelength, double* vis, void* workspace,
         size_t workspace_bytes, void* stream);
 
+/* Direct (FP64 or FP32) block correlator with smearing: for every (dump t,
+ * channel c) of a block, in ONE persistent launch,
+ *   vis[t][c][pq] += sum_s smear_pq(s) (J_p B J_q^H)(s),  J = K(t, c) E,
+ * with K exactly as oskar_evaluate_jones_K forms it (phase
+ * 2 pi / lambda_c (u l + v m + w (n - 1)) in the working precision; K = 0
+ * where I is outside (source_filter_min, source_filter_max]), and smear_pq
+ * the Gaussian, bandwidth and time-average factors of the reference's
+ * correlator (oskar/correlate/define_cross_correlate.h:16-111). Replaces
+ * the per-(dump, chunk, channel) sequence Jones K -> join -> correlate of
+ * sim_baselines (oskar/interferometer/src/oskar_interferometer_run_block.c:
+ * 156-336); K and J are formed in shared memory, never stored.
+ *   E: [station][source] 2x2 (or [dump][station][source] if E_per_dump);
+ *      NULL for identity (J = K);
+ *   a, b, c: Gaussian shape per source, or all NULL for point sources.
+ *      Sources of the reference's point-source chunks carry a = b = c = 0
+ *      (exp(-0) = 1 exactly), so one call covers chunks of both kinds;
+ *   station_uvw: [dump][3][station] metres; station_x/y: ECEF offsets
+ *      (time smearing only); inv_wavelength: [channel] = f_c / c0;
+ *      gha0_rad: [dump] Greenwich hour angle of the phase centre (time
+ *      smearing only);
+ *   uv_filter_units: 0 metres (scaled per channel), 1 wavelengths;
+ *   vis: [dump][channel][baseline][2x2], accumulated.
+ * All arrays are device memory; inv_wavelength and gha0_rad are double in
+ * both precisions. The launch schedule (grid, item order) is chosen per
+ * block shape by timing candidates on a sample of the block the first time
+ * that shape is seen (OSKB_AUTOTUNE=0: fixed default; OSKB_BLOCK_SCHEDULE=
+ * "ctas_per_sm,tile_major": forced). Results do not depend on it. */
+OSKB_API int oskb_correlate_block_direct_d(int casa, int num_sources,
+        int num_stations, int num_times, int num_channels, const double* E,
+        int E_per_dump, const double* I, const double* Q, const double* U,
+        const double* V, const double* l, const double* m, const double* n,
+        const double* a, const double* b, const double* c,
+        const double* station_uvw, const double* station_x,
+        const double* station_y, const double* inv_wavelength,
+        double channel_bandwidth_hz, double time_average_sec,
+        const double* gha0_rad, double dec0_rad, double uv_min,
+        double uv_max, int uv_filter_units, double source_filter_min,
+        double source_filter_max, double* vis, void* stream);
+OSKB_API int oskb_correlate_block_direct_f(int casa, int num_sources,
+        int num_stations, int num_times, int num_channels, const float* E,
+        int E_per_dump, const float* I, const float* Q, const float* U,
+        const float* V, const float* l, const float* m, const float* n,
+        const float* a, const float* b, const float* c,
+        const float* station_uvw, const float* station_x,
+        const float* station_y, const double* inv_wavelength,
+        double channel_bandwidth_hz, double time_average_sec,
+        const double* gha0_rad, double dec0_rad, double uv_min,
+        double uv_max, int uv_filter_units, double source_filter_min,
+        double source_filter_max, float* vis, void* stream);
+/* Text report of the schedules the block autotuner has chosen (one line
+ * per block shape, with the sample time of every candidate). Returns the
+ * number of characters written. */
+OSKB_API int oskb_block_tune_report(char* buf, int len);
+
 /* Fused block: for every (time t, channel c) of a block,
  *   vis[t][c] += sum_s (K_p E_p C)(s) (K_q E_q C)(s)^H
  * with K_p(s) = exp(2 pi i (u_p l + v_p m + w_p (n - 1)) / lambda_c) formed

@@ -1,19 +1,33 @@
-// Direct cross-correlation kernel (all source types and smearing modes).
+// Direct cross-correlation kernel (all source types and smearing modes), and
+// its batched form over whole (dump x channel) blocks.
 //
 // Replaces the reference's warp-per-baseline kernel
 // (oskar/correlate/src/oskar_cross_correlate_cuda.cu:45-224) with a
 // register-tiled form: one CTA owns a 32 x 32 block of stations (rows p,
 // columns q, lower triangle p > q as in the reference), each thread a 2 x 2
-// group of baselines. Sources are staged through shared memory in chunks:
-// the "left" factor J B (or I J in scalar mode) and the "right" factor J are
-// computed once per station-source for the whole CTA, so the per
-// source-baseline work is the 8 complex MACs of (J_p B) J_q^H. Smearing
-// arguments are per-station source phases (phi_p - phi_q), which turns the
-// reference's three multiply-adds per source-baseline into one subtraction.
-// FP64 mode accumulates in FP64; FP32 mode sums each chunk in FP32 and the
-// chunk sums in FP64.
+// group of baselines. Sources are staged through shared memory in chunks of
+// 8: cp.async lands the next chunk's raw Jones while the current chunk is
+// correlated, then a shared-to-shared transform forms the "left" factor J B
+// (or I J in scalar mode) and the "right" factor J once per station-source
+// for the whole CTA, so the per source-baseline work is the 8 complex MACs
+// of (J_p B) J_q^H. Smearing arguments are per-station source phases
+// (phi_p - phi_q), which turns the reference's three multiply-adds per
+// source-baseline into one subtraction. FP64 mode accumulates in FP64; FP32
+// mode sums each chunk in FP32 and the chunk sums in FP64.
+//
+// Work items. A launch covers items (dump t, channel c, station tile, source
+// slice); each CTA loops over items. The single-call entry points are one
+// dump and one channel with the sources split into slices (partial sums
+// reduced in slice order); the block entry point (oskb_correlate_block_direct)
+// covers every (t, c) of a block in one persistent launch with one slice per
+// item, and forms J = K(t, c) E in the staging transform, so neither K nor J
+// is ever written to memory (the reference's sim_baselines,
+// oskar/interferometer/src/oskar_interferometer_run_block.c:156-336, runs
+// K, join and correlate as separate launches per (t, chunk, c)).
 #include <stdlib.h>
 #include <string.h>
+
+#include <mutex>
 
 #include "common.cuh"
 
@@ -28,20 +42,35 @@ template <typename T>
 struct XcorrParams
 {
     int num_src, num_st, offset_out;
-    const T* jones;
+    int src_stride;  // sources per station row of jones (= num_src)
+    const T* jones;  // J [station][source], or E when K is fused
     const T *I, *Q, *U, *V, *l, *m, *n, *a, *b, *c;
+    // Station (u, v, w) metres of dump t at st_u + t * uvw_time_stride
+    // (v and w follow at +num_st and +2 num_st in block mode).
     const T *st_u, *st_v, *st_w, *st_x, *st_y;
-    double uv_min, uv_max, inv_wavelength;
-    double bw_scale;  // pi * frac_bandwidth * inv_wavelength
-    double ts_scale;  // pi * inv_wavelength * omega_earth * time_int_sec
-    double s_ha, c_ha, s_dec, c_dec;
+    long long uvw_time_stride;
+    double uv_min, uv_max;  // wavelengths (single call) or metres (block)
+    int uv_filter_in_metres;
+    double inv_wavelength;            // single call
+    const double* inv_wavelength_c;   // block: [channel]
+    double bw_scale;  // pi * frac_bandwidth * inv_wavelength (= pi bw / c0)
+    double ts_base;   // pi * omega_earth * time_int_sec (x inv_wavelength)
+    double gha0;                      // single call
+    const double* gha0_t;             // block: [dump]
+    double s_dec, c_dec;
     T* vis;
-    // Source slices: CTA (tile, y) sums sources [y * slice_len,
-    // (y + 1) * slice_len). With more than one slice, each CTA writes its
-    // sums to partial[y][baseline][comp] and reduce_partials adds them to
-    // vis in slice order (deterministic); with one slice it adds to vis.
-    int slice_len;
+    // Items: num_times x num_channels x tiles x slices, in that nesting
+    // (slices fastest). Source slice y covers [y * slice_len,
+    // (y + 1) * slice_len). With more than one slice (single call only),
+    // each CTA writes its sums to partial[y][baseline][comp] and
+    // reduce_partials adds them to vis in slice order (deterministic).
+    int num_times, num_channels, tiles, slices, slice_len;
+    int tile_major;  // item order: tile outermost instead of innermost
     double* partial;
+    // Fused Jones K (block mode): J = K E, K = exp(i 2 pi / lambda (u l +
+    // v m + w (n - 1))), zero where I is outside (filter_min, filter_max].
+    long long e_time_stride;  // E of dump t at jones + t * e_time_stride
+    double filter_min, filter_max;
 };
 
 template <typename T, bool MATRIX>
@@ -71,12 +100,22 @@ struct Smem
     // row (p) and column (q) blocks.
     T2 row[NCOMP][kChunk][kTile];
     T2 col[NCOMP][kChunk][kTile];
-    T ph_row[kChunk][kTile], ph_col[kChunk][kTile];  // bandwidth phases
-    T ps_row[kChunk][kTile], ps_col[kChunk][kTile];  // time-smearing phases
+    // Per-station smearing phases phi and their sin, cos:
+    // [block][phi, sin, cos][source][station], bandwidth (ph) and time (ps).
+    T ph[2][3][kChunk][kTile];
+    T ps[2][3][kChunk][kTile];
     T ga[kChunk], gb[kChunk], gc[kChunk];
-    // Per-station phase terms, loaded once per CTA: u, v, w (bandwidth)
-    // and the rotated x, y pair (time smearing).
-    double st_terms[2][kTile][5];
+    // Per-station terms, loaded once per item: u, v, w (bandwidth phase and
+    // fused K) and the rotated x, y pair (time smearing).
+    T st_uvw[2][kTile][3];
+    double st_xy[2][kTile][2];
+};
+
+// Per-item constants.
+struct ItemCtx
+{
+    int t, c, p0, q0, src_begin, src_end;
+    double inv_wavelength, ts_scale, s_ha, c_ha;
 };
 
 __device__ __forceinline__ void cp_async(void* smem, const void* gmem,
@@ -105,10 +144,27 @@ __device__ __forceinline__ void cp_async_wait_all()
     asm volatile("cp.async.wait_group 0;\n" ::: "memory");
 }
 
+// sinc(phi_p - phi_q) = sin(phi_p - phi_q) / (phi_p - phi_q), the
+// reference's smearing factor (define_cross_correlate.h:16-32), from the
+// per-station sin and cos: sin(a - b) = sin a cos b - cos a sin b. Where the
+// difference d is small the identity loses relative accuracy (its absolute
+// error is a few ulp of 1), so below |d| = tau the Taylor series of sinc is
+// summed instead, 1 - d^2/6 + d^4/120 - d^6/5040 + d^8/362880, whose
+// truncation error d^10/39916800 is below 1e-20 (FP64, tau = 0.05) and
+// 3e-11 (FP32, tau = 0.5); above tau the identity's relative error is below
+// ~1e-14 (FP64) and ~1e-6 (FP32).
 template <typename T>
-__device__ __forceinline__ T sinc(T x)
+__device__ __forceinline__ T sinc_diff(T pa, T sa, T ca, T pb, T sb, T cb)
 {
-    return x == (T) 0 ? (T) 1 : sin(x) / x;
+    const T d = pa - pb;
+    const T tau = sizeof(T) == 8 ? (T) 0.05 : (T) 0.5;
+    if (fabs(d) < tau)
+    {
+        const T d2 = d * d;
+        return (T) 1 + d2 * ((T) (-1.0 / 6) + d2 * ((T) (1.0 / 120) +
+                d2 * ((T) (-1.0 / 5040) + d2 * (T) (1.0 / 362880))));
+    }
+    return (sa * cb - ca * sb) / d;
 }
 
 // Maps a linear block index to (bp, bq) with bp >= bq.
@@ -124,30 +180,36 @@ __device__ __forceinline__ void tri_block(int k, int& bp, int& bq)
 // Issues the cp.async copies of one chunk (sources [s0, min(s0 + kChunk,
 // src_end))) of both station blocks and of the per-source arrays; entries
 // outside the stations or sources are zero-filled without a global read.
+// jsrc: the Jones (or, fused, E) array of this item; NULL for identity E.
 template <typename T, bool MATRIX, bool GAUSS, bool LMN>
 __device__ __forceinline__ void issue_chunk(Smem<T, MATRIX>& sm,
-        const XcorrParams<T>& prm, int p0, int q0, int s0, int src_end)
+        const XcorrParams<T>& prm, const T* jsrc, const ItemCtx& it_ctx,
+        int s0)
 {
     typedef Staging<T, MATRIX> G;
     const int tid = threadIdx.x, N = prm.num_st;
-    const unsigned char* jb = reinterpret_cast<const unsigned char*>(prm.jones);
-    // Thread mapping: 8 stations x PIECES x 4 station groups x sources x
-    // blocks, so a warp reads whole elements of 8 stations and writes 8
-    // consecutive station slots per piece.
-    constexpr int total = 2 * G::PIECES * kChunk * kTile;
-    for (int it = tid; it < total; it += kThreads)
+    const int src_end = it_ctx.src_end;
+    if (jsrc)
     {
-        const int a = it & 7;
-        const int pc = (it >> 3) % G::PIECES;
-        const int rest = (it >> 3) / G::PIECES;
-        const int stl = a + 8 * (rest & 3);
-        const int rest2 = rest >> 2;
-        const int sl = rest2 % kChunk, blk = rest2 / kChunk;
-        const int st = (blk ? q0 : p0) + stl, s = s0 + sl;
-        const bool in = st < N && s < src_end;
-        const unsigned char* src = in ? jb + ((size_t) st * prm.num_src + s) *
-                G::ELEM + pc * G::COPY : jb;
-        cp_async(sm.raw[blk][pc][sl][stl], src, in, G::COPY);
+        const unsigned char* jb = reinterpret_cast<const unsigned char*>(jsrc);
+        // Thread mapping: 8 stations x PIECES x 4 station groups x sources
+        // x blocks, so a warp reads whole elements of 8 stations and writes
+        // 8 consecutive station slots per piece.
+        constexpr int total = 2 * G::PIECES * kChunk * kTile;
+        for (int it = tid; it < total; it += kThreads)
+        {
+            const int a = it & 7;
+            const int pc = (it >> 3) % G::PIECES;
+            const int rest = (it >> 3) / G::PIECES;
+            const int stl = a + 8 * (rest & 3);
+            const int rest2 = rest >> 2;
+            const int sl = rest2 % kChunk, blk = rest2 / kChunk;
+            const int st = (blk ? it_ctx.q0 : it_ctx.p0) + stl, s = s0 + sl;
+            const bool in = st < N && s < src_end;
+            const unsigned char* src = in ? jb + ((size_t) st *
+                    prm.src_stride + s) * G::ELEM + pc * G::COPY : jb;
+            cp_async(sm.raw[blk][pc][sl][stl], src, in, G::COPY);
+        }
     }
     // Per-source arrays: only those this variant reads.
     const T* arrs[kNumSrcArr] = {prm.I, prm.Q, prm.U, prm.V, prm.l, prm.m,
@@ -166,47 +228,98 @@ __device__ __forceinline__ void issue_chunk(Smem<T, MATRIX>& sm,
     cp_async_commit();
 }
 
-template <typename T, bool MATRIX, bool GAUSS, bool BW, bool TS, bool CASA>
+template <typename T, bool MATRIX, bool GAUSS, bool BW, bool TS, bool CASA,
+        bool FUSED>
 __global__ void __launch_bounds__(kThreads,
-        (sizeof(T) == 8 && !(MATRIX && (GAUSS || BW || TS))) ? 2 : 1)
+        (sizeof(T) == 8 && !FUSED && (MATRIX ? !(GAUSS || BW || TS) : !GAUSS))
+        ? 2 : 1)
 xcorr_direct_kernel(const XcorrParams<T> prm)
 {
     typedef typename vec2<T>::type T2;
     typedef Smem<T, MATRIX> S;
     typedef Staging<T, MATRIX> G;
     constexpr int NC = S::NCOMP;
+    constexpr bool LMN = BW || TS || FUSED;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     S& sm = *reinterpret_cast<S*>(smem_raw);
-
-    int bp, bq;
-    tri_block(blockIdx.x, bp, bq);
-    const int p0 = bp * kTile, q0 = bq * kTile;
     const int tid = threadIdx.x, tx = tid & 15, ty = tid >> 4;
     const int N = prm.num_st;
-    const int src_begin = blockIdx.y * prm.slice_len;
-    const int src_end = min(prm.num_src, src_begin + prm.slice_len);
+    const long long nbl = (long long) N * (N - 1) / 2;
+    const int num_items = prm.num_times * prm.num_channels * prm.tiles *
+            prm.slices;
 
-    // First chunk in flight while the per-baseline terms are set up.
-    if (src_begin < src_end)
-        issue_chunk<T, MATRIX, GAUSS, BW || TS>(sm, prm, p0, q0, src_begin,
-                src_end);
+    for (int item = blockIdx.x; item < num_items; item += gridDim.x)
+    {
+    // ---- item: (dump, channel, station tile, source slice)
+    ItemCtx ctx;
+    int r = item;
+    const int slice = r % prm.slices; r /= prm.slices;
+    int tile;
+    if (prm.tile_major)
+    {
+        // Consecutive items share a station tile (its E rows stay in L2).
+        const int tc = r % (prm.num_times * prm.num_channels);
+        tile = r / (prm.num_times * prm.num_channels);
+        ctx.c = tc % prm.num_channels;
+        ctx.t = tc / prm.num_channels;
+    }
+    else
+    {
+        tile = r % prm.tiles;
+        r /= prm.tiles;
+        ctx.c = r % prm.num_channels;
+        ctx.t = r / prm.num_channels;
+    }
+    {
+        int bp, bq;
+        tri_block(tile, bp, bq);
+        ctx.p0 = bp * kTile;
+        ctx.q0 = bq * kTile;
+    }
+    ctx.src_begin = slice * prm.slice_len;
+    ctx.src_end = min(prm.num_src, ctx.src_begin + prm.slice_len);
+    ctx.inv_wavelength = prm.inv_wavelength_c ?
+            prm.inv_wavelength_c[ctx.c] : prm.inv_wavelength;
+    ctx.ts_scale = prm.ts_base * ctx.inv_wavelength;
+    ctx.s_ha = ctx.c_ha = 0;
+    if (TS) sincos(prm.gha0_t ? prm.gha0_t[ctx.t] : prm.gha0, &ctx.s_ha,
+            &ctx.c_ha);
+    const T* su = prm.st_u + ctx.t * prm.uvw_time_stride;
+    const T* sv = prm.st_v + ctx.t * prm.uvw_time_stride;
+    const T* sw = prm.st_w + ctx.t * prm.uvw_time_stride;
+    const T* jsrc = !FUSED ? prm.jones : (prm.jones ?
+            prm.jones + ctx.t * prm.e_time_stride : nullptr);
+    const T wavenumber = (T) (2.0 * kPi * ctx.inv_wavelength);
+    const double uv_scale = prm.uv_filter_in_metres ? ctx.inv_wavelength :
+            1.0;
+    const T uv_lo = (T) (prm.uv_min * uv_scale);
+    const T uv_hi = (T) (prm.uv_max * uv_scale);
 
-    if (BW || TS)
+    __syncthreads();  // the previous item is done with shared memory
+    // First chunk in flight while the per-station and baseline terms are
+    // set up.
+    if (ctx.src_begin < ctx.src_end)
+        issue_chunk<T, MATRIX, GAUSS, LMN>(sm, prm, jsrc, ctx,
+                ctx.src_begin);
+
+    if (LMN)
     {
         for (int it = tid; it < 2 * kTile; it += kThreads)
         {
             const int blk = it / kTile, stl = it % kTile;
-            const int st = (blk ? q0 : p0) + stl;
-            double* t = sm.st_terms[blk][stl];
-            t[0] = t[1] = t[2] = t[3] = t[4] = 0;
+            const int st = (blk ? ctx.q0 : ctx.p0) + stl;
+            T* u = sm.st_uvw[blk][stl];
+            double* xy = sm.st_xy[blk][stl];
+            u[0] = u[1] = u[2] = 0;
+            xy[0] = xy[1] = 0;
             if (st < N)
             {
-                t[0] = prm.st_u[st]; t[1] = prm.st_v[st]; t[2] = prm.st_w[st];
+                u[0] = su[st]; u[1] = sv[st]; u[2] = sw[st];
                 if (TS)
                 {
                     const double x = prm.st_x[st], y = prm.st_y[st];
-                    t[3] = x * prm.c_ha - y * prm.s_ha;
-                    t[4] = x * prm.s_ha + y * prm.c_ha;
+                    xy[0] = x * ctx.c_ha - y * ctx.s_ha;
+                    xy[1] = x * ctx.s_ha + y * ctx.c_ha;
                 }
             }
         }
@@ -222,15 +335,15 @@ xcorr_direct_kernel(const XcorrParams<T> prm)
         {
             // Baseline terms as the reference forms them
             // (oskar/correlate/define_correlate_utils.h:5-13).
-            const int p = p0 + ty + 16 * i, q = q0 + tx + 16 * j;
+            const int p = ctx.p0 + ty + 16 * i, q = ctx.q0 + tx + 16 * j;
             bool ok = (p < N) && (q < p);
             T uu = 0, vv = 0;
             if (ok)
             {
-                uu = (prm.st_u[p] - prm.st_u[q]) * (T) prm.inv_wavelength;
-                vv = (prm.st_v[p] - prm.st_v[q]) * (T) prm.inv_wavelength;
+                uu = (su[p] - su[q]) * (T) ctx.inv_wavelength;
+                vv = (sv[p] - sv[q]) * (T) ctx.inv_wavelength;
                 const T len = sqrt(uu * uu + vv * vv);
-                ok = !(len < (T) prm.uv_min || len > (T) prm.uv_max);
+                ok = !(len < uv_lo || len > uv_hi);
             }
             valid[i][j] = ok;
             uu2[i][j] = uu * uu;
@@ -252,9 +365,9 @@ xcorr_direct_kernel(const XcorrParams<T> prm)
                 part[i][j][k] = 0;
             }
 
-    for (int s0 = src_begin; s0 < src_end; s0 += kChunk)
+    for (int s0 = ctx.src_begin; s0 < ctx.src_end; s0 += kChunk)
     {
-        const int ns = min(kChunk, src_end - s0);
+        const int ns = min(kChunk, ctx.src_end - s0);
         cp_async_wait_all();
         __syncthreads();  // chunk landed; previous chunk's factors consumed
 
@@ -265,21 +378,54 @@ xcorr_direct_kernel(const XcorrParams<T> prm)
             const int rem = it - blk * (kTile * kChunk);
             const int stl = rem % kTile, sl = rem / kTile;
             T v[2 * NC];
-#pragma unroll
-            for (int pc = 0; pc < G::PIECES; ++pc)
+            if (jsrc)
             {
-                constexpr int PER = G::COPY / (int) sizeof(T);
-                if constexpr (G::COPY == 16)
+#pragma unroll
+                for (int pc = 0; pc < G::PIECES; ++pc)
                 {
-                    const uint4 u = *reinterpret_cast<const uint4*>(
-                            sm.raw[blk][pc][sl][stl]);
-                    memcpy(&v[pc * PER], &u, 16);
+                    constexpr int PER = G::COPY / (int) sizeof(T);
+                    if constexpr (G::COPY == 16)
+                    {
+                        const uint4 u = *reinterpret_cast<const uint4*>(
+                                sm.raw[blk][pc][sl][stl]);
+                        memcpy(&v[pc * PER], &u, 16);
+                    }
+                    else
+                    {
+                        const uint2 u = *reinterpret_cast<const uint2*>(
+                                sm.raw[blk][pc][sl][stl]);
+                        memcpy(&v[pc * PER], &u, 8);
+                    }
                 }
-                else
+            }
+            else
+            {
+                // Identity E (fused mode without a station beam).
+#pragma unroll
+                for (int k = 0; k < 2 * NC; ++k) v[k] = (T) 0;
+                v[0] = (T) 1;
+                if (MATRIX) v[6] = (T) 1;
+            }
+            if (FUSED)
+            {
+                // J = K E with the reference's K
+                // (oskar/interferometer/define_evaluate_jones_K.h:53-70).
+                const T* u = sm.st_uvw[blk][stl];
+                const T l = sm.raw_src[kL][sl], m = sm.raw_src[kM][sl];
+                const T n1 = sm.raw_src[kN][sl] - (T) 1;
+                const T flux = sm.raw_src[kI][sl];
+                const T phase = (u[0] * l + u[1] * m + u[2] * n1) * wavenumber;
+                T ks, kc;
+                sincos(phase, &ks, &kc);
+                if (!(sl < ns && flux > (T) prm.filter_min &&
+                        flux <= (T) prm.filter_max))
+                    ks = kc = (T) 0;
+#pragma unroll
+                for (int k = 0; k < NC; ++k)
                 {
-                    const uint2 u = *reinterpret_cast<const uint2*>(
-                            sm.raw[blk][pc][sl][stl]);
-                    memcpy(&v[pc * PER], &u, 8);
+                    const T re = v[2 * k], im = v[2 * k + 1];
+                    v[2 * k] = kc * re - ks * im;
+                    v[2 * k + 1] = kc * im + ks * re;
                 }
             }
             // Left factor (J B, or I J) lives in the row block unless CASA.
@@ -324,33 +470,53 @@ xcorr_direct_kernel(const XcorrParams<T> prm)
             {
                 // Per-station source phases (phi_p - phi_q is the
                 // reference's baseline argument), in FP64.
-                const double* t = sm.st_terms[blk][stl];
+                const T* u = sm.st_uvw[blk][stl];
+                const double* xy = sm.st_xy[blk][stl];
                 const double l = sm.raw_src[kL][sl], m = sm.raw_src[kM][sl];
                 const double n1 = (double) sm.raw_src[kN][sl] - 1.0;
                 T ph = 0, ps = 0;
                 if (BW)
-                    ph = (T) ((t[0] * l + t[1] * m + t[2] * n1) *
-                            prm.bw_scale);
+                    ph = (T) (((double) u[0] * l + (double) u[1] * m +
+                            (double) u[2] * n1) * prm.bw_scale);
                 if (TS)
-                    ps = (T) ((t[3] * l + t[4] * (prm.s_dec * m -
-                            prm.c_dec * n1)) * prm.ts_scale);
-                if (blk) { sm.ph_col[sl][stl] = ph; sm.ps_col[sl][stl] = ps; }
-                else { sm.ph_row[sl][stl] = ph; sm.ps_row[sl][stl] = ps; }
+                    ps = (T) ((xy[0] * l + xy[1] * (prm.s_dec * m -
+                            prm.c_dec * n1)) * ctx.ts_scale);
+                if (BW)
+                {
+                    T sn, cs;
+                    sincos(ph, &sn, &cs);
+                    sm.ph[blk][0][sl][stl] = ph;
+                    sm.ph[blk][1][sl][stl] = sn;
+                    sm.ph[blk][2][sl][stl] = cs;
+                }
+                if (TS)
+                {
+                    T sn, cs;
+                    sincos(ps, &sn, &cs);
+                    sm.ps[blk][0][sl][stl] = ps;
+                    sm.ps[blk][1][sl][stl] = sn;
+                    sm.ps[blk][2][sl][stl] = cs;
+                }
             }
         }
+        int g = 0;
         if (GAUSS && tid < kChunk)
         {
             sm.ga[tid] = sm.raw_src[kGa][tid];
             sm.gb[tid] = sm.raw_src[kGb][tid];
             sm.gc[tid] = sm.raw_src[kGc][tid];
+            g = sm.ga[tid] != (T) 0 || sm.gb[tid] != (T) 0 ||
+                    sm.gc[tid] != (T) 0;
         }
-        __syncthreads();  // factors ready; the raw buffer is free
+        // Factors ready; the raw buffer is free. A chunk of point sources
+        // (a = b = c = 0, exp(-0) = 1 exactly) skips the Gaussian factor.
+        const bool gauss_chunk = GAUSS && __syncthreads_or(g);
+        if (!GAUSS) __syncthreads();
 
         // ---- next chunk's copies overlap this chunk's arithmetic
-        if (s0 + kChunk < src_end)
-            issue_chunk<T, MATRIX, GAUSS, BW || TS>(sm, prm, p0, q0,
-                    s0 + kChunk, src_end);
-
+        if (s0 + kChunk < ctx.src_end)
+            issue_chunk<T, MATRIX, GAUSS, LMN>(sm, prm, jsrc, ctx,
+                    s0 + kChunk);
         // ---- accumulate
         for (int sl = 0; sl < ns; ++sl)
         {
@@ -370,15 +536,20 @@ xcorr_direct_kernel(const XcorrParams<T> prm)
                 for (int j = 0; j < 2; ++j)
                 {
                     T f = (T) 1;
-                    if (GAUSS)
+                    if (GAUSS && gauss_chunk)
                         f = exp(-(sm.ga[sl] * uu2[i][j] + sm.gb[sl] * uuvv[i][j]
                                 + sm.gc[sl] * vv2[i][j]));
+                    const int pr = ty + 16 * i, qc = tx + 16 * j;
                     if (BW)
-                        f *= sinc<T>(sm.ph_row[sl][ty + 16 * i] -
-                                sm.ph_col[sl][tx + 16 * j]);
+                        f *= sinc_diff<T>(sm.ph[0][0][sl][pr],
+                                sm.ph[0][1][sl][pr], sm.ph[0][2][sl][pr],
+                                sm.ph[1][0][sl][qc], sm.ph[1][1][sl][qc],
+                                sm.ph[1][2][sl][qc]);
                     if (TS)
-                        f *= sinc<T>(sm.ps_row[sl][ty + 16 * i] -
-                                sm.ps_col[sl][tx + 16 * j]);
+                        f *= sinc_diff<T>(sm.ps[0][0][sl][pr],
+                                sm.ps[0][1][sl][pr], sm.ps[0][2][sl][pr],
+                                sm.ps[1][0][sl][qc], sm.ps[1][1][sl][qc],
+                                sm.ps[1][2][sl][qc]);
                     smear[i][j] = f;
                 }
             if constexpr (!(GAUSS || BW || TS))
@@ -471,22 +642,22 @@ xcorr_direct_kernel(const XcorrParams<T> prm)
         }
     }
 
+
     // ---- write out: each baseline is owned by exactly one thread
 #pragma unroll
     for (int i = 0; i < 2; ++i)
 #pragma unroll
         for (int j = 0; j < 2; ++j)
         {
-            const int p = p0 + ty + 16 * i, q = q0 + tx + 16 * j;
+            const int p = ctx.p0 + ty + 16 * i, q = ctx.q0 + tx + 16 * j;
             if (p >= N || q >= p) continue;
             const long long bl = baseline_index(N, p, q);
             if (prm.partial)
             {
                 // Every baseline of the slice is written (zero where the uv
                 // filter drops it), so the reduction reads no stale data.
-                const long long nbl = (long long) N * (N - 1) / 2;
                 double* out = prm.partial + (size_t) (2 * NC) *
-                        (size_t) (blockIdx.y * nbl + bl);
+                        (size_t) (slice * nbl + bl);
 #pragma unroll
                 for (int k = 0; k < 2 * NC; ++k)
                     out[k] = !valid[i][j] ? 0.0 : (sizeof(T) == 4) ?
@@ -494,8 +665,11 @@ xcorr_direct_kernel(const XcorrParams<T> prm)
                 continue;
             }
             if (!valid[i][j]) continue;
-            T* out = prm.vis + (size_t) (2 * NC) *
-                    (size_t) (bl + prm.offset_out);
+            // Block layout [dump][channel][baseline] (the reference's
+            // oskar_VisBlock order, private_vis_block.h:33-57).
+            T* out = prm.vis + (size_t) (2 * NC) * (size_t) (((long long)
+                    ctx.t * prm.num_channels + ctx.c) * nbl + bl +
+                    prm.offset_out);
 #pragma unroll
             for (int k = 0; k < 2 * NC; ++k)
             {
@@ -504,6 +678,7 @@ xcorr_direct_kernel(const XcorrParams<T> prm)
                 out[k] = (T) ((double) out[k] + v);
             }
         }
+    }  // items
 }
 
 // Adds the slices' partial sums to the visibilities, in slice order.
@@ -530,27 +705,50 @@ int num_sms()
     return n;
 }
 
-template <typename T, bool MATRIX, bool GAUSS, bool BW, bool TS>
-void launch_casa(bool casa, const XcorrParams<T>& p, dim3 grid,
-        cudaStream_t stream)
+template <typename T, bool MATRIX, bool GAUSS, bool BW, bool TS, bool CASA,
+        bool FUSED>
+void launch_one(const XcorrParams<T>& p, int grid, cudaStream_t stream)
 {
     const size_t smem = sizeof(Smem<T, MATRIX>);
-    if (casa)
+    auto k = xcorr_direct_kernel<T, MATRIX, GAUSS, BW, TS, CASA, FUSED>;
+    cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize,
+            (int) smem);
+    k<<<grid, kThreads, smem, stream>>>(p);
+}
+
+// Selects the kernel variant. FUSED (K formed in the staging) exists for
+// the matrix form only.
+template <typename T, bool MATRIX, bool FUSED>
+void launch_variant(bool casa, bool gauss, bool bw, bool ts,
+        const XcorrParams<T>& p, int grid, cudaStream_t s)
+{
+#define OSKB_L(G, B, S)                                                      \
+    (casa ? launch_one<T, MATRIX, G, B, S, true, FUSED>(p, grid, s)          \
+          : launch_one<T, MATRIX, G, B, S, false, FUSED>(p, grid, s))
+    if (gauss)
     {
-        auto k = xcorr_direct_kernel<T, MATRIX, GAUSS, BW, TS, true>;
-        cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                (int) smem);
-        k<<<grid, kThreads, smem, stream>>>(p);
+        if (!bw && !ts) OSKB_L(true, false, false);
+        else if (bw && !ts) OSKB_L(true, true, false);
+        else if (!bw && ts) OSKB_L(true, false, true);
+        else OSKB_L(true, true, true);
     }
     else
     {
-        auto k = xcorr_direct_kernel<T, MATRIX, GAUSS, BW, TS, false>;
-        cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                (int) smem);
-        k<<<grid, kThreads, smem, stream>>>(p);
+        if (!bw && !ts) OSKB_L(false, false, false);
+        else if (bw && !ts) OSKB_L(false, true, false);
+        else if (!bw && ts) OSKB_L(false, false, true);
+        else OSKB_L(false, true, true);
     }
+#undef OSKB_L
 }
 
+int tiles_for(int num_st)
+{
+    const int nb = (num_st + kTile - 1) / kTile;
+    return nb * (nb + 1) / 2;
+}
+
+// One call: one dump, one channel, sources split into slices.
 template <typename T, bool MATRIX>
 int xcorr_dispatch(bool casa, bool gauss, XcorrParams<T> p,
         bool bw, bool ts, cudaStream_t stream)
@@ -561,8 +759,7 @@ int xcorr_dispatch(bool casa, bool gauss, XcorrParams<T> p,
     // or an offset into one by whole elements, is).
     if ((uintptr_t) p.jones % Staging<T, MATRIX>::COPY != 0)
         return OSKB_ERR_INVALID_ARGUMENT;
-    const int nb = (p.num_st + kTile - 1) / kTile;
-    const int tiles = nb * (nb + 1) / 2;
+    const int tiles = tiles_for(p.num_st);
     // Split the sources into slices so that about four waves of two CTAs
     // per SM are in flight, each slice at least 64 sources long.
     const int max_slices = (p.num_src + 8 * kChunk - 1) / (8 * kChunk);
@@ -574,7 +771,11 @@ int xcorr_dispatch(bool casa, bool gauss, XcorrParams<T> p,
     slices = (p.num_src + slice_len - 1) / slice_len;
     constexpr int ncomp2 = MATRIX ? 8 : 2;
     const long long nbl = (long long) p.num_st * (p.num_st - 1) / 2;
+    p.num_times = p.num_channels = 1;
+    p.tiles = tiles;
+    p.slices = slices;
     p.slice_len = slice_len;
+    p.tile_major = 0;
     p.partial = nullptr;
     if (slices > 1)
     {
@@ -584,27 +785,12 @@ int xcorr_dispatch(bool casa, bool gauss, XcorrParams<T> p,
         {
             cudaGetLastError();  // no room for partials: one slice
             p.partial = nullptr;
-            slices = 1;
+            p.slices = slices = 1;
             p.slice_len = p.num_src;
         }
     }
-    const dim3 grid(tiles, slices);
-#define OSKB_SEL(G, B, S) launch_casa<T, MATRIX, G, B, S>(casa, p, grid, stream)
-    if (gauss)
-    {
-        if (!bw && !ts) OSKB_SEL(true, false, false);
-        else if (bw && !ts) OSKB_SEL(true, true, false);
-        else if (!bw && ts) OSKB_SEL(true, false, true);
-        else OSKB_SEL(true, true, true);
-    }
-    else
-    {
-        if (!bw && !ts) OSKB_SEL(false, false, false);
-        else if (bw && !ts) OSKB_SEL(false, true, false);
-        else if (!bw && ts) OSKB_SEL(false, false, true);
-        else OSKB_SEL(false, true, true);
-    }
-#undef OSKB_SEL
+    launch_variant<T, MATRIX, false>(casa, gauss, bw, ts, p,
+            tiles * slices, stream);
     int err = check_launch("xcorr_direct");
     if (p.partial)
     {
@@ -621,6 +807,137 @@ int xcorr_dispatch(bool casa, bool gauss, XcorrParams<T> p,
     return err;
 }
 
+// ---------------------------------------------------------------- blocks
+// Schedule of one block launch: grid size (CTAs; 0 = one per item) and
+// item order. Picked per block shape by timing the candidates on a sample
+// of the block (the first dump, the first 4,096 sources) into scratch
+// visibilities; cached for the process. Every schedule sums each
+// (dump, channel, baseline) over the sources in the same order, so the
+// choice changes speed only, never a bit of the result.
+struct BlockSchedule
+{
+    int ctas_per_sm;  // grid = ctas_per_sm x SMs; 0: one CTA per item
+    int tile_major;
+};
+
+constexpr int kNumCandidates = 8;
+const BlockSchedule kCandidates[kNumCandidates] = {
+    {2, 0}, {2, 1}, {4, 0}, {4, 1}, {8, 0}, {8, 1}, {0, 0}, {0, 1}};
+
+struct TuneEntry
+{
+    long long key[10];
+    BlockSchedule sched;
+    float ms[kNumCandidates];
+};
+
+TuneEntry g_tune[64];
+int g_num_tune = 0;
+std::mutex g_tune_mutex;
+
+int grid_for(const BlockSchedule& s, int items)
+{
+    if (s.ctas_per_sm <= 0) return items;
+    return max(1, min(items, s.ctas_per_sm * num_sms()));
+}
+
+template <typename T>
+BlockSchedule block_schedule(bool casa, bool gauss, bool bw, bool ts,
+        const XcorrParams<T>& p, cudaStream_t stream)
+{
+    const BlockSchedule dflt = {2, 1};
+    if (const char* e = getenv("OSKB_BLOCK_SCHEDULE"))
+    {
+        BlockSchedule s = dflt;
+        if (sscanf(e, "%d,%d", &s.ctas_per_sm, &s.tile_major) == 2) return s;
+    }
+    std::lock_guard<std::mutex> lock(g_tune_mutex);
+    int dev = 0;
+    cudaGetDevice(&dev);
+    (void) dev;
+    const long long key[10] = {(long long) sizeof(T), casa, gauss, bw, ts,
+            p.num_st, p.num_src, p.num_times, p.num_channels,
+            p.jones != nullptr};
+    for (int i = 0; i < g_num_tune; ++i)
+        if (!memcmp(g_tune[i].key, key, sizeof(key))) return g_tune[i].sched;
+    const char* at = getenv("OSKB_AUTOTUNE");
+    cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+    cudaStreamIsCapturing(stream, &cap);
+    if ((at && at[0] == '0') || cap != cudaStreamCaptureStatusNone ||
+            g_num_tune >= 64)
+        return dflt;
+
+    // Sample: the first dump, all channels, up to 4,096 sources.
+    XcorrParams<T> q = p;
+    q.num_times = 1;
+    q.num_src = min(p.num_src, 4096);
+    q.slice_len = q.num_src;
+    const long long nbl = (long long) p.num_st * (p.num_st - 1) / 2;
+    const size_t vis_bytes = (size_t) q.num_channels * nbl * 8 * sizeof(T);
+    TuneEntry ent;
+    memcpy(ent.key, key, sizeof(key));
+    ent.sched = dflt;
+    if (cudaMallocAsync((void**) &q.vis, vis_bytes, stream) != cudaSuccess)
+    {
+        cudaGetLastError();
+        return dflt;
+    }
+    cudaMemsetAsync(q.vis, 0, vis_bytes, stream);
+    q.offset_out = 0;
+    const int items = q.num_times * q.num_channels * q.tiles;
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    float best = 3e38f;
+    for (int i = 0; i < kNumCandidates; ++i)
+    {
+        q.tile_major = kCandidates[i].tile_major;
+        const int grid = grid_for(kCandidates[i], items);
+        launch_variant<T, true, true>(casa, gauss, bw, ts, q, grid, stream);
+        cudaEventRecord(e0, stream);
+        launch_variant<T, true, true>(casa, gauss, bw, ts, q, grid, stream);
+        cudaEventRecord(e1, stream);
+        float ms = 3e38f;
+        if (cudaEventSynchronize(e1) == cudaSuccess)
+            cudaEventElapsedTime(&ms, e0, e1);
+        ent.ms[i] = ms;
+        if (ms < best)
+        {
+            best = ms;
+            ent.sched = kCandidates[i];
+        }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    cudaFreeAsync(q.vis, stream);
+    cudaGetLastError();
+    g_tune[g_num_tune++] = ent;
+    return ent.sched;
+}
+
+// A whole block: every (dump, channel) in one persistent launch, K fused.
+template <typename T>
+int block_dispatch(bool casa, bool gauss, bool bw, bool ts, XcorrParams<T> p,
+        cudaStream_t stream)
+{
+    if (p.num_st < 2 || p.num_src <= 0 || p.num_times <= 0 ||
+            p.num_channels <= 0)
+        return 0;
+    if (p.jones && (uintptr_t) p.jones % Staging<T, true>::COPY != 0)
+        return OSKB_ERR_INVALID_ARGUMENT;
+    p.tiles = tiles_for(p.num_st);
+    p.slices = 1;
+    p.slice_len = p.num_src;
+    p.partial = nullptr;
+    const long long items = (long long) p.num_times * p.num_channels *
+            p.tiles;
+    if (items > 0x7fffffffLL) return OSKB_ERR_INVALID_ARGUMENT;
+    const BlockSchedule s = block_schedule<T>(casa, gauss, bw, ts, p, stream);
+    p.tile_major = s.tile_major;
+    launch_variant<T, true, true>(casa, gauss, bw, ts, p,
+            grid_for(s, (int) items), stream);
+    return check_launch("correlate_block_direct");
+}
 template <typename T>
 XcorrParams<T> make_params(int num_sources, int num_stations, int offset_out,
         const T* jones, const T* I, const T* Q, const T* U, const T* V,
@@ -630,15 +947,16 @@ XcorrParams<T> make_params(int num_sources, int num_stations, int offset_out,
         T time_int_sec, T gha0, T dec0, T* vis)
 {
     XcorrParams<T> p;
+    memset(&p, 0, sizeof(p));
     p.num_src = num_sources; p.num_st = num_stations; p.offset_out = offset_out;
+    p.src_stride = num_sources;
     p.jones = jones; p.I = I; p.Q = Q; p.U = U; p.V = V;
     p.l = l; p.m = m; p.n = n; p.a = a; p.b = b; p.c = c;
     p.st_u = su; p.st_v = sv; p.st_w = sw; p.st_x = sx; p.st_y = sy;
     p.uv_min = uv_min; p.uv_max = uv_max; p.inv_wavelength = inv_wavelength;
     p.bw_scale = kPi * (double) frac_bandwidth * (double) inv_wavelength;
-    p.ts_scale = kPi * (double) inv_wavelength * kOmegaEarth *
-            (double) time_int_sec;
-    p.s_ha = sin((double) gha0); p.c_ha = cos((double) gha0);
+    p.ts_base = kPi * kOmegaEarth * (double) time_int_sec;
+    p.gha0 = gha0;
     p.s_dec = sin((double) dec0); p.c_dec = cos((double) dec0);
     p.vis = vis;
     return p;
@@ -741,3 +1059,113 @@ extern "C" int oskb_cross_correlate_scalar_f(int casa, int gaussian,
             su, sv, sw, sx, sy, uv_min, uv_max, inv_wavelength,
             frac_bandwidth, time_int_sec, gha0, dec0, vis, stream);
 }
+
+namespace oskb {
+namespace {
+
+template <typename T>
+int correlate_block_direct(int casa, int num_sources, int num_stations,
+        int num_times, int num_channels, const T* E, int E_per_dump,
+        const T* I, const T* Q, const T* U, const T* V, const T* l,
+        const T* m, const T* n, const T* a, const T* b, const T* c,
+        const T* station_uvw, const T* station_x, const T* station_y,
+        const double* inv_wavelength, double channel_bandwidth_hz,
+        double time_average_sec, const double* gha0_rad, double dec0_rad,
+        double uv_min, double uv_max, int uv_filter_units,
+        double source_filter_min, double source_filter_max, T* vis,
+        void* stream)
+{
+    if (num_sources < 0 || num_stations < 0 || num_times < 0 ||
+            num_channels < 0)
+        return OSKB_ERR_INVALID_ARGUMENT;
+    if (num_sources == 0 || num_stations < 2 || num_times == 0 ||
+            num_channels == 0)
+        return 0;
+    const bool bw = channel_bandwidth_hz != 0.0;
+    const bool ts = time_average_sec != 0.0;
+    const bool gauss = a && b && c;
+    if (!I || !Q || !U || !V || !l || !m || !n || !station_uvw ||
+            !inv_wavelength || !vis || (ts && (!station_x || !station_y ||
+            !gha0_rad)))
+        return OSKB_ERR_INVALID_ARGUMENT;
+    XcorrParams<T> p;
+    memset(&p, 0, sizeof(p));
+    p.num_src = num_sources;
+    p.src_stride = num_sources;
+    p.num_st = num_stations;
+    p.jones = E;
+    p.e_time_stride = E_per_dump ? 8LL * num_stations * num_sources : 0;
+    p.I = I; p.Q = Q; p.U = U; p.V = V; p.l = l; p.m = m; p.n = n;
+    p.a = a; p.b = b; p.c = c;
+    p.st_u = station_uvw;
+    p.st_v = station_uvw + num_stations;
+    p.st_w = station_uvw + 2 * (size_t) num_stations;
+    p.uvw_time_stride = 3LL * num_stations;
+    p.st_x = station_x; p.st_y = station_y;
+    p.uv_min = uv_min; p.uv_max = uv_max;
+    p.uv_filter_in_metres = uv_filter_units == 0;
+    p.inv_wavelength_c = inv_wavelength;
+    p.bw_scale = kPi * channel_bandwidth_hz / 299792458.0;
+    p.ts_base = kPi * kOmegaEarth * time_average_sec;
+    p.gha0_t = gha0_rad;
+    p.s_dec = sin(dec0_rad); p.c_dec = cos(dec0_rad);
+    p.vis = vis;
+    p.num_times = num_times;
+    p.num_channels = num_channels;
+    p.filter_min = source_filter_min;
+    p.filter_max = source_filter_max;
+    return block_dispatch<T>(casa != 0, gauss, bw, ts, p, as_stream(stream));
+}
+
+}  // namespace
+}  // namespace oskb
+
+extern "C" {
+
+#define OSKB_BLOCK_ENTRY(T, S)                                               \
+int oskb_correlate_block_direct_##S(int casa, int num_sources,               \
+        int num_stations, int num_times, int num_channels, const T* E,       \
+        int E_per_dump, const T* I, const T* Q, const T* U, const T* V,      \
+        const T* l, const T* m, const T* n, const T* a, const T* b,          \
+        const T* c, const T* station_uvw, const T* station_x,                \
+        const T* station_y, const double* inv_wavelength,                    \
+        double channel_bandwidth_hz, double time_average_sec,                \
+        const double* gha0_rad, double dec0_rad, double uv_min,              \
+        double uv_max, int uv_filter_units, double source_filter_min,        \
+        double source_filter_max, T* vis, void* stream)                      \
+{                                                                            \
+    return oskb::correlate_block_direct<T>(casa, num_sources, num_stations,  \
+            num_times, num_channels, E, E_per_dump, I, Q, U, V, l, m, n, a,  \
+            b, c, station_uvw, station_x, station_y, inv_wavelength,         \
+            channel_bandwidth_hz, time_average_sec, gha0_rad, dec0_rad,      \
+            uv_min, uv_max, uv_filter_units, source_filter_min,              \
+            source_filter_max, vis, stream);                                 \
+}
+
+OSKB_BLOCK_ENTRY(double, d)
+OSKB_BLOCK_ENTRY(float, f)
+#undef OSKB_BLOCK_ENTRY
+
+int oskb_block_tune_report(char* buf, int len)
+{
+    std::lock_guard<std::mutex> lock(oskb::g_tune_mutex);
+    int used = 0;
+    if (len > 0) buf[0] = 0;
+    for (int i = 0; i < oskb::g_num_tune && used < len; ++i)
+    {
+        const oskb::TuneEntry& e = oskb::g_tune[i];
+        used += snprintf(buf + used, len - used,
+                "fp%lld casa=%lld gauss=%lld bw=%lld ts=%lld stations=%lld "
+                "sources=%lld dumps=%lld channels=%lld beam=%lld -> "
+                "ctas_per_sm=%d tile_major=%d; sample ms:",
+                8 * e.key[0], e.key[1], e.key[2], e.key[3], e.key[4],
+                e.key[5], e.key[6], e.key[7], e.key[8], e.key[9],
+                e.sched.ctas_per_sm, e.sched.tile_major);
+        for (int k = 0; k < oskb::kNumCandidates && used < len; ++k)
+            used += snprintf(buf + used, len - used, " %.3f", e.ms[k]);
+        if (used < len) used += snprintf(buf + used, len - used, "\n");
+    }
+    return used < len ? used : len;
+}
+
+}  // extern "C"
