@@ -337,6 +337,41 @@ OSKB_API int oskb_correlate_block_direct_f(int casa, int num_sources,
  * number of characters written. */
 OSKB_API int oskb_block_tune_report(char* buf, int len);
 
+/* Block plan: the host driver of oskb_correlate_block_direct for one block
+ * shape. It keeps the sky, station offsets and beam on the device, and
+ * page-locked host buffers for the per-block inputs (station uvw
+ * [dump][3][station] and Greenwich hour angle [dump] of the phase centre)
+ * and the output (visibilities [dump][channel][baseline][2x2]). Execute
+ * runs: upload uvw and hour angles, clear, correlate, download, on the
+ * plan's own stream; the first execute runs eagerly and captures the
+ * sequence as a CUDA graph, later executes replay the graph. Arrays passed
+ * to the setters are host arrays of the plan's precision (precision_bytes
+ * 8: double, 4: float); frequency_hz is a host array [num_channels]. The
+ * other arguments mean what they mean for oskb_correlate_block_direct. */
+typedef struct oskb_BlockPlan oskb_BlockPlan;
+OSKB_API oskb_BlockPlan* oskb_block_plan_create(int precision_bytes,
+        int casa, int num_stations, int num_sources, int num_times,
+        int num_channels, int gaussian, int with_beam, int beam_per_dump,
+        const double* frequency_hz, double channel_bandwidth_hz,
+        double time_average_sec, double dec0_rad, double uv_min,
+        double uv_max, int uv_filter_units, double source_filter_min,
+        double source_filter_max, int* status);
+OSKB_API int oskb_block_plan_set_sky(oskb_BlockPlan* plan, const void* I,
+        const void* Q, const void* U, const void* V, const void* l,
+        const void* m, const void* n, const void* a, const void* b,
+        const void* c);
+OSKB_API int oskb_block_plan_set_stations(oskb_BlockPlan* plan,
+        const void* ecef_x, const void* ecef_y);
+OSKB_API int oskb_block_plan_set_beam(oskb_BlockPlan* plan, const void* E);
+OSKB_API void* oskb_block_plan_host_uvw(oskb_BlockPlan* plan);
+OSKB_API double* oskb_block_plan_host_gha0(oskb_BlockPlan* plan);
+OSKB_API const void* oskb_block_plan_host_vis(oskb_BlockPlan* plan);
+OSKB_API int oskb_block_plan_execute(oskb_BlockPlan* plan);
+OSKB_API int oskb_block_plan_synchronize(oskb_BlockPlan* plan);
+/* Graph replays so far, or -1 while the plan runs without a graph. */
+OSKB_API int oskb_block_plan_graph_launches(const oskb_BlockPlan* plan);
+OSKB_API void oskb_block_plan_free(oskb_BlockPlan* plan);
+
 /* Fused block: for every (time t, channel c) of a block,
  *   vis[t][c] += sum_s (K_p E_p C)(s) (K_q E_q C)(s)^H
  * with K_p(s) = exp(2 pi i (u_p l + v_p m + w_p (n - 1)) / lambda_c) formed

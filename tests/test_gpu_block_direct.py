@@ -131,3 +131,52 @@ def test_block_empty_and_invalid():
     assert st == -3
     torch.cuda.synchronize()
     assert not vis.cpu().numpy().any()
+
+
+def _host_view(ptr, count, real):
+    import ctypes
+    ctype = ctypes.c_double if real == np.float64 else ctypes.c_float
+    buf = (ctype * count).from_address(ptr)
+    return np.frombuffer(buf, dtype=real)
+
+
+@pytest.mark.parametrize("real", [np.float64, np.float32])
+def test_block_plan_graph_replay(real):
+    """The block plan: first block eager and captured, second block a graph
+    replay with new uvw and hour angles; both equal the oracle."""
+    import ctypes
+    lib = ob.load()
+    c = BlockCase(real=real, num_st=50, chunks=(90, 30), gaussian=(1, 0))
+    st = ctypes.c_int(0)
+    plan = lib.oskb_block_plan_create(
+        8 if real == np.float64 else 4, c.casa, c.num_st, c.num_src,
+        c.num_times, c.num_channels, 1, 1, 0,
+        c.freqs.ctypes.data, c.bw, c.tavg, c.dec0, c.uv_min_m, c.uv_max_m,
+        0, c.filter_min, c.filter_max, ctypes.addressof(st))
+    assert st.value == 0 and plan
+    try:
+        assert ob.call("oskb_block_plan_set_sky", plan, c.I, c.Q, c.U, c.V,
+                       c.l, c.m, c.n, c.a, c.b, c.c) == 0
+        assert ob.call("oskb_block_plan_set_stations", plan, c.st_x,
+                       c.st_y) == 0
+        assert ob.call("oskb_block_plan_set_beam", plan, c.E) == 0
+        nvis = c.num_times * c.num_channels * c.nbl * 8
+        uvw = _host_view(lib.oskb_block_plan_host_uvw(plan), c.uvw.size,
+                         real)
+        gha0 = _host_view(lib.oskb_block_plan_host_gha0(plan), c.num_times,
+                          np.float64)
+        vis = _host_view(lib.oskb_block_plan_host_vis(plan), nvis, real)
+        tol = TOL[real]
+        for block in range(3):
+            if block:
+                rng = np.random.default_rng(100 + block)
+                c.uvw = rng.uniform(-3e3, 3e3, c.uvw.shape).astype(real)
+                c.gha0 = rng.uniform(-1, 1, c.num_times)
+            uvw[:] = c.uvw.ravel()
+            gha0[:] = c.gha0
+            assert ob.call("oskb_block_plan_execute", plan) == 0
+            assert ob.call("oskb_block_plan_synchronize", plan) == 0
+            assert rel(vis.copy(), c.oracle_vis()) <= tol, block
+        assert lib.oskb_block_plan_graph_launches(plan) == 2
+    finally:
+        lib.oskb_block_plan_free(plan)
