@@ -246,6 +246,81 @@ OSKB_API int oskb_station_beam_aa_f(int num_stations, int num_elements,
         const float* y, const float* z, int directions_per_station,
         float* beam, void* stream);
 
+/* ------------------------------------------------------------------------
+ * Learned station-beam surrogate.
+ * ------------------------------------------------------------------------
+ * A multilayer perceptron with sine activations (dims[0] -> ... ->
+ * dims[num_layers]; sin(omega0 z) after every layer but the last), trained
+ * and evaluated by this library's own FP32 kernels. Parameters are one
+ * device array: per layer W [out][in] then b [out].
+ *   oskb_mlp_forward keeps the activations of the batch for
+ *   oskb_mlp_backward, which overwrites the gradients (same layout as the
+ *   parameters) with d loss / d parameter for the output gradient dy;
+ *   oskb_mlp_mse: loss += mean (y - t)^2, dy = 2 (y - t) / count (dy may
+ *   alias y; loss may be NULL);
+ *   oskb_mlp_train: steps of Adam (beta 0.9, 0.999) on random minibatches
+ *   of the (x, target) samples with a cosine-decayed learning rate; the
+ *   loss of every report_every-th step (and of the last) goes to
+ *   loss_history (host, (steps - 1) / report_every + 2 entries);
+ *   oskb_mlp_infer: outputs for count inputs, in chunks.
+ * x, y, target, dy: device, row-major [sample][feature]. */
+typedef struct oskb_Mlp oskb_Mlp;
+OSKB_API oskb_Mlp* oskb_mlp_create(int num_layers, const int* dims,
+        float omega0, unsigned long long seed, int* status);
+OSKB_API void oskb_mlp_free(oskb_Mlp* net);
+OSKB_API int oskb_mlp_num_params(const oskb_Mlp* net);
+OSKB_API float* oskb_mlp_params(oskb_Mlp* net);
+OSKB_API float* oskb_mlp_grads(oskb_Mlp* net);
+/* which: 0 parameters, 1 gradients; host arrays of oskb_mlp_num_params. */
+OSKB_API int oskb_mlp_copy_to_host(const oskb_Mlp* net, int which,
+        float* host);
+OSKB_API int oskb_mlp_set_params(oskb_Mlp* net, const float* host);
+OSKB_API int oskb_mlp_forward(oskb_Mlp* net, int batch, const float* x,
+        float* y, void* stream);
+OSKB_API int oskb_mlp_backward(oskb_Mlp* net, int batch, const float* dy,
+        void* stream);
+OSKB_API int oskb_mlp_mse(long long count, const float* y,
+        const float* target, float* dy, float* loss, void* stream);
+OSKB_API int oskb_mlp_adam_step(oskb_Mlp* net, float lr, float beta1,
+        float beta2, float eps, void* stream);
+OSKB_API int oskb_mlp_train(oskb_Mlp* net, int num_samples, const float* x,
+        const float* target, int batch, int steps, float lr_max,
+        unsigned long long seed, int report_every, float* loss_history,
+        void* stream);
+OSKB_API int oskb_mlp_infer(oskb_Mlp* net, long long count, const float* x,
+        float* y, int chunk, void* stream);
+
+/* Exact normalised array factor A(kappa) = (1/N) sum_e exp(i (x_e kx +
+ * y_e ky)) of a planar layout, for training samples (FP64 phases, FP32
+ * output [count][2]). kappa in rad/m, layout in metres; device arrays. */
+OSKB_API int oskb_array_factor_samples_f(int num_elements,
+        const float* layout_x, const float* layout_y, long long count,
+        const float* kappa_x, const float* kappa_y, float* af, void* stream);
+
+/* Station beam (Jones E, FP32) of stations built from num_types planar
+ * dipole layouts, station st being layout station_type_host[st] rotated by
+ * rotation_rad[st] (elements and dipole orientation: Euler angles x = y =
+ * rotation), phased to beam_enu[st] and normalised there (array and final
+ * normalisation on, element normalisation optional) - the beam that
+ * oskb_station_beam_aa_f gives for those stations. The array factor comes
+ * from networks[type] (trained on A(kappa) with inputs kappa / kappa_scale)
+ * wherever |kappa| >= kappa_main and from the exact sum inside the main
+ * lobe. Every audit_stride-th network value is checked against the exact
+ * sum; if the largest difference exceeds audit_bound (A is 1 at the
+ * pointing), every network value is replaced by the exact sum. audit (host,
+ * 5 values): largest audited |A_net - A|, rms audited error, number
+ * audited, 1 if the fallback ran, number of network evaluations.
+ * station_type_host and networks are host arrays; the rest device. */
+OSKB_API int oskb_station_beam_surrogate_f(int num_stations, int num_types,
+        int num_elements, const int* station_type_host,
+        const double* rotation_rad, const float* layout_x,
+        const float* layout_y, oskb_Mlp* const* networks,
+        double dipole_length_m, int normalise_element, double frequency_hz,
+        const double* beam_enu, int num_directions, const float* x,
+        const float* y, const float* z, double kappa_main,
+        double kappa_scale, int audit_stride, double audit_bound,
+        float* beam, double* audit, void* stream);
+
 /* Parallactic-angle rotation R [station][source] (real 2x2 rotation) for
  * stations at latitude lat_rad[station] and local sidereal time
  * lst_rad[station] = gast + longitude. Replaces the kernel behind

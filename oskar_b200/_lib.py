@@ -25,6 +25,7 @@ _SCALARS = {
     "size_t": ctypes.c_size_t,
     "long long": ctypes.c_longlong,
     "unsigned int": ctypes.c_uint,
+    "unsigned long long": ctypes.c_ulonglong,
 }
 
 
