@@ -568,6 +568,140 @@ def run_profile_case(args):
     return 0
 
 
+def run_c5(args):
+    """Learned station-beam surrogate against the exact station beam, one
+    step = the Jones E of every station for every source at one (dump,
+    channel): 512 stations built from 3 planar layouts of 256 dipoles in a
+    38 m disc, each station a layout rotated by a random angle, 200,000
+    sources of which ~90% lie outside the first null of the main lobe,
+    100 MHz. Prints one JSON line: exact and surrogate throughput
+    (station-source beam values per second), the audit record, the beam
+    error over the whole step and the visibility error it causes (FP64
+    correlation of 32 stations with either beam)."""
+    import torch
+    import oskar_b200 as ob
+    from oskar_b200.surrogate import BeamSurrogate, first_null_kappa
+    torch.cuda.set_device(0)
+    dev = lambda a: torch.from_numpy(np.ascontiguousarray(a)).cuda()
+    rng = np.random.default_rng(5)
+    ns, ne, nsrc, freq = 512, 256, 200_000, 100e6
+    layouts = []
+    for _ in range(3):
+        r = 19.0 * np.sqrt(rng.uniform(0, 1, ne))
+        t = rng.uniform(0, 2 * math.pi, ne)
+        layouts.append((r * np.cos(t), r * np.sin(t)))
+    types = np.arange(ns) % 3
+    rot = rng.uniform(0, 2 * math.pi, ns)
+    # pointing: 60 deg elevation; sources: 10% within the main lobe
+    b = np.array([0.0, math.cos(math.radians(60)), math.sin(math.radians(60))])
+    null = first_null_kappa(38.0) / (2 * math.pi * freq / 299792458.0)
+    n_in = nsrc // 10
+    rr = null * np.sqrt(rng.uniform(0, 1, n_in))
+    th = rng.uniform(0, 2 * math.pi, n_in)
+    xi, yi = b[0] + rr * np.cos(th), b[1] + rr * np.sin(th)
+    az = rng.uniform(0, 2 * math.pi, nsrc - n_in)
+    el = np.arcsin(rng.uniform(0, 1, nsrc - n_in))
+    xo, yo = np.cos(el) * np.sin(az), np.cos(el) * np.cos(az)
+    x = np.concatenate([xi, xo]); y = np.concatenate([yi, yo])
+    z = np.sqrt(np.maximum(0.0, 1 - x * x - y * y))
+    outside = (np.hypot(x - b[0], y - b[1]) > null).mean()
+    dirs = [torch.from_numpy(a.astype(np.float32)).cuda() for a in (x, y, z)]
+    dirs_st = [d.unsqueeze(0).expand(ns, nsrc).contiguous() for d in dirs]
+    bb = dev(np.tile(b, (ns, 1)))
+    d_rot = dev(rot)
+    # exact beam: rotated layouts per station
+    ex = np.zeros((ns, ne), np.float32); ey = np.zeros_like(ex)
+    for s in range(ns):
+        lx, ly = layouts[types[s]]
+        co, si = math.cos(rot[s]), math.sin(rot[s])
+        ex[s] = co * lx - si * ly
+        ey[s] = si * lx + co * ly
+    d_ex, d_ey, d_ez = dev(ex), dev(ey), dev(np.zeros_like(ex))
+    E_exact = torch.empty((ns, nsrc, 8), dtype=torch.float32, device="cuda")
+
+    def exact():
+        ob.call("oskb_station_beam_aa_f", ns, ne, d_ex, d_ey, d_ez, None,
+                None, None, None, d_rot, d_rot, 1.5, 0, 1, 1, 0, 0, freq, bb,
+                bb, nsrc, *dirs, 0, E_exact, ob.stream_ptr())
+
+    sur = BeamSurrogate(layouts, freq, seed=5)
+    t0 = time.perf_counter()
+    train = sur.train(num_samples=1_000_000, steps=args.c5_steps,
+                      batch=4096, lr=1e-4, report_every=1000, seed=5)
+    train_s = time.perf_counter() - t0
+    E_sur = torch.empty_like(E_exact)
+    audit = {}
+
+    def surrogate():
+        _, a = sur.beam(types, d_rot, bb, *dirs_st, freq, audit_stride=100,
+                        audit_bound=args.c5_bound, out=E_sur)
+        audit.update(a)
+
+    def timed(fn, reps):
+        fn()
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(reps):
+            fn()
+        e1.record()
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / reps
+
+    ms_exact = timed(exact, 3)
+    ms_sur = timed(surrogate, 3)
+    d = (E_sur - E_exact).float()
+    beam_max = d.abs().max().item()
+    beam_rms = d.pow(2).mean().sqrt().item()
+    # visibility error: 32 stations, FP64 direct correlation of either beam
+    nv = 32
+    rng2 = np.random.default_rng(6)
+    I = 10 ** rng2.uniform(-2, 1, nsrc)
+    zeros = np.zeros(nsrc)
+    lmn = [dev(x), dev(y), dev(z)]
+    uvw = [dev(rng2.uniform(-2e3, 2e3, nv)) for _ in range(3)]
+    vis = []
+    for E in (E_exact, E_sur):
+        J = E[:nv].double().contiguous()
+        v = torch.zeros((nv * (nv - 1) // 2, 8), dtype=torch.float64,
+                        device="cuda")
+        ob.call("oskb_cross_correlate_d", 0, 0, nsrc, nv, 0, J, dev(I),
+                dev(zeros), dev(zeros), dev(zeros), *[a.double() for a in
+                lmn], None, None, None, *uvw, None, None, 0.0, 3e38,
+                freq / 299792458.0, 0.0, 0.0, 0.0, 0.0, v, ob.stream_ptr())
+        vis.append(v)
+    torch.cuda.synchronize()
+    vd = vis[1] - vis[0]
+    vis_l2 = (vd.norm() / vis[0].norm()).item()
+    vis_max = (vd.abs().max() / vis[0].abs().max()).item()
+    n_vals = ns * nsrc
+    print(json.dumps({
+        "workload": "c5: learned station-beam surrogate vs exact station "
+                    "beam, 512 stations (3 layouts x 256 dipoles, rotated), "
+                    "200,000 sources (%.0f%% outside the first null), "
+                    "100 MHz, FP32 beams" % (100 * outside),
+        "unit": "G station-source beam values/s",
+        "exact": {"ms": ms_exact, "value": n_vals / ms_exact / 1e6,
+                  "kernel": "oskb station_beam_kernel<float> (256-element "
+                            "array factor per value)"},
+        "surrogate": {"ms": ms_sur, "value": n_vals / ms_sur / 1e6,
+                      "audit": audit, "audit_bound": args.c5_bound},
+        "speedup": ms_exact / ms_sur,
+        "beam_error_vs_exact": {"max": beam_max, "rms": beam_rms,
+                                "note": "beam normalised to 1 at the "
+                                        "pointing"},
+        "vis_error_vs_exact": {"l2": vis_l2, "max_over_max": vis_max,
+                               "sample": "32 stations x 200,000 sources, "
+                                         "FP64 correlation"},
+        "training": {"seconds_all_types": train_s,
+                     "steps": args.c5_steps, "samples_per_type": 1_000_000,
+                     "final_loss": [float(t["loss"][-1]) for t in train]},
+    }))
+    sur.free()
+    return 0
+
+
 def cpu_baseline(cfg):
     cores = cpu_cores()
     if ref_lib() is None:
@@ -591,12 +725,18 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--path", default="tc", choices=["tc", "direct"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--workload", default="c3", choices=["c3", "c5"],
+                    help="c5: the learned station-beam surrogate measurement")
+    ap.add_argument("--c5-steps", type=int, default=20000)
+    ap.add_argument("--c5-bound", type=float, default=1e-4)
     ap.add_argument("--profile-case", default=None,
                     choices=["tc_small", "direct_small", "beam_small"],
                     help="run one small kernel case for an ncu capture")
     args = ap.parse_args()
     if args.profile_case:
         return run_profile_case(args)
+    if args.workload == "c5":
+        return run_c5(args)
     os.environ.setdefault("OMP_NUM_THREADS", str(cpu_cores()))
     if args.impl == "reference":
         return run_reference(args)

@@ -552,9 +552,13 @@ gemm_kernel(const GemmParams prm)
             const int prob = task / ntile;
             int rb, cb;
             tile_of(task - prob * ntile, rb, cb);
-            double acc[64];
+            // FP64 sums of Re V (accR) and Im V (accI) of the 16 baselines
+            // (station columns) this thread owns: thread (row c) keeps the
+            // polarisation j = c of its row's pair.
+            const int c = row & 1;
+            double accR[16], accI[16];
 #pragma unroll
-            for (int j = 0; j < 64; ++j) acc[j] = 0.0;
+            for (int j = 0; j < 16; ++j) accR[j] = accI[j] = 0.0;
             for (int ch = 0; ch < nchunk; ++ch)
             {
                 if (!ptx::mbar_wait(&ctl->tfull[buf], (tpar >> buf) & 1,
@@ -572,10 +576,30 @@ gemm_kernel(const GemmParams prm)
                     ptx::tmem_ld16(ta + j0, vm);
                     ptx::tmem_ld16(ta + kAccCols + j0, vc);
                     ptx::tmem_ld_wait();
+                    float v[16];
 #pragma unroll
                     for (int j = 0; j < 16; ++j)
-                        acc[j0 + j] += (double) (__uint_as_float(vm[j]) +
-                                                 __uint_as_float(vc[j]));
+                        v[j] = __uint_as_float(vm[j]) + __uint_as_float(vc[j]);
+                    // Re V = G00 + G11, Im V = G10 - G01 (rows c = 0, 1 of
+                    // the pair are lanes l, l ^ 1; columns 2j + c' of the
+                    // group of four): combined in FP32 before the FP64
+                    // accumulation, which halves the FP32 -> FP64
+                    // conversions of the drain.
+#pragma unroll
+                    for (int qq = 0; qq < 4; ++qq)
+                    {
+                        const int jb = 4 * qq;
+                        const float s0 = c ? v[jb + 0] : v[jb + 2];
+                        const float s1 = c ? v[jb + 1] : v[jb + 3];
+                        const float r0 = __shfl_xor_sync(0xffffffffu, s0, 1);
+                        const float r1 = __shfl_xor_sync(0xffffffffu, s1, 1);
+                        const float g00 = c ? r0 : v[jb + 0];
+                        const float g01 = c ? r1 : v[jb + 1];
+                        const float g10 = c ? v[jb + 2] : r0;
+                        const float g11 = c ? v[jb + 3] : r1;
+                        accR[j0 / 4 + qq] += (double) (g00 + g11);
+                        accI[j0 / 4 + qq] += (double) (g10 - g01);
+                    }
                 }
                 ptx::tc_fence_before();
                 __syncwarp();
@@ -590,7 +614,7 @@ gemm_kernel(const GemmParams prm)
             const float S = scale_from_bits(
                     prm.maxabs_bits[prm.maxabs_stride * g]);
             const double inv_s2 = 1.0 / ((double) S * (double) S);
-            const int c = row & 1, i = (row >> 1) & 1;
+            const int i = (row >> 1) & 1;
             const int p = rb * kStPerBlock + (row >> 2);
             const int N = prm.num_st;
             const double* su = prm.st_u + prm.uv_stride * t;
@@ -602,15 +626,6 @@ gemm_kernel(const GemmParams prm)
 #pragma unroll
             for (int ql = 0; ql < 16; ++ql)
             {
-                const int jb = 4 * ql;
-                const double s0 = c ? acc[jb + 0] : acc[jb + 2];
-                const double s1 = c ? acc[jb + 1] : acc[jb + 3];
-                const double r0 = __shfl_xor_sync(0xffffffffu, s0, 1);
-                const double r1 = __shfl_xor_sync(0xffffffffu, s1, 1);
-                const double g00 = c ? r0 : acc[jb + 0];
-                const double g01 = c ? r1 : acc[jb + 1];
-                const double g10 = c ? acc[jb + 2] : r0;
-                const double g11 = c ? acc[jb + 3] : r1;
                 const int q = cb * kStPerBlock + 16 * h + ql;
                 if (p < q && q < N)
                 {
@@ -619,8 +634,8 @@ gemm_kernel(const GemmParams prm)
                     const double len = sqrt(uu * uu + vv * vv);
                     if (!(len < prm.uv_min || len > prm.uv_max))
                     {
-                        const double re = (g00 + g11) * inv_s2;
-                        const double im = (g10 - g01) * inv_s2;
+                        const double re = accR[ql] * inv_s2;
+                        const double im = accI[ql] * inv_s2;
                         // this thread holds V_pq[i][j] with j = c; the
                         // reference stores J_q B J_p^H (p < q) unless CASA
                         const int ro = prm.casa ? i : c;
