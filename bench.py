@@ -500,7 +500,10 @@ def run_profile_case(args):
       direct_small  the FP64 direct cross-correlation: 512 stations x 2,000
                     sources, 1 channel;
       beam_small    the fused station beam: 32 stations x 256 dipoles x
-                    12,001 directions (FP64)."""
+                    12,001 directions (FP64);
+      block_small   the block correlator with Jones K fused: 256 stations x
+                    10,000 sources (30% Gaussian) x 2 channels, bandwidth and
+                    time smearing, FP64, seed 4."""
     import torch
     import oskar_b200 as ob
     from oskar_b200 import workloads
@@ -544,6 +547,33 @@ def run_profile_case(args):
                         Q, U, V, l, m, n, None, None, None, u, v, w, z, z,
                         0.0, 3e38, f / 299792458.0, 0.0, 0.0, 0.0, 0.0,
                         vis[0], stream)
+    elif case == "block_small":
+        rng = np.random.default_rng(4)
+        nst, nsrc, nch = 256, 10_000, 2
+        r = np.sqrt(rng.uniform(0, 1, nsrc)) * math.sin(math.radians(4))
+        th = rng.uniform(0, 2 * math.pi, nsrc)
+        l, m = r * np.cos(th), r * np.sin(th)
+        n = np.sqrt(1 - l * l - m * m)
+        I = rng.uniform(0.2, 3.0, nsrc)
+        Q, U, V = (I * rng.uniform(-0.1, 0.1, nsrc) for _ in range(3))
+        ga, gb, gc = (rng.uniform(1e-8, 5e-7, nsrc) for _ in range(3))
+        for g in (ga, gb, gc):
+            g[3000:] = 0  # 30% Gaussian, the rest point sources
+        E = rng.normal(0, 0.1, (nst, nsrc, 8))
+        E[..., 0] += 1
+        E[..., 6] += 1
+        uvw = rng.uniform(-3e3, 3e3, (1, 3, nst))
+        sx, sy = (rng.uniform(-3e3, 3e3, nst) for _ in range(2))
+        inv_wl = (100e6 + 1e6 * np.arange(nch)) / 299792458.0
+        nbl = nst * (nst - 1) // 2
+        vis = torch.zeros(nch * nbl * 8, dtype=torch.float64, device="cuda")
+        args_ = [0, nsrc, nst, 1, nch, dev(E), 0] + [dev(a) for a in (
+            I, Q, U, V, l, m, n, ga, gb, gc, uvw, sx, sy, inv_wl)] + [
+            1e5, 10.0, dev(np.array([0.3])), -0.45, 0.0, 3e38, 0, 0.0, 3e38,
+            vis, stream]
+        os.environ["OSKB_BLOCK_SCHEDULE"] = "2,0"
+        for _ in range(2):
+            ob.call("oskb_correlate_block_direct_d", *args_)
     elif case == "beam_small":
         st, ne, nd = 32, 256, 12_001
         rng = np.random.default_rng(2)
@@ -730,7 +760,8 @@ def main():
     ap.add_argument("--c5-steps", type=int, default=20000)
     ap.add_argument("--c5-bound", type=float, default=1e-4)
     ap.add_argument("--profile-case", default=None,
-                    choices=["tc_small", "direct_small", "beam_small"],
+                    choices=["tc_small", "direct_small", "beam_small",
+                             "block_small"],
                     help="run one small kernel case for an ncu capture")
     args = ap.parse_args()
     if args.profile_case:

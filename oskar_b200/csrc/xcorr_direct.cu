@@ -656,8 +656,10 @@ xcorr_direct_kernel(const XcorrParams<T> prm)
             {
                 // Every baseline of the slice is written (zero where the uv
                 // filter drops it), so the reduction reads no stale data.
-                double* out = prm.partial + (size_t) (2 * NC) *
-                        (size_t) (slice * nbl + bl);
+                double* out = prm.partial + (size_t) (2 * NC) * (size_t) (
+                        ((long long) slice * prm.num_times * prm.num_channels
+                        + (long long) ctx.t * prm.num_channels + ctx.c) *
+                        nbl + bl);
 #pragma unroll
                 for (int k = 0; k < 2 * NC; ++k)
                     out[k] = !valid[i][j] ? 0.0 : (sizeof(T) == 4) ?
@@ -929,14 +931,58 @@ int block_dispatch(bool casa, bool gauss, bool bw, bool ts, XcorrParams<T> p,
     p.slices = 1;
     p.slice_len = p.num_src;
     p.partial = nullptr;
-    const long long items = (long long) p.num_times * p.num_channels *
+    const long long tc_items = (long long) p.num_times * p.num_channels *
             p.tiles;
-    if (items > 0x7fffffffLL) return OSKB_ERR_INVALID_ARGUMENT;
+    if (tc_items > 0x7fffffffLL) return OSKB_ERR_INVALID_ARGUMENT;
     const BlockSchedule s = block_schedule<T>(casa, gauss, bw, ts, p, stream);
     p.tile_major = s.tile_major;
+    // Too few (dump, channel, tile) items to fill the GPU: split the
+    // sources too (at least 64 per slice), the slices' sums reduced into
+    // vis in slice order afterwards.
+    const long long want = 4LL * num_sms();
+    if (tc_items < want)
+    {
+        const int max_slices = (p.num_src + 8 * kChunk - 1) / (8 * kChunk);
+        int slices = (int) min((long long) max_slices,
+                (want + tc_items - 1) / tc_items);
+        if (slices > 1)
+        {
+            int len = (p.num_src + slices - 1) / slices;
+            len = (len + kChunk - 1) / kChunk * kChunk;
+            slices = (p.num_src + len - 1) / len;
+            const size_t bytes = (size_t) slices * tc_items / p.tiles *
+                    ((size_t) p.num_st * (p.num_st - 1) / 2) * 8 *
+                    sizeof(double);
+            if (slices > 1 && cudaMallocAsync((void**) &p.partial, bytes,
+                    stream) == cudaSuccess)
+            {
+                p.slices = slices;
+                p.slice_len = len;
+            }
+            else
+            {
+                cudaGetLastError();
+                p.partial = nullptr;
+            }
+        }
+    }
+    const long long items = tc_items * p.slices;
     launch_variant<T, true, true>(casa, gauss, bw, ts, p,
             grid_for(s, (int) items), stream);
-    return check_launch("correlate_block_direct");
+    int err = check_launch("correlate_block_direct");
+    if (p.partial)
+    {
+        const long long n = (long long) p.num_times * p.num_channels *
+                ((long long) p.num_st * (p.num_st - 1) / 2) * 8;
+        if (!err)
+        {
+            reduce_partials_kernel<T><<<(unsigned) ((n + 255) / 256), 256, 0,
+                    stream>>>(p.partial, p.slices, n, 0, p.vis);
+            err = check_launch("correlate_block_direct reduce");
+        }
+        cudaFreeAsync(p.partial, stream);
+    }
+    return err;
 }
 template <typename T>
 XcorrParams<T> make_params(int num_sources, int num_stations, int offset_out,
