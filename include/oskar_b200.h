@@ -247,6 +247,66 @@ OSKB_API int oskb_station_beam_aa_f(int num_stations, int num_elements,
         float* beam, void* stream);
 
 /* ------------------------------------------------------------------------
+ * Sky and baseline preparation on the device.
+ * ------------------------------------------------------------------------
+ * (lon, lat) -> direction cosines (l, m[, n]) about (lon0, lat0); n may be
+ * NULL. Replaces the kernel behind oskar_convert_lon_lat_to_relative_
+ * directions (convert/define_convert_lon_lat_to_relative_directions.h). */
+OSKB_API int oskb_convert_lon_lat_to_relative_directions_d(int num,
+        const double* lon, const double* lat, double lon0_rad,
+        double lat0_rad, double* l, double* m, double* n, void* stream);
+OSKB_API int oskb_convert_lon_lat_to_relative_directions_f(int num,
+        const float* lon, const float* lat, double lon0_rad,
+        double lat0_rad, float* l, float* m, float* n, void* stream);
+/* Apparent (RA, Dec) -> ENU direction cosines [station][source] for every
+ * station in one launch (station st at local sidereal time lst_rad[st] and
+ * latitude lat_rad[st], device double arrays). Replaces the per-station
+ * kernel of oskar_convert_apparent_ra_dec_to_enu_directions
+ * (convert/define_convert_apparent_ra_dec_to_enu_directions.h). */
+OSKB_API int oskb_convert_ra_dec_to_enu_directions_d(int num_sources,
+        const double* ra, const double* dec, int num_stations,
+        const double* lst_rad, const double* lat_rad, double* x, double* y,
+        double* z, void* stream);
+OSKB_API int oskb_convert_ra_dec_to_enu_directions_f(int num_sources,
+        const float* ra, const float* dec, int num_stations,
+        const double* lst_rad, const double* lat_rad, float* x, float* y,
+        float* z, void* stream);
+/* mask[s] |= source s (direction cosines l, m, n about the phase centre) is
+ * above the horizon of any of the stations (hour angle of the phase centre
+ * ha0_rad_host[st], latitude lat_rad_host[st]: host arrays). The mask step
+ * of oskar_sky_horizon_clip (sky/src/oskar_sky_horizon_clip.c:63-79,
+ * sky/define_update_horizon_mask.h). */
+OSKB_API int oskb_sky_horizon_mask_d(int num_sources, const double* l,
+        const double* m, const double* n, int num_stations,
+        const double* ha0_rad_host, const double* lat_rad_host,
+        double dec0_rad, int* mask, void* stream);
+OSKB_API int oskb_sky_horizon_mask_f(int num_sources, const float* l,
+        const float* m, const float* n, int num_stations,
+        const double* ha0_rad_host, const double* lat_rad_host,
+        double dec0_rad, int* mask, void* stream);
+/* Order-preserving compaction of num_columns sky columns by mask (the copy
+ * step of oskar_sky_horizon_clip, sky/src/oskar_sky_horizon_clip.c:80-95):
+ * columns_in / columns_out are host arrays of device pointers; *num_out
+ * (host) receives the number kept. Synchronises the stream. */
+OSKB_API int oskb_sky_compact_d(int num, const int* mask, int num_columns,
+        const double* const* columns_in, double* const* columns_out,
+        int* num_out, void* stream);
+OSKB_API int oskb_sky_compact_f(int num, const int* mask, int num_columns,
+        const float* const* columns_in, float* const* columns_out,
+        int* num_out, void* stream);
+/* Station (u, v, w) -> baseline (uu, vv, ww) = station q - station p for
+ * p < q in the reference's baseline order, negated in the CASA convention
+ * (convert/src/oskar_convert_station_uvw_to_baseline_uvw.c:13-29). */
+OSKB_API int oskb_convert_station_uvw_to_baseline_uvw_d(int use_casa,
+        int num_stations, int offset_in, const double* u, const double* v,
+        const double* w, int offset_out, double* uu, double* vv, double* ww,
+        void* stream);
+OSKB_API int oskb_convert_station_uvw_to_baseline_uvw_f(int use_casa,
+        int num_stations, int offset_in, const float* u, const float* v,
+        const float* w, int offset_out, float* uu, float* vv, float* ww,
+        void* stream);
+
+/* ------------------------------------------------------------------------
  * Learned station-beam surrogate.
  * ------------------------------------------------------------------------
  * A multilayer perceptron with sine activations (dims[0] -> ... ->

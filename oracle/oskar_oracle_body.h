@@ -730,3 +730,71 @@ void ORC_FN(orc_station_beam_aa)(int num_el, const REAL* x, const REAL* y,
     free(X); free(Y); free(Z); free(theta); free(phi1); free(phi2);
     free(signal); free(out); free(w); free(types);
 }
+
+/* Relative direction cosines of (lon, lat) about (lon0, lat0)
+ * (convert/define_convert_lon_lat_to_relative_directions.h:3-19); n is
+ * skipped when NULL. */
+void ORC_FN(orc_lon_lat_to_relative_directions)(int num, const REAL* lon,
+        const REAL* lat, REAL lon0, REAL cos_lat0, REAL sin_lat0, REAL* l,
+        REAL* m, REAL* n)
+{
+    int i;
+    for (i = 0; i < num; ++i)
+    {
+        const REAL dl = lon[i] - lon0;
+        const REAL sl = ORC_SIN(dl), cl = ORC_COS(dl);
+        const REAL sb = ORC_SIN(lat[i]), cb = ORC_COS(lat[i]);
+        l[i] = cb * sl;
+        m[i] = cos_lat0 * sb - sin_lat0 * cb * cl;
+        if (n) n[i] = sin_lat0 * sb + cos_lat0 * cb * cl;
+    }
+}
+
+/* Apparent (RA, Dec) to the ENU direction cosines of a station at local
+ * sidereal time lst and latitude lat
+ * (convert/define_convert_apparent_ra_dec_to_enu_directions.h:3-30). */
+void ORC_FN(orc_ra_dec_to_enu_directions)(int num, const REAL* ra,
+        const REAL* dec, REAL lst, REAL sin_lat, REAL cos_lat, int offset_out,
+        REAL* x, REAL* y, REAL* z)
+{
+    int i;
+    for (i = 0; i < num; ++i)
+    {
+        const REAL ha = lst - ra[i];
+        const REAL sh = ORC_SIN(ha), ch = ORC_COS(ha);
+        const REAL sd = ORC_SIN(dec[i]), cd = ORC_COS(dec[i]);
+        x[i + offset_out] = -cd * sh;
+        y[i + offset_out] = cos_lat * sd - sin_lat * cd * ch;
+        z[i + offset_out] = sin_lat * sd + cos_lat * cd * ch;
+    }
+}
+
+/* mask |= (l l_mul + m m_mul + n n_mul > 0): the source is above a
+ * station's horizon (sky/define_update_horizon_mask.h:3-12). */
+void ORC_FN(orc_update_horizon_mask)(int num, const REAL* l, const REAL* m,
+        const REAL* n, REAL l_mul, REAL m_mul, REAL n_mul, int* mask)
+{
+    int i;
+    for (i = 0; i < num; ++i)
+        mask[i] |= ((l[i] * l_mul + m[i] * m_mul + n[i] * n_mul) > 0);
+}
+
+/* Baseline (uu, vv, ww) = station 2 - station 1 for every pair s1 < s2,
+ * negated in the CASA convention
+ * (convert/define_convert_station_uvw_to_baseline_uvw.h:3-20). */
+void ORC_FN(orc_station_uvw_to_baseline_uvw)(int casa, int num,
+        int offset_in, const REAL* u, const REAL* v, const REAL* w,
+        int offset_out, REAL* uu, REAL* vv, REAL* ww)
+{
+    const REAL f = casa ? -1 : 1;
+    int s1, s2;
+    for (s1 = 0; s1 < num; ++s1)
+        for (s2 = s1 + 1; s2 < num; ++s2)
+        {
+            const int b = s1 * (num - 1) - (s1 - 1) * s1 / 2 + s2 - s1 - 1 +
+                    offset_out;
+            uu[b] = f * (u[s2 + offset_in] - u[s1 + offset_in]);
+            vv[b] = f * (v[s2 + offset_in] - v[s1 + offset_in]);
+            ww[b] = f * (w[s2 + offset_in] - w[s1 + offset_in]);
+        }
+}

@@ -24,6 +24,9 @@
 #include "telescope/station/define_blank_below_horizon.h"
 #include "mem/define_mem_normalise.h"
 #include "interferometer/define_evaluate_jones_R.h"
+#include "convert/define_convert_lon_lat_to_relative_directions.h"
+#include "convert/define_convert_apparent_ra_dec_to_enu_directions.h"
+#include "sky/define_update_horizon_mask.h"
 
 #define INST(REAL, S, REAL2, REAL4c) \
 OSKAR_ACORR_CPU(k_acorr_##S, REAL, REAL2, REAL4c) \
@@ -123,3 +126,29 @@ void ref_jones_r_##S(int num_sources, const REAL* ra, const REAL* dec, \
 
 INST_BEAM(double, d, double2, double4c)
 INST_BEAM(float, f, float2, float4c)
+
+/* Direction conversions and the horizon mask. */
+#define INST_DIR(REAL, S) \
+OSKAR_CONVERT_LON_LAT_TO_REL_DIR(k_lonlat_3d_##S, 1, REAL) \
+OSKAR_CONVERT_LON_LAT_TO_REL_DIR(k_lonlat_2d_##S, 0, REAL) \
+OSKAR_CONVERT_RA_DEC_TO_ENU_DIR(k_radec_enu_##S, REAL) \
+OSKAR_UPDATE_HORIZON_MASK(k_horizon_##S, REAL) \
+void ref_lon_lat_to_relative_directions_##S(int num, const REAL* lon, \
+        const REAL* lat, REAL lon0, REAL cos_lat0, REAL sin_lat0, REAL* l, \
+        REAL* m, REAL* n) \
+{ \
+    if (n) k_lonlat_3d_##S(num, lon, lat, lon0, cos_lat0, sin_lat0, l, m, \
+            n); \
+    else k_lonlat_2d_##S(num, lon, lat, lon0, cos_lat0, sin_lat0, l, m, n); \
+} \
+void ref_ra_dec_to_enu_directions_##S(int num, const REAL* ra, \
+        const REAL* dec, REAL lst, REAL sin_lat, REAL cos_lat, \
+        int offset_out, REAL* x, REAL* y, REAL* z) \
+{ k_radec_enu_##S(num, ra, dec, lst, sin_lat, cos_lat, offset_out, x, y, \
+        z); } \
+void ref_update_horizon_mask_##S(int num, const REAL* l, const REAL* m, \
+        const REAL* n, REAL l_mul, REAL m_mul, REAL n_mul, int* mask) \
+{ k_horizon_##S(num, l, m, n, l_mul, m_mul, n_mul, mask); }
+
+INST_DIR(double, d)
+INST_DIR(float, f)

@@ -252,3 +252,50 @@ def test_station_beam_composition(real, flags):
     assert np.array_equal(got, out[:8 * nd]) or _close(got, out[:8 * nd],
                                                         real)
     assert np.count_nonzero(got) > 0
+
+
+@pytest.mark.parametrize("real", [np.float64, np.float32])
+def test_direction_conversions_and_horizon(real):
+    rng = np.random.default_rng(16)
+    n = 500
+    lon = rng.uniform(0, 2 * np.pi, n).astype(real)
+    lat = rng.uniform(-1.5, 1.5, n).astype(real)
+    c0, s0 = real(np.cos(-0.5)), real(np.sin(-0.5))
+    for three_d in (True, False):
+        outs = [[np.zeros(n, real) for _ in range(3)] for _ in range(2)]
+        for lib, o in zip([oracle(), reference()], outs):
+            lib.call("lon_lat_to_relative_directions_" + suffix(real), real,
+                     n, lon, lat, real(0.3), c0, s0, o[0], o[1],
+                     o[2] if three_d else None)
+        for a, b in zip(*outs):
+            assert _close(a, b, real) or not b.any()
+    outs = [[np.zeros(n + 3, real) for _ in range(3)] for _ in range(2)]
+    for lib, o in zip([oracle(), reference()], outs):
+        lib.call("ra_dec_to_enu_directions_" + suffix(real), real, n, lon,
+                 lat, real(1.7), real(np.sin(-0.47)), real(np.cos(-0.47)), 3,
+                 *o)
+    for a, b in zip(*outs):
+        assert _close(a, b, real)
+    l, m, nn = (rng.uniform(-1, 1, n).astype(real) for _ in range(3))
+    masks = [np.zeros(n, np.int32), np.zeros(n, np.int32)]
+    for lib, mk in zip([oracle(), reference()], masks):
+        for mul in ((0.3, -0.2, 0.9), (-0.8, 0.1, 0.2)):
+            lib.call("update_horizon_mask_" + suffix(real), real, n, l, m, nn,
+                     *(real(x) for x in mul), mk)
+    assert np.array_equal(masks[0], masks[1])
+    assert 0 < masks[0].sum() < n
+
+
+@pytest.mark.parametrize("casa", [0, 1])
+def test_baseline_uvw_known_answer(casa):
+    """The reference's baseline order (p < q, q fastest) and sign
+    (convert/src/oskar_convert_station_uvw_to_baseline_uvw.c:18-28)."""
+    u = np.array([0.0, 1.0, 3.0, 7.0]); v = 2 * u; w = -u
+    out = [np.zeros(8) for _ in range(3)]
+    oracle().call("station_uvw_to_baseline_uvw_d", np.float64, casa, 4, 0,
+                  u, v, w, 2, *out)
+    f = -1 if casa else 1
+    pairs = [(0, 1), (0, 2), (0, 3), (1, 2), (1, 3), (2, 3)]
+    assert np.array_equal(out[0][2:], [f * (u[q] - u[p]) for p, q in pairs])
+    assert np.array_equal(out[1][2:], [f * (v[q] - v[p]) for p, q in pairs])
+    assert np.array_equal(out[2][2:], [f * (w[q] - w[p]) for p, q in pairs])
