@@ -598,6 +598,212 @@ def run_profile_case(args):
     return 0
 
 
+def c2_cpu_sample(cfg, t=0, ch=0, num_beam_st=32, num_corr_src=3000):
+    """The reference's own CPU kernels (OpenMP, oracle/_ref) on bounded
+    samples of one (dump, channel) of the aperture-array chain: the station
+    beam (element pattern, weights, weighted DFT, blanking, final
+    normalisation) of num_beam_st stations for every source, and Jones K,
+    the join and the cross-correlation of all stations for num_corr_src
+    sources. Returns the seconds the whole (dump, channel) would take,
+    scaled linearly from the two samples, and the sample description."""
+    lib = ref_lib()
+    if lib is None:
+        raise RuntimeError("oracle/_ref/liboskar_ref.so not built")
+    D = ctypes.c_double
+    N, S, ne = cfg["num_st"], cfg["num_src"], cfg["num_el"]
+    f = float(cfg["freqs"][ch])
+    k = 2 * math.pi * f / 299792458.0
+    kL = 0.5 * 299792458.0 / f * (math.pi * f / 299792458.0)
+    lst = cfg["gast"][t] + cfg["lon"]
+    t0 = time.perf_counter()
+    for p in range(num_beam_st):
+        sl, cl = math.sin(cfg["lat"][p]), math.cos(cfg["lat"][p])
+        ha = lst[p] - cfg["ra"]
+        x = np.ascontiguousarray(-np.cos(cfg["dec"]) * np.sin(ha))
+        y = np.ascontiguousarray(cl * np.sin(cfg["dec"]) -
+                                 sl * np.cos(cfg["dec"]) * np.cos(ha))
+        z = np.ascontiguousarray(sl * np.sin(cfg["dec"]) +
+                                 cl * np.cos(cfg["dec"]) * np.cos(ha))
+        hb = lst[p] - cfg["ra0"]
+        b = (-math.cos(cfg["dec0"]) * math.sin(hb),
+             cl * math.sin(cfg["dec0"]) - sl * math.cos(cfg["dec0"]) *
+             math.cos(hb),
+             sl * math.sin(cfg["dec0"]) + cl * math.cos(cfg["dec0"]) *
+             math.cos(hb))
+        X = np.ascontiguousarray(np.append(x, b[0]))
+        Y = np.ascontiguousarray(np.append(y, b[1]))
+        Z = np.ascontiguousarray(np.append(z, b[2]))
+        th, p1, p2 = (np.zeros(S + 2) for _ in range(3))
+        lib.ref_enu_to_theta_phi_d(0, S + 1, _p(X), _p(Y), _p(Z), 0,
+                                   D(-cfg["orient"][p]),
+                                   D(math.pi / 2 - cfg["orient"][p]),
+                                   _p(th), _p(p1), _p(p2))
+        sig = np.zeros((S + 1) * 8)
+        lib.ref_dipole_pattern_d(S + 1, _p(th), _p(p1), _p(p2), D(kL),
+                                 D(math.cos(kL)), 0, 0, _p(sig))
+        ex = np.ascontiguousarray(cfg["el_x"][p])
+        ey = np.ascontiguousarray(cfg["el_y"][p])
+        ez = np.zeros(ne)
+        w = np.zeros(2 * ne)
+        lib.ref_element_weights_dft_d(ne, _p(ex), _p(ey), _p(ez), _p(ez),
+                                      D(k), D(b[0]), D(b[1]), D(b[2]), _p(w))
+        out = np.zeros((S + 1) * 8)
+        types = np.zeros(ne, np.int32)  # one element type
+        lib.ref_dftw_d(1, 0, ne, D(k), _p(w), _p(ex), _p(ey), _p(None), 0,
+                       S + 1, _p(X), _p(Y), _p(None), _p(types), _p(sig), 1,
+                       1, 0, _p(out), D(1.0 / ne))
+        lib.ref_blank_below_horizon_d(0, S + 1, _p(Z), 0, _p(out))
+        lib.ref_mem_normalise_matrix_d(0, S + 1, _p(out), S)
+    t_beam = time.perf_counter() - t0
+    ns = num_corr_src
+    rng = np.random.default_rng(12)
+    E = rng.normal(0, 0.1, (N, ns, 8))
+    E[..., 0] += 1
+    E[..., 6] += 1
+    x, y, z = (np.ascontiguousarray(a) for a in cfg["ecef"])
+    ha0 = cfg["gast"][t] - cfg["ra0"]
+    u, v, w = (np.zeros(N) for _ in range(3))
+    lib.ref_ecef_to_station_uvw_d(N, _p(x), _p(y), _p(z), D(math.sin(ha0)),
+                                  D(math.cos(ha0)), D(math.sin(cfg["dec0"])),
+                                  D(math.cos(cfg["dec0"])), 0, 0, _p(u),
+                                  _p(v), _p(w))
+    sl_ = slice(0, ns)
+    l, m, n, I, Q, U, V = (np.ascontiguousarray(cfg[c][sl_]) for c in
+                           ("l", "m", "n", "I", "Q", "U", "V"))
+    K = np.zeros((N, ns, 2))
+    J = np.zeros((N, ns, 8))
+    nbl = N * (N - 1) // 2
+    vis = np.zeros((nbl, 8))
+    zeros = np.zeros(N)
+    t1 = time.perf_counter()
+    lib.ref_jones_k_d(ns, _p(l), _p(m), _p(n), N, _p(u), _p(v), _p(w), D(k),
+                      _p(I), D(0.0), D(1e300), 0, _p(K))
+    lib.ref_mem_mul_cm_m_d(N * ns, _p(K), _p(E), _p(J))
+    lib.oskar_cross_correlate_point_omp_d(
+        0, ns, N, 0, _p(J), _p(I), _p(Q), _p(U), _p(V), _p(l), _p(m), _p(n),
+        _p(u), _p(v), _p(w), _p(zeros), _p(zeros), D(0.0), D(3e38),
+        D(f / 299792458.0), D(0.0), D(0.0), D(0.0), D(0.0), _p(vis))
+    t_corr = time.perf_counter() - t1
+    est = t_beam * N / num_beam_st + t_corr * S / ns
+    return est, ("1 dump x 1 channel: station beams of %d of %d stations x "
+                 "%d sources (%.1f s) and K + join + correlation of %d "
+                 "stations x %d of %d sources (%.1f s), scaled linearly"
+                 % (num_beam_st, N, S, t_beam, N, ns, S, t_corr))
+
+
+def run_c2(args):
+    """Aperture-array chain per dump: ENU directions of every source at
+    every station, station beams (256 dipoles), Jones R, E R, Jones K,
+    J = K (E R), cross-correlation, for 4 channels; 128 stations, 12,000
+    sources, FP64. Prints one JSON line: source-baselines/s through the
+    chain, the station-beam kernel's share and element-directions/s, and
+    the reference's CPU kernels on the host cores beside it."""
+    import torch
+    import oskar_b200 as ob
+    from oskar_b200 import workloads
+    torch.cuda.set_device(0)
+    dev = lambda a: torch.from_numpy(np.ascontiguousarray(a)).cuda()
+    cfg = workloads.c2()
+    N, S, ne = cfg["num_st"], cfg["num_src"], cfg["num_el"]
+    C = len(cfg["freqs"])
+    nbl = N * (N - 1) // 2
+    st = ob.stream_ptr()
+    d = {k: dev(cfg[k]) for k in ("ra", "dec", "l", "m", "n", "I", "Q", "U",
+                                  "V", "lat", "el_x", "el_y", "orient")}
+    ex, ey, ez = (dev(cfg[k][i]) for k, i in (("ecef", 0), ("ecef", 1),
+                                              ("ecef", 2)))
+    el_z = torch.zeros_like(d["el_x"])
+    f64 = torch.float64
+    X, Y, Z = (torch.empty((N, S), dtype=f64, device="cuda")
+               for _ in range(3))
+    BX, BY, BZ = (torch.empty((N, 1), dtype=f64, device="cuda")
+                  for _ in range(3))
+    u, v, w = (torch.empty(N, dtype=f64, device="cuda") for _ in range(3))
+    E = torch.empty((N, S, 8), dtype=f64, device="cuda")
+    R = torch.empty_like(E)
+    K = torch.empty((N, S, 2), dtype=f64, device="cuda")
+    vis = torch.zeros((C, nbl, 8), dtype=f64, device="cuda")
+    ra0 = dev(np.array([cfg["ra0"]]))
+    dec0 = dev(np.array([cfg["dec0"]]))
+    beam_events = []
+
+    def step(t):
+        lst = d["lat"].new_tensor(cfg["gast"][t] + cfg["lon"])
+        ob.call("oskb_convert_ra_dec_to_enu_directions_d", S, d["ra"],
+                d["dec"], N, lst, d["lat"], X, Y, Z, st)
+        ob.call("oskb_convert_ra_dec_to_enu_directions_d", 1, ra0, dec0, N,
+                lst, d["lat"], BX, BY, BZ, st)
+        benu = torch.cat([BX, BY, BZ], 1).contiguous()
+        ob.call("oskb_convert_ecef_to_station_uvw_d", N, ex, ey, ez,
+                cfg["ra0"], cfg["dec0"], float(cfg["gast"][t]), 0, 0, u, v,
+                w, st)
+        ob.call("oskb_evaluate_jones_R_d", S, d["ra"], d["dec"], N,
+                d["lat"], lst, R, st)
+        vis.zero_()
+        for c in range(C):
+            f = float(cfg["freqs"][c])
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record()
+            ob.call("oskb_station_beam_aa_d", N, ne, d["el_x"], d["el_y"],
+                    el_z, None, None, None, None, d["orient"], d["orient"],
+                    0.5 * 299792458.0 / f, 0, 1, 1, 0, 0, f, benu, benu, S,
+                    X, Y, Z, 1, E, st)
+            e1.record()
+            beam_events.append((e0, e1))
+            ob.call("oskb_mem_multiply_d", 5, 0, 0, 0, N * S, E, R, E, st)
+            ob.call("oskb_evaluate_jones_K_d", S, d["l"], d["m"], d["n"], N,
+                    u, v, w, 2 * math.pi * f / 299792458.0, d["I"], 0.0,
+                    1e300, 0, K, st)
+            ob.call("oskb_mem_multiply_d", 3, 0, 0, 0, N * S, K, E, E, st)
+            ob.call("oskb_cross_correlate_d", 0, 0, S, N, 0, E, d["I"],
+                    d["Q"], d["U"], d["V"], d["l"], d["m"], d["n"], None,
+                    None, None, u, v, w, None, None, 0.0, 3e38,
+                    f / 299792458.0, 0.0, 0.0, 0.0, 0.0, vis[c], st)
+
+    for i in range(args.warmup):
+        step(i % cfg["num_times"])
+    torch.cuda.synchronize()
+    beam_events.clear()
+    clocks = ClockSampler(0)
+    clocks.start()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for i in range(args.steps):
+        step((args.warmup + i) % cfg["num_times"])
+    e1.record()
+    torch.cuda.synchronize()
+    clk = clocks.stop()
+    ms = e0.elapsed_time(e1) / args.steps
+    beam_ms = sum(a.elapsed_time(b) for a, b in beam_events) / args.steps
+    sb = nbl * S * C
+    eldir = N * S * ne * C
+    est, sample = c2_cpu_sample(cfg)
+    cpu = sb / C / est / 1e9
+    print(json.dumps({
+        "workload": "c2: 128 aperture-array stations (256 dipoles each, "
+                    "38 m), 12,000 sources (10,000 in a 10 deg field + "
+                    "2,000 anywhere above the horizon), 4 channels "
+                    "100-130 MHz, 32 dumps; step = 1 dump x 4 channels of "
+                    "ENU directions -> beam -> R -> E R -> K -> J -> "
+                    "cross-correlation, FP64",
+        "metric": "G source-baselines/s through the aperture-array chain",
+        "value": sb / (ms * 1e-3) / 1e9, "unit": "G source-baselines/s",
+        "ms_per_step": ms, "steps": args.steps, "warmup": args.warmup,
+        "dtype": "f64",
+        "station_beam": {"ms_per_step": beam_ms,
+                         "share_of_step": beam_ms / ms,
+                         "G_element_directions_per_s":
+                             eldir / (beam_ms * 1e-3) / 1e9},
+        "cpu_baseline": {"value": cpu, "unit": "G source-baselines/s",
+                         "cores": cpu_cores(), "kind": "reference",
+                         "sample": sample},
+        "clocks": clk,
+    }))
+    return 0
+
+
 def run_c5(args):
     """Learned station-beam surrogate against the exact station beam, one
     step = the Jones E of every station for every source at one (dump,
@@ -755,8 +961,9 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--path", default="tc", choices=["tc", "direct"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--workload", default="c3", choices=["c3", "c5"],
-                    help="c5: the learned station-beam surrogate measurement")
+    ap.add_argument("--workload", default="c3", choices=["c3", "c2", "c5"],
+                    help="c2: the aperture-array beam chain; c5: the learned "
+                         "station-beam surrogate")
     ap.add_argument("--c5-steps", type=int, default=20000)
     ap.add_argument("--c5-bound", type=float, default=1e-4)
     ap.add_argument("--profile-case", default=None,
@@ -768,6 +975,8 @@ def main():
         return run_profile_case(args)
     if args.workload == "c5":
         return run_c5(args)
+    if args.workload == "c2":
+        return run_c2(args)
     os.environ.setdefault("OMP_NUM_THREADS", str(cpu_cores()))
     if args.impl == "reference":
         return run_reference(args)

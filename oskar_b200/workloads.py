@@ -146,3 +146,67 @@ def jones_e_host(cfg, rng_seed=None):
     e[..., 0] += 1.0
     e[..., 6] += 1.0
     return e
+
+
+def c2(num_st=128, num_el=256, num_field=10_000, num_off=2_000,
+       num_channels=4, num_times=32):
+    """Aperture-array stations with beams: num_st stations log-radial from
+    50 m to 40 km, each with num_el dipoles uniform in a 38 m disc (its own
+    layout); num_field sources in a 10 degree field plus num_off at random
+    directions (above the horizon at the first dump); I power law, Q and U
+    N(0, 0.05 I) on 10 % of sources; 4 channels over 100-130 MHz, 32 dumps
+    of 60 s from MJD 51544.5; array at latitude -27 deg, longitude
+    116.76 deg; phase centre RA 0, Dec -30 deg. Returned as a dict of FP64
+    numpy arrays."""
+    rng = np.random.default_rng(2)
+    lat0, lon0 = math.radians(-27.0), math.radians(116.76)
+    ra0, dec0 = 0.0, math.radians(-30.0)
+    r = np.exp(rng.uniform(math.log(50.0), math.log(40e3), num_st))
+    th = rng.uniform(0, 2 * math.pi, num_st)
+    e_off, n_off = r * np.cos(th), r * np.sin(th)
+    ecef = np.stack(enu_to_ecef_offsets(e_off, n_off, np.zeros(num_st),
+                                        lat0, lon0))
+    lat = lat0 + n_off / 6.371e6
+    lon = lon0 + e_off / (6.371e6 * math.cos(lat0))
+    rr = 19.0 * np.sqrt(rng.uniform(0, 1, (num_st, num_el)))
+    tt = rng.uniform(0, 2 * math.pi, (num_st, num_el))
+    el_x, el_y = rr * np.cos(tt), rr * np.sin(tt)
+    orient = np.zeros(num_st)
+    l, m, n = disc_lmn(rng, num_field, 10.0)
+    # field sources: (l, m) about the phase centre -> RA, Dec
+    dec_f = np.arcsin(m * math.cos(dec0) + n * math.sin(dec0))
+    ra_f = ra0 + np.arctan2(l, n * math.cos(dec0) - m * math.sin(dec0))
+    mjd0 = 51544.5
+    gast0 = gast_rad(mjd0 + 30.0 / 86400.0)
+    # off-field sources above the horizon at the array centre, first dump
+    ra_o, dec_o = [], []
+    while len(ra_o) < num_off:
+        ra_c = rng.uniform(0, 2 * math.pi)
+        dec_c = math.asin(rng.uniform(-1, 1))
+        ha = gast0 + lon0 - ra_c
+        el_s = (math.sin(lat0) * math.sin(dec_c) +
+                math.cos(lat0) * math.cos(dec_c) * math.cos(ha))
+        if el_s > 0.05:
+            ra_o.append(ra_c)
+            dec_o.append(dec_c)
+    ra = np.concatenate([ra_f, np.array(ra_o)])
+    dec = np.concatenate([dec_f, np.array(dec_o)])
+    dra = ra - ra0
+    l = np.cos(dec) * np.sin(dra)
+    m = math.cos(dec0) * np.sin(dec) - math.sin(dec0) * np.cos(dec) * \
+        np.cos(dra)
+    n = math.sin(dec0) * np.sin(dec) + math.cos(dec0) * np.cos(dec) * \
+        np.cos(dra)
+    ns = num_field + num_off
+    I = power_law_flux(rng, ns)
+    pol = rng.uniform(0, 1, ns) < 0.1
+    Q = np.where(pol, rng.normal(0, 0.05, ns) * I, 0.0)
+    U = np.where(pol, rng.normal(0, 0.05, ns) * I, 0.0)
+    V = np.zeros(ns)
+    freqs = np.linspace(100e6, 130e6, num_channels)
+    gast = np.array([gast_rad(mjd0 + (t + 0.5) * 60.0 / 86400.0)
+                     for t in range(num_times)])
+    return dict(num_st=num_st, num_el=num_el, num_src=ns, lat=lat, lon=lon,
+                ecef=ecef, el_x=el_x, el_y=el_y, orient=orient, ra=ra,
+                dec=dec, l=l, m=m, n=n, I=I, Q=Q, U=U, V=V, freqs=freqs,
+                gast=gast, ra0=ra0, dec0=dec0, num_times=num_times)
