@@ -15,6 +15,12 @@ FP64 phase; --path direct uses the FP64 direct kernels. The reported metric
 is source-baselines per second over all ranks; N > 1 shards dumps across
 ranks with no data-path collective (weak scaling).
 
+--workload c2 measures the aperture-array chain (station beams, Jones R,
+joins, Jones K, correlation; 128 stations x 256 dipoles, 12,000 sources);
+--workload c5 the learned station-beam surrogate against the exact beam.
+Each prints its own JSON line; the default (c3) line is the headline.
+--profile-case runs one small kernel case for an ncu capture.
+
 --impl reference times the reference's own CPU implementation of the same
 path (its OpenMP kernels compiled from its sources into
 oracle/_ref/liboskar_ref.so) on the host cores, on a bounded sample of the
