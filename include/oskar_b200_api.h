@@ -151,6 +151,23 @@ OSKB_API void oskar_convert_ecef_to_station_uvw(int num_stations,
         int ignore_w_components, int offset_out, oskar_Mem* u, oskar_Mem* v,
         oskar_Mem* w, int* status);
 
+/* oskar/convert/oskar_convert_station_uvw_to_baseline_uvw.h:39-49 */
+OSKB_API void oskar_convert_station_uvw_to_baseline_uvw(
+        int use_casa_phase_convention, int num_stations, int offset_in,
+        const oskar_Mem* u, const oskar_Mem* v, const oskar_Mem* w,
+        int offset_out, oskar_Mem* uu, oskar_Mem* vv, oskar_Mem* ww,
+        int* status);
+/* oskar/convert/oskar_convert_lon_lat_to_relative_directions.h:154-157 */
+OSKB_API void oskar_convert_lon_lat_to_relative_directions(int num_points,
+        const oskar_Mem* lon_rad, const oskar_Mem* lat_rad, double lon0_rad,
+        double lat0_rad, oskar_Mem* l, oskar_Mem* m, oskar_Mem* n,
+        int* status);
+/* oskar/convert/oskar_convert_apparent_ra_dec_to_enu_directions.h:41-45 */
+OSKB_API void oskar_convert_apparent_ra_dec_to_enu_directions(int num_points,
+        const oskar_Mem* ra_rad, const oskar_Mem* dec_rad, double lst_rad,
+        double latitude_rad, int offset_out, oskar_Mem* x, oskar_Mem* y,
+        oskar_Mem* z, int* status);
+
 #ifdef __cplusplus
 }
 #endif

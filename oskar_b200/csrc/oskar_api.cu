@@ -768,3 +768,140 @@ void oskar_convert_ecef_to_station_uvw(int num_stations, const oskar_Mem* x,
 }
 
 }  // extern "C"
+
+namespace {
+
+// Common checks of the conversion wrappers: same location and precision
+// for every array, GPU only, FP32 or FP64.
+int check_arrays(const oskar_Mem* const* a, int n, int* type)
+{
+    const oskar_Mem* first = nullptr;
+    for (int i = 0; i < n; ++i)
+    {
+        if (!a[i]) continue;
+        if (!first) { first = a[i]; continue; }
+        if (a[i]->location != first->location)
+            return OSKAR_ERR_LOCATION_MISMATCH;
+        if (a[i]->type != first->type) return OSKAR_ERR_TYPE_MISMATCH;
+    }
+    if (!first) return OSKAR_ERR_INVALID_ARGUMENT;
+    if (first->location != OSKAR_GPU) return OSKAR_ERR_BAD_LOCATION;
+    if (first->type != OSKAR_DOUBLE && first->type != OSKAR_SINGLE)
+        return OSKAR_ERR_BAD_DATA_TYPE;
+    *type = first->type;
+    return 0;
+}
+
+}  // namespace
+
+extern "C" {
+
+// oskar/convert/src/oskar_convert_station_uvw_to_baseline_uvw.c:34-100
+void oskar_convert_station_uvw_to_baseline_uvw(int use_casa_phase_convention,
+        int num_stations, int offset_in, const oskar_Mem* u,
+        const oskar_Mem* v, const oskar_Mem* w, int offset_out,
+        oskar_Mem* uu, oskar_Mem* vv, oskar_Mem* ww, int* status)
+{
+    if (*status) return;
+    const oskar_Mem* all[6] = {u, v, w, uu, vv, ww};
+    int type = 0;
+    for (int i = 0; i < 6; ++i)
+        if (!all[i]) { *status = OSKAR_ERR_INVALID_ARGUMENT; return; }
+    if ((*status = check_arrays(all, 6, &type))) return;
+    const size_t nbl = (size_t) num_stations * (num_stations - 1) / 2;
+    mem_ensure(uu, offset_out + nbl, status);
+    mem_ensure(vv, offset_out + nbl, status);
+    mem_ensure(ww, offset_out + nbl, status);
+    if (*status) return;
+    if (type == OSKAR_DOUBLE)
+        *status = oskb_convert_station_uvw_to_baseline_uvw_d(
+                use_casa_phase_convention, num_stations, offset_in, D(u),
+                D(v), D(w), offset_out, (double*) uu->data,
+                (double*) vv->data, (double*) ww->data, 0);
+    else
+        *status = oskb_convert_station_uvw_to_baseline_uvw_f(
+                use_casa_phase_convention, num_stations, offset_in, F(u),
+                F(v), F(w), offset_out, (float*) uu->data,
+                (float*) vv->data, (float*) ww->data, 0);
+}
+
+// oskar/convert/oskar_convert_lon_lat_to_relative_directions.h:154-157
+// (n may be NULL: the 2-D form)
+void oskar_convert_lon_lat_to_relative_directions(int num_points,
+        const oskar_Mem* lon_rad, const oskar_Mem* lat_rad, double lon0_rad,
+        double lat0_rad, oskar_Mem* l, oskar_Mem* m, oskar_Mem* n,
+        int* status)
+{
+    if (*status) return;
+    if (!lon_rad || !lat_rad || !l || !m)
+    {
+        *status = OSKAR_ERR_INVALID_ARGUMENT;
+        return;
+    }
+    const oskar_Mem* all[5] = {lon_rad, lat_rad, l, m, n};
+    int type = 0;
+    if ((*status = check_arrays(all, 5, &type))) return;
+    mem_ensure(l, num_points, status);
+    mem_ensure(m, num_points, status);
+    if (n) mem_ensure(n, num_points, status);
+    if (*status) return;
+    if (type == OSKAR_DOUBLE)
+        *status = oskb_convert_lon_lat_to_relative_directions_d(num_points,
+                D(lon_rad), D(lat_rad), lon0_rad, lat0_rad,
+                (double*) l->data, (double*) m->data,
+                n ? (double*) n->data : nullptr, 0);
+    else
+        *status = oskb_convert_lon_lat_to_relative_directions_f(num_points,
+                F(lon_rad), F(lat_rad), lon0_rad, lat0_rad,
+                (float*) l->data, (float*) m->data,
+                n ? (float*) n->data : nullptr, 0);
+}
+
+// oskar/convert/oskar_convert_apparent_ra_dec_to_enu_directions.h:41-45
+void oskar_convert_apparent_ra_dec_to_enu_directions(int num_points,
+        const oskar_Mem* ra_rad, const oskar_Mem* dec_rad, double lst_rad,
+        double latitude_rad, int offset_out, oskar_Mem* x, oskar_Mem* y,
+        oskar_Mem* z, int* status)
+{
+    if (*status) return;
+    if (!ra_rad || !dec_rad || !x || !y || !z)
+    {
+        *status = OSKAR_ERR_INVALID_ARGUMENT;
+        return;
+    }
+    const oskar_Mem* all[5] = {ra_rad, dec_rad, x, y, z};
+    int type = 0;
+    if ((*status = check_arrays(all, 5, &type))) return;
+    mem_ensure(x, (size_t) offset_out + num_points, status);
+    mem_ensure(y, (size_t) offset_out + num_points, status);
+    mem_ensure(z, (size_t) offset_out + num_points, status);
+    if (*status || num_points == 0) return;
+    // one station: its LST and latitude as one-element device arrays
+    double h[2] = {lst_rad, latitude_rad};
+    double* d = nullptr;
+    if (cudaMalloc(&d, sizeof(h)) != cudaSuccess ||
+            cudaMemcpy(d, h, sizeof(h), cudaMemcpyHostToDevice) !=
+            cudaSuccess)
+    {
+        oskb::set_last_error("oskar_convert_apparent_ra_dec_to_enu_"
+                "directions", cudaGetLastError());
+        cudaFree(d);
+        *status = OSKAR_ERR_MEMORY_ALLOC_FAILURE;
+        return;
+    }
+    if (type == OSKAR_DOUBLE)
+        *status = oskb_convert_ra_dec_to_enu_directions_d(num_points,
+                D(ra_rad), D(dec_rad), 1, d, d + 1,
+                (double*) x->data + offset_out,
+                (double*) y->data + offset_out,
+                (double*) z->data + offset_out, 0);
+    else
+        *status = oskb_convert_ra_dec_to_enu_directions_f(num_points,
+                F(ra_rad), F(dec_rad), 1, d, d + 1,
+                (float*) x->data + offset_out, (float*) y->data + offset_out,
+                (float*) z->data + offset_out, 0);
+    cudaStreamSynchronize(0);
+    cudaFree(d);
+}
+
+}  // extern "C"

@@ -141,3 +141,26 @@ def test_evaluate_jones_K_checks(lib):
     assert st.value == -9
     oa.free_jones(K)
     oa.free_mem(*a, *b, f)
+
+
+def test_conversion_wrapper_checks(lib):
+    a = oa.mem_from_numpy(np.zeros(5), D, CPU)
+    b = oa.mem_from_numpy(np.zeros(5, np.float32), S, CPU)
+    st = st0()
+    lib.oskar_convert_station_uvw_to_baseline_uvw(0, 5, 0, a, a, a, 0, a,
+                                                  a, b, oa.status_ptr(st))
+    assert st.value == -9
+    st = st0()
+    lib.oskar_convert_station_uvw_to_baseline_uvw(0, 5, 0, a, a, a, 0, a,
+                                                  a, a, oa.status_ptr(st))
+    assert st.value == -14  # no CPU compute path
+    st = st0()
+    lib.oskar_convert_lon_lat_to_relative_directions(5, a, a, 0.0, 0.0, a,
+                                                     a, None,
+                                                     oa.status_ptr(st))
+    assert st.value == -14
+    st = ctypes.c_int(-3)
+    lib.oskar_convert_apparent_ra_dec_to_enu_directions(
+        5, a, a, 0.0, 0.0, 0, a, a, a, oa.status_ptr(st))
+    assert st.value == -3  # status on entry is kept
+    oa.free_mem(a, b)

@@ -185,3 +185,56 @@ def test_auto_correlate_api():
     assert rel(oa.mem_to_numpy(vis), ref) <= 1e-12
     oa.free_jones(j)
     oa.free_mem(*flux, vis)
+
+
+@pytest.mark.parametrize("prec", [D, S])
+def test_conversion_wrappers(prec):
+    """oskar_convert_station_uvw_to_baseline_uvw,
+    oskar_convert_lon_lat_to_relative_directions and
+    oskar_convert_apparent_ra_dec_to_enu_directions on oskar_Mem arrays,
+    against the oracle."""
+    lib = load()
+    real = np.float64 if prec == D else np.float32
+    s = "d" if prec == D else "f"
+    rng = np.random.default_rng(9)
+    nst = 40
+    uvw = [rng.uniform(-1e4, 1e4, nst).astype(real) for _ in range(3)]
+    mu = [oa.mem_from_numpy(a, prec, GPU) for a in uvw]
+    mb = [oa.mem_from_numpy(np.zeros(1, real), prec, GPU) for _ in range(3)]
+    st = oa.ctypes.c_int(0)
+    lib.oskar_convert_station_uvw_to_baseline_uvw(1, nst, 0, *mu, 0, *mb,
+                                                  oa.status_ptr(st))
+    assert st.value == 0
+    nbl = nst * (nst - 1) // 2
+    ref = [np.zeros(nbl, real) for _ in range(3)]
+    oracle().call("station_uvw_to_baseline_uvw_" + s, real, 1, nst, 0,
+                  *uvw, 0, *ref)
+    for m, r in zip(mb, ref):
+        assert lib.oskar_mem_length(m) == nbl
+        assert np.array_equal(oa.mem_to_numpy(m), r)
+    n = 999
+    lon = rng.uniform(0, 6, n).astype(real)
+    lat = rng.uniform(-1.5, 1.5, n).astype(real)
+    ml, mlat = (oa.mem_from_numpy(a, prec, GPU) for a in (lon, lat))
+    out = [oa.mem_from_numpy(np.zeros(n, real), prec, GPU) for _ in range(3)]
+    lib.oskar_convert_lon_lat_to_relative_directions(n, ml, mlat, 0.2, -0.6,
+                                                     *out, oa.status_ptr(st))
+    assert st.value == 0
+    ref = [np.zeros(n, real) for _ in range(3)]
+    oracle().call("lon_lat_to_relative_directions_" + s, real, n, lon, lat,
+                  real(0.2), real(np.cos(-0.6)), real(np.sin(-0.6)), *ref)
+    tol = 1e-14 if prec == D else 2e-6
+    for m, r in zip(out, ref):
+        assert np.max(np.abs(oa.mem_to_numpy(m) - r)) <= tol
+    xyz = [oa.mem_from_numpy(np.zeros(n + 2, real), prec, GPU)
+           for _ in range(3)]
+    lib.oskar_convert_apparent_ra_dec_to_enu_directions(
+        n, ml, mlat, 1.3, -0.47, 2, *xyz, oa.status_ptr(st))
+    assert st.value == 0
+    ref = [np.zeros(n + 2, real) for _ in range(3)]
+    oracle().call("ra_dec_to_enu_directions_" + s, real, n, lon, lat,
+                  real(1.3), real(np.sin(-0.47)), real(np.cos(-0.47)), 2,
+                  *ref)
+    for m, r in zip(xyz, ref):
+        assert np.max(np.abs(oa.mem_to_numpy(m) - r)) <= tol
+    oa.free_mem(*mu, *mb, ml, mlat, *out, *xyz)
