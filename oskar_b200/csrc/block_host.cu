@@ -3,14 +3,16 @@
 // oskar/interferometer/src/oskar_interferometer_run_block.c:28-153, for
 // point sources without smearing): copy the block's inputs from host memory,
 // correlate every (time, channel) of the block on the GPU, copy the
-// visibility block back. Device buffers are kept by the library per device
-// and grown on demand; with page-locked host buffers the copies run at full
-// link speed.
+// visibility block back (group by group, overlapping the later groups'
+// computation). Device buffers are kept by the library per device and grown
+// on demand; with page-locked host buffers the copies run at full link
+// speed.
 #include <string.h>
 
 #include <vector>
 
 #include "common.cuh"
+#include "xcorr_tc.cuh"
 
 namespace oskb {
 namespace {
@@ -24,6 +26,8 @@ struct DevBuf
 struct BlockBuffers
 {
     DevBuf E, sky, uvw, wl, vis;
+    cudaStream_t copy = nullptr;       // visibility downloads
+    std::vector<cudaEvent_t> events;   // one per group of the current call
 };
 
 BlockBuffers g_bufs[64];
@@ -110,9 +114,47 @@ extern "C" int oskb_run_block_tc_host(int casa, int num_sources,
     if ((err = copy_in(b.wl.ptr, wl.data(), num_channels * sizeof(double),
             s)))
         return err;
-    // The block is cleared, then accumulated, as the reference does.
+    // The block is cleared, then accumulated, as the reference does. Each
+    // group of (dump, channel) problems is downloaded on a copy stream as
+    // soon as its contraction has finished, while later groups compute.
     cudaMemsetAsync(b.vis.ptr, 0, vis_bytes, s);
-    err = oskb_correlate_block_tc(casa, num_sources, num_stations, num_times,
+    if (!b.copy)
+    {
+        if (cudaStreamCreateWithFlags(&b.copy, cudaStreamNonBlocking) !=
+                cudaSuccess)
+            b.copy = nullptr;
+    }
+    struct Ctx
+    {
+        cudaStream_t s, copy;
+        std::vector<cudaEvent_t>* events;
+        double* host;
+        const double* dev;
+        size_t problem_bytes;
+        bool failed;
+    } ctx{s, b.copy, &b.events, vis, static_cast<const double*>(b.vis.ptr),
+          nbl * 64, false};
+    auto after = [](void* p, int p0, int np) {
+        Ctx& c = *static_cast<Ctx*>(p);
+        if (!c.copy) return;
+        cudaEvent_t ev = nullptr;
+        if (cudaEventCreateWithFlags(&ev, cudaEventDisableTiming) !=
+                cudaSuccess)
+        {
+            c.failed = true;
+            return;
+        }
+        c.events->push_back(ev);
+        cudaEventRecord(ev, c.s);
+        cudaStreamWaitEvent(c.copy, ev, 0);
+        const size_t off = (size_t) p0 * c.problem_bytes;
+        if (cudaMemcpyAsync(reinterpret_cast<char*>(c.host) + off,
+                reinterpret_cast<const char*>(c.dev) + off,
+                (size_t) np * c.problem_bytes, cudaMemcpyDeviceToHost,
+                c.copy) != cudaSuccess)
+            c.failed = true;
+    };
+    err = tc::correlate_block(casa, num_sources, num_stations, num_times,
             num_channels, static_cast<const float*>(b.E.ptr), sky,
             sky + num_sources, sky + 2 * (size_t) num_sources,
             sky + 3 * (size_t) num_sources, sky + 4 * (size_t) num_sources,
@@ -120,11 +162,20 @@ extern "C" int oskb_run_block_tc_host(int casa, int num_sources,
             static_cast<const double*>(b.uvw.ptr),
             static_cast<const double*>(b.wl.ptr), uv_min_lambda,
             uv_max_lambda, static_cast<double*>(b.vis.ptr), nullptr, 0,
-            stream);
+            stream, b.copy ? +after : nullptr, &ctx);
+    bool failed = ctx.failed || err != 0;
+    if (!err && !b.copy &&
+            cudaMemcpyAsync(vis, b.vis.ptr, vis_bytes,
+            cudaMemcpyDeviceToHost, s) != cudaSuccess)
+        failed = true;
+    // Both streams must drain before the host buffer is complete.
+    const cudaError_t e1 = cudaStreamSynchronize(s);
+    const cudaError_t e2 = b.copy ? cudaStreamSynchronize(b.copy) :
+            cudaSuccess;
+    for (cudaEvent_t ev : b.events) cudaEventDestroy(ev);
+    b.events.clear();
     if (err) return err;
-    if (cudaMemcpyAsync(vis, b.vis.ptr, vis_bytes, cudaMemcpyDeviceToHost, s)
-            != cudaSuccess ||
-            cudaStreamSynchronize(s) != cudaSuccess)
+    if (failed || e1 != cudaSuccess || e2 != cudaSuccess)
     {
         set_last_error("block D2H", cudaGetLastError());
         return OSKB_ERR_MEMORY_COPY_FAILURE;

@@ -34,6 +34,7 @@
 
 #include "common.cuh"
 #include "tc_ptx.cuh"
+#include "xcorr_tc.cuh"
 
 namespace oskb {
 namespace tc {
@@ -859,6 +860,26 @@ int oskb_correlate_block_tc(int casa, int num_sources, int num_stations,
         double uv_max_lambda, double* vis, void* workspace,
         size_t workspace_bytes, void* stream)
 {
+    return oskb::tc::correlate_block(casa, num_sources, num_stations,
+            num_times, num_channels, E, l, m, n, I, Q, U, V, station_uvw,
+            inv_wavelength, uv_min_lambda, uv_max_lambda, vis, workspace,
+            workspace_bytes, stream, nullptr, nullptr);
+}
+
+}  // extern "C"
+
+namespace oskb {
+namespace tc {
+
+int correlate_block(int casa, int num_sources, int num_stations,
+        int num_times, int num_channels, const float* E, const double* l,
+        const double* m, const double* n, const double* I, const double* Q,
+        const double* U, const double* V, const double* station_uvw,
+        const double* inv_wavelength, double uv_min_lambda,
+        double uv_max_lambda, double* vis, void* workspace,
+        size_t workspace_bytes, void* stream,
+        void (*after_group)(void* ctx, int p0, int np), void* ctx)
+{
     if (num_sources < 0 || num_stations < 0 || num_times < 0 ||
             num_channels < 0)
         return OSKB_ERR_INVALID_ARGUMENT;
@@ -923,9 +944,15 @@ int oskb_correlate_block_tc(int casa, int num_sources, int num_stations,
         gp.uv_min = uv_min_lambda; gp.uv_max = uv_max_lambda;
         gp.casa = casa; gp.err = &hdr->err;
         if ((err = launch_gemm(gp, s))) return err;
+        if (after_group) after_group(ctx, p0, np);
     }
     return 0;
 }
+
+}  // namespace tc
+}  // namespace oskb
+
+extern "C" {
 
 int oskb_tc_timing(int enable)
 {

@@ -1,0 +1,23 @@
+// Internal interface of the tensor-core block correlation, shared by the
+// device-buffer entry point (xcorr_tc.cu) and the host-buffer driver
+// (block_host.cu).
+#pragma once
+
+namespace oskb {
+namespace tc {
+
+// oskb_correlate_block_tc with a hook: after_group (if set) is called on the
+// host once the contraction of problems [p0, p0 + np) has been enqueued on
+// the stream, so the caller can enqueue work that depends on those
+// visibilities (for example their download) while later groups compute.
+int correlate_block(int casa, int num_sources, int num_stations,
+        int num_times, int num_channels, const float* E, const double* l,
+        const double* m, const double* n, const double* I, const double* Q,
+        const double* U, const double* V, const double* station_uvw,
+        const double* inv_wavelength, double uv_min_lambda,
+        double uv_max_lambda, double* vis, void* workspace,
+        size_t workspace_bytes, void* stream,
+        void (*after_group)(void* ctx, int p0, int np), void* ctx);
+
+}  // namespace tc
+}  // namespace oskb
