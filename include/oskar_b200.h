@@ -507,6 +507,30 @@ OSKB_API int oskb_block_plan_synchronize(oskb_BlockPlan* plan);
 OSKB_API int oskb_block_plan_graph_launches(const oskb_BlockPlan* plan);
 OSKB_API void oskb_block_plan_free(oskb_BlockPlan* plan);
 
+/* Pipelined tensor-core blocks: a plan with two slots of device buffers.
+ * oskb_tc_plan_enqueue returns at once; it uploads the block's E
+ * ([station][source][2x2] FP32) and station uvw ([time][3][station]) from
+ * host memory on a copy-in stream, correlates the block (as
+ * oskb_correlate_block_tc, the visibility block cleared first) on a compute
+ * stream once the upload and the slot's previous download are done, and
+ * downloads the visibilities ([time][channel][baseline][2x2] FP64) group by
+ * group on a copy-out stream. So block b + 1's upload overlaps block b's
+ * correlation. Host buffers must stay valid until oskb_tc_plan_wait (they
+ * should be page-locked for the copies to overlap); the sky (l, m, n and
+ * Stokes, host arrays) is uploaded once by oskb_tc_plan_set_sky. */
+typedef struct oskb_TcPlan oskb_TcPlan;
+OSKB_API oskb_TcPlan* oskb_tc_plan_create(int casa, int num_sources,
+        int num_stations, int num_times, int num_channels,
+        const double* freqs_hz, double uv_min_lambda, double uv_max_lambda,
+        int* status);
+OSKB_API int oskb_tc_plan_set_sky(oskb_TcPlan* plan, const double* l,
+        const double* m, const double* n, const double* I, const double* Q,
+        const double* U, const double* V);
+OSKB_API int oskb_tc_plan_enqueue(oskb_TcPlan* plan, const float* E_host,
+        const double* station_uvw_host, double* vis_host);
+OSKB_API int oskb_tc_plan_wait(oskb_TcPlan* plan);
+OSKB_API void oskb_tc_plan_free(oskb_TcPlan* plan);
+
 /* Fused block: for every (time t, channel c) of a block,
  *   vis[t][c] += sum_s (K_p E_p C)(s) (K_q E_q C)(s)^H
  * with K_p(s) = exp(2 pi i (u_p l + v_p m + w_p (n - 1)) / lambda_c) formed

@@ -182,3 +182,222 @@ extern "C" int oskb_run_block_tc_host(int casa, int num_sources,
     }
     return 0;
 }
+
+// ---------------------------------------------------------------------------
+// Pipelined form: a plan with two slots of device buffers, so that the
+// upload of block b + 1 (on a copy-in stream) overlaps the correlation of
+// block b (compute stream), and block b's visibilities download group by
+// group on a copy-out stream. The sky is uploaded once per plan.
+// ---------------------------------------------------------------------------
+struct oskb_TcPlan
+{
+    int casa, num_src, num_st, num_times, num_channels;
+    double uv_min, uv_max;
+    size_t e_bytes, uvw_bytes, vis_bytes, problem_bytes;
+    double *sky, *wl;
+    struct Slot
+    {
+        void *E, *uvw, *vis;
+        cudaEvent_t uploaded, computed, downloaded;
+        bool used;
+    } slot[2];
+    cudaStream_t in, compute, out;
+    std::vector<cudaEvent_t> group_events;
+    size_t next_event;
+    int next_slot;
+    bool failed;
+};
+
+namespace {
+
+struct PlanHook
+{
+    oskb_TcPlan* p;
+    int slot;
+    double* host;
+};
+
+void plan_after_group(void* ctx, int p0, int np)
+{
+    PlanHook& h = *static_cast<PlanHook*>(ctx);
+    oskb_TcPlan* p = h.p;
+    if (p->next_event == p->group_events.size())
+    {
+        cudaEvent_t ev = nullptr;
+        if (cudaEventCreateWithFlags(&ev, cudaEventDisableTiming) !=
+                cudaSuccess)
+        {
+            p->failed = true;
+            return;
+        }
+        p->group_events.push_back(ev);
+    }
+    cudaEvent_t ev = p->group_events[p->next_event++];
+    cudaEventRecord(ev, p->compute);
+    cudaStreamWaitEvent(p->out, ev, 0);
+    const size_t off = (size_t) p0 * p->problem_bytes;
+    if (cudaMemcpyAsync(reinterpret_cast<char*>(h.host) + off,
+            static_cast<const char*>(p->slot[h.slot].vis) + off,
+            (size_t) np * p->problem_bytes, cudaMemcpyDeviceToHost, p->out)
+            != cudaSuccess)
+        p->failed = true;
+}
+
+}  // namespace
+
+extern "C" {
+
+void oskb_tc_plan_free(oskb_TcPlan* p)
+{
+    if (!p) return;
+    if (p->in) cudaStreamSynchronize(p->in);
+    if (p->compute) cudaStreamSynchronize(p->compute);
+    if (p->out) cudaStreamSynchronize(p->out);
+    for (auto& s : p->slot)
+    {
+        cudaFree(s.E); cudaFree(s.uvw); cudaFree(s.vis);
+        if (s.uploaded) cudaEventDestroy(s.uploaded);
+        if (s.computed) cudaEventDestroy(s.computed);
+        if (s.downloaded) cudaEventDestroy(s.downloaded);
+    }
+    for (cudaEvent_t e : p->group_events) cudaEventDestroy(e);
+    cudaFree(p->sky); cudaFree(p->wl);
+    if (p->in) cudaStreamDestroy(p->in);
+    if (p->compute) cudaStreamDestroy(p->compute);
+    if (p->out) cudaStreamDestroy(p->out);
+    delete p;
+}
+
+oskb_TcPlan* oskb_tc_plan_create(int casa, int num_sources, int num_stations,
+        int num_times, int num_channels, const double* freqs_hz,
+        double uv_min_lambda, double uv_max_lambda, int* status)
+{
+    if (*status) return nullptr;
+    if (num_sources < 1 || num_stations < 2 || num_times < 1 ||
+            num_channels < 1 || !freqs_hz)
+    {
+        *status = OSKB_ERR_INVALID_ARGUMENT;
+        return nullptr;
+    }
+    oskb_TcPlan* p = new oskb_TcPlan();
+    p->casa = casa; p->num_src = num_sources; p->num_st = num_stations;
+    p->num_times = num_times; p->num_channels = num_channels;
+    p->uv_min = uv_min_lambda; p->uv_max = uv_max_lambda;
+    const size_t nbl = (size_t) num_stations * (num_stations - 1) / 2;
+    p->problem_bytes = nbl * 64;
+    p->vis_bytes = (size_t) num_times * num_channels * p->problem_bytes;
+    p->e_bytes = (size_t) num_stations * num_sources * 8 * sizeof(float);
+    p->uvw_bytes = (size_t) num_times * 3 * num_stations * sizeof(double);
+    bool ok = cudaStreamCreateWithFlags(&p->in, cudaStreamNonBlocking) ==
+            cudaSuccess &&
+            cudaStreamCreateWithFlags(&p->compute, cudaStreamNonBlocking) ==
+            cudaSuccess &&
+            cudaStreamCreateWithFlags(&p->out, cudaStreamNonBlocking) ==
+            cudaSuccess &&
+            cudaMalloc((void**) &p->sky, 7 * sizeof(double) * num_sources) ==
+            cudaSuccess &&
+            cudaMalloc((void**) &p->wl, sizeof(double) * num_channels) ==
+            cudaSuccess;
+    for (auto& s : p->slot)
+        ok = ok && cudaMalloc(&s.E, p->e_bytes) == cudaSuccess &&
+                cudaMalloc(&s.uvw, p->uvw_bytes) == cudaSuccess &&
+                cudaMalloc(&s.vis, p->vis_bytes) == cudaSuccess &&
+                cudaEventCreateWithFlags(&s.uploaded,
+                cudaEventDisableTiming) == cudaSuccess &&
+                cudaEventCreateWithFlags(&s.computed,
+                cudaEventDisableTiming) == cudaSuccess &&
+                cudaEventCreateWithFlags(&s.downloaded,
+                cudaEventDisableTiming) == cudaSuccess;
+    if (ok)
+    {
+        std::vector<double> wl(num_channels);
+        for (int c = 0; c < num_channels; ++c)
+            wl[c] = freqs_hz[c] / 299792458.0;
+        ok = cudaMemcpy(p->wl, wl.data(), sizeof(double) * num_channels,
+                cudaMemcpyHostToDevice) == cudaSuccess;
+    }
+    if (!ok)
+    {
+        set_last_error("oskb_tc_plan_create", cudaGetLastError());
+        oskb_tc_plan_free(p);
+        *status = OSKB_ERR_MEMORY_ALLOC_FAILURE;
+        return nullptr;
+    }
+    return p;
+}
+
+int oskb_tc_plan_set_sky(oskb_TcPlan* p, const double* l, const double* m,
+        const double* n, const double* I, const double* Q, const double* U,
+        const double* V)
+{
+    const double* src[7] = {l, m, n, I, Q, U, V};
+    for (int k = 0; k < 7; ++k)
+    {
+        if (!src[k]) return OSKB_ERR_INVALID_ARGUMENT;
+        if (cudaMemcpy(p->sky + (size_t) k * p->num_src, src[k],
+                sizeof(double) * p->num_src, cudaMemcpyHostToDevice) !=
+                cudaSuccess)
+        {
+            set_last_error("oskb_tc_plan_set_sky", cudaGetLastError());
+            return OSKB_ERR_MEMORY_COPY_FAILURE;
+        }
+    }
+    return 0;
+}
+
+int oskb_tc_plan_enqueue(oskb_TcPlan* p, const float* E_host,
+        const double* station_uvw_host, double* vis_host)
+{
+    if (!E_host || !station_uvw_host || !vis_host)
+        return OSKB_ERR_INVALID_ARGUMENT;
+    const int k = p->next_slot;
+    p->next_slot ^= 1;
+    oskb_TcPlan::Slot& s = p->slot[k];
+    // upload: the slot's E and uvw are free once its last block computed
+    if (s.used) cudaStreamWaitEvent(p->in, s.computed, 0);
+    if (cudaMemcpyAsync(s.E, E_host, p->e_bytes, cudaMemcpyHostToDevice,
+            p->in) != cudaSuccess ||
+            cudaMemcpyAsync(s.uvw, station_uvw_host, p->uvw_bytes,
+            cudaMemcpyHostToDevice, p->in) != cudaSuccess)
+    {
+        set_last_error("oskb_tc_plan_enqueue", cudaGetLastError());
+        return OSKB_ERR_MEMORY_COPY_FAILURE;
+    }
+    cudaEventRecord(s.uploaded, p->in);
+    // compute: after the upload, and once the slot's visibilities of its
+    // last block have been downloaded
+    cudaStreamWaitEvent(p->compute, s.uploaded, 0);
+    if (s.used) cudaStreamWaitEvent(p->compute, s.downloaded, 0);
+    cudaMemsetAsync(s.vis, 0, p->vis_bytes, p->compute);
+    PlanHook hook{p, k, vis_host};
+    p->next_event = 0;
+    const double* sky = p->sky;
+    const size_t ns = p->num_src;
+    int err = tc::correlate_block(p->casa, p->num_src, p->num_st,
+            p->num_times, p->num_channels, static_cast<const float*>(s.E),
+            sky, sky + ns, sky + 2 * ns, sky + 3 * ns, sky + 4 * ns,
+            sky + 5 * ns, sky + 6 * ns, static_cast<const double*>(s.uvw),
+            p->wl, p->uv_min, p->uv_max, static_cast<double*>(s.vis), nullptr,
+            0, p->compute, plan_after_group, &hook);
+    cudaEventRecord(s.computed, p->compute);
+    cudaEventRecord(s.downloaded, p->out);
+    s.used = true;
+    if (err) return err;
+    return p->failed ? OSKB_ERR_MEMORY_COPY_FAILURE : 0;
+}
+
+int oskb_tc_plan_wait(oskb_TcPlan* p)
+{
+    const cudaError_t a = cudaStreamSynchronize(p->in);
+    const cudaError_t b = cudaStreamSynchronize(p->compute);
+    const cudaError_t c = cudaStreamSynchronize(p->out);
+    if (a != cudaSuccess || b != cudaSuccess || c != cudaSuccess ||
+            p->failed)
+    {
+        set_last_error("oskb_tc_plan_wait", cudaGetLastError());
+        return OSKB_ERR_KERNEL_LAUNCH_FAILURE;
+    }
+    return 0;
+}
+
+}  // extern "C"

@@ -104,6 +104,39 @@ def test_c1_host_block_driver():
     assert l2 <= 1e-6 and mx <= 1e-6, (l2, mx)
 
 
+def test_c1_pipelined_plan():
+    """The pipelined host-buffer plan: three blocks in flight (the c1
+    dumps split 4 + 4 + 2 would not share a shape, so each block is the
+    first 5 dumps with a different order of dumps), every block equal to
+    the golden visibilities of its dumps."""
+    import ctypes
+    g = load("c1_vis.npz")
+    nst, nsrc = g["ecef"].shape[1], g["l"].size
+    nbl = nst * (nst - 1) // 2
+    nt = 5
+    E = c1_identity_e(nst, nsrc, np.float32)
+    lib = ob.load()
+    st = ctypes.c_int(0)
+    freqs = np.array([float(g["freq"])])
+    plan = lib.oskb_tc_plan_create(0, nsrc, nst, nt, 1, freqs.ctypes.data,
+                                   0.0, 3e38, ctypes.addressof(st))
+    assert st.value == 0 and plan
+    try:
+        ob.call("oskb_tc_plan_set_sky", plan, *[np.ascontiguousarray(g[k])
+                                               for k in "l m n I Q U V".split()])
+        orders = [list(range(0, 5)), list(range(5, 10)), [9, 0, 4, 2, 7]]
+        uvws = [np.ascontiguousarray(g["uvw"][o]) for o in orders]
+        outs = [np.zeros((nt, 1, nbl, 8)) for _ in orders]
+        for u, o in zip(uvws, outs):
+            assert ob.call("oskb_tc_plan_enqueue", plan, E, u, o) == 0
+        assert ob.call("oskb_tc_plan_wait", plan) == 0
+        for o, order in zip(outs, orders):
+            l2, mx = rel_err(o[:, 0], g["vis"][order])
+            assert l2 <= 1e-6 and mx <= 1e-6, (order, l2, mx)
+    finally:
+        lib.oskb_tc_plan_free(plan)
+
+
 @pytest.mark.parametrize("matrix", [True, False])
 def test_smearing_gaussian(matrix):
     g = load("smear_vis.npz")
