@@ -683,6 +683,198 @@ xcorr_direct_kernel(const XcorrParams<T> prm)
     }  // items
 }
 
+// ---------------------------------------------------------------------------
+// FP64 tensor-core form for point sources without smearing (matrix, FP64):
+// the same staging (cp.async of the raw Jones, shared-to-shared transform
+// to the left factor J B and the right factor J), then the per-tile
+// product on the FP64 tensor pipe with mma.sync m8n8k4 f64 instead of SIMT
+// FMAs. Real embedding: with M = left factor (station p, rows) and
+// R = right factor (station q, columns), entries W[(s, i, c)][(src, k)] =
+// Re (c = 0) or Im (c = 1) of the 2x2 entry (i, k), and
+//     G = W_M W_R^T,  Re V_ij = G[(p,i,0)][(q,j,0)] + G[(p,i,1)][(q,j,1)],
+//                     Im V_ij = G[(p,i,1)][(q,j,0)] - G[(p,i,0)][(q,j,1)].
+// The 128 x 128 G tile of a 32 x 32 station tile is split over 8 warps as
+// 4 (rows) x 2 (columns) warp tiles of 32 x 64 = 4 x 8 m8n8 accumulators;
+// a k4 step is two sources. Accumulation is FP64 throughout (no
+// brightness factorisation, so any B).
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ void dmma_m8n8k4(double& d0, double& d1,
+        double a, double b)
+{
+    asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 "
+                 "{%0, %1}, {%2}, {%3}, {%0, %1};\n"
+                 : "+d"(d0), "+d"(d1) : "d"(a), "d"(b));
+}
+
+template <bool CASA>
+__global__ void __launch_bounds__(kThreads, 1)
+xcorr_dmma_kernel(const XcorrParams<double> prm)
+{
+    typedef double2 T2;
+    typedef Smem<double, true> S;
+    typedef Staging<double, true> G;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    S& sm = *reinterpret_cast<S*>(smem_raw);
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int wm = warp & 3, wn = warp >> 2;   // warp tile: rows, columns
+    const int g = lane >> 2, t = lane & 3;     // mma fragment coordinates
+    const int N = prm.num_st;
+    const long long nbl = (long long) N * (N - 1) / 2;
+    const int num_items = prm.tiles * prm.slices;
+
+    for (int item = blockIdx.x; item < num_items; item += gridDim.x)
+    {
+    ItemCtx ctx;
+    const int slice = item % prm.slices;
+    const int tile = item / prm.slices;
+    ctx.t = ctx.c = 0;
+    {
+        int bp, bq;
+        tri_block(tile, bp, bq);
+        ctx.p0 = bp * kTile;
+        ctx.q0 = bq * kTile;
+    }
+    ctx.src_begin = slice * prm.slice_len;
+    ctx.src_end = min(prm.num_src, ctx.src_begin + prm.slice_len);
+    __syncthreads();  // the previous item is done with shared memory
+    if (ctx.src_begin < ctx.src_end)
+        issue_chunk<double, true, false, false>(sm, prm, prm.jones, ctx,
+                ctx.src_begin);
+
+    double acc[4][8][2];
+#pragma unroll
+    for (int ms = 0; ms < 4; ++ms)
+#pragma unroll
+        for (int ns = 0; ns < 8; ++ns) acc[ms][ns][0] = acc[ms][ns][1] = 0.0;
+
+    for (int s0 = ctx.src_begin; s0 < ctx.src_end; s0 += kChunk)
+    {
+        cp_async_wait_all();
+        __syncthreads();
+        // ---- transform: left factor J B (rows unless CASA), right J
+        for (int it = tid; it < 2 * kTile * kChunk; it += kThreads)
+        {
+            const int blk = it / (kTile * kChunk);
+            const int rem = it - blk * (kTile * kChunk);
+            const int stl = rem % kTile, sl = rem / kTile;
+            double v[8];
+#pragma unroll
+            for (int pc = 0; pc < G::PIECES; ++pc)
+            {
+                const uint4 u = *reinterpret_cast<const uint4*>(
+                        sm.raw[blk][pc][sl][stl]);
+                memcpy(&v[2 * pc], &u, 16);
+            }
+            Mat2<double> J;
+            J.a = T2{v[0], v[1]}; J.b = T2{v[2], v[3]};
+            J.c = T2{v[4], v[5]}; J.d = T2{v[6], v[7]};
+            if ((blk == 0) != CASA)
+            {
+                const double I = sm.raw_src[kI][sl], Q = sm.raw_src[kQ][sl];
+                const T2 buv = T2{sm.raw_src[kU][sl], sm.raw_src[kV][sl]};
+                const T2 buvc = T2{buv.x, -buv.y};
+                const double xx = I + Q, yy = I - Q;
+                Mat2<double> M;
+                const T2 t0 = cmul<double>(J.b, buvc), t1 = cmul<double>(J.d, buvc);
+                const T2 t2 = cmul<double>(J.a, buv), t3 = cmul<double>(J.c, buv);
+                M.a = T2{J.a.x * xx + t0.x, J.a.y * xx + t0.y};
+                M.c = T2{J.c.x * xx + t1.x, J.c.y * xx + t1.y};
+                M.b = T2{J.b.x * yy + t2.x, J.b.y * yy + t2.y};
+                M.d = T2{J.d.x * yy + t3.x, J.d.y * yy + t3.y};
+                J = M;
+            }
+            // Fragment order: W entry (row r, k) of this block at
+            // frag[k / 4][r / 8][4 (r % 8) + k % 4], so the mma.sync
+            // operand of lane (g, t) = (r % 8, k % 4) is one consecutive
+            // 8-byte load per lane (row r = 4 stl + 2 i + c, k = 2 sl + kk).
+            double* frag = reinterpret_cast<double*>(blk ? &sm.col[0][0][0] :
+                    &sm.row[0][0][0]);
+            const T2 comp[4] = {J.a, J.b, J.c, J.d};
+#pragma unroll
+            for (int i = 0; i < 2; ++i)
+#pragma unroll
+                for (int kk = 0; kk < 2; ++kk)
+#pragma unroll
+                    for (int c = 0; c < 2; ++c)
+                    {
+                        const int r = 4 * stl + 2 * i + c, k = 2 * sl + kk;
+                        const T2 z = comp[2 * i + kk];
+                        frag[(k >> 2) * (kTile * 4 / 8) * 32 + (r >> 3) * 32 +
+                                4 * (r & 7) + (k & 3)] = c ? z.y : z.x;
+                    }
+        }
+        __syncthreads();
+        if (s0 + kChunk < ctx.src_end)
+            issue_chunk<double, true, false, false>(sm, prm, prm.jones, ctx,
+                    s0 + kChunk);
+
+        // ---- FP64 tensor-core products: 4 k4 steps of 2 sources
+#pragma unroll
+        for (int k4 = 0; k4 < kChunk / 2; ++k4)
+        {
+            const double* fa = reinterpret_cast<const double*>(
+                    &sm.row[0][0][0]) + k4 * (kTile * 4 / 8) * 32;
+            const double* fb = reinterpret_cast<const double*>(
+                    &sm.col[0][0][0]) + k4 * (kTile * 4 / 8) * 32;
+            double a[4], b[8];
+#pragma unroll
+            for (int ms = 0; ms < 4; ++ms)
+                a[ms] = fa[(4 * wm + ms) * 32 + lane];
+#pragma unroll
+            for (int ns = 0; ns < 8; ++ns)
+                b[ns] = fb[(8 * wn + ns) * 32 + lane];
+#pragma unroll
+            for (int ms = 0; ms < 4; ++ms)
+#pragma unroll
+                for (int ns = 0; ns < 8; ++ns)
+                    dmma_m8n8k4(acc[ms][ns][0], acc[ms][ns][1], a[ms],
+                            b[ns]);
+        }
+    }
+
+    // ---- visibilities: thread pairs (rows c = 0, 1: lanes l, l ^ 4) form
+    // Re (c = 0) and Im (c = 1) of V_ij for their (p, q, i, j)
+    const double kw = prm.inv_wavelength;
+    const double* su = prm.st_u;
+    const double* sv = prm.st_v;
+    const double uv_lo = prm.uv_min, uv_hi = prm.uv_max;
+#pragma unroll
+    for (int ms = 0; ms < 4; ++ms)
+#pragma unroll
+        for (int ns = 0; ns < 8; ++ns)
+        {
+            const double d0 = acc[ms][ns][0], d1 = acc[ms][ns][1];
+            const double other = __shfl_xor_sync(0xffffffffu, d1, 4);
+            const int r = 32 * wm + 8 * ms + g;
+            const int c = r & 1, i = (r >> 1) & 1;
+            const int p = ctx.p0 + (r >> 2);
+            const int n0 = 64 * wn + 8 * ns + 2 * t;
+            const int j = (n0 >> 1) & 1;
+            const int q = ctx.q0 + (n0 >> 2);
+            if (p >= N || q >= p) continue;
+            const double val = c ? d0 - other : d0 + other;
+            // V'_ji = conj(V_ij) in the CASA convention
+            const int e = CASA ? 2 * j + i : 2 * i + j;
+            const double out_val = (CASA && c) ? -val : val;
+            const double uu = (su[p] - su[q]) * kw;
+            const double vv = (sv[p] - sv[q]) * kw;
+            const double len = sqrt(uu * uu + vv * vv);
+            const bool ok = !(len < uv_lo || len > uv_hi);
+            const long long bl = baseline_index(N, p, q);
+            if (prm.partial)
+            {
+                prm.partial[(size_t) 8 * (slice * nbl + bl) + 2 * e + c] =
+                        ok ? out_val : 0.0;
+                continue;
+            }
+            if (!ok) continue;
+            double* o = prm.vis + (size_t) 8 * (bl + prm.offset_out) +
+                    2 * e + c;
+            *o += out_val;
+        }
+    }  // items
+}
+
 // Adds the slices' partial sums to the visibilities, in slice order.
 template <typename T>
 __global__ void __launch_bounds__(256)
@@ -744,6 +936,42 @@ void launch_variant(bool casa, bool gauss, bool bw, bool ts,
 #undef OSKB_L
 }
 
+// The FP64 tensor-core kernel can serve FP64 matrix point sources without
+// smearing when OSKB_XCORR_DMMA=1. It is off by default: with 8-source
+// chunks its per-chunk staging is not amortised and it runs at ~0.7x the
+// SIMT kernel (173 against 243 G source-baselines/s at 512 stations).
+template <typename T, bool MATRIX>
+bool use_dmma(bool gauss, bool bw, bool ts)
+{
+    if (sizeof(T) != 8 || !MATRIX || gauss || bw || ts) return false;
+    const char* e = getenv("OSKB_XCORR_DMMA");
+    return e && e[0] == '1';
+}
+
+template <typename T>
+void launch_dmma(bool casa, const XcorrParams<T>& p, int grid,
+        cudaStream_t stream)
+{
+    if constexpr (sizeof(T) == 8)
+    {
+        const size_t smem = sizeof(Smem<double, true>);
+        if (casa)
+        {
+            auto k = xcorr_dmma_kernel<true>;
+            cudaFuncSetAttribute(k,
+                    cudaFuncAttributeMaxDynamicSharedMemorySize, (int) smem);
+            k<<<grid, kThreads, smem, stream>>>(p);
+        }
+        else
+        {
+            auto k = xcorr_dmma_kernel<false>;
+            cudaFuncSetAttribute(k,
+                    cudaFuncAttributeMaxDynamicSharedMemorySize, (int) smem);
+            k<<<grid, kThreads, smem, stream>>>(p);
+        }
+    }
+}
+
 int tiles_for(int num_st)
 {
     const int nb = (num_st + kTile - 1) / kTile;
@@ -791,8 +1019,11 @@ int xcorr_dispatch(bool casa, bool gauss, XcorrParams<T> p,
             p.slice_len = p.num_src;
         }
     }
-    launch_variant<T, MATRIX, false>(casa, gauss, bw, ts, p,
-            tiles * slices, stream);
+    if (use_dmma<T, MATRIX>(gauss, bw, ts))
+        launch_dmma(casa, p, tiles * slices, stream);
+    else
+        launch_variant<T, MATRIX, false>(casa, gauss, bw, ts, p,
+                tiles * slices, stream);
     int err = check_launch("xcorr_direct");
     if (p.partial)
     {

@@ -125,6 +125,27 @@ def test_xcorr_slices_deterministic():
                           run_gpu_xcorr(c, np.float64))
 
 
+@pytest.mark.parametrize("casa", [0, 1])
+@pytest.mark.parametrize("slices", ["1", "4"])
+def test_xcorr_fp64_tensor_core_vs_simt(casa, slices, monkeypatch):
+    """FP64 point sources without smearing on the FP64 tensor pipe
+    (mma.sync f64, opt-in with OSKB_XCORR_DMMA=1) agree with the SIMT
+    kernel and the oracle to 1e-13, with the uv filter, an output offset
+    and slices."""
+    monkeypatch.setenv("OSKB_XCORR_SLICES", slices)
+    c = XcorrCase(75, 1003, casa=casa, uv_min=0.5, uv_max=1.2,
+                  offset_out=7, seed=5)
+    ref = run_oracle_xcorr(c, np.float64)
+    monkeypatch.setenv("OSKB_XCORR_DMMA", "1")
+    tc = run_gpu_xcorr(c, np.float64)
+    monkeypatch.setenv("OSKB_XCORR_DMMA", "0")
+    simt = run_gpu_xcorr(c, np.float64)
+    assert_close(tc, ref, np.float64, 1e-13)
+    assert_close(tc, simt, np.float64, 1e-13)
+    changed = np.any((tc != c.vis0).reshape(-1, 8), axis=1)
+    assert changed.any() and not changed.all()
+
+
 def test_xcorr_empty_inputs():
     c = XcorrCase(5, 4)
     vis = dev(c.vis0)
