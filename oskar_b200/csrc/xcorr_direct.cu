@@ -211,18 +211,21 @@ __device__ __forceinline__ void issue_chunk(Smem<T, MATRIX>& sm,
             cp_async(sm.raw[blk][pc][sl][stl], src, in, G::COPY);
         }
     }
-    // Per-source arrays: only those this variant reads.
-    const T* arrs[kNumSrcArr] = {prm.I, prm.Q, prm.U, prm.V, prm.l, prm.m,
-            prm.n, prm.a, prm.b, prm.c};
+    // Per-source arrays: only those this variant reads. (A select chain,
+    // not an array of pointers, which would live in local memory.)
     for (int it = tid; it < kNumSrcArr * kChunk; it += kThreads)
     {
         const int k = it / kChunk, sl = it % kChunk;
         const bool want = (k == kI) || (MATRIX && k <= kV) ||
                 (LMN && k >= kL && k <= kN) || (GAUSS && k >= kGa);
         if (!want) continue;
+        const T* arr = k == kI ? prm.I : k == kQ ? prm.Q : k == kU ? prm.U :
+                k == kV ? prm.V : k == kL ? prm.l : k == kM ? prm.m :
+                k == kN ? prm.n : k == kGa ? prm.a : k == kGb ? prm.b :
+                prm.c;
         const int s = s0 + sl;
         const bool in = s < src_end;
-        cp_async(&sm.raw_src[k][sl], in ? arrs[k] + s : arrs[kI], in,
+        cp_async(&sm.raw_src[k][sl], in ? arr + s : prm.I, in,
                 (int) sizeof(T));
     }
     cp_async_commit();
@@ -698,6 +701,22 @@ xcorr_direct_kernel(const XcorrParams<T> prm)
 // a k4 step is two sources. Accumulation is FP64 throughout (no
 // brightness factorisation, so any B).
 // ---------------------------------------------------------------------------
+// Fragment-ordered operands of one chunk: per block (rows, columns),
+// kChunk / 2 k4 steps x 16 tiles of 8 rows x kFragTile doubles. They live
+// in the shared-memory factor and phase areas, which this kernel does not
+// otherwise use (contiguous in Smem).
+constexpr int kFragTile = 33;
+constexpr int kFragK4 = (4 * kTile / 8) * kFragTile;
+constexpr int kFragBlock = (kChunk / 2) * kFragK4;
+static_assert(2 * kFragBlock * sizeof(double) <=
+        sizeof(Smem<double, true>::row) + sizeof(Smem<double, true>::col) +
+        sizeof(Smem<double, true>::ph), "fragment area exceeds its space");
+
+__device__ __forceinline__ double* fragment_base(Smem<double, true>& sm)
+{
+    return reinterpret_cast<double*>(&sm.row[0][0][0]);
+}
+
 __device__ __forceinline__ void dmma_m8n8k4(double& d0, double& d1,
         double a, double b)
 {
@@ -757,17 +776,11 @@ xcorr_dmma_kernel(const XcorrParams<double> prm)
             const int blk = it / (kTile * kChunk);
             const int rem = it - blk * (kTile * kChunk);
             const int stl = rem % kTile, sl = rem / kTile;
-            double v[8];
-#pragma unroll
-            for (int pc = 0; pc < G::PIECES; ++pc)
-            {
-                const uint4 u = *reinterpret_cast<const uint4*>(
-                        sm.raw[blk][pc][sl][stl]);
-                memcpy(&v[2 * pc], &u, 16);
-            }
             Mat2<double> J;
-            J.a = T2{v[0], v[1]}; J.b = T2{v[2], v[3]};
-            J.c = T2{v[4], v[5]}; J.d = T2{v[6], v[7]};
+            J.a = *reinterpret_cast<const T2*>(sm.raw[blk][0][sl][stl]);
+            J.b = *reinterpret_cast<const T2*>(sm.raw[blk][1][sl][stl]);
+            J.c = *reinterpret_cast<const T2*>(sm.raw[blk][2][sl][stl]);
+            J.d = *reinterpret_cast<const T2*>(sm.raw[blk][3][sl][stl]);
             if ((blk == 0) != CASA)
             {
                 const double I = sm.raw_src[kI][sl], Q = sm.raw_src[kQ][sl];
@@ -784,24 +797,22 @@ xcorr_dmma_kernel(const XcorrParams<double> prm)
                 J = M;
             }
             // Fragment order: W entry (row r, k) of this block at
-            // frag[k / 4][r / 8][4 (r % 8) + k % 4], so the mma.sync
-            // operand of lane (g, t) = (r % 8, k % 4) is one consecutive
-            // 8-byte load per lane (row r = 4 stl + 2 i + c, k = 2 sl + kk).
-            double* frag = reinterpret_cast<double*>(blk ? &sm.col[0][0][0] :
-                    &sm.row[0][0][0]);
-            const T2 comp[4] = {J.a, J.b, J.c, J.d};
-#pragma unroll
-            for (int i = 0; i < 2; ++i)
-#pragma unroll
-                for (int kk = 0; kk < 2; ++kk)
-#pragma unroll
-                    for (int c = 0; c < 2; ++c)
-                    {
-                        const int r = 4 * stl + 2 * i + c, k = 2 * sl + kk;
-                        const T2 z = comp[2 * i + kk];
-                        frag[(k >> 2) * (kTile * 4 / 8) * 32 + (r >> 3) * 32 +
-                                4 * (r & 7) + (k & 3)] = c ? z.y : z.x;
-                    }
+            // frag[k / 4][r / 8][4 (r % 8) + k % 4] (tiles of 8 rows padded
+            // to kFragTile doubles against bank conflicts of these stores),
+            // so the mma.sync operand of lane (g, t) = (r % 8, k % 4) is one
+            // consecutive 8-byte load per lane (row r = 4 stl + 2 i + c,
+            // k = 2 sl + kk).
+            double* frag = fragment_base(sm) + (blk ? kFragBlock : 0);
+#define OSKB_FRAG(I, KK, C, VAL)                                             \
+            frag[((2 * sl + KK) >> 2) * kFragK4 +                            \
+                    ((4 * stl + 2 * I + C) >> 3) * kFragTile +               \
+                    4 * ((4 * stl + 2 * I + C) & 7) + ((2 * sl + KK) & 3)] =  \
+                    VAL;
+            OSKB_FRAG(0, 0, 0, J.a.x) OSKB_FRAG(0, 0, 1, J.a.y)
+            OSKB_FRAG(0, 1, 0, J.b.x) OSKB_FRAG(0, 1, 1, J.b.y)
+            OSKB_FRAG(1, 0, 0, J.c.x) OSKB_FRAG(1, 0, 1, J.c.y)
+            OSKB_FRAG(1, 1, 0, J.d.x) OSKB_FRAG(1, 1, 1, J.d.y)
+#undef OSKB_FRAG
         }
         __syncthreads();
         if (s0 + kChunk < ctx.src_end)
@@ -812,17 +823,15 @@ xcorr_dmma_kernel(const XcorrParams<double> prm)
 #pragma unroll
         for (int k4 = 0; k4 < kChunk / 2; ++k4)
         {
-            const double* fa = reinterpret_cast<const double*>(
-                    &sm.row[0][0][0]) + k4 * (kTile * 4 / 8) * 32;
-            const double* fb = reinterpret_cast<const double*>(
-                    &sm.col[0][0][0]) + k4 * (kTile * 4 / 8) * 32;
+            const double* fa = fragment_base(sm) + k4 * kFragK4;
+            const double* fb = fa + kFragBlock;
             double a[4], b[8];
 #pragma unroll
             for (int ms = 0; ms < 4; ++ms)
-                a[ms] = fa[(4 * wm + ms) * 32 + lane];
+                a[ms] = fa[(4 * wm + ms) * kFragTile + lane];
 #pragma unroll
             for (int ns = 0; ns < 8; ++ns)
-                b[ns] = fb[(8 * wn + ns) * 32 + lane];
+                b[ns] = fb[(8 * wn + ns) * kFragTile + lane];
 #pragma unroll
             for (int ms = 0; ms < 4; ++ms)
 #pragma unroll
@@ -938,8 +947,9 @@ void launch_variant(bool casa, bool gauss, bool bw, bool ts,
 
 // The FP64 tensor-core kernel can serve FP64 matrix point sources without
 // smearing when OSKB_XCORR_DMMA=1. It is off by default: with 8-source
-// chunks its per-chunk staging is not amortised and it runs at ~0.7x the
-// SIMT kernel (173 against 243 G source-baselines/s at 512 stations).
+// chunks the shared staging, not the FP64 tensor pipe, bounds both forms,
+// and they run at the same speed (261 and 258 G source-baselines/s at 512
+// stations x 100,000 sources).
 template <typename T, bool MATRIX>
 bool use_dmma(bool gauss, bool bw, bool ts)
 {
