@@ -823,6 +823,139 @@ def run_c2(args):
     return 0
 
 
+def c4_sky(rng, num_chunks=32):
+    """Sky of the batched-smearing configuration: chunk sizes log-uniform on
+    [500, 50,000] sources; 30 % of sources Gaussian (FWHM major and minor
+    uniform in [1, 60] arcsec, position angle uniform in [0, pi)), the rest
+    points; a chunk holding any Gaussian is a Gaussian chunk, as the
+    reference groups its sky (oskar_sky_append_to_set.c:119), and its point
+    sources have a = b = c = 0. Gaussian coefficients as the reference forms
+    them (sky/src/oskar_sky_evaluate_gaussian_source_parameters.c:171-178:
+    0.5 FWHM^2 pi^2 / (2 ln 2) along each axis, rotated by the angle)."""
+    sizes = np.exp(rng.uniform(math.log(500), math.log(50_000),
+                               num_chunks)).astype(int)
+    ns = int(sizes.sum())
+    r = np.sqrt(rng.uniform(0, 1, ns)) * math.sin(math.radians(5))
+    th = rng.uniform(0, 2 * math.pi, ns)
+    l, m = r * np.cos(th), r * np.sin(th)
+    n = np.sqrt(1 - l * l - m * m)
+    I = np.exp(rng.uniform(math.log(0.01), math.log(10.0), ns))
+    Q, U, V = (I * rng.uniform(-0.1, 0.1, ns) for _ in range(3))
+    gauss = rng.uniform(0, 1, ns) < 0.3
+    arcsec = math.pi / 180 / 3600
+    maj = rng.uniform(1, 60, ns) * arcsec
+    mnr = np.minimum(maj, rng.uniform(1, 60, ns) * arcsec)
+    pa = rng.uniform(0, math.pi, ns)
+    k = math.pi ** 2 / (2 * math.log(2))
+    imaj, imin = 0.5 * maj ** 2 * k, 0.5 * mnr ** 2 * k
+    cp2, sp2, s2p = np.cos(pa) ** 2, np.sin(pa) ** 2, np.sin(2 * pa)
+    a = cp2 * imin + sp2 * imaj
+    b = -s2p * imin * 0.5 + s2p * imaj * 0.5
+    c = sp2 * imin + cp2 * imaj
+    for g in (a, b, c):
+        g[~gauss] = 0.0
+    return sizes, dict(l=l, m=m, n=n, I=I, Q=Q, U=U, V=V, a=a, b=b, c=c)
+
+
+def run_c4(args):
+    """Batched blocks with smearing: 256 stations (32,640 baselines), a sky
+    in uneven chunks (log-uniform 500-50,000 sources, 30 % Gaussian),
+    channels of 100 kHz, 10 s time averaging, FP64. The measured step is a
+    bounded block: 1 dump x 4 channels x the first chunks (about 10,000
+    sources) through the block plan (one graph per block: upload, clear, one
+    persistent launch with K fused, download). The reference's OpenMP
+    Gaussian/smearing kernel is timed on 200 sources beside it."""
+    import ctypes
+    import torch
+    import oskar_b200 as ob
+    from oskar_b200 import workloads
+    torch.cuda.set_device(0)
+    rng = np.random.default_rng(4)
+    st = workloads.c3(num_src=1, num_st=256, num_channels=1, num_times=16)
+    sizes, sky = c4_sky(rng)
+    keep = int(np.searchsorted(np.cumsum(sizes), 10_000)) + 1
+    ns = int(np.sum(sizes[:keep]))
+    sky = {k: np.ascontiguousarray(v[:ns]) for k, v in sky.items()}
+    N, C, T = st.num_st, 4, 1
+    nbl = N * (N - 1) // 2
+    freqs = 100e6 + 1e5 * np.arange(C)
+    x, y = (np.ascontiguousarray(a) for a in st.ecef[:2])
+    E = rng.normal(0, 0.1, (N, ns, 8))
+    E[..., 0] += 1
+    E[..., 6] += 1
+    lib = ob.load()
+    status = ctypes.c_int(0)
+    plan = lib.oskb_block_plan_create(8, 0, N, ns, T, C, 1, 1, 0,
+                                      freqs.ctypes.data, 1e5, 10.0,
+                                      st.dec0, 0.0, 3e38, 0, 0.0, 3e38,
+                                      ctypes.addressof(status))
+    if status.value or not plan:
+        raise RuntimeError("oskb_block_plan_create failed")
+    ob.call("oskb_block_plan_set_sky", plan, *[sky[k] for k in
+                                               "I Q U V l m n a b c".split()])
+    ob.call("oskb_block_plan_set_stations", plan, x, y)
+    ob.call("oskb_block_plan_set_beam", plan, np.ascontiguousarray(E))
+
+    def host(ptr, count, dtype=np.float64):
+        buf = (ctypes.c_double * count).from_address(ptr)
+        return np.frombuffer(buf, dtype=dtype)
+    uvw_h = host(lib.oskb_block_plan_host_uvw(plan), T * 3 * N)
+    gha_h = host(lib.oskb_block_plan_host_gha0(plan), T)
+
+    def block(t):
+        uvw_h[:] = st.station_uvw(t).ravel()
+        gha_h[:] = [st.gast(t) - st.ra0]
+        ob.call("oskb_block_plan_execute", plan)
+        ob.call("oskb_block_plan_synchronize", plan)
+    for i in range(args.warmup):
+        block(i)
+    t0 = time.perf_counter()
+    for i in range(args.steps):
+        block(args.warmup + i)
+    dt = (time.perf_counter() - t0) / args.steps
+    graphs = lib.oskb_block_plan_graph_launches(plan)
+    buf = ctypes.create_string_buffer(4096)
+    ob.call("oskb_block_tune_report", ctypes.addressof(buf), 4096,
+            check=False)
+    lib.oskb_block_plan_free(plan)
+    work = nbl * ns * C * T
+    # reference CPU: Gaussian + bandwidth + time smearing, one channel
+    nc = 200
+    ref = ref_lib()
+    cpu = None
+    if ref is not None:
+        D = ctypes.c_double
+        u, v, w = (np.ascontiguousarray(a) for a in st.station_uvw(0))
+        J = np.ascontiguousarray(E[:, :nc].reshape(N, nc, 8))
+        vis = np.zeros((nbl, 8))
+        cs = {k: np.ascontiguousarray(sky[k][:nc]) for k in sky}
+        t1 = time.perf_counter()
+        ref.oskar_cross_correlate_gaussian_omp_d(
+            0, nc, N, 0, _p(J), _p(cs["I"]), _p(cs["Q"]), _p(cs["U"]),
+            _p(cs["V"]), _p(cs["l"]), _p(cs["m"]), _p(cs["n"]), _p(cs["a"]),
+            _p(cs["b"]), _p(cs["c"]), _p(u), _p(v), _p(w), _p(x), _p(y),
+            D(0.0), D(3e38), D(freqs[0] / 299792458.0), D(1e5 / freqs[0]),
+            D(10.0), D(st.gast(0) - st.ra0), D(st.dec0), _p(vis))
+        cpu = nbl * nc / (time.perf_counter() - t1) / 1e9
+    print(json.dumps({
+        "workload": "c4: 256 stations, %d sources in %d uneven chunks "
+                    "(log-uniform 500-50,000; 30%% Gaussian), 1 dump x %d "
+                    "channels of 100 kHz, 10 s averaging, bandwidth and "
+                    "time smearing, FP64 E per station-source" % (ns, keep, C),
+        "metric": "G source-baselines/s through the block plan",
+        "value": work / dt / 1e9, "unit": "G source-baselines/s",
+        "ms_per_step": dt * 1e3, "steps": args.steps, "warmup": args.warmup,
+        "graph_replays": graphs,
+        "schedule": buf.value.decode().strip(),
+        "cpu_baseline": {"value": cpu, "unit": "G source-baselines/s",
+                         "cores": cpu_cores(), "kind": "reference",
+                         "sample": "oskar_cross_correlate_gaussian_omp_d "
+                                   "with both smearings, 1 channel x %d "
+                                   "sources x %d baselines" % (nc, nbl)},
+    }))
+    return 0
+
+
 def run_c5(args):
     """Learned station-beam surrogate against the exact station beam, one
     step = the Jones E of every station for every source at one (dump,
@@ -980,7 +1113,8 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--path", default="tc", choices=["tc", "direct"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--workload", default="c3", choices=["c3", "c2", "c5"],
+    ap.add_argument("--workload", default="c3",
+                    choices=["c3", "c2", "c4", "c5"],
                     help="c2: the aperture-array beam chain; c5: the learned "
                          "station-beam surrogate")
     ap.add_argument("--c5-steps", type=int, default=20000)
@@ -996,6 +1130,8 @@ def main():
         return run_c5(args)
     if args.workload == "c2":
         return run_c2(args)
+    if args.workload == "c4":
+        return run_c4(args)
     os.environ.setdefault("OMP_NUM_THREADS", str(cpu_cores()))
     if args.impl == "reference":
         return run_reference(args)
