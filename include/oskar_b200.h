@@ -306,6 +306,81 @@ OSKB_API int oskb_convert_station_uvw_to_baseline_uvw_f(int use_casa,
         const float* w, int offset_out, float* uu, float* vv, float* ww,
         void* stream);
 
+/* Scaled Stokes I, Q, U, V of every source at freq_hz from the spectral
+ * columns of a sky table: the reference channel nearest freq_hz, Q and U
+ * from polarisation angle and fraction where only those are given, then
+ * Gaussian line profiles, a curved power law, or a logarithmic or linear
+ * spectral-index polynomial for I (Q, U, V follow I's ratio), or Faraday
+ * rotation with a rotation measure. NaN coefficients count as 0; a source
+ * whose nearest reference frequency is 0 keeps its values.
+ * The arguments are those of the reference's kernel
+ * (sky/src/oskar_sky_scale_flux_with_frequency.c:165-189, body
+ * sky/define_sky_scale_flux_with_frequency.h:89-253), plus num_columns:
+ * the table holds num_columns columns of capacity values (column k of
+ * source s at table[capacity * k + s]); num_valid_columns is
+ * [source][20] counts per column type (sky/oskar_sky_enum.h:14-35); a
+ * col_ argument is the first column of its type, -1 if absent; a column
+ * index outside [0, num_columns) reads as 0. col_i < 0 is
+ * OSKB_ERR_INVALID_ARGUMENT (the reference's "no Stokes I column",
+ * oskar_sky_scale_flux_with_frequency.c:57-62). All arrays on the device. */
+OSKB_API int oskb_sky_scale_flux_with_frequency_d(int num_sources,
+        int capacity, int num_columns, double freq_hz, const double* table,
+        const int* num_valid_columns, int col_i, int col_q, int col_u,
+        int col_v, int col_ref_freq, int col_lin_sp_index, int col_sp_index,
+        int col_rot_meas, int col_pol_frac, int col_pol_ang,
+        int col_ref_wavelength, int col_sp_curvature, int col_line_width,
+        int col_freq_inc, double* out_i, double* out_q, double* out_u,
+        double* out_v, void* stream);
+OSKB_API int oskb_sky_scale_flux_with_frequency_f(int num_sources,
+        int capacity, int num_columns, float freq_hz, const float* table,
+        const int* num_valid_columns, int col_i, int col_q, int col_u,
+        int col_v, int col_ref_freq, int col_lin_sp_index, int col_sp_index,
+        int col_rot_meas, int col_pol_frac, int col_pol_ang,
+        int col_ref_wavelength, int col_sp_curvature, int col_line_width,
+        int col_freq_inc, float* out_i, float* out_q, float* out_u,
+        float* out_v, void* stream);
+/* The same for every channel of a band in one launch: frequency_hz is a
+ * device array [num_channels]; columns is a host array of the 14 first
+ * columns in the order of the col_ arguments above; outputs are
+ * [channel][source], channel c at c * out_channel_stride
+ * (>= num_sources when num_channels > 1). The FP32 variant rounds each
+ * frequency to float, as the reference's FP32 kernel receives it. */
+OSKB_API int oskb_sky_scale_flux_channels_d(int num_sources, int capacity,
+        int num_columns, int num_channels, const double* frequency_hz,
+        const double* table, const int* num_valid_columns,
+        const int* columns, long long out_channel_stride, double* out_i,
+        double* out_q, double* out_u, double* out_v, void* stream);
+OSKB_API int oskb_sky_scale_flux_channels_f(int num_sources, int capacity,
+        int num_columns, int num_channels, const double* frequency_hz,
+        const float* table, const int* num_valid_columns,
+        const int* columns, long long out_channel_stride, float* out_i,
+        float* out_q, float* out_u, float* out_v, void* stream);
+
+/* Cable-length phase errors applied in place to Jones [station][source]:
+ * J <- diag(e^{i k dx_p}, e^{i k dy_p}) J for matrix Jones (matrix != 0;
+ * an absent array keeps gain 1), J <- e^{i k dx_p} J for scalar Jones
+ * (nothing without errors_x); wavenumber k = 2 pi f / c
+ * (interferometer/define_jones_apply_cable_length_errors.h:3-74, called
+ * from interferometer/src/oskar_jones_apply_cable_length_errors.c:23-141).
+ * errors_x, errors_y: [station] metres, device, either may be NULL. */
+OSKB_API int oskb_jones_apply_cable_length_errors_d(int matrix,
+        int num_sources, int num_stations, double wavenumber,
+        const double* errors_x, const double* errors_y, double* jones,
+        void* stream);
+OSKB_API int oskb_jones_apply_cable_length_errors_f(int matrix,
+        int num_sources, int num_stations, float wavenumber,
+        const float* errors_x, const float* errors_y, float* jones,
+        void* stream);
+/* Station gains applied in place: J[p][s] <- G_p J[p][s], G_p a 2x2
+ * complex matrix (matrix != 0) or a complex scalar
+ * (interferometer/define_jones_apply_station_gains.h:3-45, called from
+ * interferometer/src/oskar_jones_apply_station_gains.c:23-121). gains:
+ * [station], device. */
+OSKB_API int oskb_jones_apply_station_gains_d(int matrix, int num_sources,
+        int num_stations, const double* gains, double* jones, void* stream);
+OSKB_API int oskb_jones_apply_station_gains_f(int matrix, int num_sources,
+        int num_stations, const float* gains, float* jones, void* stream);
+
 /* ------------------------------------------------------------------------
  * Learned station-beam surrogate.
  * ------------------------------------------------------------------------

@@ -125,6 +125,15 @@ OSKB_API void oskar_auto_correlate(int num_sources, const oskar_Jones* jones,
 /* oskar/interferometer/oskar_jones_join.h:69 */
 OSKB_API void oskar_jones_join(oskar_Jones* j3, oskar_Jones* j1,
         const oskar_Jones* j2, int* status);
+/* oskar/interferometer/oskar_jones_apply_cable_length_errors.h:37-43.
+ * The error arrays must match the Jones array's precision and location. */
+OSKB_API void oskar_jones_apply_cable_length_errors(oskar_Jones* jones,
+        double frequency_hz, const oskar_Mem* errors_x,
+        const oskar_Mem* errors_y, int* status);
+/* oskar/interferometer/oskar_jones_apply_station_gains.h:32-36. The gains
+ * must match the Jones array's type and location. */
+OSKB_API void oskar_jones_apply_station_gains(oskar_Jones* jones,
+        oskar_Mem* gains, int* status);
 /* oskar/mem/oskar_mem_multiply.h:63 */
 OSKB_API void oskar_mem_multiply(oskar_Mem* out, const oskar_Mem* in1,
         const oskar_Mem* in2, size_t offset_out, size_t offset_in1,

@@ -90,7 +90,20 @@ void orc_station_beam_aa_##S(int num_el, const REAL* x, const REAL* y, \
         int norm_array, int norm_final, int swap_xy, int is_3d, \
         double frequency_hz, double bx, double by, double bz, double nx, \
         double ny, double nz, int num_dir, const REAL* dx, const REAL* dy, \
-        const REAL* dz, REAL* beam);
+        const REAL* dz, REAL* beam); \
+void orc_sky_scale_flux_##S(int num_sources, int capacity, \
+        int num_columns, REAL freq_hz, const REAL* table, \
+        const int* num_valid, int col_i, int col_q, int col_u, int col_v, \
+        int col_ref_freq, int col_lin_sp_index, int col_sp_index, \
+        int col_rot_meas, int col_pol_frac, int col_pol_ang, \
+        int col_ref_wavelength, int col_sp_curvature, int col_line_width, \
+        int col_freq_inc, REAL* out_i, REAL* out_q, REAL* out_u, \
+        REAL* out_v); \
+void orc_cable_length_errors_##S(int matrix, int num_sources, \
+        int num_stations, REAL wavenumber, const REAL* errors_x, \
+        const REAL* errors_y, REAL* jones); \
+void orc_station_gains_##S(int matrix, int num_sources, int num_stations, \
+        const REAL* gains, REAL* jones);
 
 ORC_DECLARE(double, d)
 ORC_DECLARE(float, f)

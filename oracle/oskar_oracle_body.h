@@ -798,3 +798,322 @@ void ORC_FN(orc_station_uvw_to_baseline_uvw)(int casa, int num,
             ww[b] = f * (w[s2 + offset_in] - w[s1 + offset_in]);
         }
 }
+
+/* ---- Sky flux scaling with frequency ----
+ * The sky table is column-major: column k of source s at
+ * table[capacity * k + s]; columns of one type are adjacent, in index order.
+ * num_valid[s * 20 + type] counts the columns of each type that hold data
+ * for source s. Type numbers follow the reference's column enumeration
+ * (sky/oskar_sky_enum.h:14-35): I 3, Q 4, U 5, V 6, reference frequency 7,
+ * spectral index 8, rotation measure 9, linear-index flag 13, polarisation
+ * angle 14, polarisation fraction 15, reference wavelength 16, spectral
+ * curvature 17, line width 18, frequency increment 19; 20 types in all.
+ * A column index outside [0, num_columns) reads as 0 (the reference reads
+ * past its table there). */
+#ifndef ORC_SKY_ENUM_
+#define ORC_SKY_ENUM_
+enum { ORC_SKY_I = 3, ORC_SKY_Q = 4, ORC_SKY_U = 5, ORC_SKY_V = 6,
+    ORC_SKY_REF_HZ = 7, ORC_SKY_SPX = 8, ORC_SKY_RM = 9, ORC_SKY_LIN_SI = 13,
+    ORC_SKY_POLA = 14, ORC_SKY_POLF = 15, ORC_SKY_REF_WAVE = 16,
+    ORC_SKY_CURV = 17, ORC_SKY_LINE_WIDTH = 18, ORC_SKY_INC_HZ = 19,
+    ORC_SKY_NUM_TYPES = 20 };
+#define ORC_C0_M_PER_S 299792458
+/* slots of the column table below */
+enum { ORC_CI = 0, ORC_CQ, ORC_CU, ORC_CV, ORC_CREF, ORC_CLIN, ORC_CSPX,
+    ORC_CRM, ORC_CPOLF, ORC_CPOLA, ORC_CREFW, ORC_CCURV, ORC_CLW, ORC_CINC };
+#endif
+
+typedef struct
+{
+    const REAL* table;
+    int capacity, num_columns;
+    /* first column of: I Q U V ref_hz lin_si spx rm polf pola ref_wave curv
+     * line_width inc_hz */
+    int col[14];
+} ORC_T(sky);
+
+
+static REAL ORC_T(sky_at)(const ORC_T(sky)* k, int column, int s)
+{
+    if (column < 0 || column >= k->num_columns) return 0;
+    return k->table[(size_t) k->capacity * column + s];
+}
+
+static REAL ORC_T(nan0)(REAL x) { return x != x ? (REAL) 0 : x; }
+
+/* Stokes I of source s at freq_hz, given its value i_in at freq0_hz
+ * (sky/define_sky_scale_flux_with_frequency.h:5-86): a sum of Gaussian line
+ * profiles when line widths are given; the value unchanged when several I
+ * columns are given; a curved power law (Callingham et al. 2017, eq. 2)
+ * when a curvature is given; else the logarithmic spectral-index polynomial
+ * (the default) or the linear one, both by Horner's rule. NaN coefficients
+ * count as 0. Math in double, as the reference's C build computes it. */
+static REAL ORC_T(stokes_i_at)(const ORC_T(sky)* k, const int* nv, int s,
+        REAL i_in, REAL freq_hz, REAL freq0_hz)
+{
+    int c;
+    const int n_i = nv[ORC_SKY_I], n_lw = nv[ORC_SKY_LINE_WIDTH];
+    const int n_spx = nv[ORC_SKY_SPX];
+    if (n_lw > 0)
+    {
+        const int n_ref = nv[ORC_SKY_REF_HZ];
+        const REAL inc = nv[ORC_SKY_INC_HZ] > 0 ?
+                ORC_T(sky_at)(k, k->col[ORC_CINC], s) : (REAL) 0;
+        REAL sum = 0;
+        for (c = 0; c < n_i; ++c)
+        {
+            const REAL amp = ORC_T(sky_at)(k, k->col[ORC_CI] + c, s);
+            const REAL ref = c < n_ref ?
+                    ORC_T(sky_at)(k, k->col[ORC_CREF] + c, s) :
+                    ORC_T(sky_at)(k, k->col[ORC_CREF], s) + c * inc;
+            const REAL sigma = ORC_T(sky_at)(k,
+                    k->col[ORC_CLW] + (c < n_lw ? c : 0), s);
+            const REAL x = freq_hz - ref;
+            sum += amp * exp(-(x * x) / (2 * sigma * sigma));
+        }
+        return sum;
+    }
+    if (n_i > 1) return i_in;
+    if (nv[ORC_SKY_CURV] > 0)
+    {
+        const REAL spx = n_spx > 0 ?
+                ORC_T(nan0)(ORC_T(sky_at)(k, k->col[ORC_CSPX], s)) : 0;
+        const REAL curv_coef = ORC_T(nan0)(
+                ORC_T(sky_at)(k, k->col[ORC_CCURV], s));
+        const REAL ratio = freq_hz / freq0_hz;
+        const REAL lr = (REAL) log(ratio);
+        const REAL curv = (REAL) exp(curv_coef * (lr * lr));
+        return (REAL) (i_in * curv * pow(ratio, spx));
+    }
+    {
+        const REAL lin = nv[ORC_SKY_LIN_SI] > 0 ?
+                ORC_T(sky_at)(k, k->col[ORC_CLIN], s) : (REAL) 0;
+        REAL acc = 0;
+        if (lin == (REAL) 0)
+        {
+            const REAL base = (REAL) log10(freq_hz / freq0_hz);
+            for (c = n_spx - 1; c >= 0; --c)
+                acc = base * acc + ORC_T(nan0)(
+                        ORC_T(sky_at)(k, k->col[ORC_CSPX] + c, s));
+            return (REAL) (i_in * pow((REAL) 10, base * acc));
+        }
+        {
+            const REAL base = freq_hz / freq0_hz - (REAL) 1;
+            for (c = n_spx - 1; c >= 0; --c)
+                acc = base * acc + ORC_T(nan0)(
+                        ORC_T(sky_at)(k, k->col[ORC_CSPX] + c, s));
+            return i_in + base * acc;
+        }
+    }
+}
+
+/* Scaled I, Q, U, V of every source at freq_hz
+ * (sky/define_sky_scale_flux_with_frequency.h:89-253): the reference
+ * channel nearest freq_hz, its Stokes values, Q and U from polarisation
+ * angle and fraction where only those are given, then spectral scaling of
+ * I (Q, U, V follow I's ratio) or, with a rotation measure, Faraday
+ * rotation of the polarisation angle. Column arguments in the reference
+ * kernel's order. */
+void ORC_FN(orc_sky_scale_flux)(int num_sources, int capacity,
+        int num_columns, REAL freq_hz, const REAL* table,
+        const int* num_valid, int col_i, int col_q, int col_u, int col_v,
+        int col_ref_freq, int col_lin_sp_index, int col_sp_index,
+        int col_rot_meas, int col_pol_frac, int col_pol_ang,
+        int col_ref_wavelength, int col_sp_curvature, int col_line_width,
+        int col_freq_inc, REAL* out_i, REAL* out_q, REAL* out_u,
+        REAL* out_v)
+{
+    ORC_T(sky) k;
+    int s;
+    k.table = table;
+    k.capacity = capacity;
+    k.num_columns = num_columns;
+    k.col[ORC_CI] = col_i; k.col[ORC_CQ] = col_q; k.col[ORC_CU] = col_u;
+    k.col[ORC_CV] = col_v; k.col[ORC_CREF] = col_ref_freq;
+    k.col[ORC_CLIN] = col_lin_sp_index; k.col[ORC_CSPX] = col_sp_index;
+    k.col[ORC_CRM] = col_rot_meas; k.col[ORC_CPOLF] = col_pol_frac;
+    k.col[ORC_CPOLA] = col_pol_ang; k.col[ORC_CREFW] = col_ref_wavelength;
+    k.col[ORC_CCURV] = col_sp_curvature; k.col[ORC_CLW] = col_line_width;
+    k.col[ORC_CINC] = col_freq_inc;
+    for (s = 0; s < num_sources; ++s)
+    {
+        const int* nv = num_valid + (size_t) s * ORC_SKY_NUM_TYPES;
+        const int n_i = nv[ORC_SKY_I];
+        const int n_ref = nv[ORC_SKY_REF_HZ], n_inc = nv[ORC_SKY_INC_HZ];
+        const int n_pola = nv[ORC_SKY_POLA], n_polf = nv[ORC_SKY_POLF];
+        REAL iquv[4] = {0, 0, 0, 0}, diff = (REAL) 1e38, f0 = 0;
+        int j, chan = 0;
+        /* nearest reference channel */
+        for (j = 0; j < n_i; ++j)
+        {
+            const REAL tf = (n_inc == 1 && n_ref == 1) ?
+                    ORC_T(sky_at)(&k, col_ref_freq, s) +
+                    j * ORC_T(sky_at)(&k, col_freq_inc, s) :
+                    ORC_T(sky_at)(&k, col_ref_freq + j, s);
+            const REAL d = (REAL) fabs(tf - freq_hz);
+            if (d < diff)
+            {
+                diff = d;
+                chan = j;
+                f0 = tf;
+            }
+        }
+        for (j = 0; j < 4; ++j)
+        {
+            const int n = nv[ORC_SKY_I + j];
+            if (n > 0)
+                iquv[j] = ORC_T(sky_at)(&k, k.col[ORC_CI + j] +
+                        (chan < n ? chan : 0), s);
+            iquv[j] = ORC_T(nan0)(iquv[j]);
+        }
+        if (n_pola > 0 && n_polf > 0 && (nv[ORC_SKY_Q] <= 0 ||
+                nv[ORC_SKY_U] <= 0))
+        {
+            const REAL ang = ORC_T(sky_at)(&k, col_pol_ang +
+                    (chan < n_pola ? chan : 0), s);
+            const REAL frac = ORC_T(sky_at)(&k, col_pol_frac +
+                    (chan < n_polf ? chan : 0), s);
+            const REAL sn = (REAL) sin(2 * ang), cs = (REAL) cos(2 * ang);
+            iquv[1] = frac * iquv[0] * cs;
+            iquv[2] = frac * iquv[0] * sn;
+        }
+        if (f0 == (REAL) 0)
+        {
+            out_i[s] = iquv[0]; out_q[s] = iquv[1];
+            out_u[s] = iquv[2]; out_v[s] = iquv[3];
+            continue;
+        }
+        {
+            const REAL i_out = ORC_T(stokes_i_at)(&k, nv, s, iquv[0],
+                    freq_hz, f0);
+            const REAL scale = iquv[0] != (REAL) 0 ? i_out / iquv[0] : 0;
+            if (nv[ORC_SKY_RM] > 0)
+            {
+                const REAL rm = ORC_T(nan0)(
+                        ORC_T(sky_at)(&k, col_rot_meas, s));
+                const REAL lambda = ((REAL) ORC_C0_M_PER_S) / freq_hz;
+                REAL chi0, frac;
+                if (n_pola <= 0 || n_polf <= 0)
+                {
+                    const REAL lambda0 = nv[ORC_SKY_REF_WAVE] > 0 ?
+                            ORC_T(sky_at)(&k, col_ref_wavelength, s) :
+                            ((REAL) ORC_C0_M_PER_S) / f0;
+                    const REAL f_lambda0 = ((REAL) ORC_C0_M_PER_S) / lambda0;
+                    const REAL i_ref = ORC_T(stokes_i_at)(&k, nv, s,
+                            iquv[0], freq_hz, f_lambda0);
+                    chi0 = (REAL) 0.5 * (REAL) atan2(iquv[2], iquv[1]) -
+                            lambda0 * lambda0 * rm;
+                    frac = (REAL) sqrt(iquv[1] * iquv[1] +
+                            iquv[2] * iquv[2]) / i_ref;
+                }
+                else
+                {
+                    chi0 = ORC_T(sky_at)(&k, col_pol_ang +
+                            (chan < n_pola ? chan : 0), s);
+                    frac = ORC_T(sky_at)(&k, col_pol_frac +
+                            (chan < n_polf ? chan : 0), s);
+                }
+                {
+                    const REAL chi = chi0 + rm * (lambda * lambda);
+                    out_q[s] = frac * i_out * (REAL) cos(2 * chi);
+                    out_u[s] = frac * i_out * (REAL) sin(2 * chi);
+                }
+            }
+            else
+            {
+                out_q[s] = scale * iquv[1];
+                out_u[s] = scale * iquv[2];
+            }
+            out_i[s] = i_out;
+            out_v[s] = scale * iquv[3];
+        }
+    }
+}
+
+/* Cable-length phase per station: J[p][s] <- diag(e^{i k dx_p},
+ * e^{i k dy_p}) J[p][s] for a matrix Jones (an absent polarisation keeps
+ * gain 1), J[p][s] <- e^{i k dx_p} J[p][s] for a scalar Jones (nothing
+ * without x errors); k = 2 pi f / c
+ * (interferometer/define_jones_apply_cable_length_errors.h:3-74). */
+void ORC_FN(orc_cable_length_errors)(int matrix, int num_sources,
+        int num_stations, REAL wavenumber, const REAL* errors_x,
+        const REAL* errors_y, REAL* jones)
+{
+    int p, s;
+    for (p = 0; p < num_stations; ++p)
+    {
+        ORC_T(cx) gx = {1, 0}, gy = {1, 0};
+        if (errors_x)
+        {
+            const REAL ph = wavenumber * errors_x[p];
+            gx.re = ORC_COS(ph);
+            gx.im = ORC_SIN(ph);
+        }
+        if (errors_y)
+        {
+            const REAL ph = wavenumber * errors_y[p];
+            gy.re = ORC_COS(ph);
+            gy.im = ORC_SIN(ph);
+        }
+        if (!matrix && !errors_x) return;
+        for (s = 0; s < num_sources; ++s)
+        {
+            REAL* e = jones + (size_t) (matrix ? 8 : 2) *
+                    ((size_t) num_sources * p + s);
+            int k;
+            if (!matrix)
+            {
+                ORC_T(cx) v = {e[0], e[1]};
+                v = ORC_T(cmul)(gx, v);
+                e[0] = v.re; e[1] = v.im;
+                continue;
+            }
+            /* rows a, b scale by gx; rows c, d by gy */
+            for (k = 0; k < 4; ++k)
+            {
+                ORC_T(cx) v = {e[2 * k], e[2 * k + 1]};
+                v = ORC_T(cmul)(k < 2 ? gx : gy, v);
+                e[2 * k] = v.re; e[2 * k + 1] = v.im;
+            }
+        }
+    }
+}
+
+/* J[p][s] <- G_p J[p][s]: 2x2 matrix product for matrix Jones, complex
+ * product for scalar Jones
+ * (interferometer/define_jones_apply_station_gains.h:3-45). */
+void ORC_FN(orc_station_gains)(int matrix, int num_sources,
+        int num_stations, const REAL* gains, REAL* jones)
+{
+    int p, s;
+    for (p = 0; p < num_stations; ++p)
+        for (s = 0; s < num_sources; ++s)
+        {
+            REAL* e = jones + (size_t) (matrix ? 8 : 2) *
+                    ((size_t) num_sources * p + s);
+            if (!matrix)
+            {
+                ORC_T(cx) g = {gains[2 * p], gains[2 * p + 1]};
+                ORC_T(cx) v = {e[0], e[1]};
+                v = ORC_T(cmul)(g, v);
+                e[0] = v.re; e[1] = v.im;
+            }
+            else
+            {
+                const ORC_T(mat) G = ORC_T(load_mat)(gains + 8 * p);
+                const ORC_T(mat) M = ORC_T(load_mat)(e);
+                ORC_T(mat) out;
+                out.a = ORC_T(cadd)(ORC_T(cmul)(G.a, M.a),
+                        ORC_T(cmul)(G.b, M.c));
+                out.b = ORC_T(cadd)(ORC_T(cmul)(G.a, M.b),
+                        ORC_T(cmul)(G.b, M.d));
+                out.c = ORC_T(cadd)(ORC_T(cmul)(G.c, M.a),
+                        ORC_T(cmul)(G.d, M.c));
+                out.d = ORC_T(cadd)(ORC_T(cmul)(G.c, M.b),
+                        ORC_T(cmul)(G.d, M.d));
+                e[0] = out.a.re; e[1] = out.a.im; e[2] = out.b.re;
+                e[3] = out.b.im; e[4] = out.c.re; e[5] = out.c.im;
+                e[6] = out.d.re; e[7] = out.d.im;
+            }
+        }
+}

@@ -152,3 +152,60 @@ void ref_update_horizon_mask_##S(int num, const REAL* l, const REAL* m, \
 
 INST_DIR(double, d)
 INST_DIR(float, f)
+
+/* Sky flux scaling with frequency; station cable-length phases and station
+ * gains applied to Jones arrays. The flux kernel's calc_stokes_i_flux_<FP>
+ * helpers must carry these exact names (the kernel body refers to them).
+ * The ref_ wrapper takes the oracle's extra num_columns argument and
+ * ignores it. */
+#include "sky/oskar_sky_enum.h"
+#include "sky/define_sky_scale_flux_with_frequency.h"
+#include "interferometer/define_jones_apply_cable_length_errors.h"
+#include "interferometer/define_jones_apply_station_gains.h"
+
+OSKAR_SKY_CALC_STOKES_I_FLUX(calc_stokes_i_flux_float, float)
+OSKAR_SKY_CALC_STOKES_I_FLUX(calc_stokes_i_flux_double, double)
+
+#define INST_SKY(REAL, S, REAL2, REAL4c) \
+OSKAR_SKY_SCALE_FLUX_WITH_FREQUENCY(k_scale_flux_##S, REAL) \
+OSKAR_JONES_APPLY_CABLE_LENGTH_ERRORS_M(k_cable_m_##S, REAL, REAL4c) \
+OSKAR_JONES_APPLY_CABLE_LENGTH_ERRORS_C(k_cable_c_##S, REAL, REAL2) \
+OSKAR_JONES_APPLY_STATION_GAINS_M(k_gains_m_##S, REAL4c) \
+OSKAR_JONES_APPLY_STATION_GAINS_C(k_gains_c_##S, REAL2) \
+void ref_sky_scale_flux_##S(int num_sources, int capacity, int num_columns, \
+        REAL freq_hz, const REAL* table, const int* num_valid, int col_i, \
+        int col_q, int col_u, int col_v, int col_ref_freq, \
+        int col_lin_sp_index, int col_sp_index, int col_rot_meas, \
+        int col_pol_frac, int col_pol_ang, int col_ref_wavelength, \
+        int col_sp_curvature, int col_line_width, int col_freq_inc, \
+        REAL* out_i, REAL* out_q, REAL* out_u, REAL* out_v) \
+{ \
+    (void) num_columns; \
+    k_scale_flux_##S(num_sources, capacity, freq_hz, table, num_valid, \
+            col_i, col_q, col_u, col_v, col_ref_freq, col_lin_sp_index, \
+            col_sp_index, col_rot_meas, col_pol_frac, col_pol_ang, \
+            col_ref_wavelength, col_sp_curvature, col_line_width, \
+            col_freq_inc, out_i, out_q, out_u, out_v); \
+} \
+void ref_cable_length_errors_##S(int matrix, int num_sources, \
+        int num_stations, REAL wavenumber, const REAL* errors_x, \
+        const REAL* errors_y, void* jones) \
+{ \
+    if (matrix) k_cable_m_##S(num_sources, num_stations, wavenumber, \
+            errors_x != 0, errors_y != 0, errors_x, errors_y, \
+            (REAL4c*) jones); \
+    else k_cable_c_##S(num_sources, num_stations, wavenumber, \
+            errors_x != 0, errors_y != 0, errors_x, errors_y, \
+            (REAL2*) jones); \
+} \
+void ref_station_gains_##S(int matrix, int num_sources, int num_stations, \
+        const void* gains, void* jones) \
+{ \
+    if (matrix) k_gains_m_##S(num_sources, num_stations, \
+            (const REAL4c*) gains, (REAL4c*) jones); \
+    else k_gains_c_##S(num_sources, num_stations, (const REAL2*) gains, \
+            (REAL2*) jones); \
+}
+
+INST_SKY(double, d, double2, double4c)
+INST_SKY(float, f, float2, float4c)

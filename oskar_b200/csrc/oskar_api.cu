@@ -600,6 +600,109 @@ void oskar_jones_join(oskar_Jones* j3, oskar_Jones* j1, const oskar_Jones* j2,
     oskar_mem_multiply(j3->data, j1->data, j2->data, 0, 0, 0, n, status);
 }
 
+// oskar/interferometer/src/oskar_jones_apply_cable_length_errors.c:23-141.
+// Error arrays must have the Jones array's precision and location (the
+// reference launches without checking them).
+void oskar_jones_apply_cable_length_errors(oskar_Jones* jones,
+        double frequency_hz, const oskar_Mem* errors_x,
+        const oskar_Mem* errors_y, int* status)
+{
+    if (*status) return;
+    if (!errors_x && !errors_y) return;
+    const oskar_Mem* J = jones->data;
+    const int precision = J->type & 0x0F;
+    const int num_stations = jones->num_stations;
+    if ((errors_x && (int) errors_x->num_elements < num_stations) ||
+            (errors_y && (int) errors_y->num_elements < num_stations))
+    {
+        *status = OSKAR_ERR_DIMENSION_MISMATCH;
+        return;
+    }
+    const oskar_Mem* e[2] = {errors_x, errors_y};
+    for (const oskar_Mem* m : e)
+    {
+        if (!m) continue;
+        if (m->location != J->location)
+        {
+            *status = OSKAR_ERR_LOCATION_MISMATCH;
+            return;
+        }
+        if (m->type != precision)
+        {
+            *status = OSKAR_ERR_TYPE_MISMATCH;
+            return;
+        }
+    }
+    if (J->location != OSKAR_GPU)
+    {
+        *status = OSKAR_ERR_BAD_LOCATION;
+        return;
+    }
+    const int matrix = (J->type & OSKAR_MATRIX) != 0;
+    if (!(J->type & OSKAR_COMPLEX))
+    {
+        *status = OSKAR_ERR_BAD_DATA_TYPE;
+        return;
+    }
+    const double k = 2.0 * M_PI * frequency_hz / kC0;
+    if (precision == OSKAR_DOUBLE)
+        *status = oskb_jones_apply_cable_length_errors_d(matrix,
+                jones->num_sources, num_stations, k,
+                errors_x ? (const double*) errors_x->data : nullptr,
+                errors_y ? (const double*) errors_y->data : nullptr,
+                (double*) J->data, 0);
+    else
+        *status = oskb_jones_apply_cable_length_errors_f(matrix,
+                jones->num_sources, num_stations, (float) k,
+                errors_x ? (const float*) errors_x->data : nullptr,
+                errors_y ? (const float*) errors_y->data : nullptr,
+                (float*) J->data, 0);
+}
+
+// oskar/interferometer/src/oskar_jones_apply_station_gains.c:23-121.
+// The gains must have the Jones array's type and location (the reference
+// launches by the gains' type alone).
+void oskar_jones_apply_station_gains(oskar_Jones* jones, oskar_Mem* gains,
+        int* status)
+{
+    if (*status) return;
+    const oskar_Mem* J = jones->data;
+    if ((int) gains->num_elements < jones->num_stations)
+    {
+        *status = OSKAR_ERR_DIMENSION_MISMATCH;
+        return;
+    }
+    if (gains->location != J->location)
+    {
+        *status = OSKAR_ERR_LOCATION_MISMATCH;
+        return;
+    }
+    if (gains->type != J->type)
+    {
+        *status = OSKAR_ERR_TYPE_MISMATCH;
+        return;
+    }
+    if (J->location != OSKAR_GPU)
+    {
+        *status = OSKAR_ERR_BAD_LOCATION;
+        return;
+    }
+    if (!(J->type & OSKAR_COMPLEX))
+    {
+        *status = OSKAR_ERR_BAD_DATA_TYPE;
+        return;
+    }
+    const int matrix = (J->type & OSKAR_MATRIX) != 0;
+    if ((J->type & 0x0F) == OSKAR_DOUBLE)
+        *status = oskb_jones_apply_station_gains_d(matrix, jones->num_sources,
+                jones->num_stations, (const double*) gains->data,
+                (double*) J->data, 0);
+    else
+        *status = oskb_jones_apply_station_gains_f(matrix, jones->num_sources,
+                jones->num_stations, (const float*) gains->data,
+                (float*) J->data, 0);
+}
+
 // oskar/interferometer/src/oskar_evaluate_jones_K.c:19-157
 void oskar_evaluate_jones_K(oskar_Jones* K, int num_sources,
         const oskar_Mem* l, const oskar_Mem* m, const oskar_Mem* n,

@@ -299,3 +299,62 @@ def test_baseline_uvw_known_answer(casa):
     assert np.array_equal(out[0][2:], [f * (u[q] - u[p]) for p, q in pairs])
     assert np.array_equal(out[1][2:], [f * (v[q] - v[p]) for p, q in pairs])
     assert np.array_equal(out[2][2:], [f * (w[q] - w[p]) for p, q in pairs])
+
+
+@pytest.mark.parametrize("real", [np.float64, np.float32])
+@pytest.mark.parametrize("freq", [40e6, 101e6, 150e6, 102.4e6, 250e6])
+def test_sky_scale_flux(real, freq):
+    """Every spectral and polarisation model, NaN coefficients included,
+    against the reference's flux-scaling kernel."""
+    from sky_cases import SkyTable, call_scale, random_sky
+    sky = SkyTable(random_sky(700, 17), real)
+    got = call_scale(oracle(), real, sky, freq)
+    ref = call_scale(reference(), real, sky, freq)
+    tol = 1e-15 if real == np.float64 else 1e-6
+    for g, r in zip(got, ref):
+        np.testing.assert_allclose(g, r, rtol=tol, atol=tol * 10)
+
+
+@pytest.mark.parametrize("real", [np.float64, np.float32])
+def test_sky_scale_flux_sparse_table(real):
+    """A table with only I, reference frequency and spectral index columns
+    (every other column index is -1)."""
+    from sky_cases import SkyTable, call_scale
+    rng = np.random.default_rng(3)
+    srcs = [{"I": [float(rng.uniform(1, 5))],
+             "REF_HZ": [float(rng.uniform(80e6, 120e6))],
+             "SPX": list(rng.uniform(-1, 0.5, 1 + s % 3))}
+            for s in range(300)]
+    sky = SkyTable(srcs, real)
+    assert sky.cols.count(-1) == 11
+    got = call_scale(oracle(), real, sky, 110e6)
+    ref = call_scale(reference(), real, sky, 110e6)
+    for g, r in zip(got, ref):
+        np.testing.assert_allclose(g, r, rtol=1e-6, atol=0)
+
+
+@pytest.mark.parametrize("real", [np.float64, np.float32])
+@pytest.mark.parametrize("matrix", [True, False])
+@pytest.mark.parametrize("ex,ey", [(1, 1), (1, 0), (0, 1)])
+def test_cable_length_errors_and_gains(real, matrix, ex, ey):
+    rng = np.random.default_rng(5)
+    nst, nsrc = 13, 71
+    width = 8 if matrix else 2
+    J = rng.normal(size=nst * nsrc * width).astype(real)
+    dx = rng.uniform(-2, 2, nst).astype(real) if ex else None
+    dy = rng.uniform(-2, 2, nst).astype(real) if ey else None
+    k = real(2 * np.pi * 150e6 / 299792458.0)
+    a, b = J.copy(), J.copy()
+    oracle().call("cable_length_errors_" + suffix(real), real, int(matrix),
+                  nsrc, nst, k, dx, dy, a)
+    reference().call("cable_length_errors_" + suffix(real), real,
+                     int(matrix), nsrc, nst, k, dx, dy, b)
+    assert _close(a, b, real)
+    if ex or matrix:
+        assert not np.array_equal(a, J)
+    G = rng.normal(size=nst * width).astype(real)
+    oracle().call("station_gains_" + suffix(real), real, int(matrix), nsrc,
+                  nst, G, a)
+    reference().call("station_gains_" + suffix(real), real, int(matrix),
+                     nsrc, nst, G, b)
+    assert _close(a, b, real)
