@@ -542,6 +542,36 @@ OSKB_API int oskb_correlate_block_direct_f(int casa, int num_sources,
         const double* gha0_rad, double dec0_rad, double uv_min,
         double uv_max, int uv_filter_units, double source_filter_min,
         double source_filter_max, float* vis, void* stream);
+/* As oskb_correlate_block_direct, with the brightness of every channel:
+ * I, Q, U, V hold [channel][source] values, channel c at
+ * c * flux_channel_stride (>= num_sources; 0 = one set for every channel),
+ * e.g. from oskb_sky_scale_flux_channels. The source filter applies to
+ * each channel's own I, as the reference filters on the flux scaled to the
+ * channel frequency (oskar_interferometer_run_block.c:183-190, 277-281). */
+OSKB_API int oskb_correlate_block_direct_spectral_d(int casa,
+        int num_sources, int num_stations, int num_times, int num_channels,
+        const double* E, int E_per_dump, const double* I, const double* Q,
+        const double* U, const double* V, long long flux_channel_stride,
+        const double* l, const double* m, const double* n, const double* a,
+        const double* b, const double* c, const double* station_uvw,
+        const double* station_x, const double* station_y,
+        const double* inv_wavelength, double channel_bandwidth_hz,
+        double time_average_sec, const double* gha0_rad, double dec0_rad,
+        double uv_min, double uv_max, int uv_filter_units,
+        double source_filter_min, double source_filter_max, double* vis,
+        void* stream);
+OSKB_API int oskb_correlate_block_direct_spectral_f(int casa,
+        int num_sources, int num_stations, int num_times, int num_channels,
+        const float* E, int E_per_dump, const float* I, const float* Q,
+        const float* U, const float* V, long long flux_channel_stride,
+        const float* l, const float* m, const float* n, const float* a,
+        const float* b, const float* c, const float* station_uvw,
+        const float* station_x, const float* station_y,
+        const double* inv_wavelength, double channel_bandwidth_hz,
+        double time_average_sec, const double* gha0_rad, double dec0_rad,
+        double uv_min, double uv_max, int uv_filter_units,
+        double source_filter_min, double source_filter_max, float* vis,
+        void* stream);
 /* Text report of the schedules the block autotuner has chosen (one line
  * per block shape, with the sample time of every candidate). Returns the
  * number of characters written. */
@@ -570,6 +600,18 @@ OSKB_API int oskb_block_plan_set_sky(oskb_BlockPlan* plan, const void* I,
         const void* Q, const void* U, const void* V, const void* l,
         const void* m, const void* n, const void* a, const void* b,
         const void* c);
+/* Spectral sky: the plan scales the brightness of every source to every
+ * channel once, on the device (oskb_sky_scale_flux_channels), and each
+ * block correlates with those per-channel values; the reference rescales
+ * per dump and channel inside its block loop
+ * (oskar_interferometer_run_block.c:183-190). table: host [num_columns]
+ * [capacity] sky table of the plan's precision; num_valid_columns: host
+ * [num_sources][20]; columns: host, the 14 first-column indices in the
+ * order of oskb_sky_scale_flux_with_frequency's col_ arguments. Once it is
+ * set, oskb_block_plan_set_sky may pass NULL for I, Q, U and V. */
+OSKB_API int oskb_block_plan_set_spectral_sky(oskb_BlockPlan* plan,
+        int capacity, int num_columns, const void* table,
+        const int* num_valid_columns, const int* columns);
 OSKB_API int oskb_block_plan_set_stations(oskb_BlockPlan* plan,
         const void* ecef_x, const void* ecef_y);
 OSKB_API int oskb_block_plan_set_beam(oskb_BlockPlan* plan, const void* E);

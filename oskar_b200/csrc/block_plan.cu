@@ -15,6 +15,9 @@
 // (oskar/interferometer/src/oskar_interferometer_run_block.c:156-336), whose
 // visibility block is cleared per block (run_block.c:55) and copied to the
 // host for finalisation (oskar_interferometer_finalise_block.c:32-40).
+// With a spectral sky the plan scales every source's brightness to every
+// channel once, when the sky is set, instead of once per (dump, channel) as
+// the reference's block loop does (run_block.c:183-190).
 #include <stdlib.h>
 #include <string.h>
 
@@ -31,7 +34,10 @@ struct oskb_BlockPlan
     // device
     void* sky[10];  // I, Q, U, V, l, m, n, a, b, c
     void *st_x, *st_y, *E, *uvw, *vis;
-    double *inv_wl, *gha0;
+    double *inv_wl, *gha0, *freq;
+    // Spectral sky: brightness per channel [channel][source] (4 arrays),
+    // scaled once from the sky table when it is set.
+    void* flux_c[4];
     // host (page-locked)
     void *h_uvw, *h_vis;
     double* h_gha0;
@@ -58,11 +64,14 @@ int enqueue_block(oskb_BlockPlan* p)
     }
     int err;
     void* const* k = p->sky;
+    void* const* f = p->flux_c[0] ? p->flux_c : p->sky;
+    const long long fs = p->flux_c[0] ? p->num_src : 0;
     if (p->elem == 8)
-        err = oskb_correlate_block_direct_d(p->casa, p->num_src, p->num_st,
-                p->num_times, p->num_channels, (const double*) p->E,
-                p->beam_per_dump, (const double*) k[0], (const double*) k[1],
-                (const double*) k[2], (const double*) k[3],
+        err = oskb_correlate_block_direct_spectral_d(p->casa, p->num_src,
+                p->num_st, p->num_times, p->num_channels,
+                (const double*) p->E, p->beam_per_dump, (const double*) f[0],
+                (const double*) f[1], (const double*) f[2],
+                (const double*) f[3], fs,
                 (const double*) k[4], (const double*) k[5],
                 (const double*) k[6], (const double*) k[7],
                 (const double*) k[8], (const double*) k[9],
@@ -72,10 +81,11 @@ int enqueue_block(oskb_BlockPlan* p)
                 p->uv_units, p->filter_min, p->filter_max,
                 (double*) p->vis, s);
     else
-        err = oskb_correlate_block_direct_f(p->casa, p->num_src, p->num_st,
-                p->num_times, p->num_channels, (const float*) p->E,
-                p->beam_per_dump, (const float*) k[0], (const float*) k[1],
-                (const float*) k[2], (const float*) k[3],
+        err = oskb_correlate_block_direct_spectral_f(p->casa, p->num_src,
+                p->num_st, p->num_times, p->num_channels,
+                (const float*) p->E, p->beam_per_dump, (const float*) f[0],
+                (const float*) f[1], (const float*) f[2],
+                (const float*) f[3], fs,
                 (const float*) k[4], (const float*) k[5],
                 (const float*) k[6], (const float*) k[7],
                 (const float*) k[8], (const float*) k[9],
@@ -116,8 +126,10 @@ void oskb_block_plan_free(oskb_BlockPlan* p)
     if (p->exec) cudaGraphExecDestroy(p->exec);
     if (p->graph) cudaGraphDestroy(p->graph);
     for (int i = 0; i < 10; ++i) cudaFree(p->sky[i]);
+    for (int i = 0; i < 4; ++i) cudaFree(p->flux_c[i]);
     cudaFree(p->st_x); cudaFree(p->st_y); cudaFree(p->E); cudaFree(p->uvw);
     cudaFree(p->vis); cudaFree(p->inv_wl); cudaFree(p->gha0);
+    cudaFree(p->freq);
     cudaFreeHost(p->h_uvw); cudaFreeHost(p->h_vis); cudaFreeHost(p->h_gha0);
     if (p->stream) cudaStreamDestroy(p->stream);
     free(p);
@@ -159,6 +171,7 @@ oskb_BlockPlan* oskb_block_plan_create(int precision_bytes, int casa,
             cudaSuccess;
     for (int i = 0; i < 10 && ok; ++i)
         if (i < 7 || gaussian) ok = cudaMalloc(&p->sky[i], e * ns) ==
+                cudaSuccess && cudaMemset(p->sky[i], 0, e * ns) ==
                 cudaSuccess;
     ok = ok && cudaMalloc(&p->st_x, e * nst) == cudaSuccess &&
             cudaMalloc(&p->st_y, e * nst) == cudaSuccess &&
@@ -167,6 +180,8 @@ oskb_BlockPlan* oskb_block_plan_create(int precision_bytes, int casa,
             cudaMalloc((void**) &p->inv_wl, sizeof(double) * num_channels)
             == cudaSuccess &&
             cudaMalloc((void**) &p->gha0, sizeof(double) * num_times) ==
+            cudaSuccess &&
+            cudaMalloc((void**) &p->freq, sizeof(double) * num_channels) ==
             cudaSuccess &&
             (!with_beam || cudaMalloc(&p->E, p->e_bytes) == cudaSuccess) &&
             cudaMallocHost(&p->h_uvw, p->uvw_bytes) == cudaSuccess &&
@@ -180,6 +195,8 @@ oskb_BlockPlan* oskb_block_plan_create(int precision_bytes, int casa,
             inv[c] = frequency_hz[c] / 299792458.0;
         ok = cudaMemcpy(p->inv_wl, inv, sizeof(double) * num_channels,
                 cudaMemcpyHostToDevice) == cudaSuccess &&
+                cudaMemcpy(p->freq, frequency_hz, sizeof(double) *
+                num_channels, cudaMemcpyHostToDevice) == cudaSuccess &&
                 cudaMemset(p->st_x, 0, e * nst) == cudaSuccess &&
                 cudaMemset(p->st_y, 0, e * nst) == cudaSuccess;
         free(inv);
@@ -203,8 +220,73 @@ int oskb_block_plan_set_sky(oskb_BlockPlan* p, const void* I, const void* Q,
     const void* src[10] = {I, Q, U, V, l, m, n, a, b, c};
     const size_t bytes = (size_t) p->elem * p->num_src;
     for (int i = 0; i < (p->gaussian ? 10 : 7); ++i)
+    {
+        if (i < 4 && !src[i] && p->flux_c[0]) continue;
         if (int err = upload(p->sky[i], src[i], bytes)) return err;
+    }
     return 0;
+}
+
+int oskb_block_plan_set_spectral_sky(oskb_BlockPlan* p, int capacity,
+        int num_columns, const void* table, const int* num_valid_columns,
+        const int* columns)
+{
+    if (!table || !num_valid_columns || !columns || capacity < p->num_src ||
+            num_columns < 1)
+        return OSKB_ERR_INVALID_ARGUMENT;
+    const size_t e = p->elem, ns = p->num_src;
+    const size_t table_bytes = e * (size_t) capacity * num_columns;
+    const size_t nv_bytes = sizeof(int) * 20 * ns;
+    const size_t flux_bytes = e * ns * p->num_channels;
+    void *d_table = nullptr, *d_nv = nullptr;
+    bool ok = cudaMalloc(&d_table, table_bytes) == cudaSuccess &&
+            cudaMalloc(&d_nv, nv_bytes) == cudaSuccess;
+    for (int i = 0; i < 4 && ok; ++i)
+        if (!p->flux_c[i])
+            ok = cudaMalloc(&p->flux_c[i], flux_bytes) == cudaSuccess;
+    int err = ok ? 0 : OSKB_ERR_MEMORY_ALLOC_FAILURE;
+    if (ok)
+    {
+        err = upload(d_table, table, table_bytes);
+        if (!err) err = upload(d_nv, num_valid_columns, nv_bytes);
+    }
+    if (!err)
+    {
+        if (p->elem == 8)
+            err = oskb_sky_scale_flux_channels_d(p->num_src, capacity,
+                    num_columns, p->num_channels, p->freq,
+                    (const double*) d_table, (const int*) d_nv, columns,
+                    p->num_src, (double*) p->flux_c[0],
+                    (double*) p->flux_c[1], (double*) p->flux_c[2],
+                    (double*) p->flux_c[3], p->stream);
+        else
+            err = oskb_sky_scale_flux_channels_f(p->num_src, capacity,
+                    num_columns, p->num_channels, p->freq,
+                    (const float*) d_table, (const int*) d_nv, columns,
+                    p->num_src, (float*) p->flux_c[0],
+                    (float*) p->flux_c[1], (float*) p->flux_c[2],
+                    (float*) p->flux_c[3], p->stream);
+    }
+    if (cudaStreamSynchronize(p->stream) != cudaSuccess && !err)
+        err = OSKB_ERR_KERNEL_LAUNCH_FAILURE;
+    cudaFree(d_table);
+    cudaFree(d_nv);
+    if (err)
+    {
+        if (!ok) oskb::set_last_error("oskb_block_plan_set_spectral_sky",
+                cudaGetLastError());
+        for (int i = 0; i < 4; ++i)
+        {
+            cudaFree(p->flux_c[i]);
+            p->flux_c[i] = nullptr;
+        }
+    }
+    // The captured block reads the brightness arrays: capture again.
+    if (p->exec) cudaGraphExecDestroy(p->exec);
+    if (p->graph) cudaGraphDestroy(p->graph);
+    p->exec = nullptr;
+    p->graph = nullptr;
+    return err;
 }
 
 int oskb_block_plan_set_stations(oskb_BlockPlan* p, const void* ecef_x,

@@ -71,6 +71,9 @@ struct XcorrParams
     // v m + w (n - 1))), zero where I is outside (filter_min, filter_max].
     long long e_time_stride;  // E of dump t at jones + t * e_time_stride
     double filter_min, filter_max;
+    // Brightness per channel (block mode): I, Q, U, V of channel c at
+    // + c * flux_channel_stride (0: the same for every channel).
+    long long flux_channel_stride;
 };
 
 template <typename T, bool MATRIX>
@@ -225,7 +228,9 @@ __device__ __forceinline__ void issue_chunk(Smem<T, MATRIX>& sm,
                 prm.c;
         const int s = s0 + sl;
         const bool in = s < src_end;
-        cp_async(&sm.raw_src[k][sl], in ? arr + s : prm.I, in,
+        const long long off = k <= kV ? it_ctx.c * prm.flux_channel_stride :
+                0;
+        cp_async(&sm.raw_src[k][sl], in ? arr + off + s : prm.I, in,
                 (int) sizeof(T));
     }
     cp_async_commit();
@@ -1360,10 +1365,12 @@ int correlate_block_direct(int casa, int num_sources, int num_stations,
         double time_average_sec, const double* gha0_rad, double dec0_rad,
         double uv_min, double uv_max, int uv_filter_units,
         double source_filter_min, double source_filter_max, T* vis,
-        void* stream)
+        void* stream, long long flux_channel_stride)
 {
     if (num_sources < 0 || num_stations < 0 || num_times < 0 ||
             num_channels < 0)
+        return OSKB_ERR_INVALID_ARGUMENT;
+    if (flux_channel_stride != 0 && flux_channel_stride < num_sources)
         return OSKB_ERR_INVALID_ARGUMENT;
     if (num_sources == 0 || num_stations < 2 || num_times == 0 ||
             num_channels == 0)
@@ -1401,6 +1408,7 @@ int correlate_block_direct(int casa, int num_sources, int num_stations,
     p.num_channels = num_channels;
     p.filter_min = source_filter_min;
     p.filter_max = source_filter_max;
+    p.flux_channel_stride = flux_channel_stride;
     return block_dispatch<T>(casa != 0, gauss, bw, ts, p, as_stream(stream));
 }
 
@@ -1426,7 +1434,26 @@ int oskb_correlate_block_direct_##S(int casa, int num_sources,               \
             b, c, station_uvw, station_x, station_y, inv_wavelength,         \
             channel_bandwidth_hz, time_average_sec, gha0_rad, dec0_rad,      \
             uv_min, uv_max, uv_filter_units, source_filter_min,              \
-            source_filter_max, vis, stream);                                 \
+            source_filter_max, vis, stream, 0);                              \
+}                                                                            \
+int oskb_correlate_block_direct_spectral_##S(int casa, int num_sources,      \
+        int num_stations, int num_times, int num_channels, const T* E,       \
+        int E_per_dump, const T* I, const T* Q, const T* U, const T* V,      \
+        long long flux_channel_stride, const T* l, const T* m, const T* n,   \
+        const T* a, const T* b, const T* c, const T* station_uvw,            \
+        const T* station_x, const T* station_y,                              \
+        const double* inv_wavelength, double channel_bandwidth_hz,           \
+        double time_average_sec, const double* gha0_rad, double dec0_rad,    \
+        double uv_min, double uv_max, int uv_filter_units,                   \
+        double source_filter_min, double source_filter_max, T* vis,          \
+        void* stream)                                                        \
+{                                                                            \
+    return oskb::correlate_block_direct<T>(casa, num_sources, num_stations,  \
+            num_times, num_channels, E, E_per_dump, I, Q, U, V, l, m, n, a,  \
+            b, c, station_uvw, station_x, station_y, inv_wavelength,         \
+            channel_bandwidth_hz, time_average_sec, gha0_rad, dec0_rad,      \
+            uv_min, uv_max, uv_filter_units, source_filter_min,              \
+            source_filter_max, vis, stream, flux_channel_stride);            \
 }
 
 OSKB_BLOCK_ENTRY(double, d)

@@ -58,6 +58,17 @@ class BlockCase:
         self.E = cast(E) if beam else None
         self.beam_per_dump = beam_per_dump
         self.nbl = num_st * (num_st - 1) // 2
+        self.flux_c = None
+
+    def set_spectral(self, sky):
+        """Brightness per channel from a sky table (tests/sky_cases.py),
+        scaled by the oracle at each channel frequency: flux_c[k] is
+        [channel][source] for k in I, Q, U, V."""
+        from sky_cases import call_scale
+        assert sky.num_sources == self.num_src
+        per = [call_scale(oracle(), self.real, sky, f) for f in self.freqs]
+        self.flux_c = {k: np.ascontiguousarray(np.stack([p[j] for p in per]))
+                       for j, k in enumerate("IQUV")}
 
     def oracle_vis(self):
         real, s = self.real, suffix(self.real)
@@ -78,6 +89,10 @@ class BlockCase:
                     Et = np.ascontiguousarray(Et)
                 for c in range(C):
                     f = self.freqs[c]
+                    if self.flux_c is not None:
+                        for k in "IQUV":
+                            ch[k] = np.ascontiguousarray(self.flux_c[k][c,
+                                                                        sl])
                     K = np.zeros(2 * N * size, real)
                     orc.call("jones_k_" + s, real, size, ch["l"], ch["m"],
                              ch["n"], N, u, v, w, real(2 * math.pi * f / C0),

@@ -180,3 +180,100 @@ def test_block_plan_graph_replay(real):
         assert lib.oskb_block_plan_graph_launches(plan) == 2
     finally:
         lib.oskb_block_plan_free(plan)
+
+
+def _spectral_case(real, **kw):
+    from sky_cases import SkyTable, random_sky
+    c = BlockCase(real=real, **kw)
+    c.freqs = np.array([60e6, 95e6, 140e6, 210e6])[:c.num_channels]
+    c.inv_wl = c.freqs / 299792458.0
+    sky = SkyTable(random_sky(c.num_src, 41), real)
+    c.set_spectral(sky)
+    return c, sky
+
+
+@pytest.mark.parametrize("real", [np.float64, np.float32])
+def test_block_spectral_brightness(real):
+    """Brightness per channel, scaled on the device for the whole band in
+    one launch, correlated in one block launch; a flux filter that sources
+    cross between channels. Oracle: scale, K, join, correlate per dump,
+    chunk and channel, as the reference's block loop does."""
+    c, sky = _spectral_case(real, num_channels=4, bandwidth_hz=1e5,
+                            time_avg=10.0, filter_min=0.8, filter_max=6.0)
+    I = c.flux_c["I"]
+    crossing = np.any((I > 0.8) & (I <= 6.0), 0) & \
+        ~np.all((I > 0.8) & (I <= 6.0), 0)
+    assert crossing.sum() > 5
+    # no channel's I within rounding of a filter bound (FP32 would flip it)
+    assert np.min(np.abs(I / 0.8 - 1)) > 1e-4
+    assert np.min(np.abs(I / 6.0 - 1)) > 1e-4
+    C, S = c.num_channels, c.num_src
+    tt = torch.float64 if real == np.float64 else torch.float32
+    flux = [torch.zeros(C * S, dtype=tt, device="cuda") for _ in range(4)]
+    ob.call("oskb_sky_scale_flux_channels_" + suffix(real), S, sky.capacity,
+            sky.num_columns, C, dev(c.freqs), dev(sky.table),
+            dev(sky.num_valid), np.array(sky.cols, np.int32), S, *flux,
+            ob.stream_ptr())
+    vis = dev(np.zeros(c.num_times * C * c.nbl * 8, real))
+    ob.call("oskb_correlate_block_direct_spectral_" + suffix(real), c.casa,
+            S, c.num_st, c.num_times, C, dev(c.E), 0, *flux, S, dev(c.l),
+            dev(c.m), dev(c.n), dev(c.a), dev(c.b), dev(c.c), dev(c.uvw),
+            dev(c.st_x), dev(c.st_y), dev(c.inv_wl), c.bw, c.tavg,
+            dev(c.gha0), c.dec0, c.uv_min_m, c.uv_max_m, 0, c.filter_min,
+            c.filter_max, vis, ob.stream_ptr())
+    torch.cuda.synchronize()
+    assert rel(vis.cpu().numpy(), c.oracle_vis()) <= TOL[real]
+    st = ob.call("oskb_correlate_block_direct_spectral_" + suffix(real),
+                 c.casa, S, c.num_st, c.num_times, C, dev(c.E), 0, *flux,
+                 S - 1, dev(c.l), dev(c.m), dev(c.n), dev(c.a), dev(c.b),
+                 dev(c.c), dev(c.uvw), dev(c.st_x), dev(c.st_y),
+                 dev(c.inv_wl), c.bw, c.tavg, dev(c.gha0), c.dec0,
+                 c.uv_min_m, c.uv_max_m, 0, c.filter_min, c.filter_max, vis,
+                 ob.stream_ptr(), check=False)
+    assert st == -3  # stride shorter than a channel's sources
+
+
+@pytest.mark.parametrize("real", [np.float64, np.float32])
+def test_block_plan_spectral_sky(real):
+    """The block plan with a spectral sky: scaled once when set, then every
+    block (eager, then graph replays) correlates per-channel brightness."""
+    import ctypes
+    lib = ob.load()
+    c, sky = _spectral_case(real, num_st=45, chunks=(80, 40),
+                            gaussian=(1, 0), num_channels=3)
+    st = ctypes.c_int(0)
+    plan = lib.oskb_block_plan_create(
+        8 if real == np.float64 else 4, c.casa, c.num_st, c.num_src,
+        c.num_times, c.num_channels, 1, 1, 0,
+        c.freqs.ctypes.data, c.bw, c.tavg, c.dec0, c.uv_min_m, c.uv_max_m,
+        0, c.filter_min, c.filter_max, ctypes.addressof(st))
+    assert st.value == 0 and plan
+    try:
+        cols = np.array(sky.cols, np.int32)
+        assert ob.call("oskb_block_plan_set_spectral_sky", plan,
+                       sky.capacity, sky.num_columns, sky.table,
+                       sky.num_valid, cols) == 0
+        assert ob.call("oskb_block_plan_set_sky", plan, None, None, None,
+                       None, c.l, c.m, c.n, c.a, c.b, c.c) == 0
+        assert ob.call("oskb_block_plan_set_stations", plan, c.st_x,
+                       c.st_y) == 0
+        assert ob.call("oskb_block_plan_set_beam", plan, c.E) == 0
+        nvis = c.num_times * c.num_channels * c.nbl * 8
+        uvw = _host_view(lib.oskb_block_plan_host_uvw(plan), c.uvw.size,
+                         real)
+        gha0 = _host_view(lib.oskb_block_plan_host_gha0(plan), c.num_times,
+                          np.float64)
+        vis = _host_view(lib.oskb_block_plan_host_vis(plan), nvis, real)
+        for block in range(3):
+            if block:
+                rng = np.random.default_rng(200 + block)
+                c.uvw = rng.uniform(-3e3, 3e3, c.uvw.shape).astype(real)
+                c.gha0 = rng.uniform(-1, 1, c.num_times)
+            uvw[:] = c.uvw.ravel()
+            gha0[:] = c.gha0
+            assert ob.call("oskb_block_plan_execute", plan) == 0
+            assert ob.call("oskb_block_plan_synchronize", plan) == 0
+            assert rel(vis.copy(), c.oracle_vis()) <= TOL[real], block
+        assert lib.oskb_block_plan_graph_launches(plan) == 2
+    finally:
+        lib.oskb_block_plan_free(plan)
