@@ -314,7 +314,7 @@ OSKB_API int oskb_convert_station_uvw_to_baseline_uvw_f(int use_casa,
  * rotation with a rotation measure. NaN coefficients count as 0; a source
  * whose nearest reference frequency is 0 keeps its values.
  * The arguments are those of the reference's kernel
- * (sky/src/oskar_sky_scale_flux_with_frequency.c:165-189, body
+ * (sky/src/oskar_sky_scale_flux_with_frequency.c:127-152, body
  * sky/define_sky_scale_flux_with_frequency.h:89-253), plus num_columns:
  * the table holds num_columns columns of capacity values (column k of
  * source s at table[capacity * k + s]); num_valid_columns is
