@@ -230,10 +230,13 @@ def _load_peaks():
             "bf16_tflops_sustained": 1400.0}, "fallback"
 
 
-def _load_traffic():
-    """DRAM bytes per launch of the contraction kernel from the committed
-    ncu summary (profiles/tc_gemm_c3_traffic.json), or None."""
-    path = os.path.join(ROOT, "profiles", "tc_gemm_c3_traffic.json")
+def _load_traffic(tile):
+    """DRAM bytes per launch of the contraction kernel (square or wide
+    tiles) from the committed ncu summary
+    (profiles/tc_gemm{,_wide}_c3_traffic.json), or None."""
+    name = "tc_gemm_wide_c3_traffic.json" if tile == 256 else \
+        "tc_gemm_c3_traffic.json"
+    path = os.path.join(ROOT, "profiles", name)
     if not os.path.exists(path):
         return None
     with open(path) as f:
@@ -348,12 +351,21 @@ def run_ours(args):
             pk = peaks["bf16_tflops_sustained"]
             nrb = (nst + 31) // 32
             kp = 2 * 32 * ((nsrc + 31) // 32)
-            issued = (nch * nrb * (nrb + 1) // 2 * 128 * 128 * kp * 2 * 3)
+            tile = ob.load().oskb_tc_tile_columns()
+            if tile == 256:
+                # wide tiles: 128 x 256 columns per task over the triangle
+                ntile = sum(min(2 * cp + 2, nrb)
+                            for cp in range((nrb + 1) // 2))
+                issued = nch * ntile * 128 * 256 * kp * 2 * 3
+            else:
+                issued = nch * nrb * (nrb + 1) // 2 * 128 * 128 * kp * 2 * 3
             issued_tf = issued / (avg * 1e-3) / 1e12
-            traffic = _load_traffic()
+            traffic = _load_traffic(tile)
             roof = {"bound": "tensor", "achieved": ach, "peak": pk,
                     "unit": "TFLOP/s", "frac": ach / pk, "traffic": traffic,
-                    "kernel": "oskb::tc::gemm_kernel",
+                    "kernel": ("oskb::tc::gemm_wide_kernel" if tile == 256
+                               else "oskb::tc::gemm_kernel"),
+                    "tile_columns": tile,
                     "peak_kind": "%s bf16 sustained (fp16 same rate)"
                                  % peak_kind,
                     "algorithmic_flops_per_launch": 64.0 * sb_launch,

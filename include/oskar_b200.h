@@ -729,6 +729,10 @@ OSKB_API int oskb_cross_correlate_tc_noalloc_d(int use_casa_phase_convention,
  * bounded device-side wait expired (the call's result is invalid). */
 OSKB_API int oskb_tc_status(const void* workspace, int* flags,
         int* wait_error);
+/* Tile width (128 or 256 columns of G) of the last tensor-core contraction
+ * launched, 0 before the first. The environment variable OSKB_TC_TILE
+ * selects it (128, the default, or 256). */
+OSKB_API int oskb_tc_tile_columns(void);
 
 #ifdef __cplusplus
 }

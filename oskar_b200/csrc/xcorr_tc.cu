@@ -657,6 +657,362 @@ gemm_kernel(const GemmParams prm)
     if (warp == 1) ptx::tmem_dealloc(tmem, kTmemCols);
 }
 
+// ===========================================================================
+// Wide tiles: 128 rows x 256 columns of G per task (row block rb, column
+// blocks 2 cp and 2 cp + 1), so every A tile pair loaded feeds twice the
+// products of the 128 x 128 kernel: 96 KB of operands per k block for six
+// 128x128x64 products, where the square tiles load 64 KB for three. The
+// contraction is bound by how fast operands reach shared memory, so fewer
+// bytes per product is the lever.
+// TMEM holds a 256-column main accumulator (hi hi^T) and a 256-column
+// correction accumulator (hi lo^T + lo hi^T), both single-buffered. The
+// main accumulator is drained every drain_kb k blocks; while it drains, the
+// MMA issuer already issues the next k block's correction products, and
+// only then waits for the main accumulator. The correction accumulator
+// (2^-11 of the main one) is drained every kCorrPeriods main drains and at
+// the end of each task.
+// Warp roles as in gemm_kernel (320 threads); the epilogue warps own 128
+// columns each.
+// ===========================================================================
+constexpr int kWStages = 2;
+constexpr int kWStageBytes = 3 * kPairBytes;  // A pair + B hi x2 + B lo x2
+constexpr int kWCols = 256;                   // one accumulator
+constexpr uint32_t kWTmemCols = 512;          // main + correction
+constexpr int kCorrPeriods = 8;
+
+struct WideCtl
+{
+    uint64_t full[kWStages], empty[kWStages], mfull, mempty, cfull, cempty,
+            done;
+    uint32_t tmem_base;
+    int abort;
+};
+
+constexpr size_t gemm_wide_smem_bytes()
+{
+    return 1024 + (size_t) kWStages * kWStageBytes + sizeof(WideCtl);
+}
+
+// Wide task t of one problem -> (rb, cp): column pair cp holds the tasks
+// [cp (cp + 1), cp (cp + 1) + 2 cp + 2), rb = t - cp (cp + 1) (the last pair
+// of an odd number of row blocks holds 2 cp + 1 of them).
+__device__ __forceinline__ void wide_tile_of(int t, int& rb, int& cp)
+{
+    int c = (int) ((sqrt(4.0 * t + 1.0) - 1.0) * 0.5);
+    while ((c + 1) * (c + 2) <= t) ++c;
+    while (c * (c + 1) > t) --c;
+    cp = c;
+    rb = t - c * (c + 1);
+}
+
+__host__ __device__ inline int wide_tiles(int nrb)
+{
+    int n = 0;
+    for (int cp = 0; 2 * cp < nrb; ++cp)
+        n += (2 * cp + 2 < nrb) ? 2 * cp + 2 : nrb;
+    return n;
+}
+
+__device__ __forceinline__ bool corr_drain_at(int ch, int nchunk)
+{
+    return (ch % kCorrPeriods) == kCorrPeriods - 1 || ch == nchunk - 1;
+}
+
+__global__ void __launch_bounds__(kGemmThreads, 1)
+gemm_wide_kernel(const GemmParams prm)
+{
+    extern __shared__ uint8_t smem_raw[];
+    uint8_t* smem = reinterpret_cast<uint8_t*>(
+            (reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~(uintptr_t) 1023);
+    WideCtl* ctl = reinterpret_cast<WideCtl*>(smem + kWStages * kWStageBytes);
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    volatile int* abort = &ctl->abort;
+
+    if (threadIdx.x == 0)
+    {
+        for (int s = 0; s < kWStages; ++s)
+        {
+            ptx::mbar_init(&ctl->full[s], 1);
+            ptx::mbar_init(&ctl->empty[s], 1);
+        }
+        ptx::mbar_init(&ctl->mfull, 1);
+        ptx::mbar_init(&ctl->mempty, 8);
+        ptx::mbar_init(&ctl->cfull, 1);
+        ptx::mbar_init(&ctl->cempty, 8);
+        ptx::mbar_init(&ctl->done, 1);
+        ctl->abort = 0;
+        ptx::fence_mbar_init();
+    }
+    if (warp == 1) ptx::tmem_alloc(&ctl->tmem_base, kWTmemCols);
+    ptx::tc_fence_before();
+    __syncthreads();
+    ptx::tc_fence_after();
+    const uint32_t tmem = ctl->tmem_base;
+
+    const int ntile = wide_tiles(prm.nrb);
+    const int ntasks = ntile * prm.num_problems;
+    const int nchunk = (prm.nkb + prm.drain_kb - 1) / prm.drain_kb;
+
+    if (warp == 0)
+    {
+        if (lane == 0)
+        {
+            // ---------------- producer: A pair, then the hi tiles of both
+            // column blocks (one 256-row operand), then their lo tiles
+            int stage = 0;
+            uint32_t phase = 0;
+            uint32_t issued = 0, issued_par = 0;  // bit s: stage s
+            for (int task = blockIdx.x; task < ntasks && !*abort;
+                    task += gridDim.x)
+            {
+                const int prob = task / ntile;
+                int rb, cp;
+                wide_tile_of(task - prob * ntile, rb, cp);
+                const int cb0 = 2 * cp;
+                // an odd last column block: its partner repeats it (the
+                // columns are discarded by the q < N test)
+                const int cb1 = cb0 + 1 < prm.nrb ? cb0 + 1 : cb0;
+                const uint8_t* img = prm.W + (size_t) prob * prm.image_stride;
+                for (int kb = 0; kb < prm.nkb; ++kb)
+                {
+                    if (!ptx::mbar_wait(&ctl->empty[stage], phase ^ 1,
+                            prm.err, 21, abort))
+                        break;
+                    uint8_t* dst = smem + (size_t) stage * kWStageBytes;
+                    const uint8_t* a = img + ((size_t) rb * prm.nkb + kb) *
+                            kPairBytes;
+                    const uint8_t* b0 = img + ((size_t) cb0 * prm.nkb + kb) *
+                            kPairBytes;
+                    const uint8_t* b1 = img + ((size_t) cb1 * prm.nkb + kb) *
+                            kPairBytes;
+                    ptx::mbar_arrive_expect_tx(&ctl->full[stage],
+                            kWStageBytes);
+                    ptx::bulk_g2s(dst, a, kPairBytes, &ctl->full[stage]);
+                    ptx::bulk_g2s(dst + kPairBytes, b0, kTileBytes,
+                            &ctl->full[stage]);
+                    ptx::bulk_g2s(dst + kPairBytes + kTileBytes, b1,
+                            kTileBytes, &ctl->full[stage]);
+                    ptx::bulk_g2s(dst + 2 * kPairBytes, b0 + kTileBytes,
+                            kTileBytes, &ctl->full[stage]);
+                    ptx::bulk_g2s(dst + 2 * kPairBytes + kTileBytes,
+                            b1 + kTileBytes, kTileBytes, &ctl->full[stage]);
+                    issued |= 1u << stage;
+                    issued_par = (issued_par & ~(1u << stage)) |
+                            (phase << stage);
+                    if (++stage == kWStages) { stage = 0; phase ^= 1; }
+                }
+            }
+            for (int s = 0; s < kWStages; ++s)
+                if ((issued >> s) & 1)
+                    ptx::mbar_wait(&ctl->full[s], (issued_par >> s) & 1,
+                            prm.err, 22, abort);
+        }
+        __syncwarp();
+    }
+    else if (warp == 1)
+    {
+        if (lane == 0)
+        {
+            // ---------------- MMA issuer
+            const uint32_t idesc = ptx::idesc_f16_f32(128, kWCols);
+            const uint32_t dm = tmem, dcr = tmem + kWCols;
+            int stage = 0;
+            uint32_t phase = 0, mpar = 0, cpar = 0;
+            bool ok = true;
+            for (int task = blockIdx.x; task < ntasks && ok;
+                    task += gridDim.x)
+            {
+                for (int ch = 0; ch < nchunk && ok; ++ch)
+                {
+                    const bool fresh = (ch % kCorrPeriods) == 0;
+                    if (fresh)
+                    {
+                        if (!ptx::mbar_wait(&ctl->cempty, cpar ^ 1, prm.err,
+                                23, abort))
+                        {
+                            ok = false;
+                            break;
+                        }
+                        ptx::tc_fence_after();
+                    }
+                    const int kb0 = ch * prm.drain_kb;
+                    const int kb1 = min(prm.nkb, kb0 + prm.drain_kb);
+                    for (int kb = kb0; kb < kb1; ++kb)
+                    {
+                        if (!ptx::mbar_wait(&ctl->full[stage], phase, prm.err,
+                                24, abort))
+                        {
+                            ok = false;
+                            break;
+                        }
+                        ptx::tc_fence_after();
+                        const uint32_t a = ptx::smem_u32(smem +
+                                (size_t) stage * kWStageBytes);
+                        const uint32_t al = a + kTileBytes;
+                        const uint32_t bh = a + kPairBytes;
+                        const uint32_t bl = a + 2 * kPairBytes;
+                        // correction products first: they do not need the
+                        // main accumulator, which may still be draining
+#pragma unroll
+                        for (int k = 0; k < 4; ++k)
+                        {
+                            const uint32_t first =
+                                    (fresh && kb == kb0 && k == 0) ? 0u : 1u;
+                            ptx::mma_f16(dcr, ptx::sdesc_sw128(a + 32 * k),
+                                    ptx::sdesc_sw128(bl + 32 * k), idesc,
+                                    first);
+                            ptx::mma_f16(dcr, ptx::sdesc_sw128(al + 32 * k),
+                                    ptx::sdesc_sw128(bh + 32 * k), idesc, 1u);
+                        }
+                        if (kb == kb0)
+                        {
+                            if (!ptx::mbar_wait(&ctl->mempty, mpar ^ 1,
+                                    prm.err, 25, abort))
+                            {
+                                ok = false;
+                                break;
+                            }
+                            ptx::tc_fence_after();
+                        }
+#pragma unroll
+                        for (int k = 0; k < 4; ++k)
+                            ptx::mma_f16(dm, ptx::sdesc_sw128(a + 32 * k),
+                                    ptx::sdesc_sw128(bh + 32 * k), idesc,
+                                    (kb > kb0 || k > 0) ? 1u : 0u);
+                        ptx::mma_commit(&ctl->empty[stage]);
+                        if (++stage == kWStages) { stage = 0; phase ^= 1; }
+                    }
+                    if (!ok) break;
+                    ptx::mma_commit(&ctl->mfull);
+                    mpar ^= 1;
+                    if (corr_drain_at(ch, nchunk))
+                    {
+                        ptx::mma_commit(&ctl->cfull);
+                        cpar ^= 1;
+                    }
+                }
+            }
+            ptx::mma_commit(&ctl->done);
+            ptx::mbar_wait(&ctl->done, 0, prm.err, 26, abort);
+        }
+        __syncwarp();
+    }
+    else
+    {
+        // ---------------- epilogue: 8 warps, 128 columns each
+        const int q4 = warp & 3;          // TMEM lane quadrant of this warp
+        const int h = (warp - 2) >> 2;    // column half
+        const int row = 32 * q4 + lane;   // row of the G tile
+        const uint32_t taddr = tmem + ((uint32_t) (32 * q4) << 16) +
+                (uint32_t) (128 * h);
+        uint32_t mpar = 0, cpar = 0;
+        bool ok = true;
+        for (int task = blockIdx.x; task < ntasks && ok; task += gridDim.x)
+        {
+            const int prob = task / ntile;
+            int rb, cp;
+            wide_tile_of(task - prob * ntile, rb, cp);
+            const int c = row & 1;
+            double accR[32], accI[32];
+#pragma unroll
+            for (int j = 0; j < 32; ++j) accR[j] = accI[j] = 0.0;
+            for (int ch = 0; ch < nchunk; ++ch)
+            {
+                const bool with_corr = corr_drain_at(ch, nchunk);
+                if (!ptx::mbar_wait(&ctl->mfull, mpar, prm.err, 27, abort) ||
+                        (with_corr && !ptx::mbar_wait(&ctl->cfull, cpar,
+                        prm.err, 28, abort)))
+                {
+                    ok = false;
+                    break;
+                }
+                ptx::tc_fence_after();
+#pragma unroll
+                for (int j0 = 0; j0 < 128; j0 += 16)
+                {
+                    uint32_t vm[16], vc[16];
+                    ptx::tmem_ld16(taddr + j0, vm);
+                    if (with_corr) ptx::tmem_ld16(taddr + kWCols + j0, vc);
+                    ptx::tmem_ld_wait();
+                    float v[16];
+#pragma unroll
+                    for (int j = 0; j < 16; ++j)
+                        v[j] = __uint_as_float(vm[j]) +
+                                (with_corr ? __uint_as_float(vc[j]) : 0.0f);
+                    // polarisation pair combined in FP32, as in gemm_kernel
+#pragma unroll
+                    for (int qq = 0; qq < 4; ++qq)
+                    {
+                        const int jb = 4 * qq;
+                        const float s0 = c ? v[jb + 0] : v[jb + 2];
+                        const float s1 = c ? v[jb + 1] : v[jb + 3];
+                        const float r0 = __shfl_xor_sync(0xffffffffu, s0, 1);
+                        const float r1 = __shfl_xor_sync(0xffffffffu, s1, 1);
+                        const float g00 = c ? r0 : v[jb + 0];
+                        const float g01 = c ? r1 : v[jb + 1];
+                        const float g10 = c ? v[jb + 2] : r0;
+                        const float g11 = c ? v[jb + 3] : r1;
+                        accR[j0 / 4 + qq] += (double) (g00 + g11);
+                        accI[j0 / 4 + qq] += (double) (g10 - g01);
+                    }
+                }
+                ptx::tc_fence_before();
+                __syncwarp();
+                if (lane == 0)
+                {
+                    ptx::mbar_arrive(&ctl->mempty);
+                    if (with_corr) ptx::mbar_arrive(&ctl->cempty);
+                }
+                mpar ^= 1;
+                if (with_corr) cpar ^= 1;
+            }
+            if (!ok) break;
+            // ---- visibilities of this tile
+            const int g = prm.prob0 + prob, t = g / prm.nch;
+            const int chan = g - t * prm.nch;
+            const float S = scale_from_bits(
+                    prm.maxabs_bits[prm.maxabs_stride * g]);
+            const double inv_s2 = 1.0 / ((double) S * (double) S);
+            const int i = (row >> 1) & 1;
+            const int p = rb * kStPerBlock + (row >> 2);
+            const int N = prm.num_st;
+            const double* su = prm.st_u + prm.uv_stride * t;
+            const double* sv = prm.st_v + prm.uv_stride * t;
+            const double kw = prm.inv_wavelength ? prm.inv_wavelength[chan]
+                                                  : prm.kw_scalar;
+            double* vbase = prm.vis + 8 * ((size_t) g * prm.vis_stride +
+                    (size_t) prm.offset_out);
+#pragma unroll
+            for (int ql = 0; ql < 32; ++ql)
+            {
+                const int q = 2 * cp * kStPerBlock + 32 * h + ql;
+                if (p < q && q < N)
+                {
+                    const double uu = (su[p] - su[q]) * kw;
+                    const double vv = (sv[p] - sv[q]) * kw;
+                    const double len = sqrt(uu * uu + vv * vv);
+                    if (!(len < prm.uv_min || len > prm.uv_max))
+                    {
+                        const double re = accR[ql] * inv_s2;
+                        const double im = accI[ql] * inv_s2;
+                        const int ro = prm.casa ? i : c;
+                        const int co = prm.casa ? c : i;
+                        double* o = vbase + 8 * (size_t) baseline_index(N, q, p)
+                                + 2 * (2 * ro + co);
+                        o[0] += re;
+                        o[1] += prm.casa ? im : -im;
+                    }
+                }
+            }
+        }
+    }
+
+    ptx::tc_fence_before();
+    __syncthreads();
+    ptx::tc_fence_after();
+    if (warp == 1) ptx::tmem_dealloc(tmem, kWTmemCols);
+}
+
 }  // namespace tc
 }  // namespace oskb
 
@@ -753,6 +1109,17 @@ bool g_timing = false;
 std::vector<std::pair<cudaEvent_t, cudaEvent_t>> g_ev;
 size_t g_ev_used = 0;
 
+// Tile width of the contraction: OSKB_TC_TILE=128 (square tiles, the
+// default) or 256 (wide tiles).
+int tile_setting()
+{
+    const char* e = getenv("OSKB_TC_TILE");
+    const int t = e ? atoi(e) : 0;
+    return (t == 128 || t == 256) ? t : 0;
+}
+
+int g_last_tile = 0;
+
 int launch_gemm(GemmParams& gp, cudaStream_t stream)
 {
     static bool attr_set = false;
@@ -761,11 +1128,20 @@ int launch_gemm(GemmParams& gp, cudaStream_t stream)
         cudaFuncSetAttribute(gemm_kernel,
                 cudaFuncAttributeMaxDynamicSharedMemorySize,
                 (int) gemm_smem_bytes());
+        cudaFuncSetAttribute(gemm_wide_kernel,
+                cudaFuncAttributeMaxDynamicSharedMemorySize,
+                (int) gemm_wide_smem_bytes());
         attr_set = true;
     }
-    const long long ntasks = (long long) gp.nrb * (gp.nrb + 1) / 2 *
+    const long long square = (long long) gp.nrb * (gp.nrb + 1) / 2 *
             gp.num_problems;
+    const long long wide_n = (long long) wide_tiles(gp.nrb) *
+            gp.num_problems;
+    const int setting = tile_setting();
+    const bool wide = setting == 256;
+    const long long ntasks = wide ? wide_n : square;
     const int grid = (int) (ntasks < num_sms() ? ntasks : num_sms());
+    g_last_tile = wide ? 256 : 128;
     gp.drain_kb = drain_kblocks();
     cudaEvent_t ev_stop = nullptr;
     if (g_timing)
@@ -781,7 +1157,11 @@ int launch_gemm(GemmParams& gp, cudaStream_t stream)
         ev_stop = g_ev[g_ev_used].second;
         ++g_ev_used;
     }
-    gemm_kernel<<<grid, kGemmThreads, gemm_smem_bytes(), stream>>>(gp);
+    if (wide)
+        gemm_wide_kernel<<<grid, kGemmThreads, gemm_wide_smem_bytes(),
+                stream>>>(gp);
+    else
+        gemm_kernel<<<grid, kGemmThreads, gemm_smem_bytes(), stream>>>(gp);
     if (ev_stop) cudaEventRecord(ev_stop, stream);
     return check_launch("tc gemm");
 }
@@ -977,6 +1357,11 @@ int oskb_tc_timing_read(double* total_ms, int* launches)
     if (launches) *launches = (int) g_ev_used;
     g_ev_used = 0;
     return 0;
+}
+
+int oskb_tc_tile_columns(void)
+{
+    return g_last_tile;
 }
 
 int oskb_tc_status(const void* workspace, int* flags, int* wait_error)

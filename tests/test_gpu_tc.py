@@ -90,6 +90,68 @@ def test_tc_jones_api(nst, nsrc, casa):
     assert flags[0] == 0 and flags[1] == 0
 
 
+@pytest.mark.parametrize("tile", [128, 256])
+@pytest.mark.parametrize("nst,nsrc,casa", [(17, 300, 0), (64, 1000, 1),
+                                           (130, 777, 0), (161, 2050, 1)])
+def test_tc_tile_widths(tile, nst, nsrc, casa, monkeypatch):
+    """Square (128 x 128) and wide (128 x 256) contraction tiles, with an
+    even and an odd number of 32-station row blocks (17 and 161 stations:
+    one and six blocks; 130: five), against the oracle."""
+    monkeypatch.setenv("OSKB_TC_TILE", str(tile))
+    rng = np.random.default_rng(nst * 7 + nsrc)
+    l, m, n, I, Q, U, V = sky(rng, nsrc)
+    u, v, w = stations(rng, nst)
+    J = rng.normal(0, 0.3, (nst, nsrc, 8))
+    J[..., 0] += 1
+    J[..., 6] += 1
+    J = J.ravel()
+    inv_wl = 130e6 / C0
+    ref = oracle_vis(nst, nsrc, J, I, Q, U, V, l, m, n, u, v, w, inv_wl,
+                     casa=casa)
+    nbl = nst * (nst - 1) // 2
+    vis = torch.zeros(8 * nbl, dtype=torch.float64, device="cuda")
+    ob.call("oskb_cross_correlate_tc_d", casa, nsrc, nst, 0, dev(J), dev(I),
+            dev(Q), dev(U), dev(V), dev(u), dev(v), 0.0, 3e38, inv_wl, vis,
+            None, 0, ob.stream_ptr())
+    torch.cuda.synchronize()
+    assert ob.load().oskb_tc_tile_columns() == tile
+    l2, mx = errors(vis.cpu().numpy(), ref)
+    assert l2 <= TOL and mx <= TOL, (l2, mx)
+    flags = (ob._lib.ctypes.c_int * 2)()
+    ob.call("oskb_tc_status", None, ob._lib.ctypes.addressof(flags),
+            ob._lib.ctypes.addressof(flags) + 4)
+    assert flags[0] == 0 and flags[1] == 0
+
+
+@pytest.mark.parametrize("tile", [128, 256])
+def test_tc_block_tile_widths_agree(tile, monkeypatch):
+    """A block of 2 dumps x 3 channels at 97 stations (four row blocks)
+    through both tile widths: within the compensated tolerance of each
+    other and of the oracle (checked for the wide tiles in
+    test_tc_tile_widths)."""
+    rng = np.random.default_rng(5)
+    nst, nsrc, ntime, nchan = 97, 900, 2, 3
+    l, m, n, I, Q, U, V = sky(rng, nsrc)
+    E = rng.normal(0, 0.1, (nst, nsrc, 8)).astype(np.float32)
+    uvw = np.stack([np.stack(stations(rng, nst)) for _ in range(ntime)])
+    inv_wl = (120e6 + 1e6 * np.arange(nchan)) / C0
+    nbl = nst * (nst - 1) // 2
+    out = {}
+    for t in (128, 256):
+        monkeypatch.setenv("OSKB_TC_TILE", str(t))
+        vis = torch.zeros(ntime * nchan * nbl * 8, dtype=torch.float64,
+                          device="cuda")
+        ob.call("oskb_correlate_block_tc", 0, nsrc, nst, ntime, nchan,
+                dev(E), dev(l), dev(m), dev(n), dev(I), dev(Q), dev(U),
+                dev(V), dev(uvw), dev(inv_wl), 0.0, 3e38, vis, None, 0,
+                ob.stream_ptr())
+        torch.cuda.synchronize()
+        assert ob.load().oskb_tc_tile_columns() == t
+        out[t] = vis.cpu().numpy()
+    l2, mx = errors(out[tile], out[384 - tile])
+    assert l2 <= TOL and mx <= TOL, (l2, mx)
+
+
 def test_tc_accumulates_and_filters():
     """vis is accumulated (+=), and baselines outside the uv range are left
     untouched, as in the reference dispatcher."""
