@@ -731,7 +731,8 @@ OSKB_API int oskb_tc_status(const void* workspace, int* flags,
         int* wait_error);
 /* Tile width (128 or 256 columns of G) of the last tensor-core contraction
  * launched, 0 before the first. The environment variable OSKB_TC_TILE
- * selects it (128, the default, or 256). */
+ * (128 or 256) fixes it; unset, wide tiles are used when a launch has at
+ * least two of them per SM. */
 OSKB_API int oskb_tc_tile_columns(void);
 
 #ifdef __cplusplus

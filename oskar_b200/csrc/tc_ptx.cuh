@@ -170,6 +170,21 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, uint32_t* v)
                  : "r"(taddr) : "memory");
 }
 
+// Per-thread register budget of the executing warp (whole warpgroup, all
+// lanes converged): release down to N, or request up to N (waits until
+// the block's released registers cover it).
+template <int N>
+__device__ __forceinline__ void regs_release()
+{
+    asm volatile("setmaxnreg.dec.sync.aligned.u32 %0;" :: "n"(N) : "memory");
+}
+
+template <int N>
+__device__ __forceinline__ void regs_request()
+{
+    asm volatile("setmaxnreg.inc.sync.aligned.u32 %0;" :: "n"(N) : "memory");
+}
+
 __device__ __forceinline__ void tmem_ld_wait()
 {
     asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");

@@ -671,9 +671,17 @@ gemm_kernel(const GemmParams prm)
 // only then waits for the main accumulator. The correction accumulator
 // (2^-11 of the main one) is drained every kCorrPeriods main drains and at
 // the end of each task.
-// Warp roles as in gemm_kernel (320 threads); the epilogue warps own 128
-// columns each.
+// Warp roles: warpgroup 0 = producer (warp 0), MMA issuer (warp 1) and two
+// idle warps, all releasing registers down to kWLowRegs; warpgroups 1 and 2
+// = eight epilogue warps of 128 columns each, raised to kWHighRegs so that
+// the 64 FP64 sums per thread and two 32-column TMEM loads stay in
+// registers. Budget: 128 x kWLowRegs + 256 x kWHighRegs must not exceed the
+// 384 x (registers per thread at launch) the block starts with; the host
+// checks the compiled count before the first launch.
 // ===========================================================================
+constexpr int kWThreads = 384;
+constexpr int kWLowRegs = 72;
+constexpr int kWHighRegs = 216;
 constexpr int kWStages = 2;
 constexpr int kWStageBytes = 3 * kPairBytes;  // A pair + B hi x2 + B lo x2
 constexpr int kWCols = 256;                   // one accumulator
@@ -718,7 +726,7 @@ __device__ __forceinline__ bool corr_drain_at(int ch, int nchunk)
     return (ch % kCorrPeriods) == kCorrPeriods - 1 || ch == nchunk - 1;
 }
 
-__global__ void __launch_bounds__(kGemmThreads, 1)
+__global__ void __launch_bounds__(kWThreads, 1)
 gemm_wide_kernel(const GemmParams prm)
 {
     extern __shared__ uint8_t smem_raw[];
@@ -753,6 +761,9 @@ gemm_wide_kernel(const GemmParams prm)
     const int ntasks = ntile * prm.num_problems;
     const int nchunk = (prm.nkb + prm.drain_kb - 1) / prm.drain_kb;
 
+    if (warp < 4)
+    {
+    ptx::regs_release<kWLowRegs>();
     if (warp == 0)
     {
         if (lane == 0)
@@ -897,11 +908,14 @@ gemm_wide_kernel(const GemmParams prm)
         }
         __syncwarp();
     }
+    }  // warpgroup 0
     else
     {
-        // ---------------- epilogue: 8 warps, 128 columns each
+        // ---------------- epilogue: 8 warps (4-11), 128 columns each
+        ptx::regs_request<kWHighRegs>();
+        {
         const int q4 = warp & 3;          // TMEM lane quadrant of this warp
-        const int h = (warp - 2) >> 2;    // column half
+        const int h = (warp - 4) >> 2;    // column half
         const int row = 32 * q4 + lane;   // row of the G tile
         const uint32_t taddr = tmem + ((uint32_t) (32 * q4) << 16) +
                 (uint32_t) (128 * h);
@@ -927,35 +941,60 @@ gemm_wide_kernel(const GemmParams prm)
                     break;
                 }
                 ptx::tc_fence_after();
-#pragma unroll
-                for (int j0 = 0; j0 < 128; j0 += 16)
+                // One 32-column TMEM load per wait (main only), or 16 main
+                // and 16 correction columns per wait. Each group of four
+                // columns is one station of the pair of rows (lanes l,
+                // l ^ 1): Re V = G00 + G11, Im V = G10 - G01, combined in
+                // FP32, summed in FP64.
+#define OSKB_WIDE_FOLD(V, J0, NQ)                                              \
+                _Pragma("unroll")                                              \
+                for (int qq = 0; qq < (NQ); ++qq)                              \
+                {                                                              \
+                    const int jb = 4 * qq;                                     \
+                    const float s0 = c ? V[jb + 0] : V[jb + 2];                \
+                    const float s1 = c ? V[jb + 1] : V[jb + 3];                \
+                    const float r0 = __shfl_xor_sync(0xffffffffu, s0, 1);      \
+                    const float r1 = __shfl_xor_sync(0xffffffffu, s1, 1);      \
+                    const float g00 = c ? r0 : V[jb + 0];                      \
+                    const float g01 = c ? r1 : V[jb + 1];                      \
+                    const float g10 = c ? V[jb + 2] : r0;                      \
+                    const float g11 = c ? V[jb + 3] : r1;                      \
+                    accR[(J0) / 4 + qq] += (double) (g00 + g11);               \
+                    accI[(J0) / 4 + qq] += (double) (g10 - g01);               \
+                }
+                if (!with_corr)
                 {
-                    uint32_t vm[16], vc[16];
-                    ptx::tmem_ld16(taddr + j0, vm);
-                    if (with_corr) ptx::tmem_ld16(taddr + kWCols + j0, vc);
-                    ptx::tmem_ld_wait();
-                    float v[16];
 #pragma unroll
-                    for (int j = 0; j < 16; ++j)
-                        v[j] = __uint_as_float(vm[j]) +
-                                (with_corr ? __uint_as_float(vc[j]) : 0.0f);
-                    // polarisation pair combined in FP32, as in gemm_kernel
-#pragma unroll
-                    for (int qq = 0; qq < 4; ++qq)
+                    for (int j0 = 0; j0 < 128; j0 += 32)
                     {
-                        const int jb = 4 * qq;
-                        const float s0 = c ? v[jb + 0] : v[jb + 2];
-                        const float s1 = c ? v[jb + 1] : v[jb + 3];
-                        const float r0 = __shfl_xor_sync(0xffffffffu, s0, 1);
-                        const float r1 = __shfl_xor_sync(0xffffffffu, s1, 1);
-                        const float g00 = c ? r0 : v[jb + 0];
-                        const float g01 = c ? r1 : v[jb + 1];
-                        const float g10 = c ? v[jb + 2] : r0;
-                        const float g11 = c ? v[jb + 3] : r1;
-                        accR[j0 / 4 + qq] += (double) (g00 + g11);
-                        accI[j0 / 4 + qq] += (double) (g10 - g01);
+                        uint32_t va[32];
+                        ptx::tmem_ld32(taddr + j0, va);
+                        ptx::tmem_ld_wait();
+                        float v[32];
+#pragma unroll
+                        for (int j = 0; j < 32; ++j)
+                            v[j] = __uint_as_float(va[j]);
+                        OSKB_WIDE_FOLD(v, j0, 8)
                     }
                 }
+                else
+                {
+#pragma unroll
+                    for (int j0 = 0; j0 < 128; j0 += 16)
+                    {
+                        uint32_t va[16], vb[16];
+                        ptx::tmem_ld16(taddr + j0, va);
+                        ptx::tmem_ld16(taddr + kWCols + j0, vb);
+                        ptx::tmem_ld_wait();
+                        float v[16];
+#pragma unroll
+                        for (int j = 0; j < 16; ++j)
+                            v[j] = __uint_as_float(va[j]) +
+                                    __uint_as_float(vb[j]);
+                        OSKB_WIDE_FOLD(v, j0, 4)
+                    }
+                }
+#undef OSKB_WIDE_FOLD
                 ptx::tc_fence_before();
                 __syncwarp();
                 if (lane == 0)
@@ -1004,6 +1043,7 @@ gemm_wide_kernel(const GemmParams prm)
                     }
                 }
             }
+        }
         }
     }
 
@@ -1109,8 +1149,9 @@ bool g_timing = false;
 std::vector<std::pair<cudaEvent_t, cudaEvent_t>> g_ev;
 size_t g_ev_used = 0;
 
-// Tile width of the contraction: OSKB_TC_TILE=128 (square tiles, the
-// default) or 256 (wide tiles).
+// Tile width of the contraction: OSKB_TC_TILE=128 (square tiles) or 256
+// (wide tiles); unset: wide tiles when a launch has at least two per SM
+// (with fewer, the square tiles keep more SMs busy).
 int tile_setting()
 {
     const char* e = getenv("OSKB_TC_TILE");
@@ -1137,8 +1178,23 @@ int launch_gemm(GemmParams& gp, cudaStream_t stream)
             gp.num_problems;
     const long long wide_n = (long long) wide_tiles(gp.nrb) *
             gp.num_problems;
+    // The wide kernel's register split (kWLowRegs / kWHighRegs) must fit in
+    // the registers its blocks are launched with, or the epilogue's request
+    // would never be granted: checked once against the compiled count.
+    static int wide_fits = -1;
+    if (wide_fits < 0)
+    {
+        cudaFuncAttributes fa;
+        wide_fits = cudaFuncGetAttributes(&fa, gemm_wide_kernel) ==
+                cudaSuccess && (long long) fa.numRegs * kWThreads >=
+                128LL * kWLowRegs + 256LL * kWHighRegs;
+        if (!wide_fits)
+            set_last_error_msg("tc: wide contraction tiles disabled "
+                    "(register budget)");
+    }
     const int setting = tile_setting();
-    const bool wide = setting == 256;
+    const bool wide = wide_fits && (setting == 256 ||
+            (setting == 0 && wide_n >= 2LL * num_sms()));
     const long long ntasks = wide ? wide_n : square;
     const int grid = (int) (ntasks < num_sms() ? ntasks : num_sms());
     g_last_tile = wide ? 256 : 128;
@@ -1158,7 +1214,7 @@ int launch_gemm(GemmParams& gp, cudaStream_t stream)
         ++g_ev_used;
     }
     if (wide)
-        gemm_wide_kernel<<<grid, kGemmThreads, gemm_wide_smem_bytes(),
+        gemm_wide_kernel<<<grid, kWThreads, gemm_wide_smem_bytes(),
                 stream>>>(gp);
     else
         gemm_kernel<<<grid, kGemmThreads, gemm_smem_bytes(), stream>>>(gp);
