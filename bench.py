@@ -528,6 +528,10 @@ def run_profile_case(args):
       tc_small      the tensor-core contraction (gemm_kernel) and its
                     operand preparation (prep_fused_kernel): 512 stations x
                     20,000 sources x 1 channel, 1/80 of a bench launch;
+      tc_wide_small the wide-tile contraction (gemm_wide_kernel, chosen
+                    when a launch has two wide tiles per SM): 512 stations
+                    x 2,500 sources x 8 channels (576 tiles), also 1/80 of
+                    a bench launch;
       direct_small  the FP64 direct cross-correlation: 512 stations x 2,000
                     sources, 1 channel;
       beam_small    the fused station beam: 32 stations x 256 dipoles x
@@ -542,24 +546,26 @@ def run_profile_case(args):
     dev = lambda a: torch.from_numpy(np.ascontiguousarray(a)).cuda()
     stream = ob.stream_ptr()
     case = args.profile_case
-    if case in ("tc_small", "direct_small"):
-        nsrc = 20_000 if case == "tc_small" else 2_000
-        cfg = workloads.c3(num_src=nsrc, num_channels=1, num_times=1)
+    if case in ("tc_small", "tc_wide_small", "direct_small"):
+        nsrc = {"tc_small": 20_000, "tc_wide_small": 2_500,
+                "direct_small": 2_000}[case]
+        nch = 8 if case == "tc_wide_small" else 1
+        cfg = workloads.c3(num_src=nsrc, num_channels=nch, num_times=1)
         nst, nbl = cfg.num_st, cfg.num_baselines
         l, m, n, I, Q, U, V = (dev(x) for x in (cfg.l, cfg.m, cfg.n, cfg.I,
                                                 cfg.Q, cfg.U, cfg.V))
         E = workloads.jones_e_device(cfg, torch.float32)
         uvw = dev(cfg.station_uvw(0)[None])
         inv_wl = dev(cfg.freqs_hz / 299792458.0)
-        vis = torch.zeros((1, nbl, 8), dtype=torch.float64, device="cuda")
-        if case == "tc_small":
+        vis = torch.zeros((nch, nbl, 8), dtype=torch.float64, device="cuda")
+        if case != "direct_small":
             ws_bytes = ob.call("oskb_correlate_block_tc_workspace_bytes",
-                               nsrc, nst, 1, check=False)
+                               nsrc, nst, nch, check=False)
             ws = torch.empty(ws_bytes, dtype=torch.uint8, device="cuda")
             for _ in range(2):
-                ob.call("oskb_correlate_block_tc", 0, nsrc, nst, 1, 1, E, l,
-                        m, n, I, Q, U, V, uvw, inv_wl, 0.0, 3e38, vis, ws,
-                        ws_bytes, stream)
+                ob.call("oskb_correlate_block_tc", 0, nsrc, nst, 1, nch, E,
+                        l, m, n, I, Q, U, V, uvw, inv_wl, 0.0, 3e38, vis,
+                        ws, ws_bytes, stream)
         else:
             f = float(cfg.freqs_hz[0])
             u, v, w = uvw[0]
@@ -1132,7 +1138,8 @@ def main():
     ap.add_argument("--c5-steps", type=int, default=20000)
     ap.add_argument("--c5-bound", type=float, default=1e-4)
     ap.add_argument("--profile-case", default=None,
-                    choices=["tc_small", "direct_small", "beam_small",
+                    choices=["tc_small", "tc_wide_small", "direct_small",
+                             "beam_small",
                              "block_small"],
                     help="run one small kernel case for an ncu capture")
     args = ap.parse_args()
