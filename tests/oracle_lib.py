@@ -104,3 +104,46 @@ def reference_xcorr(real, matrix, gaussian, *args):
 
 def suffix(real):
     return "d" if real == np.float64 else "f"
+
+
+REF_CUDA_SO = os.path.join(ROOT, "oracle", "_ref", "liboskar_ref_cuda.so")
+
+
+def reference_cuda():
+    """The reference's own CUDA cross-correlation kernels compiled from its
+    sources (``make -C oracle ref_cuda``), or None where not built."""
+    if "ref_cuda" not in _cache:
+        _cache["ref_cuda"] = (ctypes.CDLL(REF_CUDA_SO)
+                              if os.path.exists(REF_CUDA_SO) else None)
+    return _cache["ref_cuda"]
+
+
+def reference_cuda_xcorr(real, matrix, gaussian, casa, num_src, num_st,
+                         offset_out, jones, I, Q, U, V, l, m, n, a, b, c,
+                         st_u, st_v, st_w, st_x, st_y, uv_min, uv_max,
+                         inv_wavelength, frac_bandwidth, time_int_sec, gha0,
+                         dec0, vis):
+    """Calls oskar_cross_correlate_[scalar_]{point,gaussian}_cuda_{f,d}
+    (correlate/oskar_cross_correlate_cuda.h, _scalar_cuda.h) with device
+    pointers (ints) and host scalars; launches on the legacy stream."""
+    lib = reference_cuda()
+    s = "d" if real == np.float64 else "f"
+    kind = "gaussian" if gaussian else "point"
+    fn = getattr(lib, "oskar_cross_correlate_" + ("" if matrix else
+                                                 "scalar_") + kind
+                 + "_cuda_" + s)
+    fp = ctypes.c_double if real == np.float64 else ctypes.c_float
+    p = lambda x: ctypes.c_void_p(x)
+    args = [ctypes.c_int(casa), ctypes.c_int(num_src), ctypes.c_int(num_st),
+            ctypes.c_int(offset_out), p(jones), p(I)]
+    if matrix:
+        args += [p(Q), p(U), p(V)]
+    args += [p(l), p(m), p(n)]
+    if gaussian:
+        args += [p(a), p(b), p(c)]
+    args += [p(st_u), p(st_v), p(st_w), p(st_x), p(st_y)]
+    args += [fp(x) for x in (uv_min, uv_max, inv_wavelength, frac_bandwidth,
+                             time_int_sec, gha0, dec0)]
+    args.append(p(vis))
+    fn.restype = None
+    fn(*args)
