@@ -185,7 +185,8 @@ OSKB_API int oskb_dftw_f(int matrix, int num_in, float wavenumber,
         const int* data_idx, const float* data, int eval_x, int eval_y,
         int offset_out, float* output, float norm_factor, void* stream);
 
-/* Beamforming weights w_e = exp(-i wavenumber (x x1 + y y1 + z z1 + cable_e)).
+/* Beamforming weights w_e = exp(-i wavenumber (x x1 + y y1 + z z1 + cable_e)),
+ * z and cable_length_error may be NULL (zero).
  * Replaces the kernel behind oskar_evaluate_element_weights_dft
  * (oskar/telescope/station/oskar_evaluate_element_weights_dft.h:66;
  *  define_evaluate_element_weights_dft.h:3-16). */
@@ -244,6 +245,52 @@ OSKB_API int oskb_station_beam_aa_f(int num_stations, int num_elements,
         int swap_xy, int is_3d, double frequency_hz, const double* beam_enu,
         const double* norm_enu, int num_directions, const float* x,
         const float* y, const float* z, int directions_per_station,
+        float* beam, void* stream);
+
+/* Two-level (hierarchical) aperture-array station: a station of num_tiles
+ * tiles at ENU positions tile_x/y/z [tile] (true positions, metres), tile t
+ * a dipole array of layout tile_type[t] (NULL: every tile of layout 0, the
+ * reference's identical children); layout i has num_elements dipoles at
+ * el_x/y/z [i][element] and orientations orientation_x/y_rad [i]. Beam
+ * [direction][2x2] = (1/num_tiles if normalise_station_array) x
+ * sum_t w_t exp(i k r_t . d) x tilebeam[type(t)][d], with parent weights
+ * w_t = exp(-i k r_t . b) for the pointing b = (beam_x, beam_y, beam_z)
+ * (host, ENU), and each tile beam the fused single-level beam
+ * (oskb_station_beam_aa: dipole pattern, tile array factor pointed at b,
+ * normalise_element / normalise_tile_array, blanked below the horizon).
+ * The two-level case of the reference's recursion
+ * (oskar_evaluate_station_beam_aperture_array.c:242-287, child beams as the
+ * parent's weighted-DFT data, oskar_dftw with element weights from
+ * oskar_station_evaluate_element_weights.c:15-66); the normalisation to
+ * the beam direction (oskar_station_beam.c:108-135) is the caller's, as in
+ * the reference. workspace: device, at least
+ * oskb_station_beam_two_level_workspace_bytes(sizeof(T), num_tile_types,
+ * num_tiles, num_directions) bytes. Directions x, y, z: device [direction],
+ * ENU direction cosines. */
+OSKB_API size_t oskb_station_beam_two_level_workspace_bytes(
+        int precision_bytes, int num_tile_types, int num_tiles,
+        int num_directions);
+OSKB_API int oskb_station_beam_two_level_d(int num_tile_types,
+        int num_elements, const double* el_x, const double* el_y,
+        const double* el_z, const double* orientation_x_rad,
+        const double* orientation_y_rad, double dipole_length_m,
+        int normalise_element, int normalise_tile_array, int num_tiles,
+        const double* tile_x, const double* tile_y, const double* tile_z,
+        const int* tile_type, int normalise_station_array, int swap_xy,
+        int is_3d, double frequency_hz, double beam_x, double beam_y,
+        double beam_z, int num_directions, const double* x, const double* y,
+        const double* z, void* workspace, size_t workspace_bytes,
+        double* beam, void* stream);
+OSKB_API int oskb_station_beam_two_level_f(int num_tile_types,
+        int num_elements, const float* el_x, const float* el_y,
+        const float* el_z, const double* orientation_x_rad,
+        const double* orientation_y_rad, double dipole_length_m,
+        int normalise_element, int normalise_tile_array, int num_tiles,
+        const float* tile_x, const float* tile_y, const float* tile_z,
+        const int* tile_type, int normalise_station_array, int swap_xy,
+        int is_3d, double frequency_hz, double beam_x, double beam_y,
+        double beam_z, int num_directions, const float* x, const float* y,
+        const float* z, void* workspace, size_t workspace_bytes,
         float* beam, void* stream);
 
 /* ------------------------------------------------------------------------

@@ -323,3 +323,156 @@ OSKB_BEAM_ENTRY(float, f)
 #undef OSKB_BEAM_ENTRY
 
 }  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Two-level (hierarchical) aperture-array stations: a station of tiles, each
+// tile a dipole array of one of num_tile_types layouts. The reference
+// recurses (oskar_evaluate_station_beam_aperture_array.c:242-287): it
+// evaluates every child station's beam, copying the first child's beam to
+// all children when they are identical, then forms the parent's weighted
+// DFT over its children with the child beams as the data. Here: one fused
+// station-beam launch evaluates all tile types at once (each type once,
+// however many tiles share it), one launch forms the parent's DFT weights,
+// and one weighted DFT sums the tiles with data index = the tile's type, so
+// identical tiles need no copies.
+// ---------------------------------------------------------------------------
+namespace oskb {
+namespace {
+
+__global__ void two_level_setup_kernel(int num_types, double bx, double by,
+        double bz, double* pointing, int num_tiles, int* zero_idx)
+{
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x;
+            i < num_types || i < num_tiles; i += gridDim.x * blockDim.x)
+    {
+        if (i < num_types)
+        {
+            pointing[3 * i] = bx;
+            pointing[3 * i + 1] = by;
+            pointing[3 * i + 2] = bz;
+        }
+        if (zero_idx && i < num_tiles) zero_idx[i] = 0;
+    }
+}
+
+size_t align256(size_t b) { return (b + 255) & ~(size_t) 255; }
+
+size_t two_level_workspace(size_t elem, int num_tile_types, int num_tiles,
+        int num_directions)
+{
+    return align256(elem * 8 * (size_t) num_tile_types * num_directions) +
+            align256(elem * 2 * (size_t) num_tiles) +
+            align256(sizeof(double) * 3 * (size_t) num_tile_types) +
+            align256(sizeof(int) * (size_t) num_tiles);
+}
+
+template <typename T>
+int station_beam_two_level(int num_tile_types, int num_elements,
+        const T* el_x, const T* el_y, const T* el_z,
+        const double* orientation_x, const double* orientation_y,
+        double dipole_length_m, int normalise_element,
+        int normalise_tile_array, int num_tiles, const T* tile_x,
+        const T* tile_y, const T* tile_z, const int* tile_type,
+        int normalise_station_array, int swap_xy, int is_3d,
+        double frequency_hz, double bx, double by, double bz,
+        int num_directions, const T* x, const T* y, const T* z,
+        void* workspace, size_t workspace_bytes, T* beam, void* stream)
+{
+    if (num_tile_types < 1 || num_tiles < 0 || num_directions < 0 ||
+            num_tile_types > 65535)
+        return OSKB_ERR_INVALID_ARGUMENT;
+    if (num_tiles == 0 || num_directions == 0) return 0;
+    if (!tile_x || !tile_y || (is_3d && !tile_z) || !workspace || !beam)
+        return OSKB_ERR_INVALID_ARGUMENT;
+    if (workspace_bytes < two_level_workspace(sizeof(T), num_tile_types,
+            num_tiles, num_directions))
+        return OSKB_ERR_MEMORY_ALLOC_FAILURE;
+    uint8_t* w = static_cast<uint8_t*>(workspace);
+    T* tile_beams = reinterpret_cast<T*>(w);
+    w += align256(sizeof(T) * 8 * (size_t) num_tile_types * num_directions);
+    T* weights = reinterpret_cast<T*>(w);
+    w += align256(sizeof(T) * 2 * (size_t) num_tiles);
+    double* pointing = reinterpret_cast<double*>(w);
+    w += align256(sizeof(double) * 3 * (size_t) num_tile_types);
+    int* zero_idx = tile_type ? nullptr : reinterpret_cast<int*>(w);
+    cudaStream_t s = as_stream(stream);
+    const int n = num_tile_types > num_tiles ? num_tile_types : num_tiles;
+    two_level_setup_kernel<<<(n + 255) / 256, 256, 0, s>>>(num_tile_types,
+            bx, by, bz, pointing, num_tiles, zero_idx);
+    if (int err = check_launch("station_beam_two_level")) return err;
+    // tile beams [type][direction]: element pattern x tile array factor,
+    // blanked below the horizon, no final normalisation
+    if (int err = station_beam_aa<T>(num_tile_types, num_elements, el_x,
+            el_y, el_z, nullptr, nullptr, nullptr, nullptr, orientation_x,
+            orientation_y, dipole_length_m, normalise_element,
+            normalise_tile_array, 0, swap_xy, is_3d, frequency_hz, pointing,
+            nullptr, num_directions, x, y, z, 0, tile_beams, stream))
+        return err;
+    const double k = 2.0 * kPi * frequency_hz / 299792458.0;
+    const T* zt = is_3d ? tile_z : nullptr;
+    const T* zo = is_3d ? z : nullptr;
+    const int* idx = tile_type ? tile_type : zero_idx;
+    const T norm = normalise_station_array ? (T) (1.0 / num_tiles) : (T) 1;
+    if constexpr (sizeof(T) == 8)
+    {
+        if (int err = oskb_evaluate_element_weights_dft_d(num_tiles, tile_x,
+                tile_y, zt, nullptr, k, bx, by, is_3d ? bz : 0.0, weights,
+                stream))
+            return err;
+        return oskb_dftw_d(1, num_tiles, k, weights, tile_x, tile_y, zt, 0,
+                num_directions, x, y, zo, idx, tile_beams, 1, 1, 0, beam,
+                norm, stream);
+    }
+    else
+    {
+        if (int err = oskb_evaluate_element_weights_dft_f(num_tiles, tile_x,
+                tile_y, zt, nullptr, (float) k, (float) bx, (float) by,
+                (float) (is_3d ? bz : 0.0), weights, stream))
+            return err;
+        return oskb_dftw_f(1, num_tiles, (float) k, weights, tile_x, tile_y,
+                zt, 0, num_directions, x, y, zo, idx, tile_beams, 1, 1, 0,
+                beam, norm, stream);
+    }
+}
+
+}  // namespace
+}  // namespace oskb
+
+extern "C" {
+
+size_t oskb_station_beam_two_level_workspace_bytes(int precision_bytes,
+        int num_tile_types, int num_tiles, int num_directions)
+{
+    if (num_tile_types < 1 || num_tiles < 0 || num_directions < 0 ||
+            (precision_bytes != 4 && precision_bytes != 8))
+        return 0;
+    return oskb::two_level_workspace((size_t) precision_bytes,
+            num_tile_types, num_tiles, num_directions);
+}
+
+#define OSKB_TWO_LEVEL_ENTRY(T, S)                                           \
+int oskb_station_beam_two_level_##S(int num_tile_types, int num_elements,    \
+        const T* el_x, const T* el_y, const T* el_z,                         \
+        const double* orientation_x_rad, const double* orientation_y_rad,    \
+        double dipole_length_m, int normalise_element,                       \
+        int normalise_tile_array, int num_tiles, const T* tile_x,            \
+        const T* tile_y, const T* tile_z, const int* tile_type,              \
+        int normalise_station_array, int swap_xy, int is_3d,                 \
+        double frequency_hz, double beam_x, double beam_y, double beam_z,    \
+        int num_directions, const T* x, const T* y, const T* z,              \
+        void* workspace, size_t workspace_bytes, T* beam, void* stream)      \
+{                                                                            \
+    return oskb::station_beam_two_level<T>(num_tile_types, num_elements,     \
+            el_x, el_y, el_z, orientation_x_rad, orientation_y_rad,          \
+            dipole_length_m, normalise_element, normalise_tile_array,        \
+            num_tiles, tile_x, tile_y, tile_z, tile_type,                    \
+            normalise_station_array, swap_xy, is_3d, frequency_hz, beam_x,   \
+            beam_y, beam_z, num_directions, x, y, z, workspace,              \
+            workspace_bytes, beam, stream);                                  \
+}
+
+OSKB_TWO_LEVEL_ENTRY(double, d)
+OSKB_TWO_LEVEL_ENTRY(float, f)
+#undef OSKB_TWO_LEVEL_ENTRY
+
+}  // extern "C"

@@ -238,7 +238,9 @@ __global__ void weights_kernel(int n, const T* x, const T* y, const T* z,
 {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
-    const T p = k * (x[i] * x1 + y[i] * y1 + z[i] * z1 + cable[i]);
+    // z or cable NULL: zero (a 2-D layout; no cable errors)
+    const T p = k * (x[i] * x1 + y[i] * y1 + (z ? z[i] * z1 : (T) 0) +
+            (cable ? cable[i] : (T) 0));
     T sn, cs;
     sincos(-p, &sn, &cs);
     w[2 * i] = cs;
@@ -333,7 +335,7 @@ int weights(int n, const T* x, const T* y, const T* z, const T* cable, T k,
 {
     if (n < 0) return OSKB_ERR_INVALID_ARGUMENT;
     if (n == 0) return 0;
-    if (!x || !y || !z || !cable || !w) return OSKB_ERR_INVALID_ARGUMENT;
+    if (!x || !y || !w) return OSKB_ERR_INVALID_ARGUMENT;
     weights_kernel<T><<<(n + 255) / 256, 256, 0, as_stream(stream)>>>(n, x,
             y, z, cable, k, x1, y1, z1, w);
     return check_launch("element_weights_dft");
