@@ -782,6 +782,55 @@ OSKB_API int oskb_tc_status(const void* workspace, int* flags,
  * least two of them per SM. */
 OSKB_API int oskb_tc_tile_columns(void);
 
+/* ------------------------------------------------------------------------
+ * Visibility files (.vis, OSKAR binary format version 2): block
+ * finalisation / output, replacing oskar_vis_header_write
+ * (oskar/vis/src/oskar_vis_header_write.c:20-253) and
+ * oskar_vis_block_write (oskar/vis/src/oskar_vis_block_write.c:16-70).
+ * ------------------------------------------------------------------------
+ * HOST pointers throughout. oskb_vis_file_create opens the file, writes the
+ * file header and the visibility header: amp_type is the OSKAR type code
+ * of the visibilities (complex, or complex matrix for 4 polarisations;
+ * single 0x04 or double 0x08 | complex 0x20 | matrix 0x40),
+ * coord_precision 0x04 or 0x08 the type of station_x/y/z (offset ECEF,
+ * [station]), element_x/y/z (ENU, [station][element], num_elements
+ * [station] or NULL) and of the per-block station (u, v, w);
+ * element_feed_angles: double [feed X, Y][angle a, b, c][all elements] or
+ * NULL; station_diameter_m [station] or NULL (0); station_names
+ * [station] or NULL (""); telescope_path, settings (file contents) may be
+ * NULL. date_time, version, cwd, username: the metadata strings, NULL for
+ * the current time, this library's version, the working directory and
+ * $USERNAME / $USER. max_times_per_block / max_channels_per_block <= 0
+ * mean all. On error returns NULL with *status set.
+ * oskb_vis_file_write_block writes one block: dimensions, then the
+ * auto-correlations [time][channel][station] (if the file has them), the
+ * cross-correlations [time][channel][baseline] and, when all three are
+ * given, station u, v, w [time][station] metres. */
+typedef struct oskb_VisFile oskb_VisFile;
+OSKB_API oskb_VisFile* oskb_vis_file_create(const char* filename,
+        int amp_type, int coord_precision, int max_times_per_block,
+        int num_times_total, int max_channels_per_block,
+        int num_channels_total, int num_stations, int write_autocorr,
+        int write_crosscorr, int casa_phase_convention, double freq_start_hz,
+        double freq_inc_hz, double channel_bandwidth_hz,
+        double time_start_mjd_utc, double time_inc_sec,
+        double time_average_sec, int phase_centre_coord_type,
+        double phase_centre_lon_deg, double phase_centre_lat_deg,
+        double telescope_lon_deg, double telescope_lat_deg,
+        double telescope_alt_m, const void* station_x, const void* station_y,
+        const void* station_z, const double* station_diameter_m,
+        const char* const* station_names, const int* num_elements,
+        const void* element_x, const void* element_y, const void* element_z,
+        const double* element_feed_angles, const char* telescope_path,
+        const char* settings, const char* date_time, const char* version,
+        const char* cwd, const char* username, int* status);
+OSKB_API int oskb_vis_file_write_block(oskb_VisFile* file, int block_index,
+        int start_time_index, int start_channel_index, int num_times,
+        int num_channels, const void* cross_correlations,
+        const void* auto_correlations, const void* station_u,
+        const void* station_v, const void* station_w);
+OSKB_API int oskb_vis_file_close(oskb_VisFile* file);
+
 #ifdef __cplusplus
 }
 #endif
