@@ -147,6 +147,13 @@ __device__ __forceinline__ void cp_async_wait_all()
     asm volatile("cp.async.wait_group 0;\n" ::: "memory");
 }
 
+// Waits until at most N of this thread's cp.async groups are pending.
+template <int N>
+__device__ __forceinline__ void cp_async_wait_group()
+{
+    asm volatile("cp.async.wait_group %0;\n" :: "n"(N) : "memory");
+}
+
 // sinc(phi_p - phi_q) = sin(phi_p - phi_q) / (phi_p - phi_q), the
 // reference's smearing factor (define_cross_correlate.h:16-32), from the
 // per-station sin and cos: sin(a - b) = sin a cos b - cos a sin b. Where the
@@ -738,35 +745,25 @@ xcorr_direct_kernel(const XcorrParams<T> prm)
 }
 
 // ---------------------------------------------------------------------------
-// FP64 tensor-core form for point sources without smearing (matrix, FP64):
-// the same staging (cp.async of the raw Jones, shared-to-shared transform
-// to the left factor J B and the right factor J), then the per-tile
-// product on the FP64 tensor pipe with mma.sync m8n8k4 f64 instead of SIMT
-// FMAs. Real embedding: with M = left factor (station p, rows) and
-// R = right factor (station q, columns), entries W[(s, i, c)][(src, k)] =
-// Re (c = 0) or Im (c = 1) of the 2x2 entry (i, k), and
-//     G = W_M W_R^T,  Re V_ij = G[(p,i,0)][(q,j,0)] + G[(p,i,1)][(q,j,1)],
-//                     Im V_ij = G[(p,i,1)][(q,j,0)] - G[(p,i,0)][(q,j,1)].
-// The 128 x 128 G tile of a 32 x 32 station tile is split over 8 warps as
-// 4 (rows) x 2 (columns) warp tiles of 32 x 64 = 4 x 8 m8n8 accumulators;
-// a k4 step is two sources. Accumulation is FP64 throughout (no
-// brightness factorisation, so any B).
+// FP64 tensor-core form: staging, transform and kernel.
 // ---------------------------------------------------------------------------
 // Fragment-ordered operands of one chunk: per block (rows, columns),
-// kChunk / 2 k4 steps x 16 tiles of 8 rows x kFragTile doubles. They live
-// in the shared-memory factor and phase areas, which this kernel does not
-// otherwise use (contiguous in Smem).
+// kChunk / 2 k4 steps x 16 tiles of 8 rows x kFragTile doubles.
 constexpr int kFragTile = 33;
 constexpr int kFragK4 = (4 * kTile / 8) * kFragTile;
 constexpr int kFragBlock = (kChunk / 2) * kFragK4;
-static_assert(2 * kFragBlock * sizeof(double) <=
-        sizeof(Smem<double, true>::row) + sizeof(Smem<double, true>::col) +
-        sizeof(Smem<double, true>::ph), "fragment area exceeds its space");
 
-__device__ __forceinline__ double* fragment_base(Smem<double, true>& sm)
+// Shared memory of the FP64 tensor-core kernel: the raw Jones of two
+// chunks and the fragment-ordered operands of two chunks, so that one
+// chunk's products run while the next chunk is transformed (one barrier per
+// chunk).
+struct DmmaSmem
 {
-    return reinterpret_cast<double*>(&sm.row[0][0][0]);
-}
+    // [buffer][block][piece][source][station] x 16 bytes
+    __align__(16) unsigned char raw[2][2][4][kChunk][kTile][16];
+    double src[2][kChunk][4];        // [buffer][source][I, Q, U, V]
+    double frag[2][2 * kFragBlock];  // [buffer][rows block, columns block]
+};
 
 __device__ __forceinline__ void dmma_m8n8k4(double& d0, double& d1,
         double a, double b)
@@ -776,15 +773,110 @@ __device__ __forceinline__ void dmma_m8n8k4(double& d0, double& d1,
                  : "+d"(d0), "+d"(d1) : "d"(a), "d"(b));
 }
 
+// Warp w stages and transforms source sl = w of every chunk, both blocks
+// (64 elements): its copies land 8 stations x 4 pieces per instruction
+// (whole 64-byte elements of 8 stations, coalesced; 4 x 128 contiguous
+// bytes in shared memory), and its own cp.async wait plus __syncwarp make
+// them visible to its lanes, so no block barrier is needed before the
+// transform. Lanes 0-3 stage the source's I, Q, U, V.
+__device__ __forceinline__ void dmma_issue(DmmaSmem& sm, int buf,
+        const XcorrParams<double>& prm, const ItemCtx& ctx, int s0)
+{
+    const int lane = threadIdx.x & 31, sl = threadIdx.x >> 5;
+    const unsigned char* jb = reinterpret_cast<const unsigned char*>(
+            prm.jones);
+    const int s = s0 + sl;
+    const bool src_in = s < ctx.src_end;
+    const int a = lane & 7, pc = lane >> 3;
+#pragma unroll
+    for (int i = 0; i < 8; ++i)
+    {
+        const int blk = i >> 2, stl = 8 * (i & 3) + a;
+        const int st = (blk ? ctx.q0 : ctx.p0) + stl;
+        const bool in = st < prm.num_st && src_in;
+        const unsigned char* src = in ? jb + ((size_t) st * prm.src_stride +
+                s) * 64 + 16 * pc : jb;
+        cp_async(sm.raw[buf][blk][pc][sl][stl], src, in, 16);
+    }
+    if (lane < 4)
+    {
+        const double* arr = lane == 0 ? prm.I : lane == 1 ? prm.Q :
+                lane == 2 ? prm.U : prm.V;
+        cp_async(&sm.src[buf][sl][lane], src_in ? arr + s : prm.I, src_in,
+                8);
+    }
+    cp_async_commit();
+}
+
+// Left factor J B (rows unless CASA) and right factor J of lane stl's two
+// elements of the warp's source, written in fragment order: W entry (row
+// r, k) of a block at frag[k / 4][r / 8][4 (r % 8) + k % 4] (tiles of 8 rows
+// padded to kFragTile doubles against bank conflicts), so the mma.sync
+// operand of lane (g, t) = (r % 8, k % 4) is one 8-byte load per lane (row
+// r = 4 stl + 2 i + c, k = 2 sl + kk).
+template <bool CASA>
+__device__ __forceinline__ void dmma_transform(DmmaSmem& sm, int buf,
+        int fbuf)
+{
+    typedef double2 T2;
+    const int stl = threadIdx.x & 31, sl = threadIdx.x >> 5;
+    __syncwarp();  // the warp's own copies, landed, visible to all lanes
+#pragma unroll
+    for (int blk = 0; blk < 2; ++blk)
+    {
+        Mat2<double> J;
+        J.a = *reinterpret_cast<const T2*>(sm.raw[buf][blk][0][sl][stl]);
+        J.b = *reinterpret_cast<const T2*>(sm.raw[buf][blk][1][sl][stl]);
+        J.c = *reinterpret_cast<const T2*>(sm.raw[buf][blk][2][sl][stl]);
+        J.d = *reinterpret_cast<const T2*>(sm.raw[buf][blk][3][sl][stl]);
+        if ((blk == 0) != CASA)
+        {
+            const double I = sm.src[buf][sl][0], Q = sm.src[buf][sl][1];
+            const T2 buv = T2{sm.src[buf][sl][2], sm.src[buf][sl][3]};
+            const T2 buvc = T2{buv.x, -buv.y};
+            const double xx = I + Q, yy = I - Q;
+            Mat2<double> M;
+            const T2 t0 = cmul<double>(J.b, buvc), t1 = cmul<double>(J.d, buvc);
+            const T2 t2 = cmul<double>(J.a, buv), t3 = cmul<double>(J.c, buv);
+            M.a = T2{J.a.x * xx + t0.x, J.a.y * xx + t0.y};
+            M.c = T2{J.c.x * xx + t1.x, J.c.y * xx + t1.y};
+            M.b = T2{J.b.x * yy + t2.x, J.b.y * yy + t2.y};
+            M.d = T2{J.d.x * yy + t3.x, J.d.y * yy + t3.y};
+            J = M;
+        }
+        double* frag = sm.frag[fbuf] + (blk ? kFragBlock : 0);
+#define OSKB_FRAG(I, KK, C, VAL)                                             \
+        frag[((2 * sl + KK) >> 2) * kFragK4 +                                \
+                ((4 * stl + 2 * I + C) >> 3) * kFragTile +                   \
+                4 * ((4 * stl + 2 * I + C) & 7) + ((2 * sl + KK) & 3)] = VAL;
+        OSKB_FRAG(0, 0, 0, J.a.x) OSKB_FRAG(0, 0, 1, J.a.y)
+        OSKB_FRAG(0, 1, 0, J.b.x) OSKB_FRAG(0, 1, 1, J.b.y)
+        OSKB_FRAG(1, 0, 0, J.c.x) OSKB_FRAG(1, 0, 1, J.c.y)
+        OSKB_FRAG(1, 1, 0, J.d.x) OSKB_FRAG(1, 1, 1, J.d.y)
+#undef OSKB_FRAG
+    }
+}
+
+// FP64 tensor-core form for point sources without smearing (matrix, FP64):
+// the product of each 32 x 32 station tile on the FP64 tensor pipe with
+// mma.sync m8n8k4 f64. Real embedding: with M = left factor (station p,
+// rows) and R = right factor (station q, columns), entries
+// W[(s, i, c)][(src, k)] = Re (c = 0) or Im (c = 1) of the 2x2 entry (i, k),
+// and
+//     G = W_M W_R^T,  Re V_ij = G[(p,i,0)][(q,j,0)] + G[(p,i,1)][(q,j,1)],
+//                     Im V_ij = G[(p,i,1)][(q,j,0)] - G[(p,i,0)][(q,j,1)].
+// The 128 x 128 G tile is split over 8 warps as 4 (rows) x 2 (columns) warp
+// tiles of 32 x 64 = 4 x 8 m8n8 accumulators; a k4 step is two sources.
+// Accumulation is FP64 throughout (no brightness factorisation, so any B).
+// Pipeline per chunk c: copies of chunk c + 2 in flight, products of chunk
+// c on the tensor pipe, transform of chunk c + 1 on the FP64 pipe, one
+// barrier.
 template <bool CASA>
 __global__ void __launch_bounds__(kThreads, 1)
 xcorr_dmma_kernel(const XcorrParams<double> prm)
 {
-    typedef double2 T2;
-    typedef Smem<double, true> S;
-    typedef Staging<double, true> G;
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    S& sm = *reinterpret_cast<S*>(smem_raw);
+    DmmaSmem& sm = *reinterpret_cast<DmmaSmem*>(smem_raw);
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int wm = warp & 3, wn = warp >> 2;   // warp tile: rows, columns
     const int g = lane >> 2, t = lane & 3;     // mma fragment coordinates
@@ -806,10 +898,8 @@ xcorr_dmma_kernel(const XcorrParams<double> prm)
     }
     ctx.src_begin = slice * prm.slice_len;
     ctx.src_end = min(prm.num_src, ctx.src_begin + prm.slice_len);
-    __syncthreads();  // the previous item is done with shared memory
-    if (ctx.src_begin < ctx.src_end)
-        issue_chunk<double, true, false, false>(sm, prm, prm.jones, ctx,
-                ctx.src_begin);
+    const int nchunks = ctx.src_end > ctx.src_begin ?
+            (ctx.src_end - ctx.src_begin + kChunk - 1) / kChunk : 0;
 
     double acc[4][8][2];
 #pragma unroll
@@ -817,64 +907,35 @@ xcorr_dmma_kernel(const XcorrParams<double> prm)
 #pragma unroll
         for (int ns = 0; ns < 8; ++ns) acc[ms][ns][0] = acc[ms][ns][1] = 0.0;
 
-    for (int s0 = ctx.src_begin; s0 < ctx.src_end; s0 += kChunk)
+    __syncthreads();  // the previous item is done with shared memory
+    if (nchunks > 0)
     {
-        cp_async_wait_all();
-        __syncthreads();
-        // ---- transform: left factor J B (rows unless CASA), right J
-        for (int it = tid; it < 2 * kTile * kChunk; it += kThreads)
+        dmma_issue(sm, 0, prm, ctx, ctx.src_begin);
+        if (nchunks > 1)
         {
-            const int blk = it / (kTile * kChunk);
-            const int rem = it - blk * (kTile * kChunk);
-            const int stl = rem % kTile, sl = rem / kTile;
-            Mat2<double> J;
-            J.a = *reinterpret_cast<const T2*>(sm.raw[blk][0][sl][stl]);
-            J.b = *reinterpret_cast<const T2*>(sm.raw[blk][1][sl][stl]);
-            J.c = *reinterpret_cast<const T2*>(sm.raw[blk][2][sl][stl]);
-            J.d = *reinterpret_cast<const T2*>(sm.raw[blk][3][sl][stl]);
-            if ((blk == 0) != CASA)
-            {
-                const double I = sm.raw_src[kI][sl], Q = sm.raw_src[kQ][sl];
-                const T2 buv = T2{sm.raw_src[kU][sl], sm.raw_src[kV][sl]};
-                const T2 buvc = T2{buv.x, -buv.y};
-                const double xx = I + Q, yy = I - Q;
-                Mat2<double> M;
-                const T2 t0 = cmul<double>(J.b, buvc), t1 = cmul<double>(J.d, buvc);
-                const T2 t2 = cmul<double>(J.a, buv), t3 = cmul<double>(J.c, buv);
-                M.a = T2{J.a.x * xx + t0.x, J.a.y * xx + t0.y};
-                M.c = T2{J.c.x * xx + t1.x, J.c.y * xx + t1.y};
-                M.b = T2{J.b.x * yy + t2.x, J.b.y * yy + t2.y};
-                M.d = T2{J.d.x * yy + t3.x, J.d.y * yy + t3.y};
-                J = M;
-            }
-            // Fragment order: W entry (row r, k) of this block at
-            // frag[k / 4][r / 8][4 (r % 8) + k % 4] (tiles of 8 rows padded
-            // to kFragTile doubles against bank conflicts of these stores),
-            // so the mma.sync operand of lane (g, t) = (r % 8, k % 4) is one
-            // consecutive 8-byte load per lane (row r = 4 stl + 2 i + c,
-            // k = 2 sl + kk).
-            double* frag = fragment_base(sm) + (blk ? kFragBlock : 0);
-#define OSKB_FRAG(I, KK, C, VAL)                                             \
-            frag[((2 * sl + KK) >> 2) * kFragK4 +                            \
-                    ((4 * stl + 2 * I + C) >> 3) * kFragTile +               \
-                    4 * ((4 * stl + 2 * I + C) & 7) + ((2 * sl + KK) & 3)] =  \
-                    VAL;
-            OSKB_FRAG(0, 0, 0, J.a.x) OSKB_FRAG(0, 0, 1, J.a.y)
-            OSKB_FRAG(0, 1, 0, J.b.x) OSKB_FRAG(0, 1, 1, J.b.y)
-            OSKB_FRAG(1, 0, 0, J.c.x) OSKB_FRAG(1, 0, 1, J.c.y)
-            OSKB_FRAG(1, 1, 0, J.d.x) OSKB_FRAG(1, 1, 1, J.d.y)
-#undef OSKB_FRAG
+            dmma_issue(sm, 1, prm, ctx, ctx.src_begin + kChunk);
+            cp_async_wait_group<1>();
         }
+        else
+        {
+            cp_async_wait_group<0>();
+        }
+        dmma_transform<CASA>(sm, 0, 0);
         __syncthreads();
-        if (s0 + kChunk < ctx.src_end)
-            issue_chunk<double, true, false, false>(sm, prm, prm.jones, ctx,
-                    s0 + kChunk);
-
-        // ---- FP64 tensor-core products: 4 k4 steps of 2 sources
+    }
+    for (int c = 0; c < nchunks; ++c)
+    {
+        const int s0 = ctx.src_begin + c * kChunk;
+        // copies of chunk c + 2 into the raw buffer chunk c used (this
+        // warp transformed its own elements of it already)
+        if (c + 2 < nchunks)
+            dmma_issue(sm, c & 1, prm, ctx, s0 + 2 * kChunk);
+        // ---- products of chunk c: 4 k4 steps of 2 sources
+        const double* fbase = sm.frag[c & 1];
 #pragma unroll
         for (int k4 = 0; k4 < kChunk / 2; ++k4)
         {
-            const double* fa = fragment_base(sm) + k4 * kFragK4;
+            const double* fa = fbase + k4 * kFragK4;
             const double* fb = fa + kFragBlock;
             double a[4], b[8];
 #pragma unroll
@@ -890,6 +951,14 @@ xcorr_dmma_kernel(const XcorrParams<double> prm)
                     dmma_m8n8k4(acc[ms][ns][0], acc[ms][ns][1], a[ms],
                             b[ns]);
         }
+        // ---- transform of chunk c + 1 while the products run
+        if (c + 1 < nchunks)
+        {
+            if (c + 2 < nchunks) cp_async_wait_group<1>();
+            else cp_async_wait_group<0>();
+            dmma_transform<CASA>(sm, (c + 1) & 1, (c + 1) & 1);
+        }
+        __syncthreads();
     }
 
     // ---- visibilities: thread pairs (rows c = 0, 1: lanes l, l ^ 4) form
@@ -996,17 +1065,17 @@ void launch_variant(bool casa, bool gauss, bool bw, bool ts,
 #undef OSKB_L
 }
 
-// The FP64 tensor-core kernel can serve FP64 matrix point sources without
-// smearing when OSKB_XCORR_DMMA=1. It is off by default: with 8-source
-// chunks the shared staging, not the FP64 tensor pipe, bounds both forms,
-// and they run at the same speed (261 and 258 G source-baselines/s at 512
-// stations x 100,000 sources).
+// FP64 matrix point sources without smearing run on the FP64 tensor pipe
+// (xcorr_dmma_kernel) by default: with the transform of the next chunk
+// overlapping the current chunk's products it measured 8 % faster than the
+// SIMT kernel (256 against 236 G source-baselines/s at 512 stations x 8,000
+// sources on one B200). OSKB_XCORR_DMMA=0 selects the SIMT kernel.
 template <typename T, bool MATRIX>
 bool use_dmma(bool gauss, bool bw, bool ts)
 {
     if (sizeof(T) != 8 || !MATRIX || gauss || bw || ts) return false;
     const char* e = getenv("OSKB_XCORR_DMMA");
-    return e && e[0] == '1';
+    return !(e && e[0] == '0');
 }
 
 template <typename T>
@@ -1015,7 +1084,7 @@ void launch_dmma(bool casa, const XcorrParams<T>& p, int grid,
 {
     if constexpr (sizeof(T) == 8)
     {
-        const size_t smem = sizeof(Smem<double, true>);
+        const size_t smem = sizeof(DmmaSmem);
         if (casa)
         {
             auto k = xcorr_dmma_kernel<true>;

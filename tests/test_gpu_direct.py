@@ -129,9 +129,9 @@ def test_xcorr_slices_deterministic():
 @pytest.mark.parametrize("slices", ["1", "4"])
 def test_xcorr_fp64_tensor_core_vs_simt(casa, slices, monkeypatch):
     """FP64 point sources without smearing on the FP64 tensor pipe
-    (mma.sync f64, opt-in with OSKB_XCORR_DMMA=1) agree with the SIMT
-    kernel and the oracle to 1e-13, with the uv filter, an output offset
-    and slices."""
+    (mma.sync f64, the default; OSKB_XCORR_DMMA=0 selects SIMT) agree with
+    the SIMT kernel and the oracle to 1e-13, with the uv filter, an output
+    offset and slices."""
     monkeypatch.setenv("OSKB_XCORR_SLICES", slices)
     c = XcorrCase(75, 1003, casa=casa, uv_min=0.5, uv_max=1.2,
                   offset_out=7, seed=5)
@@ -144,6 +144,18 @@ def test_xcorr_fp64_tensor_core_vs_simt(casa, slices, monkeypatch):
     assert_close(tc, simt, np.float64, 1e-13)
     changed = np.any((tc != c.vis0).reshape(-1, 8), axis=1)
     assert changed.any() and not changed.all()
+
+
+@pytest.mark.parametrize("nsrc", [1, 5, 8, 13, 16, 17, 40])
+def test_xcorr_fp64_tensor_core_chunk_counts(nsrc, monkeypatch):
+    """The FP64 tensor-core pipeline (two chunks staged ahead, one
+    transformed while the other's products run) for one, two, three and
+    more chunks per item, full and partial."""
+    monkeypatch.setenv("OSKB_XCORR_SLICES", "1")
+    c = XcorrCase(41, nsrc, seed=nsrc)
+    ref = run_oracle_xcorr(c, np.float64)
+    monkeypatch.setenv("OSKB_XCORR_DMMA", "1")
+    assert_close(run_gpu_xcorr(c, np.float64), ref, np.float64, 1e-13)
 
 
 def test_xcorr_empty_inputs():
