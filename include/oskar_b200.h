@@ -717,6 +717,20 @@ OSKB_API int oskb_correlate_block_tc(int use_casa_phase_convention,
         const double* station_uvw, const double* inv_wavelength,
         double uv_min_lambda, double uv_max_lambda, double* vis,
         void* workspace, size_t workspace_bytes, void* stream);
+/* The same, with the auto-correlations of every station from the same
+ * contraction: the diagonal station pairs of the diagonal tiles are
+ * V_pp = J_p B J_p^H, added into autos [num_times][num_channels]
+ * [num_stations][2x2] FP64 (the reference's oskar_auto_correlate per
+ * (dump, channel), oskar/correlate/define_auto_correlate.h:8-82, fused into
+ * the correlation at no extra tensor work). */
+OSKB_API int oskb_correlate_block_tc_auto(int use_casa_phase_convention,
+        int num_sources, int num_stations, int num_times, int num_channels,
+        const float* E, const double* l, const double* m, const double* n,
+        const double* I, const double* Q, const double* U, const double* V,
+        const double* station_uvw, const double* inv_wavelength,
+        double uv_min_lambda, double uv_max_lambda, double* vis,
+        double* autos, void* workspace, size_t workspace_bytes,
+        void* stream);
 
 /* Host-buffer block driver: the same computation as
  * oskb_correlate_block_tc with every array in HOST memory (page-locked for

@@ -360,6 +360,10 @@ struct GemmParams
     double uv_min, uv_max;
     int casa;
     int* err;
+    // Auto-correlations (optional): the diagonal station pairs of the
+    // diagonal tiles, V_pp = J_p B J_p^H, added into
+    // autos[(g * num_st + p) * 8 + 2 x 2] for global problem g; NULL: none.
+    double* autos;
 };
 
 struct GemmCtl
@@ -624,6 +628,20 @@ gemm_kernel(const GemmParams prm)
                                                   : prm.kw_scalar;
             double* vbase = prm.vis + 8 * ((size_t) g * prm.vis_stride +
                     (size_t) prm.offset_out);
+            if (prm.autos && rb == cb && p < N)
+            {
+                // column station q = p of this thread's 16: V_pp[i][c]
+                const int ql = p - cb * kStPerBlock - 16 * h;
+#pragma unroll
+                for (int k = 0; k < 16; ++k)
+                    if (k == ql)
+                    {
+                        double* o = prm.autos + 8 * ((size_t) g * N + p) +
+                                2 * (2 * i + c);
+                        o[0] += accR[k] * inv_s2;
+                        o[1] += accI[k] * inv_s2;
+                    }
+            }
 #pragma unroll
             for (int ql = 0; ql < 16; ++ql)
             {
@@ -1021,6 +1039,20 @@ gemm_wide_kernel(const GemmParams prm)
                                                   : prm.kw_scalar;
             double* vbase = prm.vis + 8 * ((size_t) g * prm.vis_stride +
                     (size_t) prm.offset_out);
+            if (prm.autos && p < N)
+            {
+                // the column station q = p, where this thread's 32 hold it
+                const int ql = p - 2 * cp * kStPerBlock - 32 * h;
+#pragma unroll
+                for (int k = 0; k < 32; ++k)
+                    if (k == ql)
+                    {
+                        double* o = prm.autos + 8 * ((size_t) g * N + p) +
+                                2 * (2 * i + c);
+                        o[0] += accR[k] * inv_s2;
+                        o[1] += accI[k] * inv_s2;
+                    }
+            }
 #pragma unroll
             for (int ql = 0; ql < 32; ++ql)
             {
@@ -1275,7 +1307,7 @@ int oskb_cross_correlate_tc_d(int casa, int num_sources, int num_stations,
     gp.st_u = station_u; gp.st_v = station_v; gp.uv_stride = 0;
     gp.inv_wavelength = nullptr; gp.kw_scalar = inv_wavelength;
     gp.uv_min = uv_min_lambda; gp.uv_max = uv_max_lambda;
-    gp.casa = casa; gp.err = &hdr->err;
+    gp.casa = casa; gp.err = &hdr->err; gp.autos = nullptr;
     return launch_gemm(gp, s);
 }
 
@@ -1299,7 +1331,21 @@ int oskb_correlate_block_tc(int casa, int num_sources, int num_stations,
     return oskb::tc::correlate_block(casa, num_sources, num_stations,
             num_times, num_channels, E, l, m, n, I, Q, U, V, station_uvw,
             inv_wavelength, uv_min_lambda, uv_max_lambda, vis, workspace,
-            workspace_bytes, stream, nullptr, nullptr);
+            workspace_bytes, stream, nullptr, nullptr, nullptr);
+}
+
+int oskb_correlate_block_tc_auto(int casa, int num_sources,
+        int num_stations, int num_times, int num_channels, const float* E,
+        const double* l, const double* m, const double* n, const double* I,
+        const double* Q, const double* U, const double* V,
+        const double* station_uvw, const double* inv_wavelength,
+        double uv_min_lambda, double uv_max_lambda, double* vis,
+        double* autos, void* workspace, size_t workspace_bytes, void* stream)
+{
+    return oskb::tc::correlate_block(casa, num_sources, num_stations,
+            num_times, num_channels, E, l, m, n, I, Q, U, V, station_uvw,
+            inv_wavelength, uv_min_lambda, uv_max_lambda, vis, workspace,
+            workspace_bytes, stream, nullptr, nullptr, autos);
 }
 
 }  // extern "C"
@@ -1314,7 +1360,8 @@ int correlate_block(int casa, int num_sources, int num_stations,
         const double* inv_wavelength, double uv_min_lambda,
         double uv_max_lambda, double* vis, void* workspace,
         size_t workspace_bytes, void* stream,
-        void (*after_group)(void* ctx, int p0, int np), void* ctx)
+        void (*after_group)(void* ctx, int p0, int np), void* ctx,
+        double* autos)
 {
     if (num_sources < 0 || num_stations < 0 || num_times < 0 ||
             num_channels < 0)
@@ -1378,7 +1425,7 @@ int correlate_block(int casa, int num_sources, int num_stations,
         gp.uv_stride = 3 * (size_t) num_stations;
         gp.inv_wavelength = inv_wavelength; gp.kw_scalar = 0.0;
         gp.uv_min = uv_min_lambda; gp.uv_max = uv_max_lambda;
-        gp.casa = casa; gp.err = &hdr->err;
+        gp.casa = casa; gp.err = &hdr->err; gp.autos = autos;
         if ((err = launch_gemm(gp, s))) return err;
         if (after_group) after_group(ctx, p0, np);
     }
@@ -1548,6 +1595,6 @@ extern "C" int oskb_cross_correlate_tc_noalloc_d(int casa, int num_sources,
     gp.st_u = station_u; gp.st_v = station_v; gp.uv_stride = 0;
     gp.inv_wavelength = nullptr; gp.kw_scalar = inv_wavelength;
     gp.uv_min = uv_min_lambda; gp.uv_max = uv_max_lambda;
-    gp.casa = casa; gp.err = &hdr->err;
+    gp.casa = casa; gp.err = &hdr->err; gp.autos = nullptr;
     return launch_gemm(gp, s);
 }

@@ -9,7 +9,9 @@ namespace tc {
 // oskb_correlate_block_tc with a hook: after_group (if set) is called on the
 // host once the contraction of problems [p0, p0 + np) has been enqueued on
 // the stream, so the caller can enqueue work that depends on those
-// visibilities (for example their download) while later groups compute.
+// visibilities (for example their download) while later groups compute;
+// autos (if set) receives the auto-correlations from the same contraction
+// ([time][channel][station][2x2], added).
 int correlate_block(int casa, int num_sources, int num_stations,
         int num_times, int num_channels, const float* E, const double* l,
         const double* m, const double* n, const double* I, const double* Q,
@@ -17,7 +19,8 @@ int correlate_block(int casa, int num_sources, int num_stations,
         const double* inv_wavelength, double uv_min_lambda,
         double uv_max_lambda, double* vis, void* workspace,
         size_t workspace_bytes, void* stream,
-        void (*after_group)(void* ctx, int p0, int np), void* ctx);
+        void (*after_group)(void* ctx, int p0, int np), void* ctx,
+        double* autos = nullptr);
 
 }  // namespace tc
 }  // namespace oskb

@@ -252,3 +252,52 @@ def test_tc_block_small_workspace_groups():
         torch.cuda.synchronize()
         out.append(vis.cpu().numpy())
     assert np.array_equal(out[0], out[1])
+
+
+@pytest.mark.parametrize("tile", [128, 256])
+def test_tc_block_auto_correlations_fused(tile, monkeypatch):
+    """Auto-correlations from the same contraction (the diagonal station
+    pairs of the diagonal tiles) against the oracle's auto-correlation of
+    J = K E per (dump, channel), to the compensated tolerance; the cross
+    visibilities are the same bits as without them."""
+    monkeypatch.setenv("OSKB_TC_TILE", str(tile))
+    rng = np.random.default_rng(21)
+    nst, nsrc, ntime, nchan = 97, 700, 2, 2
+    l, m, n, I, Q, U, V = sky(rng, nsrc)
+    E = rng.normal(0, 0.1, (nst, nsrc, 8))
+    E[..., 0] += 1
+    E[..., 6] += 1
+    E32 = E.astype(np.float32)
+    uvw = np.stack([np.stack(stations(rng, nst, rmax=20e3))
+                    for _ in range(ntime)])
+    inv_wl = (100e6 + 7e6 * np.arange(nchan)) / C0
+    nbl = nst * (nst - 1) // 2
+    args = [dev(E32), dev(l), dev(m), dev(n), dev(I), dev(Q), dev(U), dev(V),
+            dev(uvw), dev(inv_wl), 0.0, 3e38]
+    vis = torch.zeros(ntime * nchan * nbl * 8, dtype=torch.float64,
+                      device="cuda")
+    autos = torch.zeros(ntime * nchan * nst * 8, dtype=torch.float64,
+                        device="cuda")
+    ob.call("oskb_correlate_block_tc_auto", 0, nsrc, nst, ntime, nchan,
+            *args, vis, autos, None, 0, ob.stream_ptr())
+    vis0 = torch.zeros_like(vis)
+    ob.call("oskb_correlate_block_tc", 0, nsrc, nst, ntime, nchan, *args,
+            vis0, None, 0, ob.stream_ptr())
+    torch.cuda.synchronize()
+    assert ob.load().oskb_tc_tile_columns() == tile
+    assert torch.equal(vis, vis0)
+    got = autos.cpu().numpy().reshape(ntime, nchan, -1)
+    Ed = E32.astype(np.float64).ravel()
+    for t in range(ntime):
+        u, v, w = uvw[t]
+        for c in range(nchan):
+            K = np.zeros(2 * nst * nsrc)
+            oracle().call("jones_k_d", np.float64, nsrc, l, m, n, nst, u, v,
+                          w, 2 * np.pi * inv_wl[c], I, 0.0, 1e300, 0, K)
+            J = np.zeros(8 * nst * nsrc)
+            oracle().call("mem_mul_cm_m_d", np.float64, nst * nsrc, K, Ed, J)
+            ref = np.zeros(8 * nst)
+            oracle().call("acorr_matrix_d", np.float64, nsrc, nst, 0, J, I,
+                          Q, U, V, ref)
+            l2, mx = errors(got[t, c], ref)
+            assert l2 <= TOL and mx <= TOL, (t, c, l2, mx)
