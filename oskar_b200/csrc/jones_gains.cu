@@ -74,27 +74,29 @@ __global__ void __launch_bounds__(kThreads) cable_kernel(int num_sources,
                 s += gridDim.x * blockDim.x)
         {
             T* e = row + (size_t) (MATRIX ? 8 : 2) * s;
-            if (!MATRIX)
+            if constexpr (!MATRIX)
             {
                 const C2<T> r = cx_mul(gx, C2<T>{e[0], e[1]});
                 e[0] = r.re;
                 e[1] = r.im;
-                continue;
             }
-            T v[8];
-#pragma unroll
-            for (int k = 0; k < 8; ++k) v[k] = e[k];
-#pragma unroll
-            for (int k = 0; k < 4; ++k)
+            else
             {
-                // rows a, b take the x gain; rows c, d the y gain
-                const C2<T> r = cx_mul(k < 2 ? gx : gy,
-                        C2<T>{v[2 * k], v[2 * k + 1]});
-                v[2 * k] = r.re;
-                v[2 * k + 1] = r.im;
-            }
+                T v[8];
 #pragma unroll
-            for (int k = 0; k < 8; ++k) e[k] = v[k];
+                for (int k = 0; k < 8; ++k) v[k] = e[k];
+#pragma unroll
+                for (int k = 0; k < 4; ++k)
+                {
+                    // rows a, b take the x gain; rows c, d the y gain
+                    const C2<T> r = cx_mul(k < 2 ? gx : gy,
+                            C2<T>{v[2 * k], v[2 * k + 1]});
+                    v[2 * k] = r.re;
+                    v[2 * k + 1] = r.im;
+                }
+#pragma unroll
+                for (int k = 0; k < 8; ++k) e[k] = v[k];
+            }
         }
     }
 }
@@ -114,33 +116,35 @@ __global__ void __launch_bounds__(kThreads) gains_kernel(int num_sources,
                 s += gridDim.x * blockDim.x)
         {
             T* e = row + (size_t) W * s;
-            if (!MATRIX)
+            if constexpr (!MATRIX)
             {
                 const C2<T> r = cx_mul(C2<T>{g[0], g[1]}, C2<T>{e[0], e[1]});
                 e[0] = r.re;
                 e[1] = r.im;
-                continue;
             }
-            T v[8];
-#pragma unroll
-            for (int k = 0; k < 8; ++k) v[k] = e[k];
-            const C2<T> ga{g[0], g[1]}, gb{g[2], g[3]}, gc{g[4], g[5]},
-                    gd{g[6], g[7]}, ja{v[0], v[1]}, jb{v[2], v[3]},
-                    jc{v[4], v[5]}, jd{v[6], v[7]};
-            C2<T> o[4];
-            C2<T> t0 = cx_mul(ga, ja), t1 = cx_mul(gb, jc);
-            o[0] = C2<T>{t0.re + t1.re, t0.im + t1.im};
-            t0 = cx_mul(ga, jb); t1 = cx_mul(gb, jd);
-            o[1] = C2<T>{t0.re + t1.re, t0.im + t1.im};
-            t0 = cx_mul(gc, ja); t1 = cx_mul(gd, jc);
-            o[2] = C2<T>{t0.re + t1.re, t0.im + t1.im};
-            t0 = cx_mul(gc, jb); t1 = cx_mul(gd, jd);
-            o[3] = C2<T>{t0.re + t1.re, t0.im + t1.im};
-#pragma unroll
-            for (int k = 0; k < 4; ++k)
+            else
             {
-                e[2 * k] = o[k].re;
-                e[2 * k + 1] = o[k].im;
+                T v[8];
+#pragma unroll
+                for (int k = 0; k < 8; ++k) v[k] = e[k];
+                const C2<T> ga{g[0], g[1]}, gb{g[2], g[3]}, gc{g[4], g[5]},
+                        gd{g[6], g[7]}, ja{v[0], v[1]}, jb{v[2], v[3]},
+                        jc{v[4], v[5]}, jd{v[6], v[7]};
+                C2<T> o[4];
+                C2<T> t0 = cx_mul(ga, ja), t1 = cx_mul(gb, jc);
+                o[0] = C2<T>{t0.re + t1.re, t0.im + t1.im};
+                t0 = cx_mul(ga, jb); t1 = cx_mul(gb, jd);
+                o[1] = C2<T>{t0.re + t1.re, t0.im + t1.im};
+                t0 = cx_mul(gc, ja); t1 = cx_mul(gd, jc);
+                o[2] = C2<T>{t0.re + t1.re, t0.im + t1.im};
+                t0 = cx_mul(gc, jb); t1 = cx_mul(gd, jd);
+                o[3] = C2<T>{t0.re + t1.re, t0.im + t1.im};
+#pragma unroll
+                for (int k = 0; k < 4; ++k)
+                {
+                    e[2 * k] = o[k].re;
+                    e[2 * k + 1] = o[k].im;
+                }
             }
         }
     }

@@ -146,9 +146,9 @@ __global__ void bias_grad_kernel(int batch, int out,
 }
 
 // Mean squared error over n values: dy = 2 (y - t) / n; loss += sum / n.
-__global__ void mse_kernel(long long n, const float* __restrict__ y,
-        const float* __restrict__ t, float* __restrict__ dy,
-        float* __restrict__ loss)
+// y and dy may be the same array (the gradient overwrites the outputs).
+__global__ void mse_kernel(long long n, const float* y,
+        const float* __restrict__ t, float* dy, float* __restrict__ loss)
 {
     const long long i = blockIdx.x * (long long) blockDim.x + threadIdx.x;
     float e = 0.f;
