@@ -136,3 +136,106 @@ def test_speed_against_reference_cuda(real, gaussian, bw, ts):
         old = json.load(open(path)) if os.path.exists(path) else []
         old.append(rec)
         json.dump(old, open(path, "w"), indent=1)
+
+
+# ---- station-beam DFT against the reference's GPU weighted-DFT kernels
+# (math/define_dftw_m2m.h, define_dftw_c2c.h; oracle/ref_cuda_shim.cu)
+
+def _dft_case(real, num_in, num_out, seed, matrix, is_3d, n_types=None):
+    rng = np.random.default_rng(seed)
+    c = {}
+    c["w"] = rng.normal(size=2 * num_in).astype(real)
+    c["xi"], c["yi"] = (rng.uniform(-20, 20, num_in).astype(real)
+                        for _ in range(2))
+    c["zi"] = rng.uniform(-1, 1, num_in).astype(real)
+    az = rng.uniform(0, 2 * np.pi, num_out)
+    el = rng.uniform(0, np.pi / 2, num_out)
+    c["xo"] = (np.cos(el) * np.sin(az)).astype(real)
+    c["yo"] = (np.cos(el) * np.cos(az)).astype(real)
+    c["zo"] = np.sin(el).astype(real)
+    nd = n_types if n_types else num_in
+    c["idx"] = (rng.integers(0, n_types, num_in).astype(np.int32)
+                if n_types else None)
+    c["data"] = rng.normal(size=nd * num_out * (8 if matrix else 2)).astype(
+        real)
+    c["k"] = real(2 * np.pi * 150e6 / 299792458.0)
+    return c
+
+
+def _dft_run(c, real, matrix, is_3d, num_in, num_out, ev, ref, reps=0):
+    d = {k: (dev(v) if v is not None else None) for k, v in c.items()
+         if k != "k"}
+    out = torch.zeros(num_out * (8 if matrix else 2), dtype=d["w"].dtype,
+                      device="cuda")
+    norm = real(1.0 / num_in)
+    zi = d["zi"] if is_3d else None
+    zo = d["zo"] if is_3d else None
+    if ref:
+        lib = reference_cuda()
+        fn = getattr(lib, "ref_cuda_dftw_" + ("double" if real == np.float64
+                                              else "float"))
+        fp = ctypes.c_double if real == np.float64 else ctypes.c_float
+        P = lambda t: ctypes.c_void_p(t.data_ptr() if t is not None else 0)
+        call = lambda: fn(ctypes.c_int(int(matrix)), ctypes.c_int(is_3d),
+                          ctypes.c_int(num_in), fp(c["k"]), P(d["w"]),
+                          P(d["xi"]), P(d["yi"]), P(zi), ctypes.c_int(0),
+                          ctypes.c_int(num_out), P(d["xo"]), P(d["yo"]),
+                          P(zo), P(d["idx"]), P(d["data"]),
+                          ctypes.c_int(ev[0]), ctypes.c_int(ev[1]),
+                          ctypes.c_int(0), P(out), fp(norm), None)
+    else:
+        call = lambda: ob.call("oskb_dftw_" + suffix(real), int(matrix),
+                               num_in, float(c["k"]), d["w"], d["xi"],
+                               d["yi"], zi, 0, num_out, d["xo"], d["yo"],
+                               zo, d["idx"], d["data"], ev[0], ev[1], 0, out,
+                               float(norm), 0)
+    if reps:
+        return out, _time(call, reps)
+    call()
+    torch.cuda.synchronize()
+    return out.cpu().numpy(), None
+
+
+import ctypes  # noqa: E402
+
+
+@pytest.mark.parametrize("real", [np.float64, np.float32])
+@pytest.mark.parametrize("matrix,is_3d,n_types,ev", [
+    (True, 1, 1, (1, 1)), (True, 0, None, (1, 1)), (True, 1, 3, (1, 0)),
+    (True, 1, None, (0, 1)), (False, 1, None, (1, 1)), (False, 0, 2, (1, 1))])
+def test_dftw_parity_with_reference_cuda(real, matrix, is_3d, n_types, ev):
+    num_in, num_out = 300, 1031
+    c = _dft_case(real, num_in, num_out, 3, matrix, is_3d, n_types)
+    ours, _ = _dft_run(c, real, matrix, is_3d, num_in, num_out, ev, False)
+    ref, _ = _dft_run(c, real, matrix, is_3d, num_in, num_out, ev, True)
+    assert _rel(ours, ref) <= (1e-12 if real == np.float64 else 2e-5)
+
+
+@pytest.mark.parametrize("real", [np.float64, np.float32])
+def test_dftw_speed_against_reference_cuda(real):
+    """One station of the aperture-array configuration (256 dipoles, one
+    element type, 12,001 directions, 3-D, 2x2 data), as oskar_dftw runs it
+    per station; speeds recorded, not asserted."""
+    num_in, num_out = 256, 12001
+    c = _dft_case(real, num_in, num_out, 8, True, 1, 1)
+    o1, ms_ours = _dft_run(c, real, True, 1, num_in, num_out, (1, 1), False,
+                           reps=5)
+    o2, ms_ref = _dft_run(c, real, True, 1, num_in, num_out, (1, 1), True,
+                          reps=5)
+    assert _rel(o1.cpu().numpy(), o2.cpu().numpy()) <= (
+        1e-12 if real == np.float64 else 2e-5)
+    work = num_in * num_out
+    rec = {"case": "weighted DFT m2m 3-D, 256 elements x 12001 directions, "
+                   "%s" % ("FP64" if real == np.float64 else "FP32"),
+           "ours_ms": ms_ours, "reference_cuda_ms": ms_ref,
+           "ours_g_element_directions_per_s": work / (ms_ours * 1e-3) / 1e9,
+           "reference_cuda_g_element_directions_per_s":
+               work / (ms_ref * 1e-3) / 1e9,
+           "speedup": ms_ref / ms_ours}
+    print(json.dumps(rec))
+    out = os.environ.get("OSKB_REPORT_DIR")
+    if out:
+        path = os.path.join(out, "ref_cuda_timing.json")
+        old = json.load(open(path)) if os.path.exists(path) else []
+        old.append(rec)
+        json.dump(old, open(path, "w"), indent=1)
