@@ -7,13 +7,29 @@
 // (2-3 FMA), one sincos, one complex weight multiply and 1 (c2c) or 4 (m2m)
 // complex multiply-adds; the direction's data rows are read through L1 since
 // all threads of a warp read consecutive directions.
+//
+// A station beam has a few thousand to a few tens of thousands of
+// directions, which at one thread per direction leaves most of the 148 SMs
+// idle. When the direction grid is small the elements are split into
+// `slices` contiguous ranges, one per CTA of a thread-block cluster
+// (gridDim.y == cluster height); each CTA sums its range and CTA 0 of the
+// cluster adds the partial sums from the others' shared memory in rank
+// order, so the result does not depend on scheduling. The accumulators are
+// fully unrolled with the eval_x/eval_y selection as a predicate so they
+// stay in registers.
 #include "common.cuh"
+
+#include <cooperative_groups.h>
 
 namespace oskb {
 namespace {
 
+namespace cg = cooperative_groups;
+
 constexpr int kChunk = 512;
 constexpr int kThreads = 128;
+constexpr int kMaxSlices = 8;      // portable cluster size
+constexpr int kMinSliceElements = 16;
 
 template <typename T, bool MATRIX, bool IS3D>
 __global__ void __launch_bounds__(kThreads)
@@ -26,6 +42,7 @@ dftw_kernel(int num_in, T wavenumber, const T* __restrict__ weights_in,
         T* __restrict__ output, T norm_factor)
 {
     typedef typename vec2<T>::type T2;
+    constexpr int NC = MATRIX ? 4 : 1;
     __shared__ T2 s_w[kChunk];
     __shared__ T s_x[kChunk], s_y[kChunk], s_z[IS3D ? kChunk : 1];
     __shared__ int s_idx[kChunk];
@@ -38,7 +55,6 @@ dftw_kernel(int num_in, T wavenumber, const T* __restrict__ weights_in,
         yo = wavenumber * y_out[d + offset_coord_out];
         if (IS3D) zo = wavenumber * z_out[d + offset_coord_out];
     }
-    constexpr int NC = MATRIX ? 4 : 1;
     T2 acc[NC];
 #pragma unroll
     for (int k = 0; k < NC; ++k) acc[k].x = acc[k].y = (T) 0;
@@ -46,9 +62,14 @@ dftw_kernel(int num_in, T wavenumber, const T* __restrict__ weights_in,
     const int k1 = MATRIX ? (eval_y ? 4 : 2) : 1;
     const T2* data2 = reinterpret_cast<const T2*>(data);
 
-    for (int e0 = 0; e0 < num_in; e0 += kChunk)
+    // this CTA's element range
+    const int slices = gridDim.y;
+    const int per = (num_in + slices - 1) / slices;
+    const int lo = min(num_in, (int) blockIdx.y * per);
+    const int hi = min(num_in, lo + per);
+    for (int e0 = lo; e0 < hi; e0 += kChunk)
     {
-        const int ne = min(kChunk, num_in - e0);
+        const int ne = min(kChunk, hi - e0);
         for (int t = threadIdx.x; t < ne; t += kThreads)
         {
             const int g = e0 + t;
@@ -71,38 +92,111 @@ dftw_kernel(int num_in, T wavenumber, const T* __restrict__ weights_in,
                 const T re = cs * w.x - w.y * sn;
                 const T im = sn * w.x + w.y * cs;
                 const size_t base = (size_t) s_idx[i] * num_out + d;
-                if (MATRIX)
+#pragma unroll
+                for (int k = 0; k < NC; ++k)
                 {
-                    for (int k = k0; k < k1; ++k)
-                    {
-                        const T2 v = __ldg(&data2[4 * base + k]);
-                        acc[k].x += v.x * re - v.y * im;
-                        acc[k].y += v.y * re + v.x * im;
-                    }
-                }
-                else
-                {
-                    const T2 v = __ldg(&data2[base]);
-                    acc[0].x += v.x * re - v.y * im;
-                    acc[0].y += v.y * re + v.x * im;
+                    if (k < k0 || k >= k1) continue;
+                    const T2 v = __ldg(&data2[(size_t) NC * base + k]);
+                    acc[k].x += v.x * re - v.y * im;
+                    acc[k].y += v.y * re + v.x * im;
                 }
             }
         }
         __syncthreads();
     }
+    if (slices > 1)
+    {
+        // partial sums of the cluster's CTAs, added in rank order by rank 0
+        __shared__ T2 s_part[NC][kThreads];
+#pragma unroll
+        for (int k = 0; k < NC; ++k) s_part[k][threadIdx.x] = acc[k];
+        cg::cluster_group cluster = cg::this_cluster();
+        cluster.sync();
+        if (blockIdx.y == 0)
+        {
+            for (int r = 1; r < slices; ++r)
+            {
+                const T2* p = cluster.map_shared_rank(&s_part[0][0], r);
+#pragma unroll
+                for (int k = 0; k < NC; ++k)
+                {
+                    const T2 v = p[k * kThreads + threadIdx.x];
+                    acc[k].x += v.x;
+                    acc[k].y += v.y;
+                }
+            }
+        }
+        // keep every CTA's shared memory alive until rank 0 has read it
+        cluster.sync();
+        if (blockIdx.y != 0) return;
+    }
     if (!active) return;
     T2* out2 = reinterpret_cast<T2*>(output);
-    if (MATRIX)
+#pragma unroll
+    for (int k = 0; k < NC; ++k)
     {
-        for (int k = k0; k < k1; ++k)
-            out2[4 * ((size_t) d + offset_out) + k] =
-                    T2{acc[k].x * norm_factor, acc[k].y * norm_factor};
+        if (k < k0 || k >= k1) continue;
+        out2[(size_t) NC * ((size_t) d + offset_out) + k] =
+                T2{acc[k].x * norm_factor, acc[k].y * norm_factor};
     }
-    else
+}
+
+int num_sms()
+{
+    static int n = 0;
+    if (!n)
     {
-        out2[(size_t) d + offset_out] =
-                T2{acc[0].x * norm_factor, acc[0].y * norm_factor};
+        int dev = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev);
+        if (n <= 0) n = 148;
     }
+    return n;
+}
+
+// Number of element slices: grow the cluster while the direction grid is
+// below about 8 CTAs (32 warps) per SM and each slice keeps at least
+// kMinSliceElements elements.
+int choose_slices(int num_in, int blocks_x)
+{
+    const long long target = 8LL * num_sms();
+    int s = 1;
+    while (s < kMaxSlices && (long long) blocks_x * s < target &&
+            num_in / (2 * s) >= kMinSliceElements)
+        s *= 2;
+    return s;
+}
+
+template <typename T, bool MATRIX, bool IS3D>
+int launch_dftw(int slices, int blocks_x, cudaStream_t s, int num_in,
+        T wavenumber, const T* weights_in, const T* x_in, const T* y_in,
+        const T* z_in, int offset_coord_out, int num_out, const T* x_out,
+        const T* y_out, const T* z_out, const int* data_idx, const T* data,
+        int eval_x, int eval_y, int offset_out, T* output, T norm_factor)
+{
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(blocks_x, slices, 1);
+    cfg.blockDim = dim3(kThreads, 1, 1);
+    cfg.dynamicSmemBytes = 0;
+    cfg.stream = s;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = 1;
+    attr[0].val.clusterDim.y = slices;
+    attr[0].val.clusterDim.z = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = slices > 1 ? 1 : 0;
+    cudaError_t e = cudaLaunchKernelEx(&cfg, dftw_kernel<T, MATRIX, IS3D>,
+            num_in, wavenumber, weights_in, x_in, y_in, z_in,
+            offset_coord_out, num_out, x_out, y_out, z_out, data_idx, data,
+            eval_x, eval_y, offset_out, output, norm_factor);
+    if (e != cudaSuccess)
+    {
+        cudaGetLastError();
+        set_last_error("dftw", e);
+        return OSKB_ERR_KERNEL_LAUNCH_FAILURE;
+    }
+    return check_launch("dftw");
 }
 
 template <typename T>
@@ -118,16 +212,16 @@ int dftw(int matrix, int num_in, T wavenumber, const T* weights_in,
             !output)
         return OSKB_ERR_INVALID_ARGUMENT;
     const bool is3d = (z_in != nullptr && z_out != nullptr);
-    const int grid = (num_out + kThreads - 1) / kThreads;
+    const int blocks_x = (num_out + kThreads - 1) / kThreads;
+    const int slices = choose_slices(num_in, blocks_x);
     cudaStream_t s = as_stream(stream);
-#define OSKB_DFTW(M, D) dftw_kernel<T, M, D><<<grid, kThreads, 0, s>>>(       \
+#define OSKB_DFTW(M, D) return launch_dftw<T, M, D>(slices, blocks_x, s,      \
         num_in, wavenumber, weights_in, x_in, y_in, z_in, offset_coord_out,  \
         num_out, x_out, y_out, z_out, data_idx, data, eval_x, eval_y,        \
         offset_out, output, norm_factor)
     if (matrix) { if (is3d) OSKB_DFTW(true, true); else OSKB_DFTW(true, false); }
     else { if (is3d) OSKB_DFTW(false, true); else OSKB_DFTW(false, false); }
 #undef OSKB_DFTW
-    return check_launch("dftw");
 }
 
 }  // namespace
