@@ -52,6 +52,12 @@ extern "C" {
 OSKB_API const char* oskb_version(void);
 OSKB_API const char* oskb_last_error(void);
 
+/* Per-call temporaries (partial sums of source slices and the like) come
+ * from a library-owned stream-ordered pool that keeps up to 4 GiB cached
+ * across host synchronisations; this returns the cached blocks to the
+ * driver. No OSKAR counterpart. */
+OSKB_API int oskb_scratch_release(void);
+
 /* ------------------------------------------------------------------------
  * Cross-correlation, direct kernel (all source types and smearing modes).
  * ------------------------------------------------------------------------

@@ -31,6 +31,11 @@ inline int check_launch(const char* where)
 
 inline cudaStream_t as_stream(void* s) { return (cudaStream_t) s; }
 
+// Stream-ordered temporaries from the library's own memory pool, which
+// keeps freed blocks across host synchronisations (scratch.cu).
+cudaError_t scratch_alloc(void** ptr, size_t bytes, cudaStream_t stream);
+cudaError_t scratch_free(void* ptr, cudaStream_t stream);
+
 template <typename T> struct vec2;
 template <> struct vec2<float> { typedef float2 type; };
 template <> struct vec2<double> { typedef double2 type; };

@@ -270,19 +270,19 @@ int oskb_station_beam_surrogate_f(int num_stations, int num_types,
     float* queue_y = nullptr;
     unsigned char* stats = nullptr;  // max bits, count, sum_sq
     const size_t qn = (size_t) num_types * cap;
-    bool ok = cudaMallocAsync((void**) &d_type, sizeof(int) * num_stations,
+    bool ok = scratch_alloc((void**) &d_type, sizeof(int) * num_stations,
             s) == cudaSuccess &&
-            cudaMallocAsync((void**) &a.af, sizeof(float2) * total, s) ==
+            scratch_alloc((void**) &a.af, sizeof(float2) * total, s) ==
             cudaSuccess &&
-            cudaMallocAsync((void**) &a.queue_count, sizeof(int) * num_types,
+            scratch_alloc((void**) &a.queue_count, sizeof(int) * num_types,
             s) == cudaSuccess &&
-            cudaMallocAsync((void**) &a.queue_index, sizeof(int) * qn, s) ==
+            scratch_alloc((void**) &a.queue_index, sizeof(int) * qn, s) ==
             cudaSuccess &&
-            cudaMallocAsync((void**) &a.queue_x, sizeof(float) * 2 * qn, s) ==
+            scratch_alloc((void**) &a.queue_x, sizeof(float) * 2 * qn, s) ==
             cudaSuccess &&
-            cudaMallocAsync((void**) &queue_y, sizeof(float) * 2 * qn, s) ==
+            scratch_alloc((void**) &queue_y, sizeof(float) * 2 * qn, s) ==
             cudaSuccess &&
-            cudaMallocAsync((void**) &stats, 16, s) == cudaSuccess;
+            scratch_alloc((void**) &stats, 16, s) == cudaSuccess;
     int err = 0;
     if (!ok)
     {
@@ -374,10 +374,10 @@ int oskb_station_beam_surrogate_f(int num_stations, int num_types,
                     (float) cos(kL), beam);
         err = check_launch("surrogate assemble");
     }
-    cudaFreeAsync(d_type, s); cudaFreeAsync(a.af, s);
-    cudaFreeAsync(a.queue_count, s); cudaFreeAsync(a.queue_index, s);
-    cudaFreeAsync(a.queue_x, s); cudaFreeAsync(queue_y, s);
-    cudaFreeAsync(stats, s);
+    scratch_free(d_type, s); scratch_free(a.af, s);
+    scratch_free(a.queue_count, s); scratch_free(a.queue_index, s);
+    scratch_free(a.queue_x, s); scratch_free(queue_y, s);
+    scratch_free(stats, s);
     if (audit)
     {
         long long surrogate = 0;

@@ -1140,7 +1140,7 @@ int xcorr_dispatch(bool casa, bool gauss, XcorrParams<T> p,
     if (slices > 1)
     {
         const size_t bytes = (size_t) slices * nbl * ncomp2 * sizeof(double);
-        if (cudaMallocAsync((void**) &p.partial, bytes, stream) !=
+        if (scratch_alloc((void**) &p.partial, bytes, stream) !=
                 cudaSuccess)
         {
             cudaGetLastError();  // no room for partials: one slice
@@ -1165,7 +1165,7 @@ int xcorr_dispatch(bool casa, bool gauss, XcorrParams<T> p,
                     (long long) p.offset_out * ncomp2, p.vis);
             err = check_launch("xcorr_direct reduce");
         }
-        cudaFreeAsync(p.partial, stream);
+        scratch_free(p.partial, stream);
     }
     return err;
 }
@@ -1240,7 +1240,7 @@ BlockSchedule block_schedule(bool casa, bool gauss, bool bw, bool ts,
     TuneEntry ent;
     memcpy(ent.key, key, sizeof(key));
     ent.sched = dflt;
-    if (cudaMallocAsync((void**) &q.vis, vis_bytes, stream) != cudaSuccess)
+    if (scratch_alloc((void**) &q.vis, vis_bytes, stream) != cudaSuccess)
     {
         cudaGetLastError();
         return dflt;
@@ -1272,7 +1272,7 @@ BlockSchedule block_schedule(bool casa, bool gauss, bool bw, bool ts,
     }
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
-    cudaFreeAsync(q.vis, stream);
+    scratch_free(q.vis, stream);
     cudaGetLastError();
     g_tune[g_num_tune++] = ent;
     return ent.sched;
@@ -1314,7 +1314,7 @@ int block_dispatch(bool casa, bool gauss, bool bw, bool ts, XcorrParams<T> p,
             const size_t bytes = (size_t) slices * tc_items / p.tiles *
                     ((size_t) p.num_st * (p.num_st - 1) / 2) * 8 *
                     sizeof(double);
-            if (slices > 1 && cudaMallocAsync((void**) &p.partial, bytes,
+            if (slices > 1 && scratch_alloc((void**) &p.partial, bytes,
                     stream) == cudaSuccess)
             {
                 p.slices = slices;
@@ -1341,7 +1341,7 @@ int block_dispatch(bool casa, bool gauss, bool bw, bool ts, XcorrParams<T> p,
                     stream>>>(p.partial, p.slices, n, 0, p.vis);
             err = check_launch("correlate_block_direct reduce");
         }
-        cudaFreeAsync(p.partial, stream);
+        scratch_free(p.partial, stream);
     }
     return err;
 }

@@ -119,10 +119,14 @@ def test_xcorr_source_slices(slices, real, monkeypatch):
 
 
 def test_xcorr_slices_deterministic():
-    """Two runs with the default slicing give bit-identical output."""
+    """Two runs with the default slicing give bit-identical output, also
+    when the scratch pool that holds the slices' partial sums has been
+    handed back to the driver in between."""
     c = XcorrCase(100, 5000, ranges="physical", seed=9)
-    assert np.array_equal(run_gpu_xcorr(c, np.float64),
-                          run_gpu_xcorr(c, np.float64))
+    first = run_gpu_xcorr(c, np.float64)
+    assert np.array_equal(first, run_gpu_xcorr(c, np.float64))
+    assert ob.load().oskb_scratch_release() == 0
+    assert np.array_equal(first, run_gpu_xcorr(c, np.float64))
 
 
 @pytest.mark.parametrize("casa", [0, 1])
