@@ -19,7 +19,10 @@
 // Element weights and positions are staged in shared memory in chunks.
 // The normalisation direction's beam (one per station) is recomputed by each
 // CTA cooperatively before the main loop, so there is no second launch.
+// In FP64 the element loops take their phase factors from a shared-memory
+// table (trig_table.cuh) instead of a library sincos per element-direction.
 #include "beam_common.cuh"
+#include "trig_table.cuh"
 
 namespace oskb {
 namespace {
@@ -31,6 +34,18 @@ struct BeamFlags
 {
     int normalise_element, normalise_array, normalise_final, swap_xy;
 };
+
+// e^{i ph}: the shared table in FP64, sincosf in FP32.
+__device__ __forceinline__ void phase_factor(const double2* table, double ph,
+        double* s, double* c)
+{
+    trig_table_sincos(table, ph, s, c);
+}
+__device__ __forceinline__ void phase_factor(const double2*, float ph,
+        float* s, float* c)
+{
+    sincosf(ph, s, c);
+}
 
 template <typename T>
 __device__ __forceinline__ T half_frobenius(const T p[4], T ar, T ai)
@@ -59,6 +74,8 @@ station_beam_kernel(int num_elements, const T* __restrict__ el_x,
     __shared__ T2 s_w[kChunk];
     __shared__ T s_x[kChunk], s_y[kChunk], s_z[IS3D ? kChunk : 1];
     __shared__ T s_red[2][kThreads / 32];
+    // FP64: phase factors of the element loops from the shared table
+    __shared__ double2 s_trig[sizeof(T) == 8 ? kTrigTableSize : 1];
     const int st = blockIdx.y;
     const int d = blockIdx.x * kThreads + threadIdx.x;
     const bool active = d < num_dir;
@@ -73,6 +90,11 @@ station_beam_kernel(int num_elements, const T* __restrict__ el_x,
         if (active)
             for (int k = 0; k < 4; ++k) out[k] = T2{(T) 0, (T) 0};
         return;
+    }
+    if constexpr (sizeof(T) == 8)
+    {
+        trig_table_fill(s_trig);
+        __syncthreads();
     }
     const T dphi1 = (T) (kPi / 2 - (orientation_x[st] + kPi / 2));
     const T dphi2 = (T) (kPi / 2 - orientation_y[st]);
@@ -120,7 +142,7 @@ station_beam_kernel(int num_elements, const T* __restrict__ el_x,
                 T ph = knX * s_x[t] + knY * s_y[t];
                 if (IS3D) ph += knZ * s_z[t];
                 T s2, c2;
-                sincos(ph, &s2, &c2);
+                phase_factor(s_trig, ph, &s2, &c2);
                 nr += c2 * cs - sn * s2;
                 ni += s2 * cs + sn * c2;
             }
@@ -128,16 +150,53 @@ station_beam_kernel(int num_elements, const T* __restrict__ el_x,
         __syncthreads();
         if (active)
         {
-#pragma unroll 4
-            for (int i = 0; i < ne; ++i)
+            if constexpr (sizeof(T) == 8)
             {
-                T ph = kX * s_x[i] + kY * s_y[i];
-                if (IS3D) ph += kZ * s_z[i];
-                T sn, cs;
-                sincos(ph, &sn, &cs);
-                const T2 w = s_w[i];
-                ar += cs * w.x - w.y * sn;
-                ai += sn * w.x + w.y * cs;
+                // Branch-free table loop; a thread that met a phase the
+                // table does not cover redoes the chunk with sincos.
+                const T ar0 = ar, ai0 = ai;
+                bool covered = true;
+#pragma unroll 4
+                for (int i = 0; i < ne; ++i)
+                {
+                    T ph = kX * s_x[i] + kY * s_y[i];
+                    if (IS3D) ph += kZ * s_z[i];
+                    covered &= trig_table_covers(ph);
+                    T sn, cs;
+                    trig_table_sincos_unchecked(s_trig, ph, &sn, &cs);
+                    const T2 w = s_w[i];
+                    ar += cs * w.x - w.y * sn;
+                    ai += sn * w.x + w.y * cs;
+                }
+                if (!covered)
+                {
+                    ar = ar0;
+                    ai = ai0;
+                    for (int i = 0; i < ne; ++i)
+                    {
+                        T ph = kX * s_x[i] + kY * s_y[i];
+                        if (IS3D) ph += kZ * s_z[i];
+                        T sn, cs;
+                        sincos(ph, &sn, &cs);
+                        const T2 w = s_w[i];
+                        ar += cs * w.x - w.y * sn;
+                        ai += sn * w.x + w.y * cs;
+                    }
+                }
+            }
+            else
+            {
+#pragma unroll 4
+                for (int i = 0; i < ne; ++i)
+                {
+                    T ph = kX * s_x[i] + kY * s_y[i];
+                    if (IS3D) ph += kZ * s_z[i];
+                    T sn, cs;
+                    sincosf(ph, &sn, &cs);
+                    const T2 w = s_w[i];
+                    ar += cs * w.x - w.y * sn;
+                    ai += sn * w.x + w.y * cs;
+                }
             }
         }
         __syncthreads();

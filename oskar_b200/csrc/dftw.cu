@@ -16,9 +16,11 @@
 // cluster adds the partial sums from the others' shared memory in rank
 // order, so the result does not depend on scheduling. The accumulators are
 // fully unrolled with the eval_x/eval_y selection as a predicate so they
-// stay in registers.
-#include "common.cuh"
+// stay in registers. In FP64 the phase factors come from a shared-memory
+// table (trig_table.cuh) instead of a library sincos per element-direction.
+#include "trig_table.cuh"
 
+#include <algorithm>
 #include <cooperative_groups.h>
 
 namespace oskb {
@@ -26,10 +28,30 @@ namespace {
 
 namespace cg = cooperative_groups;
 
-constexpr int kChunk = 512;
+constexpr int kChunk = 256;
 constexpr int kThreads = 128;
 constexpr int kMaxSlices = 8;      // portable cluster size
 constexpr int kMinSliceElements = 16;
+
+// acc[k] += w e^{i ph} data[idx][d][k] for the evaluated k.
+template <typename T, int NC>
+__device__ __forceinline__ void accumulate(typename vec2<T>::type* acc,
+        const typename vec2<T>::type* __restrict__ data2,
+        typename vec2<T>::type w, int idx, int num_out, int d, int k0,
+        int k1, T sn, T cs)
+{
+    const T re = cs * w.x - w.y * sn;
+    const T im = sn * w.x + w.y * cs;
+    const size_t base = (size_t) idx * num_out + d;
+#pragma unroll
+    for (int k = 0; k < NC; ++k)
+    {
+        if (k < k0 || k >= k1) continue;
+        const typename vec2<T>::type v = __ldg(&data2[(size_t) NC * base + k]);
+        acc[k].x += v.x * re - v.y * im;
+        acc[k].y += v.y * re + v.x * im;
+    }
+}
 
 template <typename T, bool MATRIX, bool IS3D>
 __global__ void __launch_bounds__(kThreads)
@@ -46,6 +68,8 @@ dftw_kernel(int num_in, T wavenumber, const T* __restrict__ weights_in,
     __shared__ T2 s_w[kChunk];
     __shared__ T s_x[kChunk], s_y[kChunk], s_z[IS3D ? kChunk : 1];
     __shared__ int s_idx[kChunk];
+    __shared__ double2 s_trig[sizeof(T) == 8 ? kTrigTableSize : 1];
+    if constexpr (sizeof(T) == 8) trig_table_fill(s_trig);  // synced below
     const int d = blockIdx.x * kThreads + threadIdx.x;
     const bool active = d < num_out;
     T xo = 0, yo = 0, zo = 0;
@@ -82,23 +106,50 @@ dftw_kernel(int num_in, T wavenumber, const T* __restrict__ weights_in,
         __syncthreads();
         if (active)
         {
-            for (int i = 0; i < ne; ++i)
+            if constexpr (sizeof(T) == 8)
             {
-                T ph = xo * s_x[i] + yo * s_y[i];
-                if (IS3D) ph += zo * s_z[i];
-                T sn, cs;
-                sincos(ph, &sn, &cs);
-                const T2 w = s_w[i];
-                const T re = cs * w.x - w.y * sn;
-                const T im = sn * w.x + w.y * cs;
-                const size_t base = (size_t) s_idx[i] * num_out + d;
+                // Branch-free table loop; a thread that met a phase the
+                // table does not cover redoes the chunk with sincos.
+                T2 acc0[NC];
 #pragma unroll
-                for (int k = 0; k < NC; ++k)
+                for (int k = 0; k < NC; ++k) acc0[k] = acc[k];
+                bool covered = true;
+#pragma unroll 2
+                for (int i = 0; i < ne; ++i)
                 {
-                    if (k < k0 || k >= k1) continue;
-                    const T2 v = __ldg(&data2[(size_t) NC * base + k]);
-                    acc[k].x += v.x * re - v.y * im;
-                    acc[k].y += v.y * re + v.x * im;
+                    T ph = xo * s_x[i] + yo * s_y[i];
+                    if (IS3D) ph += zo * s_z[i];
+                    covered &= trig_table_covers(ph);
+                    T sn, cs;
+                    trig_table_sincos_unchecked(s_trig, ph, &sn, &cs);
+                    accumulate<T, NC>(acc, data2, s_w[i], s_idx[i], num_out,
+                            d, k0, k1, sn, cs);
+                }
+                if (!covered)
+                {
+#pragma unroll
+                    for (int k = 0; k < NC; ++k) acc[k] = acc0[k];
+                    for (int i = 0; i < ne; ++i)
+                    {
+                        T ph = xo * s_x[i] + yo * s_y[i];
+                        if (IS3D) ph += zo * s_z[i];
+                        T sn, cs;
+                        sincos(ph, &sn, &cs);
+                        accumulate<T, NC>(acc, data2, s_w[i], s_idx[i],
+                                num_out, d, k0, k1, sn, cs);
+                    }
+                }
+            }
+            else
+            {
+                for (int i = 0; i < ne; ++i)
+                {
+                    T ph = xo * s_x[i] + yo * s_y[i];
+                    if (IS3D) ph += zo * s_z[i];
+                    T sn, cs;
+                    sincosf(ph, &sn, &cs);
+                    accumulate<T, NC>(acc, data2, s_w[i], s_idx[i], num_out,
+                            d, k0, k1, sn, cs);
                 }
             }
         }
@@ -199,6 +250,21 @@ int launch_dftw(int slices, int blocks_x, cudaStream_t s, int num_in,
     return check_launch("dftw");
 }
 
+__global__ void __launch_bounds__(kThreads) phase_factors_kernel(int n,
+        const double* __restrict__ phase, double2* __restrict__ out)
+{
+    __shared__ double2 s_trig[kTrigTableSize];
+    trig_table_fill(s_trig);
+    __syncthreads();
+    for (int i = blockIdx.x * kThreads + threadIdx.x; i < n;
+            i += gridDim.x * kThreads)
+    {
+        double s, c;
+        trig_table_sincos(s_trig, phase[i], &s, &c);
+        out[i] = make_double2(c, s);
+    }
+}
+
 template <typename T>
 int dftw(int matrix, int num_in, T wavenumber, const T* weights_in,
         const T* x_in, const T* y_in, const T* z_in, int offset_coord_out,
@@ -253,6 +319,21 @@ int oskb_dftw_f(int matrix, int num_in, float wavenumber,
             y_in, z_in, offset_coord_out, num_out, x_out, y_out, z_out,
             data_idx, data, eval_x, eval_y, offset_out, output, norm_factor,
             stream);
+}
+
+int oskb_phase_factors_d(int n, const double* phase, double* out,
+        void* stream)
+{
+    if (n < 0) return OSKB_ERR_INVALID_ARGUMENT;
+    if (n == 0) return 0;
+    if (!phase || !out) return OSKB_ERR_INVALID_ARGUMENT;
+    const int grid = (int) std::min<long long>(
+            (n + oskb::kThreads - 1) / oskb::kThreads,
+            8LL * oskb::num_sms());
+    oskb::phase_factors_kernel<<<grid, oskb::kThreads, 0,
+            oskb::as_stream(stream)>>>(n, phase,
+            reinterpret_cast<double2*>(out));
+    return oskb::check_launch("phase_factors");
 }
 
 }  // extern "C"
