@@ -191,12 +191,13 @@ OSKB_API int oskb_dftw_f(int matrix, int num_in, float wavenumber,
         const int* data_idx, const float* data, int eval_x, int eval_y,
         int offset_out, float* output, float norm_factor, void* stream);
 
-/* out[2 i], out[2 i + 1] = cos, sin of phase[i] by the table-driven method
- * the FP64 element loops of the weighted DFT and the station beam use
- * (128-entry table, Cody-Waite reduction, Taylor series of the remainder;
- * library sincos beyond |phase| = 2^40). Device arrays. No OSKAR
- * counterpart: exposed so the method can be checked against sincos. */
-OSKB_API int oskb_phase_factors_d(int n, const double* phase, double* out,
+/* out[2 i], out[2 i + 1] = cos, sin of (pi / 64) steps[i]: a phase given
+ * in steps of 2 pi / 128, by the table-driven method the FP64 element loops
+ * of the weighted DFT and the station beam use (128-entry table, Taylor
+ * series of the remainder; sincospi(steps / 64) where the table does not
+ * reach, beyond |steps| = 2^32). Device arrays. No OSKAR counterpart:
+ * exposed so the method can be checked against exact values. */
+OSKB_API int oskb_phase_factors_d(int n, const double* steps, double* out,
         void* stream);
 
 /* Beamforming weights w_e = exp(-i wavenumber (x x1 + y y1 + z z1 + cable_e)),

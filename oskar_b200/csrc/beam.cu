@@ -35,11 +35,12 @@ struct BeamFlags
     int normalise_element, normalise_array, normalise_final, swap_xy;
 };
 
-// e^{i ph}: the shared table in FP64, sincosf in FP32.
+// e^{i ph} for the normalisation direction: ph in table steps through
+// the shared table in FP64, in radians through sincosf in FP32.
 __device__ __forceinline__ void phase_factor(const double2* table, double ph,
         double* s, double* c)
 {
-    trig_table_sincos(table, ph, s, c);
+    trig_steps_checked(table, ph, s, c);
 }
 __device__ __forceinline__ void phase_factor(const double2*, float ph,
         float* s, float* c)
@@ -113,9 +114,13 @@ station_beam_kernel(int num_elements, const T* __restrict__ el_x,
         nY = (T) norm_enu[3 * st + 1];
         nZ = (T) norm_enu[3 * st + 2];
     }
-    const T kX = wavenumber * X, kY = wavenumber * Y, kZ = wavenumber * Z;
-    const T knX = wavenumber * nX, knY = wavenumber * nY,
-            knZ = wavenumber * nZ;
+    // Phase factors per element coordinate: radians in FP32, table steps
+    // (radians x 64 / pi) in FP64.
+    const T to_steps = sizeof(T) == 8 ? (T) kTrigStepsPerRadian : (T) 1;
+    const T kX = wavenumber * X * to_steps, kY = wavenumber * Y * to_steps,
+            kZ = wavenumber * Z * to_steps;
+    const T knX = wavenumber * nX * to_steps, knY = wavenumber * nY * to_steps,
+            knZ = wavenumber * nZ * to_steps;
 
     T ar = 0, ai = 0;    // array factor, this thread's direction
     T nr = 0, ni = 0;    // array factor of the normalisation direction
@@ -161,9 +166,8 @@ station_beam_kernel(int num_elements, const T* __restrict__ el_x,
                 {
                     T ph = kX * s_x[i] + kY * s_y[i];
                     if (IS3D) ph += kZ * s_z[i];
-                    covered &= trig_table_covers(ph);
                     T sn, cs;
-                    trig_table_sincos_unchecked(s_trig, ph, &sn, &cs);
+                    trig_steps_sincos(s_trig, ph, &sn, &cs, covered);
                     const T2 w = s_w[i];
                     ar += cs * w.x - w.y * sn;
                     ai += sn * w.x + w.y * cs;
@@ -177,7 +181,7 @@ station_beam_kernel(int num_elements, const T* __restrict__ el_x,
                         T ph = kX * s_x[i] + kY * s_y[i];
                         if (IS3D) ph += kZ * s_z[i];
                         T sn, cs;
-                        sincos(ph, &sn, &cs);
+                        trig_steps_exact(ph, &sn, &cs);
                         const T2 w = s_w[i];
                         ar += cs * w.x - w.y * sn;
                         ai += sn * w.x + w.y * cs;

@@ -32,6 +32,7 @@ constexpr int kChunk = 256;
 constexpr int kThreads = 128;
 constexpr int kMaxSlices = 8;      // portable cluster size
 constexpr int kMinSliceElements = 16;
+constexpr int kTableMinElements = 64;
 
 // acc[k] += w e^{i ph} data[idx][d][k] for the evaluated k.
 template <typename T, int NC>
@@ -69,15 +70,17 @@ dftw_kernel(int num_in, T wavenumber, const T* __restrict__ weights_in,
     __shared__ T s_x[kChunk], s_y[kChunk], s_z[IS3D ? kChunk : 1];
     __shared__ int s_idx[kChunk];
     __shared__ double2 s_trig[sizeof(T) == 8 ? kTrigTableSize : 1];
-    if constexpr (sizeof(T) == 8) trig_table_fill(s_trig);  // synced below
     const int d = blockIdx.x * kThreads + threadIdx.x;
     const bool active = d < num_out;
     T xo = 0, yo = 0, zo = 0;
     if (active)
     {
-        xo = wavenumber * x_out[d + offset_coord_out];
-        yo = wavenumber * y_out[d + offset_coord_out];
-        if (IS3D) zo = wavenumber * z_out[d + offset_coord_out];
+        // radians in FP32, table steps (radians x 64 / pi) in FP64
+        const T k = sizeof(T) == 8 ? (T) (wavenumber * kTrigStepsPerRadian)
+                                   : wavenumber;
+        xo = k * x_out[d + offset_coord_out];
+        yo = k * y_out[d + offset_coord_out];
+        if (IS3D) zo = k * z_out[d + offset_coord_out];
     }
     T2 acc[NC];
 #pragma unroll
@@ -91,6 +94,9 @@ dftw_kernel(int num_in, T wavenumber, const T* __restrict__ weights_in,
     const int per = (num_in + slices - 1) / slices;
     const int lo = min(num_in, (int) blockIdx.y * per);
     const int hi = min(num_in, lo + per);
+    // The table costs 128 sincospi per CTA: worth it from about 64 elements.
+    const bool use_table = sizeof(T) == 8 && hi - lo >= kTableMinElements;
+    if (use_table) trig_table_fill(s_trig);  // synced in the chunk loop
     for (int e0 = lo; e0 < hi; e0 += kChunk)
     {
         const int ne = min(kChunk, hi - e0);
@@ -108,33 +114,40 @@ dftw_kernel(int num_in, T wavenumber, const T* __restrict__ weights_in,
         {
             if constexpr (sizeof(T) == 8)
             {
-                // Branch-free table loop; a thread that met a phase the
-                // table does not cover redoes the chunk with sincos.
-                T2 acc0[NC];
+                bool exact = !use_table;
+                if (use_table)
+                {
+                    // Branch-free table loop; a thread that met a phase
+                    // the table does not cover redoes the chunk exactly.
+                    T2 acc0[NC];
 #pragma unroll
-                for (int k = 0; k < NC; ++k) acc0[k] = acc[k];
-                bool covered = true;
+                    for (int k = 0; k < NC; ++k) acc0[k] = acc[k];
+                    bool covered = true;
 #pragma unroll 2
-                for (int i = 0; i < ne; ++i)
-                {
-                    T ph = xo * s_x[i] + yo * s_y[i];
-                    if (IS3D) ph += zo * s_z[i];
-                    covered &= trig_table_covers(ph);
-                    T sn, cs;
-                    trig_table_sincos_unchecked(s_trig, ph, &sn, &cs);
-                    accumulate<T, NC>(acc, data2, s_w[i], s_idx[i], num_out,
-                            d, k0, k1, sn, cs);
-                }
-                if (!covered)
-                {
-#pragma unroll
-                    for (int k = 0; k < NC; ++k) acc[k] = acc0[k];
                     for (int i = 0; i < ne; ++i)
                     {
                         T ph = xo * s_x[i] + yo * s_y[i];
                         if (IS3D) ph += zo * s_z[i];
                         T sn, cs;
-                        sincos(ph, &sn, &cs);
+                        trig_steps_sincos(s_trig, ph, &sn, &cs, covered);
+                        accumulate<T, NC>(acc, data2, s_w[i], s_idx[i],
+                                num_out, d, k0, k1, sn, cs);
+                    }
+                    if (!covered)
+                    {
+#pragma unroll
+                        for (int k = 0; k < NC; ++k) acc[k] = acc0[k];
+                        exact = true;
+                    }
+                }
+                if (exact)
+                {
+                    for (int i = 0; i < ne; ++i)
+                    {
+                        T ph = xo * s_x[i] + yo * s_y[i];
+                        if (IS3D) ph += zo * s_z[i];
+                        T sn, cs;
+                        trig_steps_exact(ph, &sn, &cs);
                         accumulate<T, NC>(acc, data2, s_w[i], s_idx[i],
                                 num_out, d, k0, k1, sn, cs);
                     }
@@ -251,7 +264,7 @@ int launch_dftw(int slices, int blocks_x, cudaStream_t s, int num_in,
 }
 
 __global__ void __launch_bounds__(kThreads) phase_factors_kernel(int n,
-        const double* __restrict__ phase, double2* __restrict__ out)
+        const double* __restrict__ steps, double2* __restrict__ out)
 {
     __shared__ double2 s_trig[kTrigTableSize];
     trig_table_fill(s_trig);
@@ -260,7 +273,7 @@ __global__ void __launch_bounds__(kThreads) phase_factors_kernel(int n,
             i += gridDim.x * kThreads)
     {
         double s, c;
-        trig_table_sincos(s_trig, phase[i], &s, &c);
+        trig_steps_checked(s_trig, steps[i], &s, &c);
         out[i] = make_double2(c, s);
     }
 }
@@ -321,17 +334,17 @@ int oskb_dftw_f(int matrix, int num_in, float wavenumber,
             stream);
 }
 
-int oskb_phase_factors_d(int n, const double* phase, double* out,
+int oskb_phase_factors_d(int n, const double* steps, double* out,
         void* stream)
 {
     if (n < 0) return OSKB_ERR_INVALID_ARGUMENT;
     if (n == 0) return 0;
-    if (!phase || !out) return OSKB_ERR_INVALID_ARGUMENT;
+    if (!steps || !out) return OSKB_ERR_INVALID_ARGUMENT;
     const int grid = (int) std::min<long long>(
             (n + oskb::kThreads - 1) / oskb::kThreads,
             8LL * oskb::num_sms());
     oskb::phase_factors_kernel<<<grid, oskb::kThreads, 0,
-            oskb::as_stream(stream)>>>(n, phase,
+            oskb::as_stream(stream)>>>(n, steps,
             reinterpret_cast<double2*>(out));
     return oskb::check_launch("phase_factors");
 }

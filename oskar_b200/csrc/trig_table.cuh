@@ -3,20 +3,21 @@
 // bounds the kernel on the FP64 pipe.
 //
 // Method: P. T. P. Tang's table-driven scheme ("Table-lookup algorithms for
-// elementary functions and their error analysis", ARITH 1991) with
-// Cody-Waite argument reduction (W. J. Cody and W. Waite, "Software Manual
-// for the Elementary Functions", 1980):
+// elementary functions and their error analysis", ARITH 1991). The loops
+// carry the phase in table steps, u = ph / h with h = 2 pi / 128 (the
+// per-direction factors are pre-scaled by 1 / h, so u costs the same
+// multiply-adds as ph would), and
 //
-//   ph = n h + r,  h = 2 pi / 128,  |r| <= h / 2 (plus rounding),
-//   e^{i ph} = T[n mod 128] * e^{i r},  T[j] = e^{2 pi i j / 128},
+//   u = n + f,  n = round(u),  |f| <= 1/2 (f = u - n exactly),
+//   e^{i h u} = T[n mod 128] * e^{i h f},  T[j] = e^{2 pi i j / 128},
 //
-// with e^{i r} from its Taylor series: sin r to r^7 and cos r - 1 to r^6;
-// the first omitted terms, r^9/9! and r^8/8!, are below 4e-18 for
-// |r| <= pi / 128. h is carried as a head (the double nearest pi, over 64)
-// and a tail ((pi - that double) / 64), applied with fused multiply-adds,
-// so r is accurate to about one ulp of r for |ph| < 2^40; larger phases,
-// infinities and NaN take sincos(). n comes from adding 1.5 x 2^52, which
-// leaves round(ph / h) in the low bits of the sum.
+// with e^{i h f} from the Taylor series of sin and cos in x = h f,
+// |x| <= pi / 128, written as polynomials in f: sin to x^7 and cos - 1 to
+// x^6; the first omitted terms, x^9/9! and x^8/8!, are below 4e-18. n comes
+// from adding 1.5 x 2^52, which leaves round(u) in the low bits of the
+// sum; the high word of that sum is one of two values exactly when
+// -2^32 <= n < 2^32 (|ph| below 2.1e8 rad), which is the range the table
+// path covers. Other phases, infinities and NaN are flagged for sincospi().
 //
 // The table sits in shared memory as 8 copies interleaved entry by entry:
 // entry j of copy c is element 8 j + c. A 16-byte shared load is served a
@@ -24,8 +25,9 @@
 // lies in bank group l mod 8 whatever the index, so the random lookups of a
 // warp take four wavefronts and never conflict. 16 KB per CTA.
 //
-// Cost per phase factor: 16 FP64 operations, one 16-byte shared load and
-// two integer operations, against one library sincos.
+// Cost per phase factor: 15 FP64 operations (3 for the reduction, 8 for the
+// polynomials, 4 to rotate the table entry), one 16-byte shared load and
+// three integer operations, against one library sincos.
 #pragma once
 
 #include "common.cuh"
@@ -35,6 +37,9 @@ namespace oskb {
 constexpr int kTrigEntries = 128;
 constexpr int kTrigCopies = 8;
 constexpr int kTrigTableSize = kTrigEntries * kTrigCopies;  // double2 slots
+
+// 1 / h = 64 / pi: multiplies a phase in radians into table steps.
+constexpr double kTrigStepsPerRadian = 20.371832715762604;
 
 // Fills the table; all threads of the CTA take part and must reach a
 // __syncthreads() before the first lookup.
@@ -50,36 +55,29 @@ __device__ __forceinline__ void trig_table_fill(double2* table)
     }
 }
 
-// Whether the table method covers ph (false for |ph| >= 2^40 and NaN).
-__device__ __forceinline__ bool trig_table_covers(double ph)
+// e^{i h u} as (*c, *s) from the copy of this lane. Clears *covered when u
+// is outside the table's range (the result is then wrong but the lookup
+// stays inside the table): hot loops accumulate the flag and redo the rare
+// uncovered case with trig_steps_exact, so the unrolled body has no branch.
+__device__ __forceinline__ void trig_steps_sincos(const double2* table,
+        double u, double* s, double* c, bool& covered)
 {
-    return fabs(ph) < 1.0995116277760000e12;
-}
-
-// e^{i ph} as (*c, *s), reading the copy of this lane; no range check (a
-// phase outside trig_table_covers gives a wrong but finite-index result).
-// Hot loops call this and redo the rare uncovered case with sincos, so
-// that the unrolled loop body has no branch.
-__device__ __forceinline__ void trig_table_sincos_unchecked(
-        const double2* table, double ph, double* s, double* c)
-{
-    // 64 / pi and the head/tail split of pi / 64.
-    constexpr double kInvStep = 20.371832715762604;
-    constexpr double kStepHi = 3.141592653589793 / 64.0;
-    constexpr double kStepLo = 1.2246467991473532e-16 / 64.0;
     constexpr double kShift = 6755399441055744.0;  // 1.5 x 2^52
-    const double t = fma(ph, kInvStep, kShift);
+    constexpr double h = 3.141592653589793 / 64.0;
+    constexpr double s1 = h, s3 = -h * h * h / 6.0,
+            s5 = h * h * h * h * h / 120.0,
+            s7 = -h * h * h * h * h * h * h / 5040.0;
+    constexpr double c2 = -h * h / 2.0, c4 = h * h * h * h / 24.0,
+            c6 = -h * h * h * h * h * h / 720.0;
+    const double t = u + kShift;
     const int n = __double2loint(t);
-    const double nd = t - kShift;
-    double r = fma(-nd, kStepHi, ph);
-    r = fma(-nd, kStepLo, r);
-    const double r2 = r * r;
-    // sin r = r + r^3 (-1/6 + r^2 (1/120 - r^2 / 5040))
-    const double ps = fma(r2, fma(r2, -1.0 / 5040.0, 1.0 / 120.0),
-            -1.0 / 6.0);
-    const double sr = fma(r * r2, ps, r);
-    // cos r - 1 = r^2 (-1/2 + r^2 (1/24 - r^2 / 720))
-    const double cm = r2 * fma(r2, fma(r2, -1.0 / 720.0, 1.0 / 24.0), -0.5);
+    covered &= (unsigned) (__double2hiint(t) - 0x4337FFFF) <= 1u;
+    const double f = u - (t - kShift);
+    const double f2 = f * f;
+    // sin(h f) = f (s1 + f^2 (s3 + f^2 (s5 + f^2 s7)))
+    const double sr = f * fma(f2, fma(f2, fma(f2, s7, s5), s3), s1);
+    // cos(h f) - 1 = f^2 (c2 + f^2 (c4 + f^2 c6))
+    const double cm = f2 * fma(f2, fma(f2, c6, c4), c2);
     const double2 e = table[((n & (kTrigEntries - 1)) * kTrigCopies) |
             (threadIdx.x & (kTrigCopies - 1))];
     // (e.x + i e.y)(1 + cm + i sr), the small terms added to e last
@@ -87,17 +85,21 @@ __device__ __forceinline__ void trig_table_sincos_unchecked(
     *s = fma(e.y, cm, fma(e.x, sr, e.y));
 }
 
-// e^{i ph} as (*c, *s) for any ph: the table where it covers ph, else
-// sincos().
-__device__ __forceinline__ void trig_table_sincos(const double2* table,
-        double ph, double* s, double* c)
+// e^{i h u} for any u, through the library: sincospi(u / 64) (u / 64 is
+// exact).
+__device__ __forceinline__ void trig_steps_exact(double u, double* s,
+        double* c)
 {
-    if (!trig_table_covers(ph))
-    {
-        sincos(ph, s, c);
-        return;
-    }
-    trig_table_sincos_unchecked(table, ph, s, c);
+    sincospi(u * (1.0 / (kTrigEntries / 2)), s, c);
+}
+
+// e^{i h u} for any u: the table where it covers u, else the library.
+__device__ __forceinline__ void trig_steps_checked(const double2* table,
+        double u, double* s, double* c)
+{
+    bool covered = true;
+    trig_steps_sincos(table, u, s, c, covered);
+    if (!covered) trig_steps_exact(u, s, c);
 }
 
 }  // namespace oskb

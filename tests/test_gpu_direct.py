@@ -286,6 +286,46 @@ def test_dftw(real, matrix, is_3d, use_idx, ex, ey):
                  tol=1e-12 if real == np.float64 else 2e-5)
 
 
+@pytest.mark.parametrize("n_in", [40, 700])
+def test_dftw_non_finite_and_huge_phases(n_in):
+    """FP64 phases the shared table does not cover (NaN, and beyond 2^51
+    table steps) go through the exact path: one NaN element coordinate
+    makes every direction NaN, as in the oracle; an element 1e15 m away
+    (phase ~ 1e15 rad, whose value no two formulas agree on) is given zero
+    weight, so the sums must still match the oracle's to 1e-12 with every
+    CTA taking the exact path for that chunk. n_in = 40 runs the CTAs
+    without the table, 700 with it."""
+    rng = np.random.default_rng(12)
+    n_out = 900
+    k = 2 * np.pi * 100e6 / 299792458.0
+    ph = rng.uniform(0, 2 * np.pi, n_in)
+    w = np.stack([np.cos(ph), np.sin(ph)], 1).ravel()
+    xi, yi = (rng.uniform(-20, 20, n_in) for _ in range(2))
+    xo, yo = (rng.uniform(-1, 1, n_out) for _ in range(2))
+    data = rng.uniform(-1, 1, n_in * n_out * 2)
+    xi_far = xi.copy()
+    xi_far[n_in // 2] = 1e15
+    w_far = w.copy()
+    w_far[2 * (n_in // 2):2 * (n_in // 2) + 2] = 0.0
+    xi_nan = xi.copy()
+    xi_nan[n_in // 3] = np.nan
+    for x_el, w in ((xi_far, w_far), (xi_nan, w)):
+        ref = np.zeros(n_out * 2)
+        oracle().call("dftw_d", np.float64, 0, 0, n_in, k, w, x_el, yi,
+                      None, 0, n_out, xo, yo, None, None, data, 1, 1, 0,
+                      ref, 1.0 / n_in)
+        out = torch.zeros(n_out * 2, dtype=torch.float64, device="cuda")
+        ob.call("oskb_dftw_d", 0, n_in, k, dev(w), dev(x_el), dev(yi),
+                None, 0, n_out, dev(xo), dev(yo), None, None, dev(data), 1,
+                1, 0, out, 1.0 / n_in, ob.stream_ptr())
+        torch.cuda.synchronize()
+        got = out.cpu().numpy()
+        if np.isnan(x_el).any():
+            assert np.all(np.isnan(ref)) and np.all(np.isnan(got))
+        else:
+            assert_close(got, ref, np.float64, tol=1e-12)
+
+
 @pytest.mark.parametrize("real", [np.float64, np.float32])
 def test_element_weights(real):
     rng = np.random.default_rng(7)
