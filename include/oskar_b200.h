@@ -262,6 +262,74 @@ OSKB_API int oskb_station_beam_aa_f(int num_stations, int num_elements,
         const float* y, const float* z, int directions_per_station,
         float* beam, void* stream);
 
+/* oskb_station_beam_aa with one complex factor per element multiplying the
+ * element's DFT weight: element_weight_factors [station][element] complex
+ * (NULL: none), e.g. the product of time-variable element errors and
+ * apodisation from oskb_station_element_weight_factors, as
+ * oskar_station_evaluate_element_weights
+ * (oskar/telescope/station/src/oskar_station_evaluate_element_weights.c:
+ * 33-64) applies them to the weights; the normalisation direction uses the
+ * same weights. */
+OSKB_API int oskb_station_beam_aa_weighted_d(int num_stations,
+        int num_elements, const double* el_x, const double* el_y,
+        const double* el_z, const double* meas_x, const double* meas_y,
+        const double* meas_z, const double* cable_length_error,
+        const double* element_weight_factors,
+        const double* orientation_x_rad, const double* orientation_y_rad,
+        double dipole_length_m, int normalise_element, int normalise_array,
+        int normalise_final, int swap_xy, int is_3d, double frequency_hz,
+        const double* beam_enu, const double* norm_enu, int num_directions,
+        const double* x, const double* y, const double* z,
+        int directions_per_station, double* beam, void* stream);
+OSKB_API int oskb_station_beam_aa_weighted_f(int num_stations,
+        int num_elements, const float* el_x, const float* el_y,
+        const float* el_z, const float* meas_x, const float* meas_y,
+        const float* meas_z, const float* cable_length_error,
+        const float* element_weight_factors,
+        const double* orientation_x_rad, const double* orientation_y_rad,
+        double dipole_length_m, int normalise_element, int normalise_array,
+        int normalise_final, int swap_xy, int is_3d, double frequency_hz,
+        const double* beam_enu, const double* norm_enu, int num_directions,
+        const float* x, const float* y, const float* z,
+        int directions_per_station, float* beam, void* stream);
+
+/* Time-variable element gain and phase errors of one station:
+ * errors[e] = (gain[e] + gain_error[e] g) exp(i (phase[e] + phase_error[e] h))
+ * with (g, h) a standard Gaussian pair per element drawn from Philox4x32-10
+ * (key {random_seed, 0xCAFEF00D}, counter {e / 2, time_index, station_id,
+ * 0x12345678}) and the Box-Muller transform, as the reference draws them.
+ * errors: complex [element]. Replaces oskar_evaluate_element_weights_errors
+ * (oskar/telescope/station/oskar_evaluate_element_weights_errors.h;
+ * src/oskar_evaluate_element_weights_errors.c:19-110) with the random fill
+ * of oskar_mem_random_gaussian (oskar/mem/src/oskar_mem_random_gaussian.c). */
+OSKB_API int oskb_evaluate_element_weights_errors_d(int num_elements,
+        const double* gain, const double* gain_error, const double* phase,
+        const double* phase_error, unsigned int random_seed, int time_index,
+        int station_id, double* errors, void* stream);
+OSKB_API int oskb_evaluate_element_weights_errors_f(int num_elements,
+        const float* gain, const float* gain_error, const float* phase,
+        const float* phase_error, unsigned int random_seed, int time_index,
+        int station_id, float* errors, void* stream);
+
+/* Element weight factors of num_stations stations in one launch:
+ * factors[s][e] = errors (as oskb_evaluate_element_weights_errors, station
+ * id first_station_id + s; skipped when gain is NULL) times
+ * apodisation[s][e] (complex; skipped when NULL); 1 when both are skipped.
+ * gain, gain_error, phase, phase_error: [station][element] when
+ * per_station, else [element] shared by every station. No single OSKAR
+ * counterpart: the per-station steps of
+ * oskar_station_evaluate_element_weights.c:33-64 for all stations. */
+OSKB_API int oskb_station_element_weight_factors_d(int num_stations,
+        int num_elements, int first_station_id, unsigned int random_seed,
+        int time_index, const double* gain, const double* gain_error,
+        const double* phase, const double* phase_error, int per_station,
+        const double* apodisation, double* factors, void* stream);
+OSKB_API int oskb_station_element_weight_factors_f(int num_stations,
+        int num_elements, int first_station_id, unsigned int random_seed,
+        int time_index, const float* gain, const float* gain_error,
+        const float* phase, const float* phase_error, int per_station,
+        const float* apodisation, float* factors, void* stream);
+
 /* Two-level (hierarchical) aperture-array station: a station of num_tiles
  * tiles at ENU positions tile_x/y/z [tile] (true positions, metres), tile t
  * a dipole array of layout tile_type[t] (NULL: every tile of layout 0, the

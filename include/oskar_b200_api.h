@@ -134,6 +134,14 @@ OSKB_API void oskar_jones_apply_cable_length_errors(oskar_Jones* jones,
  * must match the Jones array's type and location. */
 OSKB_API void oskar_jones_apply_station_gains(oskar_Jones* jones,
         oskar_Mem* gains, int* status);
+/* oskar/telescope/station/oskar_evaluate_element_weights_errors.h:62-66.
+ * The gain and phase arrays must have the precision and location of the
+ * complex errors array. */
+OSKB_API void oskar_evaluate_element_weights_errors(int num_elements,
+        const oskar_Mem* gain, const oskar_Mem* gain_error,
+        const oskar_Mem* phase, const oskar_Mem* phase_error,
+        unsigned int random_seed, int time_index, int station_id,
+        oskar_Mem* errors, int* status);
 /* oskar/mem/oskar_mem_multiply.h:63 */
 OSKB_API void oskar_mem_multiply(oskar_Mem* out, const oskar_Mem* in1,
         const oskar_Mem* in2, size_t offset_out, size_t offset_in1,

@@ -5,6 +5,7 @@
  */
 #include <math.h>
 #include <stddef.h>
+#include <stdint.h>
 #include <stdlib.h>
 #include "oskar_oracle.h"
 
@@ -22,6 +23,7 @@
 #define ORC_COS cos
 #define ORC_EXP exp
 #define ORC_SQRT sqrt
+#define ORC_LOG log
 #define ORC_ATAN2 atan2
 #define ORC_FMOD fmod
 #define ORC_KAHAN 0
@@ -33,6 +35,7 @@
 #undef ORC_COS
 #undef ORC_EXP
 #undef ORC_SQRT
+#undef ORC_LOG
 #undef ORC_ATAN2
 #undef ORC_FMOD
 #undef ORC_KAHAN
@@ -45,6 +48,7 @@
 #define ORC_COS cosf
 #define ORC_EXP expf
 #define ORC_SQRT sqrtf
+#define ORC_LOG logf
 #define ORC_ATAN2 atan2f
 #define ORC_FMOD fmodf
 #define ORC_KAHAN 1

@@ -83,6 +83,15 @@ void orc_blank_below_horizon_##S(int off_mask, int n, const REAL* mask, \
 void orc_jones_r_##S(int num_sources, const REAL* ra, const REAL* dec, \
         REAL cos_lat, REAL sin_lat, REAL lst_rad, int offset_out, \
         REAL* jones); \
+void orc_station_beam_aa_weighted_##S(int num_el, const REAL* x, \
+        const REAL* y, const REAL* z, const REAL* x_meas, \
+        const REAL* y_meas, const REAL* z_meas, const REAL* cable, \
+        const REAL* weight_factors, double orientation_x_rad, \
+        double orientation_y_rad, double dipole_length_m, int norm_element, \
+        int norm_array, int norm_final, int swap_xy, int is_3d, \
+        double frequency_hz, double bx, double by, double bz, double nx, \
+        double ny, double nz, int num_dir, const REAL* dx, const REAL* dy, \
+        const REAL* dz, REAL* beam); \
 void orc_station_beam_aa_##S(int num_el, const REAL* x, const REAL* y, \
         const REAL* z, const REAL* x_meas, const REAL* y_meas, \
         const REAL* z_meas, const REAL* cable, double orientation_x_rad, \
@@ -103,7 +112,12 @@ void orc_cable_length_errors_##S(int matrix, int num_sources, \
         int num_stations, REAL wavenumber, const REAL* errors_x, \
         const REAL* errors_y, REAL* jones); \
 void orc_station_gains_##S(int matrix, int num_sources, int num_stations, \
-        const REAL* gains, REAL* jones);
+        const REAL* gains, REAL* jones); \
+void orc_random_gaussian_##S(unsigned int n, REAL* data, unsigned int seed, \
+        unsigned int c1, unsigned int c2, unsigned int c3, REAL std); \
+void orc_element_weights_errors_##S(int n, const REAL* gain, \
+        const REAL* gain_error, const REAL* phase, const REAL* phase_error, \
+        unsigned int seed, int time_index, int station_id, REAL* errors);
 
 ORC_DECLARE(double, d)
 ORC_DECLARE(float, f)

@@ -671,9 +671,10 @@ void ORC_FN(orc_jones_r)(int num_sources, const REAL* ra, const REAL* dec,
  *    weighted DFT over the true positions, horizon blanking.
  * Scalars that the reference derives in double (wavenumber, kL, delta phi)
  * are derived in double here too, then rounded to REAL. */
-void ORC_FN(orc_station_beam_aa)(int num_el, const REAL* x, const REAL* y,
-        const REAL* z, const REAL* x_meas, const REAL* y_meas,
-        const REAL* z_meas, const REAL* cable, double orientation_x_rad,
+void ORC_FN(orc_station_beam_aa_weighted)(int num_el, const REAL* x,
+        const REAL* y, const REAL* z, const REAL* x_meas, const REAL* y_meas,
+        const REAL* z_meas, const REAL* cable, const REAL* weight_factors,
+        double orientation_x_rad,
         double orientation_y_rad, double dipole_length_m, int norm_element,
         int norm_array, int norm_final, int swap_xy, int is_3d,
         double frequency_hz, double bx, double by, double bz, double nx,
@@ -721,6 +722,18 @@ void ORC_FN(orc_station_beam_aa)(int num_el, const REAL* x, const REAL* y,
     ORC_FN(orc_element_weights_dft)(num_el, x_meas ? x_meas : x,
             y_meas ? y_meas : y, z_meas ? z_meas : z, cable,
             (REAL) wavenumber, (REAL) bx, (REAL) by, (REAL) bz, w);
+    /* element errors, gains, apodisation: weights *= factor
+     * (oskar_station_evaluate_element_weights.c:33-64) */
+    if (weight_factors)
+        for (i = 0; i < num_el; ++i)
+        {
+            ORC_T(cx) a = {w[2 * i], w[2 * i + 1]};
+            const ORC_T(cx) f = {weight_factors[2 * i],
+                    weight_factors[2 * i + 1]};
+            a = ORC_T(cmul)(a, f);
+            w[2 * i] = a.re;
+            w[2 * i + 1] = a.im;
+        }
     ORC_FN(orc_dftw)(1, is_3d, num_el, (REAL) wavenumber, w, x, y, z, 0, np,
             X, Y, is_3d ? Z : 0, types, signal, 1, 1, 0, out,
             norm_array ? (REAL) (1.0 / num_el) : (REAL) 1);
@@ -729,6 +742,22 @@ void ORC_FN(orc_station_beam_aa)(int num_el, const REAL* x, const REAL* y,
     for (i = 0; i < 8 * num_dir; ++i) beam[i] = out[i];
     free(X); free(Y); free(Z); free(theta); free(phi1); free(phi2);
     free(signal); free(out); free(w); free(types);
+}
+
+void ORC_FN(orc_station_beam_aa)(int num_el, const REAL* x, const REAL* y,
+        const REAL* z, const REAL* x_meas, const REAL* y_meas,
+        const REAL* z_meas, const REAL* cable, double orientation_x_rad,
+        double orientation_y_rad, double dipole_length_m, int norm_element,
+        int norm_array, int norm_final, int swap_xy, int is_3d,
+        double frequency_hz, double bx, double by, double bz, double nx,
+        double ny, double nz, int num_dir, const REAL* dx, const REAL* dy,
+        const REAL* dz, REAL* beam)
+{
+    ORC_FN(orc_station_beam_aa_weighted)(num_el, x, y, z, x_meas, y_meas,
+            z_meas, cable, 0, orientation_x_rad, orientation_y_rad,
+            dipole_length_m, norm_element, norm_array, norm_final, swap_xy,
+            is_3d, frequency_hz, bx, by, bz, nx, ny, nz, num_dir, dx, dy, dz,
+            beam);
 }
 
 /* Relative direction cosines of (lon, lat) about (lon0, lat0)
@@ -1116,4 +1145,104 @@ void ORC_FN(orc_station_gains)(int matrix, int num_sources,
                 e[6] = out.d.re; e[7] = out.d.im;
             }
         }
+}
+
+#ifndef ORC_PHILOX_
+#define ORC_PHILOX_
+/* Philox4x32-10 (J. K. Salmon, M. A. Moraes, R. O. Dror, D. E. Shaw,
+ * "Parallel random numbers: as easy as 1, 2, 3", SC11, 2011), restated
+ * from the paper: ten rounds; each round multiplies counter words 0 and 2
+ * by 0xD2511F53 and 0xCD9E8D57 into 64-bit products and mixes the high
+ * halves with the other words and the round key; the key is bumped by the
+ * Weyl constants 0x9E3779B9 and 0xBB67AE85 before every round after the
+ * first. The reference calls Random123's implementation (its
+ * extern/Random123/philox.h) through math/private_random_generators.h:17-35
+ * with key {seed, 0xCAFEF00D} and counter {index, c1, c2, c3}. */
+static void orc_philox4x32_10(const uint32_t ctr[4], uint32_t seed,
+        uint32_t out[4])
+{
+    uint32_t c0 = ctr[0], c1 = ctr[1], c2 = ctr[2], c3 = ctr[3];
+    uint32_t k0 = seed, k1 = 0xCAFEF00Du;
+    int r;
+    for (r = 0; r < 10; ++r)
+    {
+        uint64_t p0, p1;
+        if (r > 0)
+        {
+            k0 += 0x9E3779B9u;
+            k1 += 0xBB67AE85u;
+        }
+        p0 = (uint64_t) 0xD2511F53u * c0;
+        p1 = (uint64_t) 0xCD9E8D57u * c2;
+        c0 = (uint32_t) (p1 >> 32) ^ c1 ^ k0;
+        c1 = (uint32_t) p1;
+        c2 = (uint32_t) (p0 >> 32) ^ c3 ^ k1;
+        c3 = (uint32_t) p0;
+    }
+    out[0] = c0; out[1] = c1; out[2] = c2; out[3] = c3;
+}
+#endif
+
+/* Box-Muller pair from two 32-bit integers as the reference's CPU path
+ * forms it (math/private_random_helpers.h:42-107): angle pi x with
+ * x = u0 2^-31 + 2^-32 (u0 taken as a non-negative integer, so x lies in
+ * (0, 2)), radius sqrt(-2 log(u1 2^-32 + 2^-33)). */
+static void ORC_T(box_muller)(uint32_t u0, uint32_t u1, REAL* f0, REAL* f1)
+{
+    const REAL f_angle = (REAL) 1 / ((REAL) 1 + (REAL) 0x7FFFFFFFuL);
+    const REAL f_unit = (REAL) 1 / ((REAL) 1 + (REAL) 0xFFFFFFFFuL);
+    const REAL x = ((REAL) (long) u0 * f_angle) + (REAL) 0.5 * f_angle;
+    const REAL y = ((REAL) u1 * f_unit) + (REAL) 0.5 * f_unit;
+    REAL t = (REAL) ORC_PI, r;
+    t *= x;
+    *f0 = ORC_SIN(t);
+    *f1 = ORC_COS(t);
+    r = ORC_SQRT((REAL) -2 * ORC_LOG(y));
+    *f0 *= r;
+    *f1 *= r;
+}
+
+/* n Gaussian values of standard deviation std, four per Philox call with
+ * counter {i / 4, c1, c2, c3} (mem/src/oskar_mem_random_gaussian.c:14-130,
+ * CPU path). */
+void ORC_FN(orc_random_gaussian)(unsigned int n, REAL* data,
+        unsigned int seed, unsigned int c1, unsigned int c2,
+        unsigned int c3, REAL std)
+{
+    unsigned int q, k;
+    for (q = 0; 4 * (size_t) q < n; ++q)
+    {
+        const uint32_t ctr[4] = {q, c1, c2, c3};
+        uint32_t u[4];
+        REAL t[4];
+        orc_philox4x32_10(ctr, seed, u);
+        ORC_T(box_muller)(u[0], u[1], &t[0], &t[1]);
+        ORC_T(box_muller)(u[2], u[3], &t[2], &t[3]);
+        for (k = 0; k < 4 && 4 * q + k < n; ++k) data[4 * q + k] = std * t[k];
+    }
+}
+
+/* Time-variable element gain and phase errors: a Gaussian pair (g, h) per
+ * element from counter {i / 2, time_index, station_id, 0x12345678}, then
+ * (gain + gain_error g) e^{i (phase + phase_error h)}
+ * (telescope/station/src/oskar_evaluate_element_weights_errors.c:19-110,
+ * define_evaluate_element_weights_errors.h:3-16). */
+void ORC_FN(orc_element_weights_errors)(int n, const REAL* gain,
+        const REAL* gain_error, const REAL* phase, const REAL* phase_error,
+        unsigned int seed, int time_index, int station_id, REAL* errors)
+{
+    int i;
+    ORC_FN(orc_random_gaussian)(2 * (unsigned int) n, errors, seed,
+            (unsigned int) time_index, (unsigned int) station_id,
+            0x12345678u, (REAL) 1);
+    for (i = 0; i < n; ++i)
+    {
+        REAL re = errors[2 * i], ph = errors[2 * i + 1];
+        re *= gain_error[i];
+        re += gain[i];
+        ph *= phase_error[i];
+        ph += phase[i];
+        errors[2 * i] = ORC_COS(ph) * re;
+        errors[2 * i + 1] = ORC_SIN(ph) * re;
+    }
 }

@@ -63,6 +63,7 @@ station_beam_kernel(int num_elements, const T* __restrict__ el_x,
         const T* __restrict__ el_y, const T* __restrict__ el_z,
         const T* __restrict__ meas_x, const T* __restrict__ meas_y,
         const T* __restrict__ meas_z, const T* __restrict__ cable,
+        const T* __restrict__ weight_factors,
         const double* __restrict__ orientation_x,
         const double* __restrict__ orientation_y, T kL, T cos_kL,
         BeamFlags flags, T wavenumber, const double* __restrict__ beam_enu,
@@ -137,6 +138,14 @@ station_beam_kernel(int num_elements, const T* __restrict__ el_x,
                     (cable ? cable[g] : (T) 0));
             T sn, cs;
             sincos(-p, &sn, &cs);
+            if (weight_factors)
+            {
+                // element errors x apodisation, applied to the DFT weight
+                const T2 f = reinterpret_cast<const T2*>(weight_factors)[g];
+                const T re = cs * f.x - sn * f.y;
+                sn = cs * f.y + sn * f.x;
+                cs = re;
+            }
             s_w[t] = T2{cs, sn};
             s_x[t] = el_x[g];
             s_y[t] = el_y[g];
@@ -303,7 +312,8 @@ namespace {
 template <typename T>
 int station_beam_aa(int num_stations, int num_elements, const T* el_x,
         const T* el_y, const T* el_z, const T* meas_x, const T* meas_y,
-        const T* meas_z, const T* cable, const double* orientation_x,
+        const T* meas_z, const T* cable, const T* weight_factors,
+        const double* orientation_x,
         const double* orientation_y, double dipole_length_m,
         int normalise_element, int normalise_array, int normalise_final,
         int swap_xy, int is_3d, double frequency_hz, const double* beam_enu,
@@ -327,7 +337,8 @@ int station_beam_aa(int num_stations, int num_elements, const T* el_x,
     cudaStream_t s = as_stream(stream);
 #define OSKB_BEAM(D) station_beam_kernel<T, D><<<grid, kThreads, 0, s>>>(     \
         num_elements, el_x, el_y, el_z, meas_x, meas_y, meas_z, cable,       \
-        orientation_x, orientation_y, (T) kL, (T) cos(kL), flags,            \
+        weight_factors, orientation_x, orientation_y, (T) kL, (T) cos(kL),   \
+        flags,                                                               \
         wavenumber, beam_enu, norm_enu, num_directions, x, y, z,             \
         directions_per_station, beam)
     if (is_3d) OSKB_BEAM(true); else OSKB_BEAM(false);
@@ -367,11 +378,30 @@ int oskb_station_beam_aa_##S(int num_stations, int num_elements,             \
         T* beam, void* stream)                                               \
 {                                                                            \
     return oskb::station_beam_aa<T>(num_stations, num_elements, el_x, el_y,  \
-            el_z, meas_x, meas_y, meas_z, cable_length_error,                \
+            el_z, meas_x, meas_y, meas_z, cable_length_error, nullptr,       \
             orientation_x_rad, orientation_y_rad, dipole_length_m,           \
             normalise_element, normalise_array, normalise_final, swap_xy,    \
             is_3d, frequency_hz, beam_enu, norm_enu, num_directions, x, y,   \
             z, directions_per_station, beam, stream);                        \
+}                                                                            \
+int oskb_station_beam_aa_weighted_##S(int num_stations, int num_elements,    \
+        const T* el_x, const T* el_y, const T* el_z, const T* meas_x,        \
+        const T* meas_y, const T* meas_z, const T* cable_length_error,       \
+        const T* element_weight_factors,                                     \
+        const double* orientation_x_rad, const double* orientation_y_rad,    \
+        double dipole_length_m, int normalise_element, int normalise_array,  \
+        int normalise_final, int swap_xy, int is_3d, double frequency_hz,    \
+        const double* beam_enu, const double* norm_enu, int num_directions,  \
+        const T* x, const T* y, const T* z, int directions_per_station,      \
+        T* beam, void* stream)                                               \
+{                                                                            \
+    return oskb::station_beam_aa<T>(num_stations, num_elements, el_x, el_y,  \
+            el_z, meas_x, meas_y, meas_z, cable_length_error,                \
+            element_weight_factors, orientation_x_rad, orientation_y_rad,    \
+            dipole_length_m, normalise_element, normalise_array,             \
+            normalise_final, swap_xy, is_3d, frequency_hz, beam_enu,         \
+            norm_enu, num_directions, x, y, z, directions_per_station, beam, \
+            stream);                                                         \
 }                                                                            \
 int oskb_evaluate_jones_R_##S(int num_sources, const T* ra_rad,              \
         const T* dec_rad, int num_stations, const double* lat_rad,           \
@@ -466,7 +496,8 @@ int station_beam_two_level(int num_tile_types, int num_elements,
     // tile beams [type][direction]: element pattern x tile array factor,
     // blanked below the horizon, no final normalisation
     if (int err = station_beam_aa<T>(num_tile_types, num_elements, el_x,
-            el_y, el_z, nullptr, nullptr, nullptr, nullptr, orientation_x,
+            el_y, el_z, nullptr, nullptr, nullptr, nullptr, nullptr,
+            orientation_x,
             orientation_y, dipole_length_m, normalise_element,
             normalise_tile_array, 0, swap_xy, is_3d, frequency_hz, pointing,
             nullptr, num_directions, x, y, z, 0, tile_beams, stream))

@@ -703,6 +703,59 @@ void oskar_jones_apply_station_gains(oskar_Jones* jones, oskar_Mem* gains,
                 (float*) J->data, 0);
 }
 
+// oskar/telescope/station/src/oskar_evaluate_element_weights_errors.c:
+// 19-110: the same location, type and length checks, then the random
+// errors on the device.
+void oskar_evaluate_element_weights_errors(int num_elements,
+        const oskar_Mem* gain, const oskar_Mem* gain_error,
+        const oskar_Mem* phase, const oskar_Mem* phase_error,
+        unsigned int random_seed, int time_index, int station_id,
+        oskar_Mem* errors, int* status)
+{
+    if (*status) return;
+    const int location = errors->location;
+    const int precision = errors->type & 0x0F;
+    if (gain->location != location || gain_error->location != location ||
+            phase->location != location || phase_error->location != location)
+    {
+        *status = OSKAR_ERR_LOCATION_MISMATCH;
+        return;
+    }
+    if (gain->type != precision || phase->type != precision ||
+            gain_error->type != precision || phase_error->type != precision)
+    {
+        *status = OSKAR_ERR_TYPE_MISMATCH;
+        return;
+    }
+    if ((int) errors->num_elements < num_elements ||
+            (int) gain->num_elements < num_elements ||
+            (int) gain_error->num_elements < num_elements ||
+            (int) phase->num_elements < num_elements ||
+            (int) phase_error->num_elements < num_elements)
+    {
+        *status = OSKAR_ERR_DIMENSION_MISMATCH;
+        return;
+    }
+    if (location != OSKAR_GPU)
+    {
+        *status = OSKAR_ERR_BAD_LOCATION;
+        return;
+    }
+    if (errors->type == OSKAR_DOUBLE_COMPLEX)
+        *status = oskb_evaluate_element_weights_errors_d(num_elements,
+                D(gain), D(gain_error), D(phase), D(phase_error),
+                random_seed, time_index, station_id, (double*) errors->data,
+                0);
+    else if (errors->type == OSKAR_SINGLE_COMPLEX)
+        *status = oskb_evaluate_element_weights_errors_f(num_elements,
+                (const float*) gain->data, (const float*) gain_error->data,
+                (const float*) phase->data, (const float*) phase_error->data,
+                random_seed, time_index, station_id, (float*) errors->data,
+                0);
+    else
+        *status = OSKAR_ERR_BAD_DATA_TYPE;
+}
+
 // oskar/interferometer/src/oskar_evaluate_jones_K.c:19-157
 void oskar_evaluate_jones_K(oskar_Jones* K, int num_sources,
         const oskar_Mem* l, const oskar_Mem* m, const oskar_Mem* n,

@@ -358,3 +358,47 @@ def test_cable_length_errors_and_gains(real, matrix, ex, ey):
     reference().call("station_gains_" + suffix(real), real, int(matrix),
                      nsrc, nst, G, b)
     assert _close(a, b, real)
+
+
+@pytest.mark.parametrize("real", [np.float64, np.float32])
+@pytest.mark.parametrize("n", [1, 2, 3, 4, 5, 255, 4096])
+def test_random_gaussian(real, n):
+    """The oracle's Philox4x32-10 + Box-Muller fill against the reference's
+    own CPU fill (mem/src/oskar_mem_random_gaussian.c with its vendored
+    Random123), bit for bit, including the ragged last quad."""
+    for seed, c1, c2, c3 in [(1, 0, 0, 0), (42, 7, 3, 0x12345678),
+                             (0xFFFFFFF0, 123456, 65535, 0xDEADBEEF)]:
+        a = np.zeros(n, real)
+        b = np.ones(n, real)
+        oracle().call("random_gaussian_" + suffix(real), real, n, a, seed,
+                      c1, c2, c3, 2.5)
+        reference().call("random_gaussian_" + suffix(real), real, n, b,
+                         seed, c1, c2, c3, 2.5)
+        assert np.array_equal(a, b)
+    big = np.zeros(200_000, real)
+    oracle().call("random_gaussian_" + suffix(real), real, len(big), big, 3,
+                  1, 2, 3, 1.0)
+    assert abs(big.mean()) < 0.01 and abs(big.std() - 1) < 0.01
+
+
+@pytest.mark.parametrize("real", [np.float64, np.float32])
+def test_element_weights_errors(real):
+    """Time-variable element gain/phase errors
+    (oskar_evaluate_element_weights_errors.c:19-110): oracle against the
+    reference's CPU chain, bit for bit, for several stations and times."""
+    rng = np.random.default_rng(8)
+    n = 257
+    gain = rng.uniform(0.9, 1.1, n).astype(real)
+    gain_err = rng.uniform(0, 0.1, n).astype(real)
+    phase = rng.uniform(-0.2, 0.2, n).astype(real)
+    phase_err = rng.uniform(0, 0.05, n).astype(real)
+    for seed, t, st in [(1, 0, 0), (99, 5, 17), (2**31 + 5, 1000, 511)]:
+        a = np.zeros(2 * n, real)
+        b = np.ones(2 * n, real)
+        oracle().call("element_weights_errors_" + suffix(real), real, n,
+                      gain, gain_err, phase, phase_err, seed, t, st, a)
+        reference().call("element_weights_errors_" + suffix(real), real, n,
+                         gain, gain_err, phase, phase_err, seed, t, st, b)
+        assert np.array_equal(a, b)
+        amp = np.hypot(a[0::2], a[1::2])
+        assert np.all(np.abs(amp - gain) <= 6 * gain_err + 1e-6)
