@@ -293,6 +293,41 @@ OSKB_API int oskb_station_beam_aa_weighted_f(int num_stations,
         const float* x, const float* y, const float* z,
         int directions_per_station, float* beam, void* stream);
 
+/* oskb_station_beam_aa_weighted for stations with up to 4 element types of
+ * common orientation (the reference's common-orientation branch,
+ * oskar_evaluate_station_beam_aperture_array.c:158-179 and its oskar_dftw
+ * with data index = element type): element e has type
+ * element_type[station][e] (device; NULL: all type 0), type t is a dipole
+ * of length dipole_length_m[t] (host array of num_element_types) with its
+ * own pole normalisation; beam = sum over types of the type's pattern
+ * times the array factor of its elements. An element whose type is outside
+ * [0, num_element_types) adds nothing (the reference stops with
+ * OSKAR_ERR_OUT_OF_RANGE). num_element_types > 4: OSKB_ERR_OUT_OF_RANGE. */
+OSKB_API int oskb_station_beam_aa_types_d(int num_stations, int num_elements,
+        const double* el_x, const double* el_y, const double* el_z,
+        const double* meas_x, const double* meas_y, const double* meas_z,
+        const double* cable_length_error,
+        const double* element_weight_factors, int num_element_types,
+        const int* element_type, const double* dipole_length_m,
+        const double* orientation_x_rad, const double* orientation_y_rad,
+        int normalise_element, int normalise_array, int normalise_final,
+        int swap_xy, int is_3d, double frequency_hz, const double* beam_enu,
+        const double* norm_enu, int num_directions, const double* x,
+        const double* y, const double* z, int directions_per_station,
+        double* beam, void* stream);
+OSKB_API int oskb_station_beam_aa_types_f(int num_stations, int num_elements,
+        const float* el_x, const float* el_y, const float* el_z,
+        const float* meas_x, const float* meas_y, const float* meas_z,
+        const float* cable_length_error,
+        const float* element_weight_factors, int num_element_types,
+        const int* element_type, const double* dipole_length_m,
+        const double* orientation_x_rad, const double* orientation_y_rad,
+        int normalise_element, int normalise_array, int normalise_final,
+        int swap_xy, int is_3d, double frequency_hz, const double* beam_enu,
+        const double* norm_enu, int num_directions, const float* x,
+        const float* y, const float* z, int directions_per_station,
+        float* beam, void* stream);
+
 /* Time-variable element gain and phase errors of one station:
  * errors[e] = (gain[e] + gain_error[e] g) exp(i (phase[e] + phase_error[e] h))
  * with (g, h) a standard Gaussian pair per element drawn from Philox4x32-10

@@ -83,6 +83,16 @@ void orc_blank_below_horizon_##S(int off_mask, int n, const REAL* mask, \
 void orc_jones_r_##S(int num_sources, const REAL* ra, const REAL* dec, \
         REAL cos_lat, REAL sin_lat, REAL lst_rad, int offset_out, \
         REAL* jones); \
+void orc_station_beam_aa_types_##S(int num_el, const REAL* x, \
+        const REAL* y, const REAL* z, const REAL* x_meas, \
+        const REAL* y_meas, const REAL* z_meas, const REAL* cable, \
+        const REAL* weight_factors, int num_types, const int* element_type, \
+        const double* dipole_length_per_type, double orientation_x_rad, \
+        double orientation_y_rad, int norm_element, \
+        int norm_array, int norm_final, int swap_xy, int is_3d, \
+        double frequency_hz, double bx, double by, double bz, double nx, \
+        double ny, double nz, int num_dir, const REAL* dx, const REAL* dy, \
+        const REAL* dz, REAL* beam); \
 void orc_station_beam_aa_weighted_##S(int num_el, const REAL* x, \
         const REAL* y, const REAL* z, const REAL* x_meas, \
         const REAL* y_meas, const REAL* z_meas, const REAL* cable, \

@@ -671,11 +671,12 @@ void ORC_FN(orc_jones_r)(int num_sources, const REAL* ra, const REAL* dec,
  *    weighted DFT over the true positions, horizon blanking.
  * Scalars that the reference derives in double (wavenumber, kL, delta phi)
  * are derived in double here too, then rounded to REAL. */
-void ORC_FN(orc_station_beam_aa_weighted)(int num_el, const REAL* x,
+void ORC_FN(orc_station_beam_aa_types)(int num_el, const REAL* x,
         const REAL* y, const REAL* z, const REAL* x_meas, const REAL* y_meas,
         const REAL* z_meas, const REAL* cable, const REAL* weight_factors,
-        double orientation_x_rad,
-        double orientation_y_rad, double dipole_length_m, int norm_element,
+        int num_types, const int* element_type,
+        const double* dipole_length_per_type, double orientation_x_rad,
+        double orientation_y_rad, int norm_element,
         int norm_array, int norm_final, int swap_xy, int is_3d,
         double frequency_hz, double bx, double by, double bz, double nx,
         double ny, double nz, int num_dir, const REAL* dx, const REAL* dy,
@@ -685,12 +686,11 @@ void ORC_FN(orc_station_beam_aa_weighted)(int num_el, const REAL* x,
     const int np = num_dir + (norm_final ? 1 : 0);
     const int npe = np + (norm_element ? 1 : 0);
     const double wavenumber = 2.0 * ORC_PI * frequency_hz / c0;
-    const double kL = dipole_length_m * (ORC_PI * frequency_hz / c0);
     const double dphi1 = ORC_PI / 2 - (orientation_x_rad + ORC_PI / 2);
     const double dphi2 = ORC_PI / 2 - orientation_y_rad;
-    REAL *X, *Y, *Z, *theta, *phi1, *phi2, *signal, *w, *out;
+    REAL *X, *Y, *Z, *theta, *phi1, *phi2, *signal, *pattern, *w, *out;
     int* types;
-    int i;
+    int i, t;
     if (bz < 0)
     {
         for (i = 0; i < 8 * num_dir; ++i) beam[i] = 0;
@@ -702,10 +702,13 @@ void ORC_FN(orc_station_beam_aa_weighted)(int num_el, const REAL* x,
     theta = (REAL*) malloc(sizeof(REAL) * npe);
     phi1 = (REAL*) malloc(sizeof(REAL) * npe);
     phi2 = (REAL*) malloc(sizeof(REAL) * npe);
-    signal = (REAL*) calloc((size_t) 8 * npe, sizeof(REAL));
+    signal = (REAL*) calloc((size_t) 8 * np * num_types, sizeof(REAL));
+    pattern = (REAL*) calloc((size_t) 8 * npe, sizeof(REAL));
     out = (REAL*) calloc((size_t) 8 * np, sizeof(REAL));
     w = (REAL*) malloc(sizeof(REAL) * 2 * num_el);
     types = (int*) calloc((size_t) num_el, sizeof(int));
+    if (element_type)
+        for (i = 0; i < num_el; ++i) types[i] = element_type[i];
     for (i = 0; i < num_dir; ++i)
     {
         X[i] = dx[i]; Y[i] = dy[i]; Z[i] = dz[i];
@@ -716,9 +719,19 @@ void ORC_FN(orc_station_beam_aa_weighted)(int num_el, const REAL* x,
     }
     ORC_FN(orc_enu_to_theta_phi)(0, np, X, Y, Z, norm_element,
             (REAL) dphi1, (REAL) dphi2, theta, phi1, phi2);
-    ORC_FN(orc_dipole_pattern)(npe, theta, phi1, phi2, (REAL) kL,
-            (REAL) cos(kL), swap_xy, 0, signal);
-    if (norm_element) ORC_FN(orc_mem_normalise_matrix)(0, np, signal, np);
+    /* one element pattern per type (oskar_evaluate_station_beam_aperture_
+     * array.c:158-179), each normalised at its own pole */
+    for (t = 0; t < num_types; ++t)
+    {
+        const double kL = dipole_length_per_type[t] *
+                (ORC_PI * frequency_hz / c0);
+        ORC_FN(orc_dipole_pattern)(npe, theta, phi1, phi2, (REAL) kL,
+                (REAL) cos(kL), swap_xy, 0, pattern);
+        if (norm_element)
+            ORC_FN(orc_mem_normalise_matrix)(0, np, pattern, np);
+        for (i = 0; i < 8 * np; ++i)
+            signal[(size_t) 8 * np * t + i] = pattern[i];
+    }
     ORC_FN(orc_element_weights_dft)(num_el, x_meas ? x_meas : x,
             y_meas ? y_meas : y, z_meas ? z_meas : z, cable,
             (REAL) wavenumber, (REAL) bx, (REAL) by, (REAL) bz, w);
@@ -741,7 +754,24 @@ void ORC_FN(orc_station_beam_aa_weighted)(int num_el, const REAL* x,
     if (norm_final) ORC_FN(orc_mem_normalise_matrix)(0, np, out, np - 1);
     for (i = 0; i < 8 * num_dir; ++i) beam[i] = out[i];
     free(X); free(Y); free(Z); free(theta); free(phi1); free(phi2);
-    free(signal); free(out); free(w); free(types);
+    free(signal); free(pattern); free(out); free(w); free(types);
+}
+
+void ORC_FN(orc_station_beam_aa_weighted)(int num_el, const REAL* x,
+        const REAL* y, const REAL* z, const REAL* x_meas, const REAL* y_meas,
+        const REAL* z_meas, const REAL* cable, const REAL* weight_factors,
+        double orientation_x_rad, double orientation_y_rad,
+        double dipole_length_m, int norm_element, int norm_array,
+        int norm_final, int swap_xy, int is_3d, double frequency_hz,
+        double bx, double by, double bz, double nx, double ny, double nz,
+        int num_dir, const REAL* dx, const REAL* dy, const REAL* dz,
+        REAL* beam)
+{
+    ORC_FN(orc_station_beam_aa_types)(num_el, x, y, z, x_meas, y_meas,
+            z_meas, cable, weight_factors, 1, 0, &dipole_length_m,
+            orientation_x_rad, orientation_y_rad, norm_element, norm_array,
+            norm_final, swap_xy, is_3d, frequency_hz, bx, by, bz, nx, ny, nz,
+            num_dir, dx, dy, dz, beam);
 }
 
 void ORC_FN(orc_station_beam_aa)(int num_el, const REAL* x, const REAL* y,

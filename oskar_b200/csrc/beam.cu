@@ -57,15 +57,51 @@ __device__ __forceinline__ T half_frobenius(const T p[4], T ar, T ai)
             (T) 2;
 }
 
-template <typename T, bool IS3D>
+// Up to kMaxTypes element types per station (a dipole length each).
+constexpr int kMaxTypes = 4;
+
+template <typename T>
+struct TypeParams
+{
+    T kL[kMaxTypes];      // dipole length x pi f / c
+    T cos_kL[kMaxTypes];
+};
+
+// (ar, ai)[t] += w e^{i ph} for the element's type t only: register selects
+// over a compile-time number of types, so the accumulators stay in
+// registers. One type: the plain complex multiply-add.
+template <typename T, int NT>
+__device__ __forceinline__ void add_term(T* ar, T* ai,
+        typename vec2<T>::type w, int type, T sn, T cs)
+{
+    if constexpr (NT == 1)
+    {
+        ar[0] += cs * w.x - w.y * sn;
+        ai[0] += sn * w.x + w.y * cs;
+    }
+    else
+    {
+#pragma unroll
+        for (int t = 0; t < NT; ++t)
+        {
+            const T wx = type == t ? w.x : (T) 0;
+            const T wy = type == t ? w.y : (T) 0;
+            ar[t] += cs * wx - wy * sn;
+            ai[t] += sn * wx + wy * cs;
+        }
+    }
+}
+
+template <typename T, bool IS3D, int NT>
 __global__ void __launch_bounds__(kThreads)
 station_beam_kernel(int num_elements, const T* __restrict__ el_x,
         const T* __restrict__ el_y, const T* __restrict__ el_z,
         const T* __restrict__ meas_x, const T* __restrict__ meas_y,
         const T* __restrict__ meas_z, const T* __restrict__ cable,
         const T* __restrict__ weight_factors,
+        const int* __restrict__ element_type,
         const double* __restrict__ orientation_x,
-        const double* __restrict__ orientation_y, T kL, T cos_kL,
+        const double* __restrict__ orientation_y, TypeParams<T> tp,
         BeamFlags flags, T wavenumber, const double* __restrict__ beam_enu,
         const double* __restrict__ norm_enu, int num_dir,
         const T* __restrict__ dir_x, const T* __restrict__ dir_y,
@@ -75,7 +111,8 @@ station_beam_kernel(int num_elements, const T* __restrict__ el_x,
     typedef typename vec2<T>::type T2;
     __shared__ T2 s_w[kChunk];
     __shared__ T s_x[kChunk], s_y[kChunk], s_z[IS3D ? kChunk : 1];
-    __shared__ T s_red[2][kThreads / 32];
+    __shared__ int s_type[NT > 1 ? kChunk : 1];
+    __shared__ T s_red[2][NT][kThreads / 32];
     // FP64: phase factors of the element loops from the shared table
     __shared__ double2 s_trig[sizeof(T) == 8 ? kTrigTableSize : 1];
     const int st = blockIdx.y;
@@ -123,8 +160,11 @@ station_beam_kernel(int num_elements, const T* __restrict__ el_x,
     const T knX = wavenumber * nX * to_steps, knY = wavenumber * nY * to_steps,
             knZ = wavenumber * nZ * to_steps;
 
-    T ar = 0, ai = 0;    // array factor, this thread's direction
-    T nr = 0, ni = 0;    // array factor of the normalisation direction
+    // array factors per element type: this thread's direction (ar, ai) and
+    // the normalisation direction (nr, ni)
+    T ar[NT], ai[NT], nr[NT], ni[NT];
+#pragma unroll
+    for (int t = 0; t < NT; ++t) ar[t] = ai[t] = nr[t] = ni[t] = (T) 0;
     for (int e0 = 0; e0 < num_elements; e0 += kChunk)
     {
         const int ne = min(kChunk, num_elements - e0);
@@ -147,6 +187,12 @@ station_beam_kernel(int num_elements, const T* __restrict__ el_x,
                 cs = re;
             }
             s_w[t] = T2{cs, sn};
+            int type = 0;
+            if constexpr (NT > 1)
+            {
+                type = element_type ? element_type[g] : 0;
+                s_type[t] = type;
+            }
             s_x[t] = el_x[g];
             s_y[t] = el_y[g];
             if (IS3D) s_z[t] = el_z[g];
@@ -157,8 +203,7 @@ station_beam_kernel(int num_elements, const T* __restrict__ el_x,
                 if (IS3D) ph += knZ * s_z[t];
                 T s2, c2;
                 phase_factor(s_trig, ph, &s2, &c2);
-                nr += c2 * cs - sn * s2;
-                ni += s2 * cs + sn * c2;
+                add_term<T, NT>(nr, ni, T2{cs, sn}, type, s2, c2);
             }
         }
         __syncthreads();
@@ -168,7 +213,13 @@ station_beam_kernel(int num_elements, const T* __restrict__ el_x,
             {
                 // Branch-free table loop; a thread that met a phase the
                 // table does not cover redoes the chunk with sincos.
-                const T ar0 = ar, ai0 = ai;
+                T ar0[NT], ai0[NT];
+#pragma unroll
+                for (int t = 0; t < NT; ++t)
+                {
+                    ar0[t] = ar[t];
+                    ai0[t] = ai[t];
+                }
                 bool covered = true;
 #pragma unroll 4
                 for (int i = 0; i < ne; ++i)
@@ -177,23 +228,25 @@ station_beam_kernel(int num_elements, const T* __restrict__ el_x,
                     if (IS3D) ph += kZ * s_z[i];
                     T sn, cs;
                     trig_steps_sincos(s_trig, ph, &sn, &cs, covered);
-                    const T2 w = s_w[i];
-                    ar += cs * w.x - w.y * sn;
-                    ai += sn * w.x + w.y * cs;
+                    add_term<T, NT>(ar, ai, s_w[i], NT > 1 ? s_type[i] : 0,
+                            sn, cs);
                 }
                 if (!covered)
                 {
-                    ar = ar0;
-                    ai = ai0;
+#pragma unroll
+                    for (int t = 0; t < NT; ++t)
+                    {
+                        ar[t] = ar0[t];
+                        ai[t] = ai0[t];
+                    }
                     for (int i = 0; i < ne; ++i)
                     {
                         T ph = kX * s_x[i] + kY * s_y[i];
                         if (IS3D) ph += kZ * s_z[i];
                         T sn, cs;
                         trig_steps_exact(ph, &sn, &cs);
-                        const T2 w = s_w[i];
-                        ar += cs * w.x - w.y * sn;
-                        ai += sn * w.x + w.y * cs;
+                        add_term<T, NT>(ar, ai, s_w[i],
+                                NT > 1 ? s_type[i] : 0, sn, cs);
                     }
                 }
             }
@@ -206,70 +259,116 @@ station_beam_kernel(int num_elements, const T* __restrict__ el_x,
                     if (IS3D) ph += kZ * s_z[i];
                     T sn, cs;
                     sincosf(ph, &sn, &cs);
-                    const T2 w = s_w[i];
-                    ar += cs * w.x - w.y * sn;
-                    ai += sn * w.x + w.y * cs;
+                    add_term<T, NT>(ar, ai, s_w[i], NT > 1 ? s_type[i] : 0,
+                            sn, cs);
                 }
             }
         }
         __syncthreads();
     }
 
-    // Element normalisation: 1 / |pattern at the pole|.
-    T pole_scale = (T) 1;
-    if (flags.normalise_element)
+    // Element normalisation: 1 / |pattern at the pole|, per type.
+    T pole_scale[NT];
+#pragma unroll
+    for (int t = 0; t < NT; ++t)
     {
-        T pp[4];
-        element_pattern<T>(0, 0, 1, true, dphi1, dphi2, kL, cos_kL,
-                flags.swap_xy, pp);
-        pole_scale = (T) 1 / sqrt(half_frobenius<T>(pp, 1, 0));
+        pole_scale[t] = (T) 1;
+        if (flags.normalise_element)
+        {
+            T pp[4];
+            element_pattern<T>(0, 0, 1, true, dphi1, dphi2, tp.kL[t],
+                    tp.cos_kL[t], flags.swap_xy, pp);
+            pole_scale[t] = (T) 1 / sqrt(half_frobenius<T>(pp, 1, 0));
+        }
     }
     const T array_scale = flags.normalise_array ?
             (T) (1.0 / num_elements) : (T) 1;
 
     // Final normalisation: amplitude of the beam in the normalisation
-    // direction (block reduction of its array factor first).
+    // direction (block reduction of its array factors first).
     T final_scale = (T) 1;
     if (flags.normalise_final)
     {
-        for (int o = 16; o > 0; o >>= 1)
+#pragma unroll
+        for (int t = 0; t < NT; ++t)
         {
-            nr += __shfl_xor_sync(0xffffffffu, nr, o);
-            ni += __shfl_xor_sync(0xffffffffu, ni, o);
-        }
-        if ((threadIdx.x & 31) == 0)
-        {
-            s_red[0][threadIdx.x >> 5] = nr;
-            s_red[1][threadIdx.x >> 5] = ni;
+            for (int o = 16; o > 0; o >>= 1)
+            {
+                nr[t] += __shfl_xor_sync(0xffffffffu, nr[t], o);
+                ni[t] += __shfl_xor_sync(0xffffffffu, ni[t], o);
+            }
+            if ((threadIdx.x & 31) == 0)
+            {
+                s_red[0][t][threadIdx.x >> 5] = nr[t];
+                s_red[1][t][threadIdx.x >> 5] = ni[t];
+            }
         }
         __syncthreads();
-        nr = ni = 0;
-        for (int w = 0; w < kThreads / 32; ++w)
+#pragma unroll
+        for (int t = 0; t < NT; ++t)
         {
-            nr += s_red[0][w];
-            ni += s_red[1][w];
+            nr[t] = ni[t] = 0;
+            for (int w = 0; w < kThreads / 32; ++w)
+            {
+                nr[t] += s_red[0][t][w];
+                ni[t] += s_red[1][t][w];
+            }
+            // A normalisation direction below the horizon is blanked, as in
+            // the reference, which then divides by zero.
+            if (nZ < (T) 0) nr[t] = ni[t] = (T) 0;
         }
-        T pn[4];
-        element_pattern<T>(nX, nY, nZ, false, dphi1, dphi2, kL, cos_kL,
-                flags.swap_xy, pn);
-        for (int k = 0; k < 4; ++k) pn[k] *= pole_scale * array_scale;
-        // A normalisation direction below the horizon is blanked, as in the
-        // reference, which then divides by zero.
-        if (nZ < (T) 0) nr = ni = (T) 0;
-        final_scale = (T) 1 / sqrt(half_frobenius<T>(pn, nr, ni));
+        if constexpr (NT == 1)
+        {
+            T pn[4];
+            element_pattern<T>(nX, nY, nZ, false, dphi1, dphi2, tp.kL[0],
+                    tp.cos_kL[0], flags.swap_xy, pn);
+            for (int k = 0; k < 4; ++k) pn[k] *= pole_scale[0] * array_scale;
+            final_scale = (T) 1 / sqrt(half_frobenius<T>(pn, nr[0], ni[0]));
+        }
+        else
+        {
+            // |sum_t pattern_t AF_t|_F^2 / 2 over the four polarisations
+            T pn[NT][4];
+#pragma unroll
+            for (int t = 0; t < NT; ++t)
+                element_pattern<T>(nX, nY, nZ, false, dphi1, dphi2,
+                        tp.kL[t], tp.cos_kL[t], flags.swap_xy, pn[t]);
+            T amp = 0;
+            for (int k = 0; k < 4; ++k)
+            {
+                T vr = 0, vi = 0;
+#pragma unroll
+                for (int t = 0; t < NT; ++t)
+                {
+                    const T pk = pn[t][k] * pole_scale[t] * array_scale;
+                    vr += pk * nr[t];
+                    vi += pk * ni[t];
+                }
+                amp += vr * vr + vi * vi;
+            }
+            final_scale = (T) 1 / sqrt(amp / (T) 2);
+        }
     }
     if (!active) return;
 
-    T p[4];
-    element_pattern<T>(X, Y, Z, false, dphi1, dphi2, kL, cos_kL,
-            flags.swap_xy, p);
     const bool blank = Z < (T) 0;
+    T p[NT][4];
+#pragma unroll
+    for (int t = 0; t < NT; ++t)
+        element_pattern<T>(X, Y, Z, false, dphi1, dphi2, tp.kL[t],
+                tp.cos_kL[t], flags.swap_xy, p[t]);
     for (int k = 0; k < 4; ++k)
     {
         // The reference's order: pattern (normalised), times the weighted
         // element sum, times the DFT norm, then the final scale.
-        const T pk = p[k] * pole_scale;
-        T2 v{pk * ar * array_scale, pk * ai * array_scale};
+        T2 v{(T) 0, (T) 0};
+#pragma unroll
+        for (int t = 0; t < NT; ++t)
+        {
+            const T pk = p[t][k] * pole_scale[t];
+            v.x += pk * ar[t] * array_scale;
+            v.y += pk * ai[t] * array_scale;
+        }
         if (blank) v = T2{(T) 0, (T) 0};
         v.x *= final_scale;
         v.y *= final_scale;
@@ -313,8 +412,9 @@ template <typename T>
 int station_beam_aa(int num_stations, int num_elements, const T* el_x,
         const T* el_y, const T* el_z, const T* meas_x, const T* meas_y,
         const T* meas_z, const T* cable, const T* weight_factors,
+        int num_element_types, const int* element_type,
         const double* orientation_x,
-        const double* orientation_y, double dipole_length_m,
+        const double* orientation_y, const double* dipole_length_m,
         int normalise_element, int normalise_array, int normalise_final,
         int swap_xy, int is_3d, double frequency_hz, const double* beam_enu,
         const double* norm_enu, int num_directions, const T* x, const T* y,
@@ -328,20 +428,38 @@ int station_beam_aa(int num_stations, int num_elements, const T* el_x,
             (normalise_final && !norm_enu) || !x || !y || !z || !beam)
         return OSKB_ERR_INVALID_ARGUMENT;
     if (num_stations > 65535) return OSKB_ERR_INVALID_ARGUMENT;
+    if (num_element_types < 1 || !dipole_length_m)
+        return OSKB_ERR_INVALID_ARGUMENT;
+    if (num_element_types > kMaxTypes) return OSKB_ERR_OUT_OF_RANGE;
     const double c0 = 299792458.0;
-    const double kL = dipole_length_m * (kPi * frequency_hz / c0);
+    TypeParams<T> tp;
+    for (int t = 0; t < kMaxTypes; ++t)
+    {
+        const double kL = t < num_element_types ?
+                dipole_length_m[t] * (kPi * frequency_hz / c0) : 0.0;
+        tp.kL[t] = (T) kL;
+        tp.cos_kL[t] = (T) cos(kL);
+    }
     const T wavenumber = (T) (2.0 * kPi * frequency_hz / c0);
     BeamFlags flags{normalise_element, normalise_array, normalise_final,
             swap_xy};
     dim3 grid((num_directions + kThreads - 1) / kThreads, num_stations);
     cudaStream_t s = as_stream(stream);
-#define OSKB_BEAM(D) station_beam_kernel<T, D><<<grid, kThreads, 0, s>>>(     \
-        num_elements, el_x, el_y, el_z, meas_x, meas_y, meas_z, cable,       \
-        weight_factors, orientation_x, orientation_y, (T) kL, (T) cos(kL),   \
-        flags,                                                               \
-        wavenumber, beam_enu, norm_enu, num_directions, x, y, z,             \
+#define OSKB_BEAM(D, NT) station_beam_kernel<T, D, NT><<<grid, kThreads, 0,    \
+        s>>>(num_elements, el_x, el_y, el_z, meas_x, meas_y, meas_z, cable,  \
+        weight_factors, element_type, orientation_x, orientation_y, tp,      \
+        flags, wavenumber, beam_enu, norm_enu, num_directions, x, y, z,      \
         directions_per_station, beam)
-    if (is_3d) OSKB_BEAM(true); else OSKB_BEAM(false);
+#define OSKB_BEAM_NT(D)                                                      \
+    switch (num_element_types)                                               \
+    {                                                                        \
+    case 1: OSKB_BEAM(D, 1); break;                                          \
+    case 2: OSKB_BEAM(D, 2); break;                                          \
+    case 3: OSKB_BEAM(D, 3); break;                                          \
+    default: OSKB_BEAM(D, 4); break;                                         \
+    }
+    if (is_3d) { OSKB_BEAM_NT(true) } else { OSKB_BEAM_NT(false) }
+#undef OSKB_BEAM_NT
 #undef OSKB_BEAM
     return check_launch("station_beam_aa");
 }
@@ -378,8 +496,8 @@ int oskb_station_beam_aa_##S(int num_stations, int num_elements,             \
         T* beam, void* stream)                                               \
 {                                                                            \
     return oskb::station_beam_aa<T>(num_stations, num_elements, el_x, el_y,  \
-            el_z, meas_x, meas_y, meas_z, cable_length_error, nullptr,       \
-            orientation_x_rad, orientation_y_rad, dipole_length_m,           \
+            el_z, meas_x, meas_y, meas_z, cable_length_error, nullptr, 1,    \
+            nullptr, orientation_x_rad, orientation_y_rad, &dipole_length_m, \
             normalise_element, normalise_array, normalise_final, swap_xy,    \
             is_3d, frequency_hz, beam_enu, norm_enu, num_directions, x, y,   \
             z, directions_per_station, beam, stream);                        \
@@ -397,11 +515,31 @@ int oskb_station_beam_aa_weighted_##S(int num_stations, int num_elements,    \
 {                                                                            \
     return oskb::station_beam_aa<T>(num_stations, num_elements, el_x, el_y,  \
             el_z, meas_x, meas_y, meas_z, cable_length_error,                \
-            element_weight_factors, orientation_x_rad, orientation_y_rad,    \
-            dipole_length_m, normalise_element, normalise_array,             \
-            normalise_final, swap_xy, is_3d, frequency_hz, beam_enu,         \
-            norm_enu, num_directions, x, y, z, directions_per_station, beam, \
-            stream);                                                         \
+            element_weight_factors, 1, nullptr, orientation_x_rad,           \
+            orientation_y_rad, &dipole_length_m, normalise_element,          \
+            normalise_array, normalise_final, swap_xy, is_3d, frequency_hz,  \
+            beam_enu, norm_enu, num_directions, x, y, z,                     \
+            directions_per_station, beam, stream);                           \
+}                                                                            \
+int oskb_station_beam_aa_types_##S(int num_stations, int num_elements,       \
+        const T* el_x, const T* el_y, const T* el_z, const T* meas_x,        \
+        const T* meas_y, const T* meas_z, const T* cable_length_error,       \
+        const T* element_weight_factors, int num_element_types,              \
+        const int* element_type, const double* dipole_length_m,              \
+        const double* orientation_x_rad, const double* orientation_y_rad,    \
+        int normalise_element, int normalise_array, int normalise_final,     \
+        int swap_xy, int is_3d, double frequency_hz,                         \
+        const double* beam_enu, const double* norm_enu, int num_directions,  \
+        const T* x, const T* y, const T* z, int directions_per_station,      \
+        T* beam, void* stream)                                               \
+{                                                                            \
+    return oskb::station_beam_aa<T>(num_stations, num_elements, el_x, el_y,  \
+            el_z, meas_x, meas_y, meas_z, cable_length_error,                \
+            element_weight_factors, num_element_types, element_type,         \
+            orientation_x_rad, orientation_y_rad, dipole_length_m,           \
+            normalise_element, normalise_array, normalise_final, swap_xy,    \
+            is_3d, frequency_hz, beam_enu, norm_enu, num_directions, x, y,   \
+            z, directions_per_station, beam, stream);                        \
 }                                                                            \
 int oskb_evaluate_jones_R_##S(int num_sources, const T* ra_rad,              \
         const T* dec_rad, int num_stations, const double* lat_rad,           \
@@ -496,9 +634,9 @@ int station_beam_two_level(int num_tile_types, int num_elements,
     // tile beams [type][direction]: element pattern x tile array factor,
     // blanked below the horizon, no final normalisation
     if (int err = station_beam_aa<T>(num_tile_types, num_elements, el_x,
-            el_y, el_z, nullptr, nullptr, nullptr, nullptr, nullptr,
-            orientation_x,
-            orientation_y, dipole_length_m, normalise_element,
+            el_y, el_z, nullptr, nullptr, nullptr, nullptr, nullptr, 1,
+            nullptr, orientation_x, orientation_y, &dipole_length_m,
+            normalise_element,
             normalise_tile_array, 0, swap_xy, is_3d, frequency_hz, pointing,
             nullptr, num_directions, x, y, z, 0, tile_beams, stream))
         return err;

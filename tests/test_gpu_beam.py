@@ -121,3 +121,63 @@ def test_jones_r_vs_oracle(real):
                       real(np.cos(lat[s])), real(np.sin(lat[s])),
                       real(lst[s]), 0, ref)
         assert rel(got[s], ref) <= (1e-13 if real == np.float64 else 2e-5)
+
+
+@pytest.mark.parametrize("real", [np.float64, np.float32])
+@pytest.mark.parametrize("num_types", [1, 2, 3, 4])
+@pytest.mark.parametrize("flags", [(1, 1, 1, 0, 1), (0, 0, 1, 1, 0)])
+def test_station_beam_element_types(real, num_types, flags):
+    """Stations with several element types of common orientation (a dipole
+    length each): one launch for three stations, each with its own type
+    map and weight factors, against the oracle composed as the reference
+    does it (a pattern per type, then the weighted DFT with data index =
+    element type; oskar_evaluate_station_beam_aperture_array.c:158-179)."""
+    norm_el, norm_arr, norm_fin, swap, is_3d = flags
+    cases = stations(real, is_3d=is_3d, num_el=200, num_dir=613)
+    nst, n, nd = len(cases), 200, 613
+    rng = np.random.default_rng(num_types)
+    types = rng.integers(0, num_types, (nst, n)).astype(np.int32)
+    lengths = np.array([1.5, 1.1, 2.0, 0.7][:num_types])
+    wf = rng.normal(1, 0.1, (nst, 2 * n)).astype(real)
+    cat = lambda key, i: dev(np.concatenate([c[key][i] for c in cases]))
+    out = torch.zeros(nst * nd * 8, dtype=torch.float64 if real ==
+                      np.float64 else torch.float32, device="cuda")
+    ob.call("oskb_station_beam_aa_types_" + suffix(real), nst, n,
+            *[cat("el", i) for i in range(3)],
+            *[cat("meas", i) for i in range(3)],
+            dev(np.concatenate([c["cable"] for c in cases])), dev(wf),
+            num_types, dev(types), lengths,
+            dev(np.array([c["orient"][0] for c in cases])),
+            dev(np.array([c["orient"][1] for c in cases])), norm_el,
+            norm_arr, norm_fin, swap, is_3d, cases[0]["freq"],
+            dev(np.stack([c["b"] for c in cases])),
+            dev(np.stack([c["norm"] for c in cases])), nd,
+            *[dev(cases[0]["dirs"][i]) for i in range(3)], 0, out,
+            ob.stream_ptr())
+    torch.cuda.synchronize()
+    got = out.cpu().numpy().reshape(nst, -1)
+    for s, c in enumerate(cases):
+        ref = np.zeros(8 * nd, real)
+        oracle().call("station_beam_aa_types_" + suffix(real), np.float64,
+                      n, *c["el"], *c["meas"], c["cable"], wf[s].copy(),
+                      num_types, types[s].copy(), lengths, *c["orient"],
+                      norm_el, norm_arr, norm_fin, swap, is_3d, c["freq"],
+                      *c["b"], *c["norm"], nd, *cases[0]["dirs"], ref)
+        assert rel(got[s], ref) <= TOL[real], (s, rel(got[s], ref))
+
+
+def test_station_beam_element_types_limits():
+    c = beam_case(np.float64, num_el=8, num_dir=5)
+    args = lambda nt, lengths: (
+        1, 8, *[dev(a) for a in c["el"]], None, None, None, None, None, nt,
+        None, lengths, dev(np.array([0.0])), dev(np.array([1.5])), 0, 0, 0,
+        0, 1, 100e6, dev(c["b"]), dev(c["norm"]), 5,
+        *[dev(a) for a in c["dirs"]], 0,
+        torch.zeros(40, dtype=torch.float64, device="cuda"), None)
+    five = np.ones(5)
+    assert ob.call("oskb_station_beam_aa_types_d", *args(5, five),
+                   check=False) == -5  # OSKB_ERR_OUT_OF_RANGE
+    assert ob.call("oskb_station_beam_aa_types_d", *args(0, five),
+                   check=False) == -3
+    assert ob.call("oskb_station_beam_aa_types_d", *args(1, None),
+                   check=False) == -3
