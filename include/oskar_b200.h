@@ -293,14 +293,17 @@ OSKB_API int oskb_station_beam_aa_weighted_f(int num_stations,
         const float* x, const float* y, const float* z,
         int directions_per_station, float* beam, void* stream);
 
-/* oskb_station_beam_aa_weighted for stations with up to 4 element types of
- * common orientation (the reference's common-orientation branch,
- * oskar_evaluate_station_beam_aperture_array.c:158-179 and its oskar_dftw
+/* oskb_station_beam_aa_weighted for stations with up to 4 element types
+ * (oskar_evaluate_station_beam_aperture_array.c:158-202 and its oskar_dftw
  * with data index = element type): element e has type
- * element_type[station][e] (device; NULL: all type 0), type t is a dipole
- * of length dipole_length_m[t] (host array of num_element_types) with its
- * own pole normalisation; beam = sum over types of the type's pattern
- * times the array factor of its elements. An element whose type is outside
+ * element_type[station][e] (device; NULL: all type 0); type t is a dipole
+ * of length dipole_length_m[t] (host array of num_element_types) with
+ * Euler angles orientation_{x,y}_rad[station][t] (device) and its own pole
+ * normalisation; beam = sum over types of the type's pattern times the
+ * array factor of its elements. A station whose elements differ in
+ * orientation (the reference's per-element branch, :180-202) maps onto
+ * this when its distinct (element model, orientation) pairs number at most
+ * four: one type per pair. An element whose type is outside
  * [0, num_element_types) adds nothing (the reference stops with
  * OSKAR_ERR_OUT_OF_RANGE). num_element_types > 4: OSKB_ERR_OUT_OF_RANGE. */
 OSKB_API int oskb_station_beam_aa_types_d(int num_stations, int num_elements,

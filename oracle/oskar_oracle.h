@@ -87,8 +87,9 @@ void orc_station_beam_aa_types_##S(int num_el, const REAL* x, \
         const REAL* y, const REAL* z, const REAL* x_meas, \
         const REAL* y_meas, const REAL* z_meas, const REAL* cable, \
         const REAL* weight_factors, int num_types, const int* element_type, \
-        const double* dipole_length_per_type, double orientation_x_rad, \
-        double orientation_y_rad, int norm_element, \
+        const double* dipole_length_per_type, \
+        const double* orientation_x_per_type, \
+        const double* orientation_y_per_type, int norm_element, \
         int norm_array, int norm_final, int swap_xy, int is_3d, \
         double frequency_hz, double bx, double by, double bz, double nx, \
         double ny, double nz, int num_dir, const REAL* dx, const REAL* dy, \

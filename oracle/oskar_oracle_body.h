@@ -675,8 +675,9 @@ void ORC_FN(orc_station_beam_aa_types)(int num_el, const REAL* x,
         const REAL* y, const REAL* z, const REAL* x_meas, const REAL* y_meas,
         const REAL* z_meas, const REAL* cable, const REAL* weight_factors,
         int num_types, const int* element_type,
-        const double* dipole_length_per_type, double orientation_x_rad,
-        double orientation_y_rad, int norm_element,
+        const double* dipole_length_per_type,
+        const double* orientation_x_per_type,
+        const double* orientation_y_per_type, int norm_element,
         int norm_array, int norm_final, int swap_xy, int is_3d,
         double frequency_hz, double bx, double by, double bz, double nx,
         double ny, double nz, int num_dir, const REAL* dx, const REAL* dy,
@@ -686,8 +687,6 @@ void ORC_FN(orc_station_beam_aa_types)(int num_el, const REAL* x,
     const int np = num_dir + (norm_final ? 1 : 0);
     const int npe = np + (norm_element ? 1 : 0);
     const double wavenumber = 2.0 * ORC_PI * frequency_hz / c0;
-    const double dphi1 = ORC_PI / 2 - (orientation_x_rad + ORC_PI / 2);
-    const double dphi2 = ORC_PI / 2 - orientation_y_rad;
     REAL *X, *Y, *Z, *theta, *phi1, *phi2, *signal, *pattern, *w, *out;
     int* types;
     int i, t;
@@ -717,14 +716,19 @@ void ORC_FN(orc_station_beam_aa_types)(int num_el, const REAL* x,
     {
         X[num_dir] = (REAL) nx; Y[num_dir] = (REAL) ny; Z[num_dir] = (REAL) nz;
     }
-    ORC_FN(orc_enu_to_theta_phi)(0, np, X, Y, Z, norm_element,
-            (REAL) dphi1, (REAL) dphi2, theta, phi1, phi2);
     /* one element pattern per type (oskar_evaluate_station_beam_aperture_
-     * array.c:158-179), each normalised at its own pole */
+     * array.c:158-202: per element type, or per element when orientations
+     * differ), each with its own orientation and normalised at its own
+     * pole */
     for (t = 0; t < num_types; ++t)
     {
         const double kL = dipole_length_per_type[t] *
                 (ORC_PI * frequency_hz / c0);
+        const double dphi1 =
+                ORC_PI / 2 - (orientation_x_per_type[t] + ORC_PI / 2);
+        const double dphi2 = ORC_PI / 2 - orientation_y_per_type[t];
+        ORC_FN(orc_enu_to_theta_phi)(0, np, X, Y, Z, norm_element,
+                (REAL) dphi1, (REAL) dphi2, theta, phi1, phi2);
         ORC_FN(orc_dipole_pattern)(npe, theta, phi1, phi2, (REAL) kL,
                 (REAL) cos(kL), swap_xy, 0, pattern);
         if (norm_element)
@@ -769,7 +773,7 @@ void ORC_FN(orc_station_beam_aa_weighted)(int num_el, const REAL* x,
 {
     ORC_FN(orc_station_beam_aa_types)(num_el, x, y, z, x_meas, y_meas,
             z_meas, cable, weight_factors, 1, 0, &dipole_length_m,
-            orientation_x_rad, orientation_y_rad, norm_element, norm_array,
+            &orientation_x_rad, &orientation_y_rad, norm_element, norm_array,
             norm_final, swap_xy, is_3d, frequency_hz, bx, by, bz, nx, ny, nz,
             num_dir, dx, dy, dz, beam);
 }

@@ -135,8 +135,14 @@ station_beam_kernel(int num_elements, const T* __restrict__ el_x,
         trig_table_fill(s_trig);
         __syncthreads();
     }
-    const T dphi1 = (T) (kPi / 2 - (orientation_x[st] + kPi / 2));
-    const T dphi2 = (T) (kPi / 2 - orientation_y[st]);
+    // element orientations per (station, type)
+    T dphi1[NT], dphi2[NT];
+#pragma unroll
+    for (int t = 0; t < NT; ++t)
+    {
+        dphi1[t] = (T) (kPi / 2 - (orientation_x[st * NT + t] + kPi / 2));
+        dphi2[t] = (T) (kPi / 2 - orientation_y[st * NT + t]);
+    }
 
     T X = 0, Y = 0, Z = 0;
     if (active)
@@ -276,7 +282,7 @@ station_beam_kernel(int num_elements, const T* __restrict__ el_x,
         if (flags.normalise_element)
         {
             T pp[4];
-            element_pattern<T>(0, 0, 1, true, dphi1, dphi2, tp.kL[t],
+            element_pattern<T>(0, 0, 1, true, dphi1[t], dphi2[t], tp.kL[t],
                     tp.cos_kL[t], flags.swap_xy, pp);
             pole_scale[t] = (T) 1 / sqrt(half_frobenius<T>(pp, 1, 0));
         }
@@ -320,7 +326,8 @@ station_beam_kernel(int num_elements, const T* __restrict__ el_x,
         if constexpr (NT == 1)
         {
             T pn[4];
-            element_pattern<T>(nX, nY, nZ, false, dphi1, dphi2, tp.kL[0],
+            element_pattern<T>(nX, nY, nZ, false, dphi1[0], dphi2[0],
+                    tp.kL[0],
                     tp.cos_kL[0], flags.swap_xy, pn);
             for (int k = 0; k < 4; ++k) pn[k] *= pole_scale[0] * array_scale;
             final_scale = (T) 1 / sqrt(half_frobenius<T>(pn, nr[0], ni[0]));
@@ -331,7 +338,7 @@ station_beam_kernel(int num_elements, const T* __restrict__ el_x,
             T pn[NT][4];
 #pragma unroll
             for (int t = 0; t < NT; ++t)
-                element_pattern<T>(nX, nY, nZ, false, dphi1, dphi2,
+                element_pattern<T>(nX, nY, nZ, false, dphi1[t], dphi2[t],
                         tp.kL[t], tp.cos_kL[t], flags.swap_xy, pn[t]);
             T amp = 0;
             for (int k = 0; k < 4; ++k)
@@ -355,7 +362,7 @@ station_beam_kernel(int num_elements, const T* __restrict__ el_x,
     T p[NT][4];
 #pragma unroll
     for (int t = 0; t < NT; ++t)
-        element_pattern<T>(X, Y, Z, false, dphi1, dphi2, tp.kL[t],
+        element_pattern<T>(X, Y, Z, false, dphi1[t], dphi2[t], tp.kL[t],
                 tp.cos_kL[t], flags.swap_xy, p[t]);
     for (int k = 0; k < 4; ++k)
     {

@@ -127,11 +127,12 @@ def test_jones_r_vs_oracle(real):
 @pytest.mark.parametrize("num_types", [1, 2, 3, 4])
 @pytest.mark.parametrize("flags", [(1, 1, 1, 0, 1), (0, 0, 1, 1, 0)])
 def test_station_beam_element_types(real, num_types, flags):
-    """Stations with several element types of common orientation (a dipole
-    length each): one launch for three stations, each with its own type
-    map and weight factors, against the oracle composed as the reference
-    does it (a pattern per type, then the weighted DFT with data index =
-    element type; oskar_evaluate_station_beam_aperture_array.c:158-179)."""
+    """Stations with several element types, each a dipole length and an
+    orientation of its own: one launch for three stations, each with its
+    own type map, orientations and weight factors, against the oracle
+    composed as the reference does it (a pattern per type, then the
+    weighted DFT with data index = element type;
+    oskar_evaluate_station_beam_aperture_array.c:158-202)."""
     norm_el, norm_arr, norm_fin, swap, is_3d = flags
     cases = stations(real, is_3d=is_3d, num_el=200, num_dir=613)
     nst, n, nd = len(cases), 200, 613
@@ -139,6 +140,8 @@ def test_station_beam_element_types(real, num_types, flags):
     types = rng.integers(0, num_types, (nst, n)).astype(np.int32)
     lengths = np.array([1.5, 1.1, 2.0, 0.7][:num_types])
     wf = rng.normal(1, 0.1, (nst, 2 * n)).astype(real)
+    ori_x = rng.uniform(0, np.pi, (nst, num_types))
+    ori_y = ori_x + np.pi / 2 + rng.normal(0, 0.05, (nst, num_types))
     cat = lambda key, i: dev(np.concatenate([c[key][i] for c in cases]))
     out = torch.zeros(nst * nd * 8, dtype=torch.float64 if real ==
                       np.float64 else torch.float32, device="cuda")
@@ -146,9 +149,7 @@ def test_station_beam_element_types(real, num_types, flags):
             *[cat("el", i) for i in range(3)],
             *[cat("meas", i) for i in range(3)],
             dev(np.concatenate([c["cable"] for c in cases])), dev(wf),
-            num_types, dev(types), lengths,
-            dev(np.array([c["orient"][0] for c in cases])),
-            dev(np.array([c["orient"][1] for c in cases])), norm_el,
+            num_types, dev(types), lengths, dev(ori_x), dev(ori_y), norm_el,
             norm_arr, norm_fin, swap, is_3d, cases[0]["freq"],
             dev(np.stack([c["b"] for c in cases])),
             dev(np.stack([c["norm"] for c in cases])), nd,
@@ -160,8 +161,9 @@ def test_station_beam_element_types(real, num_types, flags):
         ref = np.zeros(8 * nd, real)
         oracle().call("station_beam_aa_types_" + suffix(real), np.float64,
                       n, *c["el"], *c["meas"], c["cable"], wf[s].copy(),
-                      num_types, types[s].copy(), lengths, *c["orient"],
-                      norm_el, norm_arr, norm_fin, swap, is_3d, c["freq"],
+                      num_types, types[s].copy(), lengths,
+                      ori_x[s].copy(), ori_y[s].copy(), norm_el, norm_arr,
+                      norm_fin, swap, is_3d, c["freq"],
                       *c["b"], *c["norm"], nd, *cases[0]["dirs"], ref)
         assert rel(got[s], ref) <= TOL[real], (s, rel(got[s], ref))
 
