@@ -331,6 +331,40 @@ OSKB_API int oskb_station_beam_aa_types_f(int num_stations, int num_elements,
         const float* y, const float* z, int directions_per_station,
         float* beam, void* stream);
 
+/* oskb_station_beam_aa_types for stations whose two feeds have element
+ * data of their own (the reference's num_feeds = 2 when a station is not
+ * common_pol_beams: per-feed positions, cable errors, gains, errors or
+ * apodisation; oskar_evaluate_station_beam_aperture_array.c:208-223).
+ * el_*, meas_*, cable_length_error: [feed][station][element];
+ * element_weight_factors: [feed][station][element] complex (NULL: none);
+ * the x feed's array factor forms the (xx, xy) row, the y feed's the
+ * (yx, yy) row; the final normalisation uses both. num_feeds = 1 is
+ * oskb_station_beam_aa_types. */
+OSKB_API int oskb_station_beam_aa_feeds_d(int num_feeds, int num_stations,
+        int num_elements, const double* el_x, const double* el_y,
+        const double* el_z, const double* meas_x, const double* meas_y,
+        const double* meas_z, const double* cable_length_error,
+        const double* element_weight_factors, int num_element_types,
+        const int* element_type, const double* dipole_length_m,
+        const double* orientation_x_rad, const double* orientation_y_rad,
+        int normalise_element, int normalise_array, int normalise_final,
+        int swap_xy, int is_3d, double frequency_hz, const double* beam_enu,
+        const double* norm_enu, int num_directions, const double* x,
+        const double* y, const double* z, int directions_per_station,
+        double* beam, void* stream);
+OSKB_API int oskb_station_beam_aa_feeds_f(int num_feeds, int num_stations,
+        int num_elements, const float* el_x, const float* el_y,
+        const float* el_z, const float* meas_x, const float* meas_y,
+        const float* meas_z, const float* cable_length_error,
+        const float* element_weight_factors, int num_element_types,
+        const int* element_type, const double* dipole_length_m,
+        const double* orientation_x_rad, const double* orientation_y_rad,
+        int normalise_element, int normalise_array, int normalise_final,
+        int swap_xy, int is_3d, double frequency_hz, const double* beam_enu,
+        const double* norm_enu, int num_directions, const float* x,
+        const float* y, const float* z, int directions_per_station,
+        float* beam, void* stream);
+
 /* Time-variable element gain and phase errors of one station:
  * errors[e] = (gain[e] + gain_error[e] g) exp(i (phase[e] + phase_error[e] h))
  * with (g, h) a standard Gaussian pair per element drawn from Philox4x32-10

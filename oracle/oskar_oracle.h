@@ -83,7 +83,8 @@ void orc_blank_below_horizon_##S(int off_mask, int n, const REAL* mask, \
 void orc_jones_r_##S(int num_sources, const REAL* ra, const REAL* dec, \
         REAL cos_lat, REAL sin_lat, REAL lst_rad, int offset_out, \
         REAL* jones); \
-void orc_station_beam_aa_types_##S(int num_el, const REAL* x, \
+void orc_station_beam_aa_types_##S(int num_el, int num_feeds, \
+        const REAL* x, \
         const REAL* y, const REAL* z, const REAL* x_meas, \
         const REAL* y_meas, const REAL* z_meas, const REAL* cable, \
         const REAL* weight_factors, int num_types, const int* element_type, \

@@ -671,7 +671,8 @@ void ORC_FN(orc_jones_r)(int num_sources, const REAL* ra, const REAL* dec,
  *    weighted DFT over the true positions, horizon blanking.
  * Scalars that the reference derives in double (wavenumber, kL, delta phi)
  * are derived in double here too, then rounded to REAL. */
-void ORC_FN(orc_station_beam_aa_types)(int num_el, const REAL* x,
+void ORC_FN(orc_station_beam_aa_types)(int num_el, int num_feeds,
+        const REAL* x,
         const REAL* y, const REAL* z, const REAL* x_meas, const REAL* y_meas,
         const REAL* z_meas, const REAL* cable, const REAL* weight_factors,
         int num_types, const int* element_type,
@@ -689,7 +690,7 @@ void ORC_FN(orc_station_beam_aa_types)(int num_el, const REAL* x,
     const double wavenumber = 2.0 * ORC_PI * frequency_hz / c0;
     REAL *X, *Y, *Z, *theta, *phi1, *phi2, *signal, *pattern, *w, *out;
     int* types;
-    int i, t;
+    int i, t, f;
     if (bz < 0)
     {
         for (i = 0; i < 8 * num_dir; ++i) beam[i] = 0;
@@ -736,24 +737,35 @@ void ORC_FN(orc_station_beam_aa_types)(int num_el, const REAL* x,
         for (i = 0; i < 8 * np; ++i)
             signal[(size_t) 8 * np * t + i] = pattern[i];
     }
-    ORC_FN(orc_element_weights_dft)(num_el, x_meas ? x_meas : x,
-            y_meas ? y_meas : y, z_meas ? z_meas : z, cable,
-            (REAL) wavenumber, (REAL) bx, (REAL) by, (REAL) bz, w);
-    /* element errors, gains, apodisation: weights *= factor
-     * (oskar_station_evaluate_element_weights.c:33-64) */
-    if (weight_factors)
-        for (i = 0; i < num_el; ++i)
-        {
-            ORC_T(cx) a = {w[2 * i], w[2 * i + 1]};
-            const ORC_T(cx) f = {weight_factors[2 * i],
-                    weight_factors[2 * i + 1]};
-            a = ORC_T(cmul)(a, f);
-            w[2 * i] = a.re;
-            w[2 * i + 1] = a.im;
-        }
-    ORC_FN(orc_dftw)(1, is_3d, num_el, (REAL) wavenumber, w, x, y, z, 0, np,
-            X, Y, is_3d ? Z : 0, types, signal, 1, 1, 0, out,
-            norm_array ? (REAL) (1.0 / num_el) : (REAL) 1);
+    /* per feed: weights from that feed's measured positions, cable errors
+     * and factors, then the weighted DFT over its true positions into the
+     * feed's rows (oskar_evaluate_station_beam_aperture_array.c:208-223;
+     * element arrays are [feed][element]) */
+    for (f = 0; f < num_feeds; ++f)
+    {
+        const size_t o = (size_t) f * num_el;
+        const REAL* xm = x_meas ? x_meas + o : x + o;
+        const REAL* ym = y_meas ? y_meas + o : y + o;
+        const REAL* zm = z_meas ? z_meas + o : z + o;
+        ORC_FN(orc_element_weights_dft)(num_el, xm, ym, zm, cable + o,
+                (REAL) wavenumber, (REAL) bx, (REAL) by, (REAL) bz, w);
+        /* element errors, gains, apodisation: weights *= factor
+         * (oskar_station_evaluate_element_weights.c:33-64) */
+        if (weight_factors)
+            for (i = 0; i < num_el; ++i)
+            {
+                ORC_T(cx) a = {w[2 * i], w[2 * i + 1]};
+                const ORC_T(cx) fc = {weight_factors[2 * (o + i)],
+                        weight_factors[2 * (o + i) + 1]};
+                a = ORC_T(cmul)(a, fc);
+                w[2 * i] = a.re;
+                w[2 * i + 1] = a.im;
+            }
+        ORC_FN(orc_dftw)(1, is_3d, num_el, (REAL) wavenumber, w, x + o,
+                y + o, z + o, 0, np, X, Y, is_3d ? Z : 0, types, signal,
+                f == 0 || num_feeds == 1, f == 1 || num_feeds == 1, 0, out,
+                norm_array ? (REAL) (1.0 / num_el) : (REAL) 1);
+    }
     ORC_FN(orc_blank_below_horizon)(0, np, Z, 0, out);
     if (norm_final) ORC_FN(orc_mem_normalise_matrix)(0, np, out, np - 1);
     for (i = 0; i < 8 * num_dir; ++i) beam[i] = out[i];
@@ -771,7 +783,7 @@ void ORC_FN(orc_station_beam_aa_weighted)(int num_el, const REAL* x,
         int num_dir, const REAL* dx, const REAL* dy, const REAL* dz,
         REAL* beam)
 {
-    ORC_FN(orc_station_beam_aa_types)(num_el, x, y, z, x_meas, y_meas,
+    ORC_FN(orc_station_beam_aa_types)(num_el, 1, x, y, z, x_meas, y_meas,
             z_meas, cable, weight_factors, 1, 0, &dipole_length_m,
             &orientation_x_rad, &orientation_y_rad, norm_element, norm_array,
             norm_final, swap_xy, is_3d, frequency_hz, bx, by, bz, nx, ny, nz,

@@ -105,9 +105,14 @@ station_beam_kernel(int num_elements, const T* __restrict__ el_x,
         BeamFlags flags, T wavenumber, const double* __restrict__ beam_enu,
         const double* __restrict__ norm_enu, int num_dir,
         const T* __restrict__ dir_x, const T* __restrict__ dir_y,
-        const T* __restrict__ dir_z, int directions_per_station,
-        T* __restrict__ beam)
+        const T* __restrict__ dir_z, int directions_per_station, int rows,
+        T* __restrict__ norm_af, T* __restrict__ beam)
 {
+    // rows: 0 all four; 1 the x feed's (xx, xy); 2 the y feed's (yx, yy).
+    // With one feed per launch the final normalisation needs both feeds'
+    // array factors at the normalisation direction: the launch writes its
+    // own to norm_af[station][type] (complex) and leaves the scaling to
+    // feeds_finalise_kernel.
     typedef typename vec2<T>::type T2;
     __shared__ T2 s_w[kChunk];
     __shared__ T s_x[kChunk], s_y[kChunk], s_z[IS3D ? kChunk : 1];
@@ -323,7 +328,19 @@ station_beam_kernel(int num_elements, const T* __restrict__ el_x,
             // the reference, which then divides by zero.
             if (nZ < (T) 0) nr[t] = ni[t] = (T) 0;
         }
-        if constexpr (NT == 1)
+        if (rows != 0)
+        {
+            if (blockIdx.x == 0 && threadIdx.x == 0)
+            {
+#pragma unroll
+                for (int t = 0; t < NT; ++t)
+                {
+                    norm_af[2 * ((size_t) st * NT + t)] = nr[t];
+                    norm_af[2 * ((size_t) st * NT + t) + 1] = ni[t];
+                }
+            }
+        }
+        else if constexpr (NT == 1)
         {
             T pn[4];
             element_pattern<T>(nX, nY, nZ, false, dphi1[0], dphi2[0],
@@ -379,8 +396,68 @@ station_beam_kernel(int num_elements, const T* __restrict__ el_x,
         if (blank) v = T2{(T) 0, (T) 0};
         v.x *= final_scale;
         v.y *= final_scale;
-        out[k] = v;
+        if (rows == 0 || (rows == 1) == (k < 2)) out[k] = v;
     }
+}
+
+// Final normalisation of a station beam evaluated one feed per launch:
+// the beam in the normalisation direction takes its (xx, xy) row from the
+// x feed's array factors and its (yx, yy) row from the y feed's
+// (norm_af[feed][station][type], complex); every direction of the station
+// is divided by that matrix's amplitude (define_mem_normalise.h:31-51).
+template <typename T, int NT>
+__global__ void __launch_bounds__(256)
+feeds_finalise_kernel(int num_stations, int num_elements,
+        const double* __restrict__ orientation_x,
+        const double* __restrict__ orientation_y, TypeParams<T> tp,
+        BeamFlags flags, const double* __restrict__ beam_enu,
+        const double* __restrict__ norm_enu, int num_dir,
+        const T* __restrict__ norm_af, T* __restrict__ beam)
+{
+    const int st = blockIdx.y;
+    const int d = blockIdx.x * blockDim.x + threadIdx.x;
+    // a pointing below the horizon left a zero beam and no array factors
+    if (d >= num_dir || beam_enu[3 * st + 2] < 0.0) return;
+    const T nX = (T) norm_enu[3 * st], nY = (T) norm_enu[3 * st + 1],
+            nZ = (T) norm_enu[3 * st + 2];
+    const T array_scale = flags.normalise_array ?
+            (T) (1.0 / num_elements) : (T) 1;
+    T amp = 0;
+    T pn[NT][4], pole[NT];
+#pragma unroll
+    for (int t = 0; t < NT; ++t)
+    {
+        const T dphi1 = (T) (kPi / 2 - (orientation_x[st * NT + t] + kPi / 2));
+        const T dphi2 = (T) (kPi / 2 - orientation_y[st * NT + t]);
+        pole[t] = (T) 1;
+        if (flags.normalise_element)
+        {
+            T pp[4];
+            element_pattern<T>(0, 0, 1, true, dphi1, dphi2, tp.kL[t],
+                    tp.cos_kL[t], flags.swap_xy, pp);
+            pole[t] = (T) 1 / sqrt(half_frobenius<T>(pp, 1, 0));
+        }
+        element_pattern<T>(nX, nY, nZ, false, dphi1, dphi2, tp.kL[t],
+                tp.cos_kL[t], flags.swap_xy, pn[t]);
+    }
+    for (int k = 0; k < 4; ++k)
+    {
+        const T* af = norm_af + 2 * (size_t) NT *
+                ((size_t) (k < 2 ? 0 : 1) * num_stations + st);
+        T vr = 0, vi = 0;
+#pragma unroll
+        for (int t = 0; t < NT; ++t)
+        {
+            const T pk = pn[t][k] * pole[t] * array_scale;
+            vr += pk * af[2 * t];
+            vi += pk * af[2 * t + 1];
+        }
+        amp += vr * vr + vi * vi;
+    }
+    const T scale = (T) 1 / sqrt(amp / (T) 2);
+    T* b = beam + 8 * ((size_t) st * num_dir + d);
+#pragma unroll
+    for (int i = 0; i < 8; ++i) b[i] *= scale;
 }
 
 template <typename T>
@@ -425,7 +502,8 @@ int station_beam_aa(int num_stations, int num_elements, const T* el_x,
         int normalise_element, int normalise_array, int normalise_final,
         int swap_xy, int is_3d, double frequency_hz, const double* beam_enu,
         const double* norm_enu, int num_directions, const T* x, const T* y,
-        const T* z, int directions_per_station, T* beam, void* stream)
+        const T* z, int directions_per_station, T* beam, void* stream,
+        int rows = 0, T* norm_af = nullptr)
 {
     if (num_stations < 0 || num_elements < 0 || num_directions < 0)
         return OSKB_ERR_INVALID_ARGUMENT;
@@ -456,7 +534,7 @@ int station_beam_aa(int num_stations, int num_elements, const T* el_x,
         s>>>(num_elements, el_x, el_y, el_z, meas_x, meas_y, meas_z, cable,  \
         weight_factors, element_type, orientation_x, orientation_y, tp,      \
         flags, wavenumber, beam_enu, norm_enu, num_directions, x, y, z,      \
-        directions_per_station, beam)
+        directions_per_station, rows, norm_af, beam)
 #define OSKB_BEAM_NT(D)                                                      \
     switch (num_element_types)                                               \
     {                                                                        \
@@ -469,6 +547,98 @@ int station_beam_aa(int num_stations, int num_elements, const T* el_x,
 #undef OSKB_BEAM_NT
 #undef OSKB_BEAM
     return check_launch("station_beam_aa");
+}
+
+// Stations whose two feeds have their own element data (the reference's
+// num_feeds = 2 when a station is not common_pol_beams,
+// oskar_evaluate_station_beam_aperture_array.c:208-223): element arrays
+// are [feed][station][element]; one launch per feed writes that feed's
+// rows, then the final normalisation combines both feeds.
+template <typename T>
+int station_beam_aa_feeds(int num_feeds, int num_stations, int num_elements,
+        const T* el_x, const T* el_y, const T* el_z, const T* meas_x,
+        const T* meas_y, const T* meas_z, const T* cable,
+        const T* weight_factors, int num_element_types,
+        const int* element_type, const double* orientation_x,
+        const double* orientation_y, const double* dipole_length_m,
+        int normalise_element, int normalise_array, int normalise_final,
+        int swap_xy, int is_3d, double frequency_hz, const double* beam_enu,
+        const double* norm_enu, int num_directions, const T* x, const T* y,
+        const T* z, int directions_per_station, T* beam, void* stream)
+{
+    if (num_feeds == 1)
+        return station_beam_aa<T>(num_stations, num_elements, el_x, el_y,
+                el_z, meas_x, meas_y, meas_z, cable, weight_factors,
+                num_element_types, element_type, orientation_x,
+                orientation_y, dipole_length_m, normalise_element,
+                normalise_array, normalise_final, swap_xy, is_3d,
+                frequency_hz, beam_enu, norm_enu, num_directions, x, y, z,
+                directions_per_station, beam, stream);
+    if (num_feeds != 2) return OSKB_ERR_INVALID_ARGUMENT;
+    if (num_stations <= 0 || num_directions <= 0)
+        return num_stations < 0 || num_directions < 0 ?
+                OSKB_ERR_INVALID_ARGUMENT : 0;
+    if (num_element_types < 1 || !dipole_length_m)
+        return OSKB_ERR_INVALID_ARGUMENT;
+    if (num_element_types > kMaxTypes) return OSKB_ERR_OUT_OF_RANGE;
+    cudaStream_t s = as_stream(stream);
+    T* norm_af = nullptr;
+    const size_t af_count = (size_t) 2 * num_stations * num_element_types * 2;
+    if (normalise_final)
+    {
+        if (scratch_alloc((void**) &norm_af, af_count * sizeof(T), s) !=
+                cudaSuccess)
+        {
+            cudaGetLastError();
+            return OSKB_ERR_MEMORY_ALLOC_FAILURE;
+        }
+    }
+    const size_t n = (size_t) num_stations * num_elements;
+    int err = 0;
+    for (int f = 0; f < 2 && !err; ++f)
+    {
+        const size_t o = f * n;
+        err = station_beam_aa<T>(num_stations, num_elements, el_x + o,
+                el_y + o, el_z ? el_z + o : nullptr,
+                meas_x ? meas_x + o : nullptr, meas_y ? meas_y + o : nullptr,
+                meas_z ? meas_z + o : nullptr, cable ? cable + o : nullptr,
+                weight_factors ? weight_factors + 2 * o : nullptr,
+                num_element_types, element_type, orientation_x,
+                orientation_y, dipole_length_m, normalise_element,
+                normalise_array, normalise_final, swap_xy, is_3d,
+                frequency_hz, beam_enu, norm_enu, num_directions, x, y, z,
+                directions_per_station, beam, stream, 1 + f,
+                norm_af ? norm_af + f * (af_count / 2) : nullptr);
+    }
+    if (!err && normalise_final)
+    {
+        TypeParams<T> tp;
+        const double c0 = 299792458.0;
+        for (int t = 0; t < kMaxTypes; ++t)
+        {
+            const double kL = t < num_element_types ?
+                    dipole_length_m[t] * (kPi * frequency_hz / c0) : 0.0;
+            tp.kL[t] = (T) kL;
+            tp.cos_kL[t] = (T) cos(kL);
+        }
+        BeamFlags flags{normalise_element, normalise_array, normalise_final,
+                swap_xy};
+        dim3 grid((num_directions + 255) / 256, num_stations);
+#define OSKB_FIN(NT) feeds_finalise_kernel<T, NT><<<grid, 256, 0, s>>>(       \
+        num_stations, num_elements, orientation_x, orientation_y, tp, flags, \
+        beam_enu, norm_enu, num_directions, norm_af, beam)
+        switch (num_element_types)
+        {
+        case 1: OSKB_FIN(1); break;
+        case 2: OSKB_FIN(2); break;
+        case 3: OSKB_FIN(3); break;
+        default: OSKB_FIN(4); break;
+        }
+#undef OSKB_FIN
+        err = check_launch("station_beam_feeds_finalise");
+    }
+    if (norm_af) scratch_free(norm_af, s);
+    return err;
 }
 
 template <typename T>
@@ -547,6 +717,27 @@ int oskb_station_beam_aa_types_##S(int num_stations, int num_elements,       \
             normalise_element, normalise_array, normalise_final, swap_xy,    \
             is_3d, frequency_hz, beam_enu, norm_enu, num_directions, x, y,   \
             z, directions_per_station, beam, stream);                        \
+}                                                                            \
+int oskb_station_beam_aa_feeds_##S(int num_feeds, int num_stations,        \
+        int num_elements, const T* el_x, const T* el_y, const T* el_z,       \
+        const T* meas_x, const T* meas_y, const T* meas_z,                   \
+        const T* cable_length_error, const T* element_weight_factors,        \
+        int num_element_types, const int* element_type,                     \
+        const double* dipole_length_m, const double* orientation_x_rad,      \
+        const double* orientation_y_rad, int normalise_element,              \
+        int normalise_array, int normalise_final, int swap_xy, int is_3d,    \
+        double frequency_hz, const double* beam_enu, const double* norm_enu, \
+        int num_directions, const T* x, const T* y, const T* z,              \
+        int directions_per_station, T* beam, void* stream)                   \
+{                                                                            \
+    return oskb::station_beam_aa_feeds<T>(num_feeds, num_stations,           \
+            num_elements, el_x, el_y, el_z, meas_x, meas_y, meas_z,          \
+            cable_length_error, element_weight_factors, num_element_types,   \
+            element_type, orientation_x_rad, orientation_y_rad,              \
+            dipole_length_m, normalise_element, normalise_array,             \
+            normalise_final, swap_xy, is_3d, frequency_hz, beam_enu,         \
+            norm_enu, num_directions, x, y, z, directions_per_station, beam, \
+            stream);                                                         \
 }                                                                            \
 int oskb_evaluate_jones_R_##S(int num_sources, const T* ra_rad,              \
         const T* dec_rad, int num_stations, const double* lat_rad,           \

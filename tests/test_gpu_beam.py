@@ -160,7 +160,7 @@ def test_station_beam_element_types(real, num_types, flags):
     for s, c in enumerate(cases):
         ref = np.zeros(8 * nd, real)
         oracle().call("station_beam_aa_types_" + suffix(real), np.float64,
-                      n, *c["el"], *c["meas"], c["cable"], wf[s].copy(),
+                      n, 1, *c["el"], *c["meas"], c["cable"], wf[s].copy(),
                       num_types, types[s].copy(), lengths,
                       ori_x[s].copy(), ori_y[s].copy(), norm_el, norm_arr,
                       norm_fin, swap, is_3d, c["freq"],
@@ -183,3 +183,68 @@ def test_station_beam_element_types_limits():
                    check=False) == -3
     assert ob.call("oskb_station_beam_aa_types_d", *args(1, None),
                    check=False) == -3
+
+
+@pytest.mark.parametrize("real", [np.float64, np.float32])
+@pytest.mark.parametrize("num_types", [1, 2])
+@pytest.mark.parametrize("flags", [(1, 1, 1, 0, 1), (0, 1, 0, 1, 0),
+                                   (1, 0, 1, 1, 0)])
+def test_station_beam_two_feeds(real, num_types, flags):
+    """Stations whose y feed has its own element positions (true and
+    measured), cable errors and weight factors: the x feed's array factor
+    forms the (xx, xy) row, the y feed's the (yx, yy) row, and the final
+    normalisation uses both (oskar_evaluate_station_beam_aperture_array.c:
+    208-223), against the oracle's per-feed DFT with eval_x / eval_y. One
+    station points below the horizon."""
+    norm_el, norm_arr, norm_fin, swap, is_3d = flags
+    cases = stations(real, is_3d=is_3d, num_el=150, num_dir=517)
+    cases[1]["b"] = np.array([0.3, 0.2, -np.sqrt(1 - 0.13)])
+    nst, n, nd = len(cases), 150, 517
+    rng = np.random.default_rng(9 + num_types)
+    types = rng.integers(0, num_types, (nst, n)).astype(np.int32)
+    lengths = np.array([1.5, 1.1][:num_types])
+    ori_x = rng.uniform(0, np.pi, (nst, num_types))
+    ori_y = ori_x + np.pi / 2
+    # feed y: positions moved by up to 5 cm, its own cable errors, factors
+    feeds = []
+    for c in cases:
+        dxy = [rng.normal(0, 0.05, n).astype(real) for _ in range(3)]
+        if not is_3d:
+            dxy[2][:] = 0
+        fy = dict(el=[c["el"][i] + dxy[i] for i in range(3)],
+                  meas=[c["meas"][i] + dxy[i] for i in range(3)],
+                  cable=rng.normal(0, 0.02, n).astype(real))
+        feeds.append((c, fy))
+    wf = rng.normal(1, 0.1, (2, nst, 2 * n)).astype(real)
+    stack = lambda key, i: dev(np.concatenate(
+        [c[key][i] for c, _ in feeds] + [fy[key][i] for _, fy in feeds]))
+    cable = dev(np.concatenate([c["cable"] for c, _ in feeds] +
+                               [fy["cable"] for _, fy in feeds]))
+    out = torch.zeros(nst * nd * 8, dtype=torch.float64 if real ==
+                      np.float64 else torch.float32, device="cuda")
+    ob.call("oskb_station_beam_aa_feeds_" + suffix(real), 2, nst, n,
+            *[stack("el", i) for i in range(3)],
+            *[stack("meas", i) for i in range(3)], cable, dev(wf),
+            num_types, dev(types), lengths, dev(ori_x), dev(ori_y), norm_el,
+            norm_arr, norm_fin, swap, is_3d, cases[0]["freq"],
+            dev(np.stack([c["b"] for c in cases])),
+            dev(np.stack([c["norm"] for c in cases])), nd,
+            *[dev(cases[0]["dirs"][i]) for i in range(3)], 0, out,
+            ob.stream_ptr())
+    torch.cuda.synchronize()
+    got = out.cpu().numpy().reshape(nst, -1)
+    assert not got[1].any()
+    for s, (c, fy) in enumerate(feeds):
+        if s == 1:
+            continue
+        ref = np.zeros(8 * nd, real)
+        cat2 = lambda a, b: np.ascontiguousarray(np.concatenate([a, b]))
+        oracle().call("station_beam_aa_types_" + suffix(real), np.float64,
+                      n, 2, *[cat2(c["el"][i], fy["el"][i]) for i in range(3)],
+                      *[cat2(c["meas"][i], fy["meas"][i]) for i in range(3)],
+                      cat2(c["cable"], fy["cable"]),
+                      cat2(wf[0, s], wf[1, s]), num_types, types[s].copy(),
+                      lengths, ori_x[s].copy(), ori_y[s].copy(), norm_el,
+                      norm_arr, norm_fin, swap, is_3d, c["freq"], *c["b"],
+                      *c["norm"], nd, *cases[0]["dirs"], ref)
+        assert rel(got[s], ref) <= TOL[real], (s, rel(got[s], ref))
