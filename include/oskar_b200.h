@@ -293,6 +293,12 @@ OSKB_API int oskb_station_beam_aa_weighted_f(int num_stations,
         const float* x, const float* y, const float* z,
         int directions_per_station, float* beam, void* stream);
 
+#define OSKB_ELEMENT_DIPOLE    0
+#define OSKB_ELEMENT_ISOTROPIC 1
+#define OSKB_TAPER_NONE        0
+#define OSKB_TAPER_COSINE      1
+#define OSKB_TAPER_GAUSSIAN    2
+
 /* oskb_station_beam_aa_weighted for stations with up to 4 element types
  * (oskar_evaluate_station_beam_aperture_array.c:158-202 and its oskar_dftw
  * with data index = element type): element e has type
@@ -300,7 +306,12 @@ OSKB_API int oskb_station_beam_aa_weighted_f(int num_stations,
  * of length dipole_length_m[t] (host array of num_element_types) with
  * Euler angles orientation_{x,y}_rad[station][t] (device) and its own pole
  * normalisation; beam = sum over types of the type's pattern times the
- * array factor of its elements. A station whose elements differ in
+ * array factor of its elements. Host arrays per type (each may be NULL):
+ * element_kind OSKB_ELEMENT_DIPOLE or OSKB_ELEMENT_ISOTROPIC (the identity
+ * pattern); taper_kind OSKB_TAPER_NONE, OSKB_TAPER_COSINE (cos(theta) to the
+ * power taper_param) or OSKB_TAPER_GAUSSIAN (FWHM taper_param radians in
+ * theta), applied after the pole normalisation (oskar_element_evaluate.c:
+ * 82-87, 159-174). A station whose elements differ in
  * orientation (the reference's per-element branch, :180-202) maps onto
  * this when its distinct (element model, orientation) pairs number at most
  * four: one type per pair. An element whose type is outside
@@ -312,6 +323,8 @@ OSKB_API int oskb_station_beam_aa_types_d(int num_stations, int num_elements,
         const double* cable_length_error,
         const double* element_weight_factors, int num_element_types,
         const int* element_type, const double* dipole_length_m,
+        const int* element_kind, const int* taper_kind,
+        const double* taper_param,
         const double* orientation_x_rad, const double* orientation_y_rad,
         int normalise_element, int normalise_array, int normalise_final,
         int swap_xy, int is_3d, double frequency_hz, const double* beam_enu,
@@ -324,6 +337,8 @@ OSKB_API int oskb_station_beam_aa_types_f(int num_stations, int num_elements,
         const float* cable_length_error,
         const float* element_weight_factors, int num_element_types,
         const int* element_type, const double* dipole_length_m,
+        const int* element_kind, const int* taper_kind,
+        const double* taper_param,
         const double* orientation_x_rad, const double* orientation_y_rad,
         int normalise_element, int normalise_array, int normalise_final,
         int swap_xy, int is_3d, double frequency_hz, const double* beam_enu,
@@ -346,6 +361,8 @@ OSKB_API int oskb_station_beam_aa_feeds_d(int num_feeds, int num_stations,
         const double* meas_z, const double* cable_length_error,
         const double* element_weight_factors, int num_element_types,
         const int* element_type, const double* dipole_length_m,
+        const int* element_kind, const int* taper_kind,
+        const double* taper_param,
         const double* orientation_x_rad, const double* orientation_y_rad,
         int normalise_element, int normalise_array, int normalise_final,
         int swap_xy, int is_3d, double frequency_hz, const double* beam_enu,
@@ -358,6 +375,8 @@ OSKB_API int oskb_station_beam_aa_feeds_f(int num_feeds, int num_stations,
         const float* meas_z, const float* cable_length_error,
         const float* element_weight_factors, int num_element_types,
         const int* element_type, const double* dipole_length_m,
+        const int* element_kind, const int* taper_kind,
+        const double* taper_param,
         const double* orientation_x_rad, const double* orientation_y_rad,
         int normalise_element, int normalise_array, int normalise_final,
         int swap_xy, int is_3d, double frequency_hz, const double* beam_enu,

@@ -88,7 +88,8 @@ void orc_station_beam_aa_types_##S(int num_el, int num_feeds, \
         const REAL* y, const REAL* z, const REAL* x_meas, \
         const REAL* y_meas, const REAL* z_meas, const REAL* cable, \
         const REAL* weight_factors, int num_types, const int* element_type, \
-        const double* dipole_length_per_type, \
+        const double* dipole_length_per_type, const int* kind_per_type, \
+        const int* taper_per_type, const double* taper_param_per_type, \
         const double* orientation_x_per_type, \
         const double* orientation_y_per_type, int norm_element, \
         int norm_array, int norm_final, int swap_xy, int is_3d, \

@@ -676,7 +676,8 @@ void ORC_FN(orc_station_beam_aa_types)(int num_el, int num_feeds,
         const REAL* y, const REAL* z, const REAL* x_meas, const REAL* y_meas,
         const REAL* z_meas, const REAL* cable, const REAL* weight_factors,
         int num_types, const int* element_type,
-        const double* dipole_length_per_type,
+        const double* dipole_length_per_type, const int* kind_per_type,
+        const int* taper_per_type, const double* taper_param_per_type,
         const double* orientation_x_per_type,
         const double* orientation_y_per_type, int norm_element,
         int norm_array, int norm_final, int swap_xy, int is_3d,
@@ -730,10 +731,42 @@ void ORC_FN(orc_station_beam_aa_types)(int num_el, int num_feeds,
         const double dphi2 = ORC_PI / 2 - orientation_y_per_type[t];
         ORC_FN(orc_enu_to_theta_phi)(0, np, X, Y, Z, norm_element,
                 (REAL) dphi1, (REAL) dphi2, theta, phi1, phi2);
-        ORC_FN(orc_dipole_pattern)(npe, theta, phi1, phi2, (REAL) kL,
-                (REAL) cos(kL), swap_xy, 0, pattern);
+        if (kind_per_type && kind_per_type[t] == 1)
+        {
+            /* isotropic: the identity (oskar_element_evaluate.c:82-87) */
+            for (i = 0; i < npe; ++i)
+            {
+                int k;
+                for (k = 0; k < 8; ++k) pattern[8 * i + k] = 0;
+                pattern[8 * i] = pattern[8 * i + 6] = 1;
+            }
+        }
+        else
+            ORC_FN(orc_dipole_pattern)(npe, theta, phi1, phi2, (REAL) kL,
+                    (REAL) cos(kL), swap_xy, 0, pattern);
         if (norm_element)
             ORC_FN(orc_mem_normalise_matrix)(0, np, pattern, np);
+        /* element taper after the normalisation (oskar_element_evaluate.c:
+         * 159-174; define_apply_element_taper_{cosine,gaussian}.h) */
+        if (taper_per_type && taper_per_type[t] != 0)
+            for (i = 0; i < np; ++i)
+            {
+                int k;
+                REAL fac;
+                if (taper_per_type[t] == 1)
+                    fac = (REAL) pow((REAL) cos(theta[i]),
+                            (REAL) taper_param_per_type[t]);
+                else
+                {
+                    const double fwhm = taper_param_per_type[t];
+                    const REAL inv_2sigma_sq = (REAL)
+                            (4.0 * log(2.0) / (fwhm * fwhm));
+                    REAL th2 = theta[i];
+                    th2 *= th2;
+                    fac = ORC_EXP(-th2 * inv_2sigma_sq);
+                }
+                for (k = 0; k < 8; ++k) pattern[8 * i + k] *= fac;
+            }
         for (i = 0; i < 8 * np; ++i)
             signal[(size_t) 8 * np * t + i] = pattern[i];
     }
@@ -784,7 +817,7 @@ void ORC_FN(orc_station_beam_aa_weighted)(int num_el, const REAL* x,
         REAL* beam)
 {
     ORC_FN(orc_station_beam_aa_types)(num_el, 1, x, y, z, x_meas, y_meas,
-            z_meas, cable, weight_factors, 1, 0, &dipole_length_m,
+            z_meas, cable, weight_factors, 1, 0, &dipole_length_m, 0, 0, 0,
             &orientation_x_rad, &orientation_y_rad, norm_element, norm_array,
             norm_final, swap_xy, is_3d, frequency_hz, bx, by, bz, nx, ny, nz,
             num_dir, dx, dy, dz, beam);

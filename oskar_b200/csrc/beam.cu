@@ -65,7 +65,40 @@ struct TypeParams
 {
     T kL[kMaxTypes];      // dipole length x pi f / c
     T cos_kL[kMaxTypes];
+    int kind[kMaxTypes];  // 0 dipole, 1 isotropic
+    int taper[kMaxTypes]; // 0 none, 1 cos(theta)^p, 2 Gaussian in theta
+    T taper_param[kMaxTypes];  // p, or 4 ln 2 / FWHM^2
 };
+
+// Real pattern {a, b, c, d} of element type t in direction (X, Y, Z): the
+// dipole's, or the identity for an isotropic element
+// (oskar_element_evaluate.c:82-87).
+template <typename T>
+__device__ __forceinline__ void type_pattern(const TypeParams<T>& tp, int t,
+        T X, T Y, T Z, bool pole, T dphi1, T dphi2, int swap_xy, T p[4])
+{
+    if (tp.kind[t] == 1)
+    {
+        p[0] = p[3] = (T) 1;
+        p[1] = p[2] = (T) 0;
+        return;
+    }
+    element_pattern<T>(X, Y, Z, pole, dphi1, dphi2, tp.kL[t], tp.cos_kL[t],
+            swap_xy, p);
+}
+
+// Element taper of type t at polar angle theta = atan2(|(X, Y)|, Z),
+// applied after the pole normalisation (oskar_element_evaluate.c:159-174;
+// define_apply_element_taper_{cosine,gaussian}.h).
+template <typename T>
+__device__ __forceinline__ T type_taper(const TypeParams<T>& tp, int t, T X,
+        T Y, T Z)
+{
+    if (tp.taper[t] == 0) return (T) 1;
+    const T theta = atan2(sqrt(X * X + Y * Y), Z);
+    if (tp.taper[t] == 1) return pow(cos(theta), tp.taper_param[t]);
+    return exp(-(theta * theta) * tp.taper_param[t]);
+}
 
 // (ar, ai)[t] += w e^{i ph} for the element's type t only: register selects
 // over a compile-time number of types, so the accumulators stay in
@@ -287,8 +320,8 @@ station_beam_kernel(int num_elements, const T* __restrict__ el_x,
         if (flags.normalise_element)
         {
             T pp[4];
-            element_pattern<T>(0, 0, 1, true, dphi1[t], dphi2[t], tp.kL[t],
-                    tp.cos_kL[t], flags.swap_xy, pp);
+            type_pattern<T>(tp, t, 0, 0, 1, true, dphi1[t], dphi2[t],
+                    flags.swap_xy, pp);
             pole_scale[t] = (T) 1 / sqrt(half_frobenius<T>(pp, 1, 0));
         }
     }
@@ -343,10 +376,11 @@ station_beam_kernel(int num_elements, const T* __restrict__ el_x,
         else if constexpr (NT == 1)
         {
             T pn[4];
-            element_pattern<T>(nX, nY, nZ, false, dphi1[0], dphi2[0],
-                    tp.kL[0],
-                    tp.cos_kL[0], flags.swap_xy, pn);
-            for (int k = 0; k < 4; ++k) pn[k] *= pole_scale[0] * array_scale;
+            type_pattern<T>(tp, 0, nX, nY, nZ, false, dphi1[0], dphi2[0],
+                    flags.swap_xy, pn);
+            const T taper = type_taper<T>(tp, 0, nX, nY, nZ);
+            for (int k = 0; k < 4; ++k)
+                pn[k] *= pole_scale[0] * taper * array_scale;
             final_scale = (T) 1 / sqrt(half_frobenius<T>(pn, nr[0], ni[0]));
         }
         else
@@ -355,8 +389,12 @@ station_beam_kernel(int num_elements, const T* __restrict__ el_x,
             T pn[NT][4];
 #pragma unroll
             for (int t = 0; t < NT; ++t)
-                element_pattern<T>(nX, nY, nZ, false, dphi1[t], dphi2[t],
-                        tp.kL[t], tp.cos_kL[t], flags.swap_xy, pn[t]);
+            {
+                type_pattern<T>(tp, t, nX, nY, nZ, false, dphi1[t],
+                        dphi2[t], flags.swap_xy, pn[t]);
+                const T taper = type_taper<T>(tp, t, nX, nY, nZ);
+                for (int k = 0; k < 4; ++k) pn[t][k] *= taper;
+            }
             T amp = 0;
             for (int k = 0; k < 4; ++k)
             {
@@ -379,8 +417,12 @@ station_beam_kernel(int num_elements, const T* __restrict__ el_x,
     T p[NT][4];
 #pragma unroll
     for (int t = 0; t < NT; ++t)
-        element_pattern<T>(X, Y, Z, false, dphi1[t], dphi2[t], tp.kL[t],
-                tp.cos_kL[t], flags.swap_xy, p[t]);
+    {
+        type_pattern<T>(tp, t, X, Y, Z, false, dphi1[t], dphi2[t],
+                flags.swap_xy, p[t]);
+        const T taper = type_taper<T>(tp, t, X, Y, Z);
+        for (int k = 0; k < 4; ++k) p[t][k] *= taper;
+    }
     for (int k = 0; k < 4; ++k)
     {
         // The reference's order: pattern (normalised), times the weighted
@@ -433,12 +475,14 @@ feeds_finalise_kernel(int num_stations, int num_elements,
         if (flags.normalise_element)
         {
             T pp[4];
-            element_pattern<T>(0, 0, 1, true, dphi1, dphi2, tp.kL[t],
-                    tp.cos_kL[t], flags.swap_xy, pp);
+            type_pattern<T>(tp, t, 0, 0, 1, true, dphi1, dphi2,
+                    flags.swap_xy, pp);
             pole[t] = (T) 1 / sqrt(half_frobenius<T>(pp, 1, 0));
         }
-        element_pattern<T>(nX, nY, nZ, false, dphi1, dphi2, tp.kL[t],
-                tp.cos_kL[t], flags.swap_xy, pn[t]);
+        type_pattern<T>(tp, t, nX, nY, nZ, false, dphi1, dphi2,
+                flags.swap_xy, pn[t]);
+        const T taper = type_taper<T>(tp, t, nX, nY, nZ);
+        for (int k = 0; k < 4; ++k) pn[t][k] *= taper;
     }
     for (int k = 0; k < 4; ++k)
     {
@@ -492,6 +536,41 @@ jones_r_kernel(int num_sources, const T* __restrict__ ra,
 namespace oskb {
 namespace {
 
+// Per-type parameters from host arrays (NULL kinds: dipoles; NULL tapers:
+// none). Returns an OSKAR status.
+template <typename T>
+int make_type_params(int num_types, const double* dipole_length_m,
+        const int* element_kind, const int* taper_kind,
+        const double* taper_param, double frequency_hz, TypeParams<T>* tp)
+{
+    if (num_types < 1 || !dipole_length_m) return OSKB_ERR_INVALID_ARGUMENT;
+    if (num_types > kMaxTypes) return OSKB_ERR_OUT_OF_RANGE;
+    const double c0 = 299792458.0;
+    for (int t = 0; t < kMaxTypes; ++t)
+    {
+        const bool on = t < num_types;
+        const double kL = on ?
+                dipole_length_m[t] * (kPi * frequency_hz / c0) : 0.0;
+        tp->kL[t] = (T) kL;
+        tp->cos_kL[t] = (T) cos(kL);
+        tp->kind[t] = on && element_kind ? element_kind[t] : 0;
+        tp->taper[t] = on && taper_kind ? taper_kind[t] : 0;
+        if (tp->kind[t] < 0 || tp->kind[t] > 1 || tp->taper[t] < 0 ||
+                tp->taper[t] > 2 || (tp->taper[t] && !taper_param))
+            return OSKB_ERR_INVALID_ARGUMENT;
+        double q = 0.0;
+        if (tp->taper[t] == 1) q = taper_param[t];
+        if (tp->taper[t] == 2)
+        {
+            const double fwhm = taper_param[t];
+            if (!(fwhm > 0.0)) return OSKB_ERR_INVALID_ARGUMENT;
+            q = 4.0 * log(2.0) / (fwhm * fwhm);
+        }
+        tp->taper_param[t] = (T) q;
+    }
+    return 0;
+}
+
 template <typename T>
 int station_beam_aa(int num_stations, int num_elements, const T* el_x,
         const T* el_y, const T* el_z, const T* meas_x, const T* meas_y,
@@ -499,6 +578,8 @@ int station_beam_aa(int num_stations, int num_elements, const T* el_x,
         int num_element_types, const int* element_type,
         const double* orientation_x,
         const double* orientation_y, const double* dipole_length_m,
+        const int* element_kind, const int* taper_kind,
+        const double* taper_param,
         int normalise_element, int normalise_array, int normalise_final,
         int swap_xy, int is_3d, double frequency_hz, const double* beam_enu,
         const double* norm_enu, int num_directions, const T* x, const T* y,
@@ -513,18 +594,11 @@ int station_beam_aa(int num_stations, int num_elements, const T* el_x,
             (normalise_final && !norm_enu) || !x || !y || !z || !beam)
         return OSKB_ERR_INVALID_ARGUMENT;
     if (num_stations > 65535) return OSKB_ERR_INVALID_ARGUMENT;
-    if (num_element_types < 1 || !dipole_length_m)
-        return OSKB_ERR_INVALID_ARGUMENT;
-    if (num_element_types > kMaxTypes) return OSKB_ERR_OUT_OF_RANGE;
-    const double c0 = 299792458.0;
     TypeParams<T> tp;
-    for (int t = 0; t < kMaxTypes; ++t)
-    {
-        const double kL = t < num_element_types ?
-                dipole_length_m[t] * (kPi * frequency_hz / c0) : 0.0;
-        tp.kL[t] = (T) kL;
-        tp.cos_kL[t] = (T) cos(kL);
-    }
+    if (int err = make_type_params<T>(num_element_types, dipole_length_m,
+            element_kind, taper_kind, taper_param, frequency_hz, &tp))
+        return err;
+    const double c0 = 299792458.0;
     const T wavenumber = (T) (2.0 * kPi * frequency_hz / c0);
     BeamFlags flags{normalise_element, normalise_array, normalise_final,
             swap_xy};
@@ -561,6 +635,8 @@ int station_beam_aa_feeds(int num_feeds, int num_stations, int num_elements,
         const T* weight_factors, int num_element_types,
         const int* element_type, const double* orientation_x,
         const double* orientation_y, const double* dipole_length_m,
+        const int* element_kind, const int* taper_kind,
+        const double* taper_param,
         int normalise_element, int normalise_array, int normalise_final,
         int swap_xy, int is_3d, double frequency_hz, const double* beam_enu,
         const double* norm_enu, int num_directions, const T* x, const T* y,
@@ -570,7 +646,8 @@ int station_beam_aa_feeds(int num_feeds, int num_stations, int num_elements,
         return station_beam_aa<T>(num_stations, num_elements, el_x, el_y,
                 el_z, meas_x, meas_y, meas_z, cable, weight_factors,
                 num_element_types, element_type, orientation_x,
-                orientation_y, dipole_length_m, normalise_element,
+                orientation_y, dipole_length_m, element_kind, taper_kind,
+                taper_param, normalise_element,
                 normalise_array, normalise_final, swap_xy, is_3d,
                 frequency_hz, beam_enu, norm_enu, num_directions, x, y, z,
                 directions_per_station, beam, stream);
@@ -578,9 +655,10 @@ int station_beam_aa_feeds(int num_feeds, int num_stations, int num_elements,
     if (num_stations <= 0 || num_directions <= 0)
         return num_stations < 0 || num_directions < 0 ?
                 OSKB_ERR_INVALID_ARGUMENT : 0;
-    if (num_element_types < 1 || !dipole_length_m)
-        return OSKB_ERR_INVALID_ARGUMENT;
-    if (num_element_types > kMaxTypes) return OSKB_ERR_OUT_OF_RANGE;
+    TypeParams<T> tp;
+    if (int err = make_type_params<T>(num_element_types, dipole_length_m,
+            element_kind, taper_kind, taper_param, frequency_hz, &tp))
+        return err;
     cudaStream_t s = as_stream(stream);
     T* norm_af = nullptr;
     const size_t af_count = (size_t) 2 * num_stations * num_element_types * 2;
@@ -604,7 +682,8 @@ int station_beam_aa_feeds(int num_feeds, int num_stations, int num_elements,
                 meas_z ? meas_z + o : nullptr, cable ? cable + o : nullptr,
                 weight_factors ? weight_factors + 2 * o : nullptr,
                 num_element_types, element_type, orientation_x,
-                orientation_y, dipole_length_m, normalise_element,
+                orientation_y, dipole_length_m, element_kind, taper_kind,
+                taper_param, normalise_element,
                 normalise_array, normalise_final, swap_xy, is_3d,
                 frequency_hz, beam_enu, norm_enu, num_directions, x, y, z,
                 directions_per_station, beam, stream, 1 + f,
@@ -612,15 +691,6 @@ int station_beam_aa_feeds(int num_feeds, int num_stations, int num_elements,
     }
     if (!err && normalise_final)
     {
-        TypeParams<T> tp;
-        const double c0 = 299792458.0;
-        for (int t = 0; t < kMaxTypes; ++t)
-        {
-            const double kL = t < num_element_types ?
-                    dipole_length_m[t] * (kPi * frequency_hz / c0) : 0.0;
-            tp.kL[t] = (T) kL;
-            tp.cos_kL[t] = (T) cos(kL);
-        }
         BeamFlags flags{normalise_element, normalise_array, normalise_final,
                 swap_xy};
         dim3 grid((num_directions + 255) / 256, num_stations);
@@ -675,6 +745,7 @@ int oskb_station_beam_aa_##S(int num_stations, int num_elements,             \
     return oskb::station_beam_aa<T>(num_stations, num_elements, el_x, el_y,  \
             el_z, meas_x, meas_y, meas_z, cable_length_error, nullptr, 1,    \
             nullptr, orientation_x_rad, orientation_y_rad, &dipole_length_m, \
+            nullptr, nullptr, nullptr,                                       \
             normalise_element, normalise_array, normalise_final, swap_xy,    \
             is_3d, frequency_hz, beam_enu, norm_enu, num_directions, x, y,   \
             z, directions_per_station, beam, stream);                        \
@@ -693,7 +764,8 @@ int oskb_station_beam_aa_weighted_##S(int num_stations, int num_elements,    \
     return oskb::station_beam_aa<T>(num_stations, num_elements, el_x, el_y,  \
             el_z, meas_x, meas_y, meas_z, cable_length_error,                \
             element_weight_factors, 1, nullptr, orientation_x_rad,           \
-            orientation_y_rad, &dipole_length_m, normalise_element,          \
+            orientation_y_rad, &dipole_length_m, nullptr, nullptr, nullptr,  \
+            normalise_element,                                               \
             normalise_array, normalise_final, swap_xy, is_3d, frequency_hz,  \
             beam_enu, norm_enu, num_directions, x, y, z,                     \
             directions_per_station, beam, stream);                           \
@@ -703,6 +775,8 @@ int oskb_station_beam_aa_types_##S(int num_stations, int num_elements,       \
         const T* meas_y, const T* meas_z, const T* cable_length_error,       \
         const T* element_weight_factors, int num_element_types,              \
         const int* element_type, const double* dipole_length_m,              \
+        const int* element_kind, const int* taper_kind,                      \
+        const double* taper_param,                                           \
         const double* orientation_x_rad, const double* orientation_y_rad,    \
         int normalise_element, int normalise_array, int normalise_final,     \
         int swap_xy, int is_3d, double frequency_hz,                         \
@@ -714,6 +788,7 @@ int oskb_station_beam_aa_types_##S(int num_stations, int num_elements,       \
             el_z, meas_x, meas_y, meas_z, cable_length_error,                \
             element_weight_factors, num_element_types, element_type,         \
             orientation_x_rad, orientation_y_rad, dipole_length_m,           \
+            element_kind, taper_kind, taper_param,                           \
             normalise_element, normalise_array, normalise_final, swap_xy,    \
             is_3d, frequency_hz, beam_enu, norm_enu, num_directions, x, y,   \
             z, directions_per_station, beam, stream);                        \
@@ -723,7 +798,9 @@ int oskb_station_beam_aa_feeds_##S(int num_feeds, int num_stations,        \
         const T* meas_x, const T* meas_y, const T* meas_z,                   \
         const T* cable_length_error, const T* element_weight_factors,        \
         int num_element_types, const int* element_type,                     \
-        const double* dipole_length_m, const double* orientation_x_rad,      \
+        const double* dipole_length_m, const int* element_kind,              \
+        const int* taper_kind, const double* taper_param,                    \
+        const double* orientation_x_rad,                                     \
         const double* orientation_y_rad, int normalise_element,              \
         int normalise_array, int normalise_final, int swap_xy, int is_3d,    \
         double frequency_hz, const double* beam_enu, const double* norm_enu, \
@@ -734,7 +811,8 @@ int oskb_station_beam_aa_feeds_##S(int num_feeds, int num_stations,        \
             num_elements, el_x, el_y, el_z, meas_x, meas_y, meas_z,          \
             cable_length_error, element_weight_factors, num_element_types,   \
             element_type, orientation_x_rad, orientation_y_rad,              \
-            dipole_length_m, normalise_element, normalise_array,             \
+            dipole_length_m, element_kind, taper_kind, taper_param,          \
+            normalise_element, normalise_array,                              \
             normalise_final, swap_xy, is_3d, frequency_hz, beam_enu,         \
             norm_enu, num_directions, x, y, z, directions_per_station, beam, \
             stream);                                                         \
@@ -834,7 +912,7 @@ int station_beam_two_level(int num_tile_types, int num_elements,
     if (int err = station_beam_aa<T>(num_tile_types, num_elements, el_x,
             el_y, el_z, nullptr, nullptr, nullptr, nullptr, nullptr, 1,
             nullptr, orientation_x, orientation_y, &dipole_length_m,
-            normalise_element,
+            nullptr, nullptr, nullptr, normalise_element,
             normalise_tile_array, 0, swap_xy, is_3d, frequency_hz, pointing,
             nullptr, num_directions, x, y, z, 0, tile_beams, stream))
         return err;

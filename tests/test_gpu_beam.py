@@ -126,7 +126,8 @@ def test_jones_r_vs_oracle(real):
 @pytest.mark.parametrize("real", [np.float64, np.float32])
 @pytest.mark.parametrize("num_types", [1, 2, 3, 4])
 @pytest.mark.parametrize("flags", [(1, 1, 1, 0, 1), (0, 0, 1, 1, 0)])
-def test_station_beam_element_types(real, num_types, flags):
+@pytest.mark.parametrize("model", ["dipoles", "isotropic+tapers"])
+def test_station_beam_element_types(real, num_types, flags, model):
     """Stations with several element types, each a dipole length and an
     orientation of its own: one launch for three stations, each with its
     own type map, orientations and weight factors, against the oracle
@@ -139,6 +140,12 @@ def test_station_beam_element_types(real, num_types, flags):
     rng = np.random.default_rng(num_types)
     types = rng.integers(0, num_types, (nst, n)).astype(np.int32)
     lengths = np.array([1.5, 1.1, 2.0, 0.7][:num_types])
+    kinds = tapers = taper_par = None
+    if model == "isotropic+tapers":
+        # type 1 isotropic; cosine taper on type 0, Gaussian on the rest
+        kinds = np.array([0, 1, 0, 0][:num_types], np.int32)
+        tapers = np.array([1, 2, 2, 0][:num_types], np.int32)
+        taper_par = np.array([1.7, 1.2, 0.8, 0.0][:num_types])
     wf = rng.normal(1, 0.1, (nst, 2 * n)).astype(real)
     ori_x = rng.uniform(0, np.pi, (nst, num_types))
     ori_y = ori_x + np.pi / 2 + rng.normal(0, 0.05, (nst, num_types))
@@ -149,7 +156,8 @@ def test_station_beam_element_types(real, num_types, flags):
             *[cat("el", i) for i in range(3)],
             *[cat("meas", i) for i in range(3)],
             dev(np.concatenate([c["cable"] for c in cases])), dev(wf),
-            num_types, dev(types), lengths, dev(ori_x), dev(ori_y), norm_el,
+            num_types, dev(types), lengths, kinds, tapers, taper_par,
+            dev(ori_x), dev(ori_y), norm_el,
             norm_arr, norm_fin, swap, is_3d, cases[0]["freq"],
             dev(np.stack([c["b"] for c in cases])),
             dev(np.stack([c["norm"] for c in cases])), nd,
@@ -161,8 +169,9 @@ def test_station_beam_element_types(real, num_types, flags):
         ref = np.zeros(8 * nd, real)
         oracle().call("station_beam_aa_types_" + suffix(real), np.float64,
                       n, 1, *c["el"], *c["meas"], c["cable"], wf[s].copy(),
-                      num_types, types[s].copy(), lengths,
-                      ori_x[s].copy(), ori_y[s].copy(), norm_el, norm_arr,
+                      num_types, types[s].copy(), lengths, kinds, tapers,
+                      taper_par, ori_x[s].copy(), ori_y[s].copy(), norm_el,
+                      norm_arr,
                       norm_fin, swap, is_3d, c["freq"],
                       *c["b"], *c["norm"], nd, *cases[0]["dirs"], ref)
         assert rel(got[s], ref) <= TOL[real], (s, rel(got[s], ref))
@@ -172,7 +181,8 @@ def test_station_beam_element_types_limits():
     c = beam_case(np.float64, num_el=8, num_dir=5)
     args = lambda nt, lengths: (
         1, 8, *[dev(a) for a in c["el"]], None, None, None, None, None, nt,
-        None, lengths, dev(np.array([0.0])), dev(np.array([1.5])), 0, 0, 0,
+        None, lengths, None, None, None, dev(np.array([0.0])),
+        dev(np.array([1.5])), 0, 0, 0,
         0, 1, 100e6, dev(c["b"]), dev(c["norm"]), 5,
         *[dev(a) for a in c["dirs"]], 0,
         torch.zeros(40, dtype=torch.float64, device="cuda"), None)
@@ -183,6 +193,12 @@ def test_station_beam_element_types_limits():
                    check=False) == -3
     assert ob.call("oskb_station_beam_aa_types_d", *args(1, None),
                    check=False) == -3
+    # a Gaussian taper needs a positive FWHM; kinds and tapers in range
+    bad = list(args(1, np.ones(1)))
+    bad[13], bad[14], bad[15] = None, np.array([2], np.int32), np.zeros(1)
+    assert ob.call("oskb_station_beam_aa_types_d", *bad, check=False) == -3
+    bad[13], bad[14] = np.array([2], np.int32), None
+    assert ob.call("oskb_station_beam_aa_types_d", *bad, check=False) == -3
 
 
 @pytest.mark.parametrize("real", [np.float64, np.float32])
@@ -205,6 +221,7 @@ def test_station_beam_two_feeds(real, num_types, flags):
     lengths = np.array([1.5, 1.1][:num_types])
     ori_x = rng.uniform(0, np.pi, (nst, num_types))
     ori_y = ori_x + np.pi / 2
+    kinds = tapers = taper_par = None
     # feed y: positions moved by up to 5 cm, its own cable errors, factors
     feeds = []
     for c in cases:
@@ -225,7 +242,8 @@ def test_station_beam_two_feeds(real, num_types, flags):
     ob.call("oskb_station_beam_aa_feeds_" + suffix(real), 2, nst, n,
             *[stack("el", i) for i in range(3)],
             *[stack("meas", i) for i in range(3)], cable, dev(wf),
-            num_types, dev(types), lengths, dev(ori_x), dev(ori_y), norm_el,
+            num_types, dev(types), lengths, kinds, tapers, taper_par,
+            dev(ori_x), dev(ori_y), norm_el,
             norm_arr, norm_fin, swap, is_3d, cases[0]["freq"],
             dev(np.stack([c["b"] for c in cases])),
             dev(np.stack([c["norm"] for c in cases])), nd,
@@ -244,7 +262,8 @@ def test_station_beam_two_feeds(real, num_types, flags):
                       *[cat2(c["meas"][i], fy["meas"][i]) for i in range(3)],
                       cat2(c["cable"], fy["cable"]),
                       cat2(wf[0, s], wf[1, s]), num_types, types[s].copy(),
-                      lengths, ori_x[s].copy(), ori_y[s].copy(), norm_el,
+                      lengths, None, None, None, ori_x[s].copy(),
+                      ori_y[s].copy(), norm_el,
                       norm_arr, norm_fin, swap, is_3d, c["freq"], *c["b"],
                       *c["norm"], nd, *cases[0]["dirs"], ref)
         assert rel(got[s], ref) <= TOL[real], (s, rel(got[s], ref))
