@@ -346,6 +346,42 @@ OSKB_API int oskb_station_beam_aa_types_f(int num_stations, int num_elements,
         const float* y, const float* z, int directions_per_station,
         float* beam, void* stream);
 
+/* oskb_station_beam_aa_types in the scalar (Stokes-I) polarisation mode:
+ * each type's pattern is its amplitude sqrt((a^2 + b^2 + c^2 + d^2) / 2)
+ * (the reference's scalar dipole response,
+ * oskar/telescope/station/element/define_evaluate_dipole_pattern.h:51-75;
+ * 1 for isotropic elements), the beam is complex [station][direction] and
+ * the final normalisation divides by its magnitude in the normalisation
+ * direction (oskar/mem/define_mem_normalise.h:13-29). */
+OSKB_API int oskb_station_beam_aa_scalar_d(int num_stations, int num_elements,
+        const double* el_x, const double* el_y, const double* el_z,
+        const double* meas_x, const double* meas_y, const double* meas_z,
+        const double* cable_length_error,
+        const double* element_weight_factors, int num_element_types,
+        const int* element_type, const double* dipole_length_m,
+        const int* element_kind, const int* taper_kind,
+        const double* taper_param,
+        const double* orientation_x_rad, const double* orientation_y_rad,
+        int normalise_element, int normalise_array, int normalise_final,
+        int swap_xy, int is_3d, double frequency_hz, const double* beam_enu,
+        const double* norm_enu, int num_directions, const double* x,
+        const double* y, const double* z, int directions_per_station,
+        double* beam, void* stream);
+OSKB_API int oskb_station_beam_aa_scalar_f(int num_stations, int num_elements,
+        const float* el_x, const float* el_y, const float* el_z,
+        const float* meas_x, const float* meas_y, const float* meas_z,
+        const float* cable_length_error,
+        const float* element_weight_factors, int num_element_types,
+        const int* element_type, const double* dipole_length_m,
+        const int* element_kind, const int* taper_kind,
+        const double* taper_param,
+        const double* orientation_x_rad, const double* orientation_y_rad,
+        int normalise_element, int normalise_array, int normalise_final,
+        int swap_xy, int is_3d, double frequency_hz, const double* beam_enu,
+        const double* norm_enu, int num_directions, const float* x,
+        const float* y, const float* z, int directions_per_station,
+        float* beam, void* stream);
+
 /* oskb_station_beam_aa_types for stations whose two feeds have element
  * data of their own (the reference's num_feeds = 2 when a station is not
  * common_pol_beams: per-feed positions, cable errors, gains, errors or

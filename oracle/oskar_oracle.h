@@ -92,7 +92,7 @@ void orc_station_beam_aa_types_##S(int num_el, int num_feeds, \
         const int* taper_per_type, const double* taper_param_per_type, \
         const double* orientation_x_per_type, \
         const double* orientation_y_per_type, int norm_element, \
-        int norm_array, int norm_final, int swap_xy, int is_3d, \
+        int norm_array, int norm_final, int swap_xy, int scalar, int is_3d, \
         double frequency_hz, double bx, double by, double bz, double nx, \
         double ny, double nz, int num_dir, const REAL* dx, const REAL* dy, \
         const REAL* dz, REAL* beam); \

@@ -680,7 +680,7 @@ void ORC_FN(orc_station_beam_aa_types)(int num_el, int num_feeds,
         const int* taper_per_type, const double* taper_param_per_type,
         const double* orientation_x_per_type,
         const double* orientation_y_per_type, int norm_element,
-        int norm_array, int norm_final, int swap_xy, int is_3d,
+        int norm_array, int norm_final, int swap_xy, int scalar, int is_3d,
         double frequency_hz, double bx, double by, double bz, double nx,
         double ny, double nz, int num_dir, const REAL* dx, const REAL* dy,
         const REAL* dz, REAL* beam)
@@ -799,9 +799,66 @@ void ORC_FN(orc_station_beam_aa_types)(int num_el, int num_feeds,
                 f == 0 || num_feeds == 1, f == 1 || num_feeds == 1, 0, out,
                 norm_array ? (REAL) (1.0 / num_el) : (REAL) 1);
     }
-    ORC_FN(orc_blank_below_horizon)(0, np, Z, 0, out);
-    if (norm_final) ORC_FN(orc_mem_normalise_matrix)(0, np, out, np - 1);
-    for (i = 0; i < 8 * num_dir; ++i) beam[i] = out[i];
+    if (scalar)
+    {
+        /* scalar response: the pattern amplitude sqrt(sum of the four
+         * real terms squared / 2) (define_evaluate_dipole_pattern.h:51-75;
+         * it commutes with the pole normalisation and the taper), a
+         * complex DFT, horizon blanking, and division by the magnitude in
+         * the normalisation direction (define_mem_normalise.h:13-29) */
+        REAL* ssig = (REAL*) calloc((size_t) 2 * np * num_types,
+                sizeof(REAL));
+        for (i = 0; i < np * num_types; ++i)
+        {
+            const REAL* m = signal + 8 * (size_t) i;
+            ssig[2 * i] = ORC_SQRT((m[0] * m[0] + m[2] * m[2] +
+                    m[4] * m[4] + m[6] * m[6]) / 2);
+        }
+        for (i = 0; i < 2 * np; ++i) out[i] = 0;
+        for (f = 0; f < num_feeds; ++f)
+        {
+            const size_t o = (size_t) f * num_el;
+            const REAL* xm = x_meas ? x_meas + o : x + o;
+            const REAL* ym = y_meas ? y_meas + o : y + o;
+            const REAL* zm = z_meas ? z_meas + o : z + o;
+            ORC_FN(orc_element_weights_dft)(num_el, xm, ym, zm, cable + o,
+                    (REAL) wavenumber, (REAL) bx, (REAL) by, (REAL) bz, w);
+            if (weight_factors)
+                for (i = 0; i < num_el; ++i)
+                {
+                    ORC_T(cx) a = {w[2 * i], w[2 * i + 1]};
+                    const ORC_T(cx) fc = {weight_factors[2 * (o + i)],
+                            weight_factors[2 * (o + i) + 1]};
+                    a = ORC_T(cmul)(a, fc);
+                    w[2 * i] = a.re;
+                    w[2 * i + 1] = a.im;
+                }
+            ORC_FN(orc_dftw)(0, is_3d, num_el, (REAL) wavenumber, w, x + o,
+                    y + o, z + o, 0, np, X, Y, is_3d ? Z : 0, types, ssig,
+                    1, 1, 0, out,
+                    norm_array ? (REAL) (1.0 / num_el) : (REAL) 1);
+        }
+        for (i = 0; i < np; ++i)
+            if (Z[i] < 0) out[2 * i] = out[2 * i + 1] = 0;
+        if (norm_final)
+        {
+            const REAL* v = out + 2 * (size_t) (np - 1);
+            const REAL scal = 1 / ORC_SQRT(v[0] * v[0] + v[1] * v[1]);
+            for (i = 0; i < np - 1; ++i)
+            {
+                out[2 * i] *= scal;
+                out[2 * i + 1] *= scal;
+            }
+        }
+        for (i = 0; i < 2 * num_dir; ++i) beam[i] = out[i];
+        free(ssig);
+    }
+    else
+    {
+        ORC_FN(orc_blank_below_horizon)(0, np, Z, 0, out);
+        if (norm_final) ORC_FN(orc_mem_normalise_matrix)(0, np, out, np - 1);
+        for (i = 0; i < 8 * num_dir; ++i) beam[i] = out[i];
+    }
     free(X); free(Y); free(Z); free(theta); free(phi1); free(phi2);
     free(signal); free(pattern); free(out); free(w); free(types);
 }
@@ -819,7 +876,7 @@ void ORC_FN(orc_station_beam_aa_weighted)(int num_el, const REAL* x,
     ORC_FN(orc_station_beam_aa_types)(num_el, 1, x, y, z, x_meas, y_meas,
             z_meas, cable, weight_factors, 1, 0, &dipole_length_m, 0, 0, 0,
             &orientation_x_rad, &orientation_y_rad, norm_element, norm_array,
-            norm_final, swap_xy, is_3d, frequency_hz, bx, by, bz, nx, ny, nz,
+            norm_final, swap_xy, 0, is_3d, frequency_hz, bx, by, bz, nx, ny, nz,
             num_dir, dx, dy, dz, beam);
 }
 

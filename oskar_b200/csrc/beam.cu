@@ -33,6 +33,7 @@ constexpr int kChunk = 512;
 struct BeamFlags
 {
     int normalise_element, normalise_array, normalise_final, swap_xy;
+    int scalar;  // complex beam of the pattern amplitude (Stokes-I mode)
 };
 
 // e^{i ph} for the normalisation direction: ph in table steps through
@@ -158,14 +159,16 @@ station_beam_kernel(int num_elements, const T* __restrict__ el_x,
     const bool active = d < num_dir;
     const size_t el0 = (size_t) st * num_elements;
     const size_t dir0 = directions_per_station ? (size_t) st * num_dir : 0;
-    T2* out = reinterpret_cast<T2*>(beam) + 4 * ((size_t) st * num_dir + d);
+    const int per_dir = flags.scalar ? 1 : 4;
+    T2* out = reinterpret_cast<T2*>(beam) +
+            per_dir * ((size_t) st * num_dir + d);
 
     const T bx = (T) beam_enu[3 * st], by = (T) beam_enu[3 * st + 1],
             bz = (T) beam_enu[3 * st + 2];
     if (beam_enu[3 * st + 2] < 0.0)  // pointing below the horizon
     {
         if (active)
-            for (int k = 0; k < 4; ++k) out[k] = T2{(T) 0, (T) 0};
+            for (int k = 0; k < per_dir; ++k) out[k] = T2{(T) 0, (T) 0};
         return;
     }
     if constexpr (sizeof(T) == 8)
@@ -373,6 +376,24 @@ station_beam_kernel(int num_elements, const T* __restrict__ el_x,
                 }
             }
         }
+        else if (flags.scalar)
+        {
+            // |sum_t amplitude_t AF_t| (define_mem_normalise.h:13-29)
+            T vr = 0, vi = 0;
+#pragma unroll
+            for (int t = 0; t < NT; ++t)
+            {
+                T pn[4];
+                type_pattern<T>(tp, t, nX, nY, nZ, false, dphi1[t],
+                        dphi2[t], flags.swap_xy, pn);
+                const T a = sqrt(half_frobenius<T>(pn, 1, 0)) *
+                        type_taper<T>(tp, t, nX, nY, nZ) * pole_scale[t] *
+                        array_scale;
+                vr += a * nr[t];
+                vi += a * ni[t];
+            }
+            final_scale = (T) 1 / sqrt(vr * vr + vi * vi);
+        }
         else if constexpr (NT == 1)
         {
             T pn[4];
@@ -414,6 +435,26 @@ station_beam_kernel(int num_elements, const T* __restrict__ el_x,
     if (!active) return;
 
     const bool blank = Z < (T) 0;
+    if (flags.scalar)
+    {
+        // pattern amplitude sqrt(sum p_k^2 / 2)
+        // (define_evaluate_dipole_pattern.h:51-75) times the array factor
+        T2 v{(T) 0, (T) 0};
+#pragma unroll
+        for (int t = 0; t < NT; ++t)
+        {
+            T pt[4];
+            type_pattern<T>(tp, t, X, Y, Z, false, dphi1[t], dphi2[t],
+                    flags.swap_xy, pt);
+            const T a = sqrt(half_frobenius<T>(pt, 1, 0)) *
+                    type_taper<T>(tp, t, X, Y, Z) * pole_scale[t];
+            v.x += a * ar[t] * array_scale;
+            v.y += a * ai[t] * array_scale;
+        }
+        if (blank) v = T2{(T) 0, (T) 0};
+        out[0] = T2{v.x * final_scale, v.y * final_scale};
+        return;
+    }
     T p[NT][4];
 #pragma unroll
     for (int t = 0; t < NT; ++t)
@@ -584,7 +625,7 @@ int station_beam_aa(int num_stations, int num_elements, const T* el_x,
         int swap_xy, int is_3d, double frequency_hz, const double* beam_enu,
         const double* norm_enu, int num_directions, const T* x, const T* y,
         const T* z, int directions_per_station, T* beam, void* stream,
-        int rows = 0, T* norm_af = nullptr)
+        int rows = 0, T* norm_af = nullptr, int scalar = 0)
 {
     if (num_stations < 0 || num_elements < 0 || num_directions < 0)
         return OSKB_ERR_INVALID_ARGUMENT;
@@ -601,7 +642,7 @@ int station_beam_aa(int num_stations, int num_elements, const T* el_x,
     const double c0 = 299792458.0;
     const T wavenumber = (T) (2.0 * kPi * frequency_hz / c0);
     BeamFlags flags{normalise_element, normalise_array, normalise_final,
-            swap_xy};
+            swap_xy, scalar};
     dim3 grid((num_directions + kThreads - 1) / kThreads, num_stations);
     cudaStream_t s = as_stream(stream);
 #define OSKB_BEAM(D, NT) station_beam_kernel<T, D, NT><<<grid, kThreads, 0,    \
@@ -692,7 +733,7 @@ int station_beam_aa_feeds(int num_feeds, int num_stations, int num_elements,
     if (!err && normalise_final)
     {
         BeamFlags flags{normalise_element, normalise_array, normalise_final,
-                swap_xy};
+                swap_xy, 0};
         dim3 grid((num_directions + 255) / 256, num_stations);
 #define OSKB_FIN(NT) feeds_finalise_kernel<T, NT><<<grid, 256, 0, s>>>(       \
         num_stations, num_elements, orientation_x, orientation_y, tp, flags, \
@@ -792,6 +833,29 @@ int oskb_station_beam_aa_types_##S(int num_stations, int num_elements,       \
             normalise_element, normalise_array, normalise_final, swap_xy,    \
             is_3d, frequency_hz, beam_enu, norm_enu, num_directions, x, y,   \
             z, directions_per_station, beam, stream);                        \
+}                                                                            \
+int oskb_station_beam_aa_scalar_##S(int num_stations, int num_elements,      \
+        const T* el_x, const T* el_y, const T* el_z, const T* meas_x,        \
+        const T* meas_y, const T* meas_z, const T* cable_length_error,       \
+        const T* element_weight_factors, int num_element_types,              \
+        const int* element_type, const double* dipole_length_m,              \
+        const int* element_kind, const int* taper_kind,                      \
+        const double* taper_param,                                           \
+        const double* orientation_x_rad, const double* orientation_y_rad,    \
+        int normalise_element, int normalise_array, int normalise_final,     \
+        int swap_xy, int is_3d, double frequency_hz,                         \
+        const double* beam_enu, const double* norm_enu, int num_directions,  \
+        const T* x, const T* y, const T* z, int directions_per_station,      \
+        T* beam, void* stream)                                               \
+{                                                                            \
+    return oskb::station_beam_aa<T>(num_stations, num_elements, el_x, el_y,  \
+            el_z, meas_x, meas_y, meas_z, cable_length_error,                \
+            element_weight_factors, num_element_types, element_type,         \
+            orientation_x_rad, orientation_y_rad, dipole_length_m,           \
+            element_kind, taper_kind, taper_param,                           \
+            normalise_element, normalise_array, normalise_final, swap_xy,    \
+            is_3d, frequency_hz, beam_enu, norm_enu, num_directions, x, y,   \
+            z, directions_per_station, beam, stream, 0, nullptr, 1);         \
 }                                                                            \
 int oskb_station_beam_aa_feeds_##S(int num_feeds, int num_stations,        \
         int num_elements, const T* el_x, const T* el_y, const T* el_z,       \

@@ -172,7 +172,7 @@ def test_station_beam_element_types(real, num_types, flags, model):
                       num_types, types[s].copy(), lengths, kinds, tapers,
                       taper_par, ori_x[s].copy(), ori_y[s].copy(), norm_el,
                       norm_arr,
-                      norm_fin, swap, is_3d, c["freq"],
+                      norm_fin, swap, 0, is_3d, c["freq"],
                       *c["b"], *c["norm"], nd, *cases[0]["dirs"], ref)
         assert rel(got[s], ref) <= TOL[real], (s, rel(got[s], ref))
 
@@ -264,6 +264,56 @@ def test_station_beam_two_feeds(real, num_types, flags):
                       cat2(wf[0, s], wf[1, s]), num_types, types[s].copy(),
                       lengths, None, None, None, ori_x[s].copy(),
                       ori_y[s].copy(), norm_el,
-                      norm_arr, norm_fin, swap, is_3d, c["freq"], *c["b"],
+                      norm_arr, norm_fin, swap, 0, is_3d, c["freq"], *c["b"],
                       *c["norm"], nd, *cases[0]["dirs"], ref)
         assert rel(got[s], ref) <= TOL[real], (s, rel(got[s], ref))
+
+
+@pytest.mark.parametrize("real", [np.float64, np.float32])
+@pytest.mark.parametrize("num_types", [1, 3])
+@pytest.mark.parametrize("flags", [(1, 1, 1, 0, 1), (0, 0, 1, 1, 0),
+                                   (1, 1, 0, 0, 0)])
+def test_station_beam_scalar(real, num_types, flags):
+    """The scalar (Stokes-I) mode: each type's pattern amplitude times its
+    array factor, complex beam, normalised by its magnitude in the
+    normalisation direction; three stations, one pointing below the
+    horizon, dipole and isotropic types with tapers."""
+    norm_el, norm_arr, norm_fin, swap, is_3d = flags
+    cases = stations(real, is_3d=is_3d, num_el=180, num_dir=401)
+    cases[2]["b"] = np.array([0.1, 0.2, -np.sqrt(1 - 0.05)])
+    nst, n, nd = len(cases), 180, 401
+    rng = np.random.default_rng(31 + num_types)
+    types = rng.integers(0, num_types, (nst, n)).astype(np.int32)
+    lengths = np.array([1.5, 1.0, 2.1][:num_types])
+    kinds = np.array([0, 1, 0][:num_types], np.int32)
+    tapers = np.array([0, 1, 2][:num_types], np.int32)
+    taper_par = np.array([0.0, 2.0, 1.0][:num_types])
+    ori_x = rng.uniform(0, np.pi, (nst, num_types))
+    ori_y = ori_x + np.pi / 2
+    wf = rng.normal(1, 0.1, (nst, 2 * n)).astype(real)
+    cat = lambda key, i: dev(np.concatenate([c[key][i] for c in cases]))
+    out = torch.zeros(nst * nd * 2, dtype=torch.float64 if real ==
+                      np.float64 else torch.float32, device="cuda")
+    ob.call("oskb_station_beam_aa_scalar_" + suffix(real), nst, n,
+            *[cat("el", i) for i in range(3)],
+            *[cat("meas", i) for i in range(3)],
+            dev(np.concatenate([c["cable"] for c in cases])), dev(wf),
+            num_types, dev(types), lengths, kinds, tapers, taper_par,
+            dev(ori_x), dev(ori_y), norm_el, norm_arr, norm_fin, swap, is_3d,
+            cases[0]["freq"], dev(np.stack([c["b"] for c in cases])),
+            dev(np.stack([c["norm"] for c in cases])), nd,
+            *[dev(cases[0]["dirs"][i]) for i in range(3)], 0, out,
+            ob.stream_ptr())
+    torch.cuda.synchronize()
+    got = out.cpu().numpy().reshape(nst, -1)
+    assert not got[2].any()
+    for s, c in enumerate(cases[:2]):
+        ref = np.zeros(8 * nd, real)
+        oracle().call("station_beam_aa_types_" + suffix(real), np.float64,
+                      n, 1, *c["el"], *c["meas"], c["cable"], wf[s].copy(),
+                      num_types, types[s].copy(), lengths, kinds, tapers,
+                      taper_par, ori_x[s].copy(), ori_y[s].copy(), norm_el,
+                      norm_arr, norm_fin, swap, 1, is_3d, c["freq"], *c["b"],
+                      *c["norm"], nd, *cases[0]["dirs"], ref)
+        assert rel(got[s], ref[:2 * nd]) <= TOL[real], (s, rel(got[s],
+                                                               ref[:2 * nd]))
