@@ -420,6 +420,30 @@ OSKB_API int oskb_station_beam_aa_feeds_f(int num_feeds, int num_stations,
         const float* y, const float* z, int directions_per_station,
         float* beam, void* stream);
 
+/* Beam-pattern power terms for one source of brightness (I, Q, U, V):
+ * auto power out[i + offset_out] = J B J^H of jones[i + offset_in] (|J|^2
+ * for scalar Jones), and cross power out[s + offset_out] =
+ * 2 / (N (N - 1)) sum_{p<q} (J_p B) J_q^H over the N stations of
+ * jones[station][source] (scalar: J_p conj(J_q)); matrix selects 2x2 Jones.
+ * The cross power takes one pass over the stations with running prefix
+ * sums, O(N) per source where the reference loops over pairs. Replace the
+ * kernels behind oskar_evaluate_auto_power and oskar_evaluate_cross_power
+ * (oskar/correlate/oskar_evaluate_{auto,cross}_power.h;
+ * define_evaluate_auto_power.h:3-40, define_evaluate_cross_power.h:3-72). */
+OSKB_API int oskb_evaluate_auto_power_d(int matrix, int n, int offset_in,
+        const double* jones, double src_I, double src_Q, double src_U,
+        double src_V, int offset_out, double* out, void* stream);
+OSKB_API int oskb_evaluate_auto_power_f(int matrix, int n, int offset_in,
+        const float* jones, float src_I, float src_Q, float src_U,
+        float src_V, int offset_out, float* out, void* stream);
+OSKB_API int oskb_evaluate_cross_power_d(int matrix, int num_sources,
+        int num_stations, const double* jones, double src_I, double src_Q,
+        double src_U, double src_V, int offset_out, double* out,
+        void* stream);
+OSKB_API int oskb_evaluate_cross_power_f(int matrix, int num_sources,
+        int num_stations, const float* jones, float src_I, float src_Q,
+        float src_U, float src_V, int offset_out, float* out, void* stream);
+
 /* Time-variable element gain and phase errors of one station:
  * errors[e] = (gain[e] + gain_error[e] g) exp(i (phase[e] + phase_error[e] h))
  * with (g, h) a standard Gaussian pair per element drawn from Philox4x32-10

@@ -126,6 +126,12 @@ void orc_cable_length_errors_##S(int matrix, int num_sources, \
         const REAL* errors_y, REAL* jones); \
 void orc_station_gains_##S(int matrix, int num_sources, int num_stations, \
         const REAL* gains, REAL* jones); \
+void orc_auto_power_##S(int matrix, int n, int offset_in, \
+        const REAL* jones, REAL I, REAL Q, REAL U, REAL V, int offset_out, \
+        REAL* out); \
+void orc_cross_power_##S(int matrix, int num_sources, int num_stations, \
+        const REAL* jones, REAL I, REAL Q, REAL U, REAL V, REAL norm, \
+        int offset_out, REAL* out); \
 void orc_random_gaussian_##S(unsigned int n, REAL* data, unsigned int seed, \
         unsigned int c1, unsigned int c2, unsigned int c3, REAL std); \
 void orc_element_weights_errors_##S(int n, const REAL* gain, \

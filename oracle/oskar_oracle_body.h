@@ -1382,3 +1382,94 @@ void ORC_FN(orc_element_weights_errors)(int n, const REAL* gain,
         errors[2 * i + 1] = ORC_SIN(ph) * re;
     }
 }
+
+/* Beam-pattern auto power of one source's Jones terms: J B J^H, or |J|^2
+ * for scalar Jones (correlate/define_evaluate_auto_power.h:3-40). */
+void ORC_FN(orc_auto_power)(int matrix, int n, int offset_in,
+        const REAL* jones, REAL I, REAL Q, REAL U, REAL V, int offset_out,
+        REAL* out)
+{
+    int i;
+    for (i = 0; i < n; ++i)
+    {
+        if (matrix)
+        {
+            const ORC_T(mat) J = ORC_T(load_mat)(jones + 8 *
+                    (size_t) (i + offset_in));
+            const ORC_T(mat) r = ORC_T(mul_herm)(
+                    ORC_T(mul_brightness)(J, I, Q, U, V), J);
+            REAL* o = out + 8 * (size_t) (i + offset_out);
+            o[0] = r.a.re; o[1] = r.a.im; o[2] = r.b.re; o[3] = r.b.im;
+            o[4] = r.c.re; o[5] = r.c.im; o[6] = r.d.re; o[7] = r.d.im;
+        }
+        else
+        {
+            const REAL* j = jones + 2 * (size_t) (i + offset_in);
+            out[2 * (size_t) (i + offset_out)] = j[0] * j[0] + j[1] * j[1];
+            out[2 * (size_t) (i + offset_out) + 1] = 0;
+        }
+    }
+}
+
+/* Beam-pattern cross power per source: norm sum_{p<q} (J_p B) J_q^H over
+ * station pairs, or sum_{p<q} J_p conj(J_q) for scalar Jones, in the
+ * reference's loop order (correlate/define_evaluate_cross_power.h:3-72;
+ * norm = 2 / (N (N - 1)) from src/oskar_evaluate_cross_power.c:54). */
+void ORC_FN(orc_cross_power)(int matrix, int num_sources, int num_stations,
+        const REAL* jones, REAL I, REAL Q, REAL U, REAL V, REAL norm,
+        int offset_out, REAL* out)
+{
+    int i, p, q;
+    for (i = 0; i < num_sources; ++i)
+    {
+        if (matrix)
+        {
+            ORC_T(mat) sum;
+            REAL* o = out + 8 * (size_t) (i + offset_out);
+            sum.a.re = sum.a.im = sum.b.re = sum.b.im = 0;
+            sum.c.re = sum.c.im = sum.d.re = sum.d.im = 0;
+            for (p = 0; p < num_stations; ++p)
+            {
+                const ORC_T(mat) P = ORC_T(mul_brightness)(ORC_T(load_mat)(
+                        jones + 8 * ((size_t) p * num_sources + i)),
+                        I, Q, U, V);
+                for (q = p + 1; q < num_stations; ++q)
+                {
+                    const ORC_T(mat) Qm = ORC_T(load_mat)(jones + 8 *
+                            ((size_t) q * num_sources + i));
+                    sum.a = ORC_T(cadd)(sum.a, ORC_T(cmulc)(P.a, Qm.a));
+                    sum.a = ORC_T(cadd)(sum.a, ORC_T(cmulc)(P.b, Qm.b));
+                    sum.b = ORC_T(cadd)(sum.b, ORC_T(cmulc)(P.a, Qm.c));
+                    sum.b = ORC_T(cadd)(sum.b, ORC_T(cmulc)(P.b, Qm.d));
+                    sum.c = ORC_T(cadd)(sum.c, ORC_T(cmulc)(P.c, Qm.a));
+                    sum.c = ORC_T(cadd)(sum.c, ORC_T(cmulc)(P.d, Qm.b));
+                    sum.d = ORC_T(cadd)(sum.d, ORC_T(cmulc)(P.c, Qm.c));
+                    sum.d = ORC_T(cadd)(sum.d, ORC_T(cmulc)(P.d, Qm.d));
+                }
+            }
+            o[0] = sum.a.re * norm; o[1] = sum.a.im * norm;
+            o[2] = sum.b.re * norm; o[3] = sum.b.im * norm;
+            o[4] = sum.c.re * norm; o[5] = sum.c.im * norm;
+            o[6] = sum.d.re * norm; o[7] = sum.d.im * norm;
+        }
+        else
+        {
+            ORC_T(cx) sum = {0, 0};
+            for (p = 0; p < num_stations; ++p)
+            {
+                ORC_T(cx) part = {0, 0};
+                const REAL* jp = jones + 2 * ((size_t) p * num_sources + i);
+                const ORC_T(cx) P = {jp[0], jp[1]};
+                for (q = p + 1; q < num_stations; ++q)
+                {
+                    const REAL* jq = jones + 2 * ((size_t) q * num_sources + i);
+                    const ORC_T(cx) Qc = {jq[0], jq[1]};
+                    part = ORC_T(cadd)(part, ORC_T(cmulc)(P, Qc));
+                }
+                sum = ORC_T(cadd)(sum, part);
+            }
+            out[2 * (size_t) (i + offset_out)] = sum.re * norm;
+            out[2 * (size_t) (i + offset_out) + 1] = sum.im * norm;
+        }
+    }
+}

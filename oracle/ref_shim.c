@@ -27,6 +27,8 @@
 #include "convert/define_convert_lon_lat_to_relative_directions.h"
 #include "convert/define_convert_apparent_ra_dec_to_enu_directions.h"
 #include "sky/define_update_horizon_mask.h"
+#include "correlate/define_evaluate_auto_power.h"
+#include "correlate/define_evaluate_cross_power.h"
 
 #define INST(REAL, S, REAL2, REAL4c) \
 OSKAR_ACORR_CPU(k_acorr_##S, REAL, REAL2, REAL4c) \
@@ -209,3 +211,30 @@ void ref_station_gains_##S(int matrix, int num_sources, int num_stations, \
 
 INST_SKY(double, d, double2, double4c)
 INST_SKY(float, f, float2, float4c)
+
+/* Beam-pattern auto and cross power (correlate/define_evaluate_auto_power.h,
+ * define_evaluate_cross_power.h), CPU forms. */
+#define INST_POWER(REAL, S, REAL2, REAL4c) \
+OSKAR_AUTO_POWER_MATRIX(k_auto_power_m_##S, REAL, REAL2, REAL4c) \
+OSKAR_AUTO_POWER_SCALAR(k_auto_power_s_##S, REAL, REAL2) \
+OSKAR_CROSS_POWER_MATRIX(k_cross_power_m_##S, REAL, REAL2, REAL4c) \
+OSKAR_CROSS_POWER_SCALAR(k_cross_power_s_##S, REAL, REAL2) \
+void ref_auto_power_##S(int matrix, int n, int offset_in, const void* jones, \
+        REAL sI, REAL sQ, REAL sU, REAL sV, int offset_out, void* out) \
+{ \
+    if (matrix) k_auto_power_m_##S(n, offset_in, (const REAL4c*) jones, \
+            sI, sQ, sU, sV, offset_out, (REAL4c*) out); \
+    else k_auto_power_s_##S(n, offset_in, (const REAL2*) jones, sI, sQ, sU, sV, \
+            offset_out, (REAL2*) out); \
+} \
+void ref_cross_power_##S(int matrix, int ns, int nst, const void* jones, \
+        REAL sI, REAL sQ, REAL sU, REAL sV, REAL norm, int offset_out, \
+        void* out) \
+{ \
+    if (matrix) k_cross_power_m_##S(ns, nst, (const REAL4c*) jones, sI, sQ, \
+            sU, sV, norm, offset_out, (REAL4c*) out); \
+    else k_cross_power_s_##S(ns, nst, (const REAL2*) jones, sI, sQ, sU, \
+            sV, norm, offset_out, (REAL2*) out); \
+}
+INST_POWER(double, d, double2, double4c)
+INST_POWER(float, f, float2, float4c)

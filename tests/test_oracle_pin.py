@@ -402,3 +402,23 @@ def test_element_weights_errors(real):
         assert np.array_equal(a, b)
         amp = np.hypot(a[0::2], a[1::2])
         assert np.all(np.abs(amp - gain) <= 6 * gain_err + 1e-6)
+
+
+@pytest.mark.parametrize("real", [np.float64, np.float32])
+@pytest.mark.parametrize("matrix", [True, False])
+def test_beam_pattern_powers(real, matrix):
+    """Beam-pattern auto and cross power: oracle against the reference's
+    own CPU kernels (define_evaluate_{auto,cross}_power.h)."""
+    rng = np.random.default_rng(21)
+    nst, nsrc, w = 23, 97, 8 if matrix else 2
+    J = rng.normal(size=nst * nsrc * w).astype(real)
+    stokes = (1.0, 0.2, -0.1, 0.05)
+    for name, args in (("auto_power_", (int(matrix), nst * nsrc, 0, J,
+                                        *stokes, 3)),
+                       ("cross_power_", (int(matrix), nsrc, nst, J, *stokes,
+                                         2.0 / (nst * (nst - 1)), 3))):
+        n_out = (nst * nsrc if name == "auto_power_" else nsrc) + 3
+        a, b = np.zeros(n_out * w, real), np.zeros(n_out * w, real)
+        oracle().call(name + suffix(real), real, *args, a)
+        reference().call(name + suffix(real), real, *args, b)
+        assert _close(a, b, real)
