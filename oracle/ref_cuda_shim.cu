@@ -85,3 +85,30 @@ extern "C" int ref_cuda_dftw_##S(int matrix, int is_3d, int num_in,          \
 
 REF_DFTW_LAUNCHER(double, double, double2)
 REF_DFTW_LAUNCHER(float, float, float2)
+
+// The reference's GPU beam-pattern cross-power kernel
+// (correlate/define_evaluate_cross_power.h, instantiated for CUDA by
+// correlate/src/oskar_evaluate_cross_power.c:41-42) with the reference's
+// launch: one thread per source, blocks of 64 (FP64) or 128 (FP32)
+// threads (oskar_evaluate_cross_power.c:109-131).
+#include "math/define_multiply.h"
+#include "correlate/define_correlate_utils.h"
+#include "correlate/define_evaluate_cross_power.h"
+
+OSKAR_CROSS_POWER_MATRIX(ref_k_cross_power_double, double, double2, double4c)
+OSKAR_CROSS_POWER_MATRIX(ref_k_cross_power_float, float, float2, float4c)
+
+#define REF_CROSS_POWER_LAUNCHER(S, FP, FP4c, BLOCK)                          \
+extern "C" int ref_cuda_cross_power_##S(int num_sources, int num_stations,  \
+        const void* jones, FP src_I, FP src_Q, FP src_U, FP src_V, FP norm,  \
+        int offset_out, void* out, void* stream)                             \
+{                                                                            \
+    if (num_sources <= 0) return 0;                                          \
+    const int grid = (num_sources + BLOCK - 1) / BLOCK;                      \
+    ref_k_cross_power_##S<<<grid, BLOCK, 0, (cudaStream_t) stream>>>(        \
+            num_sources, num_stations, (const FP4c*) jones, src_I, src_Q,    \
+            src_U, src_V, norm, offset_out, (FP4c*) out);                    \
+    return (int) cudaGetLastError();                                         \
+}
+REF_CROSS_POWER_LAUNCHER(double, double, double4c, 64)
+REF_CROSS_POWER_LAUNCHER(float, float, float4c, 128)
