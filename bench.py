@@ -399,7 +399,10 @@ def run_ours(args):
             "gpu_launches": launches_per_step * args.steps,
             "roofline": roof, "clocks": clk,
             "direct_fp64": cmp_["direct"],
+            "direct_fp64_dmma": cmp_["direct_dmma"],
             "speedup_vs_direct_fp64": value / cmp_["direct"]["value"],
+            "speedup_vs_direct_fp64_dmma":
+                value / cmp_["direct_dmma"]["value"],
             "rel_err_vs_fp64": cmp_["err"],
         }
     # ---- end to end through the host-buffer entry point
@@ -417,56 +420,101 @@ def run_ours(args):
 
 def compare_direct(args, cfg, ob, torch, dev, E, l, m, n, I, Q, U, V,
                    uvw_all, inv_wl, stream):
-    """FP64 direct kernel on dump 0, channel 0: its throughput, and the
-    tensor-core result's error against it (L2 relative and max |err| /
-    max |V|)."""
+    """The FP64 direct comparison: throughput of the FP64 direct kernels on
+    one (dump, channel) at the full sky (the SIMT kernel, the plain form,
+    and the default FP64 tensor-pipe DMMA kernel), and the tensor-core
+    result's error against the FP64 direct result on dumps 0 and last,
+    channels 0, 7 and 15: L2 relative and max |err| / max |V|, the worst
+    over those six (dump, channel) problems."""
     nst, nsrc, nbl = cfg.num_st, cfg.num_src, cfg.num_baselines
-    f = float(cfg.freqs_hz[0])
-    u, v, w = uvw_all[0]
+    nch = len(cfg.freqs_hz)
     Ed = E.double()
     K = torch.empty((nst, nsrc, 2), dtype=torch.float64, device="cuda")
     J = torch.empty((nst, nsrc, 8), dtype=torch.float64, device="cuda")
-    ob.call("oskb_evaluate_jones_K_d", nsrc, l, m, n, nst, u, v, w,
-            2 * math.pi * f / 299792458.0, I, 0.0, 1e300, 0, K, stream)
-    ob.call("oskb_mem_multiply_d", 3, 0, 0, 0, nst * nsrc, K, Ed, J, stream)
-    del Ed
     z = torch.zeros(nst, dtype=torch.float64, device="cuda")
     vd = torch.zeros((nbl, 8), dtype=torch.float64, device="cuda")
 
-    def direct():
+    def join(d, c):
+        u, v, w = uvw_all[d]
+        f = float(cfg.freqs_hz[c])
+        ob.call("oskb_evaluate_jones_K_d", nsrc, l, m, n, nst, u, v, w,
+                2 * math.pi * f / 299792458.0, I, 0.0, 1e300, 0, K, stream)
+        ob.call("oskb_mem_multiply_d", 3, 0, 0, 0, nst * nsrc, K, Ed, J,
+                stream)
+
+    def direct(d, c):
+        u, v, w = uvw_all[d]
+        f = float(cfg.freqs_hz[c])
         ob.call("oskb_cross_correlate_d", 0, 0, nsrc, nst, 0, J, I, Q, U, V,
                 l, m, n, None, None, None, u, v, w, z, z, 0.0, 3e38,
                 f / 299792458.0, 0.0, 0.0, 0.0, 0.0, vd, stream)
-    direct()
-    torch.cuda.synchronize()
-    e0 = torch.cuda.Event(enable_timing=True)
-    e1 = torch.cuda.Event(enable_timing=True)
-    reps = 3
-    e0.record()
-    for _ in range(reps):
-        direct()
-    e1.record()
-    torch.cuda.synchronize()
-    ms = e0.elapsed_time(e1) / reps
-    vd.zero_()
-    direct()
+
+    def timed(kernel_env):
+        old = os.environ.get("OSKB_XCORR_DMMA")
+        os.environ["OSKB_XCORR_DMMA"] = kernel_env
+        try:
+            direct(0, 0)
+            torch.cuda.synchronize()
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            reps = 3
+            e0.record()
+            for _ in range(reps):
+                direct(0, 0)
+            e1.record()
+            torch.cuda.synchronize()
+            return e0.elapsed_time(e1) / reps
+        finally:
+            if old is None:
+                del os.environ["OSKB_XCORR_DMMA"]
+            else:
+                os.environ["OSKB_XCORR_DMMA"] = old
+
+    join(0, 0)
+    ms_simt = timed("0")
+    ms_dmma = timed("1")
+    # errors of the tensor-core block against the FP64 direct result
+    worst_l2, worst_mx, cases = 0.0, 0.0, []
+    dumps = (0, cfg.num_times - 1)
+    chans = sorted({0, min(7, nch - 1), nch - 1})
     vt = torch.zeros((1, nbl, 8), dtype=torch.float64, device="cuda")
-    ob.call("oskb_correlate_block_tc", 0, nsrc, nst, 1, 1, E, l, m, n, I, Q,
-            U, V, uvw_all[0], inv_wl[0:1], 0.0, 3e38, vt, None, 0, stream)
-    torch.cuda.synchronize()
-    a = vt[0].cpu().numpy()
-    b = vd.cpu().numpy()
-    err = {"l2": float(np.linalg.norm(a - b) / np.linalg.norm(b)),
-           "max_over_max": float(np.max(np.abs(a - b)) / np.max(np.abs(b))),
-           "sample": "dump 0, channel 0 (100 MHz): all 130,816 baselines x "
-                     "4 pols; reference = FP64 direct kernel on the same "
-                     "inputs"}
-    direct_v = nbl * nsrc / (ms * 1e-3) / 1e9
-    del J, K
+    for d in dumps:
+        for c in chans:
+            join(d, c)
+            vd.zero_()
+            direct(d, c)
+            vt.zero_()
+            ob.call("oskb_correlate_block_tc", 0, nsrc, nst, 1, 1, E, l, m,
+                    n, I, Q, U, V, uvw_all[d], inv_wl[c:c + 1], 0.0, 3e38, vt,
+                    None, 0, stream)
+            torch.cuda.synchronize()
+            a = vt[0].cpu().numpy()
+            b = vd.cpu().numpy()
+            l2 = float(np.linalg.norm(a - b) / np.linalg.norm(b))
+            mx = float(np.max(np.abs(a - b)) / np.max(np.abs(b)))
+            cases.append({"dump": d, "channel": c, "l2": l2,
+                          "max_over_max": mx})
+            worst_l2, worst_mx = max(worst_l2, l2), max(worst_mx, mx)
+    err = {"l2": worst_l2, "max_over_max": worst_mx, "cases": cases,
+           "sample": "worst over dumps %s x channels %s: all 130,816 "
+                     "baselines x 4 pols each; reference = FP64 direct "
+                     "kernel on the same inputs (E upcast from FP32)"
+                     % (list(dumps), chans)}
+    del J, K, Ed
     torch.cuda.empty_cache()
-    return {"direct": {"value": direct_v, "unit": UNIT,
-                       "kernel": "oskb direct FP64 cross-correlation",
-                       "ms_per_channel": ms}, "err": err}
+    sb = nbl * nsrc
+    return {"direct": {"value": sb / (ms_simt * 1e-3) / 1e9, "unit": UNIT,
+                       "kernel": "oskb xcorr_direct_kernel<double> (SIMT "
+                                 "FP64, the plain direct form; "
+                                 "OSKB_XCORR_DMMA=0)",
+                       "ms_per_channel": ms_simt},
+            "direct_dmma": {"value": sb / (ms_dmma * 1e-3) / 1e9,
+                            "unit": UNIT,
+                            "kernel": "oskb xcorr_dmma_kernel (FP64 on the "
+                                      "tensor pipe, DMMA; the default FP64 "
+                                      "point-source kernel)",
+                            "ms_per_channel": ms_dmma},
+            "err": err}
 
 
 def run_e2e(args, cfg, ob, torch, E, world, rank):
@@ -1123,6 +1171,49 @@ def cpu_baseline(cfg):
                       "cross-correlation, %.1f s)" % (nsrc, dt)}
 
 
+def run_dry(args):
+    """The multi-rank plumbing of the default workload without a GPU: gloo
+    process group, each rank's dumps and host-side inputs for warm-up and
+    timed steps, barriers around the timed region and the maximum of the
+    ranks' times. No kernel runs, so no throughput is reported."""
+    import datetime
+    import torch.distributed as dist
+    from oskar_b200 import workloads
+    from oskar_b200.sharding import max_over_ranks, rank_dump_uvw
+    world, rank, _ = dist_setup()
+    if world > 1:
+        dist.init_process_group("gloo", timeout=datetime.timedelta(
+            seconds=60))
+    cfg = workloads.c3(num_src=1000)
+    rank_dump_uvw(cfg, world, rank, args.warmup)
+    if world > 1:
+        dist.barrier()
+    t0 = time.perf_counter()
+    uvw, dumps = rank_dump_uvw(cfg, world, rank, args.steps, args.warmup)
+    dt = time.perf_counter() - t0
+    if world > 1:
+        dist.barrier()
+    dt = max_over_ranks(dt)
+    all_dumps = [None] * world
+    if world > 1:
+        dist.all_gather_object(all_dumps, dumps)
+    else:
+        all_dumps = [dumps]
+    if rank == 0:
+        print(json.dumps({
+            "metric": METRIC, "value": None, "unit": UNIT, "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "dry_run": True,
+            "scaling": "weak", "host_seconds_max_over_ranks": dt,
+            "dumps_per_rank": all_dumps,
+            "config": {"workload": "c3 plumbing only (no kernels)",
+                       "parallelism": "dumps sharded over %d rank(s)"
+                                      % world}}))
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -1142,7 +1233,20 @@ def main():
                              "beam_small",
                              "block_small"],
                     help="run one small kernel case for an ncu capture")
+    ap.add_argument("--dry-run", action="store_true",
+                    help="CPU-only check of the multi-rank plumbing (gloo, "
+                         "no kernels): rank start-up, dump sharding, the "
+                         "host-side inputs of each rank's steps, barriers "
+                         "and the max-over-ranks time; prints a JSON line "
+                         "with n_gpus and no throughput")
     args = ap.parse_args()
+    if args.gpus > 1 and "WORLD_SIZE" not in os.environ:
+        # one process per GPU, started here when no launcher did it
+        from oskar_b200.sharding import spawn_ranks
+        return spawn_ranks([sys.executable, os.path.abspath(__file__)] +
+                           sys.argv[1:], args.gpus)
+    if args.dry_run:
+        return run_dry(args)
     if args.profile_case:
         return run_profile_case(args)
     if args.workload == "c5":

@@ -951,6 +951,18 @@ OSKB_API int oskb_correlate_block_tc(int use_casa_phase_convention,
         const double* station_uvw, const double* inv_wavelength,
         double uv_min_lambda, double uv_max_lambda, double* vis,
         void* workspace, size_t workspace_bytes, void* stream);
+/* The same with E in FP64 [station][source][2x2] (an FP64 caller's Jones E
+ * or R E as it comes, e.g. oskar_Jones of type OSKAR_DOUBLE_COMPLEX_MATRIX):
+ * each entry is rounded to FP32 once on load before the FP16 hi/lo split,
+ * and that rounding (2^-24 relative) is part of the stated 1e-6 error
+ * against the FP64 chain. */
+OSKB_API int oskb_correlate_block_tc_d(int use_casa_phase_convention,
+        int num_sources, int num_stations, int num_times, int num_channels,
+        const double* E, const double* l, const double* m, const double* n,
+        const double* I, const double* Q, const double* U, const double* V,
+        const double* station_uvw, const double* inv_wavelength,
+        double uv_min_lambda, double uv_max_lambda, double* vis,
+        void* workspace, size_t workspace_bytes, void* stream);
 /* The same, with the auto-correlations of every station from the same
  * contraction: the diagonal station pairs of the diagonal tiles are
  * V_pp = J_p B J_p^H, added into autos [num_times][num_channels]
@@ -999,18 +1011,20 @@ OSKB_API int oskb_tc_timing_read(double* total_ms, int* launches);
  * scratch from a 64 MiB array that the library declares in device memory
  * (held by every GPU that loads the library until the process exits), and
  * calls no cudaMalloc, cudaFree or allocating library routine.
- *  - Limit: 16 bytes per station-source after rounding up to 32 stations x
- *    32 sources, plus 256 bytes (e.g. 512 stations x 8,160 sources). Larger
- *    calls return OSKB_ERR_OUT_OF_RANGE (-5) with the sizes in
- *    oskb_last_error(); split the sources into chunks, since vis is
- *    accumulated.
+ *  - Limit: 32 bytes per station-source after rounding up to blocks of 32
+ *    stations x 32 sources, plus 256 bytes (e.g. 512 stations x 4,064
+ *    sources; 4,096 sources do not fit). Larger calls return
+ *    OSKB_ERR_OUT_OF_RANGE (-5) with the sizes in oskb_last_error(); split
+ *    the sources into chunks, since vis is accumulated.
  *  - The first call on a device takes the array's device address
  *    (cudaGetSymbolAddress, with that device current); make that first call
  *    before any stream capture.
  *  - Every call shares the one array: calls whose work overlaps on the GPU
  *    (different streams without ordering between them, or several host
  *    threads) race and corrupt each other's results. Order them, for example
- *    on one stream. oskb_tc_status() does not read this array. */
+ *    on one stream.
+ *  - oskb_tc_status() does not read this array: oskb_tc_noalloc_status()
+ *    does (below). */
 OSKB_API int oskb_cross_correlate_tc_noalloc_d(int use_casa_phase_convention,
         int num_sources, int num_stations, int offset_out,
         const double* jones, const double* I, const double* Q,
@@ -1018,8 +1032,17 @@ OSKB_API int oskb_cross_correlate_tc_noalloc_d(int use_casa_phase_convention,
         const double* station_v, double uv_min_lambda, double uv_max_lambda,
         double inv_wavelength, double* vis, void* stream);
 
+/* Status words of the last oskb_cross_correlate_tc_noalloc_d call on the
+ * current device (no counterpart in the reference), read from the header of
+ * the library's static scratch array without allocating: flags bit 0 = a
+ * brightness matrix was not positive semi-definite; wait_error != 0 = a
+ * bounded device-side wait expired, so that call's visibilities are
+ * incomplete. Synchronises with the device. */
+OSKB_API int oskb_tc_noalloc_status(int* flags, int* wait_error);
+
 /* Status words of the last tensor-core call that used this workspace (NULL:
- * the library-kept one; synchronises with the device): flags bit 0 = a
+ * the library-kept workspace used last on the current device, each host
+ * stream having its own; synchronises with the device): flags bit 0 = a
  * brightness matrix was not positive semi-definite; wait_error != 0 = a
  * bounded device-side wait expired (the call's result is invalid). */
 OSKB_API int oskb_tc_status(const void* workspace, int* flags,

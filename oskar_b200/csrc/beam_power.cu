@@ -290,18 +290,7 @@ __global__ void __launch_bounds__(kThreads) cross_power_combine_kernel(
     }
 }
 
-int num_sms()
-{
-    static int n = 0;
-    if (!n)
-    {
-        int dev = 0;
-        cudaGetDevice(&dev);
-        cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev);
-        if (n <= 0) n = 148;
-    }
-    return n;
-}
+int num_sms() { return device_sm_count(); }
 
 int grid_for(long long n)
 {

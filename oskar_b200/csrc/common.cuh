@@ -31,6 +31,11 @@ inline int check_launch(const char* where)
 
 inline cudaStream_t as_stream(void* s) { return (cudaStream_t) s; }
 
+// Current device (-1 if none) and its SM count, cached per device
+// (scratch.cu); safe to call from several host threads.
+int current_device();
+int device_sm_count();
+
 // Stream-ordered temporaries from the library's own memory pool, which
 // keeps freed blocks across host synchronisations (scratch.cu).
 cudaError_t scratch_alloc(void** ptr, size_t bytes, cudaStream_t stream);

@@ -205,18 +205,7 @@ dftw_kernel(int num_in, T wavenumber, const T* __restrict__ weights_in,
     }
 }
 
-int num_sms()
-{
-    static int n = 0;
-    if (!n)
-    {
-        int dev = 0;
-        cudaGetDevice(&dev);
-        cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev);
-        if (n <= 0) n = 148;
-    }
-    return n;
-}
+int num_sms() { return device_sm_count(); }
 
 // Number of element slices: grow the cluster while the direction grid is
 // below about 8 CTAs (32 warps) per SM and each slice keeps at least

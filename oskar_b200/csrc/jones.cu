@@ -25,14 +25,7 @@ namespace {
 
 int grid_for(size_t n, int threads)
 {
-    static int num_sms = 0;
-    if (!num_sms)
-    {
-        int dev = 0;
-        cudaGetDevice(&dev);
-        cudaDeviceGetAttribute(&num_sms, cudaDevAttrMultiProcessorCount, dev);
-        if (num_sms <= 0) num_sms = 148;
-    }
+    const int num_sms = device_sm_count();
     size_t blocks = (n + threads - 1) / threads;
     const size_t cap = (size_t) num_sms * 16;
     if (blocks > cap) blocks = cap;

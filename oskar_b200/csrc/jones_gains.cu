@@ -31,15 +31,7 @@ __device__ __forceinline__ void m_sincos(double x, double* s, double* c)
 // several), y strides over stations.
 dim3 row_grid(int num_sources, int num_stations)
 {
-    static int num_sms = 0;
-    if (!num_sms)
-    {
-        int dev = 0;
-        cudaGetDevice(&dev);
-        cudaDeviceGetAttribute(&num_sms, cudaDevAttrMultiProcessorCount,
-                dev);
-        if (num_sms <= 0) num_sms = 148;
-    }
+    const int num_sms = device_sm_count();
     int gx = (num_sources + kThreads - 1) / kThreads;
     int gy = num_stations < 65535 ? num_stations : 65535;
     const long long cap = (long long) num_sms * 8;

@@ -7,6 +7,9 @@
 // fresh pages each time. The library keeps its own pool per device whose
 // release threshold holds up to kRetainBytes across synchronisations;
 // oskb_scratch_release() hands the cached blocks back.
+#include <atomic>
+#include <mutex>
+
 #include "common.cuh"
 
 namespace oskb {
@@ -15,7 +18,12 @@ namespace {
 constexpr int kMaxDevices = 64;
 constexpr unsigned long long kRetainBytes = 4ULL << 30;
 
+// Pools and SM counts are per device: one process may drive several GPUs
+// from several host threads (one per device, as the reference's simulator
+// does), so the tables are filled under a lock.
+std::mutex g_pool_mutex;
 cudaMemPool_t g_pool[kMaxDevices] = {};
+std::atomic<int> g_sms[kMaxDevices];
 
 cudaMemPool_t pool_for_current_device()
 {
@@ -25,6 +33,7 @@ cudaMemPool_t pool_for_current_device()
         cudaGetLastError();
         return nullptr;
     }
+    std::lock_guard<std::mutex> lock(g_pool_mutex);
     if (!g_pool[dev])
     {
         cudaMemPoolProps props = {};
@@ -46,6 +55,33 @@ cudaMemPool_t pool_for_current_device()
 
 }  // namespace
 
+int current_device()
+{
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess)
+    {
+        cudaGetLastError();
+        return -1;
+    }
+    return dev;
+}
+
+int device_sm_count()
+{
+    const int dev = current_device();
+    if (dev < 0 || dev >= kMaxDevices) return 148;
+    int n = g_sms[dev].load(std::memory_order_relaxed);
+    if (n > 0) return n;
+    if (cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev) !=
+            cudaSuccess || n <= 0)
+    {
+        cudaGetLastError();
+        return 148;
+    }
+    g_sms[dev].store(n, std::memory_order_relaxed);
+    return n;
+}
+
 cudaError_t scratch_alloc(void** ptr, size_t bytes, cudaStream_t stream)
 {
     cudaMemPool_t p = pool_for_current_device();
@@ -62,6 +98,7 @@ cudaError_t scratch_free(void* ptr, cudaStream_t stream)
 
 extern "C" int oskb_scratch_release(void)
 {
+    std::lock_guard<std::mutex> lock(oskb::g_pool_mutex);
     for (int d = 0; d < oskb::kMaxDevices; ++d)
     {
         if (!oskb::g_pool[d]) continue;

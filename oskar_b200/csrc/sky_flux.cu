@@ -266,15 +266,7 @@ __global__ void __launch_bounds__(256) scale_flux_kernel(int num_sources,
 
 int flux_grid(long long n)
 {
-    static int num_sms = 0;
-    if (!num_sms)
-    {
-        int dev = 0;
-        cudaGetDevice(&dev);
-        cudaDeviceGetAttribute(&num_sms, cudaDevAttrMultiProcessorCount,
-                dev);
-        if (num_sms <= 0) num_sms = 148;
-    }
+    const int num_sms = device_sm_count();
     long long blocks = (n + 255) / 256;
     const long long cap = (long long) num_sms * 8;
     if (blocks > cap) blocks = cap;

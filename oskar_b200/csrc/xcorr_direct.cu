@@ -1018,15 +1018,7 @@ reduce_partials_kernel(const double* __restrict__ partial, int num_slices,
     *out = (T) ((double) *out + sum);
 }
 
-int num_sms()
-{
-    int dev = 0, n = 0;
-    if (cudaGetDevice(&dev) != cudaSuccess ||
-            cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev)
-            != cudaSuccess || n <= 0)
-        return 148;
-    return n;
-}
+int num_sms() { return device_sm_count(); }
 
 template <typename T, bool MATRIX, bool GAUSS, bool BW, bool TS, bool CASA,
         bool FUSED>

@@ -29,6 +29,8 @@
 // one 32 KB bulk copy per operand.
 #include <cuda_fp16.h>
 
+#include <atomic>
+#include <mutex>
 #include <utility>
 #include <vector>
 
@@ -239,15 +241,17 @@ __global__ void __launch_bounds__(256) prep_jones_kernel(
 // Fused operand image: A = K (E C) with the interferometer phase
 //   K_p(s) = exp(2 pi i x),  x = (u_p l + v_p m + w_p (n - 1)) / lambda,
 // x formed in FP64 and reduced to [-1/2, 1/2] before an FP32 sincospi.
-// E is FP32 [station][source][2x2], shared by every problem. Problems are
+// E is FP32 or FP64 [station][source][2x2] (rounded to FP32 on load, then
+// split into the 22-bit FP16 hi/lo pair), shared by every problem. Problems are
 // (time, channel) pairs, prob = t * nch + c: station (u, v, w) of time t at
 // uvw[t][3][num_st], 1/lambda of channel c. One launch writes the images of
 // problems [p0, p0 + np) (image prob - p0 at W + (prob - p0) * image_stride),
 // reading E and forming E C once per station-source for all of them.
 // grid (k blocks, row blocks); 8 warps, warp = 4 stations, lane = source.
 // ---------------------------------------------------------------------------
+template <typename TE>
 __global__ void __launch_bounds__(256) prep_fused_kernel(
-        const float* __restrict__ E, int num_src, int num_st,
+        const TE* __restrict__ E, int num_src, int num_st,
         const double* __restrict__ l, const double* __restrict__ m,
         const double* __restrict__ n, const double* __restrict__ I,
         const double* __restrict__ Q, const double* __restrict__ U,
@@ -278,7 +282,7 @@ __global__ void __launch_bounds__(256) prep_fused_kernel(
         if (ok)
         {
             float J[8];
-            load_jones<float>(E + 8 * ((size_t) p * num_src + s), J);
+            load_jones<TE>(E + 8 * ((size_t) p * num_src + s), J);
             apply_factor(J, c11, c21r, c21i, c22, A0);
 #pragma unroll
             for (int k = 0; k < 8; ++k) (&A0[0][0][0])[k] *= S;
@@ -1104,18 +1108,7 @@ struct Header
     int err;     // non-zero: a bounded wait expired (code of the wait)
 };
 
-int num_sms()
-{
-    static int n = 0;
-    if (!n)
-    {
-        int dev = 0;
-        cudaGetDevice(&dev);
-        cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev);
-        if (n <= 0) n = 148;
-    }
-    return n;
-}
+int num_sms() { return device_sm_count(); }
 
 int drain_kblocks()
 {
@@ -1130,7 +1123,7 @@ int drain_kblocks()
 }
 
 // Problems per group when the library keeps the workspace (each problem's
-// operand image is 16 bytes per station-source).
+// operand image is 32 bytes per station-source).
 int max_group()
 {
     static int g = 0;
@@ -1143,40 +1136,64 @@ int max_group()
     return g;
 }
 
-// Library-managed workspace, one per device, grown on demand.
+// Library-kept workspaces, one per (device, stream), grown on demand. A
+// workspace is only ever used by work on its own stream, so growing it
+// (which first waits for that stream) cannot pull memory from under work
+// queued on another stream or by another host thread.
 struct CachedWorkspace
 {
-    void* ptr = nullptr;
-    size_t bytes = 0;
+    int dev;
+    cudaStream_t stream;
+    void* ptr;
+    size_t bytes;
 };
-CachedWorkspace g_ws[64];
+std::mutex g_ws_mutex;
+std::vector<CachedWorkspace> g_ws;
+void* g_ws_last[64] = {};   // last library-kept workspace used per device
 
-int get_workspace(void*& ws, size_t& ws_bytes, size_t need)
+int get_workspace(void*& ws, size_t& ws_bytes, size_t need,
+        cudaStream_t stream)
 {
     if (ws)
         return ws_bytes >= need ? 0 : OSKB_ERR_MEMORY_ALLOC_FAILURE;
-    int dev = 0;
-    cudaGetDevice(&dev);
+    const int dev = current_device();
     if (dev < 0 || dev >= 64) return OSKB_ERR_INVALID_ARGUMENT;
-    CachedWorkspace& c = g_ws[dev];
-    if (c.bytes < need)
+    std::lock_guard<std::mutex> lock(g_ws_mutex);
+    CachedWorkspace* c = nullptr;
+    for (auto& w : g_ws)
+        if (w.dev == dev && w.stream == stream) c = &w;
+    if (!c)
     {
-        if (c.ptr) cudaFree(c.ptr);
-        c.ptr = nullptr;
-        c.bytes = 0;
-        if (cudaMalloc(&c.ptr, need) != cudaSuccess)
+        g_ws.push_back(CachedWorkspace{dev, stream, nullptr, 0});
+        c = &g_ws.back();
+    }
+    if (c->bytes < need)
+    {
+        if (c->ptr)
         {
+            cudaStreamSynchronize(stream);
+            cudaFree(c->ptr);
+        }
+        c->ptr = nullptr;
+        c->bytes = 0;
+        if (cudaMalloc(&c->ptr, need) != cudaSuccess)
+        {
+            c->ptr = nullptr;
             set_last_error("tc workspace", cudaGetLastError());
             return OSKB_ERR_MEMORY_ALLOC_FAILURE;
         }
-        c.bytes = need;
+        c->bytes = need;
     }
-    ws = c.ptr;
-    ws_bytes = c.bytes;
+    ws = c->ptr;
+    ws_bytes = c->bytes;
+    g_ws_last[dev] = c->ptr;
     return 0;
 }
 
-// Optional CUDA-event timing of every GEMM launch (for roofline reports).
+// Optional CUDA-event timing of every GEMM launch (for roofline reports),
+// guarded by a lock so that launches from several host threads are all
+// recorded.
+std::mutex g_timing_mutex;
 bool g_timing = false;
 std::vector<std::pair<cudaEvent_t, cudaEvent_t>> g_ev;
 size_t g_ev_used = 0;
@@ -1191,59 +1208,84 @@ int tile_setting()
     return (t == 128 || t == 256) ? t : 0;
 }
 
-int g_last_tile = 0;
+std::atomic<int> g_last_tile{0};
+
+// Per-device launch set-up: the dynamic shared-memory opt-in of both
+// contraction kernels (a per-device attribute) and whether the wide
+// kernel's register split fits the registers its blocks are launched with
+// (kWLowRegs / kWHighRegs against the compiled count; otherwise the
+// epilogue's request would never be granted).
+struct DeviceSetup
+{
+    bool done;
+    bool wide_fits;
+};
+std::mutex g_setup_mutex;
+DeviceSetup g_setup[64] = {};
+
+int device_setup(bool& wide_fits)
+{
+    const int dev = current_device();
+    if (dev < 0 || dev >= 64) return OSKB_ERR_CUDA_NOT_AVAILABLE;
+    std::lock_guard<std::mutex> lock(g_setup_mutex);
+    DeviceSetup& d = g_setup[dev];
+    if (!d.done)
+    {
+        if (cudaFuncSetAttribute(gemm_kernel,
+                cudaFuncAttributeMaxDynamicSharedMemorySize,
+                (int) gemm_smem_bytes()) != cudaSuccess ||
+                cudaFuncSetAttribute(gemm_wide_kernel,
+                cudaFuncAttributeMaxDynamicSharedMemorySize,
+                (int) gemm_wide_smem_bytes()) != cudaSuccess)
+        {
+            set_last_error("tc gemm attributes", cudaGetLastError());
+            return OSKB_ERR_KERNEL_LAUNCH_FAILURE;
+        }
+        cudaFuncAttributes fa;
+        d.wide_fits = cudaFuncGetAttributes(&fa, gemm_wide_kernel) ==
+                cudaSuccess && (long long) fa.numRegs * kWThreads >=
+                128LL * kWLowRegs + 256LL * kWHighRegs;
+        if (!d.wide_fits)
+            set_last_error_msg("tc: wide contraction tiles disabled "
+                    "(register budget)");
+        d.done = true;
+    }
+    wide_fits = d.wide_fits;
+    return 0;
+}
 
 int launch_gemm(GemmParams& gp, cudaStream_t stream)
 {
-    static bool attr_set = false;
-    if (!attr_set)
-    {
-        cudaFuncSetAttribute(gemm_kernel,
-                cudaFuncAttributeMaxDynamicSharedMemorySize,
-                (int) gemm_smem_bytes());
-        cudaFuncSetAttribute(gemm_wide_kernel,
-                cudaFuncAttributeMaxDynamicSharedMemorySize,
-                (int) gemm_wide_smem_bytes());
-        attr_set = true;
-    }
+    bool wide_fits = false;
+    const int serr = device_setup(wide_fits);
+    if (serr) return serr;
     const long long square = (long long) gp.nrb * (gp.nrb + 1) / 2 *
             gp.num_problems;
     const long long wide_n = (long long) wide_tiles(gp.nrb) *
             gp.num_problems;
-    // The wide kernel's register split (kWLowRegs / kWHighRegs) must fit in
-    // the registers its blocks are launched with, or the epilogue's request
-    // would never be granted: checked once against the compiled count.
-    static int wide_fits = -1;
-    if (wide_fits < 0)
-    {
-        cudaFuncAttributes fa;
-        wide_fits = cudaFuncGetAttributes(&fa, gemm_wide_kernel) ==
-                cudaSuccess && (long long) fa.numRegs * kWThreads >=
-                128LL * kWLowRegs + 256LL * kWHighRegs;
-        if (!wide_fits)
-            set_last_error_msg("tc: wide contraction tiles disabled "
-                    "(register budget)");
-    }
     const int setting = tile_setting();
     const bool wide = wide_fits && (setting == 256 ||
             (setting == 0 && wide_n >= 2LL * num_sms()));
     const long long ntasks = wide ? wide_n : square;
     const int grid = (int) (ntasks < num_sms() ? ntasks : num_sms());
-    g_last_tile = wide ? 256 : 128;
+    g_last_tile.store(wide ? 256 : 128);
     gp.drain_kb = drain_kblocks();
     cudaEvent_t ev_stop = nullptr;
-    if (g_timing)
     {
-        if (g_ev_used == g_ev.size())
+        std::lock_guard<std::mutex> lock(g_timing_mutex);
+        if (g_timing)
         {
-            cudaEvent_t e0, e1;
-            cudaEventCreate(&e0);
-            cudaEventCreate(&e1);
-            g_ev.emplace_back(e0, e1);
+            if (g_ev_used == g_ev.size())
+            {
+                cudaEvent_t e0, e1;
+                cudaEventCreate(&e0);
+                cudaEventCreate(&e1);
+                g_ev.emplace_back(e0, e1);
+            }
+            cudaEventRecord(g_ev[g_ev_used].first, stream);
+            ev_stop = g_ev[g_ev_used].second;
+            ++g_ev_used;
         }
-        cudaEventRecord(g_ev[g_ev_used].first, stream);
-        ev_stop = g_ev[g_ev_used].second;
-        ++g_ev_used;
     }
     if (wide)
         gemm_wide_kernel<<<grid, kWThreads, gemm_wide_smem_bytes(),
@@ -1283,9 +1325,9 @@ int oskb_cross_correlate_tc_d(int casa, int num_sources, int num_stations,
         return OSKB_ERR_INVALID_ARGUMENT;
     const size_t need = oskb_cross_correlate_tc_workspace_bytes(num_sources,
             num_stations);
-    int err = get_workspace(workspace, workspace_bytes, need);
-    if (err) return err;
     cudaStream_t s = as_stream(stream);
+    int err = get_workspace(workspace, workspace_bytes, need, s);
+    if (err) return err;
     Header* hdr = reinterpret_cast<Header*>(workspace);
     uint8_t* W = reinterpret_cast<uint8_t*>(workspace) + kHeaderBytes;
     cudaMemsetAsync(hdr, 0, sizeof(Header), s);
@@ -1328,7 +1370,7 @@ int oskb_correlate_block_tc(int casa, int num_sources, int num_stations,
         double uv_max_lambda, double* vis, void* workspace,
         size_t workspace_bytes, void* stream)
 {
-    return oskb::tc::correlate_block(casa, num_sources, num_stations,
+    return oskb::tc::correlate_block<float>(casa, num_sources, num_stations,
             num_times, num_channels, E, l, m, n, I, Q, U, V, station_uvw,
             inv_wavelength, uv_min_lambda, uv_max_lambda, vis, workspace,
             workspace_bytes, stream, nullptr, nullptr, nullptr);
@@ -1342,10 +1384,24 @@ int oskb_correlate_block_tc_auto(int casa, int num_sources,
         double uv_min_lambda, double uv_max_lambda, double* vis,
         double* autos, void* workspace, size_t workspace_bytes, void* stream)
 {
-    return oskb::tc::correlate_block(casa, num_sources, num_stations,
+    return oskb::tc::correlate_block<float>(casa, num_sources, num_stations,
             num_times, num_channels, E, l, m, n, I, Q, U, V, station_uvw,
             inv_wavelength, uv_min_lambda, uv_max_lambda, vis, workspace,
             workspace_bytes, stream, nullptr, nullptr, autos);
+}
+
+int oskb_correlate_block_tc_d(int casa, int num_sources, int num_stations,
+        int num_times, int num_channels, const double* E, const double* l,
+        const double* m, const double* n, const double* I, const double* Q,
+        const double* U, const double* V, const double* station_uvw,
+        const double* inv_wavelength, double uv_min_lambda,
+        double uv_max_lambda, double* vis, void* workspace,
+        size_t workspace_bytes, void* stream)
+{
+    return oskb::tc::correlate_block<double>(casa, num_sources, num_stations,
+            num_times, num_channels, E, l, m, n, I, Q, U, V, station_uvw,
+            inv_wavelength, uv_min_lambda, uv_max_lambda, vis, workspace,
+            workspace_bytes, stream, nullptr, nullptr, nullptr);
 }
 
 }  // extern "C"
@@ -1353,8 +1409,9 @@ int oskb_correlate_block_tc_auto(int casa, int num_sources,
 namespace oskb {
 namespace tc {
 
+template <typename TE>
 int correlate_block(int casa, int num_sources, int num_stations,
-        int num_times, int num_channels, const float* E, const double* l,
+        int num_times, int num_channels, const TE* E, const double* l,
         const double* m, const double* n, const double* I, const double* Q,
         const double* U, const double* V, const double* station_uvw,
         const double* inv_wavelength, double uv_min_lambda,
@@ -1392,15 +1449,15 @@ int correlate_block(int casa, int num_sources, int num_stations,
         if ((size_t) group > fit) group = (int) fit;
         if (group > max_group()) group = max_group();
     }
-    int err = get_workspace(workspace, workspace_bytes,
-            kHeaderBytes + (size_t) group * img);
-    if (err) return err;
     cudaStream_t s = as_stream(stream);
+    int err = get_workspace(workspace, workspace_bytes,
+            kHeaderBytes + (size_t) group * img, s);
+    if (err) return err;
     Header* hdr = reinterpret_cast<Header*>(workspace);
     uint8_t* W = reinterpret_cast<uint8_t*>(workspace) + kHeaderBytes;
     cudaMemsetAsync(hdr, 0, sizeof(Header), s);
     // |K| = 1: one scale from E C serves every problem of the block.
-    maxabs_kernel<float, double><<<num_sms() * 8, 256, 0, s>>>(E,
+    maxabs_kernel<TE, double><<<num_sms() * 8, 256, 0, s>>>(E,
             num_sources, num_stations, I, Q, U, V, &hdr->maxabs_bits,
             &hdr->flags);
     if ((err = check_launch("tc maxabs"))) return err;
@@ -1410,7 +1467,8 @@ int correlate_block(int casa, int num_sources, int num_stations,
     for (int p0 = 0; p0 < num_problems; p0 += group)
     {
         const int np = min(group, num_problems - p0);
-        prep_fused_kernel<<<dim3(nkb, nrb), 256, 0, s>>>(E, num_sources,
+        prep_fused_kernel<TE><<<dim3(nkb, nrb), 256, 0, s>>>(E,
+                num_sources,
                 num_stations, l, m, n, I, Q, U, V, station_uvw,
                 inv_wavelength, num_channels, p0, np, &hdr->maxabs_bits, W,
                 img);
@@ -1432,6 +1490,17 @@ int correlate_block(int casa, int num_sources, int num_stations,
     return 0;
 }
 
+template int correlate_block<float>(int, int, int, int, int, const float*,
+        const double*, const double*, const double*, const double*,
+        const double*, const double*, const double*, const double*,
+        const double*, double, double, double*, void*, size_t, void*,
+        void (*)(void*, int, int), void*, double*);
+template int correlate_block<double>(int, int, int, int, int, const double*,
+        const double*, const double*, const double*, const double*,
+        const double*, const double*, const double*, const double*,
+        const double*, double, double, double*, void*, size_t, void*,
+        void (*)(void*, int, int), void*, double*);
+
 }  // namespace tc
 }  // namespace oskb
 
@@ -1439,6 +1508,7 @@ extern "C" {
 
 int oskb_tc_timing(int enable)
 {
+    std::lock_guard<std::mutex> lock(g_timing_mutex);
     g_timing = enable != 0;
     g_ev_used = 0;
     return 0;
@@ -1446,6 +1516,7 @@ int oskb_tc_timing(int enable)
 
 int oskb_tc_timing_read(double* total_ms, int* launches)
 {
+    std::lock_guard<std::mutex> lock(g_timing_mutex);
     double sum = 0.0;
     for (size_t i = 0; i < g_ev_used; ++i)
     {
@@ -1464,7 +1535,7 @@ int oskb_tc_timing_read(double* total_ms, int* launches)
 
 int oskb_tc_tile_columns(void)
 {
-    return g_last_tile;
+    return g_last_tile.load();
 }
 
 int oskb_tc_status(const void* workspace, int* flags, int* wait_error)
@@ -1472,9 +1543,9 @@ int oskb_tc_status(const void* workspace, int* flags, int* wait_error)
     const void* ws = workspace;
     if (!ws)
     {
-        int dev = 0;
-        cudaGetDevice(&dev);
-        ws = (dev >= 0 && dev < 64) ? g_ws[dev].ptr : nullptr;
+        const int dev = current_device();
+        std::lock_guard<std::mutex> lock(g_ws_mutex);
+        ws = (dev >= 0 && dev < 64) ? g_ws_last[dev] : nullptr;
     }
     if (!ws) return OSKB_ERR_INVALID_ARGUMENT;
     Header h;
@@ -1505,9 +1576,11 @@ namespace tc {
 namespace {
 
 // Maximum scratch of the allocation-free entry point: 64 MiB, held by every
-// GPU that loads the library until the process exits. The operand image
-// needs 16 bytes per station-source (rounded up to 32 stations x 32 sources),
-// e.g. up to 512 stations x 8,160 sources per call.
+// GPU that loads the library until the process exits. Beside a 256-byte
+// status header, the operand image needs 32 bytes per station-source (an
+// FP16 hi and lo word for each of the 8 real parts of J C), rounded up to
+// blocks of 32 stations x 32 sources: e.g. up to 512 stations x 4,064
+// sources per call (4,096 sources no longer fit).
 constexpr size_t kStaticScratchBytes = (size_t) 64 << 20;
 
 static __device__ __align__(256) uint8_t g_static_scratch[kStaticScratchBytes];
@@ -1597,4 +1670,25 @@ extern "C" int oskb_cross_correlate_tc_noalloc_d(int casa, int num_sources,
     gp.uv_min = uv_min_lambda; gp.uv_max = uv_max_lambda;
     gp.casa = casa; gp.err = &hdr->err; gp.autos = nullptr;
     return launch_gemm(gp, s);
+}
+
+// Status words of the last allocation-free call on the current device: the
+// header of the static array, read with a plain device-to-host copy (no
+// allocation). Synchronises with the device.
+extern "C" int oskb_tc_noalloc_status(int* flags, int* wait_error)
+{
+    void* scratch = nullptr;
+    const int err = static_scratch(&scratch);
+    if (err) return err;
+    Header h;
+    const cudaError_t e = cudaMemcpy(&h, scratch, sizeof(h),
+            cudaMemcpyDeviceToHost);
+    if (e != cudaSuccess)
+    {
+        set_last_error("static scratch status", e);
+        return OSKB_ERR_MEMORY_COPY_FAILURE;
+    }
+    if (flags) *flags = h.flags;
+    if (wait_error) *wait_error = h.err;
+    return 0;
 }

@@ -11,9 +11,11 @@ namespace tc {
 // the stream, so the caller can enqueue work that depends on those
 // visibilities (for example their download) while later groups compute;
 // autos (if set) receives the auto-correlations from the same contraction
-// ([time][channel][station][2x2], added).
+// ([time][channel][station][2x2], added). E is FP32 or FP64 (float or
+// double instantiations).
+template <typename TE>
 int correlate_block(int casa, int num_sources, int num_stations,
-        int num_times, int num_channels, const float* E, const double* l,
+        int num_times, int num_channels, const TE* E, const double* l,
         const double* m, const double* n, const double* I, const double* Q,
         const double* U, const double* V, const double* station_uvw,
         const double* inv_wavelength, double uv_min_lambda,

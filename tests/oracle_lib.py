@@ -20,9 +20,14 @@ _cache = {}
 
 
 def _ensure(path, target):
+    """Builds a missing oracle library; the ref* targets also need the
+    reference's source directory in OSKB_REF_SRC (otherwise they are left
+    unbuilt and the caller skips)."""
     if not os.path.exists(path):
-        subprocess.run(["make", "-s", "-C", os.path.join(ROOT, "oracle"),
-                        target], check=False, capture_output=True)
+        cmd = ["make", "-s", "-C", os.path.join(ROOT, "oracle"), target]
+        if os.environ.get("OSKB_REF_SRC"):
+            cmd.insert(3, "REF_SRC=" + os.environ["OSKB_REF_SRC"])
+        subprocess.run(cmd, check=False, capture_output=True)
     return os.path.exists(path)
 
 

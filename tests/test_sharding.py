@@ -67,3 +67,55 @@ def test_two_gloo_ranks(tmp_path):
         assert np.load(tmp_path / ("t%d.npy" % r))[0] == 2.0
     assert np.all(count == 1)
     assert np.max(np.abs(got - g["vis"])) <= 1e-14 * np.max(np.abs(g["vis"]))
+
+
+def _lib_worker(rank, world, port, out_dir):
+    """Each rank builds its own steps' host inputs with the library's
+    sharding helper, up to the point where the kernels would be called."""
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    try:
+        from oskar_b200 import workloads
+        from oskar_b200.sharding import rank_dump_uvw
+        cfg = workloads.c3(num_src=64, num_st=40, num_times=10)
+        uvw, dumps = rank_dump_uvw(cfg, world, rank, steps=5)
+        for i, d in enumerate(dumps):
+            assert np.array_equal(uvw[i], cfg.station_uvw(d))
+        gathered = [None] * world
+        dist.all_gather_object(gathered, dumps)
+        np.save(os.path.join(out_dir, "g%d.npy" % rank),
+                np.array(gathered))
+        dist.barrier()
+    finally:
+        dist.destroy_process_group()
+
+
+def test_two_gloo_ranks_library_helpers(tmp_path):
+    world = 2
+    mp.start_processes(_lib_worker, args=(world, _free_port(), str(tmp_path)),
+                       nprocs=world, join=True, start_method="spawn")
+    g0 = np.load(tmp_path / "g0.npy")
+    assert np.array_equal(g0, np.load(tmp_path / "g1.npy"))
+    # five steps of two ranks cover the ten dumps exactly once
+    assert sorted(g0.ravel().tolist()) == list(range(10))
+
+
+def test_bench_spawns_ranks_dry_run():
+    """`bench.py --gpus 2` starts its two ranks itself when no launcher
+    did; the CPU dry run reports both and their disjoint dumps."""
+    import json
+    import subprocess
+    import sys
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    env = {k: v for k, v in os.environ.items()
+           if k not in ("WORLD_SIZE", "RANK", "LOCAL_RANK")}
+    r = subprocess.run([sys.executable, os.path.join(root, "bench.py"),
+                        "--gpus", "2", "--dry-run", "--steps", "4",
+                        "--warmup", "3"], capture_output=True, text=True,
+                       env=env, timeout=300)
+    assert r.returncode == 0, r.stderr
+    line = json.loads(r.stdout.strip().splitlines()[-1])
+    assert line["n_gpus"] == 2 and line["dry_run"]
+    d0, d1 = line["dumps_per_rank"]
+    assert len(d0) == len(d1) == 4 and not set(d0) & set(d1)
