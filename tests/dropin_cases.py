@@ -1,0 +1,81 @@
+"""Simulation cases for the drop-in oskar_interferometer_run_block tests,
+written as the inputs of tests/ref_sim.py (reference API calls)."""
+import math
+
+import numpy as np
+
+from oskar_b200 import workloads
+
+
+def lm_to_radec(l, m, ra0, dec0):
+    """Sky directions of direction cosines (l, m) about (ra0, dec0) (the
+    inverse orthographic projection)."""
+    n = np.sqrt(1.0 - l * l - m * m)
+    dec = np.arcsin(n * math.sin(dec0) + m * math.cos(dec0))
+    ra = ra0 + np.arctan2(l, n * math.cos(dec0) - m * math.sin(dec0))
+    return ra, dec
+
+
+def c1_case(precision="double", **over):
+    """C1: 30 isotropic stations in a 1 km disc at lat -27 deg, 1,000 point
+    sources (S^-1.5 on [0.01, 10] Jy, Q = U = V = 0) in a 5 deg field about
+    RA 0, Dec -30 deg, 1 channel at 100 MHz, 10 dumps of 60 s, full
+    polarisation, no smearing."""
+    cfg = workloads.c1()
+    ra, dec = lm_to_radec(cfg.l, cfg.m, cfg.ra0, cfg.dec0)
+    n = cfg.num_src
+    z = [0.0] * n
+    case = {
+        "precision": precision, "pol_mode": "Full",
+        "lon_deg": workloads.LON_DEG, "lat_deg": workloads.LAT_DEG,
+        "station_x": cfg.station_enu[0].tolist(),
+        "station_y": cfg.station_enu[1].tolist(),
+        "station_type": "Isotropic beam",
+        "channel_bandwidth_hz": 0.0, "time_average_sec": 0.0,
+        "uv_filter": [0.0, -1.0, "Wavelengths"],
+        "ra_rad": ra.tolist(), "dec_rad": dec.tolist(),
+        "I": cfg.I.tolist(), "Q": list(z), "U": list(z), "V": list(z),
+        "ref_freq_hz": list(z), "spectral_index": list(z),
+        "rotation_measure": list(z), "major_rad": list(z),
+        "minor_rad": list(z), "pa_rad": list(z),
+        "phase_centre_ra_rad": cfg.ra0, "phase_centre_dec_rad": cfg.dec0,
+        "freq_start_hz": 100e6, "freq_inc_hz": 0.0, "num_channels": 1,
+        "mjd_start": workloads.MJD0, "inc_sec": 60.0, "num_times": 10,
+        "num_devices": 1, "max_times_per_block": 10,
+        "max_sources_per_chunk": 16384, "horizon_clip": 1,
+        "correlation_type": "Cross-correlations", "casa": 0,
+        "source_min_jy": -1e300, "source_max_jy": 1e300,
+    }
+    case.update(over)
+    return case
+
+
+def c1_extended_case(precision="double", **over):
+    """C1 widened to every stage the drop-in runs: full-Stokes fluxes with a
+    spectral index and rotation measure over 3 channels, 30 % Gaussian
+    sources, bandwidth and time-average smearing, auto-correlations, a uv
+    filter, 2 sky chunks, blocks of 4 dumps and 2 device threads."""
+    c = c1_case(precision)
+    rng = np.random.default_rng(11)
+    n = len(c["I"])
+    I = np.asarray(c["I"])
+    c["Q"] = (I * rng.uniform(-0.1, 0.1, n)).tolist()
+    c["U"] = (I * rng.uniform(-0.1, 0.1, n)).tolist()
+    c["V"] = (I * rng.uniform(-0.1, 0.1, n)).tolist()
+    c["ref_freq_hz"] = [100e6] * n
+    c["spectral_index"] = rng.uniform(-1.0, 0.5, n).tolist()
+    c["rotation_measure"] = rng.uniform(-5.0, 5.0, n).tolist()
+    gauss = rng.uniform(0, 1, n) < 0.3
+    arcsec = math.pi / 180.0 / 3600.0
+    maj = np.where(gauss, rng.uniform(1, 60, n) * arcsec, 0.0)
+    mnr = np.where(gauss, rng.uniform(0.3, 1.0, n) * maj, 0.0)
+    c["major_rad"] = maj.tolist()
+    c["minor_rad"] = mnr.tolist()
+    c["pa_rad"] = np.where(gauss, rng.uniform(0, math.pi, n), 0.0).tolist()
+    c.update({"num_channels": 3, "freq_inc_hz": 5e6,
+              "channel_bandwidth_hz": 1e5, "time_average_sec": 10.0,
+              "uv_filter": [1.0, 250.0, "Wavelengths"],
+              "correlation_type": "Both", "max_sources_per_chunk": 600,
+              "max_times_per_block": 4, "num_devices": 2})
+    c.update(over)
+    return c

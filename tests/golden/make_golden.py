@@ -14,8 +14,22 @@ Fixtures (inputs and outputs in one .npz each, FP64 unless noted):
   f32_vis.npz       the c1 chain of dump 0 in single precision.
   dftw.npz          weighted DFT, 2x2 (m2m) 3-D with element types, and
                     complex (c2c) 2-D.
+  c1_sim.npz        the c1 configuration run end to end through the
+                    reference's own simulator (oskar_interferometer_run,
+                    full polarisation with Jones R, one shared isotropic
+                    station model) by tests/ref_sim.py with the reference's
+                    CPU library (oracle/_ref/liboskar_refcpu.so, `make -C
+                    oracle ref_lib`): cross-correlations [dump][channel]
+                    [baseline x 2x2 complex] read back from its .vis file.
+  c1_stations_sim.npz  the same with one station model per station, so that
+                    Jones R follows each station's own latitude and
+                    longitude.
 Only the generator reads the reference library; the fixtures are plain data.
+Run with --sim-only to remake just the simulator fixtures.
 """
+import json
+import subprocess
+import tempfile
 import math
 import os
 import sys
@@ -127,7 +141,42 @@ def dftw_case():
                 out_c=out_c)
 
 
+def sim_fixtures():
+    """The end-to-end fixtures from the reference simulator (its horizon
+    clip off: every source of the field is above the horizon)."""
+    from dropin_cases import c1_case
+    ref_lib = os.path.join(ROOT, "oracle", "_ref", "liboskar_refcpu.so")
+    if not os.path.exists(ref_lib):
+        raise SystemExit("reference library not built: make -C oracle "
+                         "REF_SRC=... ref_lib")
+    cases = {"c1_sim.npz": c1_case("double", horizon_clip=0),
+             "c1_stations_sim.npz": c1_case("double", horizon_clip=0,
+                                            station_per_folder=1)}
+    env = {k: v for k, v in os.environ.items() if k != "LD_PRELOAD"}
+    with tempfile.TemporaryDirectory() as tmp:
+        for name, case in cases.items():
+            cj = os.path.join(tmp, "case.json")
+            with open(cj, "w") as f:
+                json.dump(case, f)
+            out = os.path.join(HERE, name)
+            # the reference's CPU run is repeated if it crashes (it was
+            # seen to, now and then, in its flux scaling)
+            for _ in range(4):
+                r = subprocess.run([sys.executable, os.path.join(
+                    os.path.dirname(HERE), "ref_sim.py"), cj, out], env=env)
+                if r.returncode == 0:
+                    break
+            if r.returncode:
+                raise SystemExit("reference simulator failed: %d"
+                                 % r.returncode)
+            d = dict(np.load(out))
+            np.savez_compressed(out, **d)
+
+
 def main():
+    if "--sim-only" in sys.argv:
+        sim_fixtures()
+        return
     if reference() is None:
         raise SystemExit("reference kernels not built: make -C oracle ref")
     np.savez_compressed(os.path.join(HERE, "c1_vis.npz"), **c1_chain())
@@ -135,6 +184,7 @@ def main():
                         **c1_chain(np.float32, dumps=[0]))
     np.savez_compressed(os.path.join(HERE, "smear_vis.npz"), **smear_case())
     np.savez_compressed(os.path.join(HERE, "dftw.npz"), **dftw_case())
+    sim_fixtures()
     for f in sorted(os.listdir(HERE)):
         if f.endswith(".npz"):
             print(f, os.path.getsize(os.path.join(HERE, f)))
