@@ -231,11 +231,12 @@ def _load_peaks():
 
 
 def _load_traffic(tile):
-    """DRAM bytes per launch of the contraction kernel (square or wide
+    """DRAM bytes per launch of the contraction kernel (square, wide or pair
     tiles) from the committed ncu summary
-    (profiles/tc_gemm{,_wide}_c3_traffic.json), or None."""
-    name = "tc_gemm_wide_c3_traffic.json" if tile == 256 else \
-        "tc_gemm_c3_traffic.json"
+    (profiles/tc_gemm{,_wide,_pair}_c3_traffic.json), or None."""
+    name = {256: "tc_gemm_wide_c3_traffic.json",
+            512: "tc_gemm_pair_c3_traffic.json"}.get(
+                tile, "tc_gemm_c3_traffic.json")
     path = os.path.join(ROOT, "profiles", name)
     if not os.path.exists(path):
         return None
@@ -352,7 +353,12 @@ def run_ours(args):
             nrb = (nst + 31) // 32
             kp = 2 * 32 * ((nsrc + 31) // 32)
             tile = ob.load().oskb_tc_tile_columns()
-            if tile == 256:
+            if tile == 512:
+                # pair tiles: 256 x 256 per CTA pair over the triangle of
+                # row-block pairs
+                npr = (nrb + 1) // 2
+                issued = nch * npr * (npr + 1) // 2 * 256 * 256 * kp * 2 * 3
+            elif tile == 256:
                 # wide tiles: 128 x 256 columns per task over the triangle
                 ntile = sum(min(2 * cp + 2, nrb)
                             for cp in range((nrb + 1) // 2))
@@ -363,8 +369,9 @@ def run_ours(args):
             traffic = _load_traffic(tile)
             roof = {"bound": "tensor", "achieved": ach, "peak": pk,
                     "unit": "TFLOP/s", "frac": ach / pk, "traffic": traffic,
-                    "kernel": ("oskb::tc::gemm_wide_kernel" if tile == 256
-                               else "oskb::tc::gemm_kernel"),
+                    "kernel": {256: "oskb::tc::gemm_wide_kernel",
+                               512: "oskb::tc::gemm_pair_kernel"}.get(
+                                   tile, "oskb::tc::gemm_kernel"),
                     "tile_columns": tile,
                     "peak_kind": "%s bf16 sustained (fp16 same rate)"
                                  % peak_kind,
@@ -576,10 +583,12 @@ def run_profile_case(args):
       tc_small      the tensor-core contraction (gemm_kernel) and its
                     operand preparation (prep_fused_kernel): 512 stations x
                     20,000 sources x 1 channel, 1/80 of a bench launch;
-      tc_wide_small the wide-tile contraction (gemm_wide_kernel, chosen
-                    when a launch has two wide tiles per SM): 512 stations
-                    x 2,500 sources x 8 channels (576 tiles), also 1/80 of
-                    a bench launch;
+      tc_wide_small the wide-tile contraction (gemm_wide_kernel, tile
+                    shape fixed to 128 x 256): 512 stations x 2,500
+                    sources x 8 channels (576 tiles), also 1/80 of a bench
+                    launch;
+      tc_pair_small the pair-tile contraction (gemm_pair_kernel, 256 x 256
+                    tiles on CTA pairs) on the same case (288 pair tiles);
       direct_small  the FP64 direct cross-correlation: 512 stations x 2,000
                     sources, 1 channel;
       beam_small    the fused station beam: 32 stations x 256 dipoles x
@@ -594,10 +603,14 @@ def run_profile_case(args):
     dev = lambda a: torch.from_numpy(np.ascontiguousarray(a)).cuda()
     stream = ob.stream_ptr()
     case = args.profile_case
-    if case in ("tc_small", "tc_wide_small", "direct_small"):
+    if case in ("tc_wide_small", "tc_pair_small"):
+        os.environ["OSKB_TC_TILE"] = "256" if case == "tc_wide_small" \
+            else "512"
+    if case in ("tc_small", "tc_wide_small", "tc_pair_small",
+                "direct_small"):
         nsrc = {"tc_small": 20_000, "tc_wide_small": 2_500,
-                "direct_small": 2_000}[case]
-        nch = 8 if case == "tc_wide_small" else 1
+                "tc_pair_small": 2_500, "direct_small": 2_000}[case]
+        nch = 8 if case in ("tc_wide_small", "tc_pair_small") else 1
         cfg = workloads.c3(num_src=nsrc, num_channels=nch, num_times=1)
         nst, nbl = cfg.num_st, cfg.num_baselines
         l, m, n, I, Q, U, V = (dev(x) for x in (cfg.l, cfg.m, cfg.n, cfg.I,
@@ -1229,7 +1242,8 @@ def main():
     ap.add_argument("--c5-steps", type=int, default=20000)
     ap.add_argument("--c5-bound", type=float, default=1e-4)
     ap.add_argument("--profile-case", default=None,
-                    choices=["tc_small", "tc_wide_small", "direct_small",
+                    choices=["tc_small", "tc_wide_small", "tc_pair_small",
+                             "direct_small",
                              "beam_small",
                              "block_small"],
                     help="run one small kernel case for an ncu capture")

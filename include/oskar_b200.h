@@ -1047,10 +1047,11 @@ OSKB_API int oskb_tc_noalloc_status(int* flags, int* wait_error);
  * bounded device-side wait expired (the call's result is invalid). */
 OSKB_API int oskb_tc_status(const void* workspace, int* flags,
         int* wait_error);
-/* Tile width (128 or 256 columns of G) of the last tensor-core contraction
- * launched, 0 before the first. The environment variable OSKB_TC_TILE
- * (128 or 256) fixes it; unset, wide tiles are used when a launch has at
- * least two of them per SM. */
+/* Tile shape of the last tensor-core contraction launched, 0 before the
+ * first: 128 (128 x 128 tiles of G per CTA), 256 (128 x 256 per CTA) or
+ * 512 (256 x 256 per pair of CTAs, cta_group::2). The environment variable
+ * OSKB_TC_TILE (128, 256 or 512) fixes it; unset, wide tiles are used
+ * when a launch has at least two per SM, else square tiles. */
 OSKB_API int oskb_tc_tile_columns(void);
 
 /* ------------------------------------------------------------------------

@@ -204,6 +204,117 @@ __device__ __forceinline__ uint64_t sdesc_sw128(uint32_t saddr)
     return d;
 }
 
+// ---- thread-block pairs (cluster of two CTAs, cta_group::2)
+__device__ __forceinline__ uint32_t cluster_ctarank()
+{
+    uint32_t r;
+    asm volatile("mov.u32 %0, %%cluster_ctarank;" : "=r"(r));
+    return r;
+}
+
+// All threads of both CTAs of the cluster.
+__device__ __forceinline__ void cluster_sync()
+{
+    asm volatile("barrier.cluster.arrive.release.aligned;\n\t"
+                 "barrier.cluster.wait.acquire.aligned;" ::: "memory");
+}
+
+// Shared::cluster address of the variable at local shared address saddr in
+// the CTA of the given rank.
+__device__ __forceinline__ uint32_t mapa_shared(uint32_t saddr, uint32_t rank)
+{
+    uint32_t r;
+    asm volatile("mapa.shared::cluster.u32 %0, %1, %2;"
+                 : "=r"(r) : "r"(saddr), "r"(rank));
+    return r;
+}
+
+// Arrive (release at cluster scope) on an mbarrier given by its
+// shared::cluster address, possibly in the peer CTA.
+__device__ __forceinline__ void mbar_arrive_cluster(uint32_t cluster_addr)
+{
+    asm volatile("mbarrier.arrive.release.cluster.shared::cluster.b64 _, "
+                 "[%0];" :: "r"(cluster_addr) : "memory");
+}
+
+__device__ __forceinline__ bool mbar_try_wait_cluster(uint64_t* bar,
+        uint32_t parity)
+{
+    uint32_t ok;
+    asm volatile("{\n\t.reg .pred p;\n\t"
+                 "mbarrier.try_wait.parity.acquire.cluster.shared::cta.b64 "
+                 "p, [%1], %2;\n\t"
+                 "selp.u32 %0, 1, 0, p;\n\t}"
+                 : "=r"(ok) : "r"(smem_u32(bar)), "r"(parity) : "memory");
+    return ok != 0;
+}
+
+// mbar_wait for barriers that threads of the peer CTA arrive on: the
+// acquire is at cluster scope, the limit and abort as in mbar_wait.
+__device__ __forceinline__ bool mbar_wait_cluster(uint64_t* bar,
+        uint32_t parity, int* err, int code, volatile int* abort)
+{
+    if (mbar_try_wait_cluster(bar, parity)) return true;
+    const uint64_t t0 = global_ns();
+    for (uint32_t it = 1;; ++it)
+    {
+        if (mbar_try_wait_cluster(bar, parity)) return true;
+        if ((it & 255u) == 0)
+        {
+            if (*abort) return false;
+            if (global_ns() - t0 > kWaitLimitNs)
+            {
+                if (err) atomicCAS(err, 0, code);
+                *abort = 1;
+                return false;
+            }
+        }
+    }
+}
+
+// TMEM of both CTAs of a pair: one warp of each CTA (the same warp index),
+// the same shared-memory destination offset in both.
+__device__ __forceinline__ void tmem_alloc_pair(uint32_t* dst_smem,
+        uint32_t ncols)
+{
+    asm volatile("tcgen05.alloc.cta_group::2.sync.aligned.shared::cta.b32 "
+                 "[%0], %1;" :: "r"(smem_u32(dst_smem)), "r"(ncols)
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::2.sync.aligned;"
+                 ::: "memory");
+}
+
+__device__ __forceinline__ void tmem_dealloc_pair(uint32_t taddr,
+        uint32_t ncols)
+{
+    asm volatile("tcgen05.dealloc.cta_group::2.sync.aligned.b32 %0, %1;"
+                 :: "r"(taddr), "r"(ncols) : "memory");
+}
+
+// Pair MMA, issued by one thread of the even CTA: D (M = 256: rows 0-127 in
+// the even CTA's TMEM, 128-255 in the odd CTA's) (+)= A B^T, A's rows
+// 0-127 and 128-255 read from the two CTAs' shared memory at the same
+// offset, B's N rows split the same way (first N/2 from the even CTA).
+__device__ __forceinline__ void mma_f16_pair(uint32_t d_tmem, uint64_t a_desc,
+        uint64_t b_desc, uint32_t idesc, uint32_t accumulate)
+{
+    asm volatile("{\n\t.reg .pred p;\n\t"
+                 "setp.ne.b32 p, %4, 0;\n\t"
+                 "tcgen05.mma.cta_group::2.kind::f16 [%0], %1, %2, %3, p;\n\t}"
+                 :: "r"(d_tmem), "l"(a_desc), "l"(b_desc), "r"(idesc),
+                    "r"(accumulate) : "memory");
+}
+
+// Arrives on the mbarrier at the same shared offset in both CTAs of the
+// pair once all previously issued pair MMAs have completed.
+__device__ __forceinline__ void mma_commit_pair(uint64_t* bar)
+{
+    const uint16_t mask = 0x3;
+    asm volatile("tcgen05.commit.cta_group::2.mbarrier::arrive::one"
+                 ".shared::cluster.multicast::cluster.b64 [%0], %1;"
+                 :: "r"(smem_u32(bar)), "h"(mask) : "memory");
+}
+
 // Instruction descriptor: FP16 A and B (K-major), FP32 accumulator, M x N.
 __host__ __device__ constexpr uint32_t idesc_f16_f32(int m, int n)
 {

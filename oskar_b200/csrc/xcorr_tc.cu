@@ -45,6 +45,7 @@ constexpr int kStPerBlock = 32;              // stations per 128-row block
 constexpr int kSrcPerBlock = 32;             // sources per 64-column block
 constexpr int kTileBytes = 128 * 128;        // 128 rows x 128 bytes
 constexpr int kPairBytes = 2 * kTileBytes;   // hi + lo
+constexpr int kKSteps = 4;                   // K = 16 MMA steps per k block
 constexpr float kScaleTarget = 16384.0f;     // largest scaled |entry|
 
 __host__ __device__ inline size_t image_bytes(int num_st, int num_src)
@@ -519,7 +520,7 @@ gemm_kernel(const GemmParams prm)
                                 (size_t) stage * kStageBytes);
                         const uint32_t b = diag ? a : a + kPairBytes;
 #pragma unroll
-                        for (int k = 0; k < 4; ++k)
+                        for (int k = 0; k < kKSteps; ++k)
                         {
                             const uint64_t ah = ptx::sdesc_sw128(a + 32 * k);
                             const uint64_t al = ptx::sdesc_sw128(
@@ -694,14 +695,16 @@ gemm_kernel(const GemmParams prm)
 // (2^-11 of the main one) is drained every kCorrPeriods main drains and at
 // the end of each task.
 // Warp roles: warpgroup 0 = producer (warp 0), MMA issuer (warp 1) and two
-// idle warps, all releasing registers down to kWLowRegs; warpgroups 1 and 2
-// = eight epilogue warps of 128 columns each, raised to kWHighRegs so that
+// other warps, all releasing registers down to kWLowRegs; warpgroups 1 and
+// 2 = eight epilogue warps of 128 columns each, raised to kWHighRegs so that
 // the 64 FP64 sums per thread and two 32-column TMEM loads stay in
 // registers. Budget: 128 x kWLowRegs + 256 x kWHighRegs must not exceed the
 // 384 x (registers per thread at launch) the block starts with; the host
 // checks the compiled count before the first launch.
 // ===========================================================================
 constexpr int kWThreads = 384;
+constexpr int kWEpiWarps = 8;
+constexpr int kWEpiCols = 128;                // columns per epilogue thread
 constexpr int kWLowRegs = 72;
 constexpr int kWHighRegs = 216;
 constexpr int kWStages = 2;
@@ -748,6 +751,144 @@ __device__ __forceinline__ bool corr_drain_at(int ch, int nchunk)
     return (ch % kCorrPeriods) == kCorrPeriods - 1 || ch == nchunk - 1;
 }
 
+// ---------------------------------------------------------------------------
+// Epilogue of one wide or pair task, run by each of the eight epilogue
+// warps. The thread's TMEM lane is row `row` of the task's 128-row block;
+// its 128 columns (taddr) are 32 stations x (polarisation j, part c') of G.
+// Every drain loads them (32 columns per TMEM load; 16 main and 16
+// correction columns when the correction accumulator is due), folds each
+// group of four into the real and imaginary parts of this thread's
+// visibility (Re V = G00 + G11, Im V = G10 - G01 across the row pair, lanes
+// l and l ^ 1) in FP32 and adds those into FP64 sums: the cross-tile sum is
+// FP64. At the end of the task the sums are scaled and added into vis (and
+// autos). Returns false if a bounded wait expired.
+// ---------------------------------------------------------------------------
+template <class Arrive>
+__device__ __forceinline__ bool wide_task_epilogue(const GemmParams& prm,
+        uint64_t* mfull, uint64_t* cfull, uint32_t& mpar, uint32_t& cpar,
+        volatile int* abort, uint32_t taddr, int row, int lane, int prob,
+        int rb, int q0, int nchunk, Arrive arrive)
+{
+    const int c = row & 1;
+    double accR[32], accI[32];
+#pragma unroll
+    for (int j = 0; j < 32; ++j) accR[j] = accI[j] = 0.0;
+    for (int ch = 0; ch < nchunk; ++ch)
+    {
+        const bool with_corr = corr_drain_at(ch, nchunk);
+        if (!ptx::mbar_wait(mfull, mpar, prm.err, 27, abort) ||
+                (with_corr && !ptx::mbar_wait(cfull, cpar, prm.err, 28,
+                abort)))
+            return false;
+        ptx::tc_fence_after();
+#define OSKB_WIDE_FOLD(V, J0, NQ)                                              \
+        _Pragma("unroll")                                                      \
+        for (int qq = 0; qq < (NQ); ++qq)                                      \
+        {                                                                      \
+            const int jb = 4 * qq;                                             \
+            const float s0 = c ? V[jb + 0] : V[jb + 2];                        \
+            const float s1 = c ? V[jb + 1] : V[jb + 3];                        \
+            const float r0 = __shfl_xor_sync(0xffffffffu, s0, 1);              \
+            const float r1 = __shfl_xor_sync(0xffffffffu, s1, 1);              \
+            const float g00 = c ? r0 : V[jb + 0];                              \
+            const float g01 = c ? r1 : V[jb + 1];                              \
+            const float g10 = c ? V[jb + 2] : r0;                              \
+            const float g11 = c ? V[jb + 3] : r1;                              \
+            accR[(J0) / 4 + qq] += (double) (g00 + g11);                       \
+            accI[(J0) / 4 + qq] += (double) (g10 - g01);                       \
+        }
+        if (!with_corr)
+        {
+#pragma unroll
+            for (int j0 = 0; j0 < 128; j0 += 32)
+            {
+                uint32_t va[32];
+                ptx::tmem_ld32(taddr + j0, va);
+                ptx::tmem_ld_wait();
+                float v[32];
+#pragma unroll
+                for (int j = 0; j < 32; ++j) v[j] = __uint_as_float(va[j]);
+                OSKB_WIDE_FOLD(v, j0, 8)
+            }
+        }
+        else
+        {
+#pragma unroll
+            for (int j0 = 0; j0 < 128; j0 += 16)
+            {
+                uint32_t va[16], vb[16];
+                ptx::tmem_ld16(taddr + j0, va);
+                ptx::tmem_ld16(taddr + kWCols + j0, vb);
+                ptx::tmem_ld_wait();
+                float v[16];
+#pragma unroll
+                for (int j = 0; j < 16; ++j)
+                    v[j] = __uint_as_float(va[j]) + __uint_as_float(vb[j]);
+                OSKB_WIDE_FOLD(v, j0, 4)
+            }
+        }
+#undef OSKB_WIDE_FOLD
+        ptx::tc_fence_before();
+        __syncwarp();
+        if (lane == 0) arrive(with_corr);
+        mpar ^= 1;
+        if (with_corr) cpar ^= 1;
+    }
+    // ---- visibilities of this thread's row of the tile
+    const int g = prm.prob0 + prob, t = g / prm.nch;
+    const int chan = g - t * prm.nch;
+    const float S = scale_from_bits(prm.maxabs_bits[prm.maxabs_stride * g]);
+    const double inv_s2 = 1.0 / ((double) S * (double) S);
+    const int i = (row >> 1) & 1;
+    const int p = rb * kStPerBlock + (row >> 2);
+    const int N = prm.num_st;
+    const double* su = prm.st_u + prm.uv_stride * t;
+    const double* sv = prm.st_v + prm.uv_stride * t;
+    const double kw = prm.inv_wavelength ? prm.inv_wavelength[chan]
+                                          : prm.kw_scalar;
+    double* vbase = prm.vis + 8 * ((size_t) g * prm.vis_stride +
+            (size_t) prm.offset_out);
+    if (prm.autos && p < N)
+    {
+        // the column station q = p, where this thread's 32 hold it
+        const int ql = p - q0;
+#pragma unroll
+        for (int k = 0; k < 32; ++k)
+            if (k == ql)
+            {
+                double* o = prm.autos + 8 * ((size_t) g * N + p) +
+                        2 * (2 * i + c);
+                o[0] += accR[k] * inv_s2;
+                o[1] += accI[k] * inv_s2;
+            }
+    }
+#pragma unroll
+    for (int ql = 0; ql < 32; ++ql)
+    {
+        const int q = q0 + ql;
+        if (p < q && q < N)
+        {
+            const double uu = (su[p] - su[q]) * kw;
+            const double vv = (sv[p] - sv[q]) * kw;
+            const double len = sqrt(uu * uu + vv * vv);
+            if (!(len < prm.uv_min || len > prm.uv_max))
+            {
+                const double re = accR[ql] * inv_s2;
+                const double im = accI[ql] * inv_s2;
+                // this thread holds V_pq[i][j] with j = c; the reference
+                // stores J_q B J_p^H (p < q) unless CASA
+                const int ro = prm.casa ? i : c;
+                const int co = prm.casa ? c : i;
+                double* o = vbase + 8 * (size_t) baseline_index(N, q, p) +
+                        2 * (2 * ro + co);
+                o[0] += re;
+                o[1] += prm.casa ? im : -im;
+            }
+        }
+    }
+    return true;
+}
+
 __global__ void __launch_bounds__(kWThreads, 1)
 gemm_wide_kernel(const GemmParams prm)
 {
@@ -766,9 +907,9 @@ gemm_wide_kernel(const GemmParams prm)
             ptx::mbar_init(&ctl->empty[s], 1);
         }
         ptx::mbar_init(&ctl->mfull, 1);
-        ptx::mbar_init(&ctl->mempty, 8);
+        ptx::mbar_init(&ctl->mempty, kWEpiWarps);
         ptx::mbar_init(&ctl->cfull, 1);
-        ptx::mbar_init(&ctl->cempty, 8);
+        ptx::mbar_init(&ctl->cempty, kWEpiWarps);
         ptx::mbar_init(&ctl->done, 1);
         ctl->abort = 0;
         ptx::fence_mbar_init();
@@ -887,7 +1028,7 @@ gemm_wide_kernel(const GemmParams prm)
                         // correction products first: they do not need the
                         // main accumulator, which may still be draining
 #pragma unroll
-                        for (int k = 0; k < 4; ++k)
+                        for (int k = 0; k < kKSteps; ++k)
                         {
                             const uint32_t first =
                                     (fresh && kb == kb0 && k == 0) ? 0u : 1u;
@@ -908,7 +1049,7 @@ gemm_wide_kernel(const GemmParams prm)
                             ptx::tc_fence_after();
                         }
 #pragma unroll
-                        for (int k = 0; k < 4; ++k)
+                        for (int k = 0; k < kKSteps; ++k)
                             ptx::mma_f16(dm, ptx::sdesc_sw128(a + 32 * k),
                                     ptx::sdesc_sw128(bh + 32 * k), idesc,
                                     (kb > kb0 || k > 0) ? 1u : 0u);
@@ -933,153 +1074,28 @@ gemm_wide_kernel(const GemmParams prm)
     }  // warpgroup 0
     else
     {
-        // ---------------- epilogue: 8 warps (4-11), 128 columns each
+        // ---------------- epilogue warps (4 and up), kWEpiCols columns each
         ptx::regs_request<kWHighRegs>();
-        {
         const int q4 = warp & 3;          // TMEM lane quadrant of this warp
-        const int h = (warp - 4) >> 2;    // column half
+        const int h = (warp - 4) >> 2;    // column slice
         const int row = 32 * q4 + lane;   // row of the G tile
         const uint32_t taddr = tmem + ((uint32_t) (32 * q4) << 16) +
-                (uint32_t) (128 * h);
+                (uint32_t) (kWEpiCols * h);
         uint32_t mpar = 0, cpar = 0;
-        bool ok = true;
-        for (int task = blockIdx.x; task < ntasks && ok; task += gridDim.x)
+        auto arrive = [&](bool with_corr) {
+            ptx::mbar_arrive(&ctl->mempty);
+            if (with_corr) ptx::mbar_arrive(&ctl->cempty);
+        };
+        for (int task = blockIdx.x; task < ntasks; task += gridDim.x)
         {
             const int prob = task / ntile;
             int rb, cp;
             wide_tile_of(task - prob * ntile, rb, cp);
-            const int c = row & 1;
-            double accR[32], accI[32];
-#pragma unroll
-            for (int j = 0; j < 32; ++j) accR[j] = accI[j] = 0.0;
-            for (int ch = 0; ch < nchunk; ++ch)
-            {
-                const bool with_corr = corr_drain_at(ch, nchunk);
-                if (!ptx::mbar_wait(&ctl->mfull, mpar, prm.err, 27, abort) ||
-                        (with_corr && !ptx::mbar_wait(&ctl->cfull, cpar,
-                        prm.err, 28, abort)))
-                {
-                    ok = false;
-                    break;
-                }
-                ptx::tc_fence_after();
-                // One 32-column TMEM load per wait (main only), or 16 main
-                // and 16 correction columns per wait. Each group of four
-                // columns is one station of the pair of rows (lanes l,
-                // l ^ 1): Re V = G00 + G11, Im V = G10 - G01, combined in
-                // FP32, summed in FP64.
-#define OSKB_WIDE_FOLD(V, J0, NQ)                                              \
-                _Pragma("unroll")                                              \
-                for (int qq = 0; qq < (NQ); ++qq)                              \
-                {                                                              \
-                    const int jb = 4 * qq;                                     \
-                    const float s0 = c ? V[jb + 0] : V[jb + 2];                \
-                    const float s1 = c ? V[jb + 1] : V[jb + 3];                \
-                    const float r0 = __shfl_xor_sync(0xffffffffu, s0, 1);      \
-                    const float r1 = __shfl_xor_sync(0xffffffffu, s1, 1);      \
-                    const float g00 = c ? r0 : V[jb + 0];                      \
-                    const float g01 = c ? r1 : V[jb + 1];                      \
-                    const float g10 = c ? V[jb + 2] : r0;                      \
-                    const float g11 = c ? V[jb + 3] : r1;                      \
-                    accR[(J0) / 4 + qq] += (double) (g00 + g11);               \
-                    accI[(J0) / 4 + qq] += (double) (g10 - g01);               \
-                }
-                if (!with_corr)
-                {
-#pragma unroll
-                    for (int j0 = 0; j0 < 128; j0 += 32)
-                    {
-                        uint32_t va[32];
-                        ptx::tmem_ld32(taddr + j0, va);
-                        ptx::tmem_ld_wait();
-                        float v[32];
-#pragma unroll
-                        for (int j = 0; j < 32; ++j)
-                            v[j] = __uint_as_float(va[j]);
-                        OSKB_WIDE_FOLD(v, j0, 8)
-                    }
-                }
-                else
-                {
-#pragma unroll
-                    for (int j0 = 0; j0 < 128; j0 += 16)
-                    {
-                        uint32_t va[16], vb[16];
-                        ptx::tmem_ld16(taddr + j0, va);
-                        ptx::tmem_ld16(taddr + kWCols + j0, vb);
-                        ptx::tmem_ld_wait();
-                        float v[16];
-#pragma unroll
-                        for (int j = 0; j < 16; ++j)
-                            v[j] = __uint_as_float(va[j]) +
-                                    __uint_as_float(vb[j]);
-                        OSKB_WIDE_FOLD(v, j0, 4)
-                    }
-                }
-#undef OSKB_WIDE_FOLD
-                ptx::tc_fence_before();
-                __syncwarp();
-                if (lane == 0)
-                {
-                    ptx::mbar_arrive(&ctl->mempty);
-                    if (with_corr) ptx::mbar_arrive(&ctl->cempty);
-                }
-                mpar ^= 1;
-                if (with_corr) cpar ^= 1;
-            }
-            if (!ok) break;
-            // ---- visibilities of this tile
-            const int g = prm.prob0 + prob, t = g / prm.nch;
-            const int chan = g - t * prm.nch;
-            const float S = scale_from_bits(
-                    prm.maxabs_bits[prm.maxabs_stride * g]);
-            const double inv_s2 = 1.0 / ((double) S * (double) S);
-            const int i = (row >> 1) & 1;
-            const int p = rb * kStPerBlock + (row >> 2);
-            const int N = prm.num_st;
-            const double* su = prm.st_u + prm.uv_stride * t;
-            const double* sv = prm.st_v + prm.uv_stride * t;
-            const double kw = prm.inv_wavelength ? prm.inv_wavelength[chan]
-                                                  : prm.kw_scalar;
-            double* vbase = prm.vis + 8 * ((size_t) g * prm.vis_stride +
-                    (size_t) prm.offset_out);
-            if (prm.autos && p < N)
-            {
-                // the column station q = p, where this thread's 32 hold it
-                const int ql = p - 2 * cp * kStPerBlock - 32 * h;
-#pragma unroll
-                for (int k = 0; k < 32; ++k)
-                    if (k == ql)
-                    {
-                        double* o = prm.autos + 8 * ((size_t) g * N + p) +
-                                2 * (2 * i + c);
-                        o[0] += accR[k] * inv_s2;
-                        o[1] += accI[k] * inv_s2;
-                    }
-            }
-#pragma unroll
-            for (int ql = 0; ql < 32; ++ql)
-            {
-                const int q = 2 * cp * kStPerBlock + 32 * h + ql;
-                if (p < q && q < N)
-                {
-                    const double uu = (su[p] - su[q]) * kw;
-                    const double vv = (sv[p] - sv[q]) * kw;
-                    const double len = sqrt(uu * uu + vv * vv);
-                    if (!(len < prm.uv_min || len > prm.uv_max))
-                    {
-                        const double re = accR[ql] * inv_s2;
-                        const double im = accI[ql] * inv_s2;
-                        const int ro = prm.casa ? i : c;
-                        const int co = prm.casa ? c : i;
-                        double* o = vbase + 8 * (size_t) baseline_index(N, q, p)
-                                + 2 * (2 * ro + co);
-                        o[0] += re;
-                        o[1] += prm.casa ? im : -im;
-                    }
-                }
-            }
-        }
+            if (!wide_task_epilogue(prm, &ctl->mfull, &ctl->cfull, mpar,
+                    cpar, abort, taddr, row, lane, prob, rb,
+                    2 * cp * kStPerBlock + (kWEpiCols / 4) * h, nchunk,
+                    arrive))
+                break;
         }
     }
 
@@ -1087,6 +1103,306 @@ gemm_wide_kernel(const GemmParams prm)
     __syncthreads();
     ptx::tc_fence_after();
     if (warp == 1) ptx::tmem_dealloc(tmem, kWTmemCols);
+}
+
+// ===========================================================================
+// Pair tiles: two CTAs of a cluster (cta_group::2) compute one 256 x 256
+// tile of G: row blocks 2i and 2i + 1 (one per CTA) against column blocks
+// 2j and 2j + 1 (i <= j). Each CTA brings only its own row block (A) and
+// its own column block (half of B) into shared memory, 64 KB per k block,
+// and the even CTA issues M = 256, N = 256 MMAs that read A and B from both
+// CTAs' shared memory; each CTA's TMEM receives its 128 rows. Against the
+// wide tiles (96 KB per CTA per k block for the same products per CTA) this
+// moves a third fewer operand bytes per product from L2, and three 64 KB
+// stages fit where two 96 KB stages did.
+// Synchronisation between the two CTAs:
+//  - each CTA's producer fills its own stage (local full barrier); in the
+//    odd CTA a relay thread waits for that and arrives on the even CTA's
+//    pfull barrier, so the MMA issuer waits for both halves;
+//  - the MMA issuer's commits arrive on the empty, mfull and cfull barriers
+//    at the same offset in both CTAs (multicast commit);
+//  - the epilogue warps of both CTAs arrive on the even CTA's mempty and
+//    cempty barriers (16 arrivals each) before the accumulators are reused.
+// Everything else (drain interval, correction period, register split,
+// epilogue) is that of the wide kernel.
+// ===========================================================================
+constexpr int kPStages = 3;
+constexpr int kPStageBytes = 2 * kPairBytes;  // A pair + B pair (own half)
+
+struct PairCtl
+{
+    uint64_t full[kPStages], pfull[kPStages], empty[kPStages], mfull,
+            mempty, cfull, cempty, done;
+    uint32_t tmem_base;
+    int abort;
+};
+
+constexpr size_t gemm_pair_smem_bytes()
+{
+    return 1024 + (size_t) kPStages * kPStageBytes + sizeof(PairCtl);
+}
+
+__host__ __device__ inline int pair_tiles(int nrb)
+{
+    const int np = (nrb + 1) / 2;
+    return np * (np + 1) / 2;
+}
+
+__global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kWThreads, 1)
+gemm_pair_kernel(const GemmParams prm)
+{
+    extern __shared__ uint8_t smem_raw[];
+    uint8_t* smem = reinterpret_cast<uint8_t*>(
+            (reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~(uintptr_t) 1023);
+    PairCtl* ctl = reinterpret_cast<PairCtl*>(smem + kPStages * kPStageBytes);
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const uint32_t rank = ptx::cluster_ctarank();
+    volatile int* abort = &ctl->abort;
+
+    if (threadIdx.x == 0)
+    {
+        for (int s = 0; s < kPStages; ++s)
+        {
+            ptx::mbar_init(&ctl->full[s], 1);
+            ptx::mbar_init(&ctl->pfull[s], 1);
+            ptx::mbar_init(&ctl->empty[s], 1);
+        }
+        ptx::mbar_init(&ctl->mfull, 1);
+        ptx::mbar_init(&ctl->mempty, 2 * kWEpiWarps);
+        ptx::mbar_init(&ctl->cfull, 1);
+        ptx::mbar_init(&ctl->cempty, 2 * kWEpiWarps);
+        ptx::mbar_init(&ctl->done, 1);
+        ctl->abort = 0;
+        ptx::fence_mbar_init();
+    }
+    if (warp == 1) ptx::tmem_alloc_pair(&ctl->tmem_base, kWTmemCols);
+    ptx::tc_fence_before();
+    // both CTAs' barriers initialised and TMEM allocated before any
+    // cross-CTA arrive or MMA
+    ptx::cluster_sync();
+    ptx::tc_fence_after();
+    const uint32_t tmem = ctl->tmem_base;
+
+    const int np = (prm.nrb + 1) / 2;
+    const int ntile = pair_tiles(prm.nrb);
+    const int npairs = gridDim.x >> 1;
+    const int pair = blockIdx.x >> 1;
+    const int ntasks = ntile * prm.num_problems;
+    const int nchunk = (prm.nkb + prm.drain_kb - 1) / prm.drain_kb;
+    (void) np;
+
+    if (warp < 4)
+    {
+    ptx::regs_release<kWLowRegs>();
+    if (warp == 0)
+    {
+        if (lane == 0)
+        {
+            // ---------------- producer: this CTA's row block (A pair) and
+            // column block (B pair) of every k block
+            int stage = 0;
+            uint32_t phase = 0;
+            uint32_t issued = 0, issued_par = 0;
+            for (int task = pair; task < ntasks && !*abort; task += npairs)
+            {
+                const int prob = task / ntile;
+                int ti, tj;
+                tile_of(task - prob * ntile, ti, tj);
+                // a missing odd block (odd number of row blocks) repeats the
+                // even one; its rows and columns are discarded (p, q >= N)
+                int rb = 2 * ti + (int) rank, cb = 2 * tj + (int) rank;
+                if (rb >= prm.nrb) rb = prm.nrb - 1;
+                if (cb >= prm.nrb) cb = prm.nrb - 1;
+                const uint8_t* img = prm.W + (size_t) prob * prm.image_stride;
+                for (int kb = 0; kb < prm.nkb; ++kb)
+                {
+                    if (!ptx::mbar_wait(&ctl->empty[stage], phase ^ 1,
+                            prm.err, 31, abort))
+                        break;
+                    uint8_t* dst = smem + (size_t) stage * kPStageBytes;
+                    ptx::mbar_arrive_expect_tx(&ctl->full[stage],
+                            kPStageBytes);
+                    ptx::bulk_g2s(dst, img + ((size_t) rb * prm.nkb + kb) *
+                            kPairBytes, kPairBytes, &ctl->full[stage]);
+                    ptx::bulk_g2s(dst + kPairBytes, img +
+                            ((size_t) cb * prm.nkb + kb) * kPairBytes,
+                            kPairBytes, &ctl->full[stage]);
+                    issued |= 1u << stage;
+                    issued_par = (issued_par & ~(1u << stage)) |
+                            (phase << stage);
+                    if (++stage == kPStages) { stage = 0; phase ^= 1; }
+                }
+            }
+            for (int s = 0; s < kPStages; ++s)
+                if ((issued >> s) & 1)
+                    ptx::mbar_wait(&ctl->full[s], (issued_par >> s) & 1,
+                            prm.err, 32, abort);
+        }
+        __syncwarp();
+    }
+    else if (warp == 1)
+    {
+        if (lane == 0 && rank == 0)
+        {
+            // ---------------- MMA issuer (even CTA only)
+            const uint32_t idesc = ptx::idesc_f16_f32(256, kWCols);
+            const uint32_t dm = tmem, dcr = tmem + kWCols;
+            int stage = 0;
+            uint32_t phase = 0, mpar = 0, cpar = 0;
+            bool ok = true;
+            for (int task = pair; task < ntasks && ok; task += npairs)
+            {
+                for (int ch = 0; ch < nchunk && ok; ++ch)
+                {
+                    const bool fresh = (ch % kCorrPeriods) == 0;
+                    if (fresh)
+                    {
+                        if (!ptx::mbar_wait_cluster(&ctl->cempty, cpar ^ 1,
+                                prm.err, 33, abort))
+                        {
+                            ok = false;
+                            break;
+                        }
+                        ptx::tc_fence_after();
+                    }
+                    const int kb0 = ch * prm.drain_kb;
+                    const int kb1 = min(prm.nkb, kb0 + prm.drain_kb);
+                    for (int kb = kb0; kb < kb1; ++kb)
+                    {
+                        if (!ptx::mbar_wait(&ctl->full[stage], phase, prm.err,
+                                34, abort) ||
+                                !ptx::mbar_wait_cluster(&ctl->pfull[stage],
+                                phase, prm.err, 35, abort))
+                        {
+                            ok = false;
+                            break;
+                        }
+                        ptx::tc_fence_after();
+                        const uint32_t a = ptx::smem_u32(smem +
+                                (size_t) stage * kPStageBytes);
+                        const uint32_t al = a + kTileBytes;
+                        const uint32_t bh = a + kPairBytes;
+                        const uint32_t bl = bh + kTileBytes;
+                        // correction products first (hi lo^T + lo hi^T)
+#pragma unroll
+                        for (int k = 0; k < kKSteps; ++k)
+                        {
+                            const uint32_t first =
+                                    (fresh && kb == kb0 && k == 0) ? 0u : 1u;
+                            ptx::mma_f16_pair(dcr,
+                                    ptx::sdesc_sw128(a + 32 * k),
+                                    ptx::sdesc_sw128(bl + 32 * k), idesc,
+                                    first);
+                            ptx::mma_f16_pair(dcr,
+                                    ptx::sdesc_sw128(al + 32 * k),
+                                    ptx::sdesc_sw128(bh + 32 * k), idesc, 1u);
+                        }
+                        if (kb == kb0)
+                        {
+                            if (!ptx::mbar_wait_cluster(&ctl->mempty,
+                                    mpar ^ 1, prm.err, 36, abort))
+                            {
+                                ok = false;
+                                break;
+                            }
+                            ptx::tc_fence_after();
+                        }
+#pragma unroll
+                        for (int k = 0; k < kKSteps; ++k)
+                            ptx::mma_f16_pair(dm,
+                                    ptx::sdesc_sw128(a + 32 * k),
+                                    ptx::sdesc_sw128(bh + 32 * k), idesc,
+                                    (kb > kb0 || k > 0) ? 1u : 0u);
+                        ptx::mma_commit_pair(&ctl->empty[stage]);
+                        if (++stage == kPStages) { stage = 0; phase ^= 1; }
+                    }
+                    if (!ok) break;
+                    ptx::mma_commit_pair(&ctl->mfull);
+                    mpar ^= 1;
+                    if (corr_drain_at(ch, nchunk))
+                    {
+                        ptx::mma_commit_pair(&ctl->cfull);
+                        cpar ^= 1;
+                    }
+                }
+            }
+            // every tcgen05 instruction of this kernel is cta_group::2
+            ptx::mma_commit_pair(&ctl->done);
+            ptx::mbar_wait(&ctl->done, 0, prm.err, 37, abort);
+        }
+        __syncwarp();
+    }
+    else if (warp == 2)
+    {
+        if (lane == 0 && rank == 1)
+        {
+            // ---------------- relay (odd CTA): each of its stages, once
+            // filled, is reported to the even CTA's MMA issuer
+            const uint32_t pfull0 = ptx::mapa_shared(
+                    ptx::smem_u32(&ctl->pfull[0]), 0);
+            int stage = 0;
+            uint32_t phase = 0;
+            for (int task = pair; task < ntasks && !*abort; task += npairs)
+            {
+                bool ok = true;
+                for (int kb = 0; kb < prm.nkb; ++kb)
+                {
+                    if (!ptx::mbar_wait(&ctl->full[stage], phase, prm.err,
+                            38, abort))
+                    {
+                        ok = false;
+                        break;
+                    }
+                    ptx::mbar_arrive_cluster(pfull0 +
+                            (uint32_t) (stage * sizeof(uint64_t)));
+                    if (++stage == kPStages) { stage = 0; phase ^= 1; }
+                }
+                if (!ok) break;
+            }
+        }
+        __syncwarp();
+    }
+    }  // warpgroup 0
+    else
+    {
+        // ---------------- epilogue warps (4 and up), kWEpiCols columns each
+        ptx::regs_request<kWHighRegs>();
+        const int q4 = warp & 3;
+        const int h = (warp - 4) >> 2;
+        const int row = 32 * q4 + lane;
+        const uint32_t taddr = tmem + ((uint32_t) (32 * q4) << 16) +
+                (uint32_t) (kWEpiCols * h);
+        const uint32_t mempty0 = ptx::mapa_shared(
+                ptx::smem_u32(&ctl->mempty), 0);
+        const uint32_t cempty0 = ptx::mapa_shared(
+                ptx::smem_u32(&ctl->cempty), 0);
+        uint32_t mpar = 0, cpar = 0;
+        auto arrive = [&](bool with_corr) {
+            ptx::mbar_arrive_cluster(mempty0);
+            if (with_corr) ptx::mbar_arrive_cluster(cempty0);
+        };
+        for (int task = pair; task < ntasks; task += npairs)
+        {
+            const int prob = task / ntile;
+            int ti, tj;
+            tile_of(task - prob * ntile, ti, tj);
+            // columns 0-127 of the accumulator are column block 2 tj,
+            // 128-255 column block 2 tj + 1
+            if (!wide_task_epilogue(prm, &ctl->mfull, &ctl->cfull, mpar,
+                    cpar, abort, taddr, row, lane, prob,
+                    2 * ti + (int) rank,
+                    2 * tj * kStPerBlock + (kWEpiCols / 4) * h, nchunk,
+                    arrive))
+                break;
+        }
+    }
+
+    ptx::tc_fence_before();
+    // no CTA leaves (or frees TMEM) while its peer may still arrive on its
+    // barriers or its MMAs read the other's shared memory
+    ptx::cluster_sync();
+    ptx::tc_fence_after();
+    if (warp == 1) ptx::tmem_dealloc_pair(tmem, kWTmemCols);
 }
 
 }  // namespace tc
@@ -1115,6 +1431,13 @@ int drain_kblocks()
     static int d = 0;
     if (!d)
     {
+        // every 2 k blocks (8 main-product MMA steps) by default. The FP32
+        // accumulator's error grows with the interval (at 512 stations x
+        // 100,000 sources, against the FP64 kernel: L2 / max relative
+        // 2.55e-7 / 3.36e-7 at 2, 3.46e-7 / 5.07e-7 at 3, 4.56e-7 / 7.02e-7
+        // at 4) while the drain's cost falls (46.1, 43.0, 40.9 ms per
+        // launch); at 3 a 31-station x 100-source case already reached
+        // 1.007e-6 max relative, past the 1e-6 bound, so 2 stays
         const char* e = getenv("OSKB_TC_DRAIN_KB");
         d = e ? atoi(e) : 2;
         if (d < 1) d = 1;
@@ -1198,14 +1521,15 @@ bool g_timing = false;
 std::vector<std::pair<cudaEvent_t, cudaEvent_t>> g_ev;
 size_t g_ev_used = 0;
 
-// Tile width of the contraction: OSKB_TC_TILE=128 (square tiles) or 256
-// (wide tiles); unset: wide tiles when a launch has at least two per SM
-// (with fewer, the square tiles keep more SMs busy).
+// Tile shape of the contraction: OSKB_TC_TILE=128 (square 128 x 128
+// tiles), 256 (wide 128 x 256 tiles) or 512 (256 x 256 pair tiles on two
+// CTAs); unset: wide tiles when a launch has at least two per SM, else
+// square tiles (with fewer tasks, the smaller tiles keep more SMs busy).
 int tile_setting()
 {
     const char* e = getenv("OSKB_TC_TILE");
     const int t = e ? atoi(e) : 0;
-    return (t == 128 || t == 256) ? t : 0;
+    return (t == 128 || t == 256 || t == 512) ? t : 0;
 }
 
 std::atomic<int> g_last_tile{0};
@@ -1219,11 +1543,12 @@ struct DeviceSetup
 {
     bool done;
     bool wide_fits;
+    bool pair_fits;
 };
 std::mutex g_setup_mutex;
 DeviceSetup g_setup[64] = {};
 
-int device_setup(bool& wide_fits)
+int device_setup(bool& wide_fits, bool& pair_fits)
 {
     const int dev = current_device();
     if (dev < 0 || dev >= 64) return OSKB_ERR_CUDA_NOT_AVAILABLE;
@@ -1236,7 +1561,10 @@ int device_setup(bool& wide_fits)
                 (int) gemm_smem_bytes()) != cudaSuccess ||
                 cudaFuncSetAttribute(gemm_wide_kernel,
                 cudaFuncAttributeMaxDynamicSharedMemorySize,
-                (int) gemm_wide_smem_bytes()) != cudaSuccess)
+                (int) gemm_wide_smem_bytes()) != cudaSuccess ||
+                cudaFuncSetAttribute(gemm_pair_kernel,
+                cudaFuncAttributeMaxDynamicSharedMemorySize,
+                (int) gemm_pair_smem_bytes()) != cudaSuccess)
         {
             set_last_error("tc gemm attributes", cudaGetLastError());
             return OSKB_ERR_KERNEL_LAUNCH_FAILURE;
@@ -1244,31 +1572,47 @@ int device_setup(bool& wide_fits)
         cudaFuncAttributes fa;
         d.wide_fits = cudaFuncGetAttributes(&fa, gemm_wide_kernel) ==
                 cudaSuccess && (long long) fa.numRegs * kWThreads >=
-                128LL * kWLowRegs + 256LL * kWHighRegs;
+                128LL * kWLowRegs + (kWThreads - 128LL) * kWHighRegs;
         if (!d.wide_fits)
             set_last_error_msg("tc: wide contraction tiles disabled "
+                    "(register budget)");
+        d.pair_fits = cudaFuncGetAttributes(&fa, gemm_pair_kernel) ==
+                cudaSuccess && (long long) fa.numRegs * kWThreads >=
+                128LL * kWLowRegs + (kWThreads - 128LL) * kWHighRegs;
+        if (!d.pair_fits)
+            set_last_error_msg("tc: pair contraction tiles disabled "
                     "(register budget)");
         d.done = true;
     }
     wide_fits = d.wide_fits;
+    pair_fits = d.pair_fits;
     return 0;
 }
 
 int launch_gemm(GemmParams& gp, cudaStream_t stream)
 {
-    bool wide_fits = false;
-    const int serr = device_setup(wide_fits);
+    bool wide_fits = false, pair_fits = false;
+    const int serr = device_setup(wide_fits, pair_fits);
     if (serr) return serr;
     const long long square = (long long) gp.nrb * (gp.nrb + 1) / 2 *
             gp.num_problems;
     const long long wide_n = (long long) wide_tiles(gp.nrb) *
             gp.num_problems;
+    const long long pair_n = (long long) pair_tiles(gp.nrb) *
+            gp.num_problems;
     const int setting = tile_setting();
-    const bool wide = wide_fits && (setting == 256 ||
+    const int pairs = num_sms() / 2;
+    // pair tiles only on request: on one B200 at 512 stations x 100,000
+    // sources x 16 channels they measured 52.6 ms per launch against 46.1 ms
+    // for the wide tiles (drain every 2 blocks), 44.8 against 43.0 (every 3)
+    const bool pair = pair_fits && setting == 512;
+    const bool wide = !pair && wide_fits && (setting == 256 ||
             (setting == 0 && wide_n >= 2LL * num_sms()));
-    const long long ntasks = wide ? wide_n : square;
-    const int grid = (int) (ntasks < num_sms() ? ntasks : num_sms());
-    g_last_tile.store(wide ? 256 : 128);
+    const long long ntasks = pair ? pair_n : wide ? wide_n : square;
+    int grid = (int) (ntasks < num_sms() ? ntasks : num_sms());
+    if (pair)
+        grid = 2 * (int) (pair_n < pairs ? pair_n : pairs);
+    g_last_tile.store(pair ? 512 : wide ? 256 : 128);
     gp.drain_kb = drain_kblocks();
     cudaEvent_t ev_stop = nullptr;
     {
@@ -1287,7 +1631,10 @@ int launch_gemm(GemmParams& gp, cudaStream_t stream)
             ++g_ev_used;
         }
     }
-    if (wide)
+    if (pair)
+        gemm_pair_kernel<<<grid, kWThreads, gemm_pair_smem_bytes(),
+                stream>>>(gp);
+    else if (wide)
         gemm_wide_kernel<<<grid, kWThreads, gemm_wide_smem_bytes(),
                 stream>>>(gp);
     else

@@ -90,13 +90,15 @@ def test_tc_jones_api(nst, nsrc, casa):
     assert flags[0] == 0 and flags[1] == 0
 
 
-@pytest.mark.parametrize("tile", [128, 256])
+@pytest.mark.parametrize("tile", [128, 256, 512])
 @pytest.mark.parametrize("nst,nsrc,casa", [(17, 300, 0), (64, 1000, 1),
-                                           (130, 777, 0), (161, 2050, 1)])
+                                           (130, 777, 0), (161, 2050, 1),
+                                           (200, 1200, 0)])
 def test_tc_tile_widths(tile, nst, nsrc, casa, monkeypatch):
-    """Square (128 x 128) and wide (128 x 256) contraction tiles, with an
-    even and an odd number of 32-station row blocks (17 and 161 stations:
-    one and six blocks; 130: five), against the oracle."""
+    """Square (128 x 128), wide (128 x 256) and pair (256 x 256 on two CTAs)
+    contraction tiles, with an even and an odd number of 32-station row
+    blocks (17, 64, 130, 161 and 200 stations: one, two, five, six and
+    seven blocks), against the oracle."""
     monkeypatch.setenv("OSKB_TC_TILE", str(tile))
     rng = np.random.default_rng(nst * 7 + nsrc)
     l, m, n, I, Q, U, V = sky(rng, nsrc)
@@ -123,12 +125,12 @@ def test_tc_tile_widths(tile, nst, nsrc, casa, monkeypatch):
     assert flags[0] == 0 and flags[1] == 0
 
 
-@pytest.mark.parametrize("tile", [128, 256])
+@pytest.mark.parametrize("tile", [256, 512])
 def test_tc_block_tile_widths_agree(tile, monkeypatch):
     """A block of 2 dumps x 3 channels at 97 stations (four row blocks)
-    through both tile widths: within the compensated tolerance of each
-    other and of the oracle (checked for the wide tiles in
-    test_tc_tile_widths)."""
+    through the square tiles and the wide or pair tiles: within the
+    compensated tolerance of each other (each is checked against the
+    oracle in test_tc_tile_widths)."""
     rng = np.random.default_rng(5)
     nst, nsrc, ntime, nchan = 97, 900, 2, 3
     l, m, n, I, Q, U, V = sky(rng, nsrc)
@@ -137,7 +139,7 @@ def test_tc_block_tile_widths_agree(tile, monkeypatch):
     inv_wl = (120e6 + 1e6 * np.arange(nchan)) / C0
     nbl = nst * (nst - 1) // 2
     out = {}
-    for t in (128, 256):
+    for t in (128, tile):
         monkeypatch.setenv("OSKB_TC_TILE", str(t))
         vis = torch.zeros(ntime * nchan * nbl * 8, dtype=torch.float64,
                           device="cuda")
@@ -148,7 +150,7 @@ def test_tc_block_tile_widths_agree(tile, monkeypatch):
         torch.cuda.synchronize()
         assert ob.load().oskb_tc_tile_columns() == t
         out[t] = vis.cpu().numpy()
-    l2, mx = errors(out[tile], out[384 - tile])
+    l2, mx = errors(out[tile], out[128])
     assert l2 <= TOL and mx <= TOL, (l2, mx)
 
 
@@ -254,7 +256,7 @@ def test_tc_block_small_workspace_groups():
     assert np.array_equal(out[0], out[1])
 
 
-@pytest.mark.parametrize("tile", [128, 256])
+@pytest.mark.parametrize("tile", [128, 256, 512])
 def test_tc_block_auto_correlations_fused(tile, monkeypatch):
     """Auto-correlations from the same contraction (the diagonal station
     pairs of the diagonal tiles) against the oracle's auto-correlation of
