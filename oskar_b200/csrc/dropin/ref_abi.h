@@ -212,6 +212,44 @@ oskar_Harp* oskar_telescope_harp_data(oskar_Telescope* model,
         double freq_hz);
 // oskar/gains/oskar_gains.h
 int oskar_gains_defined(const oskar_Gains* h);
+typedef struct oskar_Element oskar_Element;
+// oskar/telescope/station/oskar_station_accessors.h
+int oskar_station_num_elements(const oskar_Station* model);
+int oskar_station_num_element_types(const oskar_Station* model);
+int oskar_station_normalise_array_pattern(const oskar_Station* model);
+int oskar_station_normalise_element_pattern(const oskar_Station* model);
+int oskar_station_enable_array_pattern(const oskar_Station* model);
+int oskar_station_common_element_orientation(const oskar_Station* model);
+int oskar_station_common_pol_beams(const oskar_Station* model);
+int oskar_station_apply_element_errors(const oskar_Station* model);
+int oskar_station_apply_element_weight(const oskar_Station* model);
+int oskar_station_swap_xy(const oskar_Station* model);
+int oskar_station_array_is_3d(const oskar_Station* model);
+int oskar_station_has_child(const oskar_Station* model);
+double oskar_station_element_euler_index_rad(const oskar_Station* model,
+        int feed, int dim, int index);
+const oskar_Mem* oskar_station_element_true_enu_metres_const(
+        const oskar_Station* model, int feed, int dim);
+const oskar_Mem* oskar_station_element_measured_enu_metres_const(
+        const oskar_Station* model, int feed, int dim);
+const oskar_Mem* oskar_station_element_cable_length_error_metres_const(
+        const oskar_Station* model, int feed);
+const int* oskar_station_element_types_cpu_const(const oskar_Station* model);
+const oskar_Element* oskar_station_element_const(const oskar_Station* model,
+        int element_type_index);
+const oskar_Gains* oskar_station_gains_const(const oskar_Station* model);
+const oskar_Harp* oskar_station_harp_data_const(const oskar_Station* model,
+        double freq_hz);
+void oskar_station_beam_horizon_direction(const oskar_Station* station,
+        const double gast_rad, double* x, double* y, double* z, int* status);
+// oskar/telescope/station/element/oskar_element_accessors.h
+int oskar_element_num_freq(const oskar_Element* data);
+int oskar_element_is_isotropic(const oskar_Element* data);
+int oskar_element_taper_type(const oskar_Element* data);
+double oskar_element_cosine_power(const oskar_Element* data);
+double oskar_element_gaussian_fwhm_rad(const oskar_Element* data);
+double oskar_element_dipole_length(const oskar_Element* data);
+int oskar_element_dipole_length_units(const oskar_Element* data);
 // oskar/telescope/station/oskar_station_accessors.h
 int oskar_station_type(const oskar_Station* model);
 int oskar_station_normalise_final_beam(const oskar_Station* model);

@@ -28,9 +28,15 @@
 //
 // Station beams: isotropic stations (identity E, or zero while the station
 // beam direction is below the horizon, oskar_station_beam.c:84-93, 141-144)
-// are built here. Other station types, HARP element data, ionospheric
-// screens and HDF5 gain models return OSKAR_ERR_FUNCTION_NOT_AVAILABLE with
-// a log message: there is no CPU fallback.
+// and aperture-array stations without child stations whose elements share
+// one orientation and one set of data for both feeds (dipole or isotropic
+// elements, up to four element types, cosine or Gaussian tapers, measured
+// positions and cable-length errors in the weights, array, element and
+// final normalisation), through the fused station-beam kernels. Other
+// station types and features (child stations, element errors, apodisation,
+// numerical element patterns, HARP data, ionospheric screens, gain models)
+// return OSKAR_ERR_FUNCTION_NOT_AVAILABLE with a log message: there is no
+// CPU fallback.
 #include <cuda_runtime.h>
 #include <math.h>
 #include <stdint.h>
@@ -106,8 +112,8 @@ State* state_for(const void* h, int device_id)
 
 // ---------------------------------------------------------------- kernels
 // Isotropic station beams: identity (matrix) or 1 (scalar) per
-// station-source, zero for stations whose beam direction is below the
-// horizon (station_off[p] != 0).
+// station-source where station_off[p] == 0, zero where it is 1 (the beam
+// direction is below the horizon); rows with 2 are left as they are.
 template <typename T>
 __global__ void isotropic_beam_kernel(int num_src, int num_st, int matrix,
         const int* __restrict__ station_off, T* __restrict__ E)
@@ -118,6 +124,7 @@ __global__ void isotropic_beam_kernel(int num_src, int num_st, int matrix,
             i += (size_t) gridDim.x * blockDim.x)
     {
         const int p = (int) (i / num_src);
+        if (station_off[p] == 2) continue;   // computed by the AA kernel
         const T one = station_off[p] ? (T) 0 : (T) 1;
         T* e = E + w * i;
         e[0] = one;
@@ -302,7 +309,8 @@ private:
     void sim_baselines(const RefSky* sky, int num_src, const T* table,
             const int* valid, int chan_block, int time_block, int chan_sim,
             int time_sim);
-    void station_beams(int num_src, double gast);
+    void station_beams(int num_src, double gast, const T* ra, const T* dec,
+            double freq);
 
     RefInterferometer* h_;
     State* st_;
@@ -411,8 +419,57 @@ int Runner<T>::horizon_clip(const RefSky* sky, double gast)
 }
 
 // Station beams E [station][source] for this dump and channel.
+// One aperture-array station model, as the fused station-beam kernel takes
+// it (oskar_evaluate_station_beam_aperture_array.c:153-240 for a station
+// without child stations, elements of common orientation and one set of
+// element data for both feeds).
+struct AaModel
+{
+    int model;                    // index of the station model
+    int num_elements, num_types;
+    int norm_element, norm_array, norm_final, swap_xy, is_3d;
+    std::vector<double> length, taper_param;   // per element type
+    std::vector<int> length_units, kind, taper;
+    double euler_x, euler_y;
+    double lat, lst;
+    double beam_enu[3], norm_enu[3];
+
+    bool same_launch(const AaModel& o) const
+    {
+        return num_elements == o.num_elements && num_types == o.num_types &&
+                norm_element == o.norm_element &&
+                norm_array == o.norm_array && norm_final == o.norm_final &&
+                swap_xy == o.swap_xy && is_3d == o.is_3d &&
+                length == o.length && length_units == o.length_units &&
+                kind == o.kind && taper == o.taper &&
+                taper_param == o.taper_param;
+    }
+};
+
+// Copies a station model's beams into the rows of the stations that use
+// it: E[p] = E_model[slot[p]] (rows of num_src values of w reals).
 template <typename T>
-void Runner<T>::station_beams(int num_src, double gast)
+__global__ void gather_beams_kernel(int num_src, int num_st, int w,
+        const int* __restrict__ slot, const T* __restrict__ Em,
+        T* __restrict__ E)
+{
+    const size_t row = (size_t) num_src * w;
+    const size_t n = row * num_st;
+    for (size_t i = (size_t) blockIdx.x * blockDim.x + threadIdx.x; i < n;
+            i += (size_t) gridDim.x * blockDim.x)
+    {
+        const size_t p = i / row, k = i - p * row;
+        E[i] = Em[(size_t) slot[p] * row + k];
+    }
+}
+
+// Station beams E [station][source] for this dump and channel: each station
+// model that the stations use is evaluated once (the reference's
+// oskar_evaluate_jones_E with station-beam duplication, :140-188, or every
+// station without it), then copied to its stations.
+template <typename T>
+void Runner<T>::station_beams(int num_src, double gast, const T* ra,
+        const T* dec, double freq)
 {
     if (!ok()) return;
     const int dup = oskar_telescope_allow_station_beam_duplication(tel_);
@@ -424,37 +481,336 @@ void Runner<T>::station_beams(int num_src, double gast)
                 (int) oskar_mem_length(m) >= num_st_)
             type_map = (const int*) oskar_mem_void_const(m);
     }
-    std::vector<int> off(num_st_, 0);
+    // models to evaluate, in order of first use, and each station's slot
+    std::vector<int> models, slot(num_st_);
+    std::map<int, int> slot_of_model;
     for (int p = 0; p < num_st_; ++p)
     {
         const int model = type_map ? type_map[p] : p;
-        const oskar_Station* st = oskar_telescope_station_const(tel_, model);
+        auto it = slot_of_model.find(model);
+        if (it == slot_of_model.end())
+        {
+            slot_of_model[model] = (int) models.size();
+            slot[p] = (int) models.size();
+            models.push_back(model);
+        }
+        else
+            slot[p] = it->second;
+    }
+    const int nm = (int) models.size();
+    // per model: 0 = identity (isotropic), 1 = zero (beam direction below
+    // the horizon, oskar_station_beam.c:84-93), 2 = aperture array
+    std::vector<int> mode(nm, 0);
+    std::vector<AaModel> aa;
+    const double c0 = 299792458.0;
+    const int pc_type = oskar_telescope_phase_centre_coord_type(tel_);
+    const double pc_lon = oskar_telescope_phase_centre_longitude_rad(tel_);
+    const double pc_lat = oskar_telescope_phase_centre_latitude_rad(tel_);
+    for (int k = 0; k < nm; ++k)
+    {
+        const oskar_Station* st = oskar_telescope_station_const(tel_,
+                models[k]);
         if (!st)
         {
             fail(REF_ERR_SETTINGS_TELESCOPE, "missing station model");
             return;
         }
-        if (oskar_station_type(st) != REF_STATION_TYPE_ISOTROPIC)
+        const int type = oskar_station_type(st);
+        if (beam_elevation(st, gast) < 0.0)
         {
-            fail(REF_ERR_FUNCTION_NOT_AVAILABLE, "only isotropic stations "
-                    "have a B200 station beam in this drop-in");
+            mode[k] = 1;
+            continue;
+        }
+        if (type == REF_STATION_TYPE_ISOTROPIC) continue;
+        if (type != REF_STATION_TYPE_AA)
+        {
+            fail(REF_ERR_FUNCTION_NOT_AVAILABLE, "Gaussian and VLA station "
+                    "beams are not built in this drop-in");
             return;
         }
-        off[p] = beam_elevation(st, gast) < 0.0;
+        if (oskar_station_has_child(st) ||
+                !oskar_station_common_element_orientation(st) ||
+                !oskar_station_enable_array_pattern(st) ||
+                (matrix_ && !oskar_station_common_pol_beams(st)) ||
+                oskar_station_apply_element_errors(st) ||
+                oskar_station_apply_element_weight(st) ||
+                oskar_gains_defined(oskar_station_gains_const(st)) ||
+                oskar_station_harp_data_const(st, freq) ||
+                oskar_station_num_element_types(st) > 4)
+        {
+            fail(REF_ERR_FUNCTION_NOT_AVAILABLE, "this aperture-array station "
+                    "(child stations, per-element orientations, separate "
+                    "feed data, element errors, apodisation, gain models, "
+                    "HARP data or more than four element types) is not "
+                    "built in this drop-in");
+            return;
+        }
+        AaModel a;
+        a.model = models[k];
+        a.num_elements = oskar_station_num_elements(st);
+        a.num_types = oskar_station_num_element_types(st);
+        a.norm_element = oskar_station_normalise_element_pattern(st);
+        a.norm_array = oskar_station_normalise_array_pattern(st);
+        a.norm_final = oskar_station_normalise_final_beam(st);
+        a.swap_xy = oskar_station_swap_xy(st);
+        a.is_3d = oskar_station_array_is_3d(st);
+        for (int t = 0; t < a.num_types; ++t)
+        {
+            const oskar_Element* e = oskar_station_element_const(st, t);
+            if (!e || oskar_element_num_freq(e) > 0)
+            {
+                fail(REF_ERR_FUNCTION_NOT_AVAILABLE, "numerical element "
+                        "patterns are not built in this drop-in");
+                return;
+            }
+            a.kind.push_back(oskar_element_is_isotropic(e) ?
+                    OSKB_ELEMENT_ISOTROPIC : OSKB_ELEMENT_DIPOLE);
+            a.taper.push_back(oskar_element_taper_type(e));
+            a.taper_param.push_back(a.taper.back() == OSKB_TAPER_COSINE ?
+                    oskar_element_cosine_power(e) :
+                    a.taper.back() == OSKB_TAPER_GAUSSIAN ?
+                    oskar_element_gaussian_fwhm_rad(e) : 0.0);
+            a.length.push_back(oskar_element_dipole_length(e));
+            a.length_units.push_back(oskar_element_dipole_length_units(e));
+        }
+        a.euler_x = oskar_station_element_euler_index_rad(st, 0, 0, 0);
+        a.euler_y = oskar_station_element_euler_index_rad(st, 1, 0, 0);
+        a.lat = oskar_station_lat_rad(st);
+        a.lst = gast + oskar_station_lon_rad(st);
+        int stt = 0;
+        oskar_station_beam_horizon_direction(st, gast, &a.beam_enu[0],
+                &a.beam_enu[1], &a.beam_enu[2], &stt);
+        if (stt) check(stt, "station beam direction");
+        // normalisation direction: the phase centre
+        // (oskar_station_beam.c:108-126)
+        if (pc_type == REF_COORDS_RADEC)
+        {
+            const double ha = a.lst - pc_lon;
+            const double sh = sin(ha), ch = cos(ha);
+            const double sd = sin(pc_lat), cd = cos(pc_lat);
+            const double sl = sin(a.lat), cl = cos(a.lat);
+            a.norm_enu[0] = -cd * sh;
+            a.norm_enu[1] = cl * sd - sl * cd * ch;
+            a.norm_enu[2] = sl * sd + cl * cd * ch;
+        }
+        else
+        {
+            fail(REF_ERR_FUNCTION_NOT_AVAILABLE, "beam normalisation needs "
+                    "an RA/Dec phase centre in this drop-in");
+            return;
+        }
+        mode[k] = 2;
+        aa.push_back(a);
     }
-    DevBuf& flags = st_->station_off;
-    check(flags.ensure((size_t) num_st_ * sizeof(int)), "beam buffers");
-    check(st_->E.ensure((size_t) num_st_ * num_src * (matrix_ ? 8 : 2) *
-            sizeof(T)), "beam buffers");
     if (!ok()) return;
-    cudaMemcpyAsync(flags.p, off.data(), num_st_ * sizeof(int),
+    const int w = matrix_ ? 8 : 2;
+    const size_t row = (size_t) num_src * w;
+    DevBuf& em = st_->J;   // model beams (J is free until K is joined)
+    check(em.ensure((size_t) nm * row * sizeof(T)), "beam buffers");
+    check(st_->E.ensure((size_t) num_st_ * row * sizeof(T)), "beam buffers");
+    if (!ok()) return;
+
+    // ---- aperture-array models, one launch per group of alike models
+    std::vector<int> aa_slot;
+    for (int k = 0; k < nm; ++k)
+        if (mode[k] == 2) aa_slot.push_back(k);
+    std::vector<char> done(aa.size(), 0);
+    for (size_t g0 = 0; g0 < aa.size() && ok(); ++g0)
+    {
+        if (done[g0]) continue;
+        std::vector<size_t> grp;
+        for (size_t j = g0; j < aa.size(); ++j)
+            if (!done[j] && aa[j].same_launch(aa[g0]))
+            {
+                grp.push_back(j);
+                done[j] = 1;
+            }
+        const AaModel& r = aa[g0];
+        const int ng = (int) grp.size(), ne = r.num_elements;
+        std::vector<T> el((size_t) 7 * ng * ne);
+        std::vector<int> etype((size_t) ng * ne);
+        std::vector<double> geo((size_t) 10 * ng);   // lat, lst, beam, norm
+        bool have_cable = false;
+        for (int gi = 0; gi < ng && ok(); ++gi)
+        {
+            const AaModel& a = aa[grp[gi]];
+            const oskar_Station* st = oskar_telescope_station_const(tel_,
+                    a.model);
+            for (int d = 0; d < 3; ++d)
+            {
+                const oskar_Mem* tm =
+                        oskar_station_element_true_enu_metres_const(st, 0, d);
+                const oskar_Mem* mm =
+                        oskar_station_element_measured_enu_metres_const(st, 0,
+                        d);
+                if (!tm || !mm || (int) oskar_mem_length(tm) < ne ||
+                        (int) oskar_mem_length(mm) < ne)
+                {
+                    fail(REF_ERR_SETTINGS_TELESCOPE, "element coordinates");
+                    return;
+                }
+                memcpy(&el[((size_t) d * ng + gi) * ne],
+                        oskar_mem_void_const(tm), ne * sizeof(T));
+                memcpy(&el[((size_t) (3 + d) * ng + gi) * ne],
+                        oskar_mem_void_const(mm), ne * sizeof(T));
+            }
+            const oskar_Mem* cm =
+                    oskar_station_element_cable_length_error_metres_const(st,
+                    0);
+            if (cm && (int) oskar_mem_length(cm) >= ne)
+            {
+                memcpy(&el[((size_t) 6 * ng + gi) * ne],
+                        oskar_mem_void_const(cm), ne * sizeof(T));
+                have_cable = true;
+            }
+            const int* types = oskar_station_element_types_cpu_const(st);
+            for (int e = 0; e < ne; ++e)
+                etype[(size_t) gi * ne + e] = types ? types[e] : 0;
+            geo[gi] = a.lat;
+            geo[ng + gi] = a.lst;
+            for (int d = 0; d < 3; ++d)
+            {
+                geo[2 * ng + 3 * gi + d] = a.beam_enu[d];
+                geo[5 * ng + 3 * gi + d] = a.norm_enu[d];
+            }
+            geo[8 * ng + gi] = a.euler_x;
+            geo[9 * ng + gi] = a.euler_y;
+        }
+        // per-type host parameters at this frequency
+        std::vector<double> len(r.num_types), orient((size_t) 2 * ng *
+                r.num_types);
+        for (int t = 0; t < r.num_types; ++t)
+            len[t] = r.length_units[t] == REF_WAVELENGTHS ?
+                    r.length[t] * (c0 / freq) : r.length[t];
+        for (int gi = 0; gi < ng; ++gi)
+            for (int t = 0; t < r.num_types; ++t)
+            {
+                orient[(size_t) gi * r.num_types + t] = geo[8 * ng + gi];
+                orient[(size_t) (ng + gi) * r.num_types + t] =
+                        geo[9 * ng + gi];
+            }
+        const size_t ebytes = el.size() * sizeof(T);
+        const size_t tbytes = etype.size() * sizeof(int);
+        const size_t gbytes = (size_t) 8 * ng * sizeof(double);
+        const size_t obytes = orient.size() * sizeof(double);
+        const size_t dirs = (size_t) 3 * ng * num_src * sizeof(T);
+        DevBuf& buf = st_->uvw64;
+        check(buf.ensure(ebytes + tbytes + gbytes + obytes + dirs + 1024),
+                "beam buffers");
+        if (!ok()) return;
+        uint8_t* b = buf.as<uint8_t>();
+        T* d_el = (T*) b;
+        int* d_type = (int*) (b + ebytes);
+        double* d_geo = (double*) (b + ebytes + tbytes);
+        double* d_orient = (double*) (b + ebytes + tbytes + gbytes);
+        T* d_dirs = (T*) (b + ((ebytes + tbytes + gbytes + obytes + 255) &
+                ~(size_t) 255));
+        cudaMemcpyAsync(d_el, el.data(), ebytes, cudaMemcpyHostToDevice, s_);
+        cudaMemcpyAsync(d_type, etype.data(), tbytes, cudaMemcpyHostToDevice,
+                s_);
+        cudaMemcpyAsync(d_geo, geo.data(), gbytes, cudaMemcpyHostToDevice,
+                s_);
+        cudaMemcpyAsync(d_orient, orient.data(), obytes,
+                cudaMemcpyHostToDevice, s_);
+        T* dx = d_dirs;
+        T* dy = dx + (size_t) ng * num_src;
+        T* dz = dy + (size_t) ng * num_src;
+        // source directions (east, north, up) at each model's station
+        int err = sizeof(T) == 8 ?
+                oskb_convert_ra_dec_to_enu_directions_d(num_src,
+                (const double*) ra, (const double*) dec, ng, d_geo + ng,
+                d_geo, (double*) dx, (double*) dy, (double*) dz, s_) :
+                oskb_convert_ra_dec_to_enu_directions_f(num_src,
+                (const float*) ra, (const float*) dec, ng, d_geo + ng, d_geo,
+                (float*) dx, (float*) dy, (float*) dz, s_);
+        check(err, "source directions");
+        // the group's models take consecutive slots of a staging area after
+        // the nm model rows: evaluated there, then copied to their slots
+        std::vector<int> kinds(r.kind), tapers(r.taper);
+        std::vector<double> tparam(r.taper_param);
+        const size_t ge = (size_t) ng * ne;
+        check(st_->R.ensure((size_t) ng * row * sizeof(T)), "beam buffers");
+        if (!ok()) return;
+        T* out = st_->R.as<T>();
+        const T* cab = have_cable ? d_el + 6 * ge : nullptr;
+        const int nf = r.norm_final;
+        if (sizeof(T) == 8 && matrix_)
+            err = oskb_station_beam_aa_types_d(ng, ne, (const double*) d_el,
+                    (const double*) d_el + ge, (const double*) d_el + 2 * ge,
+                    (const double*) d_el + 3 * ge,
+                    (const double*) d_el + 4 * ge,
+                    (const double*) d_el + 5 * ge, (const double*) cab,
+                    nullptr, r.num_types, d_type, len.data(), kinds.data(),
+                    tapers.data(), tparam.data(), d_orient,
+                    d_orient + (size_t) ng * r.num_types, r.norm_element,
+                    r.norm_array, nf, r.swap_xy, r.is_3d, freq, d_geo + 2 * ng,
+                    d_geo + 5 * ng, num_src, (const double*) dx,
+                    (const double*) dy, (const double*) dz, 1, (double*) out,
+                    s_);
+        else if (sizeof(T) == 8)
+            err = oskb_station_beam_aa_scalar_d(ng, ne, (const double*) d_el,
+                    (const double*) d_el + ge, (const double*) d_el + 2 * ge,
+                    (const double*) d_el + 3 * ge,
+                    (const double*) d_el + 4 * ge,
+                    (const double*) d_el + 5 * ge, (const double*) cab,
+                    nullptr, r.num_types, d_type, len.data(), kinds.data(),
+                    tapers.data(), tparam.data(), d_orient,
+                    d_orient + (size_t) ng * r.num_types, r.norm_element,
+                    r.norm_array, nf, r.swap_xy, r.is_3d, freq, d_geo + 2 * ng,
+                    d_geo + 5 * ng, num_src, (const double*) dx,
+                    (const double*) dy, (const double*) dz, 1, (double*) out,
+                    s_);
+        else if (matrix_)
+            err = oskb_station_beam_aa_types_f(ng, ne, (const float*) d_el,
+                    (const float*) d_el + ge, (const float*) d_el + 2 * ge,
+                    (const float*) d_el + 3 * ge, (const float*) d_el + 4 * ge,
+                    (const float*) d_el + 5 * ge, (const float*) cab, nullptr,
+                    r.num_types, d_type, len.data(), kinds.data(),
+                    tapers.data(), tparam.data(), d_orient,
+                    d_orient + (size_t) ng * r.num_types, r.norm_element,
+                    r.norm_array, nf, r.swap_xy, r.is_3d, freq, d_geo + 2 * ng,
+                    d_geo + 5 * ng, num_src, (const float*) dx,
+                    (const float*) dy, (const float*) dz, 1, (float*) out, s_);
+        else
+            err = oskb_station_beam_aa_scalar_f(ng, ne, (const float*) d_el,
+                    (const float*) d_el + ge, (const float*) d_el + 2 * ge,
+                    (const float*) d_el + 3 * ge, (const float*) d_el + 4 * ge,
+                    (const float*) d_el + 5 * ge, (const float*) cab, nullptr,
+                    r.num_types, d_type, len.data(), kinds.data(),
+                    tapers.data(), tparam.data(), d_orient,
+                    d_orient + (size_t) ng * r.num_types, r.norm_element,
+                    r.norm_array, nf, r.swap_xy, r.is_3d, freq, d_geo + 2 * ng,
+                    d_geo + 5 * ng, num_src, (const float*) dx,
+                    (const float*) dy, (const float*) dz, 1, (float*) out, s_);
+        check(err, "aperture-array station beams");
+        for (int gi = 0; gi < ng && ok(); ++gi)
+            cudaMemcpyAsync(em.as<T>() + (size_t) aa_slot[grp[gi]] * row,
+                    out + (size_t) gi * row, row * sizeof(T),
+                    cudaMemcpyDeviceToDevice, s_);
+        // host vectors must outlive their copies
+        cudaStreamSynchronize(s_);
+    }
+    if (!ok()) return;
+
+    // ---- isotropic and below-horizon models, then the copy to stations
+    DevBuf& flags = st_->station_off;
+    check(flags.ensure((size_t) (nm + num_st_) * sizeof(int)),
+            "beam buffers");
+    if (!ok()) return;
+    std::vector<int> host(nm + num_st_);
+    for (int k = 0; k < nm; ++k) host[k] = mode[k];
+    for (int p = 0; p < num_st_; ++p) host[nm + p] = slot[p];
+    cudaMemcpyAsync(flags.p, host.data(), host.size() * sizeof(int),
             cudaMemcpyHostToDevice, s_);
-    const size_t n = (size_t) num_st_ * num_src;
-    const int grid = (int) std::min<size_t>((n + 255) / 256, 148 * 16);
-    isotropic_beam_kernel<T><<<grid, 256, 0, s_>>>(num_src, num_st_,
-            matrix_, flags.as<int>(), st_->E.as<T>());
+    const size_t n = (size_t) nm * num_src;
+    int grid = (int) std::min<size_t>((n + 255) / 256, 148 * 16);
+    isotropic_beam_kernel<T><<<grid, 256, 0, s_>>>(num_src, nm, matrix_,
+            flags.as<int>(), em.as<T>());
+    const size_t ns = (size_t) num_st_ * row;
+    grid = (int) std::min<size_t>((ns + 255) / 256, 148 * 16);
+    gather_beams_kernel<T><<<grid, 256, 0, s_>>>(num_src, num_st_, w,
+            flags.as<int>() + nm, em.as<T>(), st_->E.as<T>());
     check(launch_ok("station beams", log_), "station beams");
-    // the host vector must outlive the copy
     cudaStreamSynchronize(s_);
 }
 
@@ -560,7 +916,8 @@ void Runner<T>::sim_baselines(const RefSky* sky, int num_src, const T* tab,
     }
 
     // ---- Jones E, R and E R
-    station_beams(num_src, gast);
+    station_beams(num_src, gast, col(REF_SKY_RA_RAD), col(REF_SKY_DEC_RAD),
+            freq);
     if (!ok()) return;
     const size_t njones = (size_t) num_st_ * num_src;
     const size_t mat = njones * 8 * sizeof(T), cpx = njones * 2 * sizeof(T);

@@ -79,3 +79,60 @@ def c1_extended_case(precision="double", **over):
               "max_times_per_block": 4, "num_devices": 2})
     c.update(over)
     return c
+
+
+def c2_small_case(precision="double", per_station=True, **over):
+    """C2 scaled down: aperture-array stations (48 dipoles each at random
+    positions in a 38 m disc; one layout per station, or one shared by all)
+    placed log-radially out to 5 km, 400 point sources in a 10 deg field plus
+    80 at random directions, 10 % of them with Stokes Q and U, 3 channels
+    over 100-130 MHz, 4 dumps of 300 s, full polarisation. Sources below the
+    horizon are blanked by the station beams, so the horizon clip does not
+    change the result."""
+    rng = np.random.default_rng(22)
+    nst, nel, nsrc, noff = 12, 48, 400, 80
+    r = np.exp(rng.uniform(math.log(50.0), math.log(5e3), nst))
+    th = rng.uniform(0, 2 * math.pi, nst)
+
+    def layout():
+        rr = 19.0 * np.sqrt(rng.uniform(0, 1, nel))
+        tt = rng.uniform(0, 2 * math.pi, nel)
+        return (rr * np.cos(tt)).tolist(), (rr * np.sin(tt)).tolist()
+    lays = [layout() for _ in range(nst if per_station else 1)]
+    ra0, dec0 = 0.0, math.radians(-30.0)
+    l, m, _ = workloads.disc_lmn(rng, nsrc, 10.0)
+    ra, dec = lm_to_radec(l, m, ra0, dec0)
+    ra = np.concatenate([ra, rng.uniform(0, 2 * math.pi, noff)])
+    dec = np.concatenate([dec, np.arcsin(rng.uniform(-1, 1, noff))])
+    n = nsrc + noff
+    I = workloads.power_law_flux(rng, n)
+    pol = rng.uniform(0, 1, n) < 0.1
+    Q = np.where(pol, rng.normal(0, 0.05, n) * I, 0.0)
+    U = np.where(pol, rng.normal(0, 0.05, n) * I, 0.0)
+    z = [0.0] * n
+    case = {
+        "precision": precision, "pol_mode": "Full",
+        "lon_deg": workloads.LON_DEG, "lat_deg": workloads.LAT_DEG,
+        "station_x": (r * np.cos(th)).tolist(),
+        "station_y": (r * np.sin(th)).tolist(),
+        "station_type": "Aperture array",
+        "station_per_folder": 1 if per_station else 0,
+        "element_x": [a for a, _ in lays] if per_station else lays[0][0],
+        "element_y": [b for _, b in lays] if per_station else lays[0][1],
+        "channel_bandwidth_hz": 0.0, "time_average_sec": 0.0,
+        "uv_filter": [0.0, -1.0, "Wavelengths"],
+        "ra_rad": ra.tolist(), "dec_rad": dec.tolist(),
+        "I": I.tolist(), "Q": Q.tolist(), "U": U.tolist(), "V": list(z),
+        "ref_freq_hz": list(z), "spectral_index": list(z),
+        "rotation_measure": list(z), "major_rad": list(z),
+        "minor_rad": list(z), "pa_rad": list(z),
+        "phase_centre_ra_rad": ra0, "phase_centre_dec_rad": dec0,
+        "freq_start_hz": 100e6, "freq_inc_hz": 15e6, "num_channels": 3,
+        "mjd_start": workloads.MJD0, "inc_sec": 300.0, "num_times": 4,
+        "num_devices": 1, "max_times_per_block": 4,
+        "max_sources_per_chunk": 16384, "horizon_clip": 0,
+        "correlation_type": "Both", "casa": 0,
+        "source_min_jy": -1e300, "source_max_jy": 1e300,
+    }
+    case.update(over)
+    return case

@@ -28,7 +28,8 @@ case.json keys (all required):
   max_times_per_block, max_sources_per_chunk, horizon_clip,
   correlation_type ("Cross-correlations" | "Auto-correlations" | "Both"),
   casa, source_min_jy, source_max_jy. Optional: station_per_folder (one
-  station model per station, station-beam duplication off).
+  station model per station, station-beam duplication off), element_x and
+  element_y (aperture-array element layouts).
 """
 import ctypes
 import json
@@ -116,13 +117,22 @@ def write_telescope(d, case):
             f.write("%.17g,%.17g\n" % (x, y))
     # one station folder shared by all stations, or one per station (each
     # station then has its own model: its own latitude and longitude for
-    # Jones R, and its own beam)
+    # Jones R, and its own beam); element layouts (ENU metres) from
+    # element_x / element_y: one list for every folder, or one list per
+    # folder; a single element at the centre without them
     num = len(case["station_x"]) if case.get("station_per_folder") else 1
+    ex, ey = case.get("element_x"), case.get("element_y")
     for i in range(num):
         s = os.path.join(d, "station%04d" % i)
         os.makedirs(s)
         with open(os.path.join(s, "layout.txt"), "w") as f:
-            f.write("0,0\n")
+            if ex is None:
+                f.write("0,0\n")
+                continue
+            xs = ex[i] if isinstance(ex[0], list) else ex
+            ys = ey[i] if isinstance(ey[0], list) else ey
+            for x, y in zip(xs, ys):
+                f.write("%.17g,%.17g\n" % (x, y))
 
 
 def mem_array(lib, mem, complex_matrix):
