@@ -272,6 +272,19 @@ __device__ __forceinline__ bool mbar_wait_cluster(uint64_t* bar,
     }
 }
 
+// Tensor-map (TMA) load of a 2-D box into this CTA's shared memory whose
+// completion is reported to an mbarrier of either CTA of the pair (its
+// shared::cluster address): the copy form of cta_group::2. No multicast.
+// The box's innermost coordinate x must be a multiple of 16 bytes.
+__device__ __forceinline__ void tma_load_2d_pair(void* dst_smem,
+        const void* tmap, int x, int y, uint32_t mbar_cluster)
+{
+    asm volatile("cp.async.bulk.tensor.2d.cta_group::2.shared::cluster.global"
+                 ".mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];"
+                 :: "r"(smem_u32(dst_smem)), "l"(tmap), "r"(x), "r"(y),
+                    "r"(mbar_cluster) : "memory");
+}
+
 // TMEM of both CTAs of a pair: one warp of each CTA (the same warp index),
 // the same shared-memory destination offset in both.
 __device__ __forceinline__ void tmem_alloc_pair(uint32_t* dst_smem,

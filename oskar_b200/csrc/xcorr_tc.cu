@@ -27,6 +27,7 @@
 // reads them from shared memory (K-major, 128-byte swizzle), hi tile then lo
 // tile, ordered [row block][k block][hi, lo]. A pipeline stage is therefore
 // one 32 KB bulk copy per operand.
+#include <cuda.h>
 #include <cuda_fp16.h>
 
 #include <atomic>
@@ -1116,9 +1117,10 @@ gemm_wide_kernel(const GemmParams prm)
 // moves a third fewer operand bytes per product from L2, and three 64 KB
 // stages fit where two 96 KB stages did.
 // Synchronisation between the two CTAs:
-//  - each CTA's producer fills its own stage (local full barrier); in the
-//    odd CTA a relay thread waits for that and arrives on the even CTA's
-//    pfull barrier, so the MMA issuer waits for both halves;
+//  - each CTA's producer fills its own half of a stage with tensor-map
+//    copies (cta_group::2 form, no multicast) whose completion is counted
+//    on the even CTA's full barrier, which the even CTA's producer arms with
+//    both halves' bytes; so the MMA issuer's one wait covers both halves;
 //  - the MMA issuer's commits arrive on the empty, mfull and cfull barriers
 //    at the same offset in both CTAs (multicast commit);
 //  - the epilogue warps of both CTAs arrive on the even CTA's mempty and
@@ -1131,8 +1133,8 @@ constexpr int kPStageBytes = 2 * kPairBytes;  // A pair + B pair (own half)
 
 struct PairCtl
 {
-    uint64_t full[kPStages], pfull[kPStages], empty[kPStages], mfull,
-            mempty, cfull, cempty, done;
+    uint64_t full[kPStages], empty[kPStages], mfull, mempty, cfull, cempty,
+            done;
     uint32_t tmem_base;
     int abort;
 };
@@ -1148,8 +1150,11 @@ __host__ __device__ inline int pair_tiles(int nrb)
     return np * (np + 1) / 2;
 }
 
+// The operand image as a 2-D tensor for the copies: rows of 128 bytes (16
+// 8-byte elements), row r at byte 128 r of the workspace's image area; a
+// box is 256 rows, one hi + lo tile pair.
 __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kWThreads, 1)
-gemm_pair_kernel(const GemmParams prm)
+gemm_pair_kernel(const GemmParams prm, const __grid_constant__ CUtensorMap tmap)
 {
     extern __shared__ uint8_t smem_raw[];
     uint8_t* smem = reinterpret_cast<uint8_t*>(
@@ -1164,7 +1169,6 @@ gemm_pair_kernel(const GemmParams prm)
         for (int s = 0; s < kPStages; ++s)
         {
             ptx::mbar_init(&ctl->full[s], 1);
-            ptx::mbar_init(&ctl->pfull[s], 1);
             ptx::mbar_init(&ctl->empty[s], 1);
         }
         ptx::mbar_init(&ctl->mfull, 1);
@@ -1199,7 +1203,10 @@ gemm_pair_kernel(const GemmParams prm)
         if (lane == 0)
         {
             // ---------------- producer: this CTA's row block (A pair) and
-            // column block (B pair) of every k block
+            // column block (B pair) of every k block, counted on the even
+            // CTA's full barrier
+            const uint32_t full0 = ptx::mapa_shared(
+                    ptx::smem_u32(&ctl->full[0]), 0);
             int stage = 0;
             uint32_t phase = 0;
             uint32_t issued = 0, issued_par = 0;
@@ -1213,30 +1220,38 @@ gemm_pair_kernel(const GemmParams prm)
                 int rb = 2 * ti + (int) rank, cb = 2 * tj + (int) rank;
                 if (rb >= prm.nrb) rb = prm.nrb - 1;
                 if (cb >= prm.nrb) cb = prm.nrb - 1;
-                const uint8_t* img = prm.W + (size_t) prob * prm.image_stride;
+                const long long row0 = (long long) prob * (long long)
+                        (prm.image_stride / 128);
                 for (int kb = 0; kb < prm.nkb; ++kb)
                 {
                     if (!ptx::mbar_wait(&ctl->empty[stage], phase ^ 1,
                             prm.err, 31, abort))
                         break;
                     uint8_t* dst = smem + (size_t) stage * kPStageBytes;
-                    ptx::mbar_arrive_expect_tx(&ctl->full[stage],
-                            kPStageBytes);
-                    ptx::bulk_g2s(dst, img + ((size_t) rb * prm.nkb + kb) *
-                            kPairBytes, kPairBytes, &ctl->full[stage]);
-                    ptx::bulk_g2s(dst + kPairBytes, img +
-                            ((size_t) cb * prm.nkb + kb) * kPairBytes,
-                            kPairBytes, &ctl->full[stage]);
+                    if (rank == 0)
+                        ptx::mbar_arrive_expect_tx(&ctl->full[stage],
+                                2 * kPStageBytes);
+                    const uint32_t bar = full0 +
+                            (uint32_t) (stage * sizeof(uint64_t));
+                    ptx::tma_load_2d_pair(dst, &tmap, 0, (int) (row0 +
+                            ((long long) rb * prm.nkb + kb) * 256), bar);
+                    ptx::tma_load_2d_pair(dst + kPairBytes, &tmap, 0,
+                            (int) (row0 + ((long long) cb * prm.nkb + kb) *
+                            256), bar);
                     issued |= 1u << stage;
                     issued_par = (issued_par & ~(1u << stage)) |
                             (phase << stage);
                     if (++stage == kPStages) { stage = 0; phase ^= 1; }
                 }
             }
-            for (int s = 0; s < kPStages; ++s)
-                if ((issued >> s) & 1)
-                    ptx::mbar_wait(&ctl->full[s], (issued_par >> s) & 1,
-                            prm.err, 32, abort);
+            // the even CTA's full barrier counts both CTAs' copies: its
+            // producer waits for every stage's last phase before the CTAs
+            // can leave
+            if (rank == 0)
+                for (int s = 0; s < kPStages; ++s)
+                    if ((issued >> s) & 1)
+                        ptx::mbar_wait(&ctl->full[s], (issued_par >> s) & 1,
+                                prm.err, 32, abort);
         }
         __syncwarp();
     }
@@ -1269,10 +1284,8 @@ gemm_pair_kernel(const GemmParams prm)
                     const int kb1 = min(prm.nkb, kb0 + prm.drain_kb);
                     for (int kb = kb0; kb < kb1; ++kb)
                     {
-                        if (!ptx::mbar_wait(&ctl->full[stage], phase, prm.err,
-                                34, abort) ||
-                                !ptx::mbar_wait_cluster(&ctl->pfull[stage],
-                                phase, prm.err, 35, abort))
+                        if (!ptx::mbar_wait_cluster(&ctl->full[stage], phase,
+                                prm.err, 34, abort))
                         {
                             ok = false;
                             break;
@@ -1329,36 +1342,6 @@ gemm_pair_kernel(const GemmParams prm)
             // every tcgen05 instruction of this kernel is cta_group::2
             ptx::mma_commit_pair(&ctl->done);
             ptx::mbar_wait(&ctl->done, 0, prm.err, 37, abort);
-        }
-        __syncwarp();
-    }
-    else if (warp == 2)
-    {
-        if (lane == 0 && rank == 1)
-        {
-            // ---------------- relay (odd CTA): each of its stages, once
-            // filled, is reported to the even CTA's MMA issuer
-            const uint32_t pfull0 = ptx::mapa_shared(
-                    ptx::smem_u32(&ctl->pfull[0]), 0);
-            int stage = 0;
-            uint32_t phase = 0;
-            for (int task = pair; task < ntasks && !*abort; task += npairs)
-            {
-                bool ok = true;
-                for (int kb = 0; kb < prm.nkb; ++kb)
-                {
-                    if (!ptx::mbar_wait(&ctl->full[stage], phase, prm.err,
-                            38, abort))
-                    {
-                        ok = false;
-                        break;
-                    }
-                    ptx::mbar_arrive_cluster(pfull0 +
-                            (uint32_t) (stage * sizeof(uint64_t)));
-                    if (++stage == kPStages) { stage = 0; phase ^= 1; }
-                }
-                if (!ok) break;
-            }
         }
         __syncwarp();
     }
@@ -1631,9 +1614,31 @@ int launch_gemm(GemmParams& gp, cudaStream_t stream)
             ++g_ev_used;
         }
     }
+    CUtensorMap tmap;
+    if (pair)
+    {
+        // the operand image area as rows of 128 bytes (see gemm_pair_kernel)
+        const size_t bytes = gp.image_stride ?
+                gp.image_stride * (size_t) gp.num_problems :
+                (size_t) gp.nrb * gp.nkb * kPairBytes;
+        const cuuint64_t gdim[2] = {16, bytes / 128};
+        const cuuint64_t gstride[1] = {128};
+        const cuuint32_t box[2] = {16, 256};
+        const cuuint32_t estride[2] = {1, 1};
+        if (bytes / 128 >= (1ull << 31) ||
+                cuTensorMapEncodeTiled(&tmap, CU_TENSOR_MAP_DATA_TYPE_UINT64,
+                2, (void*) gp.W, gdim, gstride, box, estride,
+                CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
+        {
+            set_last_error_msg("tc: operand tensor map");
+            return OSKB_ERR_KERNEL_LAUNCH_FAILURE;
+        }
+    }
     if (pair)
         gemm_pair_kernel<<<grid, kWThreads, gemm_pair_smem_bytes(),
-                stream>>>(gp);
+                stream>>>(gp, tmap);
     else if (wide)
         gemm_wide_kernel<<<grid, kWThreads, gemm_wide_smem_bytes(),
                 stream>>>(gp);
