@@ -70,11 +70,15 @@ class BlockCase:
         self.flux_c = {k: np.ascontiguousarray(np.stack([p[j] for p in per]))
                        for j, k in enumerate("IQUV")}
 
-    def oracle_vis(self):
+    def oracle_vis(self, channels=None):
+        """The block's visibilities [dump][channel][baseline][2x2] from the
+        oracle; with `channels`, only those channels are computed (the
+        others stay 0)."""
         real, s = self.real, suffix(self.real)
         T, C, N, nbl = self.num_times, self.num_channels, self.num_st, \
             self.nbl
         vis = np.zeros(T * C * nbl * 8, real)
+        chans = range(C) if channels is None else channels
         orc = oracle()
         s0 = 0
         for size, g in zip(self.chunks, self.gaussian):
@@ -87,7 +91,7 @@ class BlockCase:
                 if self.E is not None:
                     Et = self.E[t if self.beam_per_dump else 0][:, sl]
                     Et = np.ascontiguousarray(Et)
-                for c in range(C):
+                for c in chans:
                     f = self.freqs[c]
                     if self.flux_c is not None:
                         for k in "IQUV":

@@ -277,3 +277,27 @@ def test_block_plan_spectral_sky(real):
         assert lib.oskb_block_plan_graph_launches(plan) == 2
     finally:
         lib.oskb_block_plan_free(plan)
+
+
+def test_block_c4_shape_sampled():
+    """The batched-smearing configuration's shape with its sky scaled down
+    200 times: 256 stations, 32 chunks whose sizes are drawn log-uniform on
+    [500, 50,000] and divided by 200 (Gaussian chunks as the reference
+    flags them), 64 channels of 100 kHz, 2 dumps, bandwidth and time
+    smearing, FP64, one launch for the whole block; the oracle computes
+    channels 0, 21, 42 and 63 of both dumps, which must agree to 1e-12 of
+    the block's largest visibility in those channels."""
+    rng = np.random.default_rng(4)
+    sizes = np.maximum(3, (np.exp(rng.uniform(np.log(500), np.log(50_000),
+                                              32)) / 200).astype(int))
+    gauss = (rng.uniform(0, 1, 32) < 0.9).astype(int)
+    c = BlockCase(num_st=256, chunks=tuple(int(x) for x in sizes),
+                  gaussian=tuple(int(g) for g in gauss), num_times=2,
+                  num_channels=64, seed=44)
+    c.freqs = 100e6 + 1e5 * np.arange(64)
+    c.inv_wl = c.freqs / 299792458.0
+    got = run_block(c).reshape(2, 64, -1)
+    chans = (0, 21, 42, 63)
+    ref = c.oracle_vis(channels=chans).reshape(2, 64, -1)
+    for ch in chans:
+        assert rel(got[:, ch], ref[:, ch]) <= 1e-12, ch
