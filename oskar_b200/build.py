@@ -89,7 +89,7 @@ def build(force=False, verbose_ptxas=False):
     dropin = [objs[s] for s in srcs
               if os.path.basename(s) != "oskar_api.cu"]
     for out, o in ((LIB, main), (DROPIN_LIB, dropin)):
-        cmd = [NVCC, *ARCH, "-shared", "-o", out, *o, "-lcuda"]
+        cmd = [NVCC, *ARCH, "-shared", "-o", out, *o]
         r = subprocess.run(cmd, capture_output=True, text=True)
         if r.returncode != 0:
             raise RuntimeError("link failed:\n%s%s" % (r.stdout, r.stderr))

@@ -1572,6 +1572,31 @@ int device_setup(bool& wide_fits, bool& pair_fits)
     return 0;
 }
 
+// cuTensorMapEncodeTiled through the runtime's driver entry point, so that
+// the library links only the CUDA runtime and still loads on a host without
+// a driver (the host-only entry points stay callable there).
+typedef CUresult (*EncodeTiledFn)(CUtensorMap*, CUtensorMapDataType,
+        cuuint32_t, void*, const cuuint64_t*, const cuuint64_t*,
+        const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
+        CUtensorMapSwizzle, CUtensorMapL2promotion,
+        CUtensorMapFloatOOBfill);
+
+EncodeTiledFn encode_tiled_fn()
+{
+    static std::atomic<EncodeTiledFn> fn{nullptr};
+    EncodeTiledFn f = fn.load();
+    if (f) return f;
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q = cudaDriverEntryPointSymbolNotFound;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p,
+            cudaEnableDefault, &q) != cudaSuccess ||
+            q != cudaDriverEntryPointSuccess)
+        return nullptr;
+    f = reinterpret_cast<EncodeTiledFn>(p);
+    fn.store(f);
+    return f;
+}
+
 int launch_gemm(GemmParams& gp, cudaStream_t stream)
 {
     bool wide_fits = false, pair_fits = false;
@@ -1625,8 +1650,9 @@ int launch_gemm(GemmParams& gp, cudaStream_t stream)
         const cuuint64_t gstride[1] = {128};
         const cuuint32_t box[2] = {16, 256};
         const cuuint32_t estride[2] = {1, 1};
-        if (bytes / 128 >= (1ull << 31) ||
-                cuTensorMapEncodeTiled(&tmap, CU_TENSOR_MAP_DATA_TYPE_UINT64,
+        EncodeTiledFn encode = encode_tiled_fn();
+        if (!encode || bytes / 128 >= (1ull << 31) ||
+                encode(&tmap, CU_TENSOR_MAP_DATA_TYPE_UINT64,
                 2, (void*) gp.W, gdim, gstride, box, estride,
                 CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
                 CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
