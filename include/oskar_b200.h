@@ -527,6 +527,63 @@ OSKB_API int oskb_station_beam_two_level_f(int num_tile_types,
         const float* z, void* workspace, size_t workspace_bytes,
         float* beam, void* stream);
 
+/* Hierarchical aperture-array station of any depth (num_levels 2..16).
+ * Level 0 holds num_types[0] leaf layouts (dipole arrays: num_elements
+ * dipoles each at el_x/y/z [type][element], orientations orientation_x/y_rad
+ * [type], one dipole length); each level l = 1..num_levels-1 holds
+ * num_types[l] node types, each an array of children of level l - 1; the top
+ * level holds one node type, the station (num_types[num_levels-1] == 1).
+ * Node types are numbered level by level from level 1 upward (node n); node
+ * n has the children child_start[n] .. child_start[n+1]-1 (host, CSR,
+ * child_start[0] == 0, at least one child each) at ENU positions
+ * child_x/y/z [child] (device, true positions in metres, relative to the
+ * node's own centre) with child_type [child] (device, the index of the
+ * child's node type in the level below, which must be less than that
+ * level's num_types; NULL: every child is type 0, the reference's identical
+ * children). normalise_array [level] (host): divide that level's array sum
+ * by its number of children (level 0: the leaf array, by num_elements).
+ * beam_enu [level][3] (host): the ENU pointing of that level's weights, the
+ * reference's oskar_station_beam_horizon_direction of a station at that
+ * depth. Beam [direction][2x2] of the station: at every level above 0,
+ * sum_c w_c exp(i k r_c . d) x beam(type(c))[d] with w_c = exp(-i k r_c . b)
+ * (oskar_dftw with the weights of oskar_station_evaluate_element_weights.c:
+ * 15-66); level 0 is the fused single-level beam (oskb_station_beam_aa:
+ * dipole pattern, leaf array factor, normalise_element, blanked below the
+ * horizon). Replaces the recursion of
+ * oskar_evaluate_station_beam_aperture_array.c:242-287 (each distinct node
+ * type is evaluated once; identical or repeated children are indexed, not
+ * copied); the normalisation to the beam direction
+ * (oskar_station_beam.c:108-135) is the caller's, as in the reference.
+ * workspace: device, at least oskb_station_beam_hierarchical_workspace_bytes
+ * bytes (0 there: the description is invalid). Directions x, y, z: device
+ * [direction], ENU direction cosines. oskb_station_beam_two_level_{d,f} is
+ * the case num_levels = 2. */
+OSKB_API size_t oskb_station_beam_hierarchical_workspace_bytes(
+        int precision_bytes, int num_levels, const int* num_types,
+        const int* child_start, int num_directions);
+OSKB_API int oskb_station_beam_hierarchical_d(int num_levels,
+        const int* num_types, int num_elements, const double* el_x,
+        const double* el_y, const double* el_z,
+        const double* orientation_x_rad, const double* orientation_y_rad,
+        double dipole_length_m, int normalise_element,
+        const int* normalise_array, const int* child_start,
+        const double* child_x, const double* child_y, const double* child_z,
+        const int* child_type, int swap_xy, int is_3d, double frequency_hz,
+        const double* beam_enu, int num_directions, const double* x,
+        const double* y, const double* z, void* workspace,
+        size_t workspace_bytes, double* beam, void* stream);
+OSKB_API int oskb_station_beam_hierarchical_f(int num_levels,
+        const int* num_types, int num_elements, const float* el_x,
+        const float* el_y, const float* el_z,
+        const double* orientation_x_rad, const double* orientation_y_rad,
+        double dipole_length_m, int normalise_element,
+        const int* normalise_array, const int* child_start,
+        const float* child_x, const float* child_y, const float* child_z,
+        const int* child_type, int swap_xy, int is_3d, double frequency_hz,
+        const double* beam_enu, int num_directions, const float* x,
+        const float* y, const float* z, void* workspace,
+        size_t workspace_bytes, float* beam, void* stream);
+
 /* ------------------------------------------------------------------------
  * Sky and baseline preparation on the device.
  * ------------------------------------------------------------------------

@@ -21,6 +21,8 @@
 // CTA cooperatively before the main loop, so there is no second launch.
 // In FP64 the element loops take their phase factors from a shared-memory
 // table (trig_table.cuh) instead of a library sincos per element-direction.
+#include <climits>
+
 #include "beam_common.cuh"
 #include "trig_table.cuh"
 
@@ -896,25 +898,29 @@ OSKB_BEAM_ENTRY(float, f)
 }  // extern "C"
 
 // ---------------------------------------------------------------------------
-// Two-level (hierarchical) aperture-array stations: a station of tiles, each
-// tile a dipole array of one of num_tile_types layouts. The reference
-// recurses (oskar_evaluate_station_beam_aperture_array.c:242-287): it
-// evaluates every child station's beam, copying the first child's beam to
-// all children when they are identical, then forms the parent's weighted
-// DFT over its children with the child beams as the data. Here: one fused
-// station-beam launch evaluates all tile types at once (each type once,
-// however many tiles share it), one launch forms the parent's DFT weights,
-// and one weighted DFT sums the tiles with data index = the tile's type, so
-// identical tiles need no copies.
+// Hierarchical aperture-array stations of any depth: level 0 holds the leaf
+// layouts (dipole arrays), each node type of level l > 0 is an array of
+// children of level l - 1, and the top level is the station itself. The
+// reference recurses (oskar_evaluate_station_beam_aperture_array.c:242-287):
+// it evaluates every child station's beam, copying the first child's beam to
+// all children when they are identical, then forms the parent's weighted DFT
+// over its children with the child beams as the data. Here the recursion runs
+// bottom-up over node TYPES instead of over the tree: one fused station-beam
+// launch evaluates every leaf layout once, however many tiles share it, and
+// each node type of each higher level is one launch of DFT weights and one
+// weighted DFT whose data index is the child's type, so identical children
+// (and any repeated sub-tree) cost no copies and no re-evaluation. Levels
+// alternate between two beam buffers of the workspace; the top level writes
+// the caller's beam.
 // ---------------------------------------------------------------------------
 namespace oskb {
 namespace {
 
-__global__ void two_level_setup_kernel(int num_types, double bx, double by,
-        double bz, double* pointing, int num_tiles, int* zero_idx)
+__global__ void hierarchy_setup_kernel(int num_types, double bx, double by,
+        double bz, double* pointing, int num_zero, int* zero_idx)
 {
     for (int i = blockIdx.x * blockDim.x + threadIdx.x;
-            i < num_types || i < num_tiles; i += gridDim.x * blockDim.x)
+            i < num_types || i < num_zero; i += gridDim.x * blockDim.x)
     {
         if (i < num_types)
         {
@@ -922,89 +928,150 @@ __global__ void two_level_setup_kernel(int num_types, double bx, double by,
             pointing[3 * i + 1] = by;
             pointing[3 * i + 2] = bz;
         }
-        if (zero_idx && i < num_tiles) zero_idx[i] = 0;
+        if (zero_idx && i < num_zero) zero_idx[i] = 0;
     }
 }
 
 size_t align256(size_t b) { return (b + 255) & ~(size_t) 255; }
 
-size_t two_level_workspace(size_t elem, int num_tile_types, int num_tiles,
-        int num_directions)
+constexpr int kMaxLevels = 16;
+
+// Checks the tree description; on success gives the most node types of the
+// even and of the odd levels below the top (the two beam buffers) and the
+// most children of any node (weights and the zero data index).
+int hierarchy_shape(int num_levels, const int* num_types,
+        const int* child_start, int& max_types_even, int& max_types_odd,
+        int& max_children)
 {
-    return align256(elem * 8 * (size_t) num_tile_types * num_directions) +
-            align256(elem * 2 * (size_t) num_tiles) +
-            align256(sizeof(double) * 3 * (size_t) num_tile_types) +
-            align256(sizeof(int) * (size_t) num_tiles);
+    if (num_levels < 2 || num_levels > kMaxLevels || !num_types ||
+            !child_start)
+        return OSKB_ERR_INVALID_ARGUMENT;
+    for (int l = 0; l < num_levels; ++l)
+        if (num_types[l] < 1 || num_types[l] > 65535)
+            return OSKB_ERR_INVALID_ARGUMENT;
+    if (num_types[num_levels - 1] != 1) return OSKB_ERR_INVALID_ARGUMENT;
+    max_types_even = max_types_odd = max_children = 0;
+    for (int l = 0; l < num_levels - 1; ++l)
+    {
+        int& m = (l % 2) ? max_types_odd : max_types_even;
+        if (num_types[l] > m) m = num_types[l];
+    }
+    if (child_start[0] != 0) return OSKB_ERR_INVALID_ARGUMENT;
+    int nodes = 0;
+    for (int l = 1; l < num_levels; ++l) nodes += num_types[l];
+    for (int n = 0; n < nodes; ++n)
+    {
+        const long long c = (long long) child_start[n + 1] - child_start[n];
+        if (c < 1 || c > INT_MAX / 2) return OSKB_ERR_INVALID_ARGUMENT;
+        if (c > max_children) max_children = (int) c;
+    }
+    return 0;
+}
+
+size_t hierarchy_workspace(size_t elem, int num_directions,
+        int max_types_even, int max_types_odd, int max_children,
+        int num_leaf_types)
+{
+    return align256(elem * 8 * (size_t) max_types_even * num_directions) +
+            align256(elem * 8 * (size_t) max_types_odd * num_directions) +
+            align256(elem * 2 * (size_t) max_children) +
+            align256(sizeof(double) * 3 * (size_t) num_leaf_types) +
+            align256(sizeof(int) * (size_t) max_children);
 }
 
 template <typename T>
-int station_beam_two_level(int num_tile_types, int num_elements,
-        const T* el_x, const T* el_y, const T* el_z,
+int station_beam_hierarchical(int num_levels, const int* num_types,
+        int num_elements, const T* el_x, const T* el_y, const T* el_z,
         const double* orientation_x, const double* orientation_y,
         double dipole_length_m, int normalise_element,
-        int normalise_tile_array, int num_tiles, const T* tile_x,
-        const T* tile_y, const T* tile_z, const int* tile_type,
-        int normalise_station_array, int swap_xy, int is_3d,
-        double frequency_hz, double bx, double by, double bz,
-        int num_directions, const T* x, const T* y, const T* z,
-        void* workspace, size_t workspace_bytes, T* beam, void* stream)
+        const int* normalise_array, const int* child_start,
+        const T* child_x, const T* child_y, const T* child_z,
+        const int* child_type, int swap_xy, int is_3d, double frequency_hz,
+        const double* beam_enu, int num_directions, const T* x, const T* y,
+        const T* z, void* workspace, size_t workspace_bytes, T* beam,
+        void* stream)
 {
-    if (num_tile_types < 1 || num_tiles < 0 || num_directions < 0 ||
-            num_tile_types > 65535)
+    int max_even = 0, max_odd = 0, max_children = 0;
+    if (int err = hierarchy_shape(num_levels, num_types, child_start,
+            max_even, max_odd, max_children))
+        return err;
+    if (num_directions < 0 || !normalise_array || !beam_enu)
         return OSKB_ERR_INVALID_ARGUMENT;
-    if (num_tiles == 0 || num_directions == 0) return 0;
-    if (!tile_x || !tile_y || (is_3d && !tile_z) || !workspace || !beam)
+    if (num_directions == 0) return 0;
+    if (!child_x || !child_y || (is_3d && !child_z) || !workspace || !beam)
         return OSKB_ERR_INVALID_ARGUMENT;
-    if (workspace_bytes < two_level_workspace(sizeof(T), num_tile_types,
-            num_tiles, num_directions))
+    if (workspace_bytes < hierarchy_workspace(sizeof(T), num_directions,
+            max_even, max_odd, max_children, num_types[0]))
         return OSKB_ERR_MEMORY_ALLOC_FAILURE;
     uint8_t* w = static_cast<uint8_t*>(workspace);
-    T* tile_beams = reinterpret_cast<T*>(w);
-    w += align256(sizeof(T) * 8 * (size_t) num_tile_types * num_directions);
+    T* level_beams[2];
+    level_beams[0] = reinterpret_cast<T*>(w);
+    w += align256(sizeof(T) * 8 * (size_t) max_even * num_directions);
+    level_beams[1] = reinterpret_cast<T*>(w);
+    w += align256(sizeof(T) * 8 * (size_t) max_odd * num_directions);
     T* weights = reinterpret_cast<T*>(w);
-    w += align256(sizeof(T) * 2 * (size_t) num_tiles);
+    w += align256(sizeof(T) * 2 * (size_t) max_children);
     double* pointing = reinterpret_cast<double*>(w);
-    w += align256(sizeof(double) * 3 * (size_t) num_tile_types);
-    int* zero_idx = tile_type ? nullptr : reinterpret_cast<int*>(w);
+    w += align256(sizeof(double) * 3 * (size_t) num_types[0]);
+    int* zero_idx = child_type ? nullptr : reinterpret_cast<int*>(w);
     cudaStream_t s = as_stream(stream);
-    const int n = num_tile_types > num_tiles ? num_tile_types : num_tiles;
-    two_level_setup_kernel<<<(n + 255) / 256, 256, 0, s>>>(num_tile_types,
-            bx, by, bz, pointing, num_tiles, zero_idx);
-    if (int err = check_launch("station_beam_two_level")) return err;
-    // tile beams [type][direction]: element pattern x tile array factor,
+    const int n = num_types[0] > max_children ? num_types[0] : max_children;
+    hierarchy_setup_kernel<<<(n + 255) / 256, 256, 0, s>>>(num_types[0],
+            beam_enu[0], beam_enu[1], beam_enu[2], pointing, max_children,
+            zero_idx);
+    if (int err = check_launch("station_beam_hierarchical")) return err;
+    // leaf beams [type][direction]: element pattern x leaf array factor,
     // blanked below the horizon, no final normalisation
-    if (int err = station_beam_aa<T>(num_tile_types, num_elements, el_x,
-            el_y, el_z, nullptr, nullptr, nullptr, nullptr, nullptr, 1,
-            nullptr, orientation_x, orientation_y, &dipole_length_m,
-            nullptr, nullptr, nullptr, normalise_element,
-            normalise_tile_array, 0, swap_xy, is_3d, frequency_hz, pointing,
-            nullptr, num_directions, x, y, z, 0, tile_beams, stream))
+    if (int err = station_beam_aa<T>(num_types[0], num_elements, el_x, el_y,
+            el_z, nullptr, nullptr, nullptr, nullptr, nullptr, 1, nullptr,
+            orientation_x, orientation_y, &dipole_length_m, nullptr, nullptr,
+            nullptr, normalise_element, normalise_array[0], 0, swap_xy,
+            is_3d, frequency_hz, pointing, nullptr, num_directions, x, y, z,
+            0, level_beams[0], stream))
         return err;
     const double k = 2.0 * kPi * frequency_hz / 299792458.0;
-    const T* zt = is_3d ? tile_z : nullptr;
     const T* zo = is_3d ? z : nullptr;
-    const int* idx = tile_type ? tile_type : zero_idx;
-    const T norm = normalise_station_array ? (T) (1.0 / num_tiles) : (T) 1;
-    if constexpr (sizeof(T) == 8)
+    const size_t beam_stride = (size_t) 8 * num_directions;
+    int node = 0;
+    for (int l = 1; l < num_levels; ++l)
     {
-        if (int err = oskb_evaluate_element_weights_dft_d(num_tiles, tile_x,
-                tile_y, zt, nullptr, k, bx, by, is_3d ? bz : 0.0, weights,
-                stream))
-            return err;
-        return oskb_dftw_d(1, num_tiles, k, weights, tile_x, tile_y, zt, 0,
-                num_directions, x, y, zo, idx, tile_beams, 1, 1, 0, beam,
-                norm, stream);
+        const T* data = level_beams[(l - 1) % 2];
+        const double* b = beam_enu + 3 * l;
+        for (int j = 0; j < num_types[l]; ++j, ++node)
+        {
+            const int c0 = child_start[node];
+            const int nc = child_start[node + 1] - c0;
+            const T* cz = is_3d ? child_z + c0 : nullptr;
+            const int* idx = child_type ? child_type + c0 : zero_idx;
+            T* out = (l == num_levels - 1) ? beam :
+                    level_beams[l % 2] + beam_stride * j;
+            const T norm = normalise_array[l] ? (T) (1.0 / nc) : (T) 1;
+            if constexpr (sizeof(T) == 8)
+            {
+                if (int err = oskb_evaluate_element_weights_dft_d(nc,
+                        child_x + c0, child_y + c0, cz, nullptr, k, b[0],
+                        b[1], is_3d ? b[2] : 0.0, weights, stream))
+                    return err;
+                if (int err = oskb_dftw_d(1, nc, k, weights, child_x + c0,
+                        child_y + c0, cz, 0, num_directions, x, y, zo, idx,
+                        data, 1, 1, 0, out, norm, stream))
+                    return err;
+            }
+            else
+            {
+                if (int err = oskb_evaluate_element_weights_dft_f(nc,
+                        child_x + c0, child_y + c0, cz, nullptr, (float) k,
+                        (float) b[0], (float) b[1],
+                        (float) (is_3d ? b[2] : 0.0), weights, stream))
+                    return err;
+                if (int err = oskb_dftw_f(1, nc, (float) k, weights,
+                        child_x + c0, child_y + c0, cz, 0, num_directions, x,
+                        y, zo, idx, data, 1, 1, 0, out, norm, stream))
+                    return err;
+            }
+        }
     }
-    else
-    {
-        if (int err = oskb_evaluate_element_weights_dft_f(num_tiles, tile_x,
-                tile_y, zt, nullptr, (float) k, (float) bx, (float) by,
-                (float) (is_3d ? bz : 0.0), weights, stream))
-            return err;
-        return oskb_dftw_f(1, num_tiles, (float) k, weights, tile_x, tile_y,
-                zt, 0, num_directions, x, y, zo, idx, tile_beams, 1, 1, 0,
-                beam, norm, stream);
-    }
+    return 0;
 }
 
 }  // namespace
@@ -1012,16 +1079,57 @@ int station_beam_two_level(int num_tile_types, int num_elements,
 
 extern "C" {
 
+size_t oskb_station_beam_hierarchical_workspace_bytes(int precision_bytes,
+        int num_levels, const int* num_types, const int* child_start,
+        int num_directions)
+{
+    int max_even = 0, max_odd = 0, max_children = 0;
+    if ((precision_bytes != 4 && precision_bytes != 8) ||
+            num_directions < 0 || oskb::hierarchy_shape(num_levels,
+                num_types, child_start, max_even, max_odd, max_children))
+        return 0;
+    return oskb::hierarchy_workspace((size_t) precision_bytes,
+            num_directions, max_even, max_odd, max_children, num_types[0]);
+}
+
 size_t oskb_station_beam_two_level_workspace_bytes(int precision_bytes,
         int num_tile_types, int num_tiles, int num_directions)
 {
-    if (num_tile_types < 1 || num_tiles < 0 || num_directions < 0 ||
-            (precision_bytes != 4 && precision_bytes != 8))
-        return 0;
-    return oskb::two_level_workspace((size_t) precision_bytes,
-            num_tile_types, num_tiles, num_directions);
+    if (num_tiles < 1)
+        return num_tile_types >= 1 && num_tiles == 0 &&
+                num_directions >= 0 ? 256 : 0;
+    const int types[2] = {num_tile_types, 1};
+    const int start[2] = {0, num_tiles};
+    return oskb_station_beam_hierarchical_workspace_bytes(precision_bytes,
+            2, types, start, num_directions);
 }
 
+#define OSKB_HIERARCHICAL_ENTRY(T, S)                                        \
+int oskb_station_beam_hierarchical_##S(int num_levels,                       \
+        const int* num_types, int num_elements, const T* el_x,               \
+        const T* el_y, const T* el_z, const double* orientation_x_rad,       \
+        const double* orientation_y_rad, double dipole_length_m,             \
+        int normalise_element, const int* normalise_array,                   \
+        const int* child_start, const T* child_x, const T* child_y,          \
+        const T* child_z, const int* child_type, int swap_xy, int is_3d,     \
+        double frequency_hz, const double* beam_enu, int num_directions,     \
+        const T* x, const T* y, const T* z, void* workspace,                 \
+        size_t workspace_bytes, T* beam, void* stream)                       \
+{                                                                            \
+    return oskb::station_beam_hierarchical<T>(num_levels, num_types,         \
+            num_elements, el_x, el_y, el_z, orientation_x_rad,               \
+            orientation_y_rad, dipole_length_m, normalise_element,           \
+            normalise_array, child_start, child_x, child_y, child_z,         \
+            child_type, swap_xy, is_3d, frequency_hz, beam_enu,              \
+            num_directions, x, y, z, workspace, workspace_bytes, beam,       \
+            stream);                                                         \
+}
+
+OSKB_HIERARCHICAL_ENTRY(double, d)
+OSKB_HIERARCHICAL_ENTRY(float, f)
+#undef OSKB_HIERARCHICAL_ENTRY
+
+// The two-level station is the hierarchy {tile layouts, station}.
 #define OSKB_TWO_LEVEL_ENTRY(T, S)                                           \
 int oskb_station_beam_two_level_##S(int num_tile_types, int num_elements,    \
         const T* el_x, const T* el_y, const T* el_z,                         \
@@ -1034,13 +1142,19 @@ int oskb_station_beam_two_level_##S(int num_tile_types, int num_elements,    \
         int num_directions, const T* x, const T* y, const T* z,              \
         void* workspace, size_t workspace_bytes, T* beam, void* stream)      \
 {                                                                            \
-    return oskb::station_beam_two_level<T>(num_tile_types, num_elements,     \
-            el_x, el_y, el_z, orientation_x_rad, orientation_y_rad,          \
-            dipole_length_m, normalise_element, normalise_tile_array,        \
-            num_tiles, tile_x, tile_y, tile_z, tile_type,                    \
-            normalise_station_array, swap_xy, is_3d, frequency_hz, beam_x,   \
-            beam_y, beam_z, num_directions, x, y, z, workspace,              \
-            workspace_bytes, beam, stream);                                  \
+    if (num_tile_types < 1 || num_tiles < 0 || num_directions < 0)           \
+        return OSKB_ERR_INVALID_ARGUMENT;                                    \
+    if (num_tiles == 0 || num_directions == 0) return 0;                     \
+    const int types[2] = {num_tile_types, 1};                                \
+    const int start[2] = {0, num_tiles};                                     \
+    const int norm[2] = {normalise_tile_array, normalise_station_array};     \
+    const double b[6] = {beam_x, beam_y, beam_z, beam_x, beam_y, beam_z};    \
+    return oskb::station_beam_hierarchical<T>(2, types, num_elements, el_x,  \
+            el_y, el_z, orientation_x_rad, orientation_y_rad,                \
+            dipole_length_m, normalise_element, norm, start, tile_x, tile_y, \
+            tile_z, tile_type, swap_xy, is_3d, frequency_hz, b,              \
+            num_directions, x, y, z, workspace, workspace_bytes, beam,       \
+            stream);                                                         \
 }
 
 OSKB_TWO_LEVEL_ENTRY(double, d)

@@ -164,3 +164,36 @@ def test_conversion_wrapper_checks(lib):
         5, a, a, 0.0, 0.0, 0, a, a, a, oa.status_ptr(st))
     assert st.value == -3  # status on entry is kept
     oa.free_mem(a, b)
+
+
+def test_hierarchical_station_description_checks():
+    """The tree description of oskb_station_beam_hierarchical is checked on
+    the host before any device work: workspace size 0 and
+    OSKB_ERR_INVALID_ARGUMENT (-3) for a bad tree."""
+    from oskar_b200._lib import call
+    i32 = lambda *v: np.asarray(v, np.int32)
+    ws = lambda nt, cs, nd=100, L=None: call(
+        "oskb_station_beam_hierarchical_workspace_bytes", 8,
+        len(nt) if L is None else L, i32(*nt), i32(*cs), nd, check=False)
+    # three levels: 2 leaf layouts, 2 sub-station types of 3 and 4 children,
+    # one station of 5 children
+    good = ws((2, 2, 1), (0, 3, 7, 12))
+    assert good > 0
+    # beam buffers 2 x 8 x 100 FP64 (level 0) and 2 x 8 x 100 (level 1), 5
+    # weights, 2 pointings, 5 zero indices, each rounded up to 256 bytes
+    r = lambda b: (b + 255) // 256 * 256
+    assert good == r(12800) + r(12800) + r(80) + r(48) + r(20)
+    assert ws((2, 2, 1), (0, 3, 7, 12), nd=-1) == 0
+    assert ws((2, 2, 2), (0, 3, 7, 12, 14)) == 0      # top level not 1
+    assert ws((2, 2, 1), (1, 3, 7, 12)) == 0          # CSR not from 0
+    assert ws((2, 2, 1), (0, 3, 3, 12)) == 0          # a childless node
+    assert ws((2, 0, 1), (0, 3)) == 0                 # a level of no types
+    assert ws((2,), (0, 3)) == 0                      # one level only
+    assert ws((1,) * 17, tuple(range(17))) == 0       # more than 16 levels
+    assert ws((1,) * 16, tuple(range(16))) > 0
+    el = np.zeros(4)
+    st = call("oskb_station_beam_hierarchical_d", 3, i32(2, 2, 2), 2, el,
+              el, el, el, el, 1.0, 1, i32(1, 1, 1), i32(0, 3, 7, 12, 14), el,
+              el, el, None, 0, 1, 1e8, np.zeros(9), 10, el, el, el, el,
+              1 << 20, el, None, check=False)
+    assert st == -3
