@@ -1110,6 +1110,13 @@ OSKB_API int oskb_tc_status(const void* workspace, int* flags,
  * OSKB_TC_TILE (128, 256 or 512) fixes it; unset, wide tiles are used
  * when a launch has at least two per SM, else square tiles. */
 OSKB_API int oskb_tc_tile_columns(void);
+/* Arithmetic of the last tensor-core contraction launched, 0 before the
+ * first: 8 for the default integer form (each scaled entry a 24-bit fixed-
+ * point integer held as three signed 8-bit limbs, eight 8-bit tcgen05 MMAs
+ * per K step into exact S32 accumulators, square tiles), 16 for the FP16
+ * hi/lo form (three FP16 MMAs per K step into FP32 accumulators drained to
+ * FP64), which OSKB_TC_ARITH=fp16, or any OSKB_TC_TILE setting, selects. */
+OSKB_API int oskb_tc_arithmetic(void);
 
 /* ------------------------------------------------------------------------
  * Visibility files (.vis, OSKAR binary format version 2): block

@@ -131,6 +131,20 @@ __device__ __forceinline__ void mma_f16(uint32_t d_tmem, uint64_t a_desc,
                     "r"(accumulate) : "memory");
 }
 
+// D (S32, TMEM) (+)= A B^T for signed 8-bit A and B (K = 32 per instruction,
+// both K-major in shared memory), no output lanes disabled.
+__device__ __forceinline__ void mma_i8(uint32_t d_tmem, uint64_t a_desc,
+        uint64_t b_desc, uint32_t idesc, uint32_t accumulate)
+{
+    asm volatile("{\n\t.reg .pred p;\n\t"
+                 "setp.ne.b32 p, %4, 0;\n\t"
+                 "tcgen05.mma.cta_group::1.kind::i8 [%0], %1, %2, %3, "
+                 "{%5, %6, %7, %8}, p;\n\t}"
+                 :: "r"(d_tmem), "l"(a_desc), "l"(b_desc), "r"(idesc),
+                    "r"(accumulate), "r"(0u), "r"(0u), "r"(0u), "r"(0u)
+                 : "memory");
+}
+
 // Arrives on an mbarrier once all previously issued MMAs have completed.
 __device__ __forceinline__ void mma_commit(uint64_t* bar)
 {
@@ -201,6 +215,20 @@ __device__ __forceinline__ uint64_t sdesc_sw128(uint32_t saddr)
     d |= (uint64_t) (1024u >> 4) << 32;          // stride byte offset
     d |= (uint64_t) 1 << 46;                     // descriptor version
     d |= (uint64_t) 2 << 61;                     // 128-byte swizzle
+    return d;
+}
+
+// The same for a tile stored with the 64-byte swizzle: rows of 64 bytes,
+// 8-row groups 512 bytes apart, tile base 512-byte aligned; byte c of row r
+// sits at r * 64 + ((c / 16) ^ ((r / 2) % 4)) * 16 + c % 16.
+__device__ __forceinline__ uint64_t sdesc_sw64(uint32_t saddr)
+{
+    uint64_t d = 0;
+    d |= (uint64_t) ((saddr & 0x3FFFFu) >> 4);  // start address
+    d |= (uint64_t) 1 << 16;                     // leading byte offset (unused)
+    d |= (uint64_t) (512u >> 4) << 32;           // stride byte offset
+    d |= (uint64_t) 1 << 46;                     // descriptor version
+    d |= (uint64_t) 4 << 61;                     // 64-byte swizzle
     return d;
 }
 
@@ -333,6 +361,15 @@ __host__ __device__ constexpr uint32_t idesc_f16_f32(int m, int n)
 {
     return (1u << 4) | ((uint32_t) (n >> 3) << 17) |
            ((uint32_t) (m >> 4) << 24);
+}
+
+// Instruction descriptor of kind::i8: S32 accumulator (bits 4-5 = 2),
+// signed 8-bit A and B (bits 7-9 and 10-12 = 1), both K-major, N / 8 at bit
+// 17, M / 16 at bit 24.
+__host__ __device__ constexpr uint32_t idesc_s8_s32(int m, int n)
+{
+    return (2u << 4) | (1u << 7) | (1u << 10) |
+           ((uint32_t) (n >> 3) << 17) | ((uint32_t) (m >> 4) << 24);
 }
 
 }  // namespace ptx

@@ -31,6 +31,7 @@
 #include <cuda_fp16.h>
 
 #include <atomic>
+#include <cstring>
 #include <mutex>
 #include <utility>
 #include <vector>
@@ -63,6 +64,72 @@ __device__ __forceinline__ float scale_from_bits(unsigned int bits)
     if (!(m > 0.0f) || !isfinite(m)) return 1.0f;
     const float e = floorf(log2f(kScaleTarget / m));
     return exp2f(fminf(fmaxf(e, -100.0f), 100.0f));
+}
+
+// Integer operand image (the default contraction): every entry x is the
+// fixed-point integer a = round(x q), |a| <= 127 * 2^16 (plus rounding),
+// held as three signed 8-bit limbs a = a0 2^16 + a1 2^8 + a2 with a1 and a2
+// in [-128, 127] (so a0 stays in [-127, 127]). Per 32-station x 32-source
+// block: three limb tiles of 128 rows x 64 bytes (one byte per K column),
+// stored with the 64-byte swizzle.
+constexpr int kI8Tile = 128 * 64;
+constexpr int kI8Block = 3 * kI8Tile;
+constexpr float kI8Target = 8323072.0f;      // 127 * 2^16
+
+__host__ __device__ inline size_t image_bytes_i8(int num_st, int num_src)
+{
+    const size_t nrb = (num_st + kStPerBlock - 1) / kStPerBlock;
+    const size_t nkb = (num_src + kSrcPerBlock - 1) / kSrcPerBlock;
+    return nrb * nkb * kI8Block;
+}
+
+// Fixed-point scale q (not a power of two) for the largest |entry| m.
+__device__ __forceinline__ float i8_scale_from_bits(unsigned int bits)
+{
+    const float m = __uint_as_float(bits);
+    if (!(m > 0.0f) || !isfinite(m)) return 1.0f;
+    return kI8Target / m;
+}
+
+// Byte offset of K column c (0..63) of row r in a limb tile.
+__device__ __forceinline__ uint32_t swz64_offset(int r, int c)
+{
+    return (uint32_t) (r * 64 + ((((c >> 4) ^ (r >> 1)) & 3) << 4) +
+                       (c & 15));
+}
+
+// The three limbs of round(x q), packed as bytes 0 (a0), 1 (a1), 2 (a2).
+__device__ __forceinline__ uint32_t i8_limbs(float xq)
+{
+    const int a = __float2int_rn(xq);
+    const int a2 = ((a & 0xff) ^ 0x80) - 0x80;
+    const int r = (a - a2) >> 8;
+    const int a1 = ((r & 0xff) ^ 0x80) - 0x80;
+    const int a0 = (r - a1) >> 8;
+    return (uint32_t) (a0 & 0xff) | ((uint32_t) (a1 & 0xff) << 8) |
+           ((uint32_t) (a2 & 0xff) << 16);
+}
+
+// Writes one station-source's 2x2 A (already scaled by q) as 4 rows of the
+// three limb tiles of its block.
+__device__ __forceinline__ void store_entry_i8(uint8_t* block, int pl,
+        int sl, const float A[2][2][2])
+{
+#pragma unroll
+    for (int i = 0; i < 2; ++i)
+#pragma unroll
+        for (int c = 0; c < 2; ++c)
+        {
+            const int r = 4 * pl + 2 * i + c;
+            const uint32_t l0 = i8_limbs(A[i][0][c]);
+            const uint32_t l1 = i8_limbs(A[i][1][c]);
+            const uint32_t off = swz64_offset(r, 2 * sl);
+#pragma unroll
+            for (int limb = 0; limb < 3; ++limb)
+                *reinterpret_cast<uint16_t*>(block + limb * kI8Tile + off) =
+                        (uint16_t) (((l0 >> (8 * limb)) & 0xff) |
+                                    (((l1 >> (8 * limb)) & 0xff) << 8));
+        }
 }
 
 // Byte offset of the 4-byte word holding columns (2*sl, 2*sl+1) of tile row
@@ -208,7 +275,7 @@ __global__ void __launch_bounds__(256) maxabs_kernel(const TJ* __restrict__ jone
 // grid (k blocks, row blocks, problems); 8 warps, warp = 4 stations,
 // lane = source.
 // ---------------------------------------------------------------------------
-template <typename TJ>
+template <typename TJ, bool I8>
 __global__ void __launch_bounds__(256) prep_jones_kernel(
         const TJ* __restrict__ jones, int num_src, int num_st,
         const TJ* __restrict__ I, const TJ* __restrict__ Q,
@@ -221,8 +288,10 @@ __global__ void __launch_bounds__(256) prep_jones_kernel(
     const bool src_ok = s < num_src;
     float c11 = 0, c21r = 0, c21i = 0, c22 = 0;
     if (src_ok) brightness_factor(I[s], Q[s], U[s], V[s], c11, c21r, c21i, c22);
-    const float S = scale_from_bits(*maxabs_bits);
-    uint8_t* tile = W + (size_t) (rb * nkb + kb) * kPairBytes;
+    const float S = I8 ? i8_scale_from_bits(*maxabs_bits)
+                       : scale_from_bits(*maxabs_bits);
+    uint8_t* tile = W + (size_t) (rb * nkb + kb) *
+            (I8 ? kI8Block : kPairBytes);
     for (int pl = warp; pl < kStPerBlock; pl += 8)
     {
         const int p = rb * kStPerBlock + pl;
@@ -235,7 +304,10 @@ __global__ void __launch_bounds__(256) prep_jones_kernel(
 #pragma unroll
             for (int k = 0; k < 8; ++k) (&A[0][0][0])[k] *= S;
         }
-        store_entry(tile, pl, lane, A);
+        if constexpr (I8)
+            store_entry_i8(tile, pl, lane, A);
+        else
+            store_entry(tile, pl, lane, A);
     }
 }
 
@@ -251,7 +323,7 @@ __global__ void __launch_bounds__(256) prep_jones_kernel(
 // reading E and forming E C once per station-source for all of them.
 // grid (k blocks, row blocks); 8 warps, warp = 4 stations, lane = source.
 // ---------------------------------------------------------------------------
-template <typename TE>
+template <typename TE, bool I8>
 __global__ void __launch_bounds__(256) prep_fused_kernel(
         const TE* __restrict__ E, int num_src, int num_st,
         const double* __restrict__ l, const double* __restrict__ m,
@@ -274,8 +346,10 @@ __global__ void __launch_bounds__(256) prep_fused_kernel(
         brightness_factor(I[s], Q[s], U[s], V[s], c11, c21r, c21i, c22);
         sl = l[s]; sm = m[s]; sn1 = n[s] - 1.0;
     }
-    const float S = scale_from_bits(*maxabs_bits);
-    uint8_t* tile0 = W + (size_t) (rb * nkb + kb) * kPairBytes;
+    const float S = I8 ? i8_scale_from_bits(*maxabs_bits)
+                       : scale_from_bits(*maxabs_bits);
+    uint8_t* tile0 = W + (size_t) (rb * nkb + kb) *
+            (I8 ? kI8Block : kPairBytes);
     for (int pl = warp; pl < kStPerBlock; pl += 8)
     {
         const int p = rb * kStPerBlock + pl;
@@ -312,7 +386,11 @@ __global__ void __launch_bounds__(256) prep_fused_kernel(
                         A[i][kk][1] = re * sn + im * cs;
                     }
             }
-            store_entry(tile0 + (size_t) j * image_stride, pl, lane, A);
+            if constexpr (I8)
+                store_entry_i8(tile0 + (size_t) j * image_stride, pl, lane,
+                        A);
+            else
+                store_entry(tile0 + (size_t) j * image_stride, pl, lane, A);
         }
     }
 }
@@ -365,6 +443,7 @@ struct GemmParams
     double kw_scalar;
     double uv_min, uv_max;
     int casa;
+    int i8;                     // operand image is the three-limb integer one
     int* err;
     // Auto-correlations (optional): the diagonal station pairs of the
     // diagonal tiles, V_pp = J_p B J_p^H, added into
@@ -391,6 +470,65 @@ __device__ __forceinline__ void tile_of(int t, int& rb, int& cb)
     while (c * (c + 1) / 2 > t) --c;
     cb = c;
     rb = t - c * (c + 1) / 2;
+}
+
+// Visibilities of one square (128 x 128) task from the FP64 sums of the
+// thread's 16 column stations: row `row` of row block rb against column
+// block cb, column half h; scaled by inv_s2.
+__device__ __forceinline__ void square_task_store(const GemmParams& prm,
+        const double (&accR)[16], const double (&accI)[16], double inv_s2,
+        int row, int h, int prob, int rb, int cb)
+{
+    const int c = row & 1;
+    const int g = prm.prob0 + prob, t = g / prm.nch;
+    const int chan = g - t * prm.nch;
+    const int i = (row >> 1) & 1;
+    const int p = rb * kStPerBlock + (row >> 2);
+    const int N = prm.num_st;
+    const double* su = prm.st_u + prm.uv_stride * t;
+    const double* sv = prm.st_v + prm.uv_stride * t;
+    const double kw = prm.inv_wavelength ? prm.inv_wavelength[chan]
+                                          : prm.kw_scalar;
+    double* vbase = prm.vis + 8 * ((size_t) g * prm.vis_stride +
+            (size_t) prm.offset_out);
+    if (prm.autos && rb == cb && p < N)
+    {
+        // column station q = p of this thread's 16: V_pp[i][c]
+        const int ql = p - cb * kStPerBlock - 16 * h;
+#pragma unroll
+        for (int k = 0; k < 16; ++k)
+            if (k == ql)
+            {
+                double* o = prm.autos + 8 * ((size_t) g * N + p) +
+                        2 * (2 * i + c);
+                o[0] += accR[k] * inv_s2;
+                o[1] += accI[k] * inv_s2;
+            }
+    }
+#pragma unroll
+    for (int ql = 0; ql < 16; ++ql)
+    {
+        const int q = cb * kStPerBlock + 16 * h + ql;
+        if (p < q && q < N)
+        {
+            const double uu = (su[p] - su[q]) * kw;
+            const double vv = (sv[p] - sv[q]) * kw;
+            const double len = sqrt(uu * uu + vv * vv);
+            if (!(len < prm.uv_min || len > prm.uv_max))
+            {
+                const double re = accR[ql] * inv_s2;
+                const double im = accI[ql] * inv_s2;
+                // this thread holds V_pq[i][j] with j = c; the
+                // reference stores J_q B J_p^H (p < q) unless CASA
+                const int ro = prm.casa ? i : c;
+                const int co = prm.casa ? c : i;
+                double* o = vbase + 8 * (size_t) baseline_index(N, q, p)
+                        + 2 * (2 * ro + co);
+                o[0] += re;
+                o[1] += prm.casa ? im : -im;
+            }
+        }
+    }
 }
 
 __global__ void __launch_bounds__(kGemmThreads, 1)
@@ -620,58 +758,11 @@ gemm_kernel(const GemmParams prm)
             }
             if (!ok) break;
             // ---- visibilities of this tile
-            const int g = prm.prob0 + prob, t = g / prm.nch;
-            const int chan = g - t * prm.nch;
+            const int g = prm.prob0 + prob;
             const float S = scale_from_bits(
                     prm.maxabs_bits[prm.maxabs_stride * g]);
             const double inv_s2 = 1.0 / ((double) S * (double) S);
-            const int i = (row >> 1) & 1;
-            const int p = rb * kStPerBlock + (row >> 2);
-            const int N = prm.num_st;
-            const double* su = prm.st_u + prm.uv_stride * t;
-            const double* sv = prm.st_v + prm.uv_stride * t;
-            const double kw = prm.inv_wavelength ? prm.inv_wavelength[chan]
-                                                  : prm.kw_scalar;
-            double* vbase = prm.vis + 8 * ((size_t) g * prm.vis_stride +
-                    (size_t) prm.offset_out);
-            if (prm.autos && rb == cb && p < N)
-            {
-                // column station q = p of this thread's 16: V_pp[i][c]
-                const int ql = p - cb * kStPerBlock - 16 * h;
-#pragma unroll
-                for (int k = 0; k < 16; ++k)
-                    if (k == ql)
-                    {
-                        double* o = prm.autos + 8 * ((size_t) g * N + p) +
-                                2 * (2 * i + c);
-                        o[0] += accR[k] * inv_s2;
-                        o[1] += accI[k] * inv_s2;
-                    }
-            }
-#pragma unroll
-            for (int ql = 0; ql < 16; ++ql)
-            {
-                const int q = cb * kStPerBlock + 16 * h + ql;
-                if (p < q && q < N)
-                {
-                    const double uu = (su[p] - su[q]) * kw;
-                    const double vv = (sv[p] - sv[q]) * kw;
-                    const double len = sqrt(uu * uu + vv * vv);
-                    if (!(len < prm.uv_min || len > prm.uv_max))
-                    {
-                        const double re = accR[ql] * inv_s2;
-                        const double im = accI[ql] * inv_s2;
-                        // this thread holds V_pq[i][j] with j = c; the
-                        // reference stores J_q B J_p^H (p < q) unless CASA
-                        const int ro = prm.casa ? i : c;
-                        const int co = prm.casa ? c : i;
-                        double* o = vbase + 8 * (size_t) baseline_index(N, q, p)
-                                + 2 * (2 * ro + co);
-                        o[0] += re;
-                        o[1] += prm.casa ? im : -im;
-                    }
-                }
-            }
+            square_task_store(prm, accR, accI, inv_s2, row, h, prob, rb, cb);
         }
     }
 
@@ -1388,6 +1479,284 @@ gemm_pair_kernel(const GemmParams prm, const __grid_constant__ CUtensorMap tmap)
     if (warp == 1) ptx::tmem_dealloc_pair(tmem, kWTmemCols);
 }
 
+// ===========================================================================
+// Integer contraction (the default): G = W W^T from the three-limb 8-bit
+// image on the tcgen05 integer path. With a = a0 2^16 + a1 2^8 + a2 and b
+// likewise,
+//     a b / 2^16 = a0 b0 2^16 + (a0 b1 + a1 b0) 2^8 + (a0 b2 + a1 b1 + a2 b0)
+//                  + (a1 b2 + a2 b1) 2^-8 + a2 b2 2^-16,
+// the last term (at most 2^-32 of the largest product) left out: eight
+// 8-bit MMAs per 32-wide K step feed four S32 TMEM accumulators (D0 .. D3,
+// 128 columns each) of 128 x 128 tiles. The class a1 b2 + a2 b1 cannot be
+// left out too: its limbs are uniform digits whatever the entry's size, so
+// over many faint sources it would add ~1e-6 of the visibilities' L2 norm.
+// The integer sums are exact: no rounding happens in the tensor core, so
+// the accumulators only need draining before they could overflow (every
+// kI8DrainKb k blocks; one k block adds at most 3 x 64 x 2^14 < 2^21.6 to
+// D2) and at the end of a task, where D0 2^16 + D1 2^8 + D2 + D3 2^-8 is
+// formed in FP64 and folded into the visibility sums. The error is that of
+// the fixed-point entries (2^-24 of the largest |entry|).
+// Warp roles (320 threads): warp 0 producer (one bulk copy per operand per
+// k block into a kI8Stages-deep ring of 48 KB stages), warp 1 MMA issuer,
+// warps 2-9 epilogue (64 columns each, as the square FP16 kernel).
+// ===========================================================================
+constexpr int kI8Stages = 4;
+constexpr int kI8StageBytes = 2 * kI8Block;   // A block + B block
+constexpr int kI8DrainKb = 512;
+constexpr uint32_t kI8TmemCols = 512;         // D0, D1, D2, D3
+
+struct I8Ctl
+{
+    uint64_t full[kI8Stages], empty[kI8Stages], dfull, dempty, done;
+    uint32_t tmem_base;
+    int abort;
+};
+
+constexpr size_t gemm_i8_smem_bytes()
+{
+    return 1024 + (size_t) kI8Stages * kI8StageBytes + sizeof(I8Ctl);
+}
+
+__global__ void __launch_bounds__(kGemmThreads, 1)
+gemm_i8_kernel(const GemmParams prm)
+{
+    extern __shared__ uint8_t smem_raw[];
+    uint8_t* smem = reinterpret_cast<uint8_t*>(
+            (reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~(uintptr_t) 1023);
+    I8Ctl* ctl = reinterpret_cast<I8Ctl*>(smem + kI8Stages * kI8StageBytes);
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    volatile int* abort = &ctl->abort;
+
+    if (threadIdx.x == 0)
+    {
+        for (int s = 0; s < kI8Stages; ++s)
+        {
+            ptx::mbar_init(&ctl->full[s], 1);
+            ptx::mbar_init(&ctl->empty[s], 1);
+        }
+        ptx::mbar_init(&ctl->dfull, 1);
+        ptx::mbar_init(&ctl->dempty, 8);
+        ptx::mbar_init(&ctl->done, 1);
+        ctl->abort = 0;
+        ptx::fence_mbar_init();
+    }
+    if (warp == 1) ptx::tmem_alloc(&ctl->tmem_base, kI8TmemCols);
+    ptx::tc_fence_before();
+    __syncthreads();
+    ptx::tc_fence_after();
+    const uint32_t tmem = ctl->tmem_base;
+
+    const int ntile = prm.nrb * (prm.nrb + 1) / 2;
+    const int ntasks = ntile * prm.num_problems;
+    const int nchunk = (prm.nkb + kI8DrainKb - 1) / kI8DrainKb;
+
+    if (warp == 0)
+    {
+        if (lane == 0)
+        {
+            // ---------------- producer: A block, then B block (not on
+            // diagonal tiles, whose B is A)
+            int stage = 0;
+            uint32_t phase = 0;
+            uint32_t issued = 0, issued_par = 0;  // bit s: stage s
+            for (int task = blockIdx.x; task < ntasks && !*abort;
+                    task += gridDim.x)
+            {
+                const int prob = task / ntile;
+                int rb, cb;
+                tile_of(task - prob * ntile, rb, cb);
+                const bool diag = rb == cb;
+                const uint8_t* img = prm.W + (size_t) prob * prm.image_stride;
+                for (int kb = 0; kb < prm.nkb; ++kb)
+                {
+                    if (!ptx::mbar_wait(&ctl->empty[stage], phase ^ 1,
+                            prm.err, 31, abort))
+                        break;
+                    uint8_t* dst = smem + (size_t) stage * kI8StageBytes;
+                    ptx::mbar_arrive_expect_tx(&ctl->full[stage],
+                            diag ? kI8Block : 2 * kI8Block);
+                    ptx::bulk_g2s(dst, img + ((size_t) rb * prm.nkb + kb) *
+                            kI8Block, kI8Block, &ctl->full[stage]);
+                    if (!diag)
+                        ptx::bulk_g2s(dst + kI8Block, img +
+                                ((size_t) cb * prm.nkb + kb) * kI8Block,
+                                kI8Block, &ctl->full[stage]);
+                    issued |= 1u << stage;
+                    issued_par = (issued_par & ~(1u << stage)) |
+                            (phase << stage);
+                    if (++stage == kI8Stages) { stage = 0; phase ^= 1; }
+                }
+            }
+            for (int s = 0; s < kI8Stages; ++s)
+                if ((issued >> s) & 1)
+                    ptx::mbar_wait(&ctl->full[s], (issued_par >> s) & 1,
+                            prm.err, 32, abort);
+        }
+        __syncwarp();
+    }
+    else if (warp == 1)
+    {
+        if (lane == 0)
+        {
+            // ---------------- MMA issuer
+            const uint32_t idesc = ptx::idesc_s8_s32(128, 128);
+            const uint32_t d0 = tmem, d1 = tmem + 128, d2 = tmem + 256,
+                    d3 = tmem + 384;
+            int stage = 0;
+            uint32_t phase = 0, dpar = 0;
+            bool ok = true;
+            for (int task = blockIdx.x; task < ntasks && ok;
+                    task += gridDim.x)
+            {
+                const int prob = task / ntile;
+                int rb, cb;
+                tile_of(task - prob * ntile, rb, cb);
+                const bool diag = rb == cb;
+                for (int ch = 0; ch < nchunk && ok; ++ch)
+                {
+                    // the epilogue has read the accumulators' last sums
+                    if (!ptx::mbar_wait(&ctl->dempty, dpar ^ 1, prm.err, 33,
+                            abort))
+                    {
+                        ok = false;
+                        break;
+                    }
+                    ptx::tc_fence_after();
+                    const int kb0 = ch * kI8DrainKb;
+                    const int kb1 = min(prm.nkb, kb0 + kI8DrainKb);
+                    for (int kb = kb0; kb < kb1; ++kb)
+                    {
+                        if (!ptx::mbar_wait(&ctl->full[stage], phase, prm.err,
+                                34, abort))
+                        {
+                            ok = false;
+                            break;
+                        }
+                        ptx::tc_fence_after();
+                        const uint32_t a = ptx::smem_u32(smem +
+                                (size_t) stage * kI8StageBytes);
+                        const uint32_t b = diag ? a : a + kI8Block;
+#pragma unroll
+                        for (int k = 0; k < 2; ++k)
+                        {
+                            const uint64_t a0 = ptx::sdesc_sw64(a + 32 * k);
+                            const uint64_t a1 = ptx::sdesc_sw64(
+                                    a + kI8Tile + 32 * k);
+                            const uint64_t a2 = ptx::sdesc_sw64(
+                                    a + 2 * kI8Tile + 32 * k);
+                            const uint64_t b0 = ptx::sdesc_sw64(b + 32 * k);
+                            const uint64_t b1 = ptx::sdesc_sw64(
+                                    b + kI8Tile + 32 * k);
+                            const uint64_t b2 = ptx::sdesc_sw64(
+                                    b + 2 * kI8Tile + 32 * k);
+                            const uint32_t acc =
+                                    (kb > kb0 || k > 0) ? 1u : 0u;
+                            ptx::mma_i8(d0, a0, b0, idesc, acc);
+                            ptx::mma_i8(d1, a0, b1, idesc, acc);
+                            ptx::mma_i8(d1, a1, b0, idesc, 1u);
+                            ptx::mma_i8(d2, a0, b2, idesc, acc);
+                            ptx::mma_i8(d2, a1, b1, idesc, 1u);
+                            ptx::mma_i8(d2, a2, b0, idesc, 1u);
+                            ptx::mma_i8(d3, a1, b2, idesc, acc);
+                            ptx::mma_i8(d3, a2, b1, idesc, 1u);
+                        }
+                        ptx::mma_commit(&ctl->empty[stage]);
+                        if (++stage == kI8Stages) { stage = 0; phase ^= 1; }
+                    }
+                    if (!ok) break;
+                    ptx::mma_commit(&ctl->dfull);
+                    dpar ^= 1;
+                }
+            }
+            // All issued MMAs must finish before TMEM is released.
+            ptx::mma_commit(&ctl->done);
+            ptx::mbar_wait(&ctl->done, 0, prm.err, 35, abort);
+        }
+        __syncwarp();
+    }
+    else
+    {
+        // ---------------- epilogue: 8 warps, 64 columns each
+        const int q4 = warp & 3;          // TMEM lane quadrant of this warp
+        const int h = (warp - 2) >> 2;    // column half
+        const int row = 32 * q4 + lane;   // row of the G tile
+        const int c = row & 1;
+        const uint32_t taddr = tmem + ((uint32_t) (32 * q4) << 16) +
+                (uint32_t) (64 * h);
+        uint32_t dpar = 0;
+        bool ok = true;
+        for (int task = blockIdx.x; task < ntasks && ok; task += gridDim.x)
+        {
+            const int prob = task / ntile;
+            int rb, cb;
+            tile_of(task - prob * ntile, rb, cb);
+            // sums of Re V and Im V, in units of 2^16 / q^2, of the
+            // thread's 16 column stations
+            double accR[16], accI[16];
+#pragma unroll
+            for (int j = 0; j < 16; ++j) accR[j] = accI[j] = 0.0;
+            for (int ch = 0; ch < nchunk; ++ch)
+            {
+                if (!ptx::mbar_wait(&ctl->dfull, dpar, prm.err, 36, abort))
+                {
+                    ok = false;
+                    break;
+                }
+                ptx::tc_fence_after();
+#pragma unroll
+                for (int j0 = 0; j0 < 64; j0 += 16)
+                {
+                    uint32_t v0[16], v1[16], v2[16], v3[16];
+                    ptx::tmem_ld16(taddr + j0, v0);
+                    ptx::tmem_ld16(taddr + 128 + j0, v1);
+                    ptx::tmem_ld16(taddr + 256 + j0, v2);
+                    ptx::tmem_ld16(taddr + 384 + j0, v3);
+                    ptx::tmem_ld_wait();
+                    double v[16];
+#pragma unroll
+                    for (int j = 0; j < 16; ++j)
+                        v[j] = ((double) (int) v0[j] * 65536.0 +
+                                (double) (int) v1[j] * 256.0 +
+                                (double) (int) v2[j]) +
+                               (double) (int) v3[j] * 0.00390625;
+                    // Re V = G00 + G11, Im V = G10 - G01 across the row pair
+                    // (lanes l, l ^ 1), as the FP16 kernels fold
+#pragma unroll
+                    for (int qq = 0; qq < 4; ++qq)
+                    {
+                        const int jb = 4 * qq;
+                        const double s0 = c ? v[jb + 0] : v[jb + 2];
+                        const double s1 = c ? v[jb + 1] : v[jb + 3];
+                        const double r0 = __shfl_xor_sync(0xffffffffu, s0, 1);
+                        const double r1 = __shfl_xor_sync(0xffffffffu, s1, 1);
+                        const double g00 = c ? r0 : v[jb + 0];
+                        const double g01 = c ? r1 : v[jb + 1];
+                        const double g10 = c ? v[jb + 2] : r0;
+                        const double g11 = c ? v[jb + 3] : r1;
+                        accR[j0 / 4 + qq] += g00 + g11;
+                        accI[j0 / 4 + qq] += g10 - g01;
+                    }
+                }
+                ptx::tc_fence_before();
+                __syncwarp();
+                if (lane == 0) ptx::mbar_arrive(&ctl->dempty);
+                dpar ^= 1;
+            }
+            if (!ok) break;
+            const int g = prm.prob0 + prob;
+            const double q = (double) i8_scale_from_bits(
+                    prm.maxabs_bits[prm.maxabs_stride * g]);
+            square_task_store(prm, accR, accI, 65536.0 / (q * q), row, h,
+                    prob, rb, cb);
+        }
+    }
+
+    ptx::tc_fence_before();
+    __syncthreads();
+    ptx::tc_fence_after();
+    if (warp == 1) ptx::tmem_dealloc(tmem, kI8TmemCols);
+}
+
 }  // namespace tc
 }  // namespace oskb
 
@@ -1516,6 +1885,22 @@ int tile_setting()
 }
 
 std::atomic<int> g_last_tile{0};
+std::atomic<int> g_last_arith{0};
+
+// Arithmetic of the contraction: the three-limb 8-bit integer form unless
+// OSKB_TC_ARITH=fp16 or an FP16 tile shape is fixed by OSKB_TC_TILE.
+bool arith_i8()
+{
+    const char* e = getenv("OSKB_TC_ARITH");
+    if (e && strcmp(e, "fp16") == 0) return false;
+    return tile_setting() == 0;
+}
+
+size_t image_bytes_for(bool i8, int num_st, int num_src)
+{
+    return i8 ? image_bytes_i8(num_st, num_src)
+              : image_bytes(num_st, num_src);
+}
 
 // Per-device launch set-up: the dynamic shared-memory opt-in of both
 // contraction kernels (a per-device attribute) and whether the wide
@@ -1547,7 +1932,10 @@ int device_setup(bool& wide_fits, bool& pair_fits)
                 (int) gemm_wide_smem_bytes()) != cudaSuccess ||
                 cudaFuncSetAttribute(gemm_pair_kernel,
                 cudaFuncAttributeMaxDynamicSharedMemorySize,
-                (int) gemm_pair_smem_bytes()) != cudaSuccess)
+                (int) gemm_pair_smem_bytes()) != cudaSuccess ||
+                cudaFuncSetAttribute(gemm_i8_kernel,
+                cudaFuncAttributeMaxDynamicSharedMemorySize,
+                (int) gemm_i8_smem_bytes()) != cudaSuccess)
         {
             set_last_error("tc gemm attributes", cudaGetLastError());
             return OSKB_ERR_KERNEL_LAUNCH_FAILURE;
@@ -1597,6 +1985,23 @@ EncodeTiledFn encode_tiled_fn()
     return f;
 }
 
+// Records the start event of a timed contraction launch (when timing is
+// on) and returns the event to record after it, else nullptr.
+cudaEvent_t timing_start(cudaStream_t stream)
+{
+    std::lock_guard<std::mutex> lock(g_timing_mutex);
+    if (!g_timing) return nullptr;
+    if (g_ev_used == g_ev.size())
+    {
+        cudaEvent_t e0, e1;
+        cudaEventCreate(&e0);
+        cudaEventCreate(&e1);
+        g_ev.emplace_back(e0, e1);
+    }
+    cudaEventRecord(g_ev[g_ev_used].first, stream);
+    return g_ev[g_ev_used++].second;
+}
+
 int launch_gemm(GemmParams& gp, cudaStream_t stream)
 {
     bool wide_fits = false, pair_fits = false;
@@ -1604,6 +2009,17 @@ int launch_gemm(GemmParams& gp, cudaStream_t stream)
     if (serr) return serr;
     const long long square = (long long) gp.nrb * (gp.nrb + 1) / 2 *
             gp.num_problems;
+    if (gp.i8)
+    {
+        const int grid = (int) (square < num_sms() ? square : num_sms());
+        g_last_tile.store(128);
+        g_last_arith.store(8);
+        cudaEvent_t ev_stop = timing_start(stream);
+        gemm_i8_kernel<<<grid, kGemmThreads, gemm_i8_smem_bytes(), stream>>>(
+                gp);
+        if (ev_stop) cudaEventRecord(ev_stop, stream);
+        return check_launch("tc gemm (integer)");
+    }
     const long long wide_n = (long long) wide_tiles(gp.nrb) *
             gp.num_problems;
     const long long pair_n = (long long) pair_tiles(gp.nrb) *
@@ -1621,24 +2037,9 @@ int launch_gemm(GemmParams& gp, cudaStream_t stream)
     if (pair)
         grid = 2 * (int) (pair_n < pairs ? pair_n : pairs);
     g_last_tile.store(pair ? 512 : wide ? 256 : 128);
+    g_last_arith.store(16);
     gp.drain_kb = drain_kblocks();
-    cudaEvent_t ev_stop = nullptr;
-    {
-        std::lock_guard<std::mutex> lock(g_timing_mutex);
-        if (g_timing)
-        {
-            if (g_ev_used == g_ev.size())
-            {
-                cudaEvent_t e0, e1;
-                cudaEventCreate(&e0);
-                cudaEventCreate(&e1);
-                g_ev.emplace_back(e0, e1);
-            }
-            cudaEventRecord(g_ev[g_ev_used].first, stream);
-            ev_stop = g_ev[g_ev_used].second;
-            ++g_ev_used;
-        }
-    }
+    cudaEvent_t ev_stop = timing_start(stream);
     CUtensorMap tmap;
     if (pair)
     {
@@ -1715,10 +2116,17 @@ int oskb_cross_correlate_tc_d(int casa, int num_sources, int num_stations,
     if ((err = check_launch("tc maxabs"))) return err;
     const int nrb = (num_stations + kStPerBlock - 1) / kStPerBlock;
     const int nkb = (num_sources + kSrcPerBlock - 1) / kSrcPerBlock;
-    prep_jones_kernel<double><<<dim3(nkb, nrb), 256, 0, s>>>(jones,
-            num_sources, num_stations, I, Q, U, V, &hdr->maxabs_bits, W);
+    const bool i8 = arith_i8();
+    if (i8)
+        prep_jones_kernel<double, true><<<dim3(nkb, nrb), 256, 0, s>>>(jones,
+                num_sources, num_stations, I, Q, U, V, &hdr->maxabs_bits, W);
+    else
+        prep_jones_kernel<double, false><<<dim3(nkb, nrb), 256, 0, s>>>(
+                jones, num_sources, num_stations, I, Q, U, V,
+                &hdr->maxabs_bits, W);
     if ((err = check_launch("tc prep"))) return err;
     GemmParams gp;
+    gp.i8 = i8;
     gp.W = W; gp.image_stride = 0; gp.nrb = nrb; gp.nkb = nkb;
     gp.num_problems = 1; gp.num_st = num_stations;
     gp.maxabs_bits = &hdr->maxabs_bits; gp.maxabs_stride = 0;
@@ -1807,7 +2215,8 @@ int correlate_block(int casa, int num_sources, int num_stations,
             !inv_wavelength || !vis)
         return OSKB_ERR_INVALID_ARGUMENT;
     // Problems (t, c) are processed in groups that fit the workspace.
-    const size_t img = image_bytes(num_stations, num_sources);
+    const bool i8 = arith_i8();
+    const size_t img = image_bytes_for(i8, num_stations, num_sources);
     int group = num_problems;
     if (workspace)
     {
@@ -1845,13 +2254,19 @@ int correlate_block(int casa, int num_sources, int num_stations,
     for (int p0 = 0; p0 < num_problems; p0 += group)
     {
         const int np = min(group, num_problems - p0);
-        prep_fused_kernel<TE><<<dim3(nkb, nrb), 256, 0, s>>>(E,
-                num_sources,
-                num_stations, l, m, n, I, Q, U, V, station_uvw,
-                inv_wavelength, num_channels, p0, np, &hdr->maxabs_bits, W,
-                img);
+        if (i8)
+            prep_fused_kernel<TE, true><<<dim3(nkb, nrb), 256, 0, s>>>(E,
+                    num_sources, num_stations, l, m, n, I, Q, U, V,
+                    station_uvw, inv_wavelength, num_channels, p0, np,
+                    &hdr->maxabs_bits, W, img);
+        else
+            prep_fused_kernel<TE, false><<<dim3(nkb, nrb), 256, 0, s>>>(E,
+                    num_sources, num_stations, l, m, n, I, Q, U, V,
+                    station_uvw, inv_wavelength, num_channels, p0, np,
+                    &hdr->maxabs_bits, W, img);
         if ((err = check_launch("tc prep fused"))) return err;
         GemmParams gp;
+        gp.i8 = i8;
         gp.W = W; gp.image_stride = img; gp.nrb = nrb; gp.nkb = nkb;
         gp.num_problems = np; gp.num_st = num_stations;
         gp.maxabs_bits = &hdr->maxabs_bits; gp.maxabs_stride = 0;
@@ -1914,6 +2329,11 @@ int oskb_tc_timing_read(double* total_ms, int* launches)
 int oskb_tc_tile_columns(void)
 {
     return g_last_tile.load();
+}
+
+int oskb_tc_arithmetic(void)
+{
+    return g_last_arith.load();
 }
 
 int oskb_tc_status(const void* workspace, int* flags, int* wait_error)
@@ -2034,10 +2454,17 @@ extern "C" int oskb_cross_correlate_tc_noalloc_d(int casa, int num_sources,
     if ((err = check_launch("tc maxabs (static scratch)"))) return err;
     const int nrb = (num_stations + kStPerBlock - 1) / kStPerBlock;
     const int nkb = (num_sources + kSrcPerBlock - 1) / kSrcPerBlock;
-    prep_jones_kernel<double><<<dim3(nkb, nrb), 256, 0, s>>>(jones,
-            num_sources, num_stations, I, Q, U, V, &hdr->maxabs_bits, W);
+    const bool i8 = arith_i8();
+    if (i8)
+        prep_jones_kernel<double, true><<<dim3(nkb, nrb), 256, 0, s>>>(jones,
+                num_sources, num_stations, I, Q, U, V, &hdr->maxabs_bits, W);
+    else
+        prep_jones_kernel<double, false><<<dim3(nkb, nrb), 256, 0, s>>>(
+                jones, num_sources, num_stations, I, Q, U, V,
+                &hdr->maxabs_bits, W);
     if ((err = check_launch("tc prep (static scratch)"))) return err;
     GemmParams gp;
+    gp.i8 = i8;
     gp.W = W; gp.image_stride = 0; gp.nrb = nrb; gp.nkb = nkb;
     gp.num_problems = 1; gp.num_st = num_stations;
     gp.maxabs_bits = &hdr->maxabs_bits; gp.maxabs_stride = 0;
