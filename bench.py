@@ -230,13 +230,14 @@ def _load_peaks():
             "bf16_tflops_sustained": 1400.0}, "fallback"
 
 
-def _load_traffic(tile):
-    """DRAM bytes per launch of the contraction kernel (square, wide or pair
-    tiles) from the committed ncu summary
-    (profiles/tc_gemm{,_wide,_pair}_c3_traffic.json), or None."""
-    name = {256: "tc_gemm_wide_c3_traffic.json",
-            512: "tc_gemm_pair_c3_traffic.json"}.get(
-                tile, "tc_gemm_c3_traffic.json")
+def _load_traffic(tile, arith=16):
+    """DRAM bytes per launch of the contraction kernel (integer, or FP16
+    square, wide or pair tiles) from the committed ncu summary
+    (profiles/tc_gemm{_i8,,_wide,_pair}_c3_traffic.json), or None."""
+    name = "tc_gemm_i8_c3_traffic.json" if arith == 8 else {
+        256: "tc_gemm_wide_c3_traffic.json",
+        512: "tc_gemm_pair_c3_traffic.json"}.get(
+            tile, "tc_gemm_c3_traffic.json")
     path = os.path.join(ROOT, "profiles", name)
     if not os.path.exists(path):
         return None
@@ -353,7 +354,23 @@ def run_ours(args):
             nrb = (nst + 31) // 32
             kp = 2 * 32 * ((nsrc + 31) // 32)
             tile = ob.load().oskb_tc_tile_columns()
-            if tile == 512:
+            arith = ob.load().oskb_tc_arithmetic()
+            issued_pk, issued_kind = pk, "measured bf16 sustained"
+            if arith == 8:
+                # integer form: eight 8-bit limb products per K step (2 ops
+                # per multiply-add) on square tiles, or on 256 x 128 pair
+                # tiles (tile 256); the 8-bit dense rate is twice the 16-bit
+                # one
+                if tile == 256:
+                    ntp = sum(nrb - 2 * ti for ti in range((nrb + 1) // 2))
+                    issued = nch * ntp * 256 * 128 * kp * 2 * 8
+                else:
+                    issued = nch * nrb * (nrb + 1) // 2 * 128 * 128 * kp * \
+                        2 * 8
+                issued_pk = 2 * pk
+                issued_kind = ("2 x measured bf16 sustained (the int8 dense "
+                               "tensor rate is twice the bf16 one)")
+            elif tile == 512:
                 # pair tiles: 256 x 256 per CTA pair over the triangle of
                 # row-block pairs
                 npr = (nrb + 1) // 2
@@ -366,18 +383,24 @@ def run_ours(args):
             else:
                 issued = nch * nrb * (nrb + 1) // 2 * 128 * 128 * kp * 2 * 3
             issued_tf = issued / (avg * 1e-3) / 1e12
-            traffic = _load_traffic(tile)
+            traffic = _load_traffic(tile, arith)
             roof = {"bound": "tensor", "achieved": ach, "peak": pk,
                     "unit": "TFLOP/s", "frac": ach / pk, "traffic": traffic,
-                    "kernel": {256: "oskb::tc::gemm_wide_kernel",
-                               512: "oskb::tc::gemm_pair_kernel"}.get(
-                                   tile, "oskb::tc::gemm_kernel"),
+                    "kernel": ("oskb::tc::gemm_pair_i8_kernel"
+                               if tile == 256 else "oskb::tc::gemm_i8_kernel")
+                              if arith == 8
+                              else {256: "oskb::tc::gemm_wide_kernel",
+                                    512: "oskb::tc::gemm_pair_kernel"}.get(
+                                        tile, "oskb::tc::gemm_kernel"),
                     "tile_columns": tile,
+                    "arithmetic": "int8 x3 limbs -> exact s32" if arith == 8
+                                  else "fp16 hi/lo x3 -> f32 -> f64",
                     "peak_kind": "%s bf16 sustained (fp16 same rate)"
                                  % peak_kind,
                     "algorithmic_flops_per_launch": 64.0 * sb_launch,
                     "issued_tflops": issued_tf,
-                    "issued_frac": issued_tf / pk,
+                    "issued_frac": issued_tf / issued_pk,
+                    "issued_peak_kind": issued_kind,
                     "avg_launch_ms": avg,
                     "share_of_step": gemm_ms / ms_total}
         else:
@@ -391,8 +414,10 @@ def run_ours(args):
             "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": ms_max / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None,
-            "dtype": "fp16x3->f32->f64 (TC), f64 phase" if args.path == "tc"
-                     else "f64",
+            "dtype": ("int8x3 limbs->s32 exact (TC), f64 phase"
+                      if roof.get("arithmetic", "").startswith("int8") else
+                      "fp16x3->f32->f64 (TC), f64 phase")
+                     if args.path == "tc" else "f64",
             "data": "synthetic",
             "config": {"workload": "c3: 512 stations log-radial to 65 km, "
                        "100,000 point sources (full Stokes), 2x2 E per "
@@ -402,7 +427,10 @@ def run_ours(args):
                        "path": args.path,
                        "parallelism": "dumps sharded over %d rank(s)" % world,
                        "l2": "inputs larger than L2 (E 1.6 GB; operand "
-                             "images 26 GB per step)"},
+                             "images %.1f GB per step)" % (
+                                 nst * nsrc * nch * (24 if roof.get(
+                                     "arithmetic", "").startswith("int8")
+                                     else 32) / 1e9)},
             "gpu_launches": launches_per_step * args.steps,
             "roofline": roof, "clocks": clk,
             "direct_fp64": cmp_["direct"],
@@ -580,8 +608,9 @@ def run_e2e(args, cfg, ob, torch, E, world, rank):
 def run_profile_case(args):
     """One small invocation of a single kernel, for ncu captures: inputs
     larger than L2 but a few GB on the device at most, two launches.
-      tc_small      the tensor-core contraction (gemm_kernel) and its
-                    operand preparation (prep_fused_kernel): 512 stations x
+      tc_small      the tensor-core contraction (gemm_i8_kernel, the
+                    default) and its operand preparation
+                    (prep_fused_kernel): 512 stations x
                     20,000 sources x 1 channel, 1/80 of a bench launch;
       tc_wide_small the wide-tile contraction (gemm_wide_kernel, tile
                     shape fixed to 128 x 256): 512 stations x 2,500
@@ -589,6 +618,8 @@ def run_profile_case(args):
                     launch;
       tc_pair_small the pair-tile contraction (gemm_pair_kernel, 256 x 256
                     tiles on CTA pairs) on the same case (288 pair tiles);
+      tc_i8_small   the integer contraction (gemm_i8_kernel, the default)
+                    on the same case (1,088 square tiles);
       direct_small  the FP64 direct cross-correlation: 512 stations x 2,000
                     sources, 1 channel;
       beam_small    the fused station beam: 32 stations x 256 dipoles x
@@ -606,11 +637,13 @@ def run_profile_case(args):
     if case in ("tc_wide_small", "tc_pair_small"):
         os.environ["OSKB_TC_TILE"] = "256" if case == "tc_wide_small" \
             else "512"
-    if case in ("tc_small", "tc_wide_small", "tc_pair_small",
+    if case in ("tc_small", "tc_wide_small", "tc_pair_small", "tc_i8_small",
                 "direct_small"):
         nsrc = {"tc_small": 20_000, "tc_wide_small": 2_500,
-                "tc_pair_small": 2_500, "direct_small": 2_000}[case]
-        nch = 8 if case in ("tc_wide_small", "tc_pair_small") else 1
+                "tc_pair_small": 2_500, "tc_i8_small": 2_500,
+                "direct_small": 2_000}[case]
+        nch = 8 if case in ("tc_wide_small", "tc_pair_small",
+                            "tc_i8_small") else 1
         cfg = workloads.c3(num_src=nsrc, num_channels=nch, num_times=1)
         nst, nbl = cfg.num_st, cfg.num_baselines
         l, m, n, I, Q, U, V = (dev(x) for x in (cfg.l, cfg.m, cfg.n, cfg.I,
@@ -1251,6 +1284,7 @@ def main():
     ap.add_argument("--c5-bound", type=float, default=1e-4)
     ap.add_argument("--profile-case", default=None,
                     choices=["tc_small", "tc_wide_small", "tc_pair_small",
+                             "tc_i8_small",
                              "direct_small",
                              "beam_small",
                              "block_small"],

@@ -1105,10 +1105,12 @@ OSKB_API int oskb_tc_noalloc_status(int* flags, int* wait_error);
 OSKB_API int oskb_tc_status(const void* workspace, int* flags,
         int* wait_error);
 /* Tile shape of the last tensor-core contraction launched, 0 before the
- * first: 128 (128 x 128 tiles of G per CTA), 256 (128 x 256 per CTA) or
- * 512 (256 x 256 per pair of CTAs, cta_group::2). The environment variable
- * OSKB_TC_TILE (128, 256 or 512) fixes it; unset, wide tiles are used
- * when a launch has at least two per SM, else square tiles. */
+ * first. FP16 form: 128 (128 x 128 tiles of G per CTA), 256 (128 x 256 per
+ * CTA) or 512 (256 x 256 per pair of CTAs, cta_group::2); the environment
+ * variable OSKB_TC_TILE (128, 256 or 512) selects the FP16 form with that
+ * tile (with OSKB_TC_ARITH=fp16 and no tile set: wide tiles when a launch
+ * has at least two per SM, else square). Integer form: 128 (128 x 128 per
+ * CTA, the default) or 256 (256 x 128 per pair of CTAs, OSKB_TC_PAIR=1). */
 OSKB_API int oskb_tc_tile_columns(void);
 /* Arithmetic of the last tensor-core contraction launched, 0 before the
  * first: 8 for the default integer form (each scaled entry a 24-bit fixed-

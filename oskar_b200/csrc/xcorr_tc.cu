@@ -1517,6 +1517,48 @@ constexpr size_t gemm_i8_smem_bytes()
     return 1024 + (size_t) kI8Stages * kI8StageBytes + sizeof(I8Ctl);
 }
 
+// One drain of the four integer accumulators over this thread's 64 columns
+// (taddr): D0 2^16 + D1 2^8 + D2 + D3 2^-8 per column, folded into the Re V
+// and Im V sums of its 16 column stations.
+__device__ __forceinline__ void i8_drain64(uint32_t taddr, int c,
+        double (&accR)[16], double (&accI)[16])
+{
+#pragma unroll
+    for (int j0 = 0; j0 < 64; j0 += 16)
+    {
+        uint32_t v0[16], v1[16], v2[16], v3[16];
+        ptx::tmem_ld16(taddr + j0, v0);
+        ptx::tmem_ld16(taddr + 128 + j0, v1);
+        ptx::tmem_ld16(taddr + 256 + j0, v2);
+        ptx::tmem_ld16(taddr + 384 + j0, v3);
+        ptx::tmem_ld_wait();
+        double v[16];
+#pragma unroll
+        for (int j = 0; j < 16; ++j)
+            v[j] = ((double) (int) v0[j] * 65536.0 +
+                    (double) (int) v1[j] * 256.0 +
+                    (double) (int) v2[j]) +
+                   (double) (int) v3[j] * 0.00390625;
+        // Re V = G00 + G11, Im V = G10 - G01 across the row pair
+        // (lanes l, l ^ 1), as the FP16 kernels fold
+#pragma unroll
+        for (int qq = 0; qq < 4; ++qq)
+        {
+            const int jb = 4 * qq;
+            const double s0 = c ? v[jb + 0] : v[jb + 2];
+            const double s1 = c ? v[jb + 1] : v[jb + 3];
+            const double r0 = __shfl_xor_sync(0xffffffffu, s0, 1);
+            const double r1 = __shfl_xor_sync(0xffffffffu, s1, 1);
+            const double g00 = c ? r0 : v[jb + 0];
+            const double g01 = c ? r1 : v[jb + 1];
+            const double g10 = c ? v[jb + 2] : r0;
+            const double g11 = c ? v[jb + 3] : r1;
+            accR[j0 / 4 + qq] += g00 + g11;
+            accI[j0 / 4 + qq] += g10 - g01;
+        }
+    }
+}
+
 __global__ void __launch_bounds__(kGemmThreads, 1)
 gemm_i8_kernel(const GemmParams prm)
 {
@@ -1703,40 +1745,7 @@ gemm_i8_kernel(const GemmParams prm)
                     break;
                 }
                 ptx::tc_fence_after();
-#pragma unroll
-                for (int j0 = 0; j0 < 64; j0 += 16)
-                {
-                    uint32_t v0[16], v1[16], v2[16], v3[16];
-                    ptx::tmem_ld16(taddr + j0, v0);
-                    ptx::tmem_ld16(taddr + 128 + j0, v1);
-                    ptx::tmem_ld16(taddr + 256 + j0, v2);
-                    ptx::tmem_ld16(taddr + 384 + j0, v3);
-                    ptx::tmem_ld_wait();
-                    double v[16];
-#pragma unroll
-                    for (int j = 0; j < 16; ++j)
-                        v[j] = ((double) (int) v0[j] * 65536.0 +
-                                (double) (int) v1[j] * 256.0 +
-                                (double) (int) v2[j]) +
-                               (double) (int) v3[j] * 0.00390625;
-                    // Re V = G00 + G11, Im V = G10 - G01 across the row pair
-                    // (lanes l, l ^ 1), as the FP16 kernels fold
-#pragma unroll
-                    for (int qq = 0; qq < 4; ++qq)
-                    {
-                        const int jb = 4 * qq;
-                        const double s0 = c ? v[jb + 0] : v[jb + 2];
-                        const double s1 = c ? v[jb + 1] : v[jb + 3];
-                        const double r0 = __shfl_xor_sync(0xffffffffu, s0, 1);
-                        const double r1 = __shfl_xor_sync(0xffffffffu, s1, 1);
-                        const double g00 = c ? r0 : v[jb + 0];
-                        const double g01 = c ? r1 : v[jb + 1];
-                        const double g10 = c ? v[jb + 2] : r0;
-                        const double g11 = c ? v[jb + 3] : r1;
-                        accR[j0 / 4 + qq] += g00 + g11;
-                        accI[j0 / 4 + qq] += g10 - g01;
-                    }
-                }
+                i8_drain64(taddr, c, accR, accI);
                 ptx::tc_fence_before();
                 __syncwarp();
                 if (lane == 0) ptx::mbar_arrive(&ctl->dempty);
@@ -1755,6 +1764,284 @@ gemm_i8_kernel(const GemmParams prm)
     __syncthreads();
     ptx::tc_fence_after();
     if (warp == 1) ptx::tmem_dealloc(tmem, kI8TmemCols);
+}
+
+// ===========================================================================
+// Integer contraction on CTA pairs (cta_group::2): one task is the 256 x
+// 128 tile of G of row blocks 2 ti and 2 ti + 1 (one per CTA) against
+// column block cb (cb >= 2 ti). Each CTA brings its own row block's three
+// limb tiles (A, 24 KB per k block) and half of the column block's (64 of
+// its 128 rows, 12 KB), so a product moves 36 KB per CTA through shared
+// memory where the square kernel moves 48 KB; per 32-wide K step the MMAs
+// then read 6 KB of operands per CTA instead of 8 KB. Shared-memory
+// bandwidth was the suspected bound of the square kernel's tensor pipe (its
+// MMAs alone read 128 bytes per cycle at the full 8-bit rate), but the
+// pairs measured slower (41.4 against 38.6 ms at 512 stations x 100,000
+// sources x 16 channels), so they are opt-in (OSKB_TC_PAIR=1). Each CTA's
+// TMEM holds the four accumulators of its 128 rows (128 columns each).
+// Synchronisation between the two CTAs is that of gemm_pair_kernel:
+// tensor-map copies (cta_group::2 form, no multicast) counted on the even
+// CTA's full barrier, multicast commits for empty / dfull, the epilogue
+// warps of both CTAs arriving on the even CTA's dempty.
+// ===========================================================================
+constexpr int kPI8Half = 3 * 64 * 64;                 // B half: 3 x 64 rows
+constexpr int kPI8StageBytes = kI8Block + kPI8Half;   // 36 KB
+constexpr int kPI8Stages = 6;
+
+struct PairI8Ctl
+{
+    uint64_t full[kPI8Stages], empty[kPI8Stages], dfull, dempty, done;
+    uint32_t tmem_base;
+    int abort;
+};
+
+constexpr size_t gemm_pair_i8_smem_bytes()
+{
+    return 1024 + (size_t) kPI8Stages * kPI8StageBytes + sizeof(PairI8Ctl);
+}
+
+__host__ __device__ inline int pair_i8_tiles(int nrb)
+{
+    int n = 0;
+    for (int ti = 0; 2 * ti < nrb; ++ti) n += nrb - 2 * ti;
+    return n;
+}
+
+// Task t of one problem -> (ti, cb), cb = 2 ti .. nrb - 1 for each ti.
+__device__ __forceinline__ void pair_i8_tile_of(int t, int nrb, int& ti,
+        int& cb)
+{
+    ti = 0;
+    while (t >= nrb - 2 * ti)
+    {
+        t -= nrb - 2 * ti;
+        ++ti;
+    }
+    cb = 2 * ti + t;
+}
+
+__global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kGemmThreads, 1)
+gemm_pair_i8_kernel(const GemmParams prm,
+        const __grid_constant__ CUtensorMap tmap_a,
+        const __grid_constant__ CUtensorMap tmap_b)
+{
+    extern __shared__ uint8_t smem_raw[];
+    uint8_t* smem = reinterpret_cast<uint8_t*>(
+            (reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~(uintptr_t) 1023);
+    PairI8Ctl* ctl = reinterpret_cast<PairI8Ctl*>(
+            smem + kPI8Stages * kPI8StageBytes);
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const uint32_t rank = ptx::cluster_ctarank();
+    volatile int* abort = &ctl->abort;
+
+    if (threadIdx.x == 0)
+    {
+        for (int s = 0; s < kPI8Stages; ++s)
+        {
+            ptx::mbar_init(&ctl->full[s], 1);
+            ptx::mbar_init(&ctl->empty[s], 1);
+        }
+        ptx::mbar_init(&ctl->dfull, 1);
+        ptx::mbar_init(&ctl->dempty, 16);
+        ptx::mbar_init(&ctl->done, 1);
+        ctl->abort = 0;
+        ptx::fence_mbar_init();
+    }
+    if (warp == 1) ptx::tmem_alloc_pair(&ctl->tmem_base, kI8TmemCols);
+    ptx::tc_fence_before();
+    // both CTAs' barriers initialised and TMEM allocated before any
+    // cross-CTA arrive or MMA
+    ptx::cluster_sync();
+    ptx::tc_fence_after();
+    const uint32_t tmem = ctl->tmem_base;
+
+    const int ntile = pair_i8_tiles(prm.nrb);
+    const int npairs = gridDim.x >> 1;
+    const int pair = blockIdx.x >> 1;
+    const int ntasks = ntile * prm.num_problems;
+    const int nchunk = (prm.nkb + kI8DrainKb - 1) / kI8DrainKb;
+    // limb tiles (8 KB each) per problem image
+    const long long tiles_per_prob = (long long) (prm.image_stride / kI8Tile);
+
+    if (warp == 0)
+    {
+        if (lane == 0)
+        {
+            // ---------------- producer: this CTA's row block (three limb
+            // tiles) and its half of the column block's, counted on the
+            // even CTA's full barrier
+            const uint32_t full0 = ptx::mapa_shared(
+                    ptx::smem_u32(&ctl->full[0]), 0);
+            int stage = 0;
+            uint32_t phase = 0;
+            uint32_t issued = 0, issued_par = 0;
+            for (int task = pair; task < ntasks && !*abort; task += npairs)
+            {
+                const int prob = task / ntile;
+                int ti, cb;
+                pair_i8_tile_of(task - prob * ntile, prm.nrb, ti, cb);
+                // a missing odd row block repeats the last one; its rows are
+                // discarded (p >= N)
+                int rb = 2 * ti + (int) rank;
+                if (rb >= prm.nrb) rb = prm.nrb - 1;
+                const long long t0 = (long long) prob * tiles_per_prob;
+                for (int kb = 0; kb < prm.nkb; ++kb)
+                {
+                    if (!ptx::mbar_wait(&ctl->empty[stage], phase ^ 1,
+                            prm.err, 41, abort))
+                        break;
+                    uint8_t* dst = smem + (size_t) stage * kPI8StageBytes;
+                    if (rank == 0)
+                        ptx::mbar_arrive_expect_tx(&ctl->full[stage],
+                                2 * kPI8StageBytes);
+                    const uint32_t bar = full0 +
+                            (uint32_t) (stage * sizeof(uint64_t));
+                    ptx::tma_load_3d_pair(dst, &tmap_a, 0, 0, (int) (t0 +
+                            3 * ((long long) rb * prm.nkb + kb)), bar);
+                    ptx::tma_load_3d_pair(dst + kI8Block, &tmap_b, 0,
+                            64 * (int) rank, (int) (t0 +
+                            3 * ((long long) cb * prm.nkb + kb)), bar);
+                    issued |= 1u << stage;
+                    issued_par = (issued_par & ~(1u << stage)) |
+                            (phase << stage);
+                    if (++stage == kPI8Stages) { stage = 0; phase ^= 1; }
+                }
+            }
+            // the even CTA's full barrier counts both CTAs' copies: its
+            // producer waits for every stage's last phase before the CTAs
+            // can leave
+            if (rank == 0)
+                for (int s = 0; s < kPI8Stages; ++s)
+                    if ((issued >> s) & 1)
+                        ptx::mbar_wait(&ctl->full[s], (issued_par >> s) & 1,
+                                prm.err, 42, abort);
+        }
+        __syncwarp();
+    }
+    else if (warp == 1)
+    {
+        if (lane == 0 && rank == 0)
+        {
+            // ---------------- MMA issuer (even CTA only)
+            const uint32_t idesc = ptx::idesc_s8_s32(256, 128);
+            const uint32_t d0 = tmem, d1 = tmem + 128, d2 = tmem + 256,
+                    d3 = tmem + 384;
+            int stage = 0;
+            uint32_t phase = 0, dpar = 0;
+            bool ok = true;
+            for (int task = pair; task < ntasks && ok; task += npairs)
+            {
+                for (int ch = 0; ch < nchunk && ok; ++ch)
+                {
+                    if (!ptx::mbar_wait_cluster(&ctl->dempty, dpar ^ 1,
+                            prm.err, 43, abort))
+                    {
+                        ok = false;
+                        break;
+                    }
+                    ptx::tc_fence_after();
+                    const int kb0 = ch * kI8DrainKb;
+                    const int kb1 = min(prm.nkb, kb0 + kI8DrainKb);
+                    for (int kb = kb0; kb < kb1; ++kb)
+                    {
+                        if (!ptx::mbar_wait_cluster(&ctl->full[stage], phase,
+                                prm.err, 44, abort))
+                        {
+                            ok = false;
+                            break;
+                        }
+                        ptx::tc_fence_after();
+                        const uint32_t a = ptx::smem_u32(smem +
+                                (size_t) stage * kPI8StageBytes);
+                        const uint32_t b = a + kI8Block;
+#pragma unroll
+                        for (int k = 0; k < 2; ++k)
+                        {
+                            const uint64_t a0 = ptx::sdesc_sw64(a + 32 * k);
+                            const uint64_t a1 = ptx::sdesc_sw64(
+                                    a + kI8Tile + 32 * k);
+                            const uint64_t a2 = ptx::sdesc_sw64(
+                                    a + 2 * kI8Tile + 32 * k);
+                            const uint64_t b0 = ptx::sdesc_sw64(b + 32 * k);
+                            const uint64_t b1 = ptx::sdesc_sw64(
+                                    b + 4096 + 32 * k);
+                            const uint64_t b2 = ptx::sdesc_sw64(
+                                    b + 8192 + 32 * k);
+                            const uint32_t acc =
+                                    (kb > kb0 || k > 0) ? 1u : 0u;
+                            ptx::mma_i8_pair(d0, a0, b0, idesc, acc);
+                            ptx::mma_i8_pair(d1, a0, b1, idesc, acc);
+                            ptx::mma_i8_pair(d1, a1, b0, idesc, 1u);
+                            ptx::mma_i8_pair(d2, a0, b2, idesc, acc);
+                            ptx::mma_i8_pair(d2, a1, b1, idesc, 1u);
+                            ptx::mma_i8_pair(d2, a2, b0, idesc, 1u);
+                            ptx::mma_i8_pair(d3, a1, b2, idesc, acc);
+                            ptx::mma_i8_pair(d3, a2, b1, idesc, 1u);
+                        }
+                        ptx::mma_commit_pair(&ctl->empty[stage]);
+                        if (++stage == kPI8Stages) { stage = 0; phase ^= 1; }
+                    }
+                    if (!ok) break;
+                    ptx::mma_commit_pair(&ctl->dfull);
+                    dpar ^= 1;
+                }
+            }
+            // every tcgen05 instruction of this kernel is cta_group::2
+            ptx::mma_commit_pair(&ctl->done);
+            ptx::mbar_wait(&ctl->done, 0, prm.err, 45, abort);
+        }
+        __syncwarp();
+    }
+    else
+    {
+        // ---------------- epilogue: 8 warps, 64 columns each
+        const int q4 = warp & 3;          // TMEM lane quadrant of this warp
+        const int h = (warp - 2) >> 2;    // column half
+        const int row = 32 * q4 + lane;   // row of this CTA's 128
+        const int c = row & 1;
+        const uint32_t taddr = tmem + ((uint32_t) (32 * q4) << 16) +
+                (uint32_t) (64 * h);
+        const uint32_t dempty0 = ptx::mapa_shared(
+                ptx::smem_u32(&ctl->dempty), 0);
+        uint32_t dpar = 0;
+        bool ok = true;
+        for (int task = pair; task < ntasks && ok; task += npairs)
+        {
+            const int prob = task / ntile;
+            int ti, cb;
+            pair_i8_tile_of(task - prob * ntile, prm.nrb, ti, cb);
+            double accR[16], accI[16];
+#pragma unroll
+            for (int j = 0; j < 16; ++j) accR[j] = accI[j] = 0.0;
+            for (int ch = 0; ch < nchunk; ++ch)
+            {
+                if (!ptx::mbar_wait(&ctl->dfull, dpar, prm.err, 46, abort))
+                {
+                    ok = false;
+                    break;
+                }
+                ptx::tc_fence_after();
+                i8_drain64(taddr, c, accR, accI);
+                ptx::tc_fence_before();
+                __syncwarp();
+                if (lane == 0) ptx::mbar_arrive_cluster(dempty0);
+                dpar ^= 1;
+            }
+            if (!ok) break;
+            const int g = prm.prob0 + prob;
+            const double q = (double) i8_scale_from_bits(
+                    prm.maxabs_bits[prm.maxabs_stride * g]);
+            square_task_store(prm, accR, accI, 65536.0 / (q * q), row, h,
+                    prob, 2 * ti + (int) rank, cb);
+        }
+    }
+
+    ptx::tc_fence_before();
+    // no CTA leaves (or frees TMEM) while its peer may still arrive on its
+    // barriers or its MMAs read the other's shared memory
+    ptx::cluster_sync();
+    ptx::tc_fence_after();
+    if (warp == 1) ptx::tmem_dealloc_pair(tmem, kI8TmemCols);
 }
 
 }  // namespace tc
@@ -1935,7 +2222,10 @@ int device_setup(bool& wide_fits, bool& pair_fits)
                 (int) gemm_pair_smem_bytes()) != cudaSuccess ||
                 cudaFuncSetAttribute(gemm_i8_kernel,
                 cudaFuncAttributeMaxDynamicSharedMemorySize,
-                (int) gemm_i8_smem_bytes()) != cudaSuccess)
+                (int) gemm_i8_smem_bytes()) != cudaSuccess ||
+                cudaFuncSetAttribute(gemm_pair_i8_kernel,
+                cudaFuncAttributeMaxDynamicSharedMemorySize,
+                (int) gemm_pair_i8_smem_bytes()) != cudaSuccess)
         {
             set_last_error("tc gemm attributes", cudaGetLastError());
             return OSKB_ERR_KERNEL_LAUNCH_FAILURE;
@@ -2011,9 +2301,53 @@ int launch_gemm(GemmParams& gp, cudaStream_t stream)
             gp.num_problems;
     if (gp.i8)
     {
+        // square tiles; CTA pairs on request (OSKB_TC_PAIR=1): at 512
+        // stations x 100,000 sources x 16 channels on one B200 the pairs
+        // took 41.4 ms per launch against 38.6 ms for the square tiles (the
+        // same bits: the sums are exact)
+        const long long pair_n = (long long) pair_i8_tiles(gp.nrb) *
+                gp.num_problems;
+        const char* pe = getenv("OSKB_TC_PAIR");
+        const bool use_pair = pe && atoi(pe) != 0;
+        g_last_arith.store(8);
+        if (use_pair)
+        {
+            const size_t bytes = gp.image_stride ?
+                    gp.image_stride * (size_t) gp.num_problems :
+                    (size_t) gp.nrb * gp.nkb * kI8Block;
+            CUtensorMap ta, tb;
+            const cuuint64_t gdim[3] = {8, 128, bytes / kI8Tile};
+            const cuuint64_t gstride[2] = {64, kI8Tile};
+            const cuuint32_t box_a[3] = {8, 128, 3};
+            const cuuint32_t box_b[3] = {8, 64, 3};
+            const cuuint32_t estride[3] = {1, 1, 1};
+            EncodeTiledFn encode = encode_tiled_fn();
+            if (!encode || bytes / kI8Tile >= (1ull << 31) ||
+                    encode(&ta, CU_TENSOR_MAP_DATA_TYPE_UINT64, 3,
+                    (void*) gp.W, gdim, gstride, box_a, estride,
+                    CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                    CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                    CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS ||
+                    encode(&tb, CU_TENSOR_MAP_DATA_TYPE_UINT64, 3,
+                    (void*) gp.W, gdim, gstride, box_b, estride,
+                    CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                    CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                    CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
+            {
+                set_last_error_msg("tc: integer operand tensor maps");
+                return OSKB_ERR_KERNEL_LAUNCH_FAILURE;
+            }
+            const int pairs = num_sms() / 2;
+            const int grid = 2 * (int) (pair_n < pairs ? pair_n : pairs);
+            g_last_tile.store(256);
+            cudaEvent_t ev_stop = timing_start(stream);
+            gemm_pair_i8_kernel<<<grid, kGemmThreads,
+                    gemm_pair_i8_smem_bytes(), stream>>>(gp, ta, tb);
+            if (ev_stop) cudaEventRecord(ev_stop, stream);
+            return check_launch("tc gemm (integer, pairs)");
+        }
         const int grid = (int) (square < num_sms() ? square : num_sms());
         g_last_tile.store(128);
-        g_last_arith.store(8);
         cudaEvent_t ev_stop = timing_start(stream);
         gemm_i8_kernel<<<grid, kGemmThreads, gemm_i8_smem_bytes(), stream>>>(
                 gp);

@@ -1,10 +1,14 @@
 """GPU parity of the tensor-core compensated cross-correlation.
 
-The tensor-core form (FP16 hi/lo split, three products, FP32 accumulation
-drained to FP64, FP64 phase) must agree with the FP64 CPU oracle to
+Both tensor-core forms must agree with the FP64 CPU oracle to
     L2 relative <= 1e-6  and  max |err| <= 1e-6 * max |V|
-on every test here (the stated tolerance of the compensated path). Calls go
-through the C ABI with torch device buffers.
+on every test here (the stated tolerance of the compensated path):
+  - the integer form (the default): entries as 24-bit fixed point in three
+    signed 8-bit limbs, eight 8-bit MMAs per K step into exact 32-bit
+    integer accumulators, FP64 phase;
+  - the FP16 form (OSKB_TC_ARITH=fp16 or any OSKB_TC_TILE): FP16 hi/lo
+    split, three products, FP32 accumulation drained to FP64, FP64 phase.
+Calls go through the C ABI with torch device buffers.
 """
 import numpy as np
 import pytest
@@ -90,16 +94,36 @@ def test_tc_jones_api(nst, nsrc, casa):
     assert flags[0] == 0 and flags[1] == 0
 
 
-@pytest.mark.parametrize("tile", [128, 256, 512])
+FORMS = ["fp16-128", "fp16-256", "fp16-512", "i8-128", "i8-pair"]
+
+
+def set_form(monkeypatch, form):
+    """Selects a contraction form; returns the (tile columns, arithmetic)
+    that oskb_tc_tile_columns / oskb_tc_arithmetic then report."""
+    if form.startswith("fp16"):
+        tile = int(form.split("-")[1])
+        monkeypatch.setenv("OSKB_TC_TILE", str(tile))
+        monkeypatch.delenv("OSKB_TC_PAIR", raising=False)
+        return tile, 16
+    monkeypatch.delenv("OSKB_TC_TILE", raising=False)
+    monkeypatch.delenv("OSKB_TC_ARITH", raising=False)
+    pair = form == "i8-pair"
+    monkeypatch.setenv("OSKB_TC_PAIR", "1" if pair else "0")
+    return (256 if pair else 128), 8
+
+
+@pytest.mark.parametrize("form", FORMS)
 @pytest.mark.parametrize("nst,nsrc,casa", [(17, 300, 0), (64, 1000, 1),
                                            (130, 777, 0), (161, 2050, 1),
                                            (200, 1200, 0)])
-def test_tc_tile_widths(tile, nst, nsrc, casa, monkeypatch):
+def test_tc_tile_widths(form, nst, nsrc, casa, monkeypatch):
     """Square (128 x 128), wide (128 x 256) and pair (256 x 256 on two CTAs)
     contraction tiles, with an even and an odd number of 32-station row
     blocks (17, 64, 130, 161 and 200 stations: one, two, five, six and
-    seven blocks), against the oracle."""
-    monkeypatch.setenv("OSKB_TC_TILE", str(tile))
+    seven blocks), against the oracle; and the integer form on square
+    tiles and on 256 x 128 tiles of CTA pairs (an odd number of row blocks
+    leaves the last pair's second half empty)."""
+    tile, arith = set_form(monkeypatch, form)
     rng = np.random.default_rng(nst * 7 + nsrc)
     l, m, n, I, Q, U, V = sky(rng, nsrc)
     u, v, w = stations(rng, nst)
@@ -117,6 +141,7 @@ def test_tc_tile_widths(tile, nst, nsrc, casa, monkeypatch):
             None, 0, ob.stream_ptr())
     torch.cuda.synchronize()
     assert ob.load().oskb_tc_tile_columns() == tile
+    assert ob.load().oskb_tc_arithmetic() == arith
     l2, mx = errors(vis.cpu().numpy(), ref)
     assert l2 <= TOL and mx <= TOL, (l2, mx)
     flags = (ob._lib.ctypes.c_int * 2)()
@@ -256,13 +281,13 @@ def test_tc_block_small_workspace_groups():
     assert np.array_equal(out[0], out[1])
 
 
-@pytest.mark.parametrize("tile", [128, 256, 512])
-def test_tc_block_auto_correlations_fused(tile, monkeypatch):
+@pytest.mark.parametrize("form", FORMS)
+def test_tc_block_auto_correlations_fused(form, monkeypatch):
     """Auto-correlations from the same contraction (the diagonal station
     pairs of the diagonal tiles) against the oracle's auto-correlation of
     J = K E per (dump, channel), to the compensated tolerance; the cross
     visibilities are the same bits as without them."""
-    monkeypatch.setenv("OSKB_TC_TILE", str(tile))
+    tile, arith = set_form(monkeypatch, form)
     rng = np.random.default_rng(21)
     nst, nsrc, ntime, nchan = 97, 700, 2, 2
     l, m, n, I, Q, U, V = sky(rng, nsrc)
@@ -287,6 +312,7 @@ def test_tc_block_auto_correlations_fused(tile, monkeypatch):
             vis0, None, 0, ob.stream_ptr())
     torch.cuda.synchronize()
     assert ob.load().oskb_tc_tile_columns() == tile
+    assert ob.load().oskb_tc_arithmetic() == arith
     assert torch.equal(vis, vis0)
     got = autos.cpu().numpy().reshape(ntime, nchan, -1)
     Ed = E32.astype(np.float64).ravel()
