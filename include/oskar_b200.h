@@ -1114,7 +1114,7 @@ OSKB_API int oskb_tc_status(const void* workspace, int* flags,
 OSKB_API int oskb_tc_tile_columns(void);
 /* Arithmetic of the last tensor-core contraction launched, 0 before the
  * first: 8 for the default integer form (each scaled entry a 24-bit fixed-
- * point integer held as three signed 8-bit limbs, eight 8-bit tcgen05 MMAs
+ * point integer held as three 8-bit limbs, eight 8-bit tcgen05 MMAs
  * per K step into exact S32 accumulators, square tiles), 16 for the FP16
  * hi/lo form (three FP16 MMAs per K step into FP32 accumulators drained to
  * FP64), which OSKB_TC_ARITH=fp16, or any OSKB_TC_TILE setting, selects. */

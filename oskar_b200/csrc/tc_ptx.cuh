@@ -94,6 +94,42 @@ __device__ __forceinline__ void bulk_g2s(void* dst_smem, const void* src,
                     "r"(smem_u32(bar)) : "memory");
 }
 
+// ---- bulk copy shared -> global (TMA engine, non-tensor form), bulk-group
+// completion. Both addresses 16-byte aligned, bytes a multiple of 16.
+// Shared-memory writes by threads must be made visible to the copy first
+// (fence_proxy_async_smem by the writing threads, then a block barrier).
+__device__ __forceinline__ void fence_proxy_async_smem()
+{
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+
+__device__ __forceinline__ void bulk_s2g(void* dst, const void* src_smem,
+        uint32_t bytes)
+{
+    asm volatile("cp.async.bulk.global.shared::cta.bulk_group [%0], [%1], %2;"
+                 :: "l"(dst), "r"(smem_u32(src_smem)), "r"(bytes)
+                 : "memory");
+}
+
+__device__ __forceinline__ void bulk_commit()
+{
+    asm volatile("cp.async.bulk.commit_group;" ::: "memory");
+}
+
+// Waits until at most N committed bulk groups still read shared memory.
+template <int N>
+__device__ __forceinline__ void bulk_wait_read()
+{
+    asm volatile("cp.async.bulk.wait_group.read %0;" :: "n"(N) : "memory");
+}
+
+// Waits until at most N committed bulk groups are incomplete.
+template <int N>
+__device__ __forceinline__ void bulk_wait()
+{
+    asm volatile("cp.async.bulk.wait_group %0;" :: "n"(N) : "memory");
+}
+
 // ---- tcgen05: TMEM allocation (whole warp), MMA, commit, loads, fences
 __device__ __forceinline__ void tmem_alloc(uint32_t* dst_smem, uint32_t ncols)
 {
@@ -131,8 +167,9 @@ __device__ __forceinline__ void mma_f16(uint32_t d_tmem, uint64_t a_desc,
                     "r"(accumulate) : "memory");
 }
 
-// D (S32, TMEM) (+)= A B^T for signed 8-bit A and B (K = 32 per instruction,
-// both K-major in shared memory), no output lanes disabled.
+// D (S32, TMEM) (+)= A B^T for 8-bit A and B (signedness in the instruction
+// descriptor; K = 32 per instruction, both K-major in shared memory), no
+// output lanes disabled.
 __device__ __forceinline__ void mma_i8(uint32_t d_tmem, uint64_t a_desc,
         uint64_t b_desc, uint32_t idesc, uint32_t accumulate)
 {
@@ -357,7 +394,7 @@ __device__ __forceinline__ void mma_f16_pair(uint32_t d_tmem, uint64_t a_desc,
                     "r"(accumulate) : "memory");
 }
 
-// Pair MMA of kind::i8 (signed 8-bit A and B, S32 accumulator): A rows
+// Pair MMA of kind::i8 (8-bit A and B, S32 accumulator): A rows
 // 0-127 from the even CTA's shared memory and 128-255 from the odd one's,
 // B columns 0 .. N/2-1 from the even CTA's and N/2 .. N-1 from the odd
 // one's, at the same offsets; no output lanes disabled.
@@ -390,12 +427,14 @@ __host__ __device__ constexpr uint32_t idesc_f16_f32(int m, int n)
            ((uint32_t) (m >> 4) << 24);
 }
 
-// Instruction descriptor of kind::i8: S32 accumulator (bits 4-5 = 2),
-// signed 8-bit A and B (bits 7-9 and 10-12 = 1), both K-major, N / 8 at bit
-// 17, M / 16 at bit 24.
-__host__ __device__ constexpr uint32_t idesc_s8_s32(int m, int n)
+// Instruction descriptor of kind::i8: S32 accumulator (bits 4-5 = 2), A and
+// B 8-bit, signed (1) or unsigned (0) at bits 7-9 and 10-12, both K-major,
+// N / 8 at bit 17, M / 16 at bit 24.
+__host__ __device__ constexpr uint32_t idesc_i8_s32(int m, int n,
+        bool a_signed, bool b_signed)
 {
-    return (2u << 4) | (1u << 7) | (1u << 10) |
+    return (2u << 4) | ((a_signed ? 1u : 0u) << 7) |
+           ((b_signed ? 1u : 0u) << 10) |
            ((uint32_t) (n >> 3) << 17) | ((uint32_t) (m >> 4) << 24);
 }
 

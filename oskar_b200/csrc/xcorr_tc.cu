@@ -68,10 +68,13 @@ __device__ __forceinline__ float scale_from_bits(unsigned int bits)
 
 // Integer operand image (the default contraction): every entry x is the
 // fixed-point integer a = round(x q), |a| <= 127 * 2^16 (plus rounding),
-// held as three signed 8-bit limbs a = a0 2^16 + a1 2^8 + a2 with a1 and a2
-// in [-128, 127] (so a0 stays in [-127, 127]). Per 32-station x 32-source
-// block: three limb tiles of 128 rows x 64 bytes (one byte per K column),
-// stored with the 64-byte swizzle.
+// held as three signed 8-bit limbs a = a0 2^16 + a1 2^8 + a2 with a1, a2
+// in [-128, 127] (balanced digits, so that the left-out product a2 b2 has
+// no bias). They are the bytes of t = a + 0x8080 with the two low bytes'
+// top bits flipped: t = a0 2^16 + (a1 + 128) 2^8 + (a2 + 128), and
+// a0 = t >> 16 stays in [-127, 127]. Per 32-station x 32-source block:
+// three limb tiles of 128 rows x 64 bytes (one byte per K column), stored
+// with the 64-byte swizzle.
 constexpr int kI8Tile = 128 * 64;
 constexpr int kI8Block = 3 * kI8Tile;
 constexpr float kI8Target = 8323072.0f;      // 127 * 2^16
@@ -98,18 +101,6 @@ __device__ __forceinline__ uint32_t swz64_offset(int r, int c)
                        (c & 15));
 }
 
-// The three limbs of round(x q), packed as bytes 0 (a0), 1 (a1), 2 (a2).
-__device__ __forceinline__ uint32_t i8_limbs(float xq)
-{
-    const int a = __float2int_rn(xq);
-    const int a2 = ((a & 0xff) ^ 0x80) - 0x80;
-    const int r = (a - a2) >> 8;
-    const int a1 = ((r & 0xff) ^ 0x80) - 0x80;
-    const int a0 = (r - a1) >> 8;
-    return (uint32_t) (a0 & 0xff) | ((uint32_t) (a1 & 0xff) << 8) |
-           ((uint32_t) (a2 & 0xff) << 16);
-}
-
 // Writes one station-source's 2x2 A (already scaled by q) as 4 rows of the
 // three limb tiles of its block.
 __device__ __forceinline__ void store_entry_i8(uint8_t* block, int pl,
@@ -121,14 +112,17 @@ __device__ __forceinline__ void store_entry_i8(uint8_t* block, int pl,
         for (int c = 0; c < 2; ++c)
         {
             const int r = 4 * pl + 2 * i + c;
-            const uint32_t l0 = i8_limbs(A[i][0][c]);
-            const uint32_t l1 = i8_limbs(A[i][1][c]);
+            const int t0 = __float2int_rn(A[i][0][c]) + 0x8080;
+            const int t1 = __float2int_rn(A[i][1][c]) + 0x8080;
             const uint32_t off = swz64_offset(r, 2 * sl);
+            // limb k of both K columns: byte 2 - k of each t, the low limbs
+            // with their top bit flipped
 #pragma unroll
             for (int limb = 0; limb < 3; ++limb)
                 *reinterpret_cast<uint16_t*>(block + limb * kI8Tile + off) =
-                        (uint16_t) (((l0 >> (8 * limb)) & 0xff) |
-                                    (((l1 >> (8 * limb)) & 0xff) << 8));
+                        (uint16_t) (__byte_perm(t0, t1,
+                                (2 - limb) | ((6 - limb) << 4)) ^
+                                (limb ? 0x8080u : 0u));
         }
 }
 
@@ -323,7 +317,7 @@ __global__ void __launch_bounds__(256) prep_jones_kernel(
 // reading E and forming E C once per station-source for all of them.
 // grid (k blocks, row blocks); 8 warps, warp = 4 stations, lane = source.
 // ---------------------------------------------------------------------------
-template <typename TE, bool I8>
+template <typename TE>
 __global__ void __launch_bounds__(256) prep_fused_kernel(
         const TE* __restrict__ E, int num_src, int num_st,
         const double* __restrict__ l, const double* __restrict__ m,
@@ -346,10 +340,8 @@ __global__ void __launch_bounds__(256) prep_fused_kernel(
         brightness_factor(I[s], Q[s], U[s], V[s], c11, c21r, c21i, c22);
         sl = l[s]; sm = m[s]; sn1 = n[s] - 1.0;
     }
-    const float S = I8 ? i8_scale_from_bits(*maxabs_bits)
-                       : scale_from_bits(*maxabs_bits);
-    uint8_t* tile0 = W + (size_t) (rb * nkb + kb) *
-            (I8 ? kI8Block : kPairBytes);
+    const float S = scale_from_bits(*maxabs_bits);
+    uint8_t* tile0 = W + (size_t) (rb * nkb + kb) * kPairBytes;
     for (int pl = warp; pl < kStPerBlock; pl += 8)
     {
         const int p = rb * kStPerBlock + pl;
@@ -386,13 +378,111 @@ __global__ void __launch_bounds__(256) prep_fused_kernel(
                         A[i][kk][1] = re * sn + im * cs;
                     }
             }
-            if constexpr (I8)
-                store_entry_i8(tile0 + (size_t) j * image_stride, pl, lane,
-                        A);
-            else
-                store_entry(tile0 + (size_t) j * image_stride, pl, lane, A);
+            store_entry(tile0 + (size_t) j * image_stride, pl, lane, A);
         }
     }
+}
+
+// ---------------------------------------------------------------------------
+// Integer form of prep_fused_kernel: the same A = K (E C) per station-source
+// and problem, written as the three limb tiles of the block. Each block of
+// one problem (24 KB, contiguous in the image) is assembled in shared memory
+// and leaves with one bulk copy, double-buffered so that the copy of one
+// problem's block overlaps forming the next. A thread keeps E C of its four
+// stations (8 values each) in registers across the problems.
+// grid (k blocks, row blocks); 8 warps, warp = 4 stations, lane = source.
+// ---------------------------------------------------------------------------
+template <typename TE>
+__global__ void __launch_bounds__(256) prep_fused_i8_kernel(
+        const TE* __restrict__ E, int num_src, int num_st,
+        const double* __restrict__ l, const double* __restrict__ m,
+        const double* __restrict__ n, const double* __restrict__ I,
+        const double* __restrict__ Q, const double* __restrict__ U,
+        const double* __restrict__ V, const double* __restrict__ uvw,
+        const double* __restrict__ inv_wavelength, int nch, int p0, int np,
+        const unsigned int* __restrict__ maxabs_bits, uint8_t* W,
+        size_t image_stride)
+{
+    // two blocks: the 48 KB of static shared memory a kernel may declare
+    __shared__ __align__(128) uint8_t buf[2 * kI8Block];
+    const int kb = blockIdx.x, rb = blockIdx.y;
+    const int nkb = gridDim.x;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int s = kb * kSrcPerBlock + lane;
+    const bool src_ok = s < num_src;
+    float c11 = 0, c21r = 0, c21i = 0, c22 = 0;
+    double sl = 0, sm = 0, sn1 = 0;
+    if (src_ok)
+    {
+        brightness_factor(I[s], Q[s], U[s], V[s], c11, c21r, c21i, c22);
+        sl = l[s]; sm = m[s]; sn1 = n[s] - 1.0;
+    }
+    const float q = i8_scale_from_bits(*maxabs_bits);
+    float A0[4][2][2][2];
+#pragma unroll
+    for (int k = 0; k < 4; ++k)
+    {
+        const int p = rb * kStPerBlock + warp + 8 * k;
+        float* a = &A0[k][0][0][0];
+#pragma unroll
+        for (int e = 0; e < 8; ++e) a[e] = 0.0f;
+        if (src_ok && p < num_st)
+        {
+            float J[8];
+            load_jones<TE>(E + 8 * ((size_t) p * num_src + s), J);
+            apply_factor(J, c11, c21r, c21i, c22, A0[k]);
+#pragma unroll
+            for (int e = 0; e < 8; ++e) a[e] *= q;
+        }
+    }
+    uint8_t* dst0 = W + (size_t) (rb * nkb + kb) * kI8Block;
+    for (int j = 0; j < np; ++j)
+    {
+        uint8_t* b = buf + (size_t) (j & 1) * kI8Block;
+        if (j >= 2)
+        {
+            // the copy that read this buffer (problem j - 2) is done
+            if (threadIdx.x == 0) ptx::bulk_wait_read<1>();
+            __syncthreads();
+        }
+        const int prob = p0 + j, t = prob / nch, c = prob - t * nch;
+        const double* pu = uvw + (size_t) t * 3 * num_st;
+#pragma unroll
+        for (int k = 0; k < 4; ++k)
+        {
+            const int pl = warp + 8 * k;
+            const int p = rb * kStPerBlock + pl;
+            float A[2][2][2] = {{{0, 0}, {0, 0}}, {{0, 0}, {0, 0}}};
+            if (src_ok && p < num_st)
+            {
+                const double x = (pu[p] * sl + pu[num_st + p] * sm +
+                                  pu[2 * num_st + p] * sn1) *
+                                 inv_wavelength[c];
+                const float f = (float) (x - rint(x));
+                float sn, cs;
+                sincospif(2.0f * f, &sn, &cs);
+#pragma unroll
+                for (int i = 0; i < 2; ++i)
+#pragma unroll
+                    for (int kk = 0; kk < 2; ++kk)
+                    {
+                        const float re = A0[k][i][kk][0];
+                        const float im = A0[k][i][kk][1];
+                        A[i][kk][0] = re * cs - im * sn;
+                        A[i][kk][1] = re * sn + im * cs;
+                    }
+            }
+            store_entry_i8(b, pl, lane, A);
+        }
+        ptx::fence_proxy_async_smem();
+        __syncthreads();
+        if (threadIdx.x == 0)
+        {
+            ptx::bulk_s2g(dst0 + (size_t) j * image_stride, b, kI8Block);
+            ptx::bulk_commit();
+        }
+    }
+    if (threadIdx.x == 0) ptx::bulk_wait<0>();
 }
 
 }  // namespace tc
@@ -1481,19 +1571,19 @@ gemm_pair_kernel(const GemmParams prm, const __grid_constant__ CUtensorMap tmap)
 
 // ===========================================================================
 // Integer contraction (the default): G = W W^T from the three-limb 8-bit
-// image on the tcgen05 integer path. With a = a0 2^16 + a1 2^8 + a2 and b
-// likewise,
+// image on the tcgen05 integer path (signed 8-bit MMAs). With
+// a = a0 2^16 + a1 2^8 + a2 and b likewise,
 //     a b / 2^16 = a0 b0 2^16 + (a0 b1 + a1 b0) 2^8 + (a0 b2 + a1 b1 + a2 b0)
 //                  + (a1 b2 + a2 b1) 2^-8 + a2 b2 2^-16,
-// the last term (at most 2^-32 of the largest product) left out: eight
-// 8-bit MMAs per 32-wide K step feed four S32 TMEM accumulators (D0 .. D3,
-// 128 columns each) of 128 x 128 tiles. The class a1 b2 + a2 b1 cannot be
+// the last term (at most 2^-32 of the largest product, mean zero) left out:
+// eight 8-bit MMAs per 32-wide K step feed four S32 TMEM accumulators (D0 ..
+// D3, 128 columns each) of 128 x 128 tiles. The class a1 b2 + a2 b1 cannot be
 // left out too: its limbs are uniform digits whatever the entry's size, so
 // over many faint sources it would add ~1e-6 of the visibilities' L2 norm.
 // The integer sums are exact: no rounding happens in the tensor core, so
 // the accumulators only need draining before they could overflow (every
-// kI8DrainKb k blocks; one k block adds at most 3 x 64 x 2^14 < 2^21.6 to
-// D2) and at the end of a task, where D0 2^16 + D1 2^8 + D2 + D3 2^-8 is
+// kI8DrainKb k blocks: one k block adds at most 3 x 64 x 2^14 < 2^21.6 to
+// |D2|, so 512 blocks stay below 2^31) and at the end of a task, where D0 2^16 + D1 2^8 + D2 + D3 2^-8 is
 // formed in FP64 and folded into the visibility sums. The error is that of
 // the fixed-point entries (2^-24 of the largest |entry|).
 // Warp roles (320 threads): warp 0 producer (one bulk copy per operand per
@@ -1641,7 +1731,7 @@ gemm_i8_kernel(const GemmParams prm)
         if (lane == 0)
         {
             // ---------------- MMA issuer
-            const uint32_t idesc = ptx::idesc_s8_s32(128, 128);
+            const uint32_t idesc = ptx::idesc_i8_s32(128, 128, true, true);
             const uint32_t d0 = tmem, d1 = tmem + 128, d2 = tmem + 256,
                     d3 = tmem + 384;
             int stage = 0;
@@ -1923,7 +2013,7 @@ gemm_pair_i8_kernel(const GemmParams prm,
         if (lane == 0 && rank == 0)
         {
             // ---------------- MMA issuer (even CTA only)
-            const uint32_t idesc = ptx::idesc_s8_s32(256, 128);
+            const uint32_t idesc = ptx::idesc_i8_s32(256, 128, true, true);
             const uint32_t d0 = tmem, d1 = tmem + 128, d2 = tmem + 256,
                     d3 = tmem + 384;
             int stage = 0;
@@ -2589,12 +2679,12 @@ int correlate_block(int casa, int num_sources, int num_stations,
     {
         const int np = min(group, num_problems - p0);
         if (i8)
-            prep_fused_kernel<TE, true><<<dim3(nkb, nrb), 256, 0, s>>>(E,
-                    num_sources, num_stations, l, m, n, I, Q, U, V,
-                    station_uvw, inv_wavelength, num_channels, p0, np,
-                    &hdr->maxabs_bits, W, img);
+            prep_fused_i8_kernel<TE><<<dim3(nkb, nrb), 256, 0, s>>>(E,
+                    num_sources, num_stations,
+                    l, m, n, I, Q, U, V, station_uvw, inv_wavelength,
+                    num_channels, p0, np, &hdr->maxabs_bits, W, img);
         else
-            prep_fused_kernel<TE, false><<<dim3(nkb, nrb), 256, 0, s>>>(E,
+            prep_fused_kernel<TE><<<dim3(nkb, nrb), 256, 0, s>>>(E,
                     num_sources, num_stations, l, m, n, I, Q, U, V,
                     station_uvw, inv_wavelength, num_channels, p0, np,
                     &hdr->maxabs_bits, W, img);
