@@ -182,6 +182,36 @@ __device__ __forceinline__ void mma_i8(uint32_t d_tmem, uint64_t a_desc,
                  : "memory");
 }
 
+// mma_i8 with the A operand kept in the tensor core's collector buffer for
+// the next MMAs of the same A: Use = 0 reads A and fills the buffer, 1 reuses
+// it, 2 reuses it for the last time.
+template <int Use>
+__device__ __forceinline__ void mma_i8_col(uint32_t d_tmem, uint64_t a_desc,
+        uint64_t b_desc, uint32_t idesc, uint32_t accumulate)
+{
+    if constexpr (Use == 0)
+        asm volatile("{\n\t.reg .pred p;\n\t"
+                     "setp.ne.b32 p, %4, 0;\n\t"
+                     "tcgen05.mma.cta_group::1.kind::i8.collector::a::fill "
+                     "[%0], %1, %2, %3, p;\n\t}"
+                     :: "r"(d_tmem), "l"(a_desc), "l"(b_desc), "r"(idesc),
+                        "r"(accumulate) : "memory");
+    else if constexpr (Use == 1)
+        asm volatile("{\n\t.reg .pred p;\n\t"
+                     "setp.ne.b32 p, %4, 0;\n\t"
+                     "tcgen05.mma.cta_group::1.kind::i8.collector::a::use "
+                     "[%0], %1, %2, %3, p;\n\t}"
+                     :: "r"(d_tmem), "l"(a_desc), "l"(b_desc), "r"(idesc),
+                        "r"(accumulate) : "memory");
+    else
+        asm volatile("{\n\t.reg .pred p;\n\t"
+                     "setp.ne.b32 p, %4, 0;\n\t"
+                     "tcgen05.mma.cta_group::1.kind::i8.collector::a::lastuse "
+                     "[%0], %1, %2, %3, p;\n\t}"
+                     :: "r"(d_tmem), "l"(a_desc), "l"(b_desc), "r"(idesc),
+                        "r"(accumulate) : "memory");
+}
+
 // Arrives on an mbarrier once all previously issued MMAs have completed.
 __device__ __forceinline__ void mma_commit(uint64_t* bar)
 {

@@ -1783,14 +1783,17 @@ gemm_i8_kernel(const GemmParams prm)
                                     b + 2 * kI8Tile + 32 * k);
                             const uint32_t acc =
                                     (kb > kb0 || k > 0) ? 1u : 0u;
-                            ptx::mma_i8(d0, a0, b0, idesc, acc);
-                            ptx::mma_i8(d1, a0, b1, idesc, acc);
-                            ptx::mma_i8(d1, a1, b0, idesc, 1u);
-                            ptx::mma_i8(d2, a0, b2, idesc, acc);
-                            ptx::mma_i8(d2, a1, b1, idesc, 1u);
-                            ptx::mma_i8(d2, a2, b0, idesc, 1u);
-                            ptx::mma_i8(d3, a1, b2, idesc, acc);
-                            ptx::mma_i8(d3, a2, b1, idesc, 1u);
+                            // grouped by A limb, A kept in the collector
+                            // buffer across its group; the first MMA into
+                            // each accumulator (program order) resets it
+                            ptx::mma_i8_col<0>(d0, a0, b0, idesc, acc);
+                            ptx::mma_i8_col<1>(d1, a0, b1, idesc, acc);
+                            ptx::mma_i8_col<2>(d2, a0, b2, idesc, acc);
+                            ptx::mma_i8_col<0>(d1, a1, b0, idesc, 1u);
+                            ptx::mma_i8_col<1>(d2, a1, b1, idesc, 1u);
+                            ptx::mma_i8_col<2>(d3, a1, b2, idesc, acc);
+                            ptx::mma_i8_col<0>(d2, a2, b0, idesc, 1u);
+                            ptx::mma_i8_col<2>(d3, a2, b1, idesc, 1u);
                         }
                         ptx::mma_commit(&ctl->empty[stage]);
                         if (++stage == kI8Stages) { stage = 0; phase ^= 1; }
