@@ -972,7 +972,17 @@ OSKB_API void oskb_block_plan_free(oskb_BlockPlan* plan);
  * group on a copy-out stream. So block b + 1's upload overlaps block b's
  * correlation. Host buffers must stay valid until oskb_tc_plan_wait (they
  * should be page-locked for the copies to overlap); the sky (l, m, n and
- * Stokes, host arrays) is uploaded once by oskb_tc_plan_set_sky. */
+ * Stokes, host arrays) is uploaded once by oskb_tc_plan_set_sky.
+ * The plan owns its contraction workspace (up to 16 problems' operand
+ * images, at most half the device memory free at creation). The first
+ * enqueue picks the contraction form by timing integer square tiles,
+ * integer CTA-pair tiles and FP16 wide tiles on its own block (it waits for
+ * them; environment OSKB_TC_PLAN_FORM = 1..5 fixes a form instead, 0 the
+ * library default; OSKB_TC_PLAN_TUNE=0 skips the timing); each slot's
+ * compute work is then captured into a CUDA graph at its first block and
+ * replayed for the later ones (OSKB_TC_PLAN_GRAPH=0: launched eagerly). The
+ * downloads stay outside the graph. No reference counterpart (the
+ * reference's block loop is oskar_interferometer_run_block.c:28-153). */
 typedef struct oskb_TcPlan oskb_TcPlan;
 OSKB_API oskb_TcPlan* oskb_tc_plan_create(int casa, int num_sources,
         int num_stations, int num_times, int num_channels,
@@ -985,6 +995,14 @@ OSKB_API int oskb_tc_plan_enqueue(oskb_TcPlan* plan, const float* E_host,
         const double* station_uvw_host, double* vis_host);
 OSKB_API int oskb_tc_plan_wait(oskb_TcPlan* plan);
 OSKB_API void oskb_tc_plan_free(oskb_TcPlan* plan);
+/* The plan's contraction form: 0 library default, 1 integer square tiles,
+ * 2 integer CTA-pair tiles, 3 FP16 square, 4 FP16 wide, 5 FP16 pairs. */
+OSKB_API int oskb_tc_plan_form(const oskb_TcPlan* plan);
+/* Graph replays so far (0 while the plan runs eagerly). */
+OSKB_API int oskb_tc_plan_graph_launches(const oskb_TcPlan* plan);
+/* The tuning times (ms) of forms 1, 2 and 4 on the first block, -1 where
+ * not timed. ms: host [3]. */
+OSKB_API int oskb_tc_plan_tuning_ms(const oskb_TcPlan* plan, double* ms);
 
 /* Fused block: for every (time t, channel c) of a block,
  *   vis[t][c] += sum_s (K_p E_p C)(s) (K_q E_q C)(s)^H

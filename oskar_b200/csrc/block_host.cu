@@ -7,8 +7,11 @@
 // computation). Device buffers are kept by the library per device and grown
 // on demand; with page-locked host buffers the copies run at full link
 // speed.
+#include <stdio.h>
+#include <stdlib.h>
 #include <string.h>
 
+#include <utility>
 #include <vector>
 
 #include "common.cuh"
@@ -187,7 +190,16 @@ extern "C" int oskb_run_block_tc_host(int casa, int num_sources,
 // Pipelined form: a plan with two slots of device buffers, so that the
 // upload of block b + 1 (on a copy-in stream) overlaps the correlation of
 // block b (compute stream), and block b's visibilities download group by
-// group on a copy-out stream. The sky is uploaded once per plan.
+// group on a copy-out stream. The sky is uploaded once per plan; the
+// contraction's workspace is the plan's own (one, as the compute stream
+// runs one block at a time).
+// The first block picks the contraction form by timing the candidates on
+// its own data (integer square tiles, integer CTA pairs, FP16 wide tiles);
+// each slot's compute work (clear, maxabs, per group prep + contraction) is
+// then captured once into a CUDA graph and replayed for every later block
+// of that slot; the downloads stay outside the graph (their host
+// destinations change) and wait on event nodes the graph records after
+// each group.
 // ---------------------------------------------------------------------------
 struct oskb_TcPlan
 {
@@ -195,14 +207,23 @@ struct oskb_TcPlan
     double uv_min, uv_max;
     size_t e_bytes, uvw_bytes, vis_bytes, problem_bytes;
     double *sky, *wl;
+    void* ws;
+    size_t ws_bytes;
+    int form;                    // contraction form in use (tc::Form)
+    bool tuned, use_graph;
+    double tune_ms[3];           // integer square, integer pairs, FP16 wide
+    int graph_launches;
     struct Slot
     {
         void *E, *uvw, *vis;
         cudaEvent_t uploaded, computed, downloaded;
         bool used;
+        cudaGraphExec_t exec;
+        std::vector<std::pair<int, int>> groups;   // (p0, np) of the graph
+        std::vector<cudaEvent_t> group_events;     // recorded by the graph
     } slot[2];
     cudaStream_t in, compute, out;
-    std::vector<cudaEvent_t> group_events;
+    std::vector<cudaEvent_t> group_events;   // the eager (non-graph) path
     size_t next_event;
     int next_slot;
     bool failed;
@@ -217,6 +238,7 @@ struct PlanHook
     double* host;
 };
 
+// Eager path: record an event after the group and download it at once.
 void plan_after_group(void* ctx, int p0, int np)
 {
     PlanHook& h = *static_cast<PlanHook*>(ctx);
@@ -243,6 +265,135 @@ void plan_after_group(void* ctx, int p0, int np)
         p->failed = true;
 }
 
+// Capture path: the graph records one event per group; the downloads are
+// enqueued after each replay.
+void plan_capture_group(void* ctx, int p0, int np)
+{
+    PlanHook& h = *static_cast<PlanHook*>(ctx);
+    oskb_TcPlan* p = h.p;
+    oskb_TcPlan::Slot& s = p->slot[h.slot];
+    const size_t g = s.groups.size();
+    // an external event-record node: waited on outside the graph
+    if (g >= s.group_events.size() ||
+            cudaEventRecordWithFlags(s.group_events[g], p->compute,
+            cudaEventRecordExternal) != cudaSuccess)
+    {
+        p->failed = true;
+        return;
+    }
+    s.groups.emplace_back(p0, np);
+}
+
+int plan_correlate(oskb_TcPlan* p, int k, int form,
+        void (*after)(void*, int, int), void* ctx)
+{
+    oskb_TcPlan::Slot& s = p->slot[k];
+    const double* sky = p->sky;
+    const size_t ns = p->num_src;
+    if (cudaMemsetAsync(s.vis, 0, p->vis_bytes, p->compute) != cudaSuccess)
+        return OSKB_ERR_KERNEL_LAUNCH_FAILURE;
+    return tc::correlate_block(p->casa, p->num_src, p->num_st,
+            p->num_times, p->num_channels, static_cast<const float*>(s.E),
+            sky, sky + ns, sky + 2 * ns, sky + 3 * ns, sky + 4 * ns,
+            sky + 5 * ns, sky + 6 * ns, static_cast<const double*>(s.uvw),
+            p->wl, p->uv_min, p->uv_max, static_cast<double*>(s.vis), p->ws,
+            p->ws_bytes, p->compute, after, ctx, nullptr, form);
+}
+
+// Times each candidate form on slot k's (uploaded) block and keeps the
+// fastest; a candidate that fails is skipped.
+int plan_tune(oskb_TcPlan* p, int k)
+{
+    static const int cand[3] = {tc::kFormI8, tc::kFormI8Pair,
+                                tc::kFormF16Wide};
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    if (cudaEventCreate(&e0) != cudaSuccess ||
+            cudaEventCreate(&e1) != cudaSuccess)
+        return OSKB_ERR_KERNEL_LAUNCH_FAILURE;
+    double best = 0.0;
+    int best_form = tc::kFormDefault;
+    for (int i = 0; i < 3; ++i)
+    {
+        p->tune_ms[i] = -1.0;
+        cudaEventRecord(e0, p->compute);
+        const int err = plan_correlate(p, k, cand[i], nullptr, nullptr);
+        cudaEventRecord(e1, p->compute);
+        if (cudaEventSynchronize(e1) != cudaSuccess || err)
+        {
+            cudaGetLastError();
+            continue;
+        }
+        float ms = 0.0f;
+        cudaEventElapsedTime(&ms, e0, e1);
+        p->tune_ms[i] = ms;
+        if (best_form == tc::kFormDefault || ms < best)
+        {
+            best = ms;
+            best_form = cand[i];
+        }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    p->form = best_form;
+    p->tuned = true;
+    return 0;
+}
+
+// Captures slot k's compute work into a graph; on failure the slot keeps
+// running eagerly.
+void plan_capture(oskb_TcPlan* p, int k)
+{
+    oskb_TcPlan::Slot& s = p->slot[k];
+    s.groups.clear();
+    if (tc::setup_device()) return;
+    // one event per group at most one per problem, created before the
+    // capture (no allocation inside it)
+    const size_t num_problems = (size_t) p->num_times * p->num_channels;
+    while (s.group_events.size() < num_problems)
+    {
+        cudaEvent_t ev = nullptr;
+        if (cudaEventCreateWithFlags(&ev, cudaEventDisableTiming) !=
+                cudaSuccess)
+            return;
+        s.group_events.push_back(ev);
+    }
+    cudaError_t ce = cudaStreamBeginCapture(p->compute,
+            cudaStreamCaptureModeThreadLocal);
+    if (ce != cudaSuccess)
+    {
+        set_last_error("tc plan: begin capture", ce);
+        cudaGetLastError();
+        return;
+    }
+    PlanHook hook{p, k, nullptr};
+    const bool failed_before = p->failed;
+    const int err = plan_correlate(p, k, p->form, plan_capture_group,
+            &hook);
+    cudaGraph_t graph = nullptr;
+    ce = cudaStreamEndCapture(p->compute, &graph);
+    if (err || ce != cudaSuccess || !graph || p->failed != failed_before ||
+            (ce = cudaGraphInstantiate(&s.exec, graph, 0)) != cudaSuccess)
+    {
+        char msg[160];
+        snprintf(msg, sizeof(msg), "tc plan: capture of slot %d failed "
+                "(correlate %d, capture status %d, hook %d); the slot runs "
+                "without a graph", k, err, (int) ce,
+                (int) (p->failed != failed_before));
+        set_last_error_msg(msg);
+        s.exec = nullptr;
+        s.groups.clear();
+        p->failed = failed_before;
+        cudaGetLastError();
+    }
+    if (graph) cudaGraphDestroy(graph);
+}
+
+bool env_flag(const char* name, bool dflt)
+{
+    const char* e = getenv(name);
+    return e ? atoi(e) != 0 : dflt;
+}
+
 }  // namespace
 
 extern "C" {
@@ -259,9 +410,11 @@ void oskb_tc_plan_free(oskb_TcPlan* p)
         if (s.uploaded) cudaEventDestroy(s.uploaded);
         if (s.computed) cudaEventDestroy(s.computed);
         if (s.downloaded) cudaEventDestroy(s.downloaded);
+        if (s.exec) cudaGraphExecDestroy(s.exec);
+        for (cudaEvent_t e : s.group_events) cudaEventDestroy(e);
     }
     for (cudaEvent_t e : p->group_events) cudaEventDestroy(e);
-    cudaFree(p->sky); cudaFree(p->wl);
+    cudaFree(p->sky); cudaFree(p->wl); cudaFree(p->ws);
     if (p->in) cudaStreamDestroy(p->in);
     if (p->compute) cudaStreamDestroy(p->compute);
     if (p->out) cudaStreamDestroy(p->out);
@@ -288,6 +441,28 @@ oskb_TcPlan* oskb_tc_plan_create(int casa, int num_sources, int num_stations,
     p->vis_bytes = (size_t) num_times * num_channels * p->problem_bytes;
     p->e_bytes = (size_t) num_stations * num_sources * 8 * sizeof(float);
     p->uvw_bytes = (size_t) num_times * 3 * num_stations * sizeof(double);
+    // an explicit form (OSKB_TC_PLAN_FORM = 1..5) skips the tuning
+    const char* fe = getenv("OSKB_TC_PLAN_FORM");
+    p->form = fe ? atoi(fe) : tc::kFormDefault;
+    if (p->form < tc::kFormDefault || p->form > tc::kFormF16Pair)
+        p->form = tc::kFormDefault;
+    p->tuned = fe != nullptr || !env_flag("OSKB_TC_PLAN_TUNE", true);
+    p->use_graph = env_flag("OSKB_TC_PLAN_GRAPH", true);
+    for (double& t : p->tune_ms) t = -1.0;
+    // workspace: up to 16 problems' operand images (the FP16 image, the
+    // larger form), and no more than half the device memory free now
+    const int num_problems = num_times * num_channels;
+    const size_t one = oskb_correlate_block_tc_workspace_bytes(num_sources,
+            num_stations, 1);
+    const size_t img = one - oskb_correlate_block_tc_workspace_bytes(
+            num_sources, num_stations, 0);
+    size_t free_b = 0, total_b = 0;
+    cudaMemGetInfo(&free_b, &total_b);
+    size_t group = num_problems < 16 ? num_problems : 16;
+    if (img && group > free_b / 2 / img) group = free_b / 2 / img;
+    if (group < 1) group = 1;
+    p->ws_bytes = oskb_correlate_block_tc_workspace_bytes(num_sources,
+            num_stations, (int) group);
     bool ok = cudaStreamCreateWithFlags(&p->in, cudaStreamNonBlocking) ==
             cudaSuccess &&
             cudaStreamCreateWithFlags(&p->compute, cudaStreamNonBlocking) ==
@@ -297,7 +472,8 @@ oskb_TcPlan* oskb_tc_plan_create(int casa, int num_sources, int num_stations,
             cudaMalloc((void**) &p->sky, 7 * sizeof(double) * num_sources) ==
             cudaSuccess &&
             cudaMalloc((void**) &p->wl, sizeof(double) * num_channels) ==
-            cudaSuccess;
+            cudaSuccess &&
+            cudaMalloc(&p->ws, p->ws_bytes) == cudaSuccess;
     for (auto& s : p->slot)
         ok = ok && cudaMalloc(&s.E, p->e_bytes) == cudaSuccess &&
                 cudaMalloc(&s.uvw, p->uvw_bytes) == cudaSuccess &&
@@ -368,17 +544,39 @@ int oskb_tc_plan_enqueue(oskb_TcPlan* p, const float* E_host,
     // last block have been downloaded
     cudaStreamWaitEvent(p->compute, s.uploaded, 0);
     if (s.used) cudaStreamWaitEvent(p->compute, s.downloaded, 0);
-    cudaMemsetAsync(s.vis, 0, p->vis_bytes, p->compute);
-    PlanHook hook{p, k, vis_host};
-    p->next_event = 0;
-    const double* sky = p->sky;
-    const size_t ns = p->num_src;
-    int err = tc::correlate_block(p->casa, p->num_src, p->num_st,
-            p->num_times, p->num_channels, static_cast<const float*>(s.E),
-            sky, sky + ns, sky + 2 * ns, sky + 3 * ns, sky + 4 * ns,
-            sky + 5 * ns, sky + 6 * ns, static_cast<const double*>(s.uvw),
-            p->wl, p->uv_min, p->uv_max, static_cast<double*>(s.vis), nullptr,
-            0, p->compute, plan_after_group, &hook);
+    if (!p->tuned)
+    {
+        const int err = plan_tune(p, k);
+        if (err) return err;
+    }
+    if (p->use_graph && !s.exec) plan_capture(p, k);
+    int err = 0;
+    if (s.exec)
+    {
+        if (cudaGraphLaunch(s.exec, p->compute) != cudaSuccess)
+        {
+            set_last_error("oskb_tc_plan_enqueue graph",
+                    cudaGetLastError());
+            return OSKB_ERR_KERNEL_LAUNCH_FAILURE;
+        }
+        ++p->graph_launches;
+        for (size_t g = 0; g < s.groups.size(); ++g)
+        {
+            const size_t off = (size_t) s.groups[g].first * p->problem_bytes;
+            cudaStreamWaitEvent(p->out, s.group_events[g], 0);
+            if (cudaMemcpyAsync(reinterpret_cast<char*>(vis_host) + off,
+                    static_cast<const char*>(s.vis) + off,
+                    (size_t) s.groups[g].second * p->problem_bytes,
+                    cudaMemcpyDeviceToHost, p->out) != cudaSuccess)
+                p->failed = true;
+        }
+    }
+    else
+    {
+        PlanHook hook{p, k, vis_host};
+        p->next_event = 0;
+        err = plan_correlate(p, k, p->form, plan_after_group, &hook);
+    }
     cudaEventRecord(s.computed, p->compute);
     cudaEventRecord(s.downloaded, p->out);
     s.used = true;
@@ -397,6 +595,23 @@ int oskb_tc_plan_wait(oskb_TcPlan* p)
         set_last_error("oskb_tc_plan_wait", cudaGetLastError());
         return OSKB_ERR_KERNEL_LAUNCH_FAILURE;
     }
+    return 0;
+}
+
+int oskb_tc_plan_form(const oskb_TcPlan* p)
+{
+    return p ? p->form : 0;
+}
+
+int oskb_tc_plan_graph_launches(const oskb_TcPlan* p)
+{
+    return p ? p->graph_launches : 0;
+}
+
+int oskb_tc_plan_tuning_ms(const oskb_TcPlan* p, double* ms)
+{
+    if (!p || !ms) return OSKB_ERR_INVALID_ARGUMENT;
+    for (int i = 0; i < 3; ++i) ms[i] = p->tune_ms[i];
     return 0;
 }
 

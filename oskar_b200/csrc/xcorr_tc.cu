@@ -534,6 +534,7 @@ struct GemmParams
     double uv_min, uv_max;
     int casa;
     int i8;                     // operand image is the three-limb integer one
+    int form;                   // Form (kFormDefault: the environment's)
     int* err;
     // Auto-correlations (optional): the diagonal station pairs of the
     // diagonal tiles, V_pp = J_p B J_p^H, added into
@@ -2374,6 +2375,12 @@ cudaEvent_t timing_start(cudaStream_t stream)
 {
     std::lock_guard<std::mutex> lock(g_timing_mutex);
     if (!g_timing) return nullptr;
+    // a launch being captured into a graph is not timed (its replays would
+    // all record into the one pair of events)
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    if (cudaStreamIsCapturing(stream, &cs) == cudaSuccess &&
+            cs != cudaStreamCaptureStatusNone)
+        return nullptr;
     if (g_ev_used == g_ev.size())
     {
         cudaEvent_t e0, e1;
@@ -2401,7 +2408,8 @@ int launch_gemm(GemmParams& gp, cudaStream_t stream)
         const long long pair_n = (long long) pair_i8_tiles(gp.nrb) *
                 gp.num_problems;
         const char* pe = getenv("OSKB_TC_PAIR");
-        const bool use_pair = pe && atoi(pe) != 0;
+        const bool use_pair = gp.form ? gp.form == kFormI8Pair :
+                (pe && atoi(pe) != 0);
         g_last_arith.store(8);
         if (use_pair)
         {
@@ -2451,7 +2459,9 @@ int launch_gemm(GemmParams& gp, cudaStream_t stream)
             gp.num_problems;
     const long long pair_n = (long long) pair_tiles(gp.nrb) *
             gp.num_problems;
-    const int setting = tile_setting();
+    const int setting = gp.form == kFormF16 ? 128 :
+            gp.form == kFormF16Wide ? 256 : gp.form == kFormF16Pair ? 512 :
+            tile_setting();
     const int pairs = num_sms() / 2;
     // pair tiles only on request: on one B200 at 512 stations x 100,000
     // sources x 16 channels they measured 52.6 ms per launch against 46.1 ms
@@ -2554,6 +2564,7 @@ int oskb_cross_correlate_tc_d(int casa, int num_sources, int num_stations,
     if ((err = check_launch("tc prep"))) return err;
     GemmParams gp;
     gp.i8 = i8;
+    gp.form = kFormDefault;
     gp.W = W; gp.image_stride = 0; gp.nrb = nrb; gp.nkb = nkb;
     gp.num_problems = 1; gp.num_st = num_stations;
     gp.maxabs_bits = &hdr->maxabs_bits; gp.maxabs_stride = 0;
@@ -2631,7 +2642,7 @@ int correlate_block(int casa, int num_sources, int num_stations,
         double uv_max_lambda, double* vis, void* workspace,
         size_t workspace_bytes, void* stream,
         void (*after_group)(void* ctx, int p0, int np), void* ctx,
-        double* autos)
+        double* autos, int form)
 {
     if (num_sources < 0 || num_stations < 0 || num_times < 0 ||
             num_channels < 0)
@@ -2642,7 +2653,7 @@ int correlate_block(int casa, int num_sources, int num_stations,
             !inv_wavelength || !vis)
         return OSKB_ERR_INVALID_ARGUMENT;
     // Problems (t, c) are processed in groups that fit the workspace.
-    const bool i8 = arith_i8();
+    const bool i8 = form ? form <= kFormI8Pair : arith_i8();
     const size_t img = image_bytes_for(i8, num_stations, num_sources);
     int group = num_problems;
     if (workspace)
@@ -2694,6 +2705,7 @@ int correlate_block(int casa, int num_sources, int num_stations,
         if ((err = check_launch("tc prep fused"))) return err;
         GemmParams gp;
         gp.i8 = i8;
+        gp.form = form;
         gp.W = W; gp.image_stride = img; gp.nrb = nrb; gp.nkb = nkb;
         gp.num_problems = np; gp.num_st = num_stations;
         gp.maxabs_bits = &hdr->maxabs_bits; gp.maxabs_stride = 0;
@@ -2714,12 +2726,18 @@ template int correlate_block<float>(int, int, int, int, int, const float*,
         const double*, const double*, const double*, const double*,
         const double*, const double*, const double*, const double*,
         const double*, double, double, double*, void*, size_t, void*,
-        void (*)(void*, int, int), void*, double*);
+        void (*)(void*, int, int), void*, double*, int);
 template int correlate_block<double>(int, int, int, int, int, const double*,
         const double*, const double*, const double*, const double*,
         const double*, const double*, const double*, const double*,
         const double*, double, double, double*, void*, size_t, void*,
-        void (*)(void*, int, int), void*, double*);
+        void (*)(void*, int, int), void*, double*, int);
+
+int setup_device()
+{
+    bool wide_fits = false, pair_fits = false;
+    return device_setup(wide_fits, pair_fits);
+}
 
 }  // namespace tc
 }  // namespace oskb
@@ -2892,6 +2910,7 @@ extern "C" int oskb_cross_correlate_tc_noalloc_d(int casa, int num_sources,
     if ((err = check_launch("tc prep (static scratch)"))) return err;
     GemmParams gp;
     gp.i8 = i8;
+    gp.form = kFormDefault;
     gp.W = W; gp.image_stride = 0; gp.nrb = nrb; gp.nkb = nkb;
     gp.num_problems = 1; gp.num_st = num_stations;
     gp.maxabs_bits = &hdr->maxabs_bits; gp.maxabs_stride = 0;

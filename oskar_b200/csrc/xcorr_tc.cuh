@@ -6,13 +6,25 @@
 namespace oskb {
 namespace tc {
 
+// Contraction forms; kFormDefault follows the environment (OSKB_TC_ARITH,
+// OSKB_TC_TILE, OSKB_TC_PAIR), the others fix the form.
+enum Form
+{
+    kFormDefault = 0,
+    kFormI8 = 1,        // integer, 128 x 128 tiles
+    kFormI8Pair = 2,    // integer, 256 x 128 tiles on CTA pairs
+    kFormF16 = 3,       // FP16 hi/lo, 128 x 128 tiles
+    kFormF16Wide = 4,   // FP16 hi/lo, 128 x 256 tiles
+    kFormF16Pair = 5    // FP16 hi/lo, 256 x 256 tiles on CTA pairs
+};
+
 // oskb_correlate_block_tc with a hook: after_group (if set) is called on the
 // host once the contraction of problems [p0, p0 + np) has been enqueued on
 // the stream, so the caller can enqueue work that depends on those
 // visibilities (for example their download) while later groups compute;
 // autos (if set) receives the auto-correlations from the same contraction
 // ([time][channel][station][2x2], added). E is FP32 or FP64 (float or
-// double instantiations).
+// double instantiations); form fixes the contraction form.
 template <typename TE>
 int correlate_block(int casa, int num_sources, int num_stations,
         int num_times, int num_channels, const TE* E, const double* l,
@@ -22,7 +34,11 @@ int correlate_block(int casa, int num_sources, int num_stations,
         double uv_max_lambda, double* vis, void* workspace,
         size_t workspace_bytes, void* stream,
         void (*after_group)(void* ctx, int p0, int np), void* ctx,
-        double* autos = nullptr);
+        double* autos = nullptr, int form = kFormDefault);
+
+// The per-device launch set-up of the contraction kernels (shared-memory
+// opt-ins), done before a stream capture so that none happens inside it.
+int setup_device();
 
 }  // namespace tc
 }  // namespace oskb
