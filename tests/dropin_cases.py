@@ -136,3 +136,39 @@ def c2_small_case(precision="double", per_station=True, **over):
     }
     case.update(over)
     return case
+
+
+def c3_shaped_case(precision="double", num_src=100_000, num_channels=16,
+                   num_times=4, **over):
+    """The C3 shape through the reference simulator: 512 isotropic stations
+    log-radial to 65 km (one shared station model), the C3 sky (point
+    sources in a 10 deg field, full Stokes, S^-1.5) about the C configurations'
+    phase centre,
+    num_channels channels of 1 MHz from 100 MHz, num_times dumps of 10 s in
+    one block, sky chunks of 16,384 sources (the reference's default), no
+    smearing, horizon clip off (the field is above the horizon), visibilities
+    not read back (a timing case). The reference's E here is its isotropic
+    station beam, not C3's random E."""
+    cfg = workloads.c3(num_src=num_src, num_channels=num_channels,
+                       num_times=num_times)
+    ra0, dec0 = cfg.ra0, cfg.dec0
+    ra, dec = lm_to_radec(cfg.l, cfg.m, ra0, dec0)
+    z = [0.0] * num_src
+    case = c1_case(precision)
+    case.update({
+        "station_x": cfg.station_enu[0].tolist(),
+        "station_y": cfg.station_enu[1].tolist(),
+        "ra_rad": ra.tolist(), "dec_rad": dec.tolist(),
+        "I": cfg.I.tolist(), "Q": cfg.Q.tolist(), "U": cfg.U.tolist(),
+        "V": cfg.V.tolist(), "ref_freq_hz": list(z),
+        "spectral_index": list(z), "rotation_measure": list(z),
+        "major_rad": list(z), "minor_rad": list(z), "pa_rad": list(z),
+        "phase_centre_ra_rad": ra0, "phase_centre_dec_rad": dec0,
+        "freq_start_hz": 100e6, "freq_inc_hz": 1e6,
+        "num_channels": num_channels, "inc_sec": 10.0,
+        "num_times": num_times, "max_times_per_block": num_times,
+        "max_sources_per_chunk": 16384, "horizon_clip": 0,
+        "read_back": False,
+    })
+    case.update(over)
+    return case

@@ -29,13 +29,17 @@ case.json keys (all required):
   correlation_type ("Cross-correlations" | "Auto-correlations" | "Both"),
   casa, source_min_jy, source_max_jy. Optional: station_per_folder (one
   station model per station, station-beam duplication off), element_x and
-  element_y (aperture-array element layouts).
+  element_y (aperture-array element layouts), read_back (default true:
+  false skips reading the .vis file back, for timing runs).
+The .npz also holds run_seconds, the wall time of oskar_interferometer_run
+alone (the simulator's block loop and .vis writer).
 """
 import ctypes
 import json
 import os
 import sys
 import tempfile
+import time
 
 import numpy as np
 
@@ -205,9 +209,16 @@ def run(case, out_path):
     vis_path = os.path.join(work, "out.vis")
     lib.oskar_interferometer_set_output_vis_file(h, vis_path.encode())
     _check(st, "simulator set-up")
+    t0 = time.perf_counter()
     lib.oskar_interferometer_run(h, ctypes.byref(st))
+    run_seconds = time.perf_counter() - t0
     _check(st, "oskar_interferometer_run")
     lib.oskar_interferometer_free(h, ctypes.byref(st))
+    if not case.get("read_back", True):
+        np.savez(out_path, run_seconds=np.array([run_seconds]),
+                 dropin=np.array([DROPIN_LIB in
+                                  os.environ.get("LD_PRELOAD", "")]))
+        return
     # read the blocks back with the reference's reader
     fb = lib.oskar_binary_create(vis_path.encode(), b"r", ctypes.byref(st))
     hdr = lib.oskar_vis_header_read(fb, ctypes.byref(st))
@@ -236,6 +247,7 @@ def run(case, out_path):
         out["autos"] = np.concatenate(autos, axis=0)
     out["dropin"] = np.array(
         [DROPIN_LIB in os.environ.get("LD_PRELOAD", "")])
+    out["run_seconds"] = np.array([run_seconds])
     np.savez(out_path, **out)
 
 

@@ -1,0 +1,90 @@
+"""The drop-in oskar_interferometer_run_block at the C3 shape (512
+stations, 130,816 baselines), inside the unmodified reference simulator:
+
+- parity on a sample (500 sources x 16 channels x 16 dumps, FP64) against
+  the reference's own CPU run of the same case, to 5e-12 (max and L2): the
+  phases reach ~3e4 radians on the 65 km baselines at 115 MHz, whose FP64
+  rounding (2^-53 x 3e4 ~ 3e-12) two correct programs computing them in a
+  different order can differ by (tests/test_gpu_dropin.py's 1e-12 is for
+  1 km);
+- speed: the reference's own driver (oskar_interferometer_run: block loop,
+  sky chunks of 16,384, .vis writer) timed around the run call, with the
+  drop-in on the full C3 sky (100,000 sources x 16 channels x 4 dumps, one
+  device thread) and with the reference's CPU path on the sample (8
+  device threads, so its 16 work units, one per dump, run in parallel);
+  both in source-baselines per second. Set
+  OSKB_DROPIN_SPEED_OUT to a path to keep the numbers (JSON).
+The reference's station beams here are isotropic (its telescope model has
+no random E), so the drop-in runs R, K, the joins and the FP64
+cross-correlation for every chunk, dump and channel."""
+import json
+import os
+import subprocess
+import sys
+
+import numpy as np
+import pytest
+
+torch = pytest.importorskip("torch")
+pytestmark = [pytest.mark.gpu,
+              pytest.mark.skipif(not torch.cuda.is_available(),
+                                 reason="needs a CUDA device")]
+
+from dropin_cases import c3_shaped_case  # noqa: E402
+from test_gpu_dropin import DROPIN, HERE, compare, need_ref  # noqa: E402
+
+NBL = 512 * 511 // 2
+
+
+def sim(case, tmp_path, tag, dropin, attempts=6):
+    cj = tmp_path / ("%s.json" % tag)
+    out = tmp_path / ("%s.npz" % tag)
+    cj.write_text(json.dumps(case))
+    env = {k: v for k, v in os.environ.items() if k != "LD_PRELOAD"}
+    if dropin:
+        env["LD_PRELOAD"] = DROPIN
+    for _ in range(attempts if not dropin else 1):
+        r = subprocess.run([sys.executable, os.path.join(HERE, "ref_sim.py"),
+                            str(cj), str(out)], env=env, capture_output=True,
+                           text=True, timeout=1200)
+        if r.returncode != -11:
+            break
+    assert r.returncode == 0, (tag, r.returncode, r.stderr[-3000:])
+    d = dict(np.load(out))
+    assert bool(d.pop("dropin")[0]) == dropin
+    return d
+
+
+def test_dropin_c3_shape(tmp_path):
+    need_ref()
+    # the reference's multi-threaded CPU path was seen to crash (SIGSEGV)
+    # now and then; its runs are repeated, and 8 threads crash less often
+    threads = min(os.cpu_count() or 1, 8)
+    sample = c3_shaped_case("double", num_src=500, num_channels=16,
+                            num_times=16, read_back=True)
+    ref = sim(dict(sample, num_devices=threads), tmp_path, "ref_sample",
+              dropin=False)
+    got = sim(sample, tmp_path, "b200_sample", dropin=True)
+    t_cpu = float(ref.pop("run_seconds")[0])
+    got.pop("run_seconds")
+    compare(got, ref, 5e-12)
+    full = c3_shaped_case("double")
+    t_gpu = float(sim(full, tmp_path, "b200_full", dropin=True)
+                  ["run_seconds"][0])
+    cpu = NBL * 500 * 16 * 16 / t_cpu / 1e9
+    gpu = NBL * 100_000 * 16 * 4 / t_gpu / 1e9
+    res = {"unit": "G source-baselines/s",
+           "dropin": {"value": gpu, "seconds": t_gpu,
+                      "case": "512 stations x 100,000 sources x 16 channels "
+                              "x 4 dumps, FP64, sky chunks of 16,384"},
+           "reference_cpu": {"value": cpu, "seconds": t_cpu,
+                             "case": "512 stations x 500 sources x 16 "
+                                     "channels x 16 dumps, FP64",
+                             "device_threads": threads},
+           "speedup": gpu / cpu}
+    path = os.environ.get("OSKB_DROPIN_SPEED_OUT")
+    if path:
+        with open(path, "w") as f:
+            json.dump(res, f, indent=1)
+    print(json.dumps(res))
+    assert gpu > 20 * cpu, res
