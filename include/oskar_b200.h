@@ -1088,7 +1088,9 @@ OSKB_API int oskb_tc_timing_read(double* total_ms, int* launches);
  * calls no cudaMalloc, cudaFree or allocating library routine.
  *  - Limit: 32 bytes per station-source after rounding up to blocks of 32
  *    stations x 32 sources, plus 256 bytes (e.g. 512 stations x 4,064
- *    sources; 4,096 sources do not fit). Larger calls return
+ *    sources; 4,096 sources do not fit): the FP16 form's operand image,
+ *    so the limit holds whichever contraction form runs (the default
+ *    integer form's image is 24 bytes per station-source). Larger calls return
  *    OSKB_ERR_OUT_OF_RANGE (-5) with the sizes in oskb_last_error(); split
  *    the sources into chunks, since vis is accumulated.
  *  - The first call on a device takes the array's device address

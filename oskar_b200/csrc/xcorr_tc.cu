@@ -2820,10 +2820,12 @@ namespace {
 
 // Maximum scratch of the allocation-free entry point: 64 MiB, held by every
 // GPU that loads the library until the process exits. Beside a 256-byte
-// status header, the operand image needs 32 bytes per station-source (an
-// FP16 hi and lo word for each of the 8 real parts of J C), rounded up to
-// blocks of 32 stations x 32 sources: e.g. up to 512 stations x 4,064
-// sources per call (4,096 sources no longer fit).
+// status header, the operand image needs 32 bytes per station-source in the
+// FP16 form (an FP16 hi and lo word for each of the 8 real parts of J C),
+// 24 in the integer form (three limbs each), rounded up to blocks of 32
+// stations x 32 sources; the size check uses the FP16 figure whichever form
+// runs: e.g. up to 512 stations x 4,064 sources per call (4,096 sources no
+// longer fit).
 constexpr size_t kStaticScratchBytes = (size_t) 64 << 20;
 
 static __device__ __align__(256) uint8_t g_static_scratch[kStaticScratchBytes];
