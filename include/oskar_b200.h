@@ -527,6 +527,34 @@ OSKB_API int oskb_station_beam_two_level_f(int num_tile_types,
         const float* z, void* workspace, size_t workspace_bytes,
         float* beam, void* stream);
 
+/* Relative direction cosines (l, m, n) about a sky position (ra0, dec0) to
+ * ENU direction cosines (x, y, z) of a station at latitude lat, for hour
+ * angle ha0 = lst - ra0 (radians). All arrays device [num]. Replaces the
+ * kernel behind oskar_convert_relative_directions_to_enu_directions
+ * (oskar/convert/define_convert_relative_directions_to_enu_directions.h;
+ * src/oskar_convert_relative_directions_to_enu_directions.c:18-60), the
+ * conversion the beam-pattern application applies to its pixel grid. */
+OSKB_API int oskb_convert_relative_directions_to_enu_directions_d(int num,
+        const double* l, const double* m, const double* n, double ha0_rad,
+        double dec0_rad, double lat_rad, double* x, double* y, double* z,
+        void* stream);
+OSKB_API int oskb_convert_relative_directions_to_enu_directions_f(int num,
+        const float* l, const float* m, const float* n, double ha0_rad,
+        double dec0_rad, double lat_rad, float* x, float* y, float* z,
+        void* stream);
+
+/* Beam-image pixel grid: direction cosines (l, m, n) of num_l x num_m
+ * pixels (m slowest, l fastest, l decreasing with the pixel index as FITS
+ * images run) over a field of fov_lon x fov_lat radians; centred (the
+ * beam-pattern application's grid): the axes run evenly between +-sin(fov
+ * / 2); otherwise pixel centres step by the cell size asin(2 sin(fov / 2) /
+ * num) from the centre pixel num / 2. Pixels beyond the sphere are NaN.
+ * Host arrays [num_l * num_m]. Restates oskar_evaluate_image_lmn_grid_d
+ * (oskar/math/src/oskar_evaluate_image_lmn_grid.c:149-227). */
+OSKB_API int oskb_evaluate_image_lmn_grid(int num_l, int num_m,
+        double fov_lon_rad, double fov_lat_rad, int centred, double* l,
+        double* m, double* n);
+
 /* Hierarchical aperture-array station of any depth (num_levels 2..16).
  * Level 0 holds num_types[0] leaf layouts (dipole arrays: num_elements
  * dipoles each at el_x/y/z [type][element], orientations orientation_x/y_rad
