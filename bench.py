@@ -357,16 +357,11 @@ def run_ours(args):
             arith = ob.load().oskb_tc_arithmetic()
             issued_pk, issued_kind = pk, "measured bf16 sustained"
             if arith == 8:
-                # integer form: eight 8-bit limb products per K step (2 ops
-                # per multiply-add) on square tiles, or on 256 x 128 pair
-                # tiles (tile 256); the 8-bit dense rate is twice the 16-bit
-                # one
-                if tile == 256:
-                    ntp = sum(nrb - 2 * ti for ti in range((nrb + 1) // 2))
-                    issued = nch * ntp * 256 * 128 * kp * 2 * 8
-                else:
-                    issued = nch * nrb * (nrb + 1) // 2 * 128 * 128 * kp * \
-                        2 * 8
+                # integer form: six 8-bit limb products per K step (2 ops
+                # per multiply-add) on square tiles (the bucket padding, at
+                # most 15 source blocks, is not counted); the 8-bit dense
+                # rate is twice the 16-bit one
+                issued = nch * nrb * (nrb + 1) // 2 * 128 * 128 * kp * 2 * 6
                 issued_pk = 2 * pk
                 issued_kind = ("2 x measured bf16 sustained (the int8 dense "
                                "tensor rate is twice the bf16 one)")
@@ -386,14 +381,13 @@ def run_ours(args):
             traffic = _load_traffic(tile, arith)
             roof = {"bound": "tensor", "achieved": ach, "peak": pk,
                     "unit": "TFLOP/s", "frac": ach / pk, "traffic": traffic,
-                    "kernel": ("oskb::tc::gemm_pair_i8_kernel"
-                               if tile == 256 else "oskb::tc::gemm_i8_kernel")
-                              if arith == 8
+                    "kernel": "oskb::tc::gemm_i8_kernel" if arith == 8
                               else {256: "oskb::tc::gemm_wide_kernel",
                                     512: "oskb::tc::gemm_pair_kernel"}.get(
                                         tile, "oskb::tc::gemm_kernel"),
                     "tile_columns": tile,
-                    "arithmetic": "int8 x3 limbs -> exact s32" if arith == 8
+                    "arithmetic": "int8 x3 limbs (6 products, amplitude "
+                                  "buckets) -> exact s32" if arith == 8
                                   else "fp16 hi/lo x3 -> f32 -> f64",
                     "peak_kind": "%s bf16 sustained (fp16 same rate)"
                                  % peak_kind,

@@ -839,9 +839,12 @@ OSKB_API int oskb_evaluate_jones_R_f(int num_sources, const float* ra_rad,
  * ------------------------------------------------------------------------
  * Same result as oskb_cross_correlate_d with gaussian = 0,
  * frac_bandwidth = 0 and time_int_sec = 0, computed as a Hermitian rank-k
- * update on the sm_100a tensor cores (tcgen05, FP16 hi/lo split, three
- * products, FP32 accumulation drained to FP64); relative visibility error
- * against FP64 below 1e-6. Every brightness matrix must be positive
+ * update on the sm_100a tensor cores (tcgen05; by default the integer form:
+ * 24-bit fixed-point entries in three signed 8-bit limbs, the sources in
+ * amplitude buckets with a scale each, exact S32 accumulation; else the
+ * FP16 hi/lo form: three products, FP32 accumulation drained to FP64; see
+ * oskb_tc_arithmetic); relative visibility error against FP64 below 1e-6
+ * (L2 and max). Every brightness matrix must be positive
  * semi-definite (I >= sqrt(Q^2 + U^2 + V^2)); oskb_tc_status() reports a
  * violation. It is the fast branch of oskar_cross_correlate
  * (oskar/correlate/oskar_cross_correlate.h:49) for source_type 0 without
@@ -1003,9 +1006,9 @@ OSKB_API void oskb_block_plan_free(oskb_BlockPlan* plan);
  * Stokes, host arrays) is uploaded once by oskb_tc_plan_set_sky.
  * The plan owns its contraction workspace (up to 16 problems' operand
  * images, at most half the device memory free at creation). The first
- * enqueue picks the contraction form by timing integer square tiles,
- * integer CTA-pair tiles and FP16 wide tiles on its own block (it waits for
- * them; environment OSKB_TC_PLAN_FORM = 1..5 fixes a form instead, 0 the
+ * enqueue picks the contraction form by timing the integer form, FP16
+ * square tiles and FP16 wide tiles on its own block (it waits for them;
+ * environment OSKB_TC_PLAN_FORM = 1, 3, 4 or 5 fixes a form instead, 0 the
  * library default; OSKB_TC_PLAN_TUNE=0 skips the timing); each slot's
  * compute work is then captured into a CUDA graph at its first block and
  * replayed for the later ones (OSKB_TC_PLAN_GRAPH=0: launched eagerly). The
@@ -1023,12 +1026,12 @@ OSKB_API int oskb_tc_plan_enqueue(oskb_TcPlan* plan, const float* E_host,
         const double* station_uvw_host, double* vis_host);
 OSKB_API int oskb_tc_plan_wait(oskb_TcPlan* plan);
 OSKB_API void oskb_tc_plan_free(oskb_TcPlan* plan);
-/* The plan's contraction form: 0 library default, 1 integer square tiles,
- * 2 integer CTA-pair tiles, 3 FP16 square, 4 FP16 wide, 5 FP16 pairs. */
+/* The plan's contraction form: 0 library default, 1 integer (square
+ * tiles), 3 FP16 square, 4 FP16 wide, 5 FP16 pairs (2 is not a form). */
 OSKB_API int oskb_tc_plan_form(const oskb_TcPlan* plan);
 /* Graph replays so far (0 while the plan runs eagerly). */
 OSKB_API int oskb_tc_plan_graph_launches(const oskb_TcPlan* plan);
-/* The tuning times (ms) of forms 1, 2 and 4 on the first block, -1 where
+/* The tuning times (ms) of forms 1, 3 and 4 on the first block, -1 where
  * not timed. ms: host [3]. */
 OSKB_API int oskb_tc_plan_tuning_ms(const oskb_TcPlan* plan, double* ms);
 
@@ -1118,7 +1121,10 @@ OSKB_API int oskb_tc_timing_read(double* total_ms, int* launches);
  *    stations x 32 sources, plus 256 bytes (e.g. 512 stations x 4,064
  *    sources; 4,096 sources do not fit): the FP16 form's operand image,
  *    so the limit holds whichever contraction form runs (the default
- *    integer form's image is 24 bytes per station-source). Larger calls return
+ *    integer form's image is 24 bytes per station-source, with up to 15
+ *    more blocks of sources of bucket padding, and its source-order tables
+ *    about 8 bytes per source: smaller for all but a few sources, and the
+ *    check takes the larger of the two). Larger calls return
  *    OSKB_ERR_OUT_OF_RANGE (-5) with the sizes in oskb_last_error(); split
  *    the sources into chunks, since vis is accumulated.
  *  - The first call on a device takes the array's device address
@@ -1158,14 +1164,16 @@ OSKB_API int oskb_tc_status(const void* workspace, int* flags,
  * variable OSKB_TC_TILE (128, 256 or 512) selects the FP16 form with that
  * tile (with OSKB_TC_ARITH=fp16 and no tile set: wide tiles when a launch
  * has at least two per SM, else square). Integer form: 128 (128 x 128 per
- * CTA, the default) or 256 (256 x 128 per pair of CTAs, OSKB_TC_PAIR=1). */
+ * CTA). */
 OSKB_API int oskb_tc_tile_columns(void);
 /* Arithmetic of the last tensor-core contraction launched, 0 before the
- * first: 8 for the default integer form (each scaled entry a 24-bit fixed-
- * point integer held as three 8-bit limbs, eight 8-bit tcgen05 MMAs
- * per K step into exact S32 accumulators, square tiles), 16 for the FP16
- * hi/lo form (three FP16 MMAs per K step into FP32 accumulators drained to
- * FP64), which OSKB_TC_ARITH=fp16, or any OSKB_TC_TILE setting, selects. */
+ * first: 8 for the default integer form (the sources ordered into
+ * amplitude buckets, factor 2 apart, each with its own scale; each scaled
+ * entry a 24-bit fixed-point integer held as three signed 8-bit limbs; six
+ * 8-bit tcgen05 MMAs per K step into exact S32 accumulators, square tiles),
+ * 16 for the FP16 hi/lo form (three FP16 MMAs per K step into FP32
+ * accumulators drained to FP64), which OSKB_TC_ARITH=fp16, or any
+ * OSKB_TC_TILE setting, selects. */
 OSKB_API int oskb_tc_arithmetic(void);
 
 /* ------------------------------------------------------------------------

@@ -304,7 +304,7 @@ int plan_correlate(oskb_TcPlan* p, int k, int form,
 // fastest; a candidate that fails is skipped.
 int plan_tune(oskb_TcPlan* p, int k)
 {
-    static const int cand[3] = {tc::kFormI8, tc::kFormI8Pair,
+    static const int cand[3] = {tc::kFormI8, tc::kFormF16,
                                 tc::kFormF16Wide};
     cudaEvent_t e0 = nullptr, e1 = nullptr;
     if (cudaEventCreate(&e0) != cudaSuccess ||
@@ -444,7 +444,8 @@ oskb_TcPlan* oskb_tc_plan_create(int casa, int num_sources, int num_stations,
     // an explicit form (OSKB_TC_PLAN_FORM = 1..5) skips the tuning
     const char* fe = getenv("OSKB_TC_PLAN_FORM");
     p->form = fe ? atoi(fe) : tc::kFormDefault;
-    if (p->form < tc::kFormDefault || p->form > tc::kFormF16Pair)
+    if (p->form < tc::kFormDefault || p->form > tc::kFormF16Pair ||
+            p->form == 2)
         p->form = tc::kFormDefault;
     p->tuned = fe != nullptr || !env_flag("OSKB_TC_PLAN_TUNE", true);
     p->use_graph = env_flag("OSKB_TC_PLAN_GRAPH", true);

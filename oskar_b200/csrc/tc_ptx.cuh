@@ -380,17 +380,6 @@ __device__ __forceinline__ void tma_load_2d_pair(void* dst_smem,
                     "r"(mbar_cluster) : "memory");
 }
 
-// The same for a 3-D box: coordinates (x, y, z) of its first element.
-__device__ __forceinline__ void tma_load_3d_pair(void* dst_smem,
-        const void* tmap, int x, int y, int z, uint32_t mbar_cluster)
-{
-    asm volatile("cp.async.bulk.tensor.3d.cta_group::2.shared::cluster.global"
-                 ".mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], "
-                 "[%5];"
-                 :: "r"(smem_u32(dst_smem)), "l"(tmap), "r"(x), "r"(y),
-                    "r"(z), "r"(mbar_cluster) : "memory");
-}
-
 // TMEM of both CTAs of a pair: one warp of each CTA (the same warp index),
 // the same shared-memory destination offset in both.
 __device__ __forceinline__ void tmem_alloc_pair(uint32_t* dst_smem,
@@ -422,22 +411,6 @@ __device__ __forceinline__ void mma_f16_pair(uint32_t d_tmem, uint64_t a_desc,
                  "tcgen05.mma.cta_group::2.kind::f16 [%0], %1, %2, %3, p;\n\t}"
                  :: "r"(d_tmem), "l"(a_desc), "l"(b_desc), "r"(idesc),
                     "r"(accumulate) : "memory");
-}
-
-// Pair MMA of kind::i8 (8-bit A and B, S32 accumulator): A rows
-// 0-127 from the even CTA's shared memory and 128-255 from the odd one's,
-// B columns 0 .. N/2-1 from the even CTA's and N/2 .. N-1 from the odd
-// one's, at the same offsets; no output lanes disabled.
-__device__ __forceinline__ void mma_i8_pair(uint32_t d_tmem, uint64_t a_desc,
-        uint64_t b_desc, uint32_t idesc, uint32_t accumulate)
-{
-    asm volatile("{\n\t.reg .pred p;\n\t"
-                 "setp.ne.b32 p, %4, 0;\n\t"
-                 "tcgen05.mma.cta_group::2.kind::i8 [%0], %1, %2, %3, "
-                 "{%5, %6, %7, %8, %9, %10, %11, %12}, p;\n\t}"
-                 :: "r"(d_tmem), "l"(a_desc), "l"(b_desc), "r"(idesc),
-                    "r"(accumulate), "r"(0u), "r"(0u), "r"(0u), "r"(0u),
-                    "r"(0u), "r"(0u), "r"(0u), "r"(0u) : "memory");
 }
 
 // Arrives on the mbarrier at the same shared offset in both CTAs of the

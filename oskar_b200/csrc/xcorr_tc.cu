@@ -79,11 +79,85 @@ constexpr int kI8Tile = 128 * 64;
 constexpr int kI8Block = 3 * kI8Tile;
 constexpr float kI8Target = 8323072.0f;      // 127 * 2^16
 
+// Sources of the integer image are ordered by amplitude bucket: bucket b
+// holds the sources whose largest |entry| over the stations is in
+// (m 2^-(b+1), m 2^-b] (m the largest of all; the last bucket also takes
+// everything fainter), each bucket padded to whole 32-source blocks and
+// scaled by its own q_b = q 2^b, so a source's entries use the limbs' full
+// range whatever its flux. The k blocks of one problem's image are the
+// padded, ordered sources (i8_kb_cap bounds their number).
+constexpr int kI8Buckets = 16;
+constexpr int kI8DrainKb = 512;
+
+// Each non-empty bucket pads to whole blocks, so the k blocks are at most
+// sum_b ceil(n_b / 32) <= (num_src + 31 B) / 32 for B non-empty buckets,
+// B <= min(kI8Buckets, num_src).
+__host__ __device__ inline int i8_kb_cap(int num_src)
+{
+    const int nb = num_src < kI8Buckets ? num_src : kI8Buckets;
+    return (int) (((long long) num_src + (long long) (kSrcPerBlock - 1) * nb)
+            / kSrcPerBlock);
+}
+
 __host__ __device__ inline size_t image_bytes_i8(int num_st, int num_src)
 {
     const size_t nrb = (num_st + kStPerBlock - 1) / kStPerBlock;
-    const size_t nkb = (num_src + kSrcPerBlock - 1) / kSrcPerBlock;
-    return nrb * nkb * kI8Block;
+    return nrb * (size_t) i8_kb_cap(num_src) * kI8Block;
+}
+
+// The contraction's chunks (accumulator drain intervals): one or more per
+// bucket, at most kI8DrainKb k blocks each.
+__host__ __device__ inline int i8_max_chunks(int num_src)
+{
+    return (i8_kb_cap(num_src) + kI8DrainKb - 1) / kI8DrainKb + kI8Buckets;
+}
+
+// Source order and scales of one call (device, in the workspace before the
+// image): counts[0] = k blocks used, counts[1] = chunks; chunk c covers k
+// blocks [chunk_kb[c], chunk_kb[c + 1]) of bucket chunk_bucket[c]; kb_bucket
+// is the bucket of each k block; perm maps each padded source position to
+// its source (-1: padding); amp_bits holds each source's largest |entry|.
+struct I8Order
+{
+    int* counts;
+    int* chunk_kb;
+    int* chunk_bucket;
+    int* kb_bucket;
+    int* perm;
+    unsigned int* amp_bits;
+};
+
+__host__ __device__ inline size_t align256_t(size_t b)
+{
+    return (b + 255) & ~(size_t) 255;
+}
+
+// Bytes of the tables for num_src sources; with base set, also their
+// addresses.
+__host__ __device__ inline size_t i8_order_bytes(int num_src, uint8_t* base,
+        I8Order* o)
+{
+    const size_t cap = (size_t) i8_kb_cap(num_src);
+    const size_t mc = (size_t) i8_max_chunks(num_src);
+    size_t off = 0;
+    const size_t sizes[6] = {align256_t(2 * sizeof(int)),
+            align256_t((mc + 1) * sizeof(int)), align256_t(mc * sizeof(int)),
+            align256_t(cap * sizeof(int)),
+            align256_t(cap * kSrcPerBlock * sizeof(int)),
+            align256_t((size_t) num_src * sizeof(unsigned int))};
+    if (base && o)
+    {
+        o->counts = reinterpret_cast<int*>(base + off); off += sizes[0];
+        o->chunk_kb = reinterpret_cast<int*>(base + off); off += sizes[1];
+        o->chunk_bucket = reinterpret_cast<int*>(base + off); off += sizes[2];
+        o->kb_bucket = reinterpret_cast<int*>(base + off); off += sizes[3];
+        o->perm = reinterpret_cast<int*>(base + off); off += sizes[4];
+        o->amp_bits = reinterpret_cast<unsigned int*>(base + off);
+        off += sizes[5];
+        return off;
+    }
+    for (size_t k = 0; k < 6; ++k) off += sizes[k];
+    return off;
 }
 
 // Fixed-point scale q (not a power of two) for the largest |entry| m.
@@ -92,6 +166,16 @@ __device__ __forceinline__ float i8_scale_from_bits(unsigned int bits)
     const float m = __uint_as_float(bits);
     if (!(m > 0.0f) || !isfinite(m)) return 1.0f;
     return kI8Target / m;
+}
+
+// Bucket of a source whose largest |entry| is a, for the largest of all m:
+// floor(log2(m / a)) in [0, kI8Buckets - 1] (so a <= m 2^-b).
+__device__ __forceinline__ int i8_bucket(float a, float m)
+{
+    if (!(a > 0.0f) || !(m > 0.0f) || !isfinite(m))
+        return a > 0.0f ? 0 : kI8Buckets - 1;
+    const int b = (int) floor(log2((double) m / (double) a));
+    return b < 0 ? 0 : (b >= kI8Buckets ? kI8Buckets - 1 : b);
 }
 
 // Byte offset of K column c (0..63) of row r in a limb tile.
@@ -265,11 +349,149 @@ __global__ void __launch_bounds__(256) maxabs_kernel(const TJ* __restrict__ jone
 }
 
 // ---------------------------------------------------------------------------
+// Largest |entry| of J C per source over the stations (amp_bits, cleared
+// before) and of all (maxabs_bits), for the integer image's buckets and
+// scales. One thread per source and station range (blockIdx.y of
+// gridDim.y), the stations in a loop (coalesced over sources); positive
+// floats order as their bit patterns, so the maxima are integer atomics.
+// ---------------------------------------------------------------------------
+template <typename TJ, typename TF>
+__global__ void __launch_bounds__(256) maxabs_src_kernel(
+        const TJ* __restrict__ jones, int num_src, int num_st,
+        const TF* __restrict__ I, const TF* __restrict__ Q,
+        const TF* __restrict__ U, const TF* __restrict__ V,
+        unsigned int* __restrict__ amp_bits, unsigned int* maxabs_bits,
+        int* flags)
+{
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    const int per = (num_st + gridDim.y - 1) / gridDim.y;
+    const int pa = blockIdx.y * per, pb = min(num_st, pa + per);
+    float mx = 0.0f;
+    bool psd = true;
+    if (s < num_src && pa < pb)
+    {
+        float c11, c21r, c21i, c22, J[8], A[2][2][2];
+        psd = brightness_factor(I[s], Q[s], U[s], V[s], c11, c21r, c21i,
+                c22);
+        for (int p = pa; p < pb; ++p)
+        {
+            load_jones<TJ>(jones + 8 * ((size_t) p * num_src + s), J);
+            apply_factor(J, c11, c21r, c21i, c22, A);
+#pragma unroll
+            for (int i = 0; i < 2; ++i)
+#pragma unroll
+                for (int kk = 0; kk < 2; ++kk)
+                    mx = fmaxf(mx, hypotf(A[i][kk][0], A[i][kk][1]));
+        }
+        atomicMax(amp_bits + s, __float_as_uint(mx));
+    }
+    for (int o = 16; o > 0; o >>= 1)
+        mx = fmaxf(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+    if ((threadIdx.x & 31) == 0) atomicMax(maxabs_bits, __float_as_uint(mx));
+    if (!psd) atomicOr(flags, 1);
+}
+
+// ---------------------------------------------------------------------------
+// The integer image's source order (one CTA of kOrderThreads): each thread
+// takes a contiguous run of sources, counts them per bucket, the counts are
+// scanned over the threads per bucket (one warp per bucket), and every
+// source is written to its bucket's next position, so each bucket keeps the
+// sources in their original order (deterministic). Then the padding, the
+// bucket of every k block and the chunk table.
+// ---------------------------------------------------------------------------
+constexpr int kOrderThreads = 512;
+
+__global__ void __launch_bounds__(kOrderThreads) i8_order_kernel(
+        int num_src, const unsigned int* __restrict__ maxabs_bits,
+        I8Order o)
+{
+    __shared__ int cnt[kI8Buckets][kOrderThreads];
+    __shared__ int start[kI8Buckets + 1], total[kI8Buckets];
+    const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
+    const int run = (num_src + kOrderThreads - 1) / kOrderThreads;
+    const int s0 = min(num_src, t * run), s1 = min(num_src, s0 + run);
+    const float m = __uint_as_float(*maxabs_bits);
+    int c[kI8Buckets];
+#pragma unroll
+    for (int b = 0; b < kI8Buckets; ++b) c[b] = 0;
+    for (int s = s0; s < s1; ++s)
+    {
+        const int b = i8_bucket(__uint_as_float(o.amp_bits[s]), m);
+#pragma unroll
+        for (int k = 0; k < kI8Buckets; ++k) c[k] += k == b;
+    }
+#pragma unroll
+    for (int b = 0; b < kI8Buckets; ++b) cnt[b][t] = c[b];
+    __syncthreads();
+    // exclusive scan of each bucket's counts over the threads
+    if (warp < kI8Buckets)
+    {
+        int running = 0;
+        for (int i = 0; i < kOrderThreads; i += 32)
+        {
+            const int v = cnt[warp][i + lane];
+            int incl = v;
+            for (int d = 1; d < 32; d <<= 1)
+            {
+                const int u = __shfl_up_sync(0xffffffffu, incl, d);
+                if (lane >= d) incl += u;
+            }
+            cnt[warp][i + lane] = running + incl - v;
+            running += __shfl_sync(0xffffffffu, incl, 31);
+        }
+        if (lane == 0) total[warp] = running;
+    }
+    __syncthreads();
+    if (t == 0)
+    {
+        start[0] = 0;
+        for (int b = 0; b < kI8Buckets; ++b)
+            start[b + 1] = start[b] + (total[b] + kSrcPerBlock - 1) /
+                    kSrcPerBlock * kSrcPerBlock;
+        const int nkb = start[kI8Buckets] / kSrcPerBlock;
+        int nchunk = 0;
+        for (int b = 0; b < kI8Buckets; ++b)
+            for (int k = start[b] / kSrcPerBlock;
+                    k < start[b + 1] / kSrcPerBlock; k += kI8DrainKb)
+            {
+                o.chunk_kb[nchunk] = k;
+                o.chunk_bucket[nchunk] = b;
+                ++nchunk;
+            }
+        o.chunk_kb[nchunk] = nkb;
+        o.counts[0] = nkb;
+        o.counts[1] = nchunk;
+    }
+    __syncthreads();
+    // scatter, in each bucket in source order
+#pragma unroll
+    for (int b = 0; b < kI8Buckets; ++b) c[b] = 0;
+    for (int s = s0; s < s1; ++s)
+    {
+        const int b = i8_bucket(__uint_as_float(o.amp_bits[s]), m);
+        int pos = 0;
+#pragma unroll
+        for (int k = 0; k < kI8Buckets; ++k)
+            if (k == b) pos = start[k] + cnt[k][t] + c[k]++;
+        o.perm[pos] = s;
+    }
+    // padding and the bucket of every k block
+    const int npos = start[kI8Buckets];
+    for (int i = t; i < npos; i += kOrderThreads)
+    {
+        int b = 0;
+        while (i >= start[b + 1]) ++b;
+        if (i >= start[b] + total[b]) o.perm[i] = -1;
+        if (i % kSrcPerBlock == 0) o.kb_bucket[i / kSrcPerBlock] = b;
+    }
+}
+
+// ---------------------------------------------------------------------------
 // Operand image from joined Jones J (the oskar_cross_correlate input).
 // grid (k blocks, row blocks, problems); 8 warps, warp = 4 stations,
 // lane = source.
 // ---------------------------------------------------------------------------
-template <typename TJ, bool I8>
+template <typename TJ>
 __global__ void __launch_bounds__(256) prep_jones_kernel(
         const TJ* __restrict__ jones, int num_src, int num_st,
         const TJ* __restrict__ I, const TJ* __restrict__ Q,
@@ -282,10 +504,8 @@ __global__ void __launch_bounds__(256) prep_jones_kernel(
     const bool src_ok = s < num_src;
     float c11 = 0, c21r = 0, c21i = 0, c22 = 0;
     if (src_ok) brightness_factor(I[s], Q[s], U[s], V[s], c11, c21r, c21i, c22);
-    const float S = I8 ? i8_scale_from_bits(*maxabs_bits)
-                       : scale_from_bits(*maxabs_bits);
-    uint8_t* tile = W + (size_t) (rb * nkb + kb) *
-            (I8 ? kI8Block : kPairBytes);
+    const float S = scale_from_bits(*maxabs_bits);
+    uint8_t* tile = W + (size_t) (rb * nkb + kb) * kPairBytes;
     for (int pl = warp; pl < kStPerBlock; pl += 8)
     {
         const int p = rb * kStPerBlock + pl;
@@ -298,10 +518,44 @@ __global__ void __launch_bounds__(256) prep_jones_kernel(
 #pragma unroll
             for (int k = 0; k < 8; ++k) (&A[0][0][0])[k] *= S;
         }
-        if constexpr (I8)
-            store_entry_i8(tile, pl, lane, A);
-        else
-            store_entry(tile, pl, lane, A);
+        store_entry(tile, pl, lane, A);
+    }
+}
+
+// Integer image from joined Jones J: the sources in bucket order (o.perm),
+// each k block scaled by its bucket's q 2^b. grid (kb cap, row blocks);
+// blocks past the used k blocks return.
+template <typename TJ>
+__global__ void __launch_bounds__(256) prep_jones_i8_kernel(
+        const TJ* __restrict__ jones, int num_src, int num_st,
+        const TJ* __restrict__ I, const TJ* __restrict__ Q,
+        const TJ* __restrict__ U, const TJ* __restrict__ V,
+        const unsigned int* __restrict__ maxabs_bits, const I8Order o,
+        uint8_t* W)
+{
+    const int kb = blockIdx.x, rb = blockIdx.y, nkb_cap = gridDim.x;
+    if (kb >= o.counts[0]) return;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int s = o.perm[kb * kSrcPerBlock + lane];
+    const bool src_ok = s >= 0;
+    float c11 = 0, c21r = 0, c21i = 0, c22 = 0;
+    if (src_ok) brightness_factor(I[s], Q[s], U[s], V[s], c11, c21r, c21i, c22);
+    const float q = scalbnf(i8_scale_from_bits(*maxabs_bits),
+            o.kb_bucket[kb]);
+    uint8_t* tile = W + (size_t) (rb * nkb_cap + kb) * kI8Block;
+    for (int pl = warp; pl < kStPerBlock; pl += 8)
+    {
+        const int p = rb * kStPerBlock + pl;
+        float A[2][2][2] = {{{0, 0}, {0, 0}}, {{0, 0}, {0, 0}}};
+        if (src_ok && p < num_st)
+        {
+            float J[8];
+            load_jones<TJ>(jones + 8 * ((size_t) p * num_src + s), J);
+            apply_factor(J, c11, c21r, c21i, c22, A);
+#pragma unroll
+            for (int k = 0; k < 8; ++k) (&A[0][0][0])[k] *= q;
+        }
+        store_entry_i8(tile, pl, lane, A);
     }
 }
 
@@ -400,16 +654,17 @@ __global__ void __launch_bounds__(256) prep_fused_i8_kernel(
         const double* __restrict__ Q, const double* __restrict__ U,
         const double* __restrict__ V, const double* __restrict__ uvw,
         const double* __restrict__ inv_wavelength, int nch, int p0, int np,
-        const unsigned int* __restrict__ maxabs_bits, uint8_t* W,
-        size_t image_stride)
+        const unsigned int* __restrict__ maxabs_bits, const I8Order o,
+        uint8_t* W, size_t image_stride)
 {
     // two blocks: the 48 KB of static shared memory a kernel may declare
     __shared__ __align__(128) uint8_t buf[2 * kI8Block];
     const int kb = blockIdx.x, rb = blockIdx.y;
     const int nkb = gridDim.x;
+    if (kb >= o.counts[0]) return;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    const int s = kb * kSrcPerBlock + lane;
-    const bool src_ok = s < num_src;
+    const int s = o.perm[kb * kSrcPerBlock + lane];
+    const bool src_ok = s >= 0;
     float c11 = 0, c21r = 0, c21i = 0, c22 = 0;
     double sl = 0, sm = 0, sn1 = 0;
     if (src_ok)
@@ -417,7 +672,8 @@ __global__ void __launch_bounds__(256) prep_fused_i8_kernel(
         brightness_factor(I[s], Q[s], U[s], V[s], c11, c21r, c21i, c22);
         sl = l[s]; sm = m[s]; sn1 = n[s] - 1.0;
     }
-    const float q = i8_scale_from_bits(*maxabs_bits);
+    const float q = scalbnf(i8_scale_from_bits(*maxabs_bits),
+            o.kb_bucket[kb]);
     float A0[4][2][2][2];
 #pragma unroll
     for (int k = 0; k < 4; ++k)
@@ -534,6 +790,12 @@ struct GemmParams
     double uv_min, uv_max;
     int casa;
     int i8;                     // operand image is the three-limb integer one
+    // integer image only: k blocks used (i8_counts[0]), chunks
+    // (i8_counts[1]) and the chunk table (I8Order); nkb is then the image's
+    // k-block capacity (its row-block stride)
+    const int* i8_counts;
+    const int* i8_chunk_kb;
+    const int* i8_chunk_bucket;
     int form;                   // Form (kFormDefault: the environment's)
     int* err;
     // Auto-correlations (optional): the diagonal station pairs of the
@@ -1576,25 +1838,30 @@ gemm_pair_kernel(const GemmParams prm, const __grid_constant__ CUtensorMap tmap)
 // a = a0 2^16 + a1 2^8 + a2 and b likewise,
 //     a b / 2^16 = a0 b0 2^16 + (a0 b1 + a1 b0) 2^8 + (a0 b2 + a1 b1 + a2 b0)
 //                  + (a1 b2 + a2 b1) 2^-8 + a2 b2 2^-16,
-// the last term (at most 2^-32 of the largest product, mean zero) left out:
-// eight 8-bit MMAs per 32-wide K step feed four S32 TMEM accumulators (D0 ..
-// D3, 128 columns each) of 128 x 128 tiles. The class a1 b2 + a2 b1 cannot be
-// left out too: its limbs are uniform digits whatever the entry's size, so
-// over many faint sources it would add ~1e-6 of the visibilities' L2 norm.
+// the last two classes left out: six 8-bit MMAs per 32-wide K step feed
+// three S32 TMEM accumulators (D0 .. D2, 128 columns each) of 128 x 128
+// tiles. The limbs are balanced digits (each in [-128, 127]), so the left-out
+// terms have mean zero and add at most 2^-23 of the largest product at
+// their k block's scale (|a1 b2 + a2 b1| 2^-8 <= 2^7 against 2^30). The
+// image orders the sources by amplitude bucket, each bucket with its own
+// scale q 2^b, so that bound follows every source's own size instead of
+// the brightest source's (without the buckets, a sky of many faint sources
+// would lose ~1e-6 of the visibilities' L2 norm to the uniform low digits
+// of its faint entries).
 // The integer sums are exact: no rounding happens in the tensor core, so
-// the accumulators only need draining before they could overflow (every
-// kI8DrainKb k blocks: one k block adds at most 3 x 64 x 2^14 < 2^21.6 to
-// |D2|, so 512 blocks stay below 2^31) and at the end of a task, where D0 2^16 + D1 2^8 + D2 + D3 2^-8 is
-// formed in FP64 and folded into the visibility sums. The error is that of
-// the fixed-point entries (2^-24 of the largest |entry|).
+// the accumulators only need draining before they could overflow (at most
+// kI8DrainKb k blocks per chunk: one k block adds at most 3 x 64 x 2^14 <
+// 2^21.6 to |D2|, so 512 blocks stay below 2^31), at the end of each bucket
+// (a chunk never spans two scales) and of a task, where
+// (D0 2^16 + D1 2^8 + D2) 2^-2b is formed in FP64 and folded into the
+// visibility sums.
 // Warp roles (320 threads): warp 0 producer (one bulk copy per operand per
 // k block into a kI8Stages-deep ring of 48 KB stages), warp 1 MMA issuer,
 // warps 2-9 epilogue (64 columns each, as the square FP16 kernel).
 // ===========================================================================
 constexpr int kI8Stages = 4;
 constexpr int kI8StageBytes = 2 * kI8Block;   // A block + B block
-constexpr int kI8DrainKb = 512;
-constexpr uint32_t kI8TmemCols = 512;         // D0, D1, D2, D3
+constexpr uint32_t kI8TmemCols = 512;         // D0, D1, D2 (+ 128 unused)
 
 struct I8Ctl
 {
@@ -1608,28 +1875,27 @@ constexpr size_t gemm_i8_smem_bytes()
     return 1024 + (size_t) kI8Stages * kI8StageBytes + sizeof(I8Ctl);
 }
 
-// One drain of the four integer accumulators over this thread's 64 columns
-// (taddr): D0 2^16 + D1 2^8 + D2 + D3 2^-8 per column, folded into the Re V
-// and Im V sums of its 16 column stations.
+// One drain of the three integer accumulators over this thread's 64
+// columns (taddr): (D0 2^16 + D1 2^8 + D2) scale per column (exact before
+// the scale, |.| < 2^48), folded into the Re V and Im V sums of its 16
+// column stations.
 __device__ __forceinline__ void i8_drain64(uint32_t taddr, int c,
-        double (&accR)[16], double (&accI)[16])
+        double scale, double (&accR)[16], double (&accI)[16])
 {
 #pragma unroll
     for (int j0 = 0; j0 < 64; j0 += 16)
     {
-        uint32_t v0[16], v1[16], v2[16], v3[16];
+        uint32_t v0[16], v1[16], v2[16];
         ptx::tmem_ld16(taddr + j0, v0);
         ptx::tmem_ld16(taddr + 128 + j0, v1);
         ptx::tmem_ld16(taddr + 256 + j0, v2);
-        ptx::tmem_ld16(taddr + 384 + j0, v3);
         ptx::tmem_ld_wait();
         double v[16];
 #pragma unroll
         for (int j = 0; j < 16; ++j)
             v[j] = ((double) (int) v0[j] * 65536.0 +
                     (double) (int) v1[j] * 256.0 +
-                    (double) (int) v2[j]) +
-                   (double) (int) v3[j] * 0.00390625;
+                    (double) (int) v2[j]) * scale;
         // Re V = G00 + G11, Im V = G10 - G01 across the row pair
         // (lanes l, l ^ 1), as the FP16 kernels fold
 #pragma unroll
@@ -1681,14 +1947,16 @@ gemm_i8_kernel(const GemmParams prm)
 
     const int ntile = prm.nrb * (prm.nrb + 1) / 2;
     const int ntasks = ntile * prm.num_problems;
-    const int nchunk = (prm.nkb + kI8DrainKb - 1) / kI8DrainKb;
+    const int nkb_used = prm.i8_counts[0];
+    const int nchunk = prm.i8_counts[1];
 
     if (warp == 0)
     {
         if (lane == 0)
         {
             // ---------------- producer: A block, then B block (not on
-            // diagonal tiles, whose B is A)
+            // diagonal tiles, whose B is A); the image's row blocks are
+            // prm.nkb (its capacity) apart, nkb_used of them filled
             int stage = 0;
             uint32_t phase = 0;
             uint32_t issued = 0, issued_par = 0;  // bit s: stage s
@@ -1700,7 +1968,7 @@ gemm_i8_kernel(const GemmParams prm)
                 tile_of(task - prob * ntile, rb, cb);
                 const bool diag = rb == cb;
                 const uint8_t* img = prm.W + (size_t) prob * prm.image_stride;
-                for (int kb = 0; kb < prm.nkb; ++kb)
+                for (int kb = 0; kb < nkb_used; ++kb)
                 {
                     if (!ptx::mbar_wait(&ctl->empty[stage], phase ^ 1,
                             prm.err, 31, abort))
@@ -1733,8 +2001,7 @@ gemm_i8_kernel(const GemmParams prm)
         {
             // ---------------- MMA issuer
             const uint32_t idesc = ptx::idesc_i8_s32(128, 128, true, true);
-            const uint32_t d0 = tmem, d1 = tmem + 128, d2 = tmem + 256,
-                    d3 = tmem + 384;
+            const uint32_t d0 = tmem, d1 = tmem + 128, d2 = tmem + 256;
             int stage = 0;
             uint32_t phase = 0, dpar = 0;
             bool ok = true;
@@ -1755,8 +2022,8 @@ gemm_i8_kernel(const GemmParams prm)
                         break;
                     }
                     ptx::tc_fence_after();
-                    const int kb0 = ch * kI8DrainKb;
-                    const int kb1 = min(prm.nkb, kb0 + kI8DrainKb);
+                    const int kb0 = prm.i8_chunk_kb[ch];
+                    const int kb1 = prm.i8_chunk_kb[ch + 1];
                     for (int kb = kb0; kb < kb1; ++kb)
                     {
                         if (!ptx::mbar_wait(&ctl->full[stage], phase, prm.err,
@@ -1791,10 +2058,8 @@ gemm_i8_kernel(const GemmParams prm)
                             ptx::mma_i8_col<1>(d1, a0, b1, idesc, acc);
                             ptx::mma_i8_col<2>(d2, a0, b2, idesc, acc);
                             ptx::mma_i8_col<0>(d1, a1, b0, idesc, 1u);
-                            ptx::mma_i8_col<1>(d2, a1, b1, idesc, 1u);
-                            ptx::mma_i8_col<2>(d3, a1, b2, idesc, acc);
-                            ptx::mma_i8_col<0>(d2, a2, b0, idesc, 1u);
-                            ptx::mma_i8_col<2>(d3, a2, b1, idesc, 1u);
+                            ptx::mma_i8_col<2>(d2, a1, b1, idesc, 1u);
+                            ptx::mma_i8(d2, a2, b0, idesc, 1u);
                         }
                         ptx::mma_commit(&ctl->empty[stage]);
                         if (++stage == kI8Stages) { stage = 0; phase ^= 1; }
@@ -1839,7 +2104,9 @@ gemm_i8_kernel(const GemmParams prm)
                     break;
                 }
                 ptx::tc_fence_after();
-                i8_drain64(taddr, c, accR, accI);
+                // the chunk's bucket b: its entries carry q 2^b each
+                i8_drain64(taddr, c, ldexp(1.0, -2 * prm.i8_chunk_bucket[ch]),
+                        accR, accI);
                 ptx::tc_fence_before();
                 __syncwarp();
                 if (lane == 0) ptx::mbar_arrive(&ctl->dempty);
@@ -1858,284 +2125,6 @@ gemm_i8_kernel(const GemmParams prm)
     __syncthreads();
     ptx::tc_fence_after();
     if (warp == 1) ptx::tmem_dealloc(tmem, kI8TmemCols);
-}
-
-// ===========================================================================
-// Integer contraction on CTA pairs (cta_group::2): one task is the 256 x
-// 128 tile of G of row blocks 2 ti and 2 ti + 1 (one per CTA) against
-// column block cb (cb >= 2 ti). Each CTA brings its own row block's three
-// limb tiles (A, 24 KB per k block) and half of the column block's (64 of
-// its 128 rows, 12 KB), so a product moves 36 KB per CTA through shared
-// memory where the square kernel moves 48 KB; per 32-wide K step the MMAs
-// then read 6 KB of operands per CTA instead of 8 KB. Shared-memory
-// bandwidth was the suspected bound of the square kernel's tensor pipe (its
-// MMAs alone read 128 bytes per cycle at the full 8-bit rate), but the
-// pairs measured slower (41.4 against 38.6 ms at 512 stations x 100,000
-// sources x 16 channels), so they are opt-in (OSKB_TC_PAIR=1). Each CTA's
-// TMEM holds the four accumulators of its 128 rows (128 columns each).
-// Synchronisation between the two CTAs is that of gemm_pair_kernel:
-// tensor-map copies (cta_group::2 form, no multicast) counted on the even
-// CTA's full barrier, multicast commits for empty / dfull, the epilogue
-// warps of both CTAs arriving on the even CTA's dempty.
-// ===========================================================================
-constexpr int kPI8Half = 3 * 64 * 64;                 // B half: 3 x 64 rows
-constexpr int kPI8StageBytes = kI8Block + kPI8Half;   // 36 KB
-constexpr int kPI8Stages = 6;
-
-struct PairI8Ctl
-{
-    uint64_t full[kPI8Stages], empty[kPI8Stages], dfull, dempty, done;
-    uint32_t tmem_base;
-    int abort;
-};
-
-constexpr size_t gemm_pair_i8_smem_bytes()
-{
-    return 1024 + (size_t) kPI8Stages * kPI8StageBytes + sizeof(PairI8Ctl);
-}
-
-__host__ __device__ inline int pair_i8_tiles(int nrb)
-{
-    int n = 0;
-    for (int ti = 0; 2 * ti < nrb; ++ti) n += nrb - 2 * ti;
-    return n;
-}
-
-// Task t of one problem -> (ti, cb), cb = 2 ti .. nrb - 1 for each ti.
-__device__ __forceinline__ void pair_i8_tile_of(int t, int nrb, int& ti,
-        int& cb)
-{
-    ti = 0;
-    while (t >= nrb - 2 * ti)
-    {
-        t -= nrb - 2 * ti;
-        ++ti;
-    }
-    cb = 2 * ti + t;
-}
-
-__global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kGemmThreads, 1)
-gemm_pair_i8_kernel(const GemmParams prm,
-        const __grid_constant__ CUtensorMap tmap_a,
-        const __grid_constant__ CUtensorMap tmap_b)
-{
-    extern __shared__ uint8_t smem_raw[];
-    uint8_t* smem = reinterpret_cast<uint8_t*>(
-            (reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~(uintptr_t) 1023);
-    PairI8Ctl* ctl = reinterpret_cast<PairI8Ctl*>(
-            smem + kPI8Stages * kPI8StageBytes);
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const uint32_t rank = ptx::cluster_ctarank();
-    volatile int* abort = &ctl->abort;
-
-    if (threadIdx.x == 0)
-    {
-        for (int s = 0; s < kPI8Stages; ++s)
-        {
-            ptx::mbar_init(&ctl->full[s], 1);
-            ptx::mbar_init(&ctl->empty[s], 1);
-        }
-        ptx::mbar_init(&ctl->dfull, 1);
-        ptx::mbar_init(&ctl->dempty, 16);
-        ptx::mbar_init(&ctl->done, 1);
-        ctl->abort = 0;
-        ptx::fence_mbar_init();
-    }
-    if (warp == 1) ptx::tmem_alloc_pair(&ctl->tmem_base, kI8TmemCols);
-    ptx::tc_fence_before();
-    // both CTAs' barriers initialised and TMEM allocated before any
-    // cross-CTA arrive or MMA
-    ptx::cluster_sync();
-    ptx::tc_fence_after();
-    const uint32_t tmem = ctl->tmem_base;
-
-    const int ntile = pair_i8_tiles(prm.nrb);
-    const int npairs = gridDim.x >> 1;
-    const int pair = blockIdx.x >> 1;
-    const int ntasks = ntile * prm.num_problems;
-    const int nchunk = (prm.nkb + kI8DrainKb - 1) / kI8DrainKb;
-    // limb tiles (8 KB each) per problem image
-    const long long tiles_per_prob = (long long) (prm.image_stride / kI8Tile);
-
-    if (warp == 0)
-    {
-        if (lane == 0)
-        {
-            // ---------------- producer: this CTA's row block (three limb
-            // tiles) and its half of the column block's, counted on the
-            // even CTA's full barrier
-            const uint32_t full0 = ptx::mapa_shared(
-                    ptx::smem_u32(&ctl->full[0]), 0);
-            int stage = 0;
-            uint32_t phase = 0;
-            uint32_t issued = 0, issued_par = 0;
-            for (int task = pair; task < ntasks && !*abort; task += npairs)
-            {
-                const int prob = task / ntile;
-                int ti, cb;
-                pair_i8_tile_of(task - prob * ntile, prm.nrb, ti, cb);
-                // a missing odd row block repeats the last one; its rows are
-                // discarded (p >= N)
-                int rb = 2 * ti + (int) rank;
-                if (rb >= prm.nrb) rb = prm.nrb - 1;
-                const long long t0 = (long long) prob * tiles_per_prob;
-                for (int kb = 0; kb < prm.nkb; ++kb)
-                {
-                    if (!ptx::mbar_wait(&ctl->empty[stage], phase ^ 1,
-                            prm.err, 41, abort))
-                        break;
-                    uint8_t* dst = smem + (size_t) stage * kPI8StageBytes;
-                    if (rank == 0)
-                        ptx::mbar_arrive_expect_tx(&ctl->full[stage],
-                                2 * kPI8StageBytes);
-                    const uint32_t bar = full0 +
-                            (uint32_t) (stage * sizeof(uint64_t));
-                    ptx::tma_load_3d_pair(dst, &tmap_a, 0, 0, (int) (t0 +
-                            3 * ((long long) rb * prm.nkb + kb)), bar);
-                    ptx::tma_load_3d_pair(dst + kI8Block, &tmap_b, 0,
-                            64 * (int) rank, (int) (t0 +
-                            3 * ((long long) cb * prm.nkb + kb)), bar);
-                    issued |= 1u << stage;
-                    issued_par = (issued_par & ~(1u << stage)) |
-                            (phase << stage);
-                    if (++stage == kPI8Stages) { stage = 0; phase ^= 1; }
-                }
-            }
-            // the even CTA's full barrier counts both CTAs' copies: its
-            // producer waits for every stage's last phase before the CTAs
-            // can leave
-            if (rank == 0)
-                for (int s = 0; s < kPI8Stages; ++s)
-                    if ((issued >> s) & 1)
-                        ptx::mbar_wait(&ctl->full[s], (issued_par >> s) & 1,
-                                prm.err, 42, abort);
-        }
-        __syncwarp();
-    }
-    else if (warp == 1)
-    {
-        if (lane == 0 && rank == 0)
-        {
-            // ---------------- MMA issuer (even CTA only)
-            const uint32_t idesc = ptx::idesc_i8_s32(256, 128, true, true);
-            const uint32_t d0 = tmem, d1 = tmem + 128, d2 = tmem + 256,
-                    d3 = tmem + 384;
-            int stage = 0;
-            uint32_t phase = 0, dpar = 0;
-            bool ok = true;
-            for (int task = pair; task < ntasks && ok; task += npairs)
-            {
-                for (int ch = 0; ch < nchunk && ok; ++ch)
-                {
-                    if (!ptx::mbar_wait_cluster(&ctl->dempty, dpar ^ 1,
-                            prm.err, 43, abort))
-                    {
-                        ok = false;
-                        break;
-                    }
-                    ptx::tc_fence_after();
-                    const int kb0 = ch * kI8DrainKb;
-                    const int kb1 = min(prm.nkb, kb0 + kI8DrainKb);
-                    for (int kb = kb0; kb < kb1; ++kb)
-                    {
-                        if (!ptx::mbar_wait_cluster(&ctl->full[stage], phase,
-                                prm.err, 44, abort))
-                        {
-                            ok = false;
-                            break;
-                        }
-                        ptx::tc_fence_after();
-                        const uint32_t a = ptx::smem_u32(smem +
-                                (size_t) stage * kPI8StageBytes);
-                        const uint32_t b = a + kI8Block;
-#pragma unroll
-                        for (int k = 0; k < 2; ++k)
-                        {
-                            const uint64_t a0 = ptx::sdesc_sw64(a + 32 * k);
-                            const uint64_t a1 = ptx::sdesc_sw64(
-                                    a + kI8Tile + 32 * k);
-                            const uint64_t a2 = ptx::sdesc_sw64(
-                                    a + 2 * kI8Tile + 32 * k);
-                            const uint64_t b0 = ptx::sdesc_sw64(b + 32 * k);
-                            const uint64_t b1 = ptx::sdesc_sw64(
-                                    b + 4096 + 32 * k);
-                            const uint64_t b2 = ptx::sdesc_sw64(
-                                    b + 8192 + 32 * k);
-                            const uint32_t acc =
-                                    (kb > kb0 || k > 0) ? 1u : 0u;
-                            ptx::mma_i8_pair(d0, a0, b0, idesc, acc);
-                            ptx::mma_i8_pair(d1, a0, b1, idesc, acc);
-                            ptx::mma_i8_pair(d1, a1, b0, idesc, 1u);
-                            ptx::mma_i8_pair(d2, a0, b2, idesc, acc);
-                            ptx::mma_i8_pair(d2, a1, b1, idesc, 1u);
-                            ptx::mma_i8_pair(d2, a2, b0, idesc, 1u);
-                            ptx::mma_i8_pair(d3, a1, b2, idesc, acc);
-                            ptx::mma_i8_pair(d3, a2, b1, idesc, 1u);
-                        }
-                        ptx::mma_commit_pair(&ctl->empty[stage]);
-                        if (++stage == kPI8Stages) { stage = 0; phase ^= 1; }
-                    }
-                    if (!ok) break;
-                    ptx::mma_commit_pair(&ctl->dfull);
-                    dpar ^= 1;
-                }
-            }
-            // every tcgen05 instruction of this kernel is cta_group::2
-            ptx::mma_commit_pair(&ctl->done);
-            ptx::mbar_wait(&ctl->done, 0, prm.err, 45, abort);
-        }
-        __syncwarp();
-    }
-    else
-    {
-        // ---------------- epilogue: 8 warps, 64 columns each
-        const int q4 = warp & 3;          // TMEM lane quadrant of this warp
-        const int h = (warp - 2) >> 2;    // column half
-        const int row = 32 * q4 + lane;   // row of this CTA's 128
-        const int c = row & 1;
-        const uint32_t taddr = tmem + ((uint32_t) (32 * q4) << 16) +
-                (uint32_t) (64 * h);
-        const uint32_t dempty0 = ptx::mapa_shared(
-                ptx::smem_u32(&ctl->dempty), 0);
-        uint32_t dpar = 0;
-        bool ok = true;
-        for (int task = pair; task < ntasks && ok; task += npairs)
-        {
-            const int prob = task / ntile;
-            int ti, cb;
-            pair_i8_tile_of(task - prob * ntile, prm.nrb, ti, cb);
-            double accR[16], accI[16];
-#pragma unroll
-            for (int j = 0; j < 16; ++j) accR[j] = accI[j] = 0.0;
-            for (int ch = 0; ch < nchunk; ++ch)
-            {
-                if (!ptx::mbar_wait(&ctl->dfull, dpar, prm.err, 46, abort))
-                {
-                    ok = false;
-                    break;
-                }
-                ptx::tc_fence_after();
-                i8_drain64(taddr, c, accR, accI);
-                ptx::tc_fence_before();
-                __syncwarp();
-                if (lane == 0) ptx::mbar_arrive_cluster(dempty0);
-                dpar ^= 1;
-            }
-            if (!ok) break;
-            const int g = prm.prob0 + prob;
-            const double q = (double) i8_scale_from_bits(
-                    prm.maxabs_bits[prm.maxabs_stride * g]);
-            square_task_store(prm, accR, accI, 65536.0 / (q * q), row, h,
-                    prob, 2 * ti + (int) rank, cb);
-        }
-    }
-
-    ptx::tc_fence_before();
-    // no CTA leaves (or frees TMEM) while its peer may still arrive on its
-    // barriers or its MMAs read the other's shared memory
-    ptx::cluster_sync();
-    ptx::tc_fence_after();
-    if (warp == 1) ptx::tmem_dealloc_pair(tmem, kI8TmemCols);
 }
 
 }  // namespace tc
@@ -2316,10 +2305,7 @@ int device_setup(bool& wide_fits, bool& pair_fits)
                 (int) gemm_pair_smem_bytes()) != cudaSuccess ||
                 cudaFuncSetAttribute(gemm_i8_kernel,
                 cudaFuncAttributeMaxDynamicSharedMemorySize,
-                (int) gemm_i8_smem_bytes()) != cudaSuccess ||
-                cudaFuncSetAttribute(gemm_pair_i8_kernel,
-                cudaFuncAttributeMaxDynamicSharedMemorySize,
-                (int) gemm_pair_i8_smem_bytes()) != cudaSuccess)
+                (int) gemm_i8_smem_bytes()) != cudaSuccess)
         {
             set_last_error("tc gemm attributes", cudaGetLastError());
             return OSKB_ERR_KERNEL_LAUNCH_FAILURE;
@@ -2401,52 +2387,8 @@ int launch_gemm(GemmParams& gp, cudaStream_t stream)
             gp.num_problems;
     if (gp.i8)
     {
-        // square tiles; CTA pairs on request (OSKB_TC_PAIR=1): at 512
-        // stations x 100,000 sources x 16 channels on one B200 the pairs
-        // took 41.4 ms per launch against 38.6 ms for the square tiles (the
-        // same bits: the sums are exact)
-        const long long pair_n = (long long) pair_i8_tiles(gp.nrb) *
-                gp.num_problems;
-        const char* pe = getenv("OSKB_TC_PAIR");
-        const bool use_pair = gp.form ? gp.form == kFormI8Pair :
-                (pe && atoi(pe) != 0);
+        // square tiles (the integer image's only shape)
         g_last_arith.store(8);
-        if (use_pair)
-        {
-            const size_t bytes = gp.image_stride ?
-                    gp.image_stride * (size_t) gp.num_problems :
-                    (size_t) gp.nrb * gp.nkb * kI8Block;
-            CUtensorMap ta, tb;
-            const cuuint64_t gdim[3] = {8, 128, bytes / kI8Tile};
-            const cuuint64_t gstride[2] = {64, kI8Tile};
-            const cuuint32_t box_a[3] = {8, 128, 3};
-            const cuuint32_t box_b[3] = {8, 64, 3};
-            const cuuint32_t estride[3] = {1, 1, 1};
-            EncodeTiledFn encode = encode_tiled_fn();
-            if (!encode || bytes / kI8Tile >= (1ull << 31) ||
-                    encode(&ta, CU_TENSOR_MAP_DATA_TYPE_UINT64, 3,
-                    (void*) gp.W, gdim, gstride, box_a, estride,
-                    CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
-                    CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
-                    CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS ||
-                    encode(&tb, CU_TENSOR_MAP_DATA_TYPE_UINT64, 3,
-                    (void*) gp.W, gdim, gstride, box_b, estride,
-                    CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
-                    CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
-                    CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
-            {
-                set_last_error_msg("tc: integer operand tensor maps");
-                return OSKB_ERR_KERNEL_LAUNCH_FAILURE;
-            }
-            const int pairs = num_sms() / 2;
-            const int grid = 2 * (int) (pair_n < pairs ? pair_n : pairs);
-            g_last_tile.store(256);
-            cudaEvent_t ev_stop = timing_start(stream);
-            gemm_pair_i8_kernel<<<grid, kGemmThreads,
-                    gemm_pair_i8_smem_bytes(), stream>>>(gp, ta, tb);
-            if (ev_stop) cudaEventRecord(ev_stop, stream);
-            return check_launch("tc gemm (integer, pairs)");
-        }
         const int grid = (int) (square < num_sms() ? square : num_sms());
         g_last_tile.store(128);
         cudaEvent_t ev_stop = timing_start(stream);
@@ -2512,6 +2454,118 @@ int launch_gemm(GemmParams& gp, cudaStream_t stream)
     return check_launch("tc gemm");
 }
 
+// Workspace layout: the Header, then (integer form) the source-order tables
+// (I8Order), then the operand images.
+size_t tables_bytes_for(bool i8, int num_src)
+{
+    return i8 ? i8_order_bytes(num_src, nullptr, nullptr) : 0;
+}
+
+// Workspace bytes of np problems' images that suit either form.
+size_t workspace_bytes_any(int num_st, int num_src, int np)
+{
+    const size_t f16 = (size_t) np * image_bytes(num_st, num_src);
+    const size_t i8 = tables_bytes_for(true, num_src) +
+            (size_t) np * image_bytes_i8(num_st, num_src);
+    return kHeaderBytes + (f16 > i8 ? f16 : i8);
+}
+
+// The integer image's scale, buckets and source order for a J (or E) block
+// of num_st x num_src ([station][source][2x2], shared by all problems):
+// per-source and overall largest |entry| of J C, then the order tables.
+template <typename TJ>
+int i8_order(const TJ* jones, int num_src, int num_st, const double* I,
+        const double* Q, const double* U, const double* V, Header* hdr,
+        const I8Order& o, cudaStream_t s)
+{
+    if (cudaMemsetAsync(o.amp_bits, 0, sizeof(unsigned int) * num_src, s) !=
+            cudaSuccess)
+    {
+        set_last_error("tc source order clear", cudaGetLastError());
+        return OSKB_ERR_KERNEL_LAUNCH_FAILURE;
+    }
+    const int gx = (num_src + 255) / 256;
+    int gy = (4 * num_sms() + gx - 1) / gx;
+    if (gy > num_st) gy = num_st;
+    if (gy < 1) gy = 1;
+    maxabs_src_kernel<TJ, double><<<dim3(gx, gy), 256, 0, s>>>(jones,
+            num_src, num_st, I, Q, U, V, o.amp_bits, &hdr->maxabs_bits,
+            &hdr->flags);
+    int err = check_launch("tc source amplitudes");
+    if (err) return err;
+    i8_order_kernel<<<1, kOrderThreads, 0, s>>>(num_src, &hdr->maxabs_bits,
+            o);
+    return check_launch("tc source order");
+}
+
+// One J block (oskb_cross_correlate_tc_d and the allocation-free entry
+// point): scale, operand image and contraction, in the workspace at ws
+// (the Header first; workspace_bytes_any(num_stations, num_sources, 1)
+// bytes).
+int jones_block(int casa, int num_sources, int num_stations, int offset_out,
+        const double* jones, const double* I, const double* Q,
+        const double* U, const double* V, const double* station_u,
+        const double* station_v, double uv_min_lambda, double uv_max_lambda,
+        double inv_wavelength, double* vis, uint8_t* ws, cudaStream_t s)
+{
+    Header* hdr = reinterpret_cast<Header*>(ws);
+    // the status words start at zero; the image is rewritten
+    if (cudaMemsetAsync(hdr, 0, sizeof(Header), s) != cudaSuccess)
+    {
+        set_last_error("tc header clear", cudaGetLastError());
+        return OSKB_ERR_KERNEL_LAUNCH_FAILURE;
+    }
+    const int nrb = (num_stations + kStPerBlock - 1) / kStPerBlock;
+    const int nkb = (num_sources + kSrcPerBlock - 1) / kSrcPerBlock;
+    const bool i8 = arith_i8();
+    GemmParams gp;
+    gp.i8 = i8;
+    gp.form = kFormDefault;
+    gp.i8_counts = gp.i8_chunk_kb = gp.i8_chunk_bucket = nullptr;
+    int err = 0;
+    if (i8)
+    {
+        I8Order o;
+        uint8_t* W = ws + kHeaderBytes +
+                i8_order_bytes(num_sources, ws + kHeaderBytes, &o);
+        if ((err = i8_order<double>(jones, num_sources, num_stations, I, Q,
+                U, V, hdr, o, s)))
+            return err;
+        const int cap = i8_kb_cap(num_sources);
+        prep_jones_i8_kernel<double><<<dim3(cap, nrb), 256, 0, s>>>(jones,
+                num_sources, num_stations, I, Q, U, V, &hdr->maxabs_bits, o,
+                W);
+        gp.W = W;
+        gp.nkb = cap;
+        gp.i8_counts = o.counts;
+        gp.i8_chunk_kb = o.chunk_kb;
+        gp.i8_chunk_bucket = o.chunk_bucket;
+    }
+    else
+    {
+        maxabs_kernel<double, double><<<num_sms() * 8, 256, 0, s>>>(jones,
+                num_sources, num_stations, I, Q, U, V, &hdr->maxabs_bits,
+                &hdr->flags);
+        if ((err = check_launch("tc maxabs"))) return err;
+        uint8_t* W = ws + kHeaderBytes;
+        prep_jones_kernel<double><<<dim3(nkb, nrb), 256, 0, s>>>(jones,
+                num_sources, num_stations, I, Q, U, V, &hdr->maxabs_bits, W);
+        gp.W = W;
+        gp.nkb = nkb;
+    }
+    if ((err = check_launch("tc prep"))) return err;
+    gp.image_stride = 0; gp.nrb = nrb;
+    gp.num_problems = 1; gp.num_st = num_stations;
+    gp.maxabs_bits = &hdr->maxabs_bits; gp.maxabs_stride = 0;
+    gp.prob0 = 0; gp.nch = 1;
+    gp.vis = vis; gp.vis_stride = 0; gp.offset_out = offset_out;
+    gp.st_u = station_u; gp.st_v = station_v; gp.uv_stride = 0;
+    gp.inv_wavelength = nullptr; gp.kw_scalar = inv_wavelength;
+    gp.uv_min = uv_min_lambda; gp.uv_max = uv_max_lambda;
+    gp.casa = casa; gp.err = &hdr->err; gp.autos = nullptr;
+    return launch_gemm(gp, s);
+}
+
 }  // namespace
 }  // namespace tc
 }  // namespace oskb
@@ -2525,7 +2579,7 @@ size_t oskb_cross_correlate_tc_workspace_bytes(int num_sources,
         int num_stations)
 {
     if (num_sources <= 0 || num_stations <= 0) return kHeaderBytes;
-    return kHeaderBytes + image_bytes(num_stations, num_sources);
+    return workspace_bytes_any(num_stations, num_sources, 1);
 }
 
 int oskb_cross_correlate_tc_d(int casa, int num_sources, int num_stations,
@@ -2544,37 +2598,9 @@ int oskb_cross_correlate_tc_d(int casa, int num_sources, int num_stations,
     cudaStream_t s = as_stream(stream);
     int err = get_workspace(workspace, workspace_bytes, need, s);
     if (err) return err;
-    Header* hdr = reinterpret_cast<Header*>(workspace);
-    uint8_t* W = reinterpret_cast<uint8_t*>(workspace) + kHeaderBytes;
-    cudaMemsetAsync(hdr, 0, sizeof(Header), s);
-    maxabs_kernel<double, double><<<num_sms() * 8, 256, 0, s>>>(jones,
-            num_sources, num_stations, I, Q, U, V, &hdr->maxabs_bits,
-            &hdr->flags);
-    if ((err = check_launch("tc maxabs"))) return err;
-    const int nrb = (num_stations + kStPerBlock - 1) / kStPerBlock;
-    const int nkb = (num_sources + kSrcPerBlock - 1) / kSrcPerBlock;
-    const bool i8 = arith_i8();
-    if (i8)
-        prep_jones_kernel<double, true><<<dim3(nkb, nrb), 256, 0, s>>>(jones,
-                num_sources, num_stations, I, Q, U, V, &hdr->maxabs_bits, W);
-    else
-        prep_jones_kernel<double, false><<<dim3(nkb, nrb), 256, 0, s>>>(
-                jones, num_sources, num_stations, I, Q, U, V,
-                &hdr->maxabs_bits, W);
-    if ((err = check_launch("tc prep"))) return err;
-    GemmParams gp;
-    gp.i8 = i8;
-    gp.form = kFormDefault;
-    gp.W = W; gp.image_stride = 0; gp.nrb = nrb; gp.nkb = nkb;
-    gp.num_problems = 1; gp.num_st = num_stations;
-    gp.maxabs_bits = &hdr->maxabs_bits; gp.maxabs_stride = 0;
-    gp.prob0 = 0; gp.nch = 1;
-    gp.vis = vis; gp.vis_stride = 0; gp.offset_out = offset_out;
-    gp.st_u = station_u; gp.st_v = station_v; gp.uv_stride = 0;
-    gp.inv_wavelength = nullptr; gp.kw_scalar = inv_wavelength;
-    gp.uv_min = uv_min_lambda; gp.uv_max = uv_max_lambda;
-    gp.casa = casa; gp.err = &hdr->err; gp.autos = nullptr;
-    return launch_gemm(gp, s);
+    return jones_block(casa, num_sources, num_stations, offset_out, jones, I,
+            Q, U, V, station_u, station_v, uv_min_lambda, uv_max_lambda,
+            inv_wavelength, vis, reinterpret_cast<uint8_t*>(workspace), s);
 }
 
 size_t oskb_correlate_block_tc_workspace_bytes(int num_sources,
@@ -2582,8 +2608,7 @@ size_t oskb_correlate_block_tc_workspace_bytes(int num_sources,
 {
     if (num_sources <= 0 || num_stations <= 0 || num_problems <= 0)
         return kHeaderBytes;
-    return kHeaderBytes + (size_t) num_problems *
-            image_bytes(num_stations, num_sources);
+    return workspace_bytes_any(num_stations, num_sources, num_problems);
 }
 
 int oskb_correlate_block_tc(int casa, int num_sources, int num_stations,
@@ -2653,14 +2678,15 @@ int correlate_block(int casa, int num_sources, int num_stations,
             !inv_wavelength || !vis)
         return OSKB_ERR_INVALID_ARGUMENT;
     // Problems (t, c) are processed in groups that fit the workspace.
-    const bool i8 = form ? form <= kFormI8Pair : arith_i8();
+    const bool i8 = form ? form == kFormI8 : arith_i8();
     const size_t img = image_bytes_for(i8, num_stations, num_sources);
+    const size_t tb = tables_bytes_for(i8, num_sources);
     int group = num_problems;
     if (workspace)
     {
-        if (workspace_bytes < kHeaderBytes + img)
+        if (workspace_bytes < kHeaderBytes + tb + img)
             return OSKB_ERR_MEMORY_ALLOC_FAILURE;
-        const size_t fit = (workspace_bytes - kHeaderBytes) / img;
+        const size_t fit = (workspace_bytes - kHeaderBytes - tb) / img;
         if ((size_t) group > fit) group = (int) fit;
     }
     else
@@ -2676,27 +2702,45 @@ int correlate_block(int casa, int num_sources, int num_stations,
     }
     cudaStream_t s = as_stream(stream);
     int err = get_workspace(workspace, workspace_bytes,
-            kHeaderBytes + (size_t) group * img, s);
+            kHeaderBytes + tb + (size_t) group * img, s);
     if (err) return err;
-    Header* hdr = reinterpret_cast<Header*>(workspace);
-    uint8_t* W = reinterpret_cast<uint8_t*>(workspace) + kHeaderBytes;
-    cudaMemsetAsync(hdr, 0, sizeof(Header), s);
-    // |K| = 1: one scale from E C serves every problem of the block.
-    maxabs_kernel<TE, double><<<num_sms() * 8, 256, 0, s>>>(E,
-            num_sources, num_stations, I, Q, U, V, &hdr->maxabs_bits,
-            &hdr->flags);
-    if ((err = check_launch("tc maxabs"))) return err;
+    uint8_t* ws = reinterpret_cast<uint8_t*>(workspace);
+    Header* hdr = reinterpret_cast<Header*>(ws);
+    uint8_t* W = ws + kHeaderBytes + tb;
+    if (cudaMemsetAsync(hdr, 0, sizeof(Header), s) != cudaSuccess)
+    {
+        set_last_error("tc header clear", cudaGetLastError());
+        return OSKB_ERR_KERNEL_LAUNCH_FAILURE;
+    }
+    // |K| = 1: one scale (and, for the integer image, one source order)
+    // from E C serves every problem of the block.
+    I8Order o = {};
+    if (i8)
+    {
+        i8_order_bytes(num_sources, ws + kHeaderBytes, &o);
+        if ((err = i8_order<TE>(E, num_sources, num_stations, I, Q, U, V,
+                hdr, o, s)))
+            return err;
+    }
+    else
+    {
+        maxabs_kernel<TE, double><<<num_sms() * 8, 256, 0, s>>>(E,
+                num_sources, num_stations, I, Q, U, V, &hdr->maxabs_bits,
+                &hdr->flags);
+        if ((err = check_launch("tc maxabs"))) return err;
+    }
     const int nrb = (num_stations + kStPerBlock - 1) / kStPerBlock;
     const int nkb = (num_sources + kSrcPerBlock - 1) / kSrcPerBlock;
+    const int cap = i8_kb_cap(num_sources);
     const size_t nbl = (size_t) num_stations * (num_stations - 1) / 2;
     for (int p0 = 0; p0 < num_problems; p0 += group)
     {
         const int np = min(group, num_problems - p0);
         if (i8)
-            prep_fused_i8_kernel<TE><<<dim3(nkb, nrb), 256, 0, s>>>(E,
+            prep_fused_i8_kernel<TE><<<dim3(cap, nrb), 256, 0, s>>>(E,
                     num_sources, num_stations,
                     l, m, n, I, Q, U, V, station_uvw, inv_wavelength,
-                    num_channels, p0, np, &hdr->maxabs_bits, W, img);
+                    num_channels, p0, np, &hdr->maxabs_bits, o, W, img);
         else
             prep_fused_kernel<TE><<<dim3(nkb, nrb), 256, 0, s>>>(E,
                     num_sources, num_stations, l, m, n, I, Q, U, V,
@@ -2705,8 +2749,12 @@ int correlate_block(int casa, int num_sources, int num_stations,
         if ((err = check_launch("tc prep fused"))) return err;
         GemmParams gp;
         gp.i8 = i8;
+        gp.i8_counts = o.counts;
+        gp.i8_chunk_kb = o.chunk_kb;
+        gp.i8_chunk_bucket = o.chunk_bucket;
         gp.form = form;
-        gp.W = W; gp.image_stride = img; gp.nrb = nrb; gp.nkb = nkb;
+        gp.W = W; gp.image_stride = img; gp.nrb = nrb;
+        gp.nkb = i8 ? cap : nkb;
         gp.num_problems = np; gp.num_st = num_stations;
         gp.maxabs_bits = &hdr->maxabs_bits; gp.maxabs_stride = 0;
         gp.prob0 = p0; gp.nch = num_channels;
@@ -2822,10 +2870,11 @@ namespace {
 // GPU that loads the library until the process exits. Beside a 256-byte
 // status header, the operand image needs 32 bytes per station-source in the
 // FP16 form (an FP16 hi and lo word for each of the 8 real parts of J C),
-// 24 in the integer form (three limbs each), rounded up to blocks of 32
-// stations x 32 sources; the size check uses the FP16 figure whichever form
-// runs: e.g. up to 512 stations x 4,064 sources per call (4,096 sources no
-// longer fit).
+// 24 in the integer form (three limbs each) plus its source-order tables
+// (about 8 bytes per source), rounded up to blocks of 32 stations x 32
+// sources (the integer form's buckets pad up to 15 more source blocks); the
+// size check takes the larger of the two whichever form runs: e.g. up to
+// 512 stations x 4,064 sources per call (4,096 sources no longer fit).
 constexpr size_t kStaticScratchBytes = (size_t) 64 << 20;
 
 static __device__ __align__(256) uint8_t g_static_scratch[kStaticScratchBytes];
@@ -2871,7 +2920,7 @@ extern "C" int oskb_cross_correlate_tc_noalloc_d(int casa, int num_sources,
     if (num_sources == 0 || num_stations < 2) return 0;
     if (!jones || !I || !Q || !U || !V || !station_u || !station_v || !vis)
         return OSKB_ERR_INVALID_ARGUMENT;
-    const size_t need = kHeaderBytes + image_bytes(num_stations, num_sources);
+    const size_t need = workspace_bytes_any(num_stations, num_sources, 1);
     if (need > kStaticScratchBytes)
     {
         char msg[200];
@@ -2885,44 +2934,12 @@ extern "C" int oskb_cross_correlate_tc_noalloc_d(int casa, int num_sources,
     void* scratch = nullptr;
     int err = static_scratch(&scratch);
     if (err) return err;
-    cudaStream_t s = as_stream(stream);
-    Header* hdr = reinterpret_cast<Header*>(scratch);
-    uint8_t* W = reinterpret_cast<uint8_t*>(scratch) + kHeaderBytes;
-    // The array keeps the previous call's contents: the status words must
-    // start at zero; the operand image is fully rewritten by the prep kernel.
-    if (cudaMemsetAsync(hdr, 0, sizeof(Header), s) != cudaSuccess)
-    {
-        set_last_error("static scratch clear", cudaGetLastError());
-        return OSKB_ERR_KERNEL_LAUNCH_FAILURE;
-    }
-    maxabs_kernel<double, double><<<num_sms() * 8, 256, 0, s>>>(jones,
-            num_sources, num_stations, I, Q, U, V, &hdr->maxabs_bits,
-            &hdr->flags);
-    if ((err = check_launch("tc maxabs (static scratch)"))) return err;
-    const int nrb = (num_stations + kStPerBlock - 1) / kStPerBlock;
-    const int nkb = (num_sources + kSrcPerBlock - 1) / kSrcPerBlock;
-    const bool i8 = arith_i8();
-    if (i8)
-        prep_jones_kernel<double, true><<<dim3(nkb, nrb), 256, 0, s>>>(jones,
-                num_sources, num_stations, I, Q, U, V, &hdr->maxabs_bits, W);
-    else
-        prep_jones_kernel<double, false><<<dim3(nkb, nrb), 256, 0, s>>>(
-                jones, num_sources, num_stations, I, Q, U, V,
-                &hdr->maxabs_bits, W);
-    if ((err = check_launch("tc prep (static scratch)"))) return err;
-    GemmParams gp;
-    gp.i8 = i8;
-    gp.form = kFormDefault;
-    gp.W = W; gp.image_stride = 0; gp.nrb = nrb; gp.nkb = nkb;
-    gp.num_problems = 1; gp.num_st = num_stations;
-    gp.maxabs_bits = &hdr->maxabs_bits; gp.maxabs_stride = 0;
-    gp.prob0 = 0; gp.nch = 1;
-    gp.vis = vis; gp.vis_stride = 0; gp.offset_out = offset_out;
-    gp.st_u = station_u; gp.st_v = station_v; gp.uv_stride = 0;
-    gp.inv_wavelength = nullptr; gp.kw_scalar = inv_wavelength;
-    gp.uv_min = uv_min_lambda; gp.uv_max = uv_max_lambda;
-    gp.casa = casa; gp.err = &hdr->err; gp.autos = nullptr;
-    return launch_gemm(gp, s);
+    // The array keeps the previous call's contents: the status words are
+    // cleared and the tables and operand image rewritten by the call.
+    return jones_block(casa, num_sources, num_stations, offset_out, jones, I,
+            Q, U, V, station_u, station_v, uv_min_lambda, uv_max_lambda,
+            inv_wavelength, vis, reinterpret_cast<uint8_t*>(scratch),
+            as_stream(stream));
 }
 
 // Status words of the last allocation-free call on the current device: the

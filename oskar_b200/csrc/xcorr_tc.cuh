@@ -7,12 +7,11 @@ namespace oskb {
 namespace tc {
 
 // Contraction forms; kFormDefault follows the environment (OSKB_TC_ARITH,
-// OSKB_TC_TILE, OSKB_TC_PAIR), the others fix the form.
+// OSKB_TC_TILE), the others fix the form (2 is not a form).
 enum Form
 {
     kFormDefault = 0,
     kFormI8 = 1,        // integer, 128 x 128 tiles
-    kFormI8Pair = 2,    // integer, 256 x 128 tiles on CTA pairs
     kFormF16 = 3,       // FP16 hi/lo, 128 x 128 tiles
     kFormF16Wide = 4,   // FP16 hi/lo, 128 x 256 tiles
     kFormF16Pair = 5    // FP16 hi/lo, 256 x 256 tiles on CTA pairs

@@ -3,9 +3,10 @@
 Both tensor-core forms must agree with the FP64 CPU oracle to
     L2 relative <= 1e-6  and  max |err| <= 1e-6 * max |V|
 on every test here (the stated tolerance of the compensated path):
-  - the integer form (the default): entries as 24-bit fixed point in three
-    signed 8-bit limbs, eight 8-bit MMAs per K step into exact 32-bit
-    integer accumulators, FP64 phase;
+  - the integer form (the default): sources ordered into amplitude buckets,
+    each with its own scale; entries as 24-bit fixed point in three signed
+    8-bit limbs, six 8-bit MMAs per K step into exact 32-bit integer
+    accumulators, FP64 phase;
   - the FP16 form (OSKB_TC_ARITH=fp16 or any OSKB_TC_TILE): FP16 hi/lo
     split, three products, FP32 accumulation drained to FP64, FP64 phase.
 Calls go through the C ABI with torch device buffers.
@@ -94,7 +95,75 @@ def test_tc_jones_api(nst, nsrc, casa):
     assert flags[0] == 0 and flags[1] == 0
 
 
-FORMS = ["fp16-128", "fp16-256", "fp16-512", "i8-128", "i8-pair"]
+def jones_case(rng, nst, nsrc, I, Q, U, V, l, m, n, casa=0):
+    """oskb_cross_correlate_tc_d against the oracle on one J block."""
+    u, v, w = stations(rng, nst)
+    J = rng.normal(0, 0.3, (nst, nsrc, 8))
+    J[..., 0] += 1
+    J[..., 6] += 1
+    J = J.ravel()
+    inv_wl = 110e6 / C0
+    ref = oracle_vis(nst, nsrc, J, I, Q, U, V, l, m, n, u, v, w, inv_wl,
+                     casa=casa)
+    nbl = nst * (nst - 1) // 2
+    vis = torch.zeros(8 * nbl, dtype=torch.float64, device="cuda")
+    ob.call("oskb_cross_correlate_tc_d", casa, nsrc, nst, 0, dev(J), dev(I),
+            dev(Q), dev(U), dev(V), dev(u), dev(v), 0.0, 3e38, inv_wl, vis,
+            None, 0, ob.stream_ptr())
+    torch.cuda.synchronize()
+    return vis.cpu().numpy(), ref
+
+
+@pytest.mark.parametrize("decades", [3, 6, 12])
+def test_tc_integer_dynamic_range(decades, monkeypatch):
+    """Fluxes log-uniform over 3, 6 and 12 decades (entries of J C scale as
+    the square root of the flux: up to 2^20 in amplitude, past the 16
+    buckets of the integer image), with some sources of zero flux: the
+    integer form's buckets keep every flux at full precision, the last
+    bucket takes all fainter sources."""
+    monkeypatch.delenv("OSKB_TC_TILE", raising=False)
+    monkeypatch.delenv("OSKB_TC_ARITH", raising=False)
+    rng = np.random.default_rng(700 + decades)
+    nsrc = 3000
+    l, m, n, I, Q, U, V = sky(rng, nsrc)
+    I = 10.0 ** rng.uniform(-decades, 0, nsrc)
+    Q, U, V = (I * rng.uniform(-0.1, 0.1, nsrc) for _ in range(3))
+    for a in (I, Q, U, V):
+        a[::97] = 0.0
+    got, ref = jones_case(rng, 40, nsrc, I, Q, U, V, l, m, n)
+    assert ob.load().oskb_tc_arithmetic() == 8
+    l2, mx = errors(got, ref)
+    assert l2 <= TOL and mx <= TOL, (l2, mx)
+
+
+def test_tc_integer_long_bucket(monkeypatch):
+    """20,000 sources of one flux (one bucket of 625 source blocks, so its
+    accumulators drain inside the bucket as well as at its end)."""
+    monkeypatch.delenv("OSKB_TC_TILE", raising=False)
+    monkeypatch.delenv("OSKB_TC_ARITH", raising=False)
+    rng = np.random.default_rng(71)
+    nsrc = 20000
+    l, m, n, I, Q, U, V = sky(rng, nsrc)
+    I = np.ones(nsrc)
+    Q = U = V = np.zeros(nsrc)
+    got, ref = jones_case(rng, 33, nsrc, I, Q, U, V, l, m, n, casa=1)
+    l2, mx = errors(got, ref)
+    assert l2 <= TOL and mx <= TOL, (l2, mx)
+
+
+def test_tc_integer_zero_sky(monkeypatch):
+    """All fluxes zero: zero visibilities, exactly."""
+    monkeypatch.delenv("OSKB_TC_TILE", raising=False)
+    monkeypatch.delenv("OSKB_TC_ARITH", raising=False)
+    rng = np.random.default_rng(72)
+    nsrc = 100
+    l, m, n, I, Q, U, V = sky(rng, nsrc)
+    z = np.zeros(nsrc)
+    got, _ = jones_case(rng, 9, nsrc, z, z, z, z, l, m, n)
+    assert not np.any(got)
+
+
+FORMS = ["fp16-128", "fp16-256", "fp16-512", "i8-128"]
 
 
 def set_form(monkeypatch, form):
@@ -103,13 +172,10 @@ def set_form(monkeypatch, form):
     if form.startswith("fp16"):
         tile = int(form.split("-")[1])
         monkeypatch.setenv("OSKB_TC_TILE", str(tile))
-        monkeypatch.delenv("OSKB_TC_PAIR", raising=False)
         return tile, 16
     monkeypatch.delenv("OSKB_TC_TILE", raising=False)
     monkeypatch.delenv("OSKB_TC_ARITH", raising=False)
-    pair = form == "i8-pair"
-    monkeypatch.setenv("OSKB_TC_PAIR", "1" if pair else "0")
-    return (256 if pair else 128), 8
+    return 128, 8
 
 
 @pytest.mark.parametrize("form", FORMS)

@@ -18,12 +18,11 @@ pytestmark = [pytest.mark.gpu,
 import oskar_b200 as ob  # noqa: E402
 from test_gpu_tc import sky, stations, C0  # noqa: E402
 
-# environment that makes the library default equal to plan form 1..5
-FORM_ENV = {1: {"OSKB_TC_PAIR": "0"}, 2: {"OSKB_TC_PAIR": "1"},
-            3: {"OSKB_TC_TILE": "128"}, 4: {"OSKB_TC_TILE": "256"},
+# environment that makes the library default equal to plan form 1, 3, 4, 5
+FORM_ENV = {1: {}, 3: {"OSKB_TC_TILE": "128"}, 4: {"OSKB_TC_TILE": "256"},
             5: {"OSKB_TC_TILE": "512"}}
-ENV_KEYS = ("OSKB_TC_PAIR", "OSKB_TC_TILE", "OSKB_TC_ARITH",
-            "OSKB_TC_PLAN_FORM", "OSKB_TC_PLAN_TUNE", "OSKB_TC_PLAN_GRAPH")
+ENV_KEYS = ("OSKB_TC_TILE", "OSKB_TC_ARITH", "OSKB_TC_PLAN_FORM",
+            "OSKB_TC_PLAN_TUNE", "OSKB_TC_PLAN_GRAPH")
 
 
 def make_case(seed=9, nst=97, nsrc=900, nt=3, nch=2, nblocks=3):
@@ -82,7 +81,7 @@ def run_direct(c, form, monkeypatch):
                 vis, None, 0, ob.stream_ptr())
         torch.cuda.synchronize()
         outs.append(vis.cpu().numpy())
-    assert ob.load().oskb_tc_arithmetic() == (8 if form <= 2 else 16)
+    assert ob.load().oskb_tc_arithmetic() == (8 if form == 1 else 16)
     return outs
 
 
@@ -91,7 +90,7 @@ def test_plan_tunes_and_replays_graphs(monkeypatch):
         monkeypatch.delenv(k, raising=False)
     c = make_case()
     outs, form, launches, ms = run_plan(c)
-    assert form in (1, 2, 4)
+    assert form in (1, 3, 4)
     assert all(t > 0 for t in ms), ms
     # slot 0 replays blocks 0 and 2, slot 1 block 1
     assert launches == 3, ob.load().oskb_last_error().decode()
@@ -100,7 +99,7 @@ def test_plan_tunes_and_replays_graphs(monkeypatch):
         assert np.array_equal(o, r)
 
 
-@pytest.mark.parametrize("form", [1, 2, 4])
+@pytest.mark.parametrize("form", [1, 3, 4])
 @pytest.mark.parametrize("graph", ["1", "0"])
 def test_plan_fixed_form(form, graph, monkeypatch):
     """A fixed form (no tuning), with and without graphs."""
