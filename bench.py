@@ -314,6 +314,10 @@ def run_ours(args):
     for i in range(args.warmup):
         step(dump(i))
     torch.cuda.synchronize()
+    if args.path == "tc" and ob.load().oskb_tc_arithmetic() == 8:
+        # the integer form adds the per-source amplitudes and the source
+        # order to scale, operand preparation and contraction
+        launches_per_step = 4
     barrier()
     torch.cuda.synchronize()
     clocks = ClockSampler(local)
@@ -548,9 +552,10 @@ def compare_direct(args, cfg, ob, torch, dev, E, l, m, n, I, Q, U, V,
 
 def run_e2e(args, cfg, ob, torch, E, world, rank):
     """Source-baselines per second through the pipelined host-buffer
-    entry point (oskb_tc_plan_*) with page-locked host buffers: a step is
-    one block of 8 dumps x 16 channels (the reference's default block
-    length); every block's E and station uvw are uploaded from host memory
+    entry point (oskb_tc_plan_*) with page-locked host buffers over the
+    whole observation (this rank's share of the dumps): a step is one block
+    of 8 dumps x 16 channels (the reference's default block length); every
+    block's E and station uvw are uploaded from host memory
     and its visibilities downloaded to host memory inside the timed region,
     the upload of block b + 1 overlapping the correlation of block b. The
     sky is uploaded once per plan, before the timed region (5.6 MB)."""
@@ -563,7 +568,8 @@ def run_e2e(args, cfg, ob, torch, E, world, rank):
     freqs = np.ascontiguousarray(cfg.freqs_hz, np.float64)
     visb = [torch.empty((nt, nch, nbl, 8), dtype=torch.float64).pin_memory()
             for _ in range(2)]
-    nblocks = max(2, args.steps // nt)
+    # the whole observation: this rank's share of the dumps, in blocks of 8
+    nblocks = max(2, -(-cfg.num_times // (nt * world)))
     uvws = [pin(np.stack([cfg.station_uvw((rank + (b * world) * nt + i)
                                           % cfg.num_times)
                           for i in range(nt)])) for b in range(nblocks)]

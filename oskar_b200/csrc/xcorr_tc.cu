@@ -647,7 +647,7 @@ __global__ void __launch_bounds__(256) prep_fused_kernel(
 // grid (k blocks, row blocks); 8 warps, warp = 4 stations, lane = source.
 // ---------------------------------------------------------------------------
 template <typename TE>
-__global__ void __launch_bounds__(256) prep_fused_i8_kernel(
+__global__ void __launch_bounds__(256, 4) prep_fused_i8_kernel(
         const TE* __restrict__ E, int num_src, int num_st,
         const double* __restrict__ l, const double* __restrict__ m,
         const double* __restrict__ n, const double* __restrict__ I,
@@ -692,6 +692,10 @@ __global__ void __launch_bounds__(256) prep_fused_i8_kernel(
         }
     }
     uint8_t* dst0 = W + (size_t) (rb * nkb + kb) * kI8Block;
+    // u l + v m + w (n - 1) of the thread's four stations at dump t_cur
+    // (the channels of one dump share it)
+    double base[4] = {0.0, 0.0, 0.0, 0.0};
+    int t_cur = -1;
     for (int j = 0; j < np; ++j)
     {
         uint8_t* b = buf + (size_t) (j & 1) * kI8Block;
@@ -702,7 +706,19 @@ __global__ void __launch_bounds__(256) prep_fused_i8_kernel(
             __syncthreads();
         }
         const int prob = p0 + j, t = prob / nch, c = prob - t * nch;
-        const double* pu = uvw + (size_t) t * 3 * num_st;
+        if (t != t_cur)
+        {
+            t_cur = t;
+            const double* pu = uvw + (size_t) t * 3 * num_st;
+#pragma unroll
+            for (int k = 0; k < 4; ++k)
+            {
+                const int p = rb * kStPerBlock + warp + 8 * k;
+                base[k] = (src_ok && p < num_st) ? pu[p] * sl +
+                        pu[num_st + p] * sm + pu[2 * num_st + p] * sn1 : 0.0;
+            }
+        }
+        const double kw = inv_wavelength[c];
 #pragma unroll
         for (int k = 0; k < 4; ++k)
         {
@@ -711,9 +727,7 @@ __global__ void __launch_bounds__(256) prep_fused_i8_kernel(
             float A[2][2][2] = {{{0, 0}, {0, 0}}, {{0, 0}, {0, 0}}};
             if (src_ok && p < num_st)
             {
-                const double x = (pu[p] * sl + pu[num_st + p] * sm +
-                                  pu[2 * num_st + p] * sn1) *
-                                 inv_wavelength[c];
+                const double x = base[k] * kw;
                 const float f = (float) (x - rint(x));
                 float sn, cs;
                 sincospif(2.0f * f, &sn, &cs);
