@@ -168,13 +168,23 @@ __device__ __forceinline__ float i8_scale_from_bits(unsigned int bits)
     return kI8Target / m;
 }
 
-// Bucket of a source whose largest |entry| is a, for the largest of all m:
-// floor(log2(m / a)) in [0, kI8Buckets - 1] (so a <= m 2^-b).
-__device__ __forceinline__ int i8_bucket(float a, float m)
+// Bucket of a source whose largest |entry| is a, for the largest of all m
+// (both as float bits): floor(log2(m / a)) in [0, kI8Buckets - 1] (so
+// a <= m 2^-b). For normal floats it is the exponent difference, less one
+// where a's significand exceeds m's (exact); zero sources go to the last
+// bucket.
+__device__ __forceinline__ int i8_bucket(unsigned int a_bits,
+        unsigned int m_bits)
 {
+    const float a = __uint_as_float(a_bits), m = __uint_as_float(m_bits);
     if (!(a > 0.0f) || !(m > 0.0f) || !isfinite(m))
         return a > 0.0f ? 0 : kI8Buckets - 1;
-    const int b = (int) floor(log2((double) m / (double) a));
+    const int ea = (int) (a_bits >> 23), em = (int) (m_bits >> 23);
+    int b;
+    if (ea > 0 && em > 0)
+        b = em - ea - ((m_bits & 0x7fffffu) < (a_bits & 0x7fffffu) ? 1 : 0);
+    else
+        b = (int) floor(log2((double) m / (double) a));
     return b < 0 ? 0 : (b >= kI8Buckets ? kI8Buckets - 1 : b);
 }
 
@@ -392,54 +402,45 @@ __global__ void __launch_bounds__(256) maxabs_src_kernel(
 }
 
 // ---------------------------------------------------------------------------
-// The integer image's source order (one CTA of kOrderThreads): each thread
-// takes a contiguous run of sources, counts them per bucket, the counts are
-// scanned over the threads per bucket (one warp per bucket), and every
-// source is written to its bucket's next position, so each bucket keeps the
-// sources in their original order (deterministic). Then the padding, the
-// bucket of every k block and the chunk table.
+// The integer image's source order (one CTA of kOrderThreads = 32 warps):
+// sources are taken kOrderThreads at a time in source order (coalesced).
+// Pass 1 counts the sources per bucket (the lanes of a warp that share a
+// bucket found with __match_any_sync, one shared-memory add per group);
+// then the bucket starts (each bucket padded to whole 32-source blocks),
+// the chunk table and the bucket of every k block. Pass 2 places every
+// source at its bucket's start plus the number of sources before it in the
+// same bucket (earlier rounds' running count, earlier warps of this round,
+// earlier lanes of its warp), so each bucket keeps the sources in their
+// original order (deterministic); then the padding.
 // ---------------------------------------------------------------------------
-constexpr int kOrderThreads = 512;
+constexpr int kOrderThreads = 1024;
 
 __global__ void __launch_bounds__(kOrderThreads) i8_order_kernel(
         int num_src, const unsigned int* __restrict__ maxabs_bits,
         I8Order o)
 {
-    __shared__ int cnt[kI8Buckets][kOrderThreads];
-    __shared__ int start[kI8Buckets + 1], total[kI8Buckets];
+    constexpr int kWarps = kOrderThreads / 32;
+    __shared__ int total[kI8Buckets], start[kI8Buckets + 1];
+    __shared__ int running[kI8Buckets];
+    __shared__ int wcnt[kWarps][kI8Buckets];
+    __shared__ int woff[kWarps][kI8Buckets];
     const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
-    const int run = (num_src + kOrderThreads - 1) / kOrderThreads;
-    const int s0 = min(num_src, t * run), s1 = min(num_src, s0 + run);
-    const float m = __uint_as_float(*maxabs_bits);
-    int c[kI8Buckets];
-#pragma unroll
-    for (int b = 0; b < kI8Buckets; ++b) c[b] = 0;
-    for (int s = s0; s < s1; ++s)
+    const unsigned int m_bits = *maxabs_bits;
+    const unsigned int lt = (1u << lane) - 1u;
+    if (t < kI8Buckets)
     {
-        const int b = i8_bucket(__uint_as_float(o.amp_bits[s]), m);
-#pragma unroll
-        for (int k = 0; k < kI8Buckets; ++k) c[k] += k == b;
+        total[t] = 0;
+        running[t] = 0;
     }
-#pragma unroll
-    for (int b = 0; b < kI8Buckets; ++b) cnt[b][t] = c[b];
     __syncthreads();
-    // exclusive scan of each bucket's counts over the threads
-    if (warp < kI8Buckets)
+    // ---- pass 1: bucket sizes
+    for (int s0 = 0; s0 < num_src; s0 += kOrderThreads)
     {
-        int running = 0;
-        for (int i = 0; i < kOrderThreads; i += 32)
-        {
-            const int v = cnt[warp][i + lane];
-            int incl = v;
-            for (int d = 1; d < 32; d <<= 1)
-            {
-                const int u = __shfl_up_sync(0xffffffffu, incl, d);
-                if (lane >= d) incl += u;
-            }
-            cnt[warp][i + lane] = running + incl - v;
-            running += __shfl_sync(0xffffffffu, incl, 31);
-        }
-        if (lane == 0) total[warp] = running;
+        const int s = s0 + t;
+        const int b = s < num_src ? i8_bucket(o.amp_bits[s], m_bits) : -1;
+        const unsigned int same = __match_any_sync(0xffffffffu, b);
+        if (b >= 0 && (same & lt) == 0)
+            atomicAdd(&total[b], __popc(same));
     }
     __syncthreads();
     if (t == 0)
@@ -463,19 +464,37 @@ __global__ void __launch_bounds__(kOrderThreads) i8_order_kernel(
         o.counts[1] = nchunk;
     }
     __syncthreads();
-    // scatter, in each bucket in source order
-#pragma unroll
-    for (int b = 0; b < kI8Buckets; ++b) c[b] = 0;
-    for (int s = s0; s < s1; ++s)
+    // ---- pass 2: positions, round by round in source order
+    for (int s0 = 0; s0 < num_src; s0 += kOrderThreads)
     {
-        const int b = i8_bucket(__uint_as_float(o.amp_bits[s]), m);
-        int pos = 0;
+        if (lane < kI8Buckets) wcnt[warp][lane] = 0;
+        __syncthreads();
+        const int s = s0 + t;
+        const int b = s < num_src ? i8_bucket(o.amp_bits[s], m_bits) : -1;
+        const unsigned int same = __match_any_sync(0xffffffffu, b);
+        if (b >= 0 && (same & lt) == 0) wcnt[warp][b] = __popc(same);
+        __syncthreads();
+        // warp k < kI8Buckets: exclusive scan of bucket k over the warps
+        if (warp < kI8Buckets)
+        {
+            const int v = wcnt[lane][warp];
+            int incl = v;
 #pragma unroll
-        for (int k = 0; k < kI8Buckets; ++k)
-            if (k == b) pos = start[k] + cnt[k][t] + c[k]++;
-        o.perm[pos] = s;
+            for (int d = 1; d < 32; d <<= 1)
+            {
+                const int u = __shfl_up_sync(0xffffffffu, incl, d);
+                if (lane >= d) incl += u;
+            }
+            const int base = running[warp];
+            woff[lane][warp] = base + incl - v;
+            __syncwarp();
+            if (lane == 31) running[warp] = base + incl;
+        }
+        __syncthreads();
+        if (b >= 0)
+            o.perm[start[b] + woff[warp][b] + __popc(same & lt)] = s;
     }
-    // padding and the bucket of every k block
+    // ---- padding and the bucket of every k block
     const int npos = start[kI8Buckets];
     for (int i = t; i < npos; i += kOrderThreads)
     {
