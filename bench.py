@@ -619,7 +619,10 @@ def run_profile_case(args):
       tc_pair_small the pair-tile contraction (gemm_pair_kernel, 256 x 256
                     tiles on CTA pairs) on the same case (288 pair tiles);
       tc_i8_small   the integer contraction (gemm_i8_kernel, the default)
-                    on the same case (1,088 square tiles);
+                    and its operand preparation (prep_fused_i8_kernel):
+                    512 stations x 10,000 sources x 4 channels (544 square
+                    tiles, 1/40 of a bench launch: enough sources that the
+                    amplitude buckets' chunks have their bench-size length);
       direct_small  the FP64 direct cross-correlation: 512 stations x 2,000
                     sources, 1 channel;
       beam_small    the fused station beam: 32 stations x 256 dipoles x
@@ -640,10 +643,10 @@ def run_profile_case(args):
     if case in ("tc_small", "tc_wide_small", "tc_pair_small", "tc_i8_small",
                 "direct_small"):
         nsrc = {"tc_small": 20_000, "tc_wide_small": 2_500,
-                "tc_pair_small": 2_500, "tc_i8_small": 2_500,
+                "tc_pair_small": 2_500, "tc_i8_small": 10_000,
                 "direct_small": 2_000}[case]
-        nch = 8 if case in ("tc_wide_small", "tc_pair_small",
-                            "tc_i8_small") else 1
+        nch = {"tc_wide_small": 8, "tc_pair_small": 8,
+               "tc_i8_small": 4}.get(case, 1)
         cfg = workloads.c3(num_src=nsrc, num_channels=nch, num_times=1)
         nst, nbl = cfg.num_st, cfg.num_baselines
         l, m, n, I, Q, U, V = (dev(x) for x in (cfg.l, cfg.m, cfg.n, cfg.I,
