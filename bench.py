@@ -433,6 +433,7 @@ def run_ours(args):
             "roofline": roof, "clocks": clk,
             "direct_fp64": cmp_["direct"],
             "direct_fp64_dmma": cmp_["direct_dmma"],
+            "fp64_class_tc64": cmp_["tc64"],
             "speedup_vs_direct_fp64": value / cmp_["direct"]["value"],
             "speedup_vs_direct_fp64_dmma":
                 value / cmp_["direct_dmma"]["value"],
@@ -503,9 +504,38 @@ def compare_direct(args, cfg, ob, torch, dev, E, l, m, n, I, Q, U, V,
             else:
                 os.environ["OSKB_XCORR_DMMA"] = old
 
+    def tc64(d, c, out):
+        u, v, w = uvw_all[d]
+        f = float(cfg.freqs_hz[c])
+        ob.call("oskb_cross_correlate_tc64_d", 0, nsrc, nst, 0, J, I, Q, U,
+                V, u, v, 0.0, 3e38, f / 299792458.0, out, None, 0, stream)
+
     join(0, 0)
     ms_simt = timed("0")
     ms_dmma = timed("1")
+    # the FP64-class integer tensor-core form on the same J, and its error
+    # against the FP64 direct (DMMA) result
+    v64 = torch.zeros((nbl, 8), dtype=torch.float64, device="cuda")
+    tc64(0, 0, v64)
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(3):
+        tc64(0, 0, v64)
+    e1.record()
+    torch.cuda.synchronize()
+    ms_tc64 = e0.elapsed_time(e1) / 3
+    v64.zero_()
+    tc64(0, 0, v64)
+    vd.zero_()
+    direct(0, 0)
+    torch.cuda.synchronize()
+    a64, b64 = v64.cpu().numpy(), vd.cpu().numpy()
+    err64 = {"l2": float(np.linalg.norm(a64 - b64) / np.linalg.norm(b64)),
+             "max_over_max": float(np.max(np.abs(a64 - b64)) /
+                                   np.max(np.abs(b64)))}
+    del v64
     # errors of the tensor-core block against the FP64 direct result
     worst_l2, worst_mx, cases = 0.0, 0.0, []
     dumps = (0, cfg.num_times - 1)
@@ -547,6 +577,13 @@ def compare_direct(args, cfg, ob, torch, dev, E, l, m, n, I, Q, U, V,
                                       "tensor pipe, DMMA; the default FP64 "
                                       "point-source kernel)",
                             "ms_per_channel": ms_dmma},
+            "tc64": {"value": sb / (ms_tc64 * 1e-3) / 1e9, "unit": UNIT,
+                     "kernel": "oskb gemm_l6_kernel (FP64-class: 48-bit "
+                               "fixed point in six 8-bit limbs on the "
+                               "integer tensor cores, "
+                               "oskb_cross_correlate_tc64_d)",
+                     "ms_per_channel": ms_tc64,
+                     "error_vs_fp64_direct": err64},
             "err": err}
 
 

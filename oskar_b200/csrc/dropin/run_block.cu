@@ -40,6 +40,7 @@
 #include <cuda_runtime.h>
 #include <math.h>
 #include <stdint.h>
+#include <stdlib.h>
 #include <string.h>
 
 #include <algorithm>
@@ -56,6 +57,19 @@
 namespace {
 
 constexpr double kC0 = 299792458.0;
+
+// FP64 point-source correlation without smearing on the FP64-class
+// integer tensor-core form (oskb_cross_correlate_tc64_d) unless the
+// environment variable OSKB_DROPIN_TC64 is 0 (then the FP64 direct
+// kernels, as for every other case).
+bool use_tc64()
+{
+    static const bool on = [] {
+        const char* e = getenv("OSKB_DROPIN_TC64");
+        return !(e && e[0] == '0');
+    }();
+    return on;
+}
 
 // ---------------------------------------------------------------- buffers
 struct DevBuf
@@ -96,6 +110,8 @@ struct State
     DevBuf uvw, uvw64, flux, E, R, K, J;
     // the block's visibilities
     DevBuf vis, autos;
+    // workspace of the FP64-class tensor-core correlation
+    DevBuf tc64ws;
     int* host_count = nullptr;   // page-locked: sources kept by the clip
 };
 
@@ -1071,7 +1087,44 @@ void Runner<T>::sim_baselines(const RefSky* sky, int num_src, const T* tab,
                 *eb = gaussian ? col(REF_SKY_SCRATCH_EXT_B) : nullptr,
                 *ec = gaussian ? col(REF_SKY_SCRATCH_EXT_C) : nullptr;
         const size_t out = (size_t) num_baselines() * offset;
-        if (dbl && matrix_)
+        // FP64 point sources without smearing: the FP64-class tensor-core
+        // form (the dispatcher's branch oskar_cross_correlate.c:434-455),
+        // unless a brightness matrix of the chunk is not positive
+        // semi-definite, which it reports having added nothing; then, and
+        // for every other case, the direct kernels
+        bool done = false;
+        if (dbl && matrix_ && !gaussian && frac_bw == 0.0 &&
+                time_avg == 0.0 && use_tc64())
+        {
+            check(st_->tc64ws.ensure(oskb_cross_correlate_tc64_workspace_bytes(
+                    num_src, num_st_)), "FP64-class correlation workspace");
+            if (!ok()) return;
+            err = oskb_cross_correlate_tc64_d(h_->casa_phase_convention,
+                    num_src, num_st_, (int) out, (const double*) EJ,
+                    (const double*) fI, (const double*) fQ,
+                    (const double*) fU, (const double*) fV,
+                    (const double*) u, (const double*) v, uv_min, uv_max,
+                    inv_wl, st_->vis.as<double>(), st_->tc64ws.p,
+                    st_->tc64ws.bytes, s_);
+            check(err, "cross-correlation (FP64-class tensor cores)");
+            if (!ok()) return;
+            int flags = 0, wait_error = 0;
+            check(cudaStreamSynchronize(s_) == cudaSuccess ?
+                    oskb_tc_status(st_->tc64ws.p, &flags, &wait_error) :
+                    REF_ERR_KERNEL_LAUNCH_FAILURE,
+                    "FP64-class correlation status");
+            if (!ok()) return;
+            if (wait_error)
+            {
+                fail(REF_ERR_KERNEL_LAUNCH_FAILURE, "FP64-class correlation: "
+                        "a bounded device-side wait expired");
+                return;
+            }
+            done = !(flags & 1);
+        }
+        if (done)
+            err = 0;
+        else if (dbl && matrix_)
             err = oskb_cross_correlate_d(h_->casa_phase_convention, gaussian,
                     num_src, num_st_, (int) out, (const double*) EJ,
                     (const double*) fI, (const double*) fQ,

@@ -106,10 +106,11 @@ __host__ __device__ inline size_t image_bytes_i8(int num_st, int num_src)
 }
 
 // The contraction's chunks (accumulator drain intervals): one or more per
-// bucket, at most kI8DrainKb k blocks each.
-__host__ __device__ inline int i8_max_chunks(int num_src)
+// bucket, at most drain_kb k blocks each (kI8DrainKb for the three-limb
+// image).
+__host__ __device__ inline int i8_max_chunks(int num_src, int drain_kb)
 {
-    return (i8_kb_cap(num_src) + kI8DrainKb - 1) / kI8DrainKb + kI8Buckets;
+    return (i8_kb_cap(num_src) + drain_kb - 1) / drain_kb + kI8Buckets;
 }
 
 // Source order and scales of one call (device, in the workspace before the
@@ -132,13 +133,13 @@ __host__ __device__ inline size_t align256_t(size_t b)
     return (b + 255) & ~(size_t) 255;
 }
 
-// Bytes of the tables for num_src sources; with base set, also their
-// addresses.
-__host__ __device__ inline size_t i8_order_bytes(int num_src, uint8_t* base,
-        I8Order* o)
+// Bytes of the tables for num_src sources and chunks of at most drain_kb
+// k blocks; with base set, also their addresses.
+__host__ __device__ inline size_t i8_order_bytes(int num_src, int drain_kb,
+        uint8_t* base, I8Order* o)
 {
     const size_t cap = (size_t) i8_kb_cap(num_src);
-    const size_t mc = (size_t) i8_max_chunks(num_src);
+    const size_t mc = (size_t) i8_max_chunks(num_src, drain_kb);
     size_t off = 0;
     const size_t sizes[6] = {align256_t(2 * sizeof(int)),
             align256_t((mc + 1) * sizeof(int)), align256_t(mc * sizeof(int)),
@@ -232,8 +233,9 @@ __device__ __forceinline__ uint32_t swz_offset(int r, int sl)
 // C = [[c11, 0], [c21, c22]], c11 and c22 real. Returns false when B is not
 // positive semi-definite (beyond rounding); C is then the factor of the
 // nearest PSD matrix with that diagonal clipped at zero.
+template <typename T>
 __device__ __forceinline__ bool brightness_factor(double I, double Q,
-        double U, double V, float& c11, float& c21r, float& c21i, float& c22)
+        double U, double V, T& c11, T& c21r, T& c21i, T& c22)
 {
     const double xx = I + Q, yy = I - Q;
     const double tol = 1e-12 * (fabs(I) + fabs(Q) + fabs(U) + fabs(V));
@@ -244,14 +246,14 @@ __device__ __forceinline__ bool brightness_factor(double I, double Q,
         const double br = U / a, bi = -V / a;
         const double d = yy - (br * br + bi * bi);
         if (d < -tol) ok = false;
-        c11 = (float) a; c21r = (float) br; c21i = (float) bi;
-        c22 = (float) sqrt(fmax(d, 0.0));
+        c11 = (T) a; c21r = (T) br; c21i = (T) bi;
+        c22 = (T) sqrt(fmax(d, 0.0));
     }
     else
     {
         if (xx < -tol || fabs(U) > tol || fabs(V) > tol) ok = false;
-        c11 = 0.0f; c21r = 0.0f; c21i = 0.0f;
-        c22 = (float) sqrt(fmax(yy, 0.0));
+        c11 = 0; c21r = 0; c21i = 0;
+        c22 = (T) sqrt(fmax(yy, 0.0));
     }
     return ok;
 }
@@ -416,8 +418,8 @@ __global__ void __launch_bounds__(256) maxabs_src_kernel(
 constexpr int kOrderThreads = 1024;
 
 __global__ void __launch_bounds__(kOrderThreads) i8_order_kernel(
-        int num_src, const unsigned int* __restrict__ maxabs_bits,
-        I8Order o)
+        int num_src, int drain_kb,
+        const unsigned int* __restrict__ maxabs_bits, I8Order o)
 {
     constexpr int kWarps = kOrderThreads / 32;
     __shared__ int total[kI8Buckets], start[kI8Buckets + 1];
@@ -453,7 +455,7 @@ __global__ void __launch_bounds__(kOrderThreads) i8_order_kernel(
         int nchunk = 0;
         for (int b = 0; b < kI8Buckets; ++b)
             for (int k = start[b] / kSrcPerBlock;
-                    k < start[b + 1] / kSrcPerBlock; k += kI8DrainKb)
+                    k < start[b + 1] / kSrcPerBlock; k += drain_kb)
             {
                 o.chunk_kb[nchunk] = k;
                 o.chunk_bucket[nchunk] = b;
@@ -830,6 +832,10 @@ struct GemmParams
     const int* i8_chunk_kb;
     const int* i8_chunk_bucket;
     int form;                   // Form (kFormDefault: the environment's)
+    // six-limb form only: when set and bit 0 of *skip_flags is set (a
+    // brightness matrix was not positive semi-definite), the contraction
+    // adds nothing
+    const int* skip_flags = nullptr;
     int* err;
     // Auto-correlations (optional): the diagonal station pairs of the
     // diagonal tiles, V_pp = J_p B J_p^H, added into
@@ -858,12 +864,13 @@ __device__ __forceinline__ void tile_of(int t, int& rb, int& cb)
     rb = t - c * (c + 1) / 2;
 }
 
-// Visibilities of one square (128 x 128) task from the FP64 sums of the
-// thread's 16 column stations: row `row` of row block rb against column
-// block cb, column half h; scaled by inv_s2.
-__device__ __forceinline__ void square_task_store(const GemmParams& prm,
-        const double (&accR)[16], const double (&accI)[16], double inv_s2,
-        int row, int h, int prob, int rb, int cb)
+// Visibilities of one task from the FP64 sums of the thread's NQ column
+// stations: row `row` of row block rb against column stations q_first ..
+// q_first + NQ - 1 of column block cb; scaled by inv_s2.
+template <int NQ>
+__device__ __forceinline__ void task_store(const GemmParams& prm,
+        const double (&accR)[NQ], const double (&accI)[NQ], double inv_s2,
+        int row, int q_first, int prob, int rb, int cb)
 {
     const int c = row & 1;
     const int g = prm.prob0 + prob, t = g / prm.nch;
@@ -879,10 +886,10 @@ __device__ __forceinline__ void square_task_store(const GemmParams& prm,
             (size_t) prm.offset_out);
     if (prm.autos && rb == cb && p < N)
     {
-        // column station q = p of this thread's 16: V_pp[i][c]
-        const int ql = p - cb * kStPerBlock - 16 * h;
+        // column station q = p of this thread's NQ: V_pp[i][c]
+        const int ql = p - cb * kStPerBlock - q_first;
 #pragma unroll
-        for (int k = 0; k < 16; ++k)
+        for (int k = 0; k < NQ; ++k)
             if (k == ql)
             {
                 double* o = prm.autos + 8 * ((size_t) g * N + p) +
@@ -892,9 +899,9 @@ __device__ __forceinline__ void square_task_store(const GemmParams& prm,
             }
     }
 #pragma unroll
-    for (int ql = 0; ql < 16; ++ql)
+    for (int ql = 0; ql < NQ; ++ql)
     {
-        const int q = cb * kStPerBlock + 16 * h + ql;
+        const int q = cb * kStPerBlock + q_first + ql;
         if (p < q && q < N)
         {
             const double uu = (su[p] - su[q]) * kw;
@@ -915,6 +922,15 @@ __device__ __forceinline__ void square_task_store(const GemmParams& prm,
             }
         }
     }
+}
+
+// task_store for a square (128 x 128) task: the thread's 16 column
+// stations of column half h.
+__device__ __forceinline__ void square_task_store(const GemmParams& prm,
+        const double (&accR)[16], const double (&accI)[16], double inv_s2,
+        int row, int h, int prob, int rb, int cb)
+{
+    task_store<16>(prm, accR, accI, inv_s2, row, 16 * h, prob, rb, cb);
 }
 
 __global__ void __launch_bounds__(kGemmThreads, 1)
@@ -2160,6 +2176,448 @@ gemm_i8_kernel(const GemmParams prm)
     if (warp == 1) ptx::tmem_dealloc(tmem, kI8TmemCols);
 }
 
+// ===========================================================================
+// FP64-class integer contraction (oskb_cross_correlate_tc64_d): the entries
+// of A = J C (FP64) as 48-bit fixed point, a = round(x q 2^b) with
+// q = 127 2^40 / max|A| and b the source's amplitude bucket, held as six
+// balanced 8-bit limbs a = sum_k a_k 2^(8 (5 - k)) (a_0 signed, a_1 .. a_5
+// in [-128, 127]). With b likewise,
+//     a b / 2^40 = sum_{i + j = c} a_i b_j 2^(8 (5 - c)),  c = 0 .. 10,
+// of which the classes c <= 5 (21 products) are kept: the rest add at most
+// ~2^-41 of the largest product at the block's scale. Tiles are 128 rows
+// x 64 columns (half of a column block) so that the six S32 accumulators
+// D0 .. D5 fit TMEM (64 columns each); 21 MMAs (M = 128, N = 64, K = 32)
+// per K step, A held in the collector buffer across its limb's products.
+// The accumulators are drained every kL6DrainKb k blocks (a k block adds at
+// most 6 x 64 x 2^14 < 2^22.6 to |D5|), at each bucket's end and at the
+// task's end: sum_c D_c 2^(8 (5 - c)) in FP64 (Horner), times 2^-2b.
+// Warp roles as gemm_i8_kernel; the epilogue warps take 32 columns each.
+// ===========================================================================
+constexpr int kL6Limbs = 6;
+constexpr int kL6Block = kL6Limbs * kI8Tile;        // 48 KB per k block
+constexpr int kL6HalfB = kL6Limbs * (kI8Tile / 2);  // 24 KB: 64 rows each
+constexpr int kL6StageBytes = kL6Block + kL6HalfB;  // 72 KB
+constexpr int kL6Stages = 3;
+constexpr int kL6DrainKb = 256;
+constexpr uint32_t kL6TmemCols = 512;               // D0 .. D5, 64 each
+constexpr double kL6Target = 127.0 * 1099511627776.0;   // 127 x 2^40
+
+__host__ __device__ inline size_t image_bytes_l6(int num_st, int num_src)
+{
+    const size_t nrb = (num_st + kStPerBlock - 1) / kStPerBlock;
+    return nrb * (size_t) i8_kb_cap(num_src) * kL6Block;
+}
+
+__device__ __forceinline__ double l6_scale_from_bits(unsigned int bits)
+{
+    const float m = __uint_as_float(bits);
+    if (!(m > 0.0f) || !isfinite(m)) return 1.0;
+    return kL6Target / (double) m;
+}
+
+// A = J C in FP64 (J row-major {a, b, c, d} complex, C lower triangular).
+__device__ __forceinline__ void apply_factor_d(const double* J, double c11,
+        double c21r, double c21i, double c22, double out[2][2][2])
+{
+#pragma unroll
+    for (int i = 0; i < 2; ++i)
+    {
+        const double j0r = J[4 * i + 0], j0i = J[4 * i + 1];
+        const double j1r = J[4 * i + 2], j1i = J[4 * i + 3];
+        out[i][0][0] = j0r * c11 + (j1r * c21r - j1i * c21i);
+        out[i][0][1] = j0i * c11 + (j1r * c21i + j1i * c21r);
+        out[i][1][0] = j1r * c22;
+        out[i][1][1] = j1i * c22;
+    }
+}
+
+// Writes one station-source's scaled 2x2 A as 4 rows of the six limb tiles
+// of its block: t = a + 0x8080808080, limb k = byte 5 - k of t (the low
+// limbs with their top bit flipped: balanced digits).
+__device__ __forceinline__ void store_entry_l6(uint8_t* block, int pl,
+        int sl, const double A[2][2][2])
+{
+#pragma unroll
+    for (int i = 0; i < 2; ++i)
+#pragma unroll
+        for (int c = 0; c < 2; ++c)
+        {
+            const int r = 4 * pl + 2 * i + c;
+            const long long t0 = __double2ll_rn(A[i][0][c]) +
+                    0x8080808080LL;
+            const long long t1 = __double2ll_rn(A[i][1][c]) +
+                    0x8080808080LL;
+            const uint32_t lo0 = (uint32_t) t0, hi0 = (uint32_t) (t0 >> 32);
+            const uint32_t lo1 = (uint32_t) t1, hi1 = (uint32_t) (t1 >> 32);
+            const uint32_t off = swz64_offset(r, 2 * sl);
+#pragma unroll
+            for (int limb = 0; limb < kL6Limbs; ++limb)
+            {
+                const int byte = 5 - limb;
+                const uint32_t v = byte >= 4 ?
+                        __byte_perm(hi0, hi1, (byte - 4) | ((byte) << 4)) :
+                        __byte_perm(lo0, lo1, byte | ((byte + 4) << 4));
+                *reinterpret_cast<uint16_t*>(block + limb * kI8Tile + off) =
+                        (uint16_t) (v ^ (limb ? 0x8080u : 0u));
+            }
+        }
+}
+
+// Six-limb image from joined Jones J (FP64): the sources in bucket order
+// (o.perm), each k block scaled by q 2^b of its bucket. grid (k-block
+// capacity, row blocks); blocks past the used k blocks return.
+__global__ void __launch_bounds__(256) prep_jones_l6_kernel(
+        const double* __restrict__ jones, int num_src, int num_st,
+        const double* __restrict__ I, const double* __restrict__ Q,
+        const double* __restrict__ U, const double* __restrict__ V,
+        const unsigned int* __restrict__ maxabs_bits, const I8Order o,
+        uint8_t* W)
+{
+    const int kb = blockIdx.x, rb = blockIdx.y, nkb_cap = gridDim.x;
+    if (kb >= o.counts[0]) return;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int s = o.perm[kb * kSrcPerBlock + lane];
+    const bool src_ok = s >= 0;
+    double c11 = 0, c21r = 0, c21i = 0, c22 = 0;
+    if (src_ok) brightness_factor(I[s], Q[s], U[s], V[s], c11, c21r, c21i, c22);
+    const double q = ldexp(l6_scale_from_bits(*maxabs_bits), o.kb_bucket[kb]);
+    uint8_t* blk = W + (size_t) (rb * nkb_cap + kb) * kL6Block;
+    for (int pl = warp; pl < kStPerBlock; pl += 8)
+    {
+        const int p = rb * kStPerBlock + pl;
+        double A[2][2][2] = {{{0, 0}, {0, 0}}, {{0, 0}, {0, 0}}};
+        if (src_ok && p < num_st)
+        {
+            const double2* jp = reinterpret_cast<const double2*>(
+                    jones + 8 * ((size_t) p * num_src + s));
+            double J[8];
+#pragma unroll
+            for (int k = 0; k < 4; ++k)
+            {
+                const double2 v = __ldg(jp + k);
+                J[2 * k] = v.x;
+                J[2 * k + 1] = v.y;
+            }
+            apply_factor_d(J, c11, c21r, c21i, c22, A);
+#pragma unroll
+            for (int k = 0; k < 8; ++k) (&A[0][0][0])[k] *= q;
+        }
+        store_entry_l6(blk, pl, lane, A);
+    }
+}
+
+struct L6Ctl
+{
+    uint64_t full[kL6Stages], empty[kL6Stages], dfull, dempty, done;
+    uint32_t tmem_base;
+    int abort;
+};
+
+constexpr size_t gemm_l6_smem_bytes()
+{
+    return 1024 + (size_t) kL6Stages * kL6StageBytes + sizeof(L6Ctl);
+}
+
+// One drain of the six accumulators over this thread's 32 columns (taddr,
+// 64 columns per accumulator): sum_c D_c 2^(8 (5 - c)) scale per column,
+// folded into the Re V and Im V sums of its 8 column stations.
+__device__ __forceinline__ void l6_drain32(uint32_t taddr, int c,
+        double scale, double (&accR)[8], double (&accI)[8])
+{
+#pragma unroll
+    for (int j0 = 0; j0 < 32; j0 += 16)
+    {
+        double v[16];
+        {
+            uint32_t u0[16], u1[16], u2[16];
+            ptx::tmem_ld16(taddr + j0, u0);
+            ptx::tmem_ld16(taddr + 64 + j0, u1);
+            ptx::tmem_ld16(taddr + 128 + j0, u2);
+            ptx::tmem_ld_wait();
+#pragma unroll
+            for (int j = 0; j < 16; ++j)
+                v[j] = ((double) (int) u0[j] * 256.0 + (double) (int) u1[j])
+                        * 256.0 + (double) (int) u2[j];
+        }
+        {
+            uint32_t u3[16], u4[16], u5[16];
+            ptx::tmem_ld16(taddr + 192 + j0, u3);
+            ptx::tmem_ld16(taddr + 256 + j0, u4);
+            ptx::tmem_ld16(taddr + 320 + j0, u5);
+            ptx::tmem_ld_wait();
+#pragma unroll
+            for (int j = 0; j < 16; ++j)
+                v[j] = (((v[j] * 256.0 + (double) (int) u3[j]) * 256.0 +
+                        (double) (int) u4[j]) * 256.0 +
+                        (double) (int) u5[j]) * scale;
+        }
+        // Re V = G00 + G11, Im V = G10 - G01 across the row pair
+        // (lanes l, l ^ 1), as i8_drain64
+#pragma unroll
+        for (int qq = 0; qq < 4; ++qq)
+        {
+            const int jb = 4 * qq;
+            const double s0 = c ? v[jb + 0] : v[jb + 2];
+            const double s1 = c ? v[jb + 1] : v[jb + 3];
+            const double r0 = __shfl_xor_sync(0xffffffffu, s0, 1);
+            const double r1 = __shfl_xor_sync(0xffffffffu, s1, 1);
+            const double g00 = c ? r0 : v[jb + 0];
+            const double g01 = c ? r1 : v[jb + 1];
+            const double g10 = c ? v[jb + 2] : r0;
+            const double g11 = c ? v[jb + 3] : r1;
+            accR[j0 / 4 + qq] += g00 + g11;
+            accI[j0 / 4 + qq] += g10 - g01;
+        }
+    }
+}
+
+// Tasks: (problem, square tile (rb <= cb), column half); 2 per tile.
+__global__ void __launch_bounds__(kGemmThreads, 1)
+gemm_l6_kernel(const GemmParams prm)
+{
+    // a brightness matrix that is not positive semi-definite: nothing is
+    // added (the caller correlates those sources another way)
+    if (prm.skip_flags && (*prm.skip_flags & 1)) return;
+    extern __shared__ uint8_t smem_raw[];
+    uint8_t* smem = reinterpret_cast<uint8_t*>(
+            (reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~(uintptr_t) 1023);
+    L6Ctl* ctl = reinterpret_cast<L6Ctl*>(smem + kL6Stages * kL6StageBytes);
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    volatile int* abort = &ctl->abort;
+
+    if (threadIdx.x == 0)
+    {
+        for (int s = 0; s < kL6Stages; ++s)
+        {
+            ptx::mbar_init(&ctl->full[s], 1);
+            ptx::mbar_init(&ctl->empty[s], 1);
+        }
+        ptx::mbar_init(&ctl->dfull, 1);
+        ptx::mbar_init(&ctl->dempty, 8);
+        ptx::mbar_init(&ctl->done, 1);
+        ctl->abort = 0;
+        ptx::fence_mbar_init();
+    }
+    if (warp == 1) ptx::tmem_alloc(&ctl->tmem_base, kL6TmemCols);
+    ptx::tc_fence_before();
+    __syncthreads();
+    ptx::tc_fence_after();
+    const uint32_t tmem = ctl->tmem_base;
+
+    const int ntile = prm.nrb * (prm.nrb + 1);     // two halves per tile
+    const int ntasks = ntile * prm.num_problems;
+    const int nkb_used = prm.i8_counts[0];
+    const int nchunk = prm.i8_counts[1];
+
+    if (warp == 0)
+    {
+        if (lane == 0)
+        {
+            // ---------------- producer: the row block's six limb tiles
+            // (one copy), then rows 64 h .. 64 h + 63 of the column
+            // block's (six copies; none on diagonal tiles, whose B rows
+            // are in A)
+            int stage = 0;
+            uint32_t phase = 0;
+            uint32_t issued = 0, issued_par = 0;  // bit s: stage s
+            for (int task = blockIdx.x; task < ntasks && !*abort;
+                    task += gridDim.x)
+            {
+                const int prob = task / ntile;
+                const int tt = task - prob * ntile;
+                const int half = tt & 1;
+                int rb, cb;
+                tile_of(tt >> 1, rb, cb);
+                const bool diag = rb == cb;
+                const uint8_t* img = prm.W + (size_t) prob * prm.image_stride;
+                for (int kb = 0; kb < nkb_used; ++kb)
+                {
+                    if (!ptx::mbar_wait(&ctl->empty[stage], phase ^ 1,
+                            prm.err, 51, abort))
+                        break;
+                    uint8_t* dst = smem + (size_t) stage * kL6StageBytes;
+                    ptx::mbar_arrive_expect_tx(&ctl->full[stage],
+                            diag ? kL6Block : kL6StageBytes);
+                    ptx::bulk_g2s(dst, img + ((size_t) rb * prm.nkb + kb) *
+                            kL6Block, kL6Block, &ctl->full[stage]);
+                    if (!diag)
+                    {
+                        const uint8_t* srcb = img + ((size_t) cb * prm.nkb +
+                                kb) * kL6Block + half * (kI8Tile / 2);
+#pragma unroll
+                        for (int l = 0; l < kL6Limbs; ++l)
+                            ptx::bulk_g2s(dst + kL6Block + l * (kI8Tile / 2),
+                                    srcb + l * kI8Tile, kI8Tile / 2,
+                                    &ctl->full[stage]);
+                    }
+                    issued |= 1u << stage;
+                    issued_par = (issued_par & ~(1u << stage)) |
+                            (phase << stage);
+                    if (++stage == kL6Stages) { stage = 0; phase ^= 1; }
+                }
+            }
+            for (int s = 0; s < kL6Stages; ++s)
+                if ((issued >> s) & 1)
+                    ptx::mbar_wait(&ctl->full[s], (issued_par >> s) & 1,
+                            prm.err, 52, abort);
+        }
+        __syncwarp();
+    }
+    else if (warp == 1)
+    {
+        if (lane == 0)
+        {
+            // ---------------- MMA issuer
+            const uint32_t idesc = ptx::idesc_i8_s32(128, 64, true, true);
+            uint32_t d[kL6Limbs];
+#pragma unroll
+            for (int c = 0; c < kL6Limbs; ++c) d[c] = tmem + 64 * c;
+            int stage = 0;
+            uint32_t phase = 0, dpar = 0;
+            bool ok = true;
+            for (int task = blockIdx.x; task < ntasks && ok;
+                    task += gridDim.x)
+            {
+                const int prob = task / ntile;
+                const int tt = task - prob * ntile;
+                const int half = tt & 1;
+                int rb, cb;
+                tile_of(tt >> 1, rb, cb);
+                const bool diag = rb == cb;
+                for (int ch = 0; ch < nchunk && ok; ++ch)
+                {
+                    // the epilogue has read the accumulators' last sums
+                    if (!ptx::mbar_wait(&ctl->dempty, dpar ^ 1, prm.err, 53,
+                            abort))
+                    {
+                        ok = false;
+                        break;
+                    }
+                    ptx::tc_fence_after();
+                    const int kb0 = prm.i8_chunk_kb[ch];
+                    const int kb1 = prm.i8_chunk_kb[ch + 1];
+                    for (int kb = kb0; kb < kb1; ++kb)
+                    {
+                        if (!ptx::mbar_wait(&ctl->full[stage], phase, prm.err,
+                                54, abort))
+                        {
+                            ok = false;
+                            break;
+                        }
+                        ptx::tc_fence_after();
+                        const uint32_t a = ptx::smem_u32(smem +
+                                (size_t) stage * kL6StageBytes);
+                        // B limb l: rows 64 half .. of A's limb tile l on a
+                        // diagonal tile, else the staged half
+                        const uint32_t b = diag ? a + half * (kI8Tile / 2)
+                                                : a + kL6Block;
+                        const uint32_t bstep = diag ? kI8Tile : kI8Tile / 2;
+#pragma unroll
+                        for (int k = 0; k < 2; ++k)
+                        {
+                            uint64_t ad[kL6Limbs], bd[kL6Limbs];
+#pragma unroll
+                            for (int l = 0; l < kL6Limbs; ++l)
+                            {
+                                ad[l] = ptx::sdesc_sw64(a + l * kI8Tile +
+                                        32 * k);
+                                bd[l] = ptx::sdesc_sw64(b + l * bstep +
+                                        32 * k);
+                            }
+                            const uint32_t acc =
+                                    (kb > kb0 || k > 0) ? 1u : 0u;
+                            // grouped by A limb i (collector buffer), the
+                            // products a_i b_j into D_(i+j), i + j <= 5;
+                            // the i = 0 group writes every accumulator
+                            // first (program order), so it resets them
+                            ptx::mma_i8_col<0>(d[0], ad[0], bd[0], idesc, acc);
+                            ptx::mma_i8_col<1>(d[1], ad[0], bd[1], idesc, acc);
+                            ptx::mma_i8_col<1>(d[2], ad[0], bd[2], idesc, acc);
+                            ptx::mma_i8_col<1>(d[3], ad[0], bd[3], idesc, acc);
+                            ptx::mma_i8_col<1>(d[4], ad[0], bd[4], idesc, acc);
+                            ptx::mma_i8_col<2>(d[5], ad[0], bd[5], idesc, acc);
+                            ptx::mma_i8_col<0>(d[1], ad[1], bd[0], idesc, 1u);
+                            ptx::mma_i8_col<1>(d[2], ad[1], bd[1], idesc, 1u);
+                            ptx::mma_i8_col<1>(d[3], ad[1], bd[2], idesc, 1u);
+                            ptx::mma_i8_col<1>(d[4], ad[1], bd[3], idesc, 1u);
+                            ptx::mma_i8_col<2>(d[5], ad[1], bd[4], idesc, 1u);
+                            ptx::mma_i8_col<0>(d[2], ad[2], bd[0], idesc, 1u);
+                            ptx::mma_i8_col<1>(d[3], ad[2], bd[1], idesc, 1u);
+                            ptx::mma_i8_col<1>(d[4], ad[2], bd[2], idesc, 1u);
+                            ptx::mma_i8_col<2>(d[5], ad[2], bd[3], idesc, 1u);
+                            ptx::mma_i8_col<0>(d[3], ad[3], bd[0], idesc, 1u);
+                            ptx::mma_i8_col<1>(d[4], ad[3], bd[1], idesc, 1u);
+                            ptx::mma_i8_col<2>(d[5], ad[3], bd[2], idesc, 1u);
+                            ptx::mma_i8_col<0>(d[4], ad[4], bd[0], idesc, 1u);
+                            ptx::mma_i8_col<2>(d[5], ad[4], bd[1], idesc, 1u);
+                            ptx::mma_i8(d[5], ad[5], bd[0], idesc, 1u);
+                        }
+                        ptx::mma_commit(&ctl->empty[stage]);
+                        if (++stage == kL6Stages) { stage = 0; phase ^= 1; }
+                    }
+                    if (!ok) break;
+                    ptx::mma_commit(&ctl->dfull);
+                    dpar ^= 1;
+                }
+            }
+            // All issued MMAs must finish before TMEM is released.
+            ptx::mma_commit(&ctl->done);
+            ptx::mbar_wait(&ctl->done, 0, prm.err, 55, abort);
+        }
+        __syncwarp();
+    }
+    else
+    {
+        // ---------------- epilogue: 8 warps, 32 columns each
+        const int q4 = warp & 3;          // TMEM lane quadrant of this warp
+        const int h = (warp - 2) >> 2;    // 32-column half of the 64
+        const int row = 32 * q4 + lane;   // row of the G tile
+        const int c = row & 1;
+        const uint32_t taddr = tmem + ((uint32_t) (32 * q4) << 16) +
+                (uint32_t) (32 * h);
+        uint32_t dpar = 0;
+        bool ok = true;
+        for (int task = blockIdx.x; task < ntasks && ok; task += gridDim.x)
+        {
+            const int prob = task / ntile;
+            const int tt = task - prob * ntile;
+            const int half = tt & 1;
+            int rb, cb;
+            tile_of(tt >> 1, rb, cb);
+            double accR[8], accI[8];
+#pragma unroll
+            for (int j = 0; j < 8; ++j) accR[j] = accI[j] = 0.0;
+            for (int ch = 0; ch < nchunk; ++ch)
+            {
+                if (!ptx::mbar_wait(&ctl->dfull, dpar, prm.err, 56, abort))
+                {
+                    ok = false;
+                    break;
+                }
+                ptx::tc_fence_after();
+                // the chunk's bucket b: its entries carry q 2^b each
+                l6_drain32(taddr, c, ldexp(1.0, -2 * prm.i8_chunk_bucket[ch]),
+                        accR, accI);
+                ptx::tc_fence_before();
+                __syncwarp();
+                if (lane == 0) ptx::mbar_arrive(&ctl->dempty);
+                dpar ^= 1;
+            }
+            if (!ok) break;
+            const int g = prm.prob0 + prob;
+            const double q = l6_scale_from_bits(
+                    prm.maxabs_bits[prm.maxabs_stride * g]);
+            task_store<8>(prm, accR, accI, 1099511627776.0 / (q * q), row,
+                    16 * half + 8 * h, prob, rb, cb);
+        }
+    }
+
+    ptx::tc_fence_before();
+    __syncthreads();
+    ptx::tc_fence_after();
+    if (warp == 1) ptx::tmem_dealloc(tmem, kL6TmemCols);
+}
+
 }  // namespace tc
 }  // namespace oskb
 
@@ -2338,7 +2796,10 @@ int device_setup(bool& wide_fits, bool& pair_fits)
                 (int) gemm_pair_smem_bytes()) != cudaSuccess ||
                 cudaFuncSetAttribute(gemm_i8_kernel,
                 cudaFuncAttributeMaxDynamicSharedMemorySize,
-                (int) gemm_i8_smem_bytes()) != cudaSuccess)
+                (int) gemm_i8_smem_bytes()) != cudaSuccess ||
+                cudaFuncSetAttribute(gemm_l6_kernel,
+                cudaFuncAttributeMaxDynamicSharedMemorySize,
+                (int) gemm_l6_smem_bytes()) != cudaSuccess)
         {
             set_last_error("tc gemm attributes", cudaGetLastError());
             return OSKB_ERR_KERNEL_LAUNCH_FAILURE;
@@ -2491,7 +2952,7 @@ int launch_gemm(GemmParams& gp, cudaStream_t stream)
 // (I8Order), then the operand images.
 size_t tables_bytes_for(bool i8, int num_src)
 {
-    return i8 ? i8_order_bytes(num_src, nullptr, nullptr) : 0;
+    return i8 ? i8_order_bytes(num_src, kI8DrainKb, nullptr, nullptr) : 0;
 }
 
 // Workspace bytes of np problems' images that suit either form.
@@ -2509,7 +2970,7 @@ size_t workspace_bytes_any(int num_st, int num_src, int np)
 template <typename TJ>
 int i8_order(const TJ* jones, int num_src, int num_st, const double* I,
         const double* Q, const double* U, const double* V, Header* hdr,
-        const I8Order& o, cudaStream_t s)
+        const I8Order& o, cudaStream_t s, int drain_kb = kI8DrainKb)
 {
     if (cudaMemsetAsync(o.amp_bits, 0, sizeof(unsigned int) * num_src, s) !=
             cudaSuccess)
@@ -2526,8 +2987,8 @@ int i8_order(const TJ* jones, int num_src, int num_st, const double* I,
             &hdr->flags);
     int err = check_launch("tc source amplitudes");
     if (err) return err;
-    i8_order_kernel<<<1, kOrderThreads, 0, s>>>(num_src, &hdr->maxabs_bits,
-            o);
+    i8_order_kernel<<<1, kOrderThreads, 0, s>>>(num_src, drain_kb,
+            &hdr->maxabs_bits, o);
     return check_launch("tc source order");
 }
 
@@ -2559,8 +3020,8 @@ int jones_block(int casa, int num_sources, int num_stations, int offset_out,
     if (i8)
     {
         I8Order o;
-        uint8_t* W = ws + kHeaderBytes +
-                i8_order_bytes(num_sources, ws + kHeaderBytes, &o);
+        uint8_t* W = ws + kHeaderBytes + i8_order_bytes(num_sources,
+                kI8DrainKb, ws + kHeaderBytes, &o);
         if ((err = i8_order<double>(jones, num_sources, num_stations, I, Q,
                 U, V, hdr, o, s)))
             return err;
@@ -2599,6 +3060,65 @@ int jones_block(int casa, int num_sources, int num_stations, int offset_out,
     return launch_gemm(gp, s);
 }
 
+// Workspace of the FP64-class form: Header, source-order tables (chunks of
+// kL6DrainKb k blocks), six-limb image.
+size_t l6_workspace_bytes(int num_st, int num_src)
+{
+    return kHeaderBytes + i8_order_bytes(num_src, kL6DrainKb, nullptr,
+            nullptr) + image_bytes_l6(num_st, num_src);
+}
+
+// One J block through the FP64-class form in the workspace at ws.
+int l6_block(int casa, int num_sources, int num_stations, int offset_out,
+        const double* jones, const double* I, const double* Q,
+        const double* U, const double* V, const double* station_u,
+        const double* station_v, double uv_min_lambda, double uv_max_lambda,
+        double inv_wavelength, double* vis, uint8_t* ws, cudaStream_t s)
+{
+    bool wide_fits = false, pair_fits = false;
+    int err = device_setup(wide_fits, pair_fits);
+    if (err) return err;
+    Header* hdr = reinterpret_cast<Header*>(ws);
+    if (cudaMemsetAsync(hdr, 0, sizeof(Header), s) != cudaSuccess)
+    {
+        set_last_error("tc64 header clear", cudaGetLastError());
+        return OSKB_ERR_KERNEL_LAUNCH_FAILURE;
+    }
+    const int nrb = (num_stations + kStPerBlock - 1) / kStPerBlock;
+    I8Order o;
+    uint8_t* W = ws + kHeaderBytes + i8_order_bytes(num_sources, kL6DrainKb,
+            ws + kHeaderBytes, &o);
+    if ((err = i8_order<double>(jones, num_sources, num_stations, I, Q, U,
+            V, hdr, o, s, kL6DrainKb)))
+        return err;
+    const int cap = i8_kb_cap(num_sources);
+    prep_jones_l6_kernel<<<dim3(cap, nrb), 256, 0, s>>>(jones, num_sources,
+            num_stations, I, Q, U, V, &hdr->maxabs_bits, o, W);
+    if ((err = check_launch("tc64 prep"))) return err;
+    GemmParams gp;
+    gp.i8 = 1;
+    gp.form = kFormDefault;
+    gp.i8_counts = o.counts;
+    gp.i8_chunk_kb = o.chunk_kb;
+    gp.i8_chunk_bucket = o.chunk_bucket;
+    gp.skip_flags = &hdr->flags;
+    gp.W = W; gp.image_stride = 0; gp.nrb = nrb; gp.nkb = cap;
+    gp.num_problems = 1; gp.num_st = num_stations;
+    gp.maxabs_bits = &hdr->maxabs_bits; gp.maxabs_stride = 0;
+    gp.prob0 = 0; gp.nch = 1;
+    gp.vis = vis; gp.vis_stride = 0; gp.offset_out = offset_out;
+    gp.st_u = station_u; gp.st_v = station_v; gp.uv_stride = 0;
+    gp.inv_wavelength = nullptr; gp.kw_scalar = inv_wavelength;
+    gp.uv_min = uv_min_lambda; gp.uv_max = uv_max_lambda;
+    gp.casa = casa; gp.err = &hdr->err; gp.autos = nullptr;
+    const long long ntasks = (long long) nrb * (nrb + 1);
+    const int grid = (int) (ntasks < num_sms() ? ntasks : num_sms());
+    cudaEvent_t ev_stop = timing_start(s);
+    gemm_l6_kernel<<<grid, kGemmThreads, gemm_l6_smem_bytes(), s>>>(gp);
+    if (ev_stop) cudaEventRecord(ev_stop, s);
+    return check_launch("tc64 gemm");
+}
+
 }  // namespace
 }  // namespace tc
 }  // namespace oskb
@@ -2633,6 +3153,34 @@ int oskb_cross_correlate_tc_d(int casa, int num_sources, int num_stations,
     if (err) return err;
     return jones_block(casa, num_sources, num_stations, offset_out, jones, I,
             Q, U, V, station_u, station_v, uv_min_lambda, uv_max_lambda,
+            inv_wavelength, vis, reinterpret_cast<uint8_t*>(workspace), s);
+}
+
+size_t oskb_cross_correlate_tc64_workspace_bytes(int num_sources,
+        int num_stations)
+{
+    if (num_sources <= 0 || num_stations <= 0) return kHeaderBytes;
+    return l6_workspace_bytes(num_stations, num_sources);
+}
+
+int oskb_cross_correlate_tc64_d(int casa, int num_sources, int num_stations,
+        int offset_out, const double* jones, const double* I,
+        const double* Q, const double* U, const double* V,
+        const double* station_u, const double* station_v,
+        double uv_min_lambda, double uv_max_lambda, double inv_wavelength,
+        double* vis, void* workspace, size_t workspace_bytes, void* stream)
+{
+    if (num_sources < 0 || num_stations < 0) return OSKB_ERR_INVALID_ARGUMENT;
+    if (num_sources == 0 || num_stations < 2) return 0;
+    if (!jones || !I || !Q || !U || !V || !station_u || !station_v || !vis)
+        return OSKB_ERR_INVALID_ARGUMENT;
+    const size_t need = oskb_cross_correlate_tc64_workspace_bytes(
+            num_sources, num_stations);
+    cudaStream_t s = as_stream(stream);
+    int err = get_workspace(workspace, workspace_bytes, need, s);
+    if (err) return err;
+    return l6_block(casa, num_sources, num_stations, offset_out, jones, I, Q,
+            U, V, station_u, station_v, uv_min_lambda, uv_max_lambda,
             inv_wavelength, vis, reinterpret_cast<uint8_t*>(workspace), s);
 }
 
@@ -2750,7 +3298,7 @@ int correlate_block(int casa, int num_sources, int num_stations,
     I8Order o = {};
     if (i8)
     {
-        i8_order_bytes(num_sources, ws + kHeaderBytes, &o);
+        i8_order_bytes(num_sources, kI8DrainKb, ws + kHeaderBytes, &o);
         if ((err = i8_order<TE>(E, num_sources, num_stations, I, Q, U, V,
                 hdr, o, s)))
             return err;
