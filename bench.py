@@ -662,6 +662,10 @@ def run_profile_case(args):
                     amplitude buckets' chunks have their bench-size length);
       direct_small  the FP64 direct cross-correlation: 512 stations x 2,000
                     sources, 1 channel;
+      tc64_small    the FP64-class integer contraction (gemm_l6_kernel) and
+                    its operand preparation (prep_jones_l6_kernel): 512
+                    stations x 10,000 sources, 1 channel (272 tasks of
+                    128 x 64, one per tile half);
       beam_small    the fused station beam: 32 stations x 256 dipoles x
                     12,001 directions (FP64);
       block_small   the block correlator with Jones K fused: 256 stations x
@@ -678,10 +682,10 @@ def run_profile_case(args):
         os.environ["OSKB_TC_TILE"] = "256" if case == "tc_wide_small" \
             else "512"
     if case in ("tc_small", "tc_wide_small", "tc_pair_small", "tc_i8_small",
-                "direct_small"):
+                "direct_small", "tc64_small"):
         nsrc = {"tc_small": 20_000, "tc_wide_small": 2_500,
                 "tc_pair_small": 2_500, "tc_i8_small": 10_000,
-                "direct_small": 2_000}[case]
+                "direct_small": 2_000, "tc64_small": 10_000}[case]
         nch = {"tc_wide_small": 8, "tc_pair_small": 8,
                "tc_i8_small": 4}.get(case, 1)
         cfg = workloads.c3(num_src=nsrc, num_channels=nch, num_times=1)
@@ -692,7 +696,23 @@ def run_profile_case(args):
         uvw = dev(cfg.station_uvw(0)[None])
         inv_wl = dev(cfg.freqs_hz / 299792458.0)
         vis = torch.zeros((nch, nbl, 8), dtype=torch.float64, device="cuda")
-        if case != "direct_small":
+        if case == "tc64_small":
+            f = float(cfg.freqs_hz[0])
+            u, v, w = uvw[0]
+            K = torch.empty((nst, nsrc, 2), dtype=torch.float64,
+                            device="cuda")
+            J = torch.empty((nst, nsrc, 8), dtype=torch.float64,
+                            device="cuda")
+            ob.call("oskb_evaluate_jones_K_d", nsrc, l, m, n, nst, u, v, w,
+                    2 * math.pi * f / 299792458.0, I, 0.0, 1e300, 0, K,
+                    stream)
+            ob.call("oskb_mem_multiply_d", 3, 0, 0, 0, nst * nsrc, K,
+                    E.double(), J, stream)
+            for _ in range(2):
+                ob.call("oskb_cross_correlate_tc64_d", 0, nsrc, nst, 0, J, I,
+                        Q, U, V, u, v, 0.0, 3e38, f / 299792458.0, vis[0],
+                        None, 0, stream)
+        elif case != "direct_small":
             ws_bytes = ob.call("oskb_correlate_block_tc_workspace_bytes",
                                nsrc, nst, nch, check=False)
             ws = torch.empty(ws_bytes, dtype=torch.uint8, device="cuda")
@@ -1324,7 +1344,7 @@ def main():
     ap.add_argument("--c5-bound", type=float, default=1e-4)
     ap.add_argument("--profile-case", default=None,
                     choices=["tc_small", "tc_wide_small", "tc_pair_small",
-                             "tc_i8_small",
+                             "tc_i8_small", "tc64_small",
                              "direct_small",
                              "beam_small",
                              "block_small"],

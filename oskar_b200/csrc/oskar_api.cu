@@ -314,10 +314,15 @@ void oskar_telescope_set_uv_filter(oskar_Telescope* t, double mn, double mx,
 
 namespace {
 
-bool tc_requested()
+// OSKAR_CORRELATE: "TC" the tensor-core compensated form (1e-6), "TC64"
+// the FP64-class tensor-core form (FP64 accuracy); 0 otherwise.
+int tc_mode()
 {
     const char* e = getenv("OSKAR_CORRELATE");
-    return e && (strcmp(e, "TC") == 0 || strcmp(e, "tc") == 0);
+    if (!e) return 0;
+    if (strcmp(e, "TC") == 0 || strcmp(e, "tc") == 0) return 1;
+    if (strcmp(e, "TC64") == 0 || strcmp(e, "tc64") == 0) return 2;
+    return 0;
 }
 
 const float* F(const oskar_Mem* m)
@@ -428,14 +433,39 @@ void oskar_cross_correlate(int casa, int source_type, int num_sources,
                 (float) dec0, (float*) vis->data, 0);
         break;
     case OSKAR_DOUBLE_COMPLEX_MATRIX:
-        if (tc_requested() && !use_extended && frac_bandwidth == 0.0 &&
-                time_avg == 0.0)
+    {
+        const int mode = tc_mode();
+        const bool point = !use_extended && frac_bandwidth == 0.0 &&
+                time_avg == 0.0;
+        bool done = false;
+        if (mode == 1 && point)
+        {
             *status = oskb_cross_correlate_tc_d(casa, num_sources,
                     num_stations, offset_out, D(jones->data), D(src_flux[0]),
                     D(src_flux[1]), D(src_flux[2]), D(src_flux[3]),
                     D(station_uvw[0]), D(station_uvw[1]), uv_min, uv_max,
                     inv_wavelength, (double*) vis->data, nullptr, 0, 0);
-        else
+            done = true;
+        }
+        else if (mode == 2 && point)
+        {
+            // nothing is added if a brightness matrix is not positive
+            // semi-definite (status flags bit 0): then the direct kernel
+            *status = oskb_cross_correlate_tc64_d(casa, num_sources,
+                    num_stations, offset_out, D(jones->data), D(src_flux[0]),
+                    D(src_flux[1]), D(src_flux[2]), D(src_flux[3]),
+                    D(station_uvw[0]), D(station_uvw[1]), uv_min, uv_max,
+                    inv_wavelength, (double*) vis->data, nullptr, 0, 0);
+            int flags = 0, wait_error = 0;
+            if (!*status)
+                *status = cudaStreamSynchronize(0) == cudaSuccess ?
+                        oskb_tc_status(nullptr, &flags, &wait_error) :
+                        OSKB_ERR_KERNEL_LAUNCH_FAILURE;
+            if (!*status && wait_error)
+                *status = OSKB_ERR_KERNEL_LAUNCH_FAILURE;
+            done = *status != 0 || !(flags & 1);
+        }
+        if (!done)
             *status = oskb_cross_correlate_d(casa, use_extended, num_sources,
                     num_stations, offset_out, D(jones->data), D(src_flux[0]),
                     D(src_flux[1]), D(src_flux[2]), D(src_flux[3]),
@@ -445,6 +475,7 @@ void oskar_cross_correlate(int casa, int source_type, int num_sources,
                     inv_wavelength, frac_bandwidth, time_avg, gha0, dec0,
                     (double*) vis->data, 0);
         break;
+    }
     case OSKAR_SINGLE_COMPLEX:
         *status = oskb_cross_correlate_scalar_f(casa, use_extended,
                 num_sources, num_stations, offset_out, F(jones->data),

@@ -95,6 +95,26 @@ def test_cross_correlate_tensor_core_env(monkeypatch):
     assert 0 < err <= 1e-6  # TC, so not bit-exact with FP64
 
 
+@pytest.mark.parametrize("psd", [True, False])
+def test_cross_correlate_fp64_class_env(psd, monkeypatch):
+    """OSKAR_CORRELATE=TC64 routes FP64 point sources without smearing to
+    the FP64-class tensor-core form (1e-12); a brightness matrix that is not
+    positive semi-definite sends the call to the direct kernel."""
+    c = XcorrCase(60, 900, ranges="physical", seed=5)
+    if not psd:
+        c.Q[3] = 3.0 * c.I[3]
+    monkeypatch.setenv("OSKAR_CORRELATE", "TC64")
+    got = run_api(c, D, 1.0, 0.0, 0)
+    ref = c.vis0.copy()
+    oracle().call("xcorr_matrix_d", np.float64, 0, 0, *c.oracle_args(ref))
+    assert rel(got - c.vis0, ref - c.vis0) <= 1e-12
+    # the FP64-class form ran (its status words report the brightness)
+    flags = (oa.ctypes.c_int * 2)()
+    assert load().oskb_tc_status(None, oa.ctypes.addressof(flags),
+                                 oa.ctypes.addressof(flags) + 4) == 0
+    assert flags[0] == (0 if psd else 1) and flags[1] == 0
+
+
 def test_jones_join_identity_known_answer():
     """Test_Jones.cpp:187-286: joining with identity leaves Jones unchanged,
     in place and out of place, matrix x matrix and scalar x matrix."""
