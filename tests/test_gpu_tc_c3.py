@@ -16,7 +16,8 @@ values) and oskb_correlate_block_tc_d (E in FP64 as an FP64 caller holds it,
 the oracle fed the unrounded values, so the bound covers the rounding of E
 on load too). Dumps 0 and 63 (the longest projected baselines differ by the
 Earth's rotation over the observation) and channels 0, 7 and 15 (the phase
-range grows with frequency) are covered.
+range grows with frequency) are covered. The FP64-class form
+(oskb_cross_correlate_tc64_d) is held to 1e-12 on the same array.
 """
 import numpy as np
 import pytest
@@ -109,3 +110,35 @@ def test_tc_c3_fp64_e(c3_sub):
         ref = oracle_problem(cfg, E, uvw[1], cfg.freqs_hz[c])
         l2, mx = errors(got[1, c], ref)
         assert l2 <= TOL and mx <= TOL, (DUMPS[1], c, l2, mx)
+
+
+def test_tc64_c3_jones(c3_sub):
+    """The FP64-class form (oskb_cross_correlate_tc64_d) on the full C3
+    array: J = K E from the oracle for dump 63, channels 0 and 15, against
+    the oracle's FP64 correlation of the same J to 1e-12."""
+    cfg, E, uvw = c3_sub
+    nst, nsrc = cfg.num_st, cfg.num_src
+    u, v, w = uvw[1]
+    z = np.zeros(nst)
+    for c in (0, 15):
+        freq = cfg.freqs_hz[c]
+        K = np.zeros(2 * nst * nsrc)
+        oracle().call("jones_k_d", np.float64, nsrc, cfg.l, cfg.m, cfg.n,
+                      nst, u, v, w, 2 * np.pi * freq / C0, cfg.I, 0.0, 1e300,
+                      0, K)
+        J = np.zeros(8 * nst * nsrc)
+        oracle().call("mem_mul_cm_m_d", np.float64, nst * nsrc, K,
+                      np.ascontiguousarray(E.ravel()), J)
+        ref = np.zeros(8 * cfg.num_baselines)
+        oracle().call("xcorr_matrix_d", np.float64, 0, 0, nsrc, nst, 0, J,
+                      cfg.I, cfg.Q, cfg.U, cfg.V, cfg.l, cfg.m, cfg.n, None,
+                      None, None, u, v, w, z, z, 0.0, 3e38, freq / C0, 0.0,
+                      0.0, 0.0, 0.0, ref)
+        vis = torch.zeros(8 * cfg.num_baselines, dtype=torch.float64,
+                          device="cuda")
+        ob.call("oskb_cross_correlate_tc64_d", 0, nsrc, nst, 0, dev(J),
+                dev(cfg.I), dev(cfg.Q), dev(cfg.U), dev(cfg.V), dev(u),
+                dev(v), 0.0, 3e38, freq / C0, vis, None, 0, ob.stream_ptr())
+        torch.cuda.synchronize()
+        l2, mx = errors(vis.cpu().numpy(), ref)
+        assert l2 <= 1e-12 and mx <= 1e-12, (c, l2, mx)
