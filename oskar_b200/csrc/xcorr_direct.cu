@@ -634,7 +634,10 @@ xcorr_direct_kernel(const XcorrParams<T> prm)
                             num *= n2;
                             den *= d2;
                         }
-                        f *= num / den;
+                        // |den| >= 0.25 here (each factor's d is 1 or
+                        // at least tau = 0.5), well inside the range where
+                        // the fast division is accurate to 2 ulp
+                        f *= __fdividef(num, den);
                     }
                     smear[i][j] = f;
                 }
