@@ -434,6 +434,7 @@ def run_ours(args):
             "direct_fp64": cmp_["direct"],
             "direct_fp64_dmma": cmp_["direct_dmma"],
             "fp64_class_tc64": cmp_["tc64"],
+            "fp64_class_block": cmp_["block64"],
             "speedup_vs_direct_fp64": value / cmp_["direct"]["value"],
             "speedup_vs_direct_fp64_dmma":
                 value / cmp_["direct_dmma"]["value"],
@@ -536,6 +537,34 @@ def compare_direct(args, cfg, ob, torch, dev, E, l, m, n, I, Q, U, V,
              "max_over_max": float(np.max(np.abs(a64 - b64)) /
                                    np.max(np.abs(b64)))}
     del v64
+    # the FP64-class fused block: one step (dump 0 x all channels) from E
+    # (FP64) with the phase formed in FP64, and its channel-0 error against
+    # the FP64 direct (DMMA) result
+    vb = torch.zeros((nch, nbl, 8), dtype=torch.float64, device="cuda")
+
+    def block64():
+        ob.call("oskb_correlate_block_tc64_d", 0, nsrc, nst, 1, nch, Ed, l,
+                m, n, I, Q, U, V, uvw_all[0], inv_wl, 0.0, 3e38, vb, None, 0,
+                stream)
+
+    block64()
+    torch.cuda.synchronize()
+    e0.record()
+    block64()
+    e1.record()
+    torch.cuda.synchronize()
+    ms_b64 = e0.elapsed_time(e1)
+    vb.zero_()
+    block64()
+    join(0, 0)
+    vd.zero_()
+    direct(0, 0)
+    torch.cuda.synchronize()
+    ab, bb = vb[0].cpu().numpy(), vd.cpu().numpy()
+    errb = {"l2": float(np.linalg.norm(ab - bb) / np.linalg.norm(bb)),
+            "max_over_max": float(np.max(np.abs(ab - bb)) /
+                                  np.max(np.abs(bb)))}
+    del vb
     # errors of the tensor-core block against the FP64 direct result
     worst_l2, worst_mx, cases = 0.0, 0.0, []
     dumps = (0, cfg.num_times - 1)
@@ -584,6 +613,15 @@ def compare_direct(args, cfg, ob, torch, dev, E, l, m, n, I, Q, U, V,
                                "oskb_cross_correlate_tc64_d)",
                      "ms_per_channel": ms_tc64,
                      "error_vs_fp64_direct": err64},
+            "block64": {"value": sb * nch / (ms_b64 * 1e-3) / 1e9,
+                        "unit": UNIT,
+                        "kernel": "oskb prep_fused_l6_kernel + "
+                                  "gemm_l6_kernel (FP64-class fused block, "
+                                  "oskb_correlate_block_tc64_d, E in FP64, "
+                                  "FP64 phase)",
+                        "ms_per_step": ms_b64,
+                        "step": "1 dump x %d channels" % nch,
+                        "error_vs_fp64_direct_channel0": errb},
             "err": err}
 
 

@@ -890,6 +890,30 @@ OSKB_API int oskb_cross_correlate_tc64_d(int use_casa_phase_convention,
         double inv_wavelength, double* vis, void* workspace,
         size_t workspace_bytes, void* stream);
 
+/* FP64-class fused block (no counterpart in the reference; replaces the
+ * per-channel Jones K -> join -> FP64 correlate sequence of sim_baselines,
+ * oskar/interferometer/src/oskar_interferometer_run_block.c:277-334, for
+ * point sources without smearing whose brightness matrices are positive
+ * semi-definite): the same block as oskb_correlate_block_tc_d (E FP64
+ * [station][source][2x2] shared by the block, station_uvw
+ * [time][3][station] metres, inv_wavelength[channel], vis
+ * [time][channel][baseline][2x2] FP64, added), at FP64-class accuracy:
+ * K E C formed in FP64 (phase reduced mod 1, sincospi) as 48-bit fixed
+ * point in six 8-bit limbs per amplitude bucket, contracted on the integer
+ * tensor cores as oskb_cross_correlate_tc64_d. If a brightness matrix is
+ * not positive semi-definite, nothing is added and oskb_tc_status reports
+ * flags bit 0 (then use oskb_correlate_block_direct_d). Problems are
+ * processed in groups that fit the workspace (NULL: library-kept). */
+OSKB_API size_t oskb_correlate_block_tc64_workspace_bytes(int num_sources,
+        int num_stations, int num_problems);
+OSKB_API int oskb_correlate_block_tc64_d(int use_casa_phase_convention,
+        int num_sources, int num_stations, int num_times, int num_channels,
+        const double* E, const double* l, const double* m, const double* n,
+        const double* I, const double* Q, const double* U, const double* V,
+        const double* station_uvw, const double* inv_wavelength,
+        double uv_min_lambda, double uv_max_lambda, double* vis,
+        void* workspace, size_t workspace_bytes, void* stream);
+
 /* Direct (FP64 or FP32) block correlator with smearing: for every (dump t,
  * channel c) of a block, in ONE persistent launch,
  *   vis[t][c][pq] += sum_s smear_pq(s) (J_p B J_q^H)(s),  J = K(t, c) E,

@@ -2306,6 +2306,87 @@ __global__ void __launch_bounds__(256) prep_jones_l6_kernel(
     }
 }
 
+// Six-limb image of a block of problems (t, c) from E (FP32 or FP64
+// [station][source][2x2], shared by the block) with the interferometer
+// phase in FP64: entry = K_p(s) (E_p C)(s) scaled by q 2^b of the source's
+// bucket, K_p(s) = exp(2 pi i (u_p l + v_p m + w_p (n - 1)) / lambda_c),
+// the argument reduced mod 1 in FP64 and its sine and cosine by sincospi
+// (FP64). grid (k-block capacity, row blocks); a thread takes one source
+// and stations warp + 8 k, and for each station every problem of the
+// group [p0, p0 + np) (problem j's image at W + j image_stride).
+template <typename TE>
+__global__ void __launch_bounds__(256) prep_fused_l6_kernel(
+        const TE* __restrict__ E, int num_src, int num_st,
+        const double* __restrict__ l, const double* __restrict__ m,
+        const double* __restrict__ n, const double* __restrict__ I,
+        const double* __restrict__ Q, const double* __restrict__ U,
+        const double* __restrict__ V, const double* __restrict__ uvw,
+        const double* __restrict__ inv_wavelength, int nch, int p0, int np,
+        const unsigned int* __restrict__ maxabs_bits, const I8Order o,
+        uint8_t* W, size_t image_stride)
+{
+    const int kb = blockIdx.x, rb = blockIdx.y, nkb_cap = gridDim.x;
+    if (kb >= o.counts[0]) return;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int s = o.perm[kb * kSrcPerBlock + lane];
+    const bool src_ok = s >= 0;
+    double c11 = 0, c21r = 0, c21i = 0, c22 = 0;
+    double sl = 0, sm = 0, sn1 = 0;
+    if (src_ok)
+    {
+        brightness_factor(I[s], Q[s], U[s], V[s], c11, c21r, c21i, c22);
+        sl = l[s]; sm = m[s]; sn1 = n[s] - 1.0;
+    }
+    const double q = ldexp(l6_scale_from_bits(*maxabs_bits), o.kb_bucket[kb]);
+    uint8_t* blk0 = W + (size_t) (rb * nkb_cap + kb) * kL6Block;
+    for (int pl = warp; pl < kStPerBlock; pl += 8)
+    {
+        const int p = rb * kStPerBlock + pl;
+        const bool ok = src_ok && p < num_st;
+        double A0[2][2][2] = {{{0, 0}, {0, 0}}, {{0, 0}, {0, 0}}};
+        if (ok)
+        {
+            double J[8];
+            const TE* e = E + 8 * ((size_t) p * num_src + s);
+#pragma unroll
+            for (int k = 0; k < 8; ++k) J[k] = (double) e[k];
+            apply_factor_d(J, c11, c21r, c21i, c22, A0);
+#pragma unroll
+            for (int k = 0; k < 8; ++k) (&A0[0][0][0])[k] *= q;
+        }
+        double base = 0.0;
+        int t_cur = -1;
+        for (int j = 0; j < np; ++j)
+        {
+            const int prob = p0 + j, t = prob / nch, c = prob - t * nch;
+            double A[2][2][2] = {{{0, 0}, {0, 0}}, {{0, 0}, {0, 0}}};
+            if (ok)
+            {
+                if (t != t_cur)
+                {
+                    t_cur = t;
+                    const double* pu = uvw + (size_t) t * 3 * num_st;
+                    base = pu[p] * sl + pu[num_st + p] * sm +
+                            pu[2 * num_st + p] * sn1;
+                }
+                const double x = base * inv_wavelength[c];
+                double sn, cs;
+                sincospi(2.0 * (x - rint(x)), &sn, &cs);
+#pragma unroll
+                for (int i = 0; i < 2; ++i)
+#pragma unroll
+                    for (int kk = 0; kk < 2; ++kk)
+                    {
+                        const double re = A0[i][kk][0], im = A0[i][kk][1];
+                        A[i][kk][0] = re * cs - im * sn;
+                        A[i][kk][1] = re * sn + im * cs;
+                    }
+            }
+            store_entry_l6(blk0 + (size_t) j * image_stride, pl, lane, A);
+        }
+    }
+}
+
 struct L6Ctl
 {
     uint64_t full[kL6Stages], empty[kL6Stages], dfull, dempty, done;
@@ -3119,6 +3200,94 @@ int l6_block(int casa, int num_sources, int num_stations, int offset_out,
     return check_launch("tc64 gemm");
 }
 
+// The FP64-class block (oskb_correlate_block_tc64_d): as correlate_block
+// with the six-limb image. Workspace: Header, tables, group x image.
+int correlate_block_l6(int casa, int num_sources, int num_stations,
+        int num_times, int num_channels, const double* E, const double* l,
+        const double* m, const double* n, const double* I, const double* Q,
+        const double* U, const double* V, const double* station_uvw,
+        const double* inv_wavelength, double uv_min_lambda,
+        double uv_max_lambda, double* vis, void* workspace,
+        size_t workspace_bytes, cudaStream_t s)
+{
+    const int num_problems = num_times * num_channels;
+    const size_t img = image_bytes_l6(num_stations, num_sources);
+    const size_t tb = i8_order_bytes(num_sources, kL6DrainKb, nullptr,
+            nullptr);
+    int group = num_problems;
+    if (workspace)
+    {
+        if (workspace_bytes < kHeaderBytes + tb + img)
+            return OSKB_ERR_MEMORY_ALLOC_FAILURE;
+        const size_t fit = (workspace_bytes - kHeaderBytes - tb) / img;
+        if ((size_t) group > fit) group = (int) fit;
+    }
+    else
+    {
+        size_t free_b = 0, total_b = 0;
+        cudaMemGetInfo(&free_b, &total_b);
+        size_t fit = free_b / 2 / img;
+        if (fit < 1) fit = 1;
+        if ((size_t) group > fit) group = (int) fit;
+        if (group > max_group()) group = max_group();
+    }
+    int err = get_workspace(workspace, workspace_bytes,
+            kHeaderBytes + tb + (size_t) group * img, s);
+    if (err) return err;
+    bool wide_fits = false, pair_fits = false;
+    if ((err = device_setup(wide_fits, pair_fits))) return err;
+    uint8_t* ws = reinterpret_cast<uint8_t*>(workspace);
+    Header* hdr = reinterpret_cast<Header*>(ws);
+    uint8_t* W = ws + kHeaderBytes + tb;
+    if (cudaMemsetAsync(hdr, 0, sizeof(Header), s) != cudaSuccess)
+    {
+        set_last_error("tc64 header clear", cudaGetLastError());
+        return OSKB_ERR_KERNEL_LAUNCH_FAILURE;
+    }
+    I8Order o;
+    i8_order_bytes(num_sources, kL6DrainKb, ws + kHeaderBytes, &o);
+    // |K| = 1: one scale and source order from E C for the whole block
+    if ((err = i8_order<double>(E, num_sources, num_stations, I, Q, U, V,
+            hdr, o, s, kL6DrainKb)))
+        return err;
+    const int nrb = (num_stations + kStPerBlock - 1) / kStPerBlock;
+    const int cap = i8_kb_cap(num_sources);
+    const size_t nbl = (size_t) num_stations * (num_stations - 1) / 2;
+    for (int p0 = 0; p0 < num_problems; p0 += group)
+    {
+        const int np = min(group, num_problems - p0);
+        prep_fused_l6_kernel<double><<<dim3(cap, nrb), 256, 0, s>>>(E,
+                num_sources, num_stations, l, m, n, I, Q, U, V, station_uvw,
+                inv_wavelength, num_channels, p0, np, &hdr->maxabs_bits, o, W,
+                img);
+        if ((err = check_launch("tc64 prep fused"))) return err;
+        GemmParams gp;
+        gp.i8 = 1;
+        gp.form = kFormDefault;
+        gp.i8_counts = o.counts;
+        gp.i8_chunk_kb = o.chunk_kb;
+        gp.i8_chunk_bucket = o.chunk_bucket;
+        gp.skip_flags = &hdr->flags;
+        gp.W = W; gp.image_stride = img; gp.nrb = nrb; gp.nkb = cap;
+        gp.num_problems = np; gp.num_st = num_stations;
+        gp.maxabs_bits = &hdr->maxabs_bits; gp.maxabs_stride = 0;
+        gp.prob0 = p0; gp.nch = num_channels;
+        gp.vis = vis; gp.vis_stride = nbl; gp.offset_out = 0;
+        gp.st_u = station_uvw; gp.st_v = station_uvw + num_stations;
+        gp.uv_stride = 3 * (size_t) num_stations;
+        gp.inv_wavelength = inv_wavelength; gp.kw_scalar = 0.0;
+        gp.uv_min = uv_min_lambda; gp.uv_max = uv_max_lambda;
+        gp.casa = casa; gp.err = &hdr->err; gp.autos = nullptr;
+        const long long ntasks = (long long) nrb * (nrb + 1) * np;
+        const int grid = (int) (ntasks < num_sms() ? ntasks : num_sms());
+        cudaEvent_t ev_stop = timing_start(s);
+        gemm_l6_kernel<<<grid, kGemmThreads, gemm_l6_smem_bytes(), s>>>(gp);
+        if (ev_stop) cudaEventRecord(ev_stop, s);
+        if ((err = check_launch("tc64 gemm"))) return err;
+    }
+    return 0;
+}
+
 }  // namespace
 }  // namespace tc
 }  // namespace oskb
@@ -3182,6 +3351,39 @@ int oskb_cross_correlate_tc64_d(int casa, int num_sources, int num_stations,
     return l6_block(casa, num_sources, num_stations, offset_out, jones, I, Q,
             U, V, station_u, station_v, uv_min_lambda, uv_max_lambda,
             inv_wavelength, vis, reinterpret_cast<uint8_t*>(workspace), s);
+}
+
+size_t oskb_correlate_block_tc64_workspace_bytes(int num_sources,
+        int num_stations, int num_problems)
+{
+    if (num_sources <= 0 || num_stations <= 0 || num_problems <= 0)
+        return kHeaderBytes;
+    return kHeaderBytes + i8_order_bytes(num_sources, kL6DrainKb, nullptr,
+            nullptr) + (size_t) num_problems *
+            image_bytes_l6(num_stations, num_sources);
+}
+
+int oskb_correlate_block_tc64_d(int casa, int num_sources, int num_stations,
+        int num_times, int num_channels, const double* E, const double* l,
+        const double* m, const double* n, const double* I, const double* Q,
+        const double* U, const double* V, const double* station_uvw,
+        const double* inv_wavelength, double uv_min_lambda,
+        double uv_max_lambda, double* vis, void* workspace,
+        size_t workspace_bytes, void* stream)
+{
+    if (num_sources < 0 || num_stations < 0 || num_times < 0 ||
+            num_channels < 0)
+        return OSKB_ERR_INVALID_ARGUMENT;
+    if (num_sources == 0 || num_stations < 2 ||
+            num_times * num_channels == 0)
+        return 0;
+    if (!E || !l || !m || !n || !I || !Q || !U || !V || !station_uvw ||
+            !inv_wavelength || !vis)
+        return OSKB_ERR_INVALID_ARGUMENT;
+    return correlate_block_l6(casa, num_sources, num_stations, num_times,
+            num_channels, E, l, m, n, I, Q, U, V, station_uvw,
+            inv_wavelength, uv_min_lambda, uv_max_lambda, vis, workspace,
+            workspace_bytes, as_stream(stream));
 }
 
 size_t oskb_correlate_block_tc_workspace_bytes(int num_sources,

@@ -18,6 +18,7 @@ pytestmark = [pytest.mark.gpu,
                                  reason="needs a CUDA device")]
 
 import oskar_b200 as ob  # noqa: E402
+from oracle_lib import oracle  # noqa: E402
 from test_gpu_tc import C0, dev, errors, oracle_vis, sky, stations  # noqa: E402
 
 TOL = 1e-12
@@ -133,3 +134,99 @@ def test_tc64_caller_workspace():
     assert err == 0 and flags == 0
     l2, mx = errors(got, ref)
     assert l2 <= TOL and mx <= TOL, (l2, mx)
+
+
+def oracle_block(nst, nsrc, E, I, Q, U, V, l, m, n, uvw, inv_wl):
+    """The oracle's Jones K -> join -> FP64 correlate per (time, channel)."""
+    out = []
+    for t in range(uvw.shape[0]):
+        u, v, w = uvw[t]
+        row = []
+        for kw in inv_wl:
+            K = np.zeros(2 * nst * nsrc)
+            oracle().call("jones_k_d", np.float64, nsrc, l, m, n, nst, u, v,
+                          w, 2 * np.pi * kw, I, 0.0, 1e300, 0, K)
+            J = np.zeros(8 * nst * nsrc)
+            oracle().call("mem_mul_cm_m_d", np.float64, nst * nsrc, K,
+                          np.ascontiguousarray(E.ravel()), J)
+            row.append(oracle_vis(nst, nsrc, J, I, Q, U, V, l, m, n, u, v, w,
+                                  kw))
+        out.append(row)
+    return np.array(out)
+
+
+def run_block64(nst, nsrc, E, I, Q, U, V, l, m, n, uvw, inv_wl, ws=None):
+    ntime, nchan = uvw.shape[0], len(inv_wl)
+    nbl = nst * (nst - 1) // 2
+    vis = torch.zeros(ntime * nchan * nbl * 8, dtype=torch.float64,
+                      device="cuda")
+    err = ob.call("oskb_correlate_block_tc64_d", 0, nsrc, nst, ntime, nchan,
+                  dev(E), dev(l), dev(m), dev(n), dev(I), dev(Q), dev(U),
+                  dev(V), dev(uvw), dev(inv_wl), 0.0, 3e38, vis, ws,
+                  0 if ws is None else ws.numel(), ob.stream_ptr(),
+                  check=False)
+    torch.cuda.synchronize()
+    flags = (ctypes.c_int * 2)()
+    ob.call("oskb_tc_status", ws, ctypes.addressof(flags),
+            ctypes.addressof(flags) + 4)
+    return err, vis.cpu().numpy().reshape(ntime, nchan, -1), flags[0], \
+        flags[1]
+
+
+@pytest.mark.parametrize("nst,nsrc,ntime,nchan", [(17, 50, 1, 3),
+                                                  (64, 1500, 2, 2),
+                                                  (97, 640, 3, 1)])
+def test_tc64_fused_block(nst, nsrc, ntime, nchan):
+    """K (FP64 phase) x E x brightness for a block of (time, channel)
+    problems in one call, against the oracle's Jones K -> join -> FP64
+    correlate per problem, to 1e-12. Stations within 300 m, so that the
+    phases (a few hundred radians) leave the two FP64 phase computations
+    (the oracle's 2 pi f / c (u l + v m + w (n - 1)), here the same sum in
+    turns reduced mod 1) within 1e-13 of each other."""
+    rng = np.random.default_rng(31 * nst + nsrc)
+    l, m, n, I, Q, U, V = sky(rng, nsrc)
+    E = rng.normal(0, 0.1, (nst, nsrc, 8))
+    E[..., 0] += 1
+    E[..., 6] += 1
+    uvw = np.stack([np.stack(stations(rng, nst, rmax=300.0))
+                    for _ in range(ntime)])
+    inv_wl = (100e6 + 7e6 * np.arange(nchan)) / C0
+    err, got, flags, wait = run_block64(nst, nsrc, E, I, Q, U, V, l, m, n,
+                                        uvw, inv_wl)
+    assert err == 0 and flags == 0 and wait == 0
+    ref = oracle_block(nst, nsrc, E, I, Q, U, V, l, m, n, uvw, inv_wl)
+    for t in range(ntime):
+        for c in range(nchan):
+            l2, mx = errors(got[t, c], ref[t, c])
+            assert l2 <= TOL and mx <= TOL, (t, c, l2, mx)
+
+
+def test_tc64_block_groups_and_not_psd():
+    """A caller workspace holding one problem's image (one problem per
+    group) gives the same sums as the library-kept one; a brightness
+    matrix that is not positive semi-definite adds nothing."""
+    rng = np.random.default_rng(95)
+    nst, nsrc, ntime, nchan = 40, 300, 2, 3
+    l, m, n, I, Q, U, V = sky(rng, nsrc)
+    E = rng.normal(0, 0.1, (nst, nsrc, 8))
+    E[..., 0] += 1
+    E[..., 6] += 1
+    uvw = np.stack([np.stack(stations(rng, nst, rmax=300.0))
+                    for _ in range(ntime)])
+    inv_wl = (120e6 + 1e6 * np.arange(nchan)) / C0
+    err, whole, flags, _ = run_block64(nst, nsrc, E, I, Q, U, V, l, m, n,
+                                       uvw, inv_wl)
+    assert err == 0 and flags == 0
+    one = ob.call("oskb_correlate_block_tc64_workspace_bytes", nsrc, nst, 1,
+                  check=False)
+    ws = torch.empty(one, dtype=torch.uint8, device="cuda")
+    err, grouped, flags, _ = run_block64(nst, nsrc, E, I, Q, U, V, l, m, n,
+                                         uvw, inv_wl, ws=ws)
+    assert err == 0 and flags == 0
+    assert np.array_equal(whole, grouped)
+    Q = Q.copy()
+    Q[5] = 2.0 * I[5]
+    err, got, flags, _ = run_block64(nst, nsrc, E, I, Q, U, V, l, m, n, uvw,
+                                     inv_wl)
+    assert err == 0 and flags & 1
+    assert not np.any(got)

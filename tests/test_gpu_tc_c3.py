@@ -142,3 +142,27 @@ def test_tc64_c3_jones(c3_sub):
         torch.cuda.synchronize()
         l2, mx = errors(vis.cpu().numpy(), ref)
         assert l2 <= 1e-12 and mx <= 1e-12, (c, l2, mx)
+
+
+def test_tc64_block_c3(c3_sub):
+    """The FP64-class fused block (oskb_correlate_block_tc64_d) on the full
+    C3 array, dump 63, channels 0 and 15, E in FP64, against the oracle's
+    Jones K -> join -> FP64 correlate to 5e-12: the phases reach ~3e4
+    radians on the 65 km baselines, and the two FP64 phase computations
+    (the oracle's 2 pi f / c times the path length, here the path length
+    times f / c reduced mod 1) differ by their rounding there."""
+    cfg, E, uvw = c3_sub
+    nst, nsrc, nbl = cfg.num_st, cfg.num_src, cfg.num_baselines
+    inv_wl = cfg.freqs_hz / C0
+    vis = torch.zeros(len(DUMPS) * len(inv_wl) * nbl * 8,
+                      dtype=torch.float64, device="cuda")
+    ob.call("oskb_correlate_block_tc64_d", 0, nsrc, nst, len(DUMPS),
+            len(inv_wl), dev(E), dev(cfg.l), dev(cfg.m), dev(cfg.n),
+            dev(cfg.I), dev(cfg.Q), dev(cfg.U), dev(cfg.V), dev(uvw),
+            dev(inv_wl), 0.0, 3e38, vis, None, 0, ob.stream_ptr())
+    torch.cuda.synchronize()
+    got = vis.cpu().numpy().reshape(len(DUMPS), len(inv_wl), -1)
+    for c in (0, 15):
+        ref = oracle_problem(cfg, E, uvw[1], cfg.freqs_hz[c])
+        l2, mx = errors(got[1, c], ref)
+        assert l2 <= 5e-12 and mx <= 5e-12, (c, l2, mx)
