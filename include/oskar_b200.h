@@ -862,6 +862,26 @@ OSKB_API int oskb_cross_correlate_tc_d(int use_casa_phase_convention,
         double inv_wavelength, double* vis, void* workspace,
         size_t workspace_bytes, void* stream);
 
+/* FP32 form of oskb_cross_correlate_tc_d: J, fluxes, station u, v and vis
+ * in FP32 (as oskb_cross_correlate_f takes them), the sums formed by the
+ * integer tensor-core form (FP64 sums of exact integer products, error
+ * ~4e-7 against FP64, inside FP32's own 1e-5) and added into vis once per
+ * call. Replaces oskar_cross_correlate's FP32 point-source branch without
+ * smearing (oskar/correlate/src/oskar_cross_correlate.c:413-433, the CUDA
+ * call of the single-precision matrix case) where every brightness matrix
+ * is positive semi-definite: otherwise nothing is added and
+ * oskb_tc_status(workspace) reports flags bit 0 (then use
+ * oskb_cross_correlate_f). jones must be 16-byte aligned. workspace: at
+ * least oskb_cross_correlate_tc_f_workspace_bytes() bytes, or NULL. */
+OSKB_API size_t oskb_cross_correlate_tc_f_workspace_bytes(int num_sources,
+        int num_stations);
+OSKB_API int oskb_cross_correlate_tc_f(int use_casa_phase_convention,
+        int num_sources, int num_stations, int offset_out, const float* jones,
+        const float* I, const float* Q, const float* U, const float* V,
+        const float* station_u, const float* station_v, float uv_min_lambda,
+        float uv_max_lambda, float inv_wavelength, float* vis,
+        void* workspace, size_t workspace_bytes, void* stream);
+
 /* FP64-class tensor-core cross-correlation (no counterpart in the
  * reference; replaces oskar_cross_correlate's FP64 point-source branch
  * without smearing, oskar/correlate/src/oskar_cross_correlate.c:434-455,

@@ -71,6 +71,18 @@ bool use_tc64()
     return on;
 }
 
+// FP32 point-source correlation without smearing on the integer
+// tensor-core form (oskb_cross_correlate_tc_f: error ~4e-7, inside FP32's
+// own) unless OSKB_DROPIN_TC32 is 0.
+bool use_tc32()
+{
+    static const bool on = [] {
+        const char* e = getenv("OSKB_DROPIN_TC32");
+        return !(e && e[0] == '0');
+    }();
+    return on;
+}
+
 // ---------------------------------------------------------------- buffers
 struct DevBuf
 {
@@ -110,7 +122,7 @@ struct State
     DevBuf uvw, uvw64, flux, E, R, K, J;
     // the block's visibilities
     DevBuf vis, autos;
-    // workspace of the FP64-class tensor-core correlation
+    // workspace of the tensor-core correlation (FP64-class or FP32 form)
     DevBuf tc64ws;
     int* host_count = nullptr;   // page-locked: sources kept by the clip
 };
@@ -1087,36 +1099,50 @@ void Runner<T>::sim_baselines(const RefSky* sky, int num_src, const T* tab,
                 *eb = gaussian ? col(REF_SKY_SCRATCH_EXT_B) : nullptr,
                 *ec = gaussian ? col(REF_SKY_SCRATCH_EXT_C) : nullptr;
         const size_t out = (size_t) num_baselines() * offset;
-        // FP64 point sources without smearing: the FP64-class tensor-core
-        // form (the dispatcher's branch oskar_cross_correlate.c:434-455),
-        // unless a brightness matrix of the chunk is not positive
-        // semi-definite, which it reports having added nothing; then, and
-        // for every other case, the direct kernels
+        // Point sources without smearing: the FP64-class tensor-core form
+        // in FP64 (the dispatcher's branch oskar_cross_correlate.c:
+        // 434-455), the integer form in FP32 (:413-433), unless a
+        // brightness matrix of the chunk is not positive semi-definite,
+        // which they report having added nothing; then, and for every
+        // other case, the direct kernels
         bool done = false;
-        if (dbl && matrix_ && !gaussian && frac_bw == 0.0 &&
-                time_avg == 0.0 && use_tc64())
+        if (matrix_ && !gaussian && frac_bw == 0.0 && time_avg == 0.0 &&
+                (dbl ? use_tc64() : use_tc32()))
         {
-            check(st_->tc64ws.ensure(oskb_cross_correlate_tc64_workspace_bytes(
-                    num_src, num_st_)), "FP64-class correlation workspace");
+            check(st_->tc64ws.ensure(dbl ?
+                    oskb_cross_correlate_tc64_workspace_bytes(num_src,
+                            num_st_) :
+                    oskb_cross_correlate_tc_f_workspace_bytes(num_src,
+                            num_st_)), "tensor-core correlation workspace");
             if (!ok()) return;
-            err = oskb_cross_correlate_tc64_d(h_->casa_phase_convention,
-                    num_src, num_st_, (int) out, (const double*) EJ,
-                    (const double*) fI, (const double*) fQ,
-                    (const double*) fU, (const double*) fV,
-                    (const double*) u, (const double*) v, uv_min, uv_max,
-                    inv_wl, st_->vis.as<double>(), st_->tc64ws.p,
-                    st_->tc64ws.bytes, s_);
-            check(err, "cross-correlation (FP64-class tensor cores)");
+            if (dbl)
+                err = oskb_cross_correlate_tc64_d(h_->casa_phase_convention,
+                        num_src, num_st_, (int) out, (const double*) EJ,
+                        (const double*) fI, (const double*) fQ,
+                        (const double*) fU, (const double*) fV,
+                        (const double*) u, (const double*) v, uv_min, uv_max,
+                        inv_wl, st_->vis.as<double>(), st_->tc64ws.p,
+                        st_->tc64ws.bytes, s_);
+            else
+                err = oskb_cross_correlate_tc_f(h_->casa_phase_convention,
+                        num_src, num_st_, (int) out, (const float*) EJ,
+                        (const float*) fI, (const float*) fQ,
+                        (const float*) fU, (const float*) fV,
+                        (const float*) u, (const float*) v, (float) uv_min,
+                        (float) uv_max, (float) inv_wl,
+                        st_->vis.as<float>(), st_->tc64ws.p,
+                        st_->tc64ws.bytes, s_);
+            check(err, "cross-correlation (tensor cores)");
             if (!ok()) return;
             int flags = 0, wait_error = 0;
             check(cudaStreamSynchronize(s_) == cudaSuccess ?
                     oskb_tc_status(st_->tc64ws.p, &flags, &wait_error) :
                     REF_ERR_KERNEL_LAUNCH_FAILURE,
-                    "FP64-class correlation status");
+                    "tensor-core correlation status");
             if (!ok()) return;
             if (wait_error)
             {
-                fail(REF_ERR_KERNEL_LAUNCH_FAILURE, "FP64-class correlation: "
+                fail(REF_ERR_KERNEL_LAUNCH_FAILURE, "tensor-core correlation: "
                         "a bounded device-side wait expired");
                 return;
             }

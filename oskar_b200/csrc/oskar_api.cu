@@ -423,6 +423,31 @@ void oskar_cross_correlate(int casa, int source_type, int num_sources,
     switch (vis->type)
     {
     case OSKAR_SINGLE_COMPLEX_MATRIX:
+    {
+        // OSKAR_CORRELATE=TC: point sources without smearing on the integer
+        // tensor-core form (FP32 in and out); nothing is added if a
+        // brightness matrix is not positive semi-definite (status flags
+        // bit 0), then the direct kernel
+        bool done = false;
+        if (tc_mode() == 1 && !use_extended && frac_bandwidth == 0.0 &&
+                time_avg == 0.0)
+        {
+            *status = oskb_cross_correlate_tc_f(casa, num_sources,
+                    num_stations, offset_out, F(jones->data), F(src_flux[0]),
+                    F(src_flux[1]), F(src_flux[2]), F(src_flux[3]),
+                    F(station_uvw[0]), F(station_uvw[1]), (float) uv_min,
+                    (float) uv_max, (float) inv_wavelength,
+                    (float*) vis->data, nullptr, 0, 0);
+            int flags = 0, wait_error = 0;
+            if (!*status)
+                *status = cudaStreamSynchronize(0) == cudaSuccess ?
+                        oskb_tc_status(nullptr, &flags, &wait_error) :
+                        OSKB_ERR_KERNEL_LAUNCH_FAILURE;
+            if (!*status && wait_error)
+                *status = OSKB_ERR_KERNEL_LAUNCH_FAILURE;
+            done = *status != 0 || !(flags & 1);
+        }
+        if (!done)
         *status = oskb_cross_correlate_f(casa, use_extended, num_sources,
                 num_stations, offset_out, F(jones->data), F(src_flux[0]),
                 F(src_flux[1]), F(src_flux[2]), F(src_flux[3]), F(src_dir[0]),
@@ -432,6 +457,7 @@ void oskar_cross_correlate(int casa, int source_type, int num_sources,
                 (float) frac_bandwidth, (float) time_avg, (float) gha0,
                 (float) dec0, (float*) vis->data, 0);
         break;
+    }
     case OSKAR_DOUBLE_COMPLEX_MATRIX:
     {
         const int mode = tc_mode();

@@ -30,6 +30,7 @@
 #include <cuda.h>
 #include <cuda_fp16.h>
 
+#include <algorithm>
 #include <atomic>
 #include <cstring>
 #include <mutex>
@@ -1968,6 +1969,9 @@ __device__ __forceinline__ void i8_drain64(uint32_t taddr, int c,
 __global__ void __launch_bounds__(kGemmThreads, 1)
 gemm_i8_kernel(const GemmParams prm)
 {
+    // a brightness matrix that is not positive semi-definite: nothing is
+    // added when the caller asked so (the FP32 entry point)
+    if (prm.skip_flags && (*prm.skip_flags & 1)) return;
     extern __shared__ uint8_t smem_raw[];
     uint8_t* smem = reinterpret_cast<uint8_t*>(
             (reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~(uintptr_t) 1023);
@@ -2699,6 +2703,28 @@ gemm_l6_kernel(const GemmParams prm)
     if (warp == 1) ptx::tmem_dealloc(tmem, kL6TmemCols);
 }
 
+// FP32 entry point helpers: station u, v widened to FP64; the FP64 sums
+// added into the FP32 visibilities (8 reals per baseline).
+__global__ void __launch_bounds__(256) widen_uv_kernel(int n,
+        const float* __restrict__ u, const float* __restrict__ v,
+        double* __restrict__ du, double* __restrict__ dv)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n)
+    {
+        du[i] = (double) u[i];
+        dv[i] = (double) v[i];
+    }
+}
+
+__global__ void __launch_bounds__(256) add_vis_f_kernel(size_t n,
+        const double* __restrict__ sums, float* __restrict__ vis)
+{
+    for (size_t i = (size_t) blockIdx.x * blockDim.x + threadIdx.x; i < n;
+            i += (size_t) gridDim.x * blockDim.x)
+        vis[i] = (float) ((double) vis[i] + sums[i]);
+}
+
 }  // namespace tc
 }  // namespace oskb
 
@@ -3048,9 +3074,9 @@ size_t workspace_bytes_any(int num_st, int num_src, int np)
 // The integer image's scale, buckets and source order for a J (or E) block
 // of num_st x num_src ([station][source][2x2], shared by all problems):
 // per-source and overall largest |entry| of J C, then the order tables.
-template <typename TJ>
-int i8_order(const TJ* jones, int num_src, int num_st, const double* I,
-        const double* Q, const double* U, const double* V, Header* hdr,
+template <typename TJ, typename TF = double>
+int i8_order(const TJ* jones, int num_src, int num_st, const TF* I,
+        const TF* Q, const TF* U, const TF* V, Header* hdr,
         const I8Order& o, cudaStream_t s, int drain_kb = kI8DrainKb)
 {
     if (cudaMemsetAsync(o.amp_bits, 0, sizeof(unsigned int) * num_src, s) !=
@@ -3063,7 +3089,7 @@ int i8_order(const TJ* jones, int num_src, int num_st, const double* I,
     int gy = (4 * num_sms() + gx - 1) / gx;
     if (gy > num_st) gy = num_st;
     if (gy < 1) gy = 1;
-    maxabs_src_kernel<TJ, double><<<dim3(gx, gy), 256, 0, s>>>(jones,
+    maxabs_src_kernel<TJ, TF><<<dim3(gx, gy), 256, 0, s>>>(jones,
             num_src, num_st, I, Q, U, V, o.amp_bits, &hdr->maxabs_bits,
             &hdr->flags);
     int err = check_launch("tc source amplitudes");
@@ -3200,6 +3226,81 @@ int l6_block(int casa, int num_sources, int num_stations, int offset_out,
     return check_launch("tc64 gemm");
 }
 
+// Workspace of the FP32 entry point: Header, order tables, the integer
+// image, FP64 sums of the visibilities, FP64 station u and v.
+size_t tcf_workspace_bytes(int num_st, int num_src)
+{
+    const size_t nbl = (size_t) num_st * (num_st - 1) / 2;
+    return kHeaderBytes + i8_order_bytes(num_src, kI8DrainKb, nullptr,
+            nullptr) + image_bytes_i8(num_st, num_src) +
+            align256_t(nbl * 8 * sizeof(double)) +
+            2 * align256_t((size_t) num_st * sizeof(double));
+}
+
+// One FP32 J block through the integer form.
+int tcf_block(int casa, int num_sources, int num_stations, int offset_out,
+        const float* jones, const float* I, const float* Q, const float* U,
+        const float* V, const float* station_u, const float* station_v,
+        double uv_min_lambda, double uv_max_lambda, double inv_wavelength,
+        float* vis, uint8_t* ws, cudaStream_t s)
+{
+    bool wide_fits = false, pair_fits = false;
+    int err = device_setup(wide_fits, pair_fits);
+    if (err) return err;
+    Header* hdr = reinterpret_cast<Header*>(ws);
+    const size_t nbl = (size_t) num_stations * (num_stations - 1) / 2;
+    I8Order o;
+    uint8_t* W = ws + kHeaderBytes + i8_order_bytes(num_sources, kI8DrainKb,
+            ws + kHeaderBytes, &o);
+    double* sums = reinterpret_cast<double*>(W +
+            image_bytes_i8(num_stations, num_sources));
+    double* du = reinterpret_cast<double*>(reinterpret_cast<uint8_t*>(sums)
+            + align256_t(nbl * 8 * sizeof(double)));
+    double* dv = reinterpret_cast<double*>(reinterpret_cast<uint8_t*>(du) +
+            align256_t((size_t) num_stations * sizeof(double)));
+    if (cudaMemsetAsync(hdr, 0, sizeof(Header), s) != cudaSuccess ||
+            cudaMemsetAsync(sums, 0, nbl * 8 * sizeof(double), s) !=
+            cudaSuccess)
+    {
+        set_last_error("tc (FP32) clear", cudaGetLastError());
+        return OSKB_ERR_KERNEL_LAUNCH_FAILURE;
+    }
+    widen_uv_kernel<<<(num_stations + 255) / 256, 256, 0, s>>>(num_stations,
+            station_u, station_v, du, dv);
+    if ((err = check_launch("tc (FP32) uv"))) return err;
+    if ((err = i8_order<float, float>(jones, num_sources, num_stations, I, Q,
+            U, V, hdr, o, s)))
+        return err;
+    const int nrb = (num_stations + kStPerBlock - 1) / kStPerBlock;
+    const int cap = i8_kb_cap(num_sources);
+    prep_jones_i8_kernel<float><<<dim3(cap, nrb), 256, 0, s>>>(jones,
+            num_sources, num_stations, I, Q, U, V, &hdr->maxabs_bits, o, W);
+    if ((err = check_launch("tc (FP32) prep"))) return err;
+    GemmParams gp;
+    gp.i8 = 1;
+    gp.form = kFormI8;
+    gp.i8_counts = o.counts;
+    gp.i8_chunk_kb = o.chunk_kb;
+    gp.i8_chunk_bucket = o.chunk_bucket;
+    gp.skip_flags = &hdr->flags;
+    gp.W = W; gp.image_stride = 0; gp.nrb = nrb; gp.nkb = cap;
+    gp.num_problems = 1; gp.num_st = num_stations;
+    gp.maxabs_bits = &hdr->maxabs_bits; gp.maxabs_stride = 0;
+    gp.prob0 = 0; gp.nch = 1;
+    gp.vis = sums; gp.vis_stride = 0; gp.offset_out = 0;
+    gp.st_u = du; gp.st_v = dv; gp.uv_stride = 0;
+    gp.inv_wavelength = nullptr; gp.kw_scalar = inv_wavelength;
+    gp.uv_min = uv_min_lambda; gp.uv_max = uv_max_lambda;
+    gp.casa = casa; gp.err = &hdr->err; gp.autos = nullptr;
+    if ((err = launch_gemm(gp, s))) return err;
+    const size_t n = nbl * 8;
+    const int grid = (int) std::min<size_t>((n + 255) / 256,
+            (size_t) num_sms() * 8);
+    add_vis_f_kernel<<<grid, 256, 0, s>>>(n, sums,
+            vis + 8 * (size_t) offset_out);
+    return check_launch("tc (FP32) add");
+}
+
 // The FP64-class block (oskb_correlate_block_tc64_d): as correlate_block
 // with the six-limb image. Workspace: Header, tables, group x image.
 int correlate_block_l6(int casa, int num_sources, int num_stations,
@@ -3322,6 +3423,36 @@ int oskb_cross_correlate_tc_d(int casa, int num_sources, int num_stations,
     if (err) return err;
     return jones_block(casa, num_sources, num_stations, offset_out, jones, I,
             Q, U, V, station_u, station_v, uv_min_lambda, uv_max_lambda,
+            inv_wavelength, vis, reinterpret_cast<uint8_t*>(workspace), s);
+}
+
+size_t oskb_cross_correlate_tc_f_workspace_bytes(int num_sources,
+        int num_stations)
+{
+    if (num_sources <= 0 || num_stations <= 0) return kHeaderBytes;
+    return tcf_workspace_bytes(num_stations, num_sources);
+}
+
+int oskb_cross_correlate_tc_f(int casa, int num_sources, int num_stations,
+        int offset_out, const float* jones, const float* I, const float* Q,
+        const float* U, const float* V, const float* station_u,
+        const float* station_v, float uv_min_lambda, float uv_max_lambda,
+        float inv_wavelength, float* vis, void* workspace,
+        size_t workspace_bytes, void* stream)
+{
+    if (num_sources < 0 || num_stations < 0) return OSKB_ERR_INVALID_ARGUMENT;
+    if (num_sources == 0 || num_stations < 2) return 0;
+    if (!jones || !I || !Q || !U || !V || !station_u || !station_v || !vis)
+        return OSKB_ERR_INVALID_ARGUMENT;
+    // 16 B per element of J: whole elements
+    if ((uintptr_t) jones % 16 != 0) return OSKB_ERR_INVALID_ARGUMENT;
+    const size_t need = oskb_cross_correlate_tc_f_workspace_bytes(
+            num_sources, num_stations);
+    cudaStream_t s = as_stream(stream);
+    int err = get_workspace(workspace, workspace_bytes, need, s);
+    if (err) return err;
+    return tcf_block(casa, num_sources, num_stations, offset_out, jones, I, Q,
+            U, V, station_u, station_v, uv_min_lambda, uv_max_lambda,
             inv_wavelength, vis, reinterpret_cast<uint8_t*>(workspace), s);
 }
 

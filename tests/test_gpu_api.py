@@ -115,6 +115,26 @@ def test_cross_correlate_fp64_class_env(psd, monkeypatch):
     assert flags[0] == (0 if psd else 1) and flags[1] == 0
 
 
+@pytest.mark.parametrize("psd", [True, False])
+def test_cross_correlate_tensor_core_env_fp32(psd, monkeypatch):
+    """OSKAR_CORRELATE=TC routes FP32 point sources without smearing to the
+    integer tensor-core form (FP32 in and out, within FP32's 1e-5); a
+    brightness matrix that is not positive semi-definite sends the call to
+    the direct kernel."""
+    c = XcorrCase(60, 900, real=np.float32, ranges="physical", seed=6)
+    if not psd:
+        c.Q[3] = 3.0 * c.I[3]
+    monkeypatch.setenv("OSKAR_CORRELATE", "TC")
+    got = run_api(c, S, 1.0, 0.0, 0)
+    ref = c.vis0.copy()
+    oracle().call("xcorr_matrix_f", np.float32, 0, 0, *c.oracle_args(ref))
+    assert rel(got - c.vis0, ref - c.vis0) <= 1e-5
+    flags = (oa.ctypes.c_int * 2)()
+    assert load().oskb_tc_status(None, oa.ctypes.addressof(flags),
+                                 oa.ctypes.addressof(flags) + 4) == 0
+    assert flags[0] == (0 if psd else 1) and flags[1] == 0
+
+
 def test_jones_join_identity_known_answer():
     """Test_Jones.cpp:187-286: joining with identity leaves Jones unchanged,
     in place and out of place, matrix x matrix and scalar x matrix."""

@@ -395,3 +395,60 @@ def test_tc_block_auto_correlations_fused(form, monkeypatch):
                           Q, U, V, ref)
             l2, mx = errors(got[t, c], ref)
             assert l2 <= TOL and mx <= TOL, (t, c, l2, mx)
+
+
+@pytest.mark.parametrize("nst,nsrc,casa", [(2, 1, 0), (33, 64, 1),
+                                           (64, 1000, 0), (130, 777, 1)])
+def test_tc_fp32_entry(nst, nsrc, casa):
+    """oskb_cross_correlate_tc_f: FP32 J, fluxes, u, v and visibilities
+    (as oskb_cross_correlate_f takes them), the integer form's sums added
+    into the FP32 visibilities; against the oracle run on the same
+    FP32-rounded inputs, to 1e-6, over two calls in a row (the second adds
+    to the first) with an output offset."""
+    rng = np.random.default_rng(5 * nst + nsrc)
+    l, m, n, I, Q, U, V = sky(rng, nsrc)
+    u, v, w = stations(rng, nst)
+    J = rng.normal(0, 0.3, (nst, nsrc, 8))
+    J[..., 0] += 1
+    J[..., 6] += 1
+    f32 = lambda a: np.asarray(a, np.float32)
+    J32, I32, Q32, U32, V32, u32, v32 = map(f32, (J.ravel(), I, Q, U, V, u,
+                                                  v))
+    inv_wl = np.float32(110e6 / C0)
+    up = lambda a: a.astype(np.float64)
+    ref = oracle_vis(nst, nsrc, up(J32), up(I32), up(Q32), up(U32), up(V32),
+                     l, m, n, up(u32), up(v32), w, float(inv_wl), casa=casa,
+                     offset_out=1)
+    nbl = nst * (nst - 1) // 2
+    vis = torch.zeros(8 * (nbl + 1), dtype=torch.float32, device="cuda")
+    for _ in range(2):
+        ob.call("oskb_cross_correlate_tc_f", casa, nsrc, nst, 1, dev(J32),
+                dev(I32), dev(Q32), dev(U32), dev(V32), dev(u32), dev(v32),
+                0.0, 3e38, inv_wl, vis, None, 0, ob.stream_ptr())
+    torch.cuda.synchronize()
+    got = vis.cpu().numpy().astype(np.float64)
+    assert not np.any(got[:8])
+    l2, mx = errors(got[8:], 2 * ref[8:])
+    assert l2 <= TOL and mx <= TOL, (l2, mx)
+
+
+def test_tc_fp32_entry_not_psd():
+    rng = np.random.default_rng(66)
+    nst, nsrc = 20, 200
+    l, m, n, I, Q, U, V = sky(rng, nsrc)
+    Q = Q.copy()
+    Q[9] = 2.5 * I[9]
+    u, v, w = stations(rng, nst)
+    J = rng.normal(0, 0.3, (nst, nsrc, 8)).astype(np.float32)
+    f32 = lambda a: dev(np.asarray(a, np.float32))
+    nbl = nst * (nst - 1) // 2
+    vis = torch.zeros(8 * nbl, dtype=torch.float32, device="cuda")
+    ob.call("oskb_cross_correlate_tc_f", 0, nsrc, nst, 0, dev(J), f32(I),
+            f32(Q), f32(U), f32(V), f32(u), f32(v), 0.0, 3e38, 1.0, vis,
+            None, 0, ob.stream_ptr())
+    torch.cuda.synchronize()
+    flags = (ob._lib.ctypes.c_int * 2)()
+    ob.call("oskb_tc_status", None, ob._lib.ctypes.addressof(flags),
+            ob._lib.ctypes.addressof(flags) + 4)
+    assert flags[0] & 1 and flags[1] == 0
+    assert not np.any(vis.cpu().numpy())
