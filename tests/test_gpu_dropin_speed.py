@@ -88,3 +88,34 @@ def test_dropin_c3_shape(tmp_path):
             json.dump(res, f, indent=1)
     print(json.dumps(res))
     assert gpu > 20 * cpu, res
+
+
+def test_dropin_c3_shape_fp32(tmp_path):
+    """The FP32 C3-shaped case through the drop-in, timed with the FP32
+    point-source correlation on the integer tensor-core form (the default)
+    and on the FP32 direct kernel (OSKB_DROPIN_TC32=0): three runs, the
+    integer form first (cold start) and last. The warm integer-form run
+    must not be slower than the direct one. Set OSKB_DROPIN_SPEED_OUT_FP32
+    to a path to keep the numbers (JSON)."""
+    need_ref()
+    full = c3_shaped_case("single")
+    runs = []
+    for tag, flag in (("tc32", "1"), ("direct_f32", "0"),
+                      ("tc32_again", "1")):
+        os.environ["OSKB_DROPIN_TC32"] = flag
+        try:
+            t = float(sim(full, tmp_path, tag, dropin=True)
+                      ["run_seconds"][0])
+        finally:
+            del os.environ["OSKB_DROPIN_TC32"]
+        runs.append({"run": tag, "seconds": t,
+                     "value": NBL * 100_000 * 16 * 4 / t / 1e9})
+    res = {"unit": "G source-baselines/s",
+           "case": "512 stations x 100,000 sources x 16 channels x 4 dumps, "
+                   "FP32, sky chunks of 16,384", "runs": runs}
+    path = os.environ.get("OSKB_DROPIN_SPEED_OUT_FP32")
+    if path:
+        with open(path, "w") as f:
+            json.dump(res, f, indent=1)
+    print(json.dumps(res))
+    assert runs[2]["seconds"] <= runs[1]["seconds"], res
