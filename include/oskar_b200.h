@@ -934,6 +934,21 @@ OSKB_API int oskb_correlate_block_tc64_d(int use_casa_phase_convention,
         double uv_min_lambda, double uv_max_lambda, double* vis,
         void* workspace, size_t workspace_bytes, void* stream);
 
+/* The same, with the auto-correlations of every station from the same
+ * contraction (the diagonal station pairs of the diagonal tiles, V_pp =
+ * J_p B J_p^H) added into autos [num_times][num_channels][num_stations]
+ * [2x2] FP64, as oskb_correlate_block_tc_auto does for the 1e-6 form
+ * (the reference's oskar_auto_correlate per (dump, channel),
+ * oskar/correlate/define_auto_correlate.h:8-82). */
+OSKB_API int oskb_correlate_block_tc64_auto_d(int use_casa_phase_convention,
+        int num_sources, int num_stations, int num_times, int num_channels,
+        const double* E, const double* l, const double* m, const double* n,
+        const double* I, const double* Q, const double* U, const double* V,
+        const double* station_uvw, const double* inv_wavelength,
+        double uv_min_lambda, double uv_max_lambda, double* vis,
+        double* autos, void* workspace, size_t workspace_bytes,
+        void* stream);
+
 /* Direct (FP64 or FP32) block correlator with smearing: for every (dump t,
  * channel c) of a block, in ONE persistent launch,
  *   vis[t][c][pq] += sum_s smear_pq(s) (J_p B J_q^H)(s),  J = K(t, c) E,

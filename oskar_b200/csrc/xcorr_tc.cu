@@ -3308,7 +3308,7 @@ int correlate_block_l6(int casa, int num_sources, int num_stations,
         const double* m, const double* n, const double* I, const double* Q,
         const double* U, const double* V, const double* station_uvw,
         const double* inv_wavelength, double uv_min_lambda,
-        double uv_max_lambda, double* vis, void* workspace,
+        double uv_max_lambda, double* vis, double* autos, void* workspace,
         size_t workspace_bytes, cudaStream_t s)
 {
     const int num_problems = num_times * num_channels;
@@ -3378,7 +3378,7 @@ int correlate_block_l6(int casa, int num_sources, int num_stations,
         gp.uv_stride = 3 * (size_t) num_stations;
         gp.inv_wavelength = inv_wavelength; gp.kw_scalar = 0.0;
         gp.uv_min = uv_min_lambda; gp.uv_max = uv_max_lambda;
-        gp.casa = casa; gp.err = &hdr->err; gp.autos = nullptr;
+        gp.casa = casa; gp.err = &hdr->err; gp.autos = autos;
         const long long ntasks = (long long) nrb * (nrb + 1) * np;
         const int grid = (int) (ntasks < num_sms() ? ntasks : num_sms());
         cudaEvent_t ev_stop = timing_start(s);
@@ -3513,8 +3513,31 @@ int oskb_correlate_block_tc64_d(int casa, int num_sources, int num_stations,
         return OSKB_ERR_INVALID_ARGUMENT;
     return correlate_block_l6(casa, num_sources, num_stations, num_times,
             num_channels, E, l, m, n, I, Q, U, V, station_uvw,
-            inv_wavelength, uv_min_lambda, uv_max_lambda, vis, workspace,
-            workspace_bytes, as_stream(stream));
+            inv_wavelength, uv_min_lambda, uv_max_lambda, vis, nullptr,
+            workspace, workspace_bytes, as_stream(stream));
+}
+
+int oskb_correlate_block_tc64_auto_d(int casa, int num_sources,
+        int num_stations, int num_times, int num_channels, const double* E,
+        const double* l, const double* m, const double* n, const double* I,
+        const double* Q, const double* U, const double* V,
+        const double* station_uvw, const double* inv_wavelength,
+        double uv_min_lambda, double uv_max_lambda, double* vis,
+        double* autos, void* workspace, size_t workspace_bytes, void* stream)
+{
+    if (num_sources < 0 || num_stations < 0 || num_times < 0 ||
+            num_channels < 0)
+        return OSKB_ERR_INVALID_ARGUMENT;
+    if (num_sources == 0 || num_stations < 2 ||
+            num_times * num_channels == 0)
+        return 0;
+    if (!E || !l || !m || !n || !I || !Q || !U || !V || !station_uvw ||
+            !inv_wavelength || !vis || !autos)
+        return OSKB_ERR_INVALID_ARGUMENT;
+    return correlate_block_l6(casa, num_sources, num_stations, num_times,
+            num_channels, E, l, m, n, I, Q, U, V, station_uvw,
+            inv_wavelength, uv_min_lambda, uv_max_lambda, vis, autos,
+            workspace, workspace_bytes, as_stream(stream));
 }
 
 size_t oskb_correlate_block_tc_workspace_bytes(int num_sources,

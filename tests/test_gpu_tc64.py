@@ -230,3 +230,48 @@ def test_tc64_block_groups_and_not_psd():
                                      inv_wl)
     assert err == 0 and flags & 1
     assert not np.any(got)
+
+
+def test_tc64_block_auto_correlations():
+    """Auto-correlations from the FP64-class block contraction against the
+    oracle's auto-correlation of J = K E per (dump, channel), to 1e-12 (the
+    phase cancels in J_p B J_p^H); the cross visibilities are the same bits
+    as without them."""
+    rng = np.random.default_rng(97)
+    nst, nsrc, ntime, nchan = 70, 500, 2, 2
+    l, m, n, I, Q, U, V = sky(rng, nsrc)
+    E = rng.normal(0, 0.1, (nst, nsrc, 8))
+    E[..., 0] += 1
+    E[..., 6] += 1
+    uvw = np.stack([np.stack(stations(rng, nst, rmax=300.0))
+                    for _ in range(ntime)])
+    inv_wl = (100e6 + 7e6 * np.arange(nchan)) / C0
+    nbl = nst * (nst - 1) // 2
+    args = [dev(E), dev(l), dev(m), dev(n), dev(I), dev(Q), dev(U), dev(V),
+            dev(uvw), dev(inv_wl), 0.0, 3e38]
+    vis = torch.zeros(ntime * nchan * nbl * 8, dtype=torch.float64,
+                      device="cuda")
+    autos = torch.zeros(ntime * nchan * nst * 8, dtype=torch.float64,
+                        device="cuda")
+    ob.call("oskb_correlate_block_tc64_auto_d", 0, nsrc, nst, ntime, nchan,
+            *args, vis, autos, None, 0, ob.stream_ptr())
+    vis0 = torch.zeros_like(vis)
+    ob.call("oskb_correlate_block_tc64_d", 0, nsrc, nst, ntime, nchan, *args,
+            vis0, None, 0, ob.stream_ptr())
+    torch.cuda.synchronize()
+    assert torch.equal(vis, vis0)
+    got = autos.cpu().numpy().reshape(ntime, nchan, -1)
+    for t in range(ntime):
+        u, v, w = uvw[t]
+        for c in range(nchan):
+            K = np.zeros(2 * nst * nsrc)
+            oracle().call("jones_k_d", np.float64, nsrc, l, m, n, nst, u, v,
+                          w, 2 * np.pi * inv_wl[c], I, 0.0, 1e300, 0, K)
+            J = np.zeros(8 * nst * nsrc)
+            oracle().call("mem_mul_cm_m_d", np.float64, nst * nsrc, K,
+                          np.ascontiguousarray(E.ravel()), J)
+            ref = np.zeros(8 * nst)
+            oracle().call("acorr_matrix_d", np.float64, nsrc, nst, 0, J, I,
+                          Q, U, V, ref)
+            l2, mx = errors(got[t, c], ref)
+            assert l2 <= TOL and mx <= TOL, (t, c, l2, mx)
